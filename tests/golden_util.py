@@ -1,0 +1,23 @@
+"""Loading of the committed golden fixtures (tests/golden/*.npz, made by
+tests/golden/make_golden.py from runs of the reference itself)."""
+import json
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+CASES = ["quad_vortex_p3_n6", "quad_vortex_p2_n5_jit", "quad_vortex_p3_n20", "hex_tgv_p3_n3",
+         "hex_tgv_p2_n3_jit", "hex_tgv_p4_n2", "hex_euler_p3_n3"]
+
+
+def load(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    meta = json.loads(str(z["meta"]))
+    arrs = {k: np.asfortranarray(z[k]) for k in z.files if k != "meta"}
+    return meta, arrs
+
+
+def rel(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
