@@ -1,0 +1,270 @@
+#!/usr/bin/env python3
+"""Throughput of the FR residual + RK45 stage on B200.
+
+Workload: 3-D Taylor-Green vortex, compressible Navier-Stokes, periodic
+[0, 2pi]^3 hex mesh of 32^3 elements at P=3 (64 solution points per element,
+2.1 M points x 5 fields), Re 1600, Mach 0.1, Pr 0.71, Rusanov + LDG, c_dg
+correction, low-storage RK45.  One bench step = one full RK45 step (5 stages);
+the metric counts DOF updates per RK stage: n_eles * n_upts * n_fields * 5 per
+step.  Data: synthetic (the analytic TGV initial field); the working set
+(~1.2 GB) is larger than L2, so no L2 flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--precision fp64|fp32] [--n 32] [--order 3]
+
+Multi-GPU: one process per GPU (torchrun); every rank advances its own
+replica of the mesh (weak scaling, no data-path collective); the time is the
+max over ranks.  `--impl reference` times the reference's own CPU code
+(oracle/_ref, built from the reference sources) on the host cores.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+for sub in ("hifiles-solver_b200", "oracle"):
+    sys.path.insert(0, os.path.join(REPO, sub))
+
+METRIC = "RK-stage DOF-updates/s (TGV P=3)"
+GAMMA, MACH, RE, PR = 1.4, 0.1, 1600.0, 0.71
+
+
+def tgv_state(pos):
+    """TGV initial field, rho0 = U0 = 1, p0 = 1/(gamma M^2)."""
+    x, y, z = pos[..., 0], pos[..., 1], pos[..., 2]
+    p0 = 1.0 / (GAMMA * MACH * MACH)
+    p = p0 + 1.0 / 16.0 * (np.cos(2 * x) + np.cos(2 * y)) * (np.cos(2 * z) + 2.0)
+    u = np.sin(x) * np.cos(y) * np.cos(z)
+    v = -np.cos(x) * np.sin(y) * np.cos(z)
+    return np.asfortranarray(np.stack([np.ones_like(x), u, v, np.zeros_like(x),
+                                       p / (GAMMA - 1.0) + 0.5 * (u * u + v * v)], axis=-1))
+
+
+def alg_bytes_per_element(dims, P, viscous, s=8, m=8, t=8):
+    """Algorithmic HBM bytes per element per RK stage: state read+write and RK
+    register read+write, metrics once (JGinv + detJ at solution points, normal +
+    dA at flux points), and the face-trace exchange (each element writes its
+    own traces and reads its neighbours': U at flux points, plus grad U when
+    viscous)."""
+    n1 = P + 1
+    nu = n1 ** dims
+    nf = 2 * dims * n1 ** (dims - 1)
+    F = dims + 2
+    v = 1 if viscous else 0
+    return s * 4 * nu * F + m * (nu * (dims * dims + 1) + nf * (dims + 1)) + t * (2 * nf * F + v * 2 * nf * F * dims)
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        self.out.flush()
+        rows = [r.split(",") for r in open(self.out.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.out.name)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for nm, flag in zip(names, r[5:9]):
+                    if flag.strip().lower() in ("active", "1", "yes"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                pass
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json"))), "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def cpu_baseline_port(n=12, P=3, steps=2):
+    """The oracle (plain-C restatement, one core) on a bounded sample of the workload."""
+    import oracle as O
+    m = O.Mesh.box(3, P, (n, n, n), (0, 0, 0), (2 * np.pi,) * 3, vcjh_scheme=1)
+    ph = O.physics(viscous=1, gamma=GAMMA, prandtl=PR, mu_inf=1.0 / RE, tau=1.0, pen_fact=0.5)
+    u0 = tgv_state(m.geometry()["pos_upts"])
+    t0 = time.perf_counter()
+    m.rk45(ph, u0, 1e-3, steps, norms=False)
+    dt = time.perf_counter() - t0
+    dof = m.n_eles * m.n_upts * m.n_fields * 5 * steps
+    return {"value": dof / dt, "unit": "DOF-updates/s", "cores": 1, "kind": "port",
+            "sample": "oracle (C restatement), TGV P=3 NS on %d^3 hexes, %d RK45 steps, 1 thread, %.1f s" % (n, steps, dt)}
+
+
+def run_b200(a, rank, world, local):
+    import torch
+    import hifiles_b200 as H
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = local
+    n, P = a.n, a.order
+    L = 2 * np.pi
+    s = H.Solver.box(3, P, (n, n, n), (0, 0, 0), (L, L, L), viscous=True, vcjh_scheme=1, gamma=GAMMA, prandtl=PR,
+                     mu_inf=1.0 / RE, rt_inf=1.0, c_sth=1.0, fix_vis=1.0, tau=1.0, pen_fact=0.5,
+                     precision=1 if a.precision == "fp32" else 0, device=dev)
+    u0 = tgv_state(s.geometry()["pos_upts"])
+    s.set_state(u0)
+    dt = 1e-3
+    E, nu, F = s.n_eles, s.n_upts, s.n_fields
+    dof_step = E * nu * F * 5
+    stream = torch.cuda.ExternalStream(s.stream(), device=dev)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda:%d" % dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    # --- device-resident throughput (graph-replayed RK45 steps)
+    s.advance(max(a.warmup, 3), dt)
+    s.sync()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = s.launch_count()
+    with Clocks(dev) as clk:
+        torch.cuda.synchronize(dev)
+        ev0.record(stream)
+        s.advance(a.steps, dt)
+        ev1.record(stream)
+        ev1.synchronize()
+        torch.cuda.synchronize(dev)
+    launches = s.launch_count() - l0
+    ms = ev0.elapsed_time(ev1) / a.steps
+    barrier()
+    ms = max_over_ranks(ms)
+    value = dof_step * world / (ms * 1e-3)
+
+    # --- per-kernel event timing for the roofline (stage by stage, not replayed)
+    ms_grad, ms_flux = s.profile_stage(10, dt)
+    stage_ms = ms_grad + ms_flux
+    pk, pk_src = peaks()
+    tc = 4 if a.precision == "fp32" else 8
+    b_elem = alg_bytes_per_element(3, P, True, s=8, m=tc, t=tc)
+    achieved = b_elem * E / (stage_ms * 1e-3) / 1e9
+    traffic = None
+    tr_path = os.path.join(REPO, "profiles", "traffic_tgv_p%d_%s.json" % (P, a.precision))
+    if os.path.exists(tr_path):
+        tr = json.load(open(tr_path))
+        traffic = tr["bytes_per_element_per_stage"] * E
+
+    # --- end to end through the public API with host buffers
+    pinned = torch.empty(u0.size, dtype=torch.float64, pin_memory=True)
+    host_u = pinned.numpy().reshape(u0.shape, order="F")
+    host_u[...] = u0
+    s.set_state(host_u)
+    s.advance(1, dt, norms=True)
+    torch.cuda.synchronize(dev)
+    barrier()
+    e2e_steps = max(1, min(a.steps, 10))
+    t0 = time.perf_counter()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        s.set_state(host_u)
+        s.advance(1, dt, norms=True)
+    e1.record(stream)
+    e1.synchronize()
+    wall = (time.perf_counter() - t0) / e2e_steps
+    e2e_ms = max_over_ranks(max(e0.elapsed_time(e1) / e2e_steps, wall * 1e3))
+    e2e = {"value": dof_step * world / (e2e_ms * 1e-3), "unit": "DOF-updates/s",
+           "h2d_bytes_per_step": int(u0.size * 8), "d2h_bytes_per_step": int(F * 8),
+           "ms_per_step": e2e_ms,
+           "path": "Solver.set_state(pinned host state) + Solver.advance(1 step, norms) -> C ABI"}
+
+    cpu = cpu_baseline_port() if (rank == 0 and world == 1 and not a.no_cpu) else None
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    out = {
+        "metric": METRIC, "value": value, "unit": "DOF-updates/s", "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if a.precision == "fp64" else "f32 (f64 state/RK/reductions)",
+        "data": "synthetic (analytic TGV initial field)",
+        "config": {"workload": "TGV %d^3 hex P=%d Navier-Stokes (Re 1600, Mach 0.1, Pr 0.71), Rusanov+LDG, "
+                               "c_dg, RK45; 1 step = 5 RK stages" % (n, P),
+                   "n_eles": E, "n_upts": nu, "n_fields": F, "dof_per_stage": E * nu * F,
+                   "precision": a.precision, "l2": "inputs larger than L2 (working set ~%.2f GB)" %
+                                                    ((E * nu * F * 8 * 2 + E * 96 * F * tc * 2 + E * 96 * 15 * tc +
+                                                      E * nu * 10 * tc) / 1e9),
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "roofline": {"bound": "hbm", "kernel": "one RK stage = fr_grad_kernel + fr_flux_kernel",
+                     "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / pk["hbm_gbs"], "peak_source": pk_src,
+                     "alg_bytes_per_element": b_elem, "traffic": traffic,
+                     "ms_grad": ms_grad, "ms_flux": ms_flux},
+        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
+    }
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--n", type=int, default=32)
+    ap.add_argument("--order", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true")
+    a = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        import bench_reference
+        bench_reference.run(a)
+        return
+    run_b200(a, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,561 @@
+// fr_fused.cuh -- fused, sum-factorised FR stage kernels for tensor-product
+// elements (quadrilaterals D=2, hexahedra D=3) on sm_100a.
+//
+// One RK stage of the reference (CalcResidual, src/solver.cpp:65-225, then
+// eles::AdvanceSolution, src/eles.cpp:1091-1188) runs as
+//   viscous :  fr_grad_kernel  -> fr_flux_kernel
+//   inviscid:                     fr_flux_kernel
+// Both are element-blocked: a CTA owns EPB elements, stages their solution in
+// shared memory, and applies the reference's operators as 1-D line
+// contractions (every dense operator opp_0..opp_6 of a Gauss-point tensor
+// element has exactly one non-trivial factor per line, so the contraction
+// reproduces the dense product term by term).  Elements exchange data only
+// through flux-point traces in HBM:
+//   UF  (n_fpts, n_eles, F)      solution at the flux points, double-buffered
+//                                across stages (written by the stage update)
+//   GF  (n_fpts, n_eles, F, D)   corrected physical gradient at flux points
+//   RP  (n_upts, n_eles, F)      divergence of the discontinuous flux minus its
+//                                own flux-point correction (viscous path)
+// mate[i] is the flat index (fpt + n_fpts*ele) of the matching point across
+// the interface; side[i] bit 0 = this side is the left one, bit 1 = the LDG
+// penalty sign is negative.  Both sides evaluate the common flux with the
+// left/right roles and the left normal nL, so the two copies are identical.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "fr_physics.cuh"
+
+namespace frb {
+
+constexpr int kMaxN1 = 6;   // P <= 5 in the fused kernels
+
+template <typename T>
+struct Line {               // 1-D operator pieces (see Line1D in fr_host.hpp)
+  T Lm[kMaxN1], Lp[kMaxN1], D[kMaxN1][kMaxN1], gL[kMaxN1], gR[kMaxN1], w[kMaxN1];
+};
+
+template <int DIM, int P>
+struct Shape {
+  static constexpr int N1 = P + 1;
+  static constexpr int NU = DIM == 2 ? N1 * N1 : N1 * N1 * N1;
+  static constexpr int NFPF = DIM == 2 ? N1 : N1 * N1;
+  static constexpr int NFACE = 2 * DIM;
+  static constexpr int NF = NFACE * NFPF;
+  static constexpr int F = DIM + 2;
+};
+
+// Line through flux point f: first solution point, stride along the line,
+// axis, and whether the face is at the +1 end.  Reference orderings:
+// quads src/eles_quads.cpp:259-300, hexes src/eles_hexas.cpp:262-324.
+template <int DIM, int P>
+__device__ __forceinline__ void fpt_line(int f, int& u0, int& stride, int& axis, bool& plus)
+{
+  constexpr int N1 = P + 1;
+  if (DIM == 2) {
+    int fc = f / N1, j = f - fc * N1;
+    switch (fc) {
+      case 0: u0 = j; stride = N1; axis = 1; plus = false; break;
+      case 1: u0 = N1 * j; stride = 1; axis = 0; plus = true; break;
+      case 2: u0 = P - j; stride = N1; axis = 1; plus = true; break;
+      default: u0 = N1 * (P - j); stride = 1; axis = 0; plus = false; break;
+    }
+  } else {
+    constexpr int N2 = N1 * N1;
+    int fc = f / N2, r = f - fc * N2, j = r / N1, k = r - j * N1;
+    switch (fc) {
+      case 0: u0 = (P - k) + N1 * j; stride = N2; axis = 2; plus = false; break;
+      case 1: u0 = k + N2 * j; stride = N1; axis = 1; plus = false; break;
+      case 2: u0 = N1 * k + N2 * j; stride = 1; axis = 0; plus = true; break;
+      case 3: u0 = (P - k) + N2 * j; stride = N1; axis = 1; plus = true; break;
+      case 4: u0 = N1 * (P - k) + N2 * j; stride = 1; axis = 0; plus = false; break;
+      default: u0 = k + N1 * j; stride = N2; axis = 2; plus = true; break;
+    }
+  }
+}
+
+// Flux point of face fc on the line through solution point (a, b, c), and the
+// index of that point along the face normal.
+template <int DIM, int P>
+__device__ __forceinline__ int face_fpt(int fc, int a, int b, int c, int& along)
+{
+  constexpr int N1 = P + 1;
+  if (DIM == 2) {
+    switch (fc) {
+      case 0: along = b; return a;
+      case 1: along = a; return N1 + b;
+      case 2: along = b; return 2 * N1 + (P - a);
+      default: along = a; return 3 * N1 + (P - b);
+    }
+  }
+  constexpr int N2 = N1 * N1;
+  switch (fc) {
+    case 0: along = c; return (P - a) + N1 * b;
+    case 1: along = b; return N2 + a + N1 * c;
+    case 2: along = a; return 2 * N2 + b + N1 * c;
+    case 3: along = b; return 3 * N2 + (P - a) + N1 * c;
+    case 4: along = a; return 4 * N2 + (P - b) + N1 * c;
+    default: along = c; return 5 * N2 + a + N1 * b;
+  }
+}
+
+// axis and end of face fc (reference normals: quads f0 -y, f1 +x, f2 +y, f3 -x;
+// hexes f0 -z, f1 -y, f2 +x, f3 +y, f4 -x, f5 +z)
+template <int DIM>
+__device__ __forceinline__ bool face_plus(int fc)
+{
+  if (DIM == 2) return fc == 1 || fc == 2;
+  return fc == 2 || fc == 3 || fc == 5;
+}
+template <int DIM>
+__device__ __forceinline__ int face_axis(int fc)
+{
+  if (DIM == 2) return (fc == 1 || fc == 3) ? 0 : 1;
+  return (fc == 2 || fc == 4) ? 0 : ((fc == 1 || fc == 3) ? 1 : 2);
+}
+
+// value at flux point f of a field stored point-major in shared memory
+// (s[u * stride_s]); explicit FMAs keep every call site bit-identical.
+template <int DIM, int P, typename T, typename S>
+__device__ __forceinline__ T line_interp(const Line<T>& L, const S* s, int sst, int f)
+{
+  int u0, st, ax; bool plus;
+  fpt_line<DIM, P>(f, u0, st, ax, plus);
+  T acc = T(0);
+#pragma unroll
+  for (int m = 0; m <= P; m++) acc = ffma((T)s[(u0 + m * st) * sst], plus ? L.Lp[m] : L.Lm[m], acc);
+  return acc;
+}
+
+template <int DIM, int P>
+__device__ __forceinline__ void upt_abc(int u, int& a, int& b, int& c)
+{
+  constexpr int N1 = P + 1;
+  if (DIM == 2) { b = u / N1; a = u - b * N1; c = 0; }
+  else { c = u / (N1 * N1); int r = u - c * N1 * N1; b = r / N1; a = r - b * N1; }
+}
+
+template <int DIM, int P>
+__device__ __forceinline__ int upt_stride(int axis)
+{
+  constexpr int N1 = P + 1;
+  return axis == 0 ? 1 : (axis == 1 ? N1 : N1 * N1);
+}
+
+// ---------------------------------------------------------------------------
+// Initial flux-point traces from the state (used once after the state is set).
+template <int DIM, int P, typename TC>
+__global__ void fr_trace_kernel(const double* __restrict__ U, TC* __restrict__ UF, long long E, Line<TC> L)
+{
+  using S = Shape<DIM, P>;
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= E * S::NF) return;
+  long long e = i / S::NF;
+  int f = (int)(i - e * S::NF);
+#pragma unroll
+  for (int k = 0; k < S::F; k++) {
+    const double* ue = U + (size_t)S::NU * (e + E * k);
+    UF[f + (size_t)S::NF * (e + E * k)] = line_interp<DIM, P, TC, double>(L, ue, 1, f);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Viscous part 1: LDG common solution -> corrected gradient at solution points
+// (calculate_gradient + correct_gradient, src/eles.cpp:1667-1968) -> gradient
+// traces (extrapolate_corrected_gradient, src/eles.cpp:1973-2052); total
+// discontinuous flux (evaluate_invFlux + evaluate_viscFlux) -> its divergence
+// (calculate_divergence) minus the correction of its own normal component
+// (the norm_tdisf_fpts half of calculate_corrected_divergence).
+template <int DIM, int P, int EPB, int NT, typename TC>
+__global__ void __launch_bounds__(NT)
+fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const int* __restrict__ mate,
+               const unsigned char* __restrict__ side, const TC* __restrict__ JG, const TC* __restrict__ detj,
+               TC* __restrict__ GF, TC* __restrict__ RP, long long E, Line<TC> L, PhysT<TC> ph)
+{
+  using S = Shape<DIM, P>;
+  constexpr int NU = S::NU, NF = S::NF, F = S::F, D = DIM;
+  __shared__ TC sU[EPB][F][NU];
+  __shared__ TC sX[EPB][F][NF];          // delta_disu_fpts, later norm_tdisf_fpts
+  __shared__ TC sG[EPB][F * D][NU];      // physical gradient, component k + F*d
+  __shared__ TC sFl[EPB][D][F][NU];      // transformed total flux
+  const long long e0 = (long long)blockIdx.x * EPB;
+
+  for (int w = threadIdx.x; w < EPB * F * NU; w += NT) {
+    int el = w / (F * NU), r = w - el * F * NU, k = r / NU, u = r - k * NU;
+    long long e = e0 + el;
+    sU[el][k][u] = e < E ? (TC)U[u + (size_t)NU * (e + E * k)] : TC(1);
+  }
+  __syncthreads();
+
+  // LDG common solution u_c = (uL+uR)/2 - beta (uL-uR); delta = u_c - u_own
+  // (int_inters::calculate_common_invFlux + ldg_solution, src/int_inters.cpp:331-350)
+  for (int w = threadIdx.x; w < EPB * NF; w += NT) {
+    int el = w / NF, f = w - el * NF;
+    long long e = e0 + el;
+    if (e >= E) continue;
+    size_t own = f + (size_t)NF * e;
+    int mt = mate[own];
+    unsigned char sd = side[own];
+    TC pen = (sd & 2) ? -ph.pen_fact : ph.pen_fact;
+#pragma unroll
+    for (int k = 0; k < F; k++) {
+      TC uo = line_interp<DIM, P, TC, TC>(L, &sU[el][k][0], 1, f);
+      TC un = UF[mt + (size_t)NF * E * k];
+      TC ul = (sd & 1) ? uo : un, ur = (sd & 1) ? un : uo;
+      TC uc = TC(0.5) * (ul + ur) - pen * (ul - ur);
+      sX[el][k][f] = uc - uo;
+    }
+  }
+  __syncthreads();
+
+  for (int w = threadIdx.x; w < EPB * NU; w += NT) {
+    int el = w / NU, u = w - el * NU;
+    long long e = e0 + el;
+    if (e >= E) continue;
+    int abc[3];
+    upt_abc<DIM, P>(u, abc[0], abc[1], abc[2]);
+    // reference gradient opp_4 U + opp_5 delta (faces of each axis in index order)
+    TC gr[F][D];
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      const int st = upt_stride<DIM, P>(d);
+      const int i = abc[d];
+      const int ub = u - i * st;
+      int fm, fp, am, ap;
+      if (DIM == 2) { fm = d == 0 ? 3 : 0; fp = d == 0 ? 1 : 2; }
+      else { fm = d == 0 ? 4 : (d == 1 ? 1 : 0); fp = d == 0 ? 2 : (d == 1 ? 3 : 5); }
+      int qm = face_fpt<DIM, P>(fm, abc[0], abc[1], abc[2], am);
+      int qp = face_fpt<DIM, P>(fp, abc[0], abc[1], abc[2], ap);
+      const bool minus_first = fm < fp;
+#pragma unroll
+      for (int k = 0; k < F; k++) {
+        TC acc = TC(0);
+#pragma unroll
+        for (int m = 0; m <= P; m++) acc = ffma(sU[el][k][ub + m * st], L.D[i][m], acc);
+        TC cm = L.gL[am] * sX[el][k][qm], cp = L.gR[ap] * sX[el][k][qp];
+        acc = minus_first ? (acc + cm) + cp : (acc + cp) + cm;
+        gr[k][d] = acc;
+      }
+    }
+    // physical gradient (JGinv^T grad_ref / detJ), src/eles.cpp:1822-1878
+    const TC* G = JG + (size_t)D * D * (u + (size_t)NU * e);
+    TC Gm[D][D];
+#pragma unroll
+    for (int r = 0; r < D; r++)
+#pragma unroll
+      for (int c = 0; c < D; c++) Gm[r][c] = G[r + D * c];
+    TC inv = TC(1) / detj[u + (size_t)NU * e];
+    TC gp[F][D];
+#pragma unroll
+    for (int k = 0; k < F; k++)
+#pragma unroll
+      for (int c = 0; c < D; c++) {
+        TC acc = TC(0);
+#pragma unroll
+        for (int r = 0; r < D; r++) acc = ffma(gr[k][r], Gm[r][c] * inv, acc);
+        gp[k][c] = acc;
+        sG[el][k + F * c][u] = acc;
+      }
+    // total discontinuous flux transformed to the reference element
+    TC q[F];
+#pragma unroll
+    for (int k = 0; k < F; k++) q[k] = sU[el][k][u];
+    TC fi[F][D], fv[F][D];
+    inv_flux<D, TC>(ph, q, fi);
+    vis_flux<D, TC>(ph, q, gp, fv);
+#pragma unroll
+    for (int k = 0; k < F; k++)
+#pragma unroll
+      for (int l = 0; l < D; l++) {
+        TC acc = TC(0);
+#pragma unroll
+        for (int m = 0; m < D; m++) acc = ffma(Gm[l][m], fi[k][m], acc);
+#pragma unroll
+        for (int m = 0; m < D; m++) acc = ffma(Gm[l][m], fv[k][m], acc);
+        sFl[el][l][k][u] = acc;
+      }
+  }
+  __syncthreads();
+
+  // gradient traces and the discontinuous normal flux at the flux points
+  for (int w = threadIdx.x; w < EPB * NF; w += NT) {
+    int el = w / NF, f = w - el * NF;
+    long long e = e0 + el;
+    if (e >= E) continue;
+#pragma unroll
+    for (int c = 0; c < F * D; c++)
+      GF[f + (size_t)NF * (e + E * (size_t)c)] = line_interp<DIM, P, TC, TC>(L, &sG[el][c][0], 1, f);
+    int u0, st, ax; bool plus;
+    fpt_line<DIM, P>(f, u0, st, ax, plus);
+#pragma unroll
+    for (int k = 0; k < F; k++) {
+      TC v = line_interp<DIM, P, TC, TC>(L, &sFl[el][ax][k][0], 1, f);
+      sX[el][k][f] = plus ? v : -v;
+    }
+  }
+  __syncthreads();
+
+  for (int w = threadIdx.x; w < EPB * NU; w += NT) {
+    int el = w / NU, u = w - el * NU;
+    long long e = e0 + el;
+    if (e >= E) continue;
+    int abc[3];
+    upt_abc<DIM, P>(u, abc[0], abc[1], abc[2]);
+#pragma unroll
+    for (int k = 0; k < F; k++) {
+      TC acc = TC(0);
+#pragma unroll
+      for (int d = 0; d < D; d++) {
+        const int st = upt_stride<DIM, P>(d), i = abc[d], ub = u - i * st;
+#pragma unroll
+        for (int m = 0; m <= P; m++) acc = ffma(sFl[el][d][k][ub + m * st], L.D[i][m], acc);
+      }
+#pragma unroll
+      for (int fc = 0; fc < S::NFACE; fc++) {
+        int al;
+        int q = face_fpt<DIM, P>(fc, abc[0], abc[1], abc[2], al);
+        TC cf = face_plus<DIM>(fc) ? L.gR[al] : -L.gL[al];
+        acc = ffma(-cf, sX[el][k][q], acc);
+      }
+      RP[u + (size_t)NU * (e + E * k)] = acc;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Common interface fluxes (Rusanov + LDG), correction, and either the
+// residual (MODE 0) or the RK45 stage update with the next stage's traces
+// (MODE 1).  For the inviscid path this kernel also evaluates the flux and
+// its divergence itself (RP unused).
+template <int DIM, int P, int EPB, int NT, int VISC, int MODE, typename TC>
+__global__ void __launch_bounds__(NT)
+fr_flux_kernel(double* __restrict__ U, double* __restrict__ REG, const TC* __restrict__ UF,
+               TC* __restrict__ UFn, const TC* __restrict__ GF, const TC* __restrict__ RP,
+               const int* __restrict__ mate, const unsigned char* __restrict__ side, const TC* __restrict__ nL,
+               const TC* __restrict__ tdA, const TC* __restrict__ JG, const double* __restrict__ detj,
+               double* __restrict__ DIV, double* __restrict__ partial, long long E, Line<TC> L, PhysT<TC> ph,
+               double rk_a, double rk_b, double dt, int first_stage)
+{
+  using S = Shape<DIM, P>;
+  constexpr int NU = S::NU, NF = S::NF, F = S::F, D = DIM;
+  __shared__ double sU[EPB][F][NU];
+  __shared__ TC sC[EPB][F][NF];                       // common minus own normal flux
+  __shared__ TC sFl[VISC ? 1 : EPB][D][VISC ? 1 : NU][VISC ? 1 : F];
+  __shared__ double sRed[NT / 32][F];
+  const long long e0 = (long long)blockIdx.x * EPB;
+
+  for (int w = threadIdx.x; w < EPB * F * NU; w += NT) {
+    int el = w / (F * NU), r = w - el * F * NU, k = r / NU, u = r - k * NU;
+    long long e = e0 + el;
+    sU[el][k][u] = e < E ? U[u + (size_t)NU * (e + E * k)] : 1.0;
+  }
+  if (!VISC) {
+    __syncthreads();
+    // transformed inviscid flux at the solution points (evaluate_invFlux,
+    // src/eles.cpp:1331-1418)
+    for (int w = threadIdx.x; w < EPB * NU; w += NT) {
+      int el = w / NU, u = w - el * NU;
+      long long e = e0 + el;
+      if (e >= E) continue;
+      TC q[F], fi[F][D];
+#pragma unroll
+      for (int k = 0; k < F; k++) q[k] = (TC)sU[el][k][u];
+      inv_flux<D, TC>(ph, q, fi);
+      const TC* G = JG + (size_t)D * D * (u + (size_t)NU * e);
+#pragma unroll
+      for (int l = 0; l < D; l++) {
+        TC g[D];
+#pragma unroll
+        for (int m = 0; m < D; m++) g[m] = G[l + D * m];
+#pragma unroll
+        for (int k = 0; k < F; k++) {
+          TC acc = TC(0);
+#pragma unroll
+          for (int m = 0; m < D; m++) acc = ffma(g[m], fi[k][m], acc);
+          sFl[el][l][u][k] = acc;
+        }
+      }
+    }
+  }
+  __syncthreads();
+
+  // common normal flux at every flux point of the block's elements
+  for (int w = threadIdx.x; w < EPB * NF; w += NT) {
+    int el = w / NF, f = w - el * NF;
+    long long e = e0 + el;
+    if (e >= E) continue;
+    size_t own = f + (size_t)NF * e;
+    int mt = mate[own];
+    bool left = side[own] & 1;
+    TC uo[F], un[F], n[D];
+#pragma unroll
+    for (int k = 0; k < F; k++) {
+      uo[k] = line_interp<DIM, P, TC, double>(L, &sU[el][k][0], 1, f);
+      un[k] = UF[mt + (size_t)NF * E * k];
+    }
+#pragma unroll
+    for (int d = 0; d < D; d++) n[d] = nL[own + (size_t)NF * E * d];
+    const TC* ul = left ? uo : un;
+    const TC* ur = left ? un : uo;
+    TC fn[F];
+    rusanov<D, TC>(ph, ul, ur, n, fn);
+    TC ta = tdA[own];
+    TC c[F];
+#pragma unroll
+    for (int k = 0; k < F; k++) c[k] = left ? fn[k] * ta : -fn[k] * ta;
+    if (VISC) {
+      TC go[F][D], gn[F][D];
+#pragma unroll
+      for (int k = 0; k < F; k++)
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+          go[k][d] = GF[own + (size_t)NF * E * (k + F * d)];
+          gn[k][d] = GF[mt + (size_t)NF * E * (k + F * d)];
+        }
+      TC fo[F][D], fnb[F][D];
+      vis_flux<D, TC>(ph, uo, go, fo);
+      vis_flux<D, TC>(ph, un, gn, fnb);
+      TC fv[F];
+      TC pen = (side[own] & 2) ? -ph.pen_fact : ph.pen_fact;
+      if (left) ldg_flux<D, TC>(ph, pen, uo, un, fo, fnb, n, fv);
+      else ldg_flux<D, TC>(ph, pen, un, uo, fnb, fo, n, fv);
+#pragma unroll
+      for (int k = 0; k < F; k++) c[k] += left ? fv[k] * ta : -fv[k] * ta;
+    } else {
+      // subtract the discontinuous normal flux (extrapolate_totalFlux + daxpy)
+      int u0, st, ax; bool plus;
+      fpt_line<DIM, P>(f, u0, st, ax, plus);
+#pragma unroll
+      for (int k = 0; k < F; k++) {
+        TC acc = TC(0);
+#pragma unroll
+        for (int m = 0; m <= P; m++) acc = ffma(sFl[el][ax][u0 + m * st][k], plus ? L.Lp[m] : L.Lm[m], acc);
+        c[k] = c[k] + (plus ? -acc : acc);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < F; k++) sC[el][k][f] = c[k];
+  }
+  __syncthreads();
+
+  double red[F];
+#pragma unroll
+  for (int k = 0; k < F; k++) red[k] = 0.0;
+  for (int w = threadIdx.x; w < EPB * NU; w += NT) {
+    int el = w / NU, u = w - el * NU;
+    long long e = e0 + el;
+    if (e >= E) continue;
+    int abc[3];
+    upt_abc<DIM, P>(u, abc[0], abc[1], abc[2]);
+    double dj = detj[u + (size_t)NU * e];
+#pragma unroll
+    for (int k = 0; k < F; k++) {
+      TC acc;
+      if (VISC) {
+        acc = RP[u + (size_t)NU * (e + E * k)];
+      } else {
+        acc = TC(0);
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+          const int st = upt_stride<DIM, P>(d), i = abc[d], ub = u - i * st;
+#pragma unroll
+          for (int m = 0; m <= P; m++) acc = ffma(sFl[el][d][ub + m * st][k], L.D[i][m], acc);
+        }
+      }
+      // correction with the VCJH function derivatives (calculate_corrected_divergence)
+#pragma unroll
+      for (int fc = 0; fc < S::NFACE; fc++) {
+        int al;
+        int q = face_fpt<DIM, P>(fc, abc[0], abc[1], abc[2], al);
+        TC cf = face_plus<DIM>(fc) ? L.gR[al] : -L.gL[al];
+        acc = ffma(cf, sC[el][k][q], acc);
+      }
+      size_t gi = u + (size_t)NU * (e + E * k);
+      double R = (double)acc;
+      if (MODE == 0) {
+        DIV[gi] = R;
+      } else {
+        double rhs = -R / dj;
+        double res = first_stage ? dt * rhs : ffma(rk_a, REG[gi], dt * rhs);
+        REG[gi] = res;
+        double un = ffma(rk_b, res, sU[el][k][u]);
+        U[gi] = un;
+        sU[el][k][u] = un;
+        red[k] += fabs(R / dj);
+      }
+    }
+  }
+  if (MODE == 1) {
+    if (partial) {
+      // deterministic per-block partial sums of |div/detjac| (CalcNormResidual)
+      const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+      for (int k = 0; k < F; k++) {
+        double v = red[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) sRed[wid][k] = v;
+      }
+    }
+    __syncthreads();
+    if (partial && threadIdx.x < F) {
+      double v = 0.0;
+      for (int i = 0; i < NT / 32; i++) v += sRed[i][threadIdx.x];
+      partial[(size_t)blockIdx.x * F + threadIdx.x] = v;
+    }
+    // traces of the updated state for the next stage
+    for (int w = threadIdx.x; w < EPB * NF; w += NT) {
+      int el = w / NF, f = w - el * NF;
+      long long e = e0 + el;
+      if (e >= E) continue;
+#pragma unroll
+      for (int k = 0; k < F; k++)
+        UFn[f + (size_t)NF * (e + E * k)] = line_interp<DIM, P, TC, double>(L, &sU[el][k][0], 1, f);
+    }
+  }
+}
+
+// Block sums -> norms (fixed order, one thread per field).
+__global__ void fr_norm_finalize(const double* __restrict__ partial, int nblk, int F, double inv_n,
+                                 double* __restrict__ out)
+{
+  int k = threadIdx.x;
+  if (k >= F) return;
+  double s = 0.0;
+  for (int b = 0; b < nblk; b++) s += partial[(size_t)b * F + k];
+  out[k] = s * inv_n;
+}
+
+// Kinetic energy: per-element quadrature with the point weights, block partials.
+template <int DIM, int P>
+__global__ void fr_ke_kernel(const double* __restrict__ U, const double* __restrict__ detj, long long E,
+                             Line<double> L, double* __restrict__ partial)
+{
+  using S = Shape<DIM, P>;
+  __shared__ double sred[32];
+  double acc = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < E * S::NU;
+       i += (long long)gridDim.x * blockDim.x) {
+    long long e = i / S::NU;
+    int u = (int)(i - e * S::NU), a, b, c;
+    upt_abc<DIM, P>(u, a, b, c);
+    double w = L.w[a] * L.w[b] * (DIM == 3 ? L.w[c] : 1.0);
+    double rho = U[u + (size_t)S::NU * e], m2 = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      double mm = U[u + (size_t)S::NU * (e + E * (1 + d))];
+      m2 += mm * mm;
+    }
+    acc += w * detj[u + (size_t)S::NU * e] * 0.5 * m2 / rho;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); i++) s += sred[i];
+    partial[blockIdx.x] = s;
+  }
+}
+
+}  // namespace frb

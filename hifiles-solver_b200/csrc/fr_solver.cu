@@ -1,0 +1,591 @@
+// fr_solver.cu -- the fr_solver object behind the C ABI of include/fr_b200.h:
+// device buffers, template dispatch over (dims, order, precision), the RK45
+// driver with CUDA-graph replay, reductions.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "fr_b200.h"
+#include "fr_fused.cuh"
+#include "fr_host.hpp"
+
+namespace frb {
+
+thread_local std::string g_err;
+
+static fr_status fail(fr_status s, const std::string& msg)
+{
+  g_err = msg;
+  return s;
+}
+
+#define FR_CUDA(call)                                                                              \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess)                                                                         \
+      return fail(FR_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));                \
+  } while (0)
+
+// RK45 coefficients (Carpenter-Kennedy low-storage, eles::AdvanceSolution,
+// src/eles.cpp:1093-1113).
+static const double kRK4A[5] = {0.0, -0.417890474499852, -1.192151694642677, -1.697784692471528,
+                                -1.514183444257156};
+static const double kRK4B[5] = {0.149659021999229, 0.379210312999627, 0.822955029386982, 0.699450455949122,
+                                0.153057247968152};
+
+struct Bufs {
+  double *U = nullptr, *REG = nullptr, *DIV = nullptr, *detj64 = nullptr, *partial = nullptr, *norms = nullptr;
+  void *UF[2] = {nullptr, nullptr}, *GF = nullptr, *RP = nullptr, *nL = nullptr, *tdA = nullptr, *JG = nullptr,
+       *detj = nullptr;
+  int* mate = nullptr;
+  unsigned char* side = nullptr;
+};
+
+struct Runner {
+  virtual ~Runner() {}
+  virtual void trace(const Bufs& b, int cur, cudaStream_t s) = 0;
+  virtual void grad(const Bufs& b, int cur, cudaStream_t s) = 0;
+  virtual void flux(const Bufs& b, int cur, int mode, int stage, double dt, bool want_partial, cudaStream_t s) = 0;
+  virtual void ke(const Bufs& b, double* partial, int nblk, cudaStream_t s) = 0;
+  virtual int flux_blocks() const = 0;
+  virtual int launches_per_stage() const = 0;
+};
+
+template <int DIM, int P> struct Cfg;     // elements per block, threads per block
+template <> struct Cfg<2, 1> { static constexpr int EPB = 32, NT = 128; };
+template <> struct Cfg<2, 2> { static constexpr int EPB = 16, NT = 128; };
+template <> struct Cfg<2, 3> { static constexpr int EPB = 8, NT = 128; };
+template <> struct Cfg<2, 4> { static constexpr int EPB = 8, NT = 256; };
+template <> struct Cfg<2, 5> { static constexpr int EPB = 4, NT = 160; };
+template <> struct Cfg<3, 1> { static constexpr int EPB = 12, NT = 128; };
+template <> struct Cfg<3, 2> { static constexpr int EPB = 4, NT = 128; };
+template <> struct Cfg<3, 3> { static constexpr int EPB = 2, NT = 128; };
+template <> struct Cfg<3, 4> { static constexpr int EPB = 1, NT = 128; };
+
+template <int DIM, int P, typename TC>
+struct RunnerT : Runner {
+  using S = Shape<DIM, P>;
+  static constexpr int EPB = Cfg<DIM, P>::EPB, NT = Cfg<DIM, P>::NT;
+  long long E;
+  int visc;
+  Line<TC> L;
+  Line<double> L64;
+  PhysT<TC> ph;
+  RunnerT(long long E_, int visc_, const Line1D& l, const Phys& p) : E(E_), visc(visc_)
+  {
+    for (int i = 0; i < kMaxN1; i++) {
+      L.Lm[i] = L.Lp[i] = L.gL[i] = L.gR[i] = L.w[i] = TC(0);
+      for (int j = 0; j < kMaxN1; j++) L.D[i][j] = TC(0);
+    }
+    for (int i = 0; i <= P; i++) {
+      L.Lm[i] = (TC)l.Lm[i]; L.Lp[i] = (TC)l.Lp[i]; L.gL[i] = (TC)l.gL[i]; L.gR[i] = (TC)l.gR[i];
+      L.w[i] = (TC)l.w[i];
+      for (int j = 0; j <= P; j++) L.D[i][j] = (TC)l.D[i][j];
+    }
+    for (int i = 0; i < kMaxN1; i++) {
+      L64.Lm[i] = i <= P ? l.Lm[i] : 0; L64.Lp[i] = i <= P ? l.Lp[i] : 0; L64.gL[i] = i <= P ? l.gL[i] : 0;
+      L64.gR[i] = i <= P ? l.gR[i] : 0; L64.w[i] = i <= P ? l.w[i] : 0;
+      for (int j = 0; j < kMaxN1; j++) L64.D[i][j] = (i <= P && j <= P) ? l.D[i][j] : 0;
+    }
+    ph = PhysT<TC>::make(p);
+  }
+  int flux_blocks() const override { return (int)((E + EPB - 1) / EPB); }
+  int launches_per_stage() const override { return visc ? 2 : 1; }
+  void trace(const Bufs& b, int cur, cudaStream_t s) override
+  {
+    long long n = E * S::NF;
+    fr_trace_kernel<DIM, P, TC><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b.U, (TC*)b.UF[cur], E, L);
+  }
+  void grad(const Bufs& b, int cur, cudaStream_t s) override
+  {
+    fr_grad_kernel<DIM, P, EPB, NT, TC><<<flux_blocks(), NT, 0, s>>>(
+        b.U, (const TC*)b.UF[cur], b.mate, b.side, (const TC*)b.JG, (const TC*)b.detj, (TC*)b.GF, (TC*)b.RP, E,
+        L, ph);
+  }
+  template <int VISC, int MODE>
+  void flux_t(const Bufs& b, int cur, int stage, double dt, bool want_partial, cudaStream_t s)
+  {
+    fr_flux_kernel<DIM, P, EPB, NT, VISC, MODE, TC><<<flux_blocks(), NT, 0, s>>>(
+        b.U, b.REG, (const TC*)b.UF[cur], (TC*)b.UF[cur ^ 1], (const TC*)b.GF, (const TC*)b.RP, b.mate, b.side,
+        (const TC*)b.nL, (const TC*)b.tdA, (const TC*)b.JG, b.detj64, b.DIV, want_partial ? b.partial : nullptr,
+        E, L, ph, kRK4A[stage], kRK4B[stage], dt, stage == 0 ? 1 : 0);
+  }
+  void flux(const Bufs& b, int cur, int mode, int stage, double dt, bool want_partial, cudaStream_t s) override
+  {
+    if (visc) {
+      if (mode == 0) flux_t<1, 0>(b, cur, stage, dt, false, s); else flux_t<1, 1>(b, cur, stage, dt, want_partial, s);
+    } else {
+      if (mode == 0) flux_t<0, 0>(b, cur, stage, dt, false, s); else flux_t<0, 1>(b, cur, stage, dt, want_partial, s);
+    }
+  }
+  void ke(const Bufs& b, double* partial, int nblk, cudaStream_t s) override
+  {
+    fr_ke_kernel<DIM, P><<<nblk, 256, 0, s>>>(b.U, b.detj64, E, L64, partial);
+  }
+};
+
+template <typename TC>
+static Runner* make_runner_t(int dims, int P, long long E, int visc, const Line1D& l, const Phys& p)
+{
+  if (dims == 2) {
+    switch (P) {
+      case 1: return new RunnerT<2, 1, TC>(E, visc, l, p);
+      case 2: return new RunnerT<2, 2, TC>(E, visc, l, p);
+      case 3: return new RunnerT<2, 3, TC>(E, visc, l, p);
+      case 4: return new RunnerT<2, 4, TC>(E, visc, l, p);
+      case 5: return new RunnerT<2, 5, TC>(E, visc, l, p);
+    }
+  } else {
+    switch (P) {
+      case 1: return new RunnerT<3, 1, TC>(E, visc, l, p);
+      case 2: return new RunnerT<3, 2, TC>(E, visc, l, p);
+      case 3: return new RunnerT<3, 3, TC>(E, visc, l, p);
+      case 4: return new RunnerT<3, 4, TC>(E, visc, l, p);
+    }
+  }
+  return nullptr;
+}
+
+}  // namespace frb
+
+using namespace frb;
+
+struct fr_solver {
+  int device = 0;
+  fr_scheme_desc sch{};
+  Line1D line;
+  Mesh mesh;
+  Bufs b;
+  std::unique_ptr<Runner> run;
+  size_t tc_size = 8;
+  int cur = 0;                      // trace buffer holding the current state's traces
+  cudaStream_t own_stream = nullptr; // used when the caller passes stream == NULL
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  double graph_dt[2] = {0, 0};
+  long long launches = 0;
+  int nblk_ke = 0;
+  double* ke_partial = nullptr;
+  double* ke_out = nullptr;
+  std::vector<void*> allocs;
+};
+
+#define STRM(s, stream) ((stream) ? (cudaStream_t)(stream) : (s)->own_stream)
+
+namespace {
+
+template <typename T>
+fr_status dalloc(fr_solver* s, T** p, size_t n)
+{
+  void* q = nullptr;
+  FR_CUDA(cudaMalloc(&q, n * sizeof(T) + 16));
+  s->allocs.push_back(q);
+  *p = (T*)q;
+  return FR_OK;
+}
+
+fr_status upload_tc(fr_solver* s, void* dst, const std::vector<double>& src)
+{
+  if (s->tc_size == 8) {
+    FR_CUDA(cudaMemcpy(dst, src.data(), src.size() * 8, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> f(src.begin(), src.end());
+    FR_CUDA(cudaMemcpy(dst, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+  }
+  return FR_OK;
+}
+
+fr_status upload_geometry(fr_solver* s)
+{
+  Mesh& m = s->mesh;
+  fr_status st;
+  if ((st = upload_tc(s, s->b.JG, m.JG))) return st;
+  if ((st = upload_tc(s, s->b.detj, m.detjac))) return st;
+  if ((st = upload_tc(s, s->b.tdA, m.tdA))) return st;
+  if ((st = upload_tc(s, s->b.nL, m.nL))) return st;
+  FR_CUDA(cudaMemcpy(s->b.detj64, m.detjac.data(), m.detjac.size() * 8, cudaMemcpyHostToDevice));
+  FR_CUDA(cudaMemcpy(s->b.mate, m.mate.data(), m.mate.size() * sizeof(int), cudaMemcpyHostToDevice));
+  std::vector<unsigned char> side(m.mate.size());
+  size_t E = m.ne;
+  for (size_t i = 0; i < side.size(); i++) {
+    size_t f = i % m.nf, e = i / m.nf;
+    double n[3] = {0, 0, 0};
+    for (int d = 0; d < m.dims; d++) n[d] = m.nL[f + m.nf * (e + E * d)];
+    // sign switch of the LDG penalty from the left normal (src/inters.cpp:555-564)
+    double sgn = m.dims == 2 ? (n[0] + n[1]) : (n[0] + n[1] + std::sqrt(2.) * n[2]);
+    side[i] = (m.is_left[i] ? 1 : 0) | (sgn < 0. ? 2 : 0);
+  }
+  FR_CUDA(cudaMemcpy(s->b.side, side.data(), side.size(), cudaMemcpyHostToDevice));
+  return FR_OK;
+}
+
+void drop_graphs(fr_solver* s)
+{
+  for (int i = 0; i < 2; i++)
+    if (s->graph[i]) { cudaGraphExecDestroy(s->graph[i]); s->graph[i] = nullptr; }
+}
+
+fr_status check_launch(const char* what)
+{
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(FR_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  return FR_OK;
+}
+
+// one RK stage: residual + update; traces flip buffers
+fr_status stage(fr_solver* s, int st, double dt, bool want_partial, cudaStream_t stream)
+{
+  if (s->sch.viscous) { s->run->grad(s->b, s->cur, stream); s->launches++; }
+  s->run->flux(s->b, s->cur, 1, st, dt, want_partial, stream);
+  s->launches++;
+  s->cur ^= 1;
+  return check_launch("fr stage kernels");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fr_status_string(fr_status s)
+{
+  switch (s) {
+    case FR_OK: return "ok";
+    case FR_ERR_ARG: return "invalid argument";
+    case FR_ERR_CUDA: return "CUDA error";
+    case FR_ERR_NONFINITE: return "non-finite residual";
+    case FR_ERR_TIMEOUT: return "device wait timed out";
+    case FR_ERR_UNSUPPORTED: return "unsupported configuration";
+    case FR_ERR_MESH: return "mesh wiring failed";
+  }
+  return "unknown status";
+}
+
+const char* fr_last_error(void) { return g_err.c_str(); }
+
+fr_status fr_solver_create(const fr_mesh_desc* md, const fr_scheme_desc* sd, int device, fr_solver** out)
+{
+  g_err.clear();
+  if (!md || !sd || !out) return fail(FR_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (md->dims != 2 && md->dims != 3) return fail(FR_ERR_ARG, "dims must be 2 or 3");
+  if (sd->riemann != 0) return fail(FR_ERR_UNSUPPORTED, "only the Rusanov common flux is built");
+  if (sd->precision != 0 && sd->precision != 1) return fail(FR_ERR_ARG, "precision must be 0 or 1");
+  int maxP = md->dims == 2 ? 5 : 4;
+  if (sd->order < 1 || sd->order > maxP) return fail(FR_ERR_UNSUPPORTED, "order outside the built range");
+  if (sd->upts_type != 0) return fail(FR_ERR_UNSUPPORTED, "fused kernels need Gauss solution points");
+  std::unique_ptr<fr_solver> s(new fr_solver());
+  s->device = device;
+  s->sch = *sd;
+  s->tc_size = sd->precision == 1 ? 4 : 8;
+  std::string err;
+  if (!make_line(sd->order, sd->upts_type, sd->vcjh_scheme, sd->eta, s->line, err)) return fail(FR_ERR_ARG, err);
+  if (!build_mesh(md->dims, s->line, md->n_verts, md->xv, md->n_eles, md->c2v, md->shift, s->mesh, err))
+    return fail(FR_ERR_MESH, err);
+  FR_CUDA(cudaSetDevice(device));
+  Phys ph{sd->gamma, sd->prandtl, sd->mu_inf, sd->rt_inf, sd->c_sth, sd->fix_vis, sd->tau, sd->pen_fact};
+  Runner* r = sd->precision == 0 ? make_runner_t<double>(md->dims, sd->order, md->n_eles, sd->viscous, s->line, ph)
+                                  : make_runner_t<float>(md->dims, sd->order, md->n_eles, sd->viscous, s->line, ph);
+  if (!r) return fail(FR_ERR_UNSUPPORTED, "no kernel for this (dims, order)");
+  s->run.reset(r);
+  Mesh& m = s->mesh;
+  size_t E = m.ne, F = m.nfields, D = m.dims, nu = m.nu, nf = m.nf, tc = s->tc_size;
+  fr_status st;
+  if ((st = dalloc(s.get(), &s->b.U, nu * E * F))) return st;
+  if ((st = dalloc(s.get(), &s->b.REG, nu * E * F))) return st;
+  if ((st = dalloc(s.get(), &s->b.DIV, nu * E * F))) return st;
+  if ((st = dalloc(s.get(), &s->b.detj64, nu * E))) return st;
+  char* p;
+  for (int i = 0; i < 2; i++) { if ((st = dalloc(s.get(), &p, nf * E * F * tc))) return st; s->b.UF[i] = p; }
+  if (sd->viscous) {
+    if ((st = dalloc(s.get(), &p, nf * E * F * D * tc))) return st; s->b.GF = p;
+    if ((st = dalloc(s.get(), &p, nu * E * F * tc))) return st; s->b.RP = p;
+  }
+  if ((st = dalloc(s.get(), &p, nf * E * D * tc))) return st; s->b.nL = p;
+  if ((st = dalloc(s.get(), &p, nf * E * tc))) return st; s->b.tdA = p;
+  if ((st = dalloc(s.get(), &p, D * D * nu * E * tc))) return st; s->b.JG = p;
+  if ((st = dalloc(s.get(), &p, nu * E * tc))) return st; s->b.detj = p;
+  if ((st = dalloc(s.get(), &s->b.mate, nf * E))) return st;
+  if ((st = dalloc(s.get(), &s->b.side, nf * E))) return st;
+  if ((st = dalloc(s.get(), &s->b.partial, (size_t)s->run->flux_blocks() * F))) return st;
+  if ((st = dalloc(s.get(), &s->b.norms, F))) return st;
+  s->nblk_ke = 296;
+  if ((st = dalloc(s.get(), &s->ke_partial, (size_t)s->nblk_ke))) return st;
+  if ((st = dalloc(s.get(), &s->ke_out, 1))) return st;
+  FR_CUDA(cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking));
+  FR_CUDA(cudaMemset(s->b.U, 0, nu * E * F * 8));
+  FR_CUDA(cudaMemset(s->b.REG, 0, nu * E * F * 8));
+  if ((st = upload_geometry(s.get()))) return st;
+  *out = s.release();
+  return FR_OK;
+}
+
+fr_status fr_solver_destroy(fr_solver* s)
+{
+  if (!s) return FR_OK;
+  cudaSetDevice(s->device);
+  drop_graphs(s);
+  if (s->own_stream) { cudaStreamSynchronize(s->own_stream); cudaStreamDestroy(s->own_stream); }
+  for (void* p : s->allocs) cudaFree(p);
+  delete s;
+  return FR_OK;
+}
+
+fr_status fr_solver_sizes(const fr_solver* s, int out[6])
+{
+  if (!s || !out) return fail(FR_ERR_ARG, "null argument");
+  out[0] = (int)s->mesh.ne; out[1] = s->mesh.nu; out[2] = s->mesh.nf; out[3] = s->mesh.nfields;
+  out[4] = s->mesh.dims; out[5] = (int)s->mesh.il.size();
+  return FR_OK;
+}
+
+fr_status fr_solver_get_geometry(const fr_solver* s, double* pos, double* detj, double* JG, double* tdA, double* nrm)
+{
+  if (!s) return fail(FR_ERR_ARG, "null solver");
+  const Mesh& m = s->mesh;
+  if (pos) memcpy(pos, m.pos_upts.data(), m.pos_upts.size() * 8);
+  if (detj) memcpy(detj, m.detjac.data(), m.detjac.size() * 8);
+  if (JG) memcpy(JG, m.JG.data(), m.JG.size() * 8);
+  if (tdA) memcpy(tdA, m.tdA.data(), m.tdA.size() * 8);
+  if (nrm) memcpy(nrm, m.nrm.data(), m.nrm.size() * 8);
+  return FR_OK;
+}
+
+fr_status fr_solver_get_interfaces(const fr_solver* s, int* l, int* r)
+{
+  if (!s || !l || !r) return fail(FR_ERR_ARG, "null argument");
+  memcpy(l, s->mesh.il.data(), s->mesh.il.size() * sizeof(int));
+  memcpy(r, s->mesh.ir.data(), s->mesh.ir.size() * sizeof(int));
+  return FR_OK;
+}
+
+fr_status fr_solver_set_geometry(fr_solver* s, const double* detj, const double* JG, const double* tdA,
+                                 const double* nrm)
+{
+  if (!s || !detj || !JG || !tdA || !nrm) return fail(FR_ERR_ARG, "null argument");
+  Mesh& m = s->mesh;
+  for (size_t i = 0; i < m.detjac.size(); i++)
+    if (!(detj[i] > 0)) return fail(FR_ERR_ARG, "non-positive Jacobian");
+  memcpy(m.detjac.data(), detj, m.detjac.size() * 8);
+  memcpy(m.JG.data(), JG, m.JG.size() * 8);
+  memcpy(m.tdA.data(), tdA, m.tdA.size() * 8);
+  memcpy(m.nrm.data(), nrm, m.nrm.size() * 8);
+  finish_wiring(m);
+  FR_CUDA(cudaSetDevice(s->device));
+  drop_graphs(s);
+  return upload_geometry(s);
+}
+
+fr_status fr_solver_state_ptrs(fr_solver* s, double** u, double** reg)
+{
+  if (!s) return fail(FR_ERR_ARG, "null solver");
+  if (u) *u = s->b.U;
+  if (reg) *reg = s->b.REG;
+  return FR_OK;
+}
+
+fr_status fr_solver_state_updated(fr_solver* s, void* stream)
+{
+  if (!s) return fail(FR_ERR_ARG, "null solver");
+  FR_CUDA(cudaSetDevice(s->device));
+  s->run->trace(s->b, s->cur, STRM(s, stream));
+  s->launches++;
+  return check_launch("fr_trace_kernel");
+}
+
+fr_status fr_solver_set_state(fr_solver* s, const double* host_u, void* stream)
+{
+  if (!s || !host_u) return fail(FR_ERR_ARG, "null argument");
+  FR_CUDA(cudaSetDevice(s->device));
+  size_t n = (size_t)s->mesh.nu * s->mesh.ne * s->mesh.nfields;
+  for (size_t i = 0; i < (size_t)s->mesh.nu * s->mesh.ne; i++)
+    if (!(host_u[i] > 0) || !std::isfinite(host_u[i])) return fail(FR_ERR_NONFINITE, "density must be positive and finite");
+  cudaStream_t st = STRM(s, stream);
+  FR_CUDA(cudaMemcpyAsync(s->b.U, host_u, n * 8, cudaMemcpyHostToDevice, st));
+  FR_CUDA(cudaMemsetAsync(s->b.REG, 0, n * 8, st));
+  return fr_solver_state_updated(s, stream);
+}
+
+fr_status fr_solver_get_state(fr_solver* s, double* host_u, void* stream)
+{
+  if (!s || !host_u) return fail(FR_ERR_ARG, "null argument");
+  FR_CUDA(cudaSetDevice(s->device));
+  size_t n = (size_t)s->mesh.nu * s->mesh.ne * s->mesh.nfields;
+  FR_CUDA(cudaMemcpyAsync(host_u, s->b.U, n * 8, cudaMemcpyDeviceToHost, STRM(s, stream)));
+  FR_CUDA(cudaStreamSynchronize(STRM(s, stream)));
+  return FR_OK;
+}
+
+fr_status fr_solver_residual(fr_solver* s, double* host_div, void* stream)
+{
+  if (!s || !host_div) return fail(FR_ERR_ARG, "null argument");
+  FR_CUDA(cudaSetDevice(s->device));
+  cudaStream_t st = STRM(s, stream);
+  if (s->sch.viscous) { s->run->grad(s->b, s->cur, st); s->launches++; }
+  s->run->flux(s->b, s->cur, 0, 0, 0.0, false, st);
+  s->launches++;
+  fr_status r = check_launch("fr residual kernels");
+  if (r) return r;
+  size_t n = (size_t)s->mesh.nu * s->mesh.ne * s->mesh.nfields;
+  FR_CUDA(cudaMemcpyAsync(host_div, s->b.DIV, n * 8, cudaMemcpyDeviceToHost, st));
+  FR_CUDA(cudaStreamSynchronize(st));
+  return FR_OK;
+}
+
+fr_status fr_solver_rk_stage(fr_solver* s, int st, double dt, void* stream)
+{
+  if (!s || st < 0 || st > 4) return fail(FR_ERR_ARG, "stage must be 0..4");
+  FR_CUDA(cudaSetDevice(s->device));
+  return stage(s, st, dt, st == 4, STRM(s, stream));
+}
+
+fr_status fr_solver_advance(fr_solver* s, int n_steps, double dt, double* norms_host, void* stream)
+{
+  if (!s || n_steps < 0) return fail(FR_ERR_ARG, "bad argument");
+  if (!(dt > 0) || !std::isfinite(dt)) return fail(FR_ERR_ARG, "dt must be positive");
+  FR_CUDA(cudaSetDevice(s->device));
+  cudaStream_t st = STRM(s, stream);
+  bool capture_ok = true;
+  for (int i = 0; i < n_steps; i++) {
+    int c = s->cur;
+    if (capture_ok && (!s->graph[c] || s->graph_dt[c] != dt)) {
+      if (s->graph[c]) { cudaGraphExecDestroy(s->graph[c]); s->graph[c] = nullptr; }
+      cudaGraph_t g;
+      FR_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      long long l0 = s->launches;
+      for (int k = 0; k < 5; k++) stage(s, k, dt, k == 4, st);
+      s->launches = l0;
+      s->cur = c;
+      FR_CUDA(cudaStreamEndCapture(st, &g));
+      cudaError_t e = cudaGraphInstantiate(&s->graph[c], g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return fail(FR_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+      s->graph_dt[c] = dt;
+    }
+    if (capture_ok) {
+      FR_CUDA(cudaGraphLaunch(s->graph[c], st));
+      s->launches += 5 * s->run->launches_per_stage();
+      s->cur ^= 1;   // five stages: an odd number of trace-buffer flips
+    } else {
+      for (int k = 0; k < 5; k++) {
+        fr_status r = stage(s, k, dt, k == 4, st);
+        if (r) return r;
+      }
+    }
+  }
+  if (norms_host) {
+    int F = s->mesh.nfields;
+    double inv_n = 1.0 / ((double)s->mesh.nu * (double)s->mesh.ne);
+    fr_norm_finalize<<<1, 32, 0, st>>>(s->b.partial, s->run->flux_blocks(), F, inv_n, s->b.norms);
+    s->launches++;
+    FR_CUDA(cudaGetLastError());
+    FR_CUDA(cudaMemcpyAsync(norms_host, s->b.norms, F * 8, cudaMemcpyDeviceToHost, st));
+    FR_CUDA(cudaStreamSynchronize(st));
+    for (int k = 0; k < F; k++)
+      if (!std::isfinite(norms_host[k])) return fail(FR_ERR_NONFINITE, "NaN/Inf in the residual");
+  }
+  return FR_OK;
+}
+
+fr_status fr_solver_kinetic_energy(fr_solver* s, double* out, void* stream)
+{
+  if (!s || !out) return fail(FR_ERR_ARG, "null argument");
+  FR_CUDA(cudaSetDevice(s->device));
+  cudaStream_t st = STRM(s, stream);
+  s->run->ke(s->b, s->ke_partial, s->nblk_ke, st);
+  fr_norm_finalize<<<1, 32, 0, st>>>(s->ke_partial, s->nblk_ke, 1, 1.0, s->ke_out);
+  s->launches += 2;
+  FR_CUDA(cudaGetLastError());
+  FR_CUDA(cudaMemcpyAsync(out, s->ke_out, 8, cudaMemcpyDeviceToHost, st));
+  FR_CUDA(cudaStreamSynchronize(st));
+  return FR_OK;
+}
+
+long long fr_solver_launch_count(const fr_solver* s) { return s ? s->launches : 0; }
+
+void* fr_solver_stream(fr_solver* s) { return s ? (void*)s->own_stream : nullptr; }
+
+fr_status fr_solver_profile_stage(fr_solver* s, int reps, double dt, double* ms_grad, double* ms_flux)
+{
+  if (!s || reps <= 0 || !ms_grad || !ms_flux) return fail(FR_ERR_ARG, "bad argument");
+  FR_CUDA(cudaSetDevice(s->device));
+  cudaStream_t st = s->own_stream;
+  cudaEvent_t ev[3];
+  for (int i = 0; i < 3; i++) FR_CUDA(cudaEventCreate(&ev[i]));
+  double tg = 0.0, tf = 0.0;
+  for (int r = 0; r < reps; r++) {
+    int k = r % 5;
+    FR_CUDA(cudaEventRecord(ev[0], st));
+    if (s->sch.viscous) { s->run->grad(s->b, s->cur, st); s->launches++; }
+    FR_CUDA(cudaEventRecord(ev[1], st));
+    s->run->flux(s->b, s->cur, 1, k, dt, k == 4, st);
+    s->launches++;
+    s->cur ^= 1;
+    FR_CUDA(cudaEventRecord(ev[2], st));
+    FR_CUDA(cudaEventSynchronize(ev[2]));
+    float a = 0.f, b = 0.f;
+    FR_CUDA(cudaEventElapsedTime(&a, ev[0], ev[1]));
+    FR_CUDA(cudaEventElapsedTime(&b, ev[1], ev[2]));
+    tg += a; tf += b;
+  }
+  for (int i = 0; i < 3; i++) cudaEventDestroy(ev[i]);
+  FR_CUDA(cudaGetLastError());
+  *ms_grad = tg / reps;
+  *ms_flux = tf / reps;
+  return FR_OK;
+}
+
+fr_status fr_mesh_geometry(const fr_mesh_desc* md, const fr_scheme_desc* sd, int out6[6], double* pos_upts,
+                           double* detjac, double* JG, double* tdA, double* nrm, int* left_idx, int* right_idx)
+{
+  g_err.clear();
+  if (!md || !sd || !out6) return fail(FR_ERR_ARG, "null argument");
+  Line1D line;
+  Mesh m;
+  std::string err;
+  if (!make_line(sd->order, sd->upts_type, sd->vcjh_scheme, sd->eta, line, err)) return fail(FR_ERR_ARG, err);
+  if (!build_mesh(md->dims, line, md->n_verts, md->xv, md->n_eles, md->c2v, md->shift, m, err))
+    return fail(FR_ERR_MESH, err);
+  out6[0] = (int)m.ne; out6[1] = m.nu; out6[2] = m.nf; out6[3] = m.nfields; out6[4] = m.dims;
+  out6[5] = (int)m.il.size();
+  if (pos_upts) memcpy(pos_upts, m.pos_upts.data(), m.pos_upts.size() * 8);
+  if (detjac) memcpy(detjac, m.detjac.data(), m.detjac.size() * 8);
+  if (JG) memcpy(JG, m.JG.data(), m.JG.size() * 8);
+  if (tdA) memcpy(tdA, m.tdA.data(), m.tdA.size() * 8);
+  if (nrm) memcpy(nrm, m.nrm.data(), m.nrm.size() * 8);
+  if (left_idx) memcpy(left_idx, m.il.data(), m.il.size() * sizeof(int));
+  if (right_idx) memcpy(right_idx, m.ir.data(), m.ir.size() * sizeof(int));
+  return FR_OK;
+}
+
+fr_status fr_line_operators(int order, int upts_type, int vcjh_scheme, double eta, double* out)
+{
+  if (!out) return fail(FR_ERR_ARG, "null argument");
+  Line1D L;
+  std::string err;
+  if (!make_line(order, upts_type, vcjh_scheme, eta, L, err)) return fail(FR_ERR_ARG, err);
+  int n = L.n1;
+  double* o = out;
+  for (int i = 0; i < n; i++) *o++ = L.loc[i];
+  for (int i = 0; i < n; i++) *o++ = L.Lm[i];
+  for (int i = 0; i < n; i++) *o++ = L.Lp[i];
+  for (int k = 0; k < n; k++) for (int m = 0; m < n; m++) *o++ = L.D[k][m];
+  for (int i = 0; i < n; i++) *o++ = L.gL[i];
+  for (int i = 0; i < n; i++) *o++ = L.gR[i];
+  for (int i = 0; i < n; i++) *o++ = L.w[i];
+  *o = L.eta;
+  return FR_OK;
+}
+
+fr_status fr_solver_sync(fr_solver* s)
+{
+  if (!s) return fail(FR_ERR_ARG, "null solver");
+  FR_CUDA(cudaSetDevice(s->device));
+  FR_CUDA(cudaStreamSynchronize(s->own_stream));
+  return FR_OK;
+}
+
+}  // extern "C"

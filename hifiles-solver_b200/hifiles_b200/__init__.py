@@ -1,0 +1,293 @@
+"""Python mirror of the HiFiLES per-element-type FR path over the C ABI of
+include/fr_b200.h (libfrb200.so, built in-tree by hifiles-solver_b200/build.py).
+
+The names follow the reference: a Solver holds one element type on a periodic
+conforming mesh and exposes CalcResidual (`residual`), one RK45 stage of
+eles::AdvanceSolution (`rk_stage`), the time loop (`advance`) and the
+diagnostics (`norms`, `kinetic_energy`).  Arrays are numpy arrays in the
+reference's array<T> layouts (Fortran order): state[upt, ele, field].
+
+There is no CPU fallback: constructing a Solver without the CUDA library or
+without a GPU raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(HERE, "libfrb200.so")
+
+FR_OK = 0
+STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "non-finite residual", 4: "device wait timed out",
+          5: "unsupported configuration", 6: "mesh wiring failed"}
+
+
+class FrError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s (%d): %s" % (STATUS.get(status, "?"), status, msg))
+        self.status = status
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("dims", C.c_int), ("n_verts", C.c_int), ("xv", C.POINTER(C.c_double)), ("n_eles", C.c_int),
+                ("c2v", C.POINTER(C.c_int)), ("shift", C.c_double * 3)]
+
+
+class SchemeDesc(C.Structure):
+    _fields_ = [("order", C.c_int), ("upts_type", C.c_int), ("vcjh_scheme", C.c_int), ("eta", C.c_double),
+                ("viscous", C.c_int), ("riemann", C.c_int), ("precision", C.c_int), ("gamma", C.c_double),
+                ("prandtl", C.c_double), ("mu_inf", C.c_double), ("rt_inf", C.c_double), ("c_sth", C.c_double),
+                ("fix_vis", C.c_double), ("tau", C.c_double), ("pen_fact", C.c_double)]
+
+
+_LIB = None
+
+
+def lib():
+    """Load libfrb200.so; raises if it has not been built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libfrb200.so is missing: run `python hifiles-solver_b200/build.py`")
+    L = C.CDLL(LIB_PATH)
+    vp, dp, ip = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int)
+    sigs = {
+        "fr_status_string": (C.c_char_p, [C.c_int]),
+        "fr_last_error": (C.c_char_p, []),
+        "fr_solver_create": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(SchemeDesc), C.c_int, C.POINTER(vp)]),
+        "fr_solver_destroy": (C.c_int, [vp]),
+        "fr_solver_sizes": (C.c_int, [vp, ip]),
+        "fr_solver_get_geometry": (C.c_int, [vp, dp, dp, dp, dp, dp]),
+        "fr_solver_get_interfaces": (C.c_int, [vp, ip, ip]),
+        "fr_solver_set_geometry": (C.c_int, [vp, dp, dp, dp, dp]),
+        "fr_solver_set_state": (C.c_int, [vp, dp, vp]),
+        "fr_solver_get_state": (C.c_int, [vp, dp, vp]),
+        "fr_solver_state_ptrs": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp)]),
+        "fr_solver_state_updated": (C.c_int, [vp, vp]),
+        "fr_solver_residual": (C.c_int, [vp, dp, vp]),
+        "fr_solver_rk_stage": (C.c_int, [vp, C.c_int, C.c_double, vp]),
+        "fr_solver_advance": (C.c_int, [vp, C.c_int, C.c_double, dp, vp]),
+        "fr_solver_kinetic_energy": (C.c_int, [vp, dp, vp]),
+        "fr_solver_launch_count": (C.c_longlong, [vp]),
+        "fr_solver_stream": (vp, [vp]),
+        "fr_solver_sync": (C.c_int, [vp]),
+        "fr_solver_profile_stage": (C.c_int, [vp, C.c_int, C.c_double, dp, dp]),
+        "fr_mesh_geometry": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(SchemeDesc), ip, dp, dp, dp, dp, dp, ip, ip]),
+        "fr_line_operators": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, dp]),
+    }
+    for name, (res, args) in sigs.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _LIB = L
+    return L
+
+
+def _check(st):
+    if st != FR_OK:
+        raise FrError(st, lib().fr_last_error().decode())
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def box_mesh(dims, n, lo, hi, jitter=0.0, seed=0):
+    """Vertices and tensor-ordered element->vertex map of a structured box,
+    interior vertices moved by a seeded uniform jitter of +-jitter*h (64-bit
+    LCG, so a seed names one mesh on every machine)."""
+    nx, ny = int(n[0]), int(n[1])
+    nz = int(n[2]) if dims == 3 else 1
+    vx, vy, vz = nx + 1, ny + 1, (nz + 1 if dims == 3 else 1)
+    nn = [nx, ny, nz]
+    idx = np.indices((vz, vy, vx)).reshape(3, -1)      # k, j, i with i fastest
+    ijk = [idx[2], idx[1], idx[0]]
+    nv = vx * vy * vz
+    mask = (1 << 64) - 1
+    A, B = 6364136223846793005, 1442695040888963407
+    rnd = np.empty((nv, dims))
+    s = (int(seed) * A + B) & mask
+    for v in range(nv):
+        for d in range(dims):
+            s = (s * A + B) & mask
+            rnd[v, d] = ((s >> 11) * (1.0 / 9007199254740992.0)) * 2.0 - 1.0
+    xv = np.empty((nv, dims))
+    interior = np.ones(nv, dtype=bool)
+    for d in range(dims):
+        interior &= (ijk[d] > 0) & (ijk[d] < nn[d])
+    for d in range(dims):
+        h = (hi[d] - lo[d]) / nn[d]
+        x = lo[d] + (hi[d] - lo[d]) * ijk[d] / nn[d]
+        if jitter > 0:
+            x = np.where(interior, x + jitter * h * rnd[:, d], x)
+        xv[:, d] = x
+    ex, ey, ez = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    ex, ey, ez = ex.transpose(2, 1, 0).ravel(), ey.transpose(2, 1, 0).ravel(), ez.transpose(2, 1, 0).ravel()
+    cols = []
+    for c in range(2 if dims == 3 else 1):
+        for b in range(2):
+            for a in range(2):
+                cols.append((ex + a) + vx * ((ey + b) + vy * (ez + c)))
+    c2v = np.stack(cols, axis=1).astype(np.int32)
+    return xv, c2v
+
+
+def _descs(dims, xv, c2v, shift, order, viscous=False, gamma=1.4, prandtl=0.72, mu_inf=0.0, rt_inf=1.0,
+           c_sth=1.0, fix_vis=1.0, tau=1.0, pen_fact=0.5, vcjh_scheme=1, eta=0.0, upts_type=0, precision=0):
+    xv = np.ascontiguousarray(xv, dtype=np.float64)
+    c2v = np.ascontiguousarray(c2v, dtype=np.int32)
+    md = MeshDesc(int(dims), xv.shape[0], _dp(xv), c2v.shape[0], c2v.ctypes.data_as(C.POINTER(C.c_int)),
+                  (C.c_double * 3)(*(list(shift) + [0.0] * (3 - len(shift)))))
+    sd = SchemeDesc(int(order), int(upts_type), int(vcjh_scheme), float(eta), int(bool(viscous)), 0, int(precision),
+                    gamma, prandtl, mu_inf, rt_inf, c_sth, fix_vis, tau, pen_fact)
+    return md, sd, (xv, c2v)
+
+
+def mesh_geometry(dims, xv, c2v, shift, order, **kw):
+    """Host-only: metrics and interface wiring as the solver builds them."""
+    md, sd, keep = _descs(dims, xv, c2v, shift, order, **kw)
+    sz = (C.c_int * 6)()
+    _check(lib().fr_mesh_geometry(C.byref(md), C.byref(sd), sz, None, None, None, None, None, None, None))
+    E, nu, nf, F, D, ni = list(sz)
+    g = dict(pos_upts=np.zeros((nu, E, D), order="F"), detjac_upts=np.zeros((nu, E), order="F"),
+             JGinv_upts=np.zeros((D, D, nu, E), order="F"), tdA_fpts=np.zeros((nf, E), order="F"),
+             norm_fpts=np.zeros((nf, E, D), order="F"), left=np.zeros(ni, dtype=np.int32),
+             right=np.zeros(ni, dtype=np.int32))
+    ipp = C.POINTER(C.c_int)
+    _check(lib().fr_mesh_geometry(C.byref(md), C.byref(sd), sz, *[_dp(g[k]) for k in
+                                  ("pos_upts", "detjac_upts", "JGinv_upts", "tdA_fpts", "norm_fpts")],
+                                  g["left"].ctypes.data_as(ipp), g["right"].ctypes.data_as(ipp)))
+    return g
+
+
+def line_operators(order, upts_type=0, vcjh_scheme=1, eta=0.0):
+    """The 1-D operator factors (see fr_line_operators in include/fr_b200.h)."""
+    n = order + 1
+    out = np.zeros(n * n + 6 * n + 1)
+    _check(lib().fr_line_operators(int(order), int(upts_type), int(vcjh_scheme), float(eta), _dp(out)))
+    o = iter(np.split(out, np.cumsum([n, n, n, n * n, n, n, n])))
+    loc, Lm, Lp, D, gL, gR, w, eta = [next(o) for _ in range(8)]
+    return dict(loc=loc, Lm=Lm, Lp=Lp, D=D.reshape(n, n), gL=gL, gR=gR, w=w, eta=float(eta[0]))
+
+
+class Solver:
+    """One element type (quads or hexes) on a periodic conforming mesh, resident on one GPU."""
+
+    def __init__(self, dims, xv, c2v, shift, order, viscous=False, gamma=1.4, prandtl=0.72, mu_inf=0.0,
+                 rt_inf=1.0, c_sth=1.0, fix_vis=1.0, tau=1.0, pen_fact=0.5, vcjh_scheme=1, eta=0.0, upts_type=0,
+                 precision=0, device=0):
+        L = lib()
+        self._xv = np.ascontiguousarray(xv, dtype=np.float64)
+        self._c2v = np.ascontiguousarray(c2v, dtype=np.int32)
+        md = MeshDesc(int(dims), self._xv.shape[0], _dp(self._xv), self._c2v.shape[0],
+                      self._c2v.ctypes.data_as(C.POINTER(C.c_int)),
+                      (C.c_double * 3)(*(list(shift) + [0.0] * (3 - len(shift)))))
+        sd = SchemeDesc(int(order), int(upts_type), int(vcjh_scheme), float(eta), int(bool(viscous)), 0,
+                        int(precision), gamma, prandtl, mu_inf, rt_inf, c_sth, fix_vis, tau, pen_fact)
+        h = C.c_void_p()
+        self.h = None
+        _check(L.fr_solver_create(C.byref(md), C.byref(sd), int(device), C.byref(h)))
+        self.h = h
+        sz = (C.c_int * 6)()
+        _check(L.fr_solver_sizes(self.h, sz))
+        self.n_eles, self.n_upts, self.n_fpts, self.n_fields, self.dims, self.n_int = list(sz)
+        self.viscous = bool(viscous)
+        self.precision = precision
+
+    @classmethod
+    def box(cls, dims, order, n, lo, hi, jitter=0.0, seed=0, **kw):
+        xv, c2v = box_mesh(dims, n, lo, hi, jitter, seed)
+        shift = [hi[d] - lo[d] for d in range(dims)]
+        return cls(dims, xv, c2v, shift, order, **kw)
+
+    def close(self):
+        if self.h is not None:
+            lib().fr_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def state_shape(self):
+        return (self.n_upts, self.n_eles, self.n_fields)
+
+    def geometry(self):
+        E, nu, nf, D = self.n_eles, self.n_upts, self.n_fpts, self.dims
+        g = dict(pos_upts=np.zeros((nu, E, D), order="F"), detjac_upts=np.zeros((nu, E), order="F"),
+                 JGinv_upts=np.zeros((D, D, nu, E), order="F"), tdA_fpts=np.zeros((nf, E), order="F"),
+                 norm_fpts=np.zeros((nf, E, D), order="F"))
+        _check(lib().fr_solver_get_geometry(self.h, *[_dp(g[k]) for k in
+                                                      ("pos_upts", "detjac_upts", "JGinv_upts", "tdA_fpts",
+                                                       "norm_fpts")]))
+        return g
+
+    def interfaces(self):
+        l = np.zeros(self.n_int, dtype=np.int32)
+        r = np.zeros(self.n_int, dtype=np.int32)
+        _check(lib().fr_solver_get_interfaces(self.h, l.ctypes.data_as(C.POINTER(C.c_int)),
+                                              r.ctypes.data_as(C.POINTER(C.c_int))))
+        return l, r
+
+    def set_geometry(self, detjac_upts, JGinv_upts, tdA_fpts, norm_fpts):
+        a = [np.asfortranarray(x, dtype=np.float64) for x in (detjac_upts, JGinv_upts, tdA_fpts, norm_fpts)]
+        _check(lib().fr_solver_set_geometry(self.h, *[_dp(x) for x in a]))
+
+    def set_state(self, u, stream=None):
+        u = np.asfortranarray(u, dtype=np.float64)
+        if u.shape != self.state_shape:
+            raise ValueError("state shape %s != %s" % (u.shape, self.state_shape))
+        _check(lib().fr_solver_set_state(self.h, _dp(u), stream))
+
+    def get_state(self, stream=None):
+        u = np.zeros(self.state_shape, order="F")
+        _check(lib().fr_solver_get_state(self.h, _dp(u), stream))
+        return u
+
+    def state_ptrs(self):
+        u, r = C.c_void_p(), C.c_void_p()
+        _check(lib().fr_solver_state_ptrs(self.h, C.byref(u), C.byref(r)))
+        return u.value, r.value
+
+    def state_updated(self, stream=None):
+        _check(lib().fr_solver_state_updated(self.h, stream))
+
+    def residual(self, stream=None):
+        """div_tconf_upts(0) of one CalcResidual on the current state."""
+        d = np.zeros(self.state_shape, order="F")
+        _check(lib().fr_solver_residual(self.h, _dp(d), stream))
+        return d
+
+    def rk_stage(self, stage, dt, stream=None):
+        _check(lib().fr_solver_rk_stage(self.h, int(stage), float(dt), stream))
+
+    def advance(self, n_steps, dt, norms=False, stream=None):
+        """n_steps RK45 steps; returns the L1 residual norms of the last stage if norms."""
+        out = np.zeros(self.n_fields) if norms else None
+        _check(lib().fr_solver_advance(self.h, int(n_steps), float(dt), _dp(out) if norms else None, stream))
+        return out
+
+    def kinetic_energy(self, stream=None):
+        v = C.c_double()
+        _check(lib().fr_solver_kinetic_energy(self.h, C.byref(v), stream))
+        return v.value
+
+    def launch_count(self):
+        return int(lib().fr_solver_launch_count(self.h))
+
+    def stream(self):
+        return lib().fr_solver_stream(self.h)
+
+    def sync(self):
+        _check(lib().fr_solver_sync(self.h))
+
+    def profile_stage(self, reps, dt):
+        """Mean CUDA-event ms of (gradient kernel, flux/update kernel) over reps stages."""
+        a, b = C.c_double(), C.c_double()
+        _check(lib().fr_solver_profile_stage(self.h, int(reps), float(dt), C.byref(a), C.byref(b)))
+        return a.value, b.value

@@ -1,0 +1,153 @@
+/* fr_b200.h -- C ABI of the B200 (sm_100a) flux-reconstruction residual and
+ * low-storage RK45 stage.  Drop-in for the GPU seam of HiFiLES's per-element
+ * operator path (the `#ifdef _GPU` bodies of class eles / int_inters and the
+ * wrappers of include/cuda_kernels.h in the reference).
+ *
+ * Conventions
+ *  - Every entry point returns fr_status; nothing calls exit().  The reference
+ *    reports errors through FatalError/exit (include/error.h:20-22,
+ *    include/array.h:461-473); here the caller decides.
+ *  - Array layouts are the reference's array<T> layouts (first index fastest,
+ *    include/array.h:287-309): states (n_upts, n_eles, n_fields), flux-point
+ *    arrays (n_fpts, n_eles, n_fields), gradients (n_pts, n_eles, n_fields,
+ *    n_dims), JGinv (n_dims, n_dims, n_upts, n_eles).  Point orderings inside
+ *    an element are the reference's (src/eles_hexas.cpp:240-324,
+ *    src/eles_quads.cpp:237-300), so reference arrays can be passed unchanged.
+ *  - `stream` is a cudaStream_t passed as void*; NULL selects the solver's own
+ *    non-blocking stream.  Device pointers are caller-owned unless stated
+ *    otherwise.
+ *  - One GPU, one rank: there is no MPI interface path.
+ */
+#ifndef FR_B200_H
+#define FR_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  FR_OK = 0,
+  FR_ERR_ARG = 1,         /* bad size, pointer or option                      */
+  FR_ERR_CUDA = 2,        /* a CUDA runtime call failed (fr_last_error says)  */
+  FR_ERR_NONFINITE = 3,   /* NaN/Inf or non-positive density/pressure found   */
+  FR_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up               */
+  FR_ERR_UNSUPPORTED = 5, /* element type / order / option not built          */
+  FR_ERR_MESH = 6         /* mesh cannot be wired (unmatched face, bad map)   */
+} fr_status;
+
+const char* fr_status_string(fr_status s);
+/* Message of the last failing call on this host thread ("" if none). */
+const char* fr_last_error(void);
+
+/* ------------------------------------------------------------------------
+ * Solver object: mesh wiring, metrics and operators built once on the host
+ * (replaces GeoPreprocess' set_transforms / set_opp_* / int_inters::set_interior,
+ * src/geometry.cpp:151-990, src/eles.cpp:3620-4847, src/int_inters.cpp:95-178),
+ * state resident in HBM, fused stage kernels.
+ * ---------------------------------------------------------------------- */
+
+typedef struct fr_solver fr_solver;
+
+typedef struct {
+  int dims;              /* 2: 4-node quadrilaterals, 3: 8-node hexahedra      */
+  int n_verts;
+  const double* xv;      /* (n_verts, dims) row-major vertex coordinates       */
+  int n_eles;
+  const int* c2v;        /* (n_eles, 2^dims) row-major; vertex m = a + 2b + 4c
+                            sits at reference corner (a, b, c) in {0,1}^dims    */
+  double shift[3];       /* periodic translation per axis (dx/dy/dz_cyclic of
+                            the reference input), 0 = not periodic             */
+} fr_mesh_desc;
+
+typedef struct {
+  int order;             /* polynomial order P (quads 1..5, hexes 1..5)        */
+  int upts_type;         /* 0 Gauss, 1 Gauss-Lobatto (upts_type_quad/hexa)     */
+  int vcjh_scheme;       /* 0 VCJH with eta, 1 DG, 2 SD, 3 Hu, 4 c_+           */
+  double eta;            /* used when vcjh_scheme == 0                         */
+  int viscous;           /* 0 Euler, 1 Navier-Stokes                           */
+  int riemann;           /* 0 Rusanov (riemann_solve_type 0)                   */
+  int precision;         /* 0 FP64 throughout; 1 FP32 traces/fluxes/operators
+                            with FP64 state, RK register and reductions        */
+  double gamma, prandtl, mu_inf, rt_inf, c_sth, fix_vis; /* gas + viscosity law */
+  double tau, pen_fact;  /* LDG penalty parameters                             */
+} fr_scheme_desc;
+
+fr_status fr_solver_create(const fr_mesh_desc* mesh, const fr_scheme_desc* scheme, int device,
+                           fr_solver** out);
+fr_status fr_solver_destroy(fr_solver* s);
+
+/* n_eles, n_upts_per_ele, n_fpts_per_ele, n_fields, n_dims, n_interface_fpts */
+fr_status fr_solver_sizes(const fr_solver* s, int out6[6]);
+
+/* Host copies of the set-up arrays (NULL entries are skipped). */
+fr_status fr_solver_get_geometry(const fr_solver* s, double* pos_upts, double* detjac_upts,
+                                 double* JGinv_upts, double* tdA_fpts, double* norm_fpts);
+/* Left/right element flux point (fpt + n_fpts*ele) of every interface flux point. */
+fr_status fr_solver_get_interfaces(const fr_solver* s, int* left_idx, int* right_idx);
+/* Replace the metrics by caller-built arrays (e.g. the reference's own). */
+fr_status fr_solver_set_geometry(fr_solver* s, const double* detjac_upts, const double* JGinv_upts,
+                                 const double* tdA_fpts, const double* norm_fpts);
+
+/* State transfer (disu_upts(0)), host memory, layout (n_upts, n_eles, n_fields).
+ * set_state zeroes the RK register (disu_upts(1)), like InitSolution. */
+fr_status fr_solver_set_state(fr_solver* s, const double* host_u, void* stream);
+fr_status fr_solver_get_state(fr_solver* s, double* host_u, void* stream);
+/* Device pointers of the resident state and RK register (owned by the solver). */
+fr_status fr_solver_state_ptrs(fr_solver* s, double** d_u, double** d_reg);
+/* Re-derive the flux-point traces after the caller wrote the state in place. */
+fr_status fr_solver_state_updated(fr_solver* s, void* stream);
+
+/* One CalcResidual (src/solver.cpp:65-225): div_tconf_upts(0) to host memory
+ * (layout (n_upts, n_eles, n_fields)); the state is not advanced. */
+fr_status fr_solver_residual(fr_solver* s, double* host_div, void* stream);
+
+/* RK45 stage `stage` (0..4) of eles::AdvanceSolution (src/eles.cpp:1091-1188)
+ * preceded by its residual evaluation: the body of the reference's
+ * HiFiLES.cpp:159-183 loop for one stage. */
+fr_status fr_solver_rk_stage(fr_solver* s, int stage, double dt, void* stream);
+
+/* n_steps full RK45 steps.  If norms_host != NULL it receives the L1 residual
+ * norms per field of the last stage of the last step (CalcNormResidual,
+ * src/output.cpp:1452-1523, res_norm_type 1).  Graph-replayed after the first
+ * call with the same dt. */
+fr_status fr_solver_advance(fr_solver* s, int n_steps, double dt, double* norms_host, void* stream);
+
+/* Volume integral of 0.5 rho |v|^2 (solution-point Gauss quadrature), FP64. */
+fr_status fr_solver_kinetic_energy(fr_solver* s, double* out_host, void* stream);
+
+/* Kernel launches issued by the solver since creation (for launch accounting). */
+long long fr_solver_launch_count(const fr_solver* s);
+
+/* The solver's own non-blocking stream (cudaStream_t), used whenever an entry
+ * point is given stream == NULL; and a synchronisation of that stream. */
+void* fr_solver_stream(fr_solver* s);
+fr_status fr_solver_sync(fr_solver* s);
+
+/* Runs `reps` RK stages one by one (advancing the state) and returns the mean
+ * CUDA-event duration of each of the two stage kernels on the solver's stream
+ * (ms_grad is 0 for inviscid runs).  For roofline accounting. */
+fr_status fr_solver_profile_stage(fr_solver* s, int reps, double dt, double* ms_grad, double* ms_flux);
+
+/* ------------------------------------------------------------------------
+ * Host-only set-up queries (no GPU is touched).
+ * ---------------------------------------------------------------------- */
+
+/* Wiring and metrics exactly as fr_solver_create builds them.  Call with NULL
+ * arrays first to get the sizes (out6 as in fr_solver_sizes). */
+fr_status fr_mesh_geometry(const fr_mesh_desc* mesh, const fr_scheme_desc* scheme, int out6[6],
+                           double* pos_upts, double* detjac_upts, double* JGinv_upts, double* tdA_fpts,
+                           double* norm_fpts, int* left_idx, int* right_idx);
+
+/* The 1-D factors of the tensor-product operators for (order, upts_type,
+ * vcjh_scheme, eta), packed as: loc[n], l_m(-1)[n], l_m(+1)[n], D[n][n]
+ * (D[k][m] = l_m'(xi_k)), g_L'(xi_k)[n], g_R'(xi_k)[n], weights[n], eta;
+ * n = order + 1, i.e. n*n + 6n + 1 doubles.  Every non-zero of the reference's
+ * opp_0..opp_6 for quads / hexes (src/eles.cpp:3620-4052) is one of these. */
+fr_status fr_line_operators(int order, int upts_type, int vcjh_scheme, double eta, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
