@@ -47,7 +47,8 @@ def build(force=False, verbose=False):
         cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-ffp-contract=off",
                "-I", os.path.join(REPO, "include"), "-I", CSRC, "-c", path, "-o", obj]
         if src.endswith(".cu"):
-            cmd[1:1] = ["-Xptxas", "-v"] if verbose else []
+            # reference rounding: no implicit contraction of a*b+c into an FMA
+            cmd[1:1] = ["-fmad=false"] + (["-Xptxas", "-v"] if verbose else [])
         if verbose:
             print(" ".join(cmd))
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))

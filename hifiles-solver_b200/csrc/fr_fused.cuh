@@ -13,9 +13,10 @@
 // through flux-point traces in HBM:
 //   UF  (n_fpts, n_eles, F)      solution at the flux points, double-buffered
 //                                across stages (written by the stage update)
-//   GF  (n_fpts, n_eles, F, D)   corrected physical gradient at flux points
-//   RP  (n_upts, n_eles, F)      divergence of the discontinuous flux minus its
-//                                own flux-point correction (viscous path)
+//   VF  (n_fpts, n_eles, F-1)    own viscous flux at the flux points projected
+//                                on the interface's left normal (viscous path)
+//   ND  (n_fpts, n_eles, F)      normal discontinuous flux (norm_tdisf_fpts)
+//   DV  (n_upts, n_eles, F)      divergence of the discontinuous flux
 // mate[i] is the flat index (fpt + n_fpts*ele) of the matching point across
 // the interface; side[i] bit 0 = this side is the left one, bit 1 = the LDG
 // penalty sign is negative.  Both sides evaluate the common flux with the
@@ -114,8 +115,8 @@ __device__ __forceinline__ int face_axis(int fc)
   return (fc == 2 || fc == 4) ? 0 : ((fc == 1 || fc == 3) ? 1 : 2);
 }
 
-// value at flux point f of a field stored point-major in shared memory
-// (s[u * stride_s]); explicit FMAs keep every call site bit-identical.
+// Value at flux point f of a field stored point-major (s[u * sst]): the
+// reference's opp_0 row of f applied in column order, (((0 + t0) + t1) + ...).
 template <int DIM, int P, typename T, typename S>
 __device__ __forceinline__ T line_interp(const Line<T>& L, const S* s, int sst, int f)
 {
@@ -123,7 +124,7 @@ __device__ __forceinline__ T line_interp(const Line<T>& L, const S* s, int sst, 
   fpt_line<DIM, P>(f, u0, st, ax, plus);
   T acc = T(0);
 #pragma unroll
-  for (int m = 0; m <= P; m++) acc = ffma((T)s[(u0 + m * st) * sst], plus ? L.Lp[m] : L.Lm[m], acc);
+  for (int m = 0; m <= P; m++) acc = acc + (T)s[(u0 + m * st) * sst] * (plus ? L.Lp[m] : L.Lm[m]);
   return acc;
 }
 
@@ -141,6 +142,24 @@ __device__ __forceinline__ int upt_stride(int axis)
   constexpr int N1 = P + 1;
   return axis == 0 ? 1 : (axis == 1 ? N1 : N1 * N1);
 }
+
+// Sum over all axes of the 1-D derivative along each axis of a field stored
+// point-major: the reference's sum_d opp_2[d] (or opp_4[d]) row of u, in
+// column order per axis and axes in order.
+template <int DIM, int P, typename T, typename S>
+__device__ __forceinline__ T deriv_line(const Line<T>& L, const S* s, int sst, int u, int d, int i)
+{
+  const int st = upt_stride<DIM, P>(d), ub = u - i * st;
+  T acc = T(0);
+#pragma unroll
+  for (int m = 0; m <= P; m++) acc = acc + (T)s[(ub + m * st) * sst] * L.D[i][m];
+  return acc;
+}
+
+template <int NT, int ITEMS>
+struct Items {
+  static constexpr int N = (ITEMS + NT - 1) / NT;
+};
 
 // ---------------------------------------------------------------------------
 // Initial flux-point traces from the state (used once after the state is set).
@@ -160,26 +179,65 @@ __global__ void fr_trace_kernel(const double* __restrict__ U, TC* __restrict__ U
 }
 
 // ---------------------------------------------------------------------------
-// Viscous part 1: LDG common solution -> corrected gradient at solution points
-// (calculate_gradient + correct_gradient, src/eles.cpp:1667-1968) -> gradient
-// traces (extrapolate_corrected_gradient, src/eles.cpp:1973-2052); total
-// discontinuous flux (evaluate_invFlux + evaluate_viscFlux) -> its divergence
-// (calculate_divergence) minus the correction of its own normal component
-// (the norm_tdisf_fpts half of calculate_corrected_divergence).
+// Viscous stage, part 1 (per element):
+//   LDG common solution at every own flux point (the delta_disu_fpts of
+//   int_inters::calculate_common_invFlux, src/int_inters.cpp:331-350)
+//   -> corrected reference gradient (calculate_gradient + correct_gradient,
+//   src/eles.cpp:1667-1968) -> physical gradient
+//   -> total discontinuous flux at the solution points (evaluate_invFlux +
+//   evaluate_viscFlux) -> its divergence DV (calculate_divergence) and its
+//   normal component at the flux points ND (extrapolate_totalFlux)
+//   -> viscous flux at the own flux points from the extrapolated state and
+//   gradient (what calculate_common_viscFlux evaluates for this side), kept
+//   only as its projection on the interface's left normal: VF (F-1 values,
+//   the mass component is zero).
+// Outputs VF (n_fpts, n_eles, F-1), ND (n_fpts, n_eles, F), DV (n_upts, n_eles, F).
 template <int DIM, int P, int EPB, int NT, typename TC>
 __global__ void __launch_bounds__(NT)
 fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const int* __restrict__ mate,
                const unsigned char* __restrict__ side, const TC* __restrict__ JG, const TC* __restrict__ detj,
-               TC* __restrict__ GF, TC* __restrict__ RP, long long E, Line<TC> L, PhysT<TC> ph)
+               const TC* __restrict__ nL, TC* __restrict__ VF, TC* __restrict__ ND, TC* __restrict__ DV,
+               long long E, Line<TC> L, PhysT<TC> ph)
 {
   using S = Shape<DIM, P>;
   constexpr int NU = S::NU, NF = S::NF, F = S::F, D = DIM;
+  constexpr int IF = Items<NT, EPB * NF>::N, IU = Items<NT, EPB * NU>::N;
   __shared__ TC sU[EPB][F][NU];
-  __shared__ TC sX[EPB][F][NF];          // delta_disu_fpts, later norm_tdisf_fpts
+  __shared__ TC sX[EPB][F][NF];          // delta_disu_fpts
   __shared__ TC sG[EPB][F * D][NU];      // physical gradient, component k + F*d
   __shared__ TC sFl[EPB][D][F][NU];      // transformed total flux
   const long long e0 = (long long)blockIdx.x * EPB;
+  const long long NFE = (long long)NF * E;
 
+  // --- issue every global gather of the block up front
+  TC pun[IF][F], pn[IF][D];
+  unsigned char psd[IF];
+#pragma unroll
+  for (int it = 0; it < IF; it++) {
+    int w = threadIdx.x + it * NT, el = w / NF, f = w - el * NF;
+    long long e = e0 + el;
+    if (w < EPB * NF && e < E) {
+      size_t own = f + (size_t)NF * e;
+      int mt = mate[own];
+      psd[it] = side[own];
+#pragma unroll
+      for (int k = 0; k < F; k++) pun[it][k] = UF[mt + NFE * k];
+#pragma unroll
+      for (int d = 0; d < D; d++) pn[it][d] = nL[own + NFE * d];
+    }
+  }
+  TC pG[IU][D * D], pdj[IU];
+#pragma unroll
+  for (int it = 0; it < IU; it++) {
+    int w = threadIdx.x + it * NT, el = w / NU, u = w - el * NU;
+    long long e = e0 + el;
+    if (w < EPB * NU && e < E) {
+      const TC* G = JG + (size_t)D * D * (u + (size_t)NU * e);
+#pragma unroll
+      for (int q = 0; q < D * D; q++) pG[it][q] = G[q];
+      pdj[it] = detj[u + (size_t)NU * e];
+    }
+  }
   for (int w = threadIdx.x; w < EPB * F * NU; w += NT) {
     int el = w / (F * NU), r = w - el * F * NU, k = r / NU, u = r - k * NU;
     long long e = e0 + el;
@@ -187,76 +245,62 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
   }
   __syncthreads();
 
-  // LDG common solution u_c = (uL+uR)/2 - beta (uL-uR); delta = u_c - u_own
-  // (int_inters::calculate_common_invFlux + ldg_solution, src/int_inters.cpp:331-350)
-  for (int w = threadIdx.x; w < EPB * NF; w += NT) {
-    int el = w / NF, f = w - el * NF;
-    long long e = e0 + el;
-    if (e >= E) continue;
-    size_t own = f + (size_t)NF * e;
-    int mt = mate[own];
-    unsigned char sd = side[own];
-    TC pen = (sd & 2) ? -ph.pen_fact : ph.pen_fact;
+  // --- LDG common solution u_c = (uL+uR)/2 - beta (uL-uR); delta = u_c - u_own
+#pragma unroll
+  for (int it = 0; it < IF; it++) {
+    int w = threadIdx.x + it * NT, el = w / NF, f = w - el * NF;
+    if (w >= EPB * NF || e0 + el >= E) continue;
+    TC pen = (psd[it] & 2) ? -ph.pen_fact : ph.pen_fact;
 #pragma unroll
     for (int k = 0; k < F; k++) {
       TC uo = line_interp<DIM, P, TC, TC>(L, &sU[el][k][0], 1, f);
-      TC un = UF[mt + (size_t)NF * E * k];
-      TC ul = (sd & 1) ? uo : un, ur = (sd & 1) ? un : uo;
+      TC un = pun[it][k];
+      TC ul = (psd[it] & 1) ? uo : un, ur = (psd[it] & 1) ? un : uo;
       TC uc = TC(0.5) * (ul + ur) - pen * (ul - ur);
       sX[el][k][f] = uc - uo;
     }
   }
   __syncthreads();
 
-  for (int w = threadIdx.x; w < EPB * NU; w += NT) {
-    int el = w / NU, u = w - el * NU;
-    long long e = e0 + el;
-    if (e >= E) continue;
+  // --- gradient and total flux at the solution points
+#pragma unroll
+  for (int it = 0; it < IU; it++) {
+    int w = threadIdx.x + it * NT, el = w / NU, u = w - el * NU;
+    if (w >= EPB * NU || e0 + el >= E) continue;
     int abc[3];
     upt_abc<DIM, P>(u, abc[0], abc[1], abc[2]);
-    // reference gradient opp_4 U + opp_5 delta (faces of each axis in index order)
     TC gr[F][D];
 #pragma unroll
     for (int d = 0; d < D; d++) {
-      const int st = upt_stride<DIM, P>(d);
       const int i = abc[d];
-      const int ub = u - i * st;
       int fm, fp, am, ap;
       if (DIM == 2) { fm = d == 0 ? 3 : 0; fp = d == 0 ? 1 : 2; }
       else { fm = d == 0 ? 4 : (d == 1 ? 1 : 0); fp = d == 0 ? 2 : (d == 1 ? 3 : 5); }
       int qm = face_fpt<DIM, P>(fm, abc[0], abc[1], abc[2], am);
       int qp = face_fpt<DIM, P>(fp, abc[0], abc[1], abc[2], ap);
-      const bool minus_first = fm < fp;
 #pragma unroll
       for (int k = 0; k < F; k++) {
-        TC acc = TC(0);
-#pragma unroll
-        for (int m = 0; m <= P; m++) acc = ffma(sU[el][k][ub + m * st], L.D[i][m], acc);
-        TC cm = L.gL[am] * sX[el][k][qm], cp = L.gR[ap] * sX[el][k][qp];
-        acc = minus_first ? (acc + cm) + cp : (acc + cp) + cm;
+        TC acc = deriv_line<DIM, P, TC, TC>(L, &sU[el][k][0], 1, u, d, i);
+        // opp_5 columns in flux-point order: the lower-numbered face first
+        TC cm = sX[el][k][qm] * L.gL[am], cp = sX[el][k][qp] * L.gR[ap];
+        acc = (fm < fp) ? (acc + cm) + cp : (acc + cp) + cm;
         gr[k][d] = acc;
       }
     }
-    // physical gradient (JGinv^T grad_ref / detJ), src/eles.cpp:1822-1878
-    const TC* G = JG + (size_t)D * D * (u + (size_t)NU * e);
-    TC Gm[D][D];
-#pragma unroll
-    for (int r = 0; r < D; r++)
-#pragma unroll
-      for (int c = 0; c < D; c++) Gm[r][c] = G[r + D * c];
-    TC inv = TC(1) / detj[u + (size_t)NU * e];
+    // physical gradient: d/dx_c = sum_r (JGinv(r,c)/detJ) d/dr (src/eles.cpp:1822-1878)
+    TC inv = TC(1.0) / pdj[it];
     TC gp[F][D];
 #pragma unroll
-    for (int k = 0; k < F; k++)
+    for (int c = 0; c < D; c++) {
+      TC m0 = pG[it][0 + D * c] * inv, m1 = pG[it][1 + D * c] * inv, m2 = D == 3 ? pG[it][2 + D * c] * inv : TC(0);
 #pragma unroll
-      for (int c = 0; c < D; c++) {
-        TC acc = TC(0);
-#pragma unroll
-        for (int r = 0; r < D; r++) acc = ffma(gr[k][r], Gm[r][c] * inv, acc);
+      for (int k = 0; k < F; k++) {
+        TC acc = gr[k][0] * m0 + gr[k][1] * m1;
+        if (D == 3) acc = acc + gr[k][2] * m2;
         gp[k][c] = acc;
         sG[el][k + F * c][u] = acc;
       }
-    // total discontinuous flux transformed to the reference element
+    }
     TC q[F];
 #pragma unroll
     for (int k = 0; k < F; k++) q[k] = sU[el][k][u];
@@ -267,208 +311,240 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
     for (int k = 0; k < F; k++)
 #pragma unroll
       for (int l = 0; l < D; l++) {
-        TC acc = TC(0);
+        TC acc = pG[it][l] * fi[k][0];
 #pragma unroll
-        for (int m = 0; m < D; m++) acc = ffma(Gm[l][m], fi[k][m], acc);
+        for (int m = 1; m < D; m++) acc = acc + pG[it][l + D * m] * fi[k][m];
 #pragma unroll
-        for (int m = 0; m < D; m++) acc = ffma(Gm[l][m], fv[k][m], acc);
+        for (int m = 0; m < D; m++) acc = acc + pG[it][l + D * m] * fv[k][m];
         sFl[el][l][k][u] = acc;
       }
   }
   __syncthreads();
 
-  // gradient traces and the discontinuous normal flux at the flux points
-  for (int w = threadIdx.x; w < EPB * NF; w += NT) {
-    int el = w / NF, f = w - el * NF;
-    long long e = e0 + el;
-    if (e >= E) continue;
+  // --- flux points: own viscous flux projected on the left normal, and the
+  //     discontinuous normal flux
 #pragma unroll
-    for (int c = 0; c < F * D; c++)
-      GF[f + (size_t)NF * (e + E * (size_t)c)] = line_interp<DIM, P, TC, TC>(L, &sG[el][c][0], 1, f);
+  for (int it = 0; it < IF; it++) {
+    int w = threadIdx.x + it * NT, el = w / NF, f = w - el * NF;
+    long long e = e0 + el;
+    if (w >= EPB * NF || e >= E) continue;
+    size_t own = f + (size_t)NF * e;
+    TC uf[F], gf[F][D], fv[F][D];
+#pragma unroll
+    for (int k = 0; k < F; k++) {
+      uf[k] = line_interp<DIM, P, TC, TC>(L, &sU[el][k][0], 1, f);
+#pragma unroll
+      for (int d = 0; d < D; d++) gf[k][d] = line_interp<DIM, P, TC, TC>(L, &sG[el][k + F * d][0], 1, f);
+    }
+    vis_flux<D, TC>(ph, uf, gf, fv);
+#pragma unroll
+    for (int k = 1; k < F; k++) VF[own + NFE * (k - 1)] = project<D, TC>(fv, k, pn[it]);
     int u0, st, ax; bool plus;
     fpt_line<DIM, P>(f, u0, st, ax, plus);
 #pragma unroll
     for (int k = 0; k < F; k++) {
       TC v = line_interp<DIM, P, TC, TC>(L, &sFl[el][ax][k][0], 1, f);
-      sX[el][k][f] = plus ? v : -v;
+      ND[own + NFE * k] = plus ? v : -v;
     }
   }
-  __syncthreads();
-
-  for (int w = threadIdx.x; w < EPB * NU; w += NT) {
-    int el = w / NU, u = w - el * NU;
+  // --- divergence of the total discontinuous flux
+#pragma unroll
+  for (int it = 0; it < IU; it++) {
+    int w = threadIdx.x + it * NT, el = w / NU, u = w - el * NU;
     long long e = e0 + el;
-    if (e >= E) continue;
+    if (w >= EPB * NU || e >= E) continue;
     int abc[3];
     upt_abc<DIM, P>(u, abc[0], abc[1], abc[2]);
 #pragma unroll
     for (int k = 0; k < F; k++) {
-      TC acc = TC(0);
+      TC acc = deriv_line<DIM, P, TC, TC>(L, &sFl[el][0][k][0], 1, u, 0, abc[0]);
 #pragma unroll
-      for (int d = 0; d < D; d++) {
-        const int st = upt_stride<DIM, P>(d), i = abc[d], ub = u - i * st;
+      for (int d = 1; d < D; d++) {
+        const int st = upt_stride<DIM, P>(d), ub = u - abc[d] * st;
 #pragma unroll
-        for (int m = 0; m <= P; m++) acc = ffma(sFl[el][d][k][ub + m * st], L.D[i][m], acc);
+        for (int m = 0; m <= P; m++) acc = acc + sFl[el][d][k][ub + m * st] * L.D[abc[d]][m];
       }
-#pragma unroll
-      for (int fc = 0; fc < S::NFACE; fc++) {
-        int al;
-        int q = face_fpt<DIM, P>(fc, abc[0], abc[1], abc[2], al);
-        TC cf = face_plus<DIM>(fc) ? L.gR[al] : -L.gL[al];
-        acc = ffma(-cf, sX[el][k][q], acc);
-      }
-      RP[u + (size_t)NU * (e + E * k)] = acc;
+      DV[u + (size_t)NU * (e + E * k)] = acc;
     }
   }
 }
 
 // ---------------------------------------------------------------------------
-// Common interface fluxes (Rusanov + LDG), correction, and either the
-// residual (MODE 0) or the RK45 stage update with the next stage's traces
-// (MODE 1).  For the inviscid path this kernel also evaluates the flux and
-// its divergence itself (RP unused).
+// Stage, part 2 (per element): common interface fluxes (Rusanov + LDG from the
+// normal projections), norm_tconf - norm_tdisf, the VCJH correction
+// (calculate_corrected_divergence), and either the residual (MODE 0) or the
+// RK45 stage update with the next stage's traces (MODE 1).  The inviscid path
+// (VISC 0) evaluates the flux, its divergence and its normal component here
+// itself, in the reference's order.
 template <int DIM, int P, int EPB, int NT, int VISC, int MODE, typename TC>
 __global__ void __launch_bounds__(NT)
 fr_flux_kernel(double* __restrict__ U, double* __restrict__ REG, const TC* __restrict__ UF,
-               TC* __restrict__ UFn, const TC* __restrict__ GF, const TC* __restrict__ RP,
-               const int* __restrict__ mate, const unsigned char* __restrict__ side, const TC* __restrict__ nL,
-               const TC* __restrict__ tdA, const TC* __restrict__ JG, const double* __restrict__ detj,
-               double* __restrict__ DIV, double* __restrict__ partial, long long E, Line<TC> L, PhysT<TC> ph,
-               double rk_a, double rk_b, double dt, int first_stage)
+               TC* __restrict__ UFn, const TC* __restrict__ VF, const TC* __restrict__ ND,
+               const TC* __restrict__ DV, const int* __restrict__ mate, const unsigned char* __restrict__ side,
+               const TC* __restrict__ nL, const TC* __restrict__ tdA, const TC* __restrict__ JG,
+               const double* __restrict__ detj, double* __restrict__ DIV, double* __restrict__ partial, long long E,
+               Line<TC> L, PhysT<TC> ph, double rk_a, double rk_b, double dt, int first_stage)
 {
   using S = Shape<DIM, P>;
   constexpr int NU = S::NU, NF = S::NF, F = S::F, D = DIM;
+  constexpr int IF = Items<NT, EPB * NF>::N, IU = Items<NT, EPB * NU>::N;
   __shared__ double sU[EPB][F][NU];
-  __shared__ TC sC[EPB][F][NF];                       // common minus own normal flux
-  __shared__ TC sFl[VISC ? 1 : EPB][D][VISC ? 1 : NU][VISC ? 1 : F];
+  __shared__ TC sC[EPB][F][NF];                       // norm_tconf - norm_tdisf
+  __shared__ TC sFl[VISC ? 1 : EPB][D][VISC ? 1 : F][VISC ? 1 : NU];
   __shared__ double sRed[NT / 32][F];
   const long long e0 = (long long)blockIdx.x * EPB;
+  const long long NFE = (long long)NF * E;
 
+  // --- global gathers first
+  TC pun[IF][F], pn[IF][D], pta[IF], pvo[IF][VISC ? F - 1 : 1], pvn[IF][VISC ? F - 1 : 1], pnd[IF][VISC ? F : 1];
+  unsigned char psd[IF];
+#pragma unroll
+  for (int it = 0; it < IF; it++) {
+    int w = threadIdx.x + it * NT, el = w / NF, f = w - el * NF;
+    long long e = e0 + el;
+    if (w < EPB * NF && e < E) {
+      size_t own = f + (size_t)NF * e;
+      int mt = mate[own];
+      psd[it] = side[own];
+      pta[it] = tdA[own];
+#pragma unroll
+      for (int k = 0; k < F; k++) pun[it][k] = UF[mt + NFE * k];
+#pragma unroll
+      for (int d = 0; d < D; d++) pn[it][d] = nL[own + NFE * d];
+      if (VISC) {
+#pragma unroll
+        for (int k = 0; k < F - 1; k++) { pvo[it][k] = VF[own + NFE * k]; pvn[it][k] = VF[mt + NFE * k]; }
+#pragma unroll
+        for (int k = 0; k < F; k++) pnd[it][k] = ND[own + NFE * k];
+      }
+    }
+  }
+  TC pdv[IU][VISC ? F : 1], pG[IU][VISC ? 1 : D * D];
+  double preg[IU][MODE ? F : 1], pdj[IU];
+#pragma unroll
+  for (int it = 0; it < IU; it++) {
+    int w = threadIdx.x + it * NT, el = w / NU, u = w - el * NU;
+    long long e = e0 + el;
+    if (w < EPB * NU && e < E) {
+      size_t p = u + (size_t)NU * e;
+      pdj[it] = detj[p];
+      if (VISC) {
+#pragma unroll
+        for (int k = 0; k < F; k++) pdv[it][k] = DV[u + (size_t)NU * (e + E * k)];
+      } else {
+#pragma unroll
+        for (int q = 0; q < D * D; q++) pG[it][q] = JG[(size_t)D * D * p + q];
+      }
+      if (MODE == 1 && !first_stage) {
+#pragma unroll
+        for (int k = 0; k < F; k++) preg[it][k] = REG[u + (size_t)NU * (e + E * k)];
+      }
+    }
+  }
   for (int w = threadIdx.x; w < EPB * F * NU; w += NT) {
     int el = w / (F * NU), r = w - el * F * NU, k = r / NU, u = r - k * NU;
     long long e = e0 + el;
     sU[el][k][u] = e < E ? U[u + (size_t)NU * (e + E * k)] : 1.0;
   }
+  __syncthreads();
+
   if (!VISC) {
-    __syncthreads();
-    // transformed inviscid flux at the solution points (evaluate_invFlux,
-    // src/eles.cpp:1331-1418)
-    for (int w = threadIdx.x; w < EPB * NU; w += NT) {
-      int el = w / NU, u = w - el * NU;
-      long long e = e0 + el;
-      if (e >= E) continue;
+    // transformed inviscid flux at the solution points (evaluate_invFlux, src/eles.cpp:1331-1418)
+#pragma unroll
+    for (int it = 0; it < IU; it++) {
+      int w = threadIdx.x + it * NT, el = w / NU, u = w - el * NU;
+      if (w >= EPB * NU || e0 + el >= E) continue;
       TC q[F], fi[F][D];
 #pragma unroll
       for (int k = 0; k < F; k++) q[k] = (TC)sU[el][k][u];
       inv_flux<D, TC>(ph, q, fi);
-      const TC* G = JG + (size_t)D * D * (u + (size_t)NU * e);
 #pragma unroll
-      for (int l = 0; l < D; l++) {
-        TC g[D];
-#pragma unroll
-        for (int m = 0; m < D; m++) g[m] = G[l + D * m];
+      for (int l = 0; l < D; l++)
 #pragma unroll
         for (int k = 0; k < F; k++) {
-          TC acc = TC(0);
+          TC acc = pG[it][l] * fi[k][0];
 #pragma unroll
-          for (int m = 0; m < D; m++) acc = ffma(g[m], fi[k][m], acc);
-          sFl[el][l][u][k] = acc;
+          for (int m = 1; m < D; m++) acc = acc + pG[it][l + D * m] * fi[k][m];
+          sFl[el][l][k][u] = acc;
         }
-      }
     }
+    __syncthreads();
   }
-  __syncthreads();
 
-  // common normal flux at every flux point of the block's elements
-  for (int w = threadIdx.x; w < EPB * NF; w += NT) {
-    int el = w / NF, f = w - el * NF;
-    long long e = e0 + el;
-    if (e >= E) continue;
-    size_t own = f + (size_t)NF * e;
-    int mt = mate[own];
-    bool left = side[own] & 1;
-    TC uo[F], un[F], n[D];
+  // --- common normal flux minus the discontinuous normal flux at every own flux point
 #pragma unroll
-    for (int k = 0; k < F; k++) {
-      uo[k] = line_interp<DIM, P, TC, double>(L, &sU[el][k][0], 1, f);
-      un[k] = UF[mt + (size_t)NF * E * k];
-    }
+  for (int it = 0; it < IF; it++) {
+    int w = threadIdx.x + it * NT, el = w / NF, f = w - el * NF;
+    if (w >= EPB * NF || e0 + el >= E) continue;
+    const bool left = psd[it] & 1;
+    TC uo[F];
 #pragma unroll
-    for (int d = 0; d < D; d++) n[d] = nL[own + (size_t)NF * E * d];
-    const TC* ul = left ? uo : un;
-    const TC* ur = left ? un : uo;
+    for (int k = 0; k < F; k++) uo[k] = line_interp<DIM, P, TC, double>(L, &sU[el][k][0], 1, f);
+    const TC* ul = left ? uo : pun[it];
+    const TC* ur = left ? pun[it] : uo;
     TC fn[F];
-    rusanov<D, TC>(ph, ul, ur, n, fn);
-    TC ta = tdA[own];
+    rusanov<D, TC>(ph, ul, ur, pn[it], fn);
+    const TC ta = pta[it];
     TC c[F];
 #pragma unroll
     for (int k = 0; k < F; k++) c[k] = left ? fn[k] * ta : -fn[k] * ta;
     if (VISC) {
-      TC go[F][D], gn[F][D];
+      TC nn = pn[it][0] * pn[it][0];
 #pragma unroll
-      for (int k = 0; k < F; k++)
+      for (int d = 1; d < D; d++) nn = nn + pn[it][d] * pn[it][d];
+      const TC pen = (psd[it] & 2) ? -ph.pen_fact : ph.pen_fact;
 #pragma unroll
-        for (int d = 0; d < D; d++) {
-          go[k][d] = GF[own + (size_t)NF * E * (k + F * d)];
-          gn[k][d] = GF[mt + (size_t)NF * E * (k + F * d)];
-        }
-      TC fo[F][D], fnb[F][D];
-      vis_flux<D, TC>(ph, uo, go, fo);
-      vis_flux<D, TC>(ph, un, gn, fnb);
-      TC fv[F];
-      TC pen = (side[own] & 2) ? -ph.pen_fact : ph.pen_fact;
-      if (left) ldg_flux<D, TC>(ph, pen, uo, un, fo, fnb, n, fv);
-      else ldg_flux<D, TC>(ph, pen, un, uo, fnb, fo, n, fv);
-#pragma unroll
-      for (int k = 0; k < F; k++) c[k] += left ? fv[k] * ta : -fv[k] * ta;
+      for (int k = 0; k < F; k++) {
+        TC ao = k ? pvo[it][k - 1] : TC(0), an = k ? pvn[it][k - 1] : TC(0);
+        TC fv = left ? ldg_normal<TC>(ao, an, ul[k], ur[k], pen, ph.tau, nn)
+                     : ldg_normal<TC>(an, ao, ul[k], ur[k], pen, ph.tau, nn);
+        c[k] = c[k] + (left ? fv * ta : -fv * ta);
+        sC[el][k][f] = c[k] - pnd[it][k];
+      }
     } else {
-      // subtract the discontinuous normal flux (extrapolate_totalFlux + daxpy)
       int u0, st, ax; bool plus;
       fpt_line<DIM, P>(f, u0, st, ax, plus);
 #pragma unroll
       for (int k = 0; k < F; k++) {
-        TC acc = TC(0);
-#pragma unroll
-        for (int m = 0; m <= P; m++) acc = ffma(sFl[el][ax][u0 + m * st][k], plus ? L.Lp[m] : L.Lm[m], acc);
-        c[k] = c[k] + (plus ? -acc : acc);
+        TC v = line_interp<DIM, P, TC, TC>(L, &sFl[el][ax][k][0], 1, f);
+        sC[el][k][f] = c[k] - (plus ? v : -v);
       }
     }
-#pragma unroll
-    for (int k = 0; k < F; k++) sC[el][k][f] = c[k];
   }
   __syncthreads();
 
   double red[F];
 #pragma unroll
   for (int k = 0; k < F; k++) red[k] = 0.0;
-  for (int w = threadIdx.x; w < EPB * NU; w += NT) {
-    int el = w / NU, u = w - el * NU;
+#pragma unroll
+  for (int it = 0; it < IU; it++) {
+    int w = threadIdx.x + it * NT, el = w / NU, u = w - el * NU;
     long long e = e0 + el;
-    if (e >= E) continue;
+    if (w >= EPB * NU || e >= E) continue;
     int abc[3];
     upt_abc<DIM, P>(u, abc[0], abc[1], abc[2]);
-    double dj = detj[u + (size_t)NU * e];
+    const double dj = pdj[it];
 #pragma unroll
     for (int k = 0; k < F; k++) {
       TC acc;
       if (VISC) {
-        acc = RP[u + (size_t)NU * (e + E * k)];
+        acc = pdv[it][k];
       } else {
-        acc = TC(0);
+        acc = deriv_line<DIM, P, TC, TC>(L, &sFl[el][0][k][0], 1, u, 0, abc[0]);
 #pragma unroll
-        for (int d = 0; d < D; d++) {
-          const int st = upt_stride<DIM, P>(d), i = abc[d], ub = u - i * st;
+        for (int d = 1; d < D; d++) {
+          const int st = upt_stride<DIM, P>(d), ub = u - abc[d] * st;
 #pragma unroll
-          for (int m = 0; m <= P; m++) acc = ffma(sFl[el][d][ub + m * st][k], L.D[i][m], acc);
+          for (int m = 0; m <= P; m++) acc = acc + sFl[el][d][k][ub + m * st] * L.D[abc[d]][m];
         }
       }
-      // correction with the VCJH function derivatives (calculate_corrected_divergence)
+      // opp_3 row of u: one column per face, in flux-point order
 #pragma unroll
       for (int fc = 0; fc < S::NFACE; fc++) {
         int al;
         int q = face_fpt<DIM, P>(fc, abc[0], abc[1], abc[2], al);
         TC cf = face_plus<DIM>(fc) ? L.gR[al] : -L.gL[al];
-        acc = ffma(cf, sC[el][k][q], acc);
+        acc = acc + sC[el][k][q] * cf;
       }
       size_t gi = u + (size_t)NU * (e + E * k);
       double R = (double)acc;
@@ -476,12 +552,12 @@ fr_flux_kernel(double* __restrict__ U, double* __restrict__ REG, const TC* __res
         DIV[gi] = R;
       } else {
         double rhs = -R / dj;
-        double res = first_stage ? dt * rhs : ffma(rk_a, REG[gi], dt * rhs);
+        double res = first_stage ? dt * rhs : rk_a * preg[it][k] + dt * rhs;
         REG[gi] = res;
-        double un = ffma(rk_b, res, sU[el][k][u]);
+        double un = sU[el][k][u] + rk_b * res;
         U[gi] = un;
         sU[el][k][u] = un;
-        red[k] += fabs(R / dj);
+        red[k] += fabs(rhs);
       }
     }
   }
@@ -504,10 +580,11 @@ fr_flux_kernel(double* __restrict__ U, double* __restrict__ REG, const TC* __res
       partial[(size_t)blockIdx.x * F + threadIdx.x] = v;
     }
     // traces of the updated state for the next stage
-    for (int w = threadIdx.x; w < EPB * NF; w += NT) {
-      int el = w / NF, f = w - el * NF;
+#pragma unroll
+    for (int it = 0; it < IF; it++) {
+      int w = threadIdx.x + it * NT, el = w / NF, f = w - el * NF;
       long long e = e0 + el;
-      if (e >= E) continue;
+      if (w >= EPB * NF || e >= E) continue;
 #pragma unroll
       for (int k = 0; k < F; k++)
         UFn[f + (size_t)NF * (e + E * k)] = line_interp<DIM, P, TC, double>(L, &sU[el][k][0], 1, f);

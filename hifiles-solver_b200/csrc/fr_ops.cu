@@ -1,0 +1,449 @@
+// fr_ops.cu -- per-operator entry points: the reference's GPU seam, one call
+// per method of class eles / int_inters, on caller-owned device arrays in the
+// reference's own layouts.  Operators are the reference's dense matrices
+// (opp_0 .. opp_6, any element type); interface data come through the same
+// device tables of device pointers that int_inters builds
+// (src/int_inters.cpp:95-178), so a caller can swap these in for the
+// cublasDgemm / *_kernel_wrapper calls without touching its data.
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "fr_b200.h"
+#include "fr_physics.cuh"
+
+namespace frb {
+extern thread_local std::string g_err;
+}
+using namespace frb;
+
+namespace {
+
+fr_status op_fail(fr_status s, const std::string& m)
+{
+  g_err = m;
+  return s;
+}
+
+fr_status launched(const char* what)
+{
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return op_fail(FR_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  return FR_OK;
+}
+
+constexpr int kTileCols = 32;
+constexpr int kDenseThreads = 256;
+
+// C(:, j) = beta*C(:, j) + A * B(:, j) for all ncols columns, A (m x k) column
+// major, B (k x ncols) and C (m x ncols) with leading dimensions k and m (the
+// reference's cublasDgemm('N','N', m, ncols, k, 1, A, m, B, k, beta, C, m)).
+// A column tile of B and C is staged through shared memory so both global
+// streams are contiguous; A is read through the read-only cache (every lane
+// of a warp reads the same entry).  Summation runs over l in increasing order.
+__global__ void __launch_bounds__(kDenseThreads)
+dense_apply_kernel(int m, int k, long long ncols, const double* __restrict__ A, const double* __restrict__ B,
+                   double* __restrict__ Cm, int beta)
+{
+  extern __shared__ double sm[];
+  double* sB = sm;                         // [k][kTileCols]
+  double* sC = sm + (size_t)k * kTileCols; // [kTileCols][m]
+  long long c0 = (long long)blockIdx.x * kTileCols;
+  int nc = (int)min((long long)kTileCols, ncols - c0);
+  const double* Bt = B + (size_t)c0 * k;
+  for (int i = threadIdx.x; i < nc * k; i += kDenseThreads) {
+    int c = i / k, l = i - c * k;
+    sB[l * kTileCols + c] = Bt[i];
+  }
+  double* Ct = Cm + (size_t)c0 * m;
+  if (beta)
+    for (int i = threadIdx.x; i < nc * m; i += kDenseThreads) sC[i] = Ct[i];
+  __syncthreads();
+  int c = threadIdx.x % kTileCols;
+  for (int r = threadIdx.x / kTileCols; r < m; r += kDenseThreads / kTileCols) {
+    if (c < nc) {
+      double acc = beta ? sC[c * m + r] : 0.0;
+      for (int l = 0; l < k; l++) acc = fma(sB[l * kTileCols + c], __ldg(A + r + (size_t)m * l), acc);
+      sC[c * m + r] = acc;
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nc * m; i += kDenseThreads) Ct[i] = sC[i];
+}
+
+fr_status dense_apply(int m, int k, long long ncols, const double* A, const double* B, double* Cm, int beta,
+                      cudaStream_t s)
+{
+  if (m <= 0 || k <= 0 || ncols < 0 || !A || !B || !Cm) return op_fail(FR_ERR_ARG, "bad operator arguments");
+  if (ncols == 0) return FR_OK;
+  size_t smem = ((size_t)k * kTileCols + (size_t)kTileCols * m) * sizeof(double);
+  if (smem > 220 * 1024) return op_fail(FR_ERR_UNSUPPORTED, "operator too large for one column tile");
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(dense_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return op_fail(FR_ERR_CUDA, cudaGetErrorString(e));
+  }
+  long long blocks = (ncols + kTileCols - 1) / kTileCols;
+  if (blocks > 2147483647LL) return op_fail(FR_ERR_ARG, "too many columns");
+  dense_apply_kernel<<<(unsigned)blocks, kDenseThreads, smem, s>>>(m, k, ncols, A, B, Cm, beta);
+  return launched("dense_apply_kernel");
+}
+
+// ------------------------------------------------------------ pointwise kernels
+
+template <int D>
+__global__ void inv_flux_kernel(int nu, long long E, const double* __restrict__ U, const double* __restrict__ JG,
+                                double* __restrict__ TF, PhysT<double> ph)
+{
+  constexpr int F = D + 2;
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)nu * E) return;
+  size_t NE = (size_t)nu * E;
+  double q[F], f[F][D];
+#pragma unroll
+  for (int k = 0; k < F; k++) q[k] = U[i + NE * k];
+  inv_flux<D, double>(ph, q, f);
+  const double* G = JG + (size_t)D * D * i;
+#pragma unroll
+  for (int k = 0; k < F; k++)
+#pragma unroll
+    for (int l = 0; l < D; l++) {
+      double acc = 0.0;
+#pragma unroll
+      for (int mm = 0; mm < D; mm++) acc = fma(G[l + D * mm], f[k][mm], acc);
+      TF[i + NE * (k + (size_t)F * l)] = acc;
+    }
+}
+
+template <int D>
+__global__ void vis_flux_kernel(int nu, long long E, const double* __restrict__ U, const double* __restrict__ GU,
+                                const double* __restrict__ JG, double* __restrict__ TF, PhysT<double> ph)
+{
+  constexpr int F = D + 2;
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)nu * E) return;
+  size_t NE = (size_t)nu * E;
+  double q[F], g[F][D], f[F][D];
+#pragma unroll
+  for (int k = 0; k < F; k++) {
+    q[k] = U[i + NE * k];
+#pragma unroll
+    for (int d = 0; d < D; d++) g[k][d] = GU[i + NE * (k + (size_t)F * d)];
+  }
+  vis_flux<D, double>(ph, q, g, f);
+  const double* G = JG + (size_t)D * D * i;
+#pragma unroll
+  for (int k = 0; k < F; k++)
+#pragma unroll
+    for (int l = 0; l < D; l++) {
+      double acc = TF[i + NE * (k + (size_t)F * l)];
+#pragma unroll
+      for (int mm = 0; mm < D; mm++) acc = fma(G[l + D * mm], f[k][mm], acc);
+      TF[i + NE * (k + (size_t)F * l)] = acc;
+    }
+}
+
+// reference gradient -> physical gradient in place (src/eles.cpp:1822-1878)
+template <int D>
+__global__ void grad_transform_kernel(int nu, long long E, int F, double* __restrict__ GU,
+                                      const double* __restrict__ JG, const double* __restrict__ detj)
+{
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)nu * E) return;
+  size_t NE = (size_t)nu * E;
+  double inv = 1.0 / detj[i];
+  const double* G = JG + (size_t)D * D * i;
+  double Gm[D][D];
+#pragma unroll
+  for (int r = 0; r < D; r++)
+#pragma unroll
+    for (int c = 0; c < D; c++) Gm[r][c] = G[r + D * c] * inv;
+  for (int k = 0; k < F; k++) {
+    double gr[D];
+#pragma unroll
+    for (int d = 0; d < D; d++) gr[d] = GU[i + NE * (k + (size_t)F * d)];
+#pragma unroll
+    for (int c = 0; c < D; c++) {
+      double acc = 0.0;
+#pragma unroll
+      for (int r = 0; r < D; r++) acc = fma(gr[r], Gm[r][c], acc);
+      GU[i + NE * (k + (size_t)F * c)] = acc;
+    }
+  }
+}
+
+__global__ void axpy_kernel(long long n, double a, const double* __restrict__ x, double* __restrict__ y)
+{
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = fma(a, x[i], y[i]);
+}
+
+// RK45 stage update (RK45_update_kernel of the reference, src/cuda_kernels.cu:2654-2690;
+// CPU form src/eles.cpp:1155-1178) for fixed time steps.
+__global__ void rk45_kernel(int nu, long long E, int F, double* __restrict__ u0, double* __restrict__ u1,
+                            const double* __restrict__ div, const double* __restrict__ detj,
+                            const double* __restrict__ src, double a, double b, double dt, double const_src)
+{
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)nu * E;
+  if (i >= n * F) return;
+  long long p = i % n;
+  double rhs = -div[i] / detj[p] + const_src + (src ? src[i] : 0.0);
+  double res = fma(a, u1[i], dt * rhs);
+  u1[i] = res;
+  u0[i] = fma(b, res, u0[i]);
+}
+
+// ---------------------------------------------------------- interface kernels
+// Tables follow int_inters (src/int_inters.cpp:95-178): *_l / *_r are
+// (n_fpts_per_inter, n_inters, n_fields[, n_dims]) arrays of pointers into the
+// elements' flux-point arrays; tdA_l/_r (n_fpts_per_inter, n_inters); norm
+// (n_fpts_per_inter, n_inters, n_dims) points at the left element's normals.
+
+template <int D>
+__global__ void common_inv_kernel(int nfpi, int ni, double* const* __restrict__ ul_p, double* const* __restrict__ ur_p,
+                                  double* const* __restrict__ tl_p, double* const* __restrict__ tr_p,
+                                  double* const* __restrict__ al_p, double* const* __restrict__ ar_p,
+                                  double* const* __restrict__ n_p, double* const* __restrict__ dl_p,
+                                  double* const* __restrict__ dr_p, PhysT<double> ph, int viscous)
+{
+  constexpr int F = D + 2;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)nfpi * ni;
+  if (t >= n) return;
+  double ul[F], ur[F], nn[D], fn[F];
+#pragma unroll
+  for (int k = 0; k < F; k++) { ul[k] = *ul_p[t + n * k]; ur[k] = *ur_p[t + n * k]; }
+#pragma unroll
+  for (int d = 0; d < D; d++) nn[d] = *n_p[t + n * d];
+  rusanov<D, double>(ph, ul, ur, nn, fn);
+  double tal = *al_p[t], tar = *ar_p[t];
+#pragma unroll
+  for (int k = 0; k < F; k++) { *tl_p[t + n * k] = fn[k] * tal; *tr_p[t + n * k] = -fn[k] * tar; }
+  if (viscous) {
+    double pen = ldg_beta<D, double>(ph.pen_fact, nn);
+#pragma unroll
+    for (int k = 0; k < F; k++) {
+      double uc = 0.5 * (ul[k] + ur[k]) - pen * (ul[k] - ur[k]);
+      *dl_p[t + n * k] = uc - ul[k];
+      *dr_p[t + n * k] = uc - ur[k];
+    }
+  }
+}
+
+template <int D>
+__global__ void common_vis_kernel(int nfpi, int ni, double* const* __restrict__ ul_p, double* const* __restrict__ ur_p,
+                                  double* const* __restrict__ gl_p, double* const* __restrict__ gr_p,
+                                  double* const* __restrict__ tl_p, double* const* __restrict__ tr_p,
+                                  double* const* __restrict__ al_p, double* const* __restrict__ ar_p,
+                                  double* const* __restrict__ n_p, PhysT<double> ph)
+{
+  constexpr int F = D + 2;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)nfpi * ni;
+  if (t >= n) return;
+  double ul[F], ur[F], gl[F][D], gr[F][D], fl[F][D], fr[F][D], nn[D], fn[F];
+#pragma unroll
+  for (int k = 0; k < F; k++) {
+    ul[k] = *ul_p[t + n * k]; ur[k] = *ur_p[t + n * k];
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      gl[k][d] = *gl_p[t + n * (k + (long long)F * d)];
+      gr[k][d] = *gr_p[t + n * (k + (long long)F * d)];
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < D; d++) nn[d] = *n_p[t + n * d];
+  vis_flux<D, double>(ph, ul, gl, fl);
+  vis_flux<D, double>(ph, ur, gr, fr);
+  ldg_flux<D, double>(ph, ldg_beta<D, double>(ph.pen_fact, nn), ul, ur, fl, fr, nn, fn);
+  double tal = *al_p[t], tar = *ar_p[t];
+#pragma unroll
+  for (int k = 0; k < F; k++) { *tl_p[t + n * k] += fn[k] * tal; *tr_p[t + n * k] += -fn[k] * tar; }
+}
+
+inline unsigned grid_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+PhysT<double> phys_of(const fr_phys_desc* p)
+{
+  Phys q{p->gamma, p->prandtl, p->mu_inf, p->rt_inf, p->c_sth, p->fix_vis, p->tau, p->pen_fact};
+  return PhysT<double>::make(q);
+}
+
+bool dims_ok(int d, int F) { return (d == 2 && F == 4) || (d == 3 && F == 5); }
+
+}  // namespace
+
+#define ST(stream) ((cudaStream_t)(stream))
+
+extern "C" {
+
+fr_status fr_op_extrapolate_solution(int n_fpts, int n_upts, int n_fields, int n_eles, const double* opp_0,
+                                     const double* disu_upts, double* disu_fpts, void* stream)
+{
+  return dense_apply(n_fpts, n_upts, (long long)n_fields * n_eles, opp_0, disu_upts, disu_fpts, 0, ST(stream));
+}
+
+fr_status fr_op_evaluate_invFlux(int n_upts, int n_dims, int n_fields, int n_eles, const double* disu_upts,
+                                 const double* JGinv_upts, double* tdisf_upts, const fr_phys_desc* phys,
+                                 void* stream)
+{
+  if (!phys || !disu_upts || !JGinv_upts || !tdisf_upts || !dims_ok(n_dims, n_fields))
+    return op_fail(FR_ERR_ARG, "bad arguments");
+  long long n = (long long)n_upts * n_eles;
+  if (n == 0) return FR_OK;
+  if (n_dims == 2) inv_flux_kernel<2><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_upts, n_eles, disu_upts, JGinv_upts, tdisf_upts, phys_of(phys));
+  else inv_flux_kernel<3><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_upts, n_eles, disu_upts, JGinv_upts, tdisf_upts, phys_of(phys));
+  return launched("inv_flux_kernel");
+}
+
+fr_status fr_op_calculate_gradient(int n_upts, int n_dims, int n_fields, int n_eles, const double* const* opp_4,
+                                   const double* disu_upts, double* grad_disu_upts, void* stream)
+{
+  if (!opp_4 || n_dims < 2 || n_dims > 3) return op_fail(FR_ERR_ARG, "bad arguments");
+  long long cols = (long long)n_fields * n_eles;
+  for (int d = 0; d < n_dims; d++) {
+    fr_status st = dense_apply(n_upts, n_upts, cols, opp_4[d], disu_upts, grad_disu_upts + (size_t)n_upts * cols * d,
+                               0, ST(stream));
+    if (st) return st;
+  }
+  return FR_OK;
+}
+
+fr_status fr_op_correct_gradient(int n_upts, int n_fpts, int n_dims, int n_fields, int n_eles,
+                                 const double* const* opp_5, const double* delta_disu_fpts, const double* JGinv_upts,
+                                 const double* detjac_upts, double* grad_disu_upts, void* stream)
+{
+  if (!opp_5 || n_dims < 2 || n_dims > 3 || !JGinv_upts || !detjac_upts) return op_fail(FR_ERR_ARG, "bad arguments");
+  long long cols = (long long)n_fields * n_eles;
+  for (int d = 0; d < n_dims; d++) {
+    fr_status st = dense_apply(n_upts, n_fpts, cols, opp_5[d], delta_disu_fpts,
+                               grad_disu_upts + (size_t)n_upts * cols * d, 1, ST(stream));
+    if (st) return st;
+  }
+  long long n = (long long)n_upts * n_eles;
+  if (n_dims == 2) grad_transform_kernel<2><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_upts, n_eles, n_fields, grad_disu_upts, JGinv_upts, detjac_upts);
+  else grad_transform_kernel<3><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_upts, n_eles, n_fields, grad_disu_upts, JGinv_upts, detjac_upts);
+  return launched("grad_transform_kernel");
+}
+
+fr_status fr_op_extrapolate_corrected_gradient(int n_fpts, int n_upts, int n_dims, int n_fields, int n_eles,
+                                               const double* opp_6, const double* grad_disu_upts,
+                                               double* grad_disu_fpts, void* stream)
+{
+  long long cols = (long long)n_fields * n_eles;
+  for (int d = 0; d < n_dims; d++) {
+    fr_status st = dense_apply(n_fpts, n_upts, cols, opp_6, grad_disu_upts + (size_t)n_upts * cols * d,
+                               grad_disu_fpts + (size_t)n_fpts * cols * d, 0, ST(stream));
+    if (st) return st;
+  }
+  return FR_OK;
+}
+
+fr_status fr_op_evaluate_viscFlux(int n_upts, int n_dims, int n_fields, int n_eles, const double* disu_upts,
+                                  const double* grad_disu_upts, const double* JGinv_upts, double* tdisf_upts,
+                                  const fr_phys_desc* phys, void* stream)
+{
+  if (!phys || !disu_upts || !grad_disu_upts || !JGinv_upts || !tdisf_upts || !dims_ok(n_dims, n_fields))
+    return op_fail(FR_ERR_ARG, "bad arguments");
+  long long n = (long long)n_upts * n_eles;
+  if (n == 0) return FR_OK;
+  if (n_dims == 2) vis_flux_kernel<2><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_upts, n_eles, disu_upts, grad_disu_upts, JGinv_upts, tdisf_upts, phys_of(phys));
+  else vis_flux_kernel<3><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_upts, n_eles, disu_upts, grad_disu_upts, JGinv_upts, tdisf_upts, phys_of(phys));
+  return launched("vis_flux_kernel");
+}
+
+fr_status fr_op_extrapolate_totalFlux(int n_fpts, int n_upts, int n_dims, int n_fields, int n_eles,
+                                      const double* const* opp_1, const double* tdisf_upts, double* norm_tdisf_fpts,
+                                      void* stream)
+{
+  if (!opp_1) return op_fail(FR_ERR_ARG, "bad arguments");
+  long long cols = (long long)n_fields * n_eles;
+  for (int d = 0; d < n_dims; d++) {
+    fr_status st = dense_apply(n_fpts, n_upts, cols, opp_1[d], tdisf_upts + (size_t)n_upts * cols * d,
+                               norm_tdisf_fpts, d > 0, ST(stream));
+    if (st) return st;
+  }
+  return FR_OK;
+}
+
+fr_status fr_op_calculate_divergence(int n_upts, int n_dims, int n_fields, int n_eles, const double* const* opp_2,
+                                     const double* tdisf_upts, double* div_tconf_upts, void* stream)
+{
+  if (!opp_2) return op_fail(FR_ERR_ARG, "bad arguments");
+  long long cols = (long long)n_fields * n_eles;
+  for (int d = 0; d < n_dims; d++) {
+    fr_status st = dense_apply(n_upts, n_upts, cols, opp_2[d], tdisf_upts + (size_t)n_upts * cols * d,
+                               div_tconf_upts, d > 0, ST(stream));
+    if (st) return st;
+  }
+  return FR_OK;
+}
+
+fr_status fr_op_calculate_corrected_divergence(int n_upts, int n_fpts, int n_fields, int n_eles, const double* opp_3,
+                                               const double* norm_tdisf_fpts, double* norm_tconf_fpts,
+                                               double* div_tconf_upts, void* stream)
+{
+  long long n = (long long)n_fpts * n_fields * n_eles;
+  if (n > 0) {
+    axpy_kernel<<<grid_for(n, 256), 256, 0, ST(stream)>>>(n, -1.0, norm_tdisf_fpts, norm_tconf_fpts);
+    fr_status st = launched("axpy_kernel");
+    if (st) return st;
+  }
+  return dense_apply(n_upts, n_fpts, (long long)n_fields * n_eles, opp_3, norm_tconf_fpts, div_tconf_upts, 1,
+                     ST(stream));
+}
+
+fr_status fr_op_int_inters_common_invFlux(int n_fpts_per_inter, int n_dims, int n_fields, int n_inters,
+                                          double* const* disu_fpts_l, double* const* disu_fpts_r,
+                                          double* const* norm_tconf_fpts_l, double* const* norm_tconf_fpts_r,
+                                          double* const* tdA_fpts_l, double* const* tdA_fpts_r,
+                                          double* const* norm_fpts, double* const* delta_disu_fpts_l,
+                                          double* const* delta_disu_fpts_r, const fr_phys_desc* phys, int viscous,
+                                          void* stream)
+{
+  if (!phys || !dims_ok(n_dims, n_fields)) return op_fail(FR_ERR_ARG, "bad arguments");
+  if (viscous && (!delta_disu_fpts_l || !delta_disu_fpts_r)) return op_fail(FR_ERR_ARG, "viscous needs delta tables");
+  long long n = (long long)n_fpts_per_inter * n_inters;
+  if (n == 0) return FR_OK;
+  if (n_dims == 2)
+    common_inv_kernel<2><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_fpts_per_inter, n_inters, disu_fpts_l, disu_fpts_r, norm_tconf_fpts_l, norm_tconf_fpts_r, tdA_fpts_l, tdA_fpts_r, norm_fpts, delta_disu_fpts_l, delta_disu_fpts_r, phys_of(phys), viscous);
+  else
+    common_inv_kernel<3><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_fpts_per_inter, n_inters, disu_fpts_l, disu_fpts_r, norm_tconf_fpts_l, norm_tconf_fpts_r, tdA_fpts_l, tdA_fpts_r, norm_fpts, delta_disu_fpts_l, delta_disu_fpts_r, phys_of(phys), viscous);
+  return launched("common_inv_kernel");
+}
+
+fr_status fr_op_int_inters_common_viscFlux(int n_fpts_per_inter, int n_dims, int n_fields, int n_inters,
+                                           double* const* disu_fpts_l, double* const* disu_fpts_r,
+                                           double* const* grad_disu_fpts_l, double* const* grad_disu_fpts_r,
+                                           double* const* norm_tconf_fpts_l, double* const* norm_tconf_fpts_r,
+                                           double* const* tdA_fpts_l, double* const* tdA_fpts_r,
+                                           double* const* norm_fpts, const fr_phys_desc* phys, void* stream)
+{
+  if (!phys || !dims_ok(n_dims, n_fields)) return op_fail(FR_ERR_ARG, "bad arguments");
+  long long n = (long long)n_fpts_per_inter * n_inters;
+  if (n == 0) return FR_OK;
+  if (n_dims == 2)
+    common_vis_kernel<2><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_fpts_per_inter, n_inters, disu_fpts_l, disu_fpts_r, grad_disu_fpts_l, grad_disu_fpts_r, norm_tconf_fpts_l, norm_tconf_fpts_r, tdA_fpts_l, tdA_fpts_r, norm_fpts, phys_of(phys));
+  else
+    common_vis_kernel<3><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_fpts_per_inter, n_inters, disu_fpts_l, disu_fpts_r, grad_disu_fpts_l, grad_disu_fpts_r, norm_tconf_fpts_l, norm_tconf_fpts_r, tdA_fpts_l, tdA_fpts_r, norm_fpts, phys_of(phys));
+  return launched("common_vis_kernel");
+}
+
+fr_status fr_op_advance_rk45(int n_upts, int n_fields, int n_eles, int stage, double dt, double const_src,
+                             double* disu_upts_0, double* disu_upts_1, const double* div_tconf_upts,
+                             const double* detjac_upts, const double* src_upts, void* stream)
+{
+  static const double A[5] = {0.0, -0.417890474499852, -1.192151694642677, -1.697784692471528, -1.514183444257156};
+  static const double B[5] = {0.149659021999229, 0.379210312999627, 0.822955029386982, 0.699450455949122,
+                              0.153057247968152};
+  if (stage < 0 || stage > 4 || !disu_upts_0 || !disu_upts_1 || !div_tconf_upts || !detjac_upts)
+    return op_fail(FR_ERR_ARG, "bad arguments");
+  long long n = (long long)n_upts * n_eles * n_fields;
+  if (n == 0) return FR_OK;
+  rk45_kernel<<<grid_for(n, 256), 256, 0, ST(stream)>>>(n_upts, n_eles, n_fields, disu_upts_0, disu_upts_1,
+                                                       div_tconf_upts, detjac_upts, src_upts, A[stage], B[stage], dt,
+                                                       const_src);
+  return launched("rk45_kernel");
+}
+
+}  // extern "C"

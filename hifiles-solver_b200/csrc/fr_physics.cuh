@@ -1,10 +1,15 @@
 // fr_physics.cuh -- pointwise Euler / Navier-Stokes physics of the FR path,
-// device side.  Templated on the compute type T (double for the FP64 form,
-// float for the FP32 form) and the number of dimensions D (F = D + 2 fields).
+// device side, templated on the compute type T (double: FP64 form, float:
+// FP32 form) and the number of dimensions D (F = D + 2 fields).
 //
-// Formulas follow the reference's CPU routines; the operation order is kept
-// where it is cheap to keep, so the FP64 form agrees with the reference to a
-// few ulp (contractions into FMA are allowed).
+// The expressions repeat the reference's CPU routines term for term (true
+// divisions, the same association order).  The translation units that include
+// this header are compiled with -fmad=false, so nothing is contracted into an
+// FMA behind the code's back: the FP64 form rounds exactly like the reference
+// wherever it evaluates the same expression.  This matters: at low Mach
+// number the flux terms are ~1e3-1e4 times larger than the residual they
+// cancel to, so ulp-level differences in the fluxes show up at 1e-12 in the
+// residual.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -27,9 +32,6 @@ struct PhysT {
   }
 };
 
-__device__ __forceinline__ double ffma(double a, double b, double c) { return fma(a, b, c); }
-__device__ __forceinline__ float ffma(float a, float b, float c) { return fmaf(a, b, c); }
-
 template <typename T> __device__ __forceinline__ T fr_sqrt(T x);
 template <> __device__ __forceinline__ double fr_sqrt<double>(double x) { return sqrt(x); }
 template <> __device__ __forceinline__ float fr_sqrt<float>(float x) { return sqrtf(x); }
@@ -46,38 +48,38 @@ template <int D, typename T>
 __device__ __forceinline__ void inv_flux(const PhysT<T>& ph, const T* u, T (*f)[D])
 {
   constexpr int F = D + 2;
-  T rinv = T(1) / u[0];
   T v[D];
 #pragma unroll
-  for (int l = 0; l < D; l++) v[l] = u[l + 1] * rinv;
-  T ke = T(0);
+  for (int l = 0; l < D; l++) v[l] = u[l + 1] / u[0];
+  T ke = v[0] * v[0];
 #pragma unroll
-  for (int l = 0; l < D; l++) ke += v[l] * v[l];
+  for (int l = 1; l < D; l++) ke = ke + v[l] * v[l];
   T p = ph.gm1 * (u[F - 1] - (T(0.5) * u[0] * ke));
 #pragma unroll
   for (int l = 0; l < D; l++) {
     f[0][l] = u[l + 1];
 #pragma unroll
-    for (int m = 0; m < D; m++) f[m + 1][l] = u[m + 1] * v[l] + (m == l ? p : T(0));
+    for (int m = 0; m < D; m++) f[m + 1][l] = (m == l) ? p + (u[m + 1] * v[l]) : u[m + 1] * v[l];
     f[F - 1][l] = v[l] * (u[F - 1] + p);
   }
 }
 
-// Viscous flux (no turbulence model): calc_visf_2d / calc_visf_3d,
-// src/flux.cpp:132-431.  With fix_vis == 1 the Sutherland value is replaced by
-// mu_inf, which is what mu + fix_vis*(mu_inf - mu) evaluates to.
+// Viscous flux, no turbulence model: calc_visf_2d / calc_visf_3d,
+// src/flux.cpp:132-431.  With fix_vis == 1 the viscosity is mu_inf (the value
+// mu + fix_vis*(mu_inf - mu) takes whenever the Sutherland value is within a
+// factor 2 of mu_inf); otherwise Sutherland's law.
 template <int D, typename T>
 __device__ __forceinline__ void vis_flux(const PhysT<T>& ph, const T* u, T (*g)[D], T (*f)[D])
 {
   constexpr int F = D + 2;
-  T rho = u[0], rinv = T(1) / rho;
+  const T rho = u[0];
   T v[D];
 #pragma unroll
-  for (int l = 0; l < D; l++) v[l] = u[l + 1] * rinv;
-  T ke = T(0);
+  for (int l = 0; l < D; l++) v[l] = u[l + 1] / rho;
+  T ke = v[0] * v[0];
 #pragma unroll
-  for (int l = 0; l < D; l++) ke += v[l] * v[l];
-  T inte = u[F - 1] * rinv - T(0.5) * ke;
+  for (int l = 1; l < D; l++) ke = ke + v[l] * v[l];
+  T inte = u[F - 1] / rho - T(0.5) * ke;
   T mu;
   if (ph.fix_vis == T(1)) {
     mu = ph.mu_inf;
@@ -86,47 +88,46 @@ __device__ __forceinline__ void vis_flux(const PhysT<T>& ph, const T* u, T (*g)[
     mu = ph.mu_inf * fr_pow15<T>(rt) * (T(1) + ph.c_sth) / (rt + ph.c_sth);
     mu = mu + ph.fix_vis * (ph.mu_inf - mu);
   }
-  // velocity gradients dv[m][l] = d v_m / d x_l
-  T dv[D][D];
+  T dv[D][D];   // dv[m][l] = d v_m / d x_l
 #pragma unroll
   for (int m = 0; m < D; m++)
 #pragma unroll
-    for (int l = 0; l < D; l++) dv[m][l] = (g[m + 1][l] - g[0][l] * v[m]) * rinv;
+    for (int l = 0; l < D; l++) dv[m][l] = (g[m + 1][l] - g[0][l] * v[m]) / rho;
   T de[D];
 #pragma unroll
   for (int l = 0; l < D; l++) {
-    T vdv = T(0);
+    T vdv = v[0] * dv[0][l];
 #pragma unroll
-    for (int m = 0; m < D; m++) vdv += v[m] * dv[m][l];
+    for (int m = 1; m < D; m++) vdv = vdv + v[m] * dv[m][l];
     T dke = T(0.5) * ke * g[0][l] + rho * vdv;
-    de[l] = (g[F - 1][l] - dke - g[0][l] * inte) * rinv;
+    de[l] = (g[F - 1][l] - dke - g[0][l] * inte) / rho;
   }
-  T div = T(0);
+  T dsum = dv[0][0];
 #pragma unroll
-  for (int l = 0; l < D; l++) div += dv[l][l];
-  T diag = div / T(3);
-  T kt = (mu / ph.prandtl) * ph.gamma;
+  for (int l = 1; l < D; l++) dsum = dsum + dv[l][l];
+  const T diag = dsum / T(3.0);
+  const T kt = mu / ph.prandtl;   // (mu/prandtl + mu_t/prandtl_t) with mu_t = 0
   T tau[D][D];
 #pragma unroll
   for (int m = 0; m < D; m++)
 #pragma unroll
     for (int l = 0; l < D; l++)
-      tau[m][l] = (m == l) ? T(2) * mu * (dv[m][m] - diag) : mu * (dv[m][l] + dv[l][m]);
+      tau[m][l] = (m == l) ? T(2.0) * mu * (dv[m][m] - diag) : mu * (dv[m][l] + dv[l][m]);
 #pragma unroll
   for (int l = 0; l < D; l++) {
     f[0][l] = T(0);
-    T w = T(0);
+    T w = v[0] * tau[0][l];
 #pragma unroll
     for (int m = 0; m < D; m++) {
       f[m + 1][l] = -tau[m][l];
-      w += v[m] * tau[m][l];
+      if (m > 0) w = w + v[m] * tau[m][l];
     }
-    f[F - 1][l] = -(w + kt * de[l]);
+    f[F - 1][l] = -(w + kt * ph.gamma * de[l]);
   }
 }
 
-// Rusanov common normal flux for a static mesh: inters::rusanov_flux,
-// src/inters.cpp:311-365.
+// Rusanov common normal flux, static mesh: inters::rusanov_flux,
+// src/inters.cpp:311-365 (the grid-velocity term v_g . n is zero).
 template <int D, typename T>
 __device__ __forceinline__ void rusanov(const PhysT<T>& ph, const T* ul, const T* ur, const T* n, T* fn)
 {
@@ -134,29 +135,31 @@ __device__ __forceinline__ void rusanov(const PhysT<T>& ph, const T* ul, const T
   T fl[F][D], fr[F][D];
   inv_flux<D, T>(ph, ul, fl);
   inv_flux<D, T>(ph, ur, fr);
-  T vnl = T(0), vnr = T(0), kl = T(0), kr = T(0);
-  T il = T(1) / ul[0], ir = T(1) / ur[0];
+  T vl[D], vr[D];
 #pragma unroll
-  for (int l = 0; l < D; l++) {
-    T a = ul[l + 1] * il, b = ur[l + 1] * ir;
-    vnl += a * n[l]; vnr += b * n[l]; kl += a * a; kr += b * b;
+  for (int l = 0; l < D; l++) { vl[l] = ul[l + 1] / ul[0]; vr[l] = ur[l + 1] / ur[0]; }
+  T vnl = vl[0] * n[0], vnr = vr[0] * n[0], kl = vl[0] * vl[0], kr = vr[0] * vr[0];
+#pragma unroll
+  for (int l = 1; l < D; l++) {
+    vnl = vnl + vl[l] * n[l]; vnr = vnr + vr[l] * n[l];
+    kl = kl + vl[l] * vl[l]; kr = kr + vr[l] * vr[l];
   }
-  T pl = ph.gm1 * (ul[F - 1] - T(0.5) * ul[0] * kl);
-  T pr = ph.gm1 * (ur[F - 1] - T(0.5) * ur[0] * kr);
+  T pl = ph.gm1 * (ul[F - 1] - (T(0.5) * ul[0] * kl));
+  T pr = ph.gm1 * (ur[F - 1] - (T(0.5) * ur[0] * kr));
   T vav = fr_sqrt<T>(T(0.25) * (vnl + vnr) * (vnl + vnr));
   T cav = fr_sqrt<T>((ph.gamma * (pl + pr)) / (ul[0] + ur[0]));
   T eig = fr_abs<T>(vav + cav);
 #pragma unroll
   for (int k = 0; k < F; k++) {
-    T a = T(0), b = T(0);
+    T a = fl[k][0] * n[0], b = fr[k][0] * n[0];
 #pragma unroll
-    for (int l = 0; l < D; l++) { a += fl[k][l] * n[l]; b += fr[k][l] * n[l]; }
+    for (int l = 1; l < D; l++) { a = a + fl[k][l] * n[l]; b = b + fr[k][l] * n[l]; }
     fn[k] = T(0.5) * ((a + b) - eig * (ur[k] - ul[k]));
   }
 }
 
-// LDG sign switch of the penalty: a fixed direction per interface point taken
-// from the left normal, src/inters.cpp:555-564, 651-660.
+// Sign of the LDG penalty: one fixed direction per interface point, taken
+// from the left normal (src/inters.cpp:555-564, 651-660).
 template <int D, typename T>
 __device__ __forceinline__ T ldg_beta(T pen, const T* n)
 {
@@ -164,9 +167,29 @@ __device__ __forceinline__ T ldg_beta(T pen, const T* n)
   return s < T(0) ? -pen : pen;
 }
 
-// LDG common normal viscous flux for an interior interface: inters::ldg_flux
-// (flux_spec 0), src/inters.cpp:550-641.  pen is the signed penalty of
-// ldg_beta, passed in so both sides of an interface use the same sign.
+// Projection of a viscous flux on the left normal: a_k = f_k . n.
+template <int D, typename T>
+__device__ __forceinline__ T project(T (*f)[D], int k, const T* n)
+{
+  T a = f[k][0] * n[0];
+#pragma unroll
+  for (int l = 1; l < D; l++) a = a + f[k][l] * n[l];
+  return a;
+}
+
+// LDG common normal viscous flux of an interior interface point from the two
+// sides' normal projections aL = fL.n, aR = fR.n (inters::ldg_flux with
+// flux_spec 0, src/inters.cpp:550-641):
+//   f_c.n = (fL+fR)/2 . n + pen (n.n) (fL-fR).n + tau (n.n) (uL-uR)
+// which is the reference's component form summed against n.
+template <typename T>
+__device__ __forceinline__ T ldg_normal(T aL, T aR, T uL, T uR, T pen, T tau, T nn)
+{
+  return T(0.5) * (aL + aR) + (pen * (aL - aR) + tau * (uL - uR)) * nn;
+}
+
+// LDG common normal viscous flux from full fluxes (component form), for the
+// per-operator path where both sides' gradients are at hand.
 template <int D, typename T>
 __device__ __forceinline__ void ldg_flux(const PhysT<T>& ph, T pen, const T* ul, const T* ur, T (*fl)[D],
                                          T (*fr)[D], const T* n, T* fn)
@@ -174,15 +197,15 @@ __device__ __forceinline__ void ldg_flux(const PhysT<T>& ph, T pen, const T* ul,
   constexpr int F = D + 2;
 #pragma unroll
   for (int k = 0; k < F; k++) {
-    T jump = T(0);
+    T jump = n[0] * (fl[k][0] - fr[k][0]);
 #pragma unroll
-    for (int l = 0; l < D; l++) jump += n[l] * (fl[k][l] - fr[k][l]);
+    for (int l = 1; l < D; l++) jump = jump + n[l] * (fl[k][l] - fr[k][l]);
     T du = ul[k] - ur[k];
     T acc = T(0);
 #pragma unroll
     for (int l = 0; l < D; l++) {
-      T fc = T(0.5) * (fl[k][l] + fr[k][l]) + pen * n[l] * jump + ph.tau * n[l] * du;
-      acc += fc * n[l];
+      T fc = T(0.5) * (fl[k][l] + fr[k][l]) + pen * n[l] * (jump) + ph.tau * n[l] * du;
+      acc = (l == 0) ? fc * n[0] : acc + fc * n[l];
     }
     fn[k] = acc;
   }

@@ -40,8 +40,8 @@ static const double kRK4B[5] = {0.149659021999229, 0.379210312999627, 0.82295502
 
 struct Bufs {
   double *U = nullptr, *REG = nullptr, *DIV = nullptr, *detj64 = nullptr, *partial = nullptr, *norms = nullptr;
-  void *UF[2] = {nullptr, nullptr}, *GF = nullptr, *RP = nullptr, *nL = nullptr, *tdA = nullptr, *JG = nullptr,
-       *detj = nullptr;
+  void *UF[2] = {nullptr, nullptr}, *VF = nullptr, *ND = nullptr, *DV = nullptr, *nL = nullptr, *tdA = nullptr,
+       *JG = nullptr, *detj = nullptr;
   int* mate = nullptr;
   unsigned char* side = nullptr;
 };
@@ -104,16 +104,16 @@ struct RunnerT : Runner {
   void grad(const Bufs& b, int cur, cudaStream_t s) override
   {
     fr_grad_kernel<DIM, P, EPB, NT, TC><<<flux_blocks(), NT, 0, s>>>(
-        b.U, (const TC*)b.UF[cur], b.mate, b.side, (const TC*)b.JG, (const TC*)b.detj, (TC*)b.GF, (TC*)b.RP, E,
-        L, ph);
+        b.U, (const TC*)b.UF[cur], b.mate, b.side, (const TC*)b.JG, (const TC*)b.detj, (const TC*)b.nL, (TC*)b.VF,
+        (TC*)b.ND, (TC*)b.DV, E, L, ph);
   }
   template <int VISC, int MODE>
   void flux_t(const Bufs& b, int cur, int stage, double dt, bool want_partial, cudaStream_t s)
   {
     fr_flux_kernel<DIM, P, EPB, NT, VISC, MODE, TC><<<flux_blocks(), NT, 0, s>>>(
-        b.U, b.REG, (const TC*)b.UF[cur], (TC*)b.UF[cur ^ 1], (const TC*)b.GF, (const TC*)b.RP, b.mate, b.side,
-        (const TC*)b.nL, (const TC*)b.tdA, (const TC*)b.JG, b.detj64, b.DIV, want_partial ? b.partial : nullptr,
-        E, L, ph, kRK4A[stage], kRK4B[stage], dt, stage == 0 ? 1 : 0);
+        b.U, b.REG, (const TC*)b.UF[cur], (TC*)b.UF[cur ^ 1], (const TC*)b.VF, (const TC*)b.ND, (const TC*)b.DV,
+        b.mate, b.side, (const TC*)b.nL, (const TC*)b.tdA, (const TC*)b.JG, b.detj64, b.DIV,
+        want_partial ? b.partial : nullptr, E, L, ph, kRK4A[stage], kRK4B[stage], dt, stage == 0 ? 1 : 0);
   }
   void flux(const Bufs& b, int cur, int mode, int stage, double dt, bool want_partial, cudaStream_t s) override
   {
@@ -301,8 +301,9 @@ fr_status fr_solver_create(const fr_mesh_desc* md, const fr_scheme_desc* sd, int
   char* p;
   for (int i = 0; i < 2; i++) { if ((st = dalloc(s.get(), &p, nf * E * F * tc))) return st; s->b.UF[i] = p; }
   if (sd->viscous) {
-    if ((st = dalloc(s.get(), &p, nf * E * F * D * tc))) return st; s->b.GF = p;
-    if ((st = dalloc(s.get(), &p, nu * E * F * tc))) return st; s->b.RP = p;
+    if ((st = dalloc(s.get(), &p, nf * E * (F - 1) * tc))) return st; s->b.VF = p;
+    if ((st = dalloc(s.get(), &p, nf * E * F * tc))) return st; s->b.ND = p;
+    if ((st = dalloc(s.get(), &p, nu * E * F * tc))) return st; s->b.DV = p;
   }
   if ((st = dalloc(s.get(), &p, nf * E * D * tc))) return st; s->b.nL = p;
   if ((st = dalloc(s.get(), &p, nf * E * tc))) return st; s->b.tdA = p;

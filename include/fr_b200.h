@@ -147,6 +147,100 @@ fr_status fr_mesh_geometry(const fr_mesh_desc* mesh, const fr_scheme_desc* schem
  * opp_0..opp_6 for quads / hexes (src/eles.cpp:3620-4052) is one of these. */
 fr_status fr_line_operators(int order, int upts_type, int vcjh_scheme, double eta, double* out);
 
+/* ------------------------------------------------------------------------
+ * Per-operator entry points: the reference's GPU seam one method at a time,
+ * on caller-owned device arrays in the reference's layouts.  Operators are
+ * the caller's dense matrices (any element type, column-major, as built by
+ * set_opp_0..6, src/eles.cpp:3620-4052); interface data come through device
+ * tables of device pointers laid out like int_inters' arrays
+ * (src/int_inters.cpp:95-178).  Each call enqueues on `stream` and returns;
+ * nothing synchronises the device.
+ * ---------------------------------------------------------------------- */
+
+typedef struct {
+  double gamma, prandtl, mu_inf, rt_inf, c_sth, fix_vis, tau, pen_fact;
+} fr_phys_desc;
+
+/* eles::extrapolate_solution, include/eles.h:109 (GPU body src/eles.cpp:1310-1314,
+ * cublasDgemm on opp_0): disu_fpts = opp_0 * disu_upts. */
+fr_status fr_op_extrapolate_solution(int n_fpts, int n_upts, int n_fields, int n_eles, const double* opp_0,
+                                     const double* disu_upts, double* disu_fpts, void* stream);
+
+/* eles::evaluate_invFlux, include/eles.h:115; replaces
+ * evaluate_invFlux_gpu_kernel_wrapper, include/cuda_kernels.h:35 (static mesh). */
+fr_status fr_op_evaluate_invFlux(int n_upts, int n_dims, int n_fields, int n_eles, const double* disu_upts,
+                                 const double* JGinv_upts, double* tdisf_upts, const fr_phys_desc* phys,
+                                 void* stream);
+
+/* eles::calculate_gradient, include/eles.h:130 (cublasDgemm on opp_4[d]);
+ * opp_4 is a host array of n_dims device pointers. */
+fr_status fr_op_calculate_gradient(int n_upts, int n_dims, int n_fields, int n_eles, const double* const* opp_4,
+                                   const double* disu_upts, double* grad_disu_upts, void* stream);
+
+/* eles::correct_gradient, include/eles.h:133: grad += opp_5[d] * delta_disu_fpts,
+ * then the transform of transform_grad_disu_upts_kernel_wrapper,
+ * include/cuda_kernels.h:45. */
+fr_status fr_op_correct_gradient(int n_upts, int n_fpts, int n_dims, int n_fields, int n_eles,
+                                 const double* const* opp_5, const double* delta_disu_fpts, const double* JGinv_upts,
+                                 const double* detjac_upts, double* grad_disu_upts, void* stream);
+
+/* eles::extrapolate_corrected_gradient, include/eles.h:136 (cublasDgemm on opp_6 per dimension). */
+fr_status fr_op_extrapolate_corrected_gradient(int n_fpts, int n_upts, int n_dims, int n_fields, int n_eles,
+                                               const double* opp_6, const double* grad_disu_upts,
+                                               double* grad_disu_fpts, void* stream);
+
+/* eles::evaluate_viscFlux, include/eles.h:142; replaces
+ * evaluate_viscFlux_gpu_kernel_wrapper, include/cuda_kernels.h:48 (no LES,
+ * no wall model, no turbulence model): tdisf_upts += JGinv * F_visc. */
+fr_status fr_op_evaluate_viscFlux(int n_upts, int n_dims, int n_fields, int n_eles, const double* disu_upts,
+                                  const double* grad_disu_upts, const double* JGinv_upts, double* tdisf_upts,
+                                  const fr_phys_desc* phys, void* stream);
+
+/* eles::extrapolate_totalFlux, include/eles.h:121: norm_tdisf_fpts = sum_d opp_1[d] * tdisf_upts[d]. */
+fr_status fr_op_extrapolate_totalFlux(int n_fpts, int n_upts, int n_dims, int n_fields, int n_eles,
+                                      const double* const* opp_1, const double* tdisf_upts, double* norm_tdisf_fpts,
+                                      void* stream);
+
+/* eles::calculate_divergence, include/eles.h:118: div = sum_d opp_2[d] * tdisf_upts[d]. */
+fr_status fr_op_calculate_divergence(int n_upts, int n_dims, int n_fields, int n_eles, const double* const* opp_2,
+                                     const double* tdisf_upts, double* div_tconf_upts, void* stream);
+
+/* eles::calculate_corrected_divergence, include/eles.h:127 (cublasDaxpy +
+ * cublasDgemm on opp_3): norm_tconf -= norm_tdisf; div += opp_3 * norm_tconf. */
+fr_status fr_op_calculate_corrected_divergence(int n_upts, int n_fpts, int n_fields, int n_eles, const double* opp_3,
+                                               const double* norm_tdisf_fpts, double* norm_tconf_fpts,
+                                               double* div_tconf_upts, void* stream);
+
+/* int_inters::calculate_common_invFlux, include/int_inters.h:61; replaces
+ * calculate_common_invFlux_gpu_kernel_wrapper, include/cuda_kernels.h:39
+ * (Rusanov, static mesh; with viscous != 0 also the LDG common solution into
+ * delta_disu_fpts_l/_r). */
+fr_status fr_op_int_inters_common_invFlux(int n_fpts_per_inter, int n_dims, int n_fields, int n_inters,
+                                          double* const* disu_fpts_l, double* const* disu_fpts_r,
+                                          double* const* norm_tconf_fpts_l, double* const* norm_tconf_fpts_r,
+                                          double* const* tdA_fpts_l, double* const* tdA_fpts_r,
+                                          double* const* norm_fpts, double* const* delta_disu_fpts_l,
+                                          double* const* delta_disu_fpts_r, const fr_phys_desc* phys, int viscous,
+                                          void* stream);
+
+/* int_inters::calculate_common_viscFlux, include/int_inters.h:64; replaces
+ * calculate_common_viscFlux_gpu_kernel_wrapper, include/cuda_kernels.h:56
+ * (LDG, no LES): norm_tconf_fpts_l/_r += +/- f_n * tdA. */
+fr_status fr_op_int_inters_common_viscFlux(int n_fpts_per_inter, int n_dims, int n_fields, int n_inters,
+                                           double* const* disu_fpts_l, double* const* disu_fpts_r,
+                                           double* const* grad_disu_fpts_l, double* const* grad_disu_fpts_r,
+                                           double* const* norm_tconf_fpts_l, double* const* norm_tconf_fpts_r,
+                                           double* const* tdA_fpts_l, double* const* tdA_fpts_r,
+                                           double* const* norm_fpts, const fr_phys_desc* phys, void* stream);
+
+/* eles::AdvanceSolution(stage, adv_type 3), include/eles.h:157; replaces
+ * RK45_update_kernel_wrapper, include/cuda_kernels.h:30 (fixed dt):
+ * res = a_s res + dt (-div/detjac + const_src + src); u += b_s res.
+ * src_upts may be NULL (zero source). */
+fr_status fr_op_advance_rk45(int n_upts, int n_fields, int n_eles, int stage, double dt, double const_src,
+                             double* disu_upts_0, double* disu_upts_1, const double* div_tconf_upts,
+                             const double* detjac_upts, const double* src_upts, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -26,6 +26,7 @@
 #include <vector>
 #include <iostream>
 #include <fstream>
+#include <time.h>
 
 #define protected public
 #include "global.h"
@@ -270,17 +271,18 @@ static void staged_residual(solution& S)
 int main(int argc, char** argv)
 {
   if (argc < 3) {
-    fprintf(stderr, "usage: ref_harness <input_file> <out_dir> [--ic NAME] [--steps N] [--stages]\n");
+    fprintf(stderr, "usage: ref_harness <input_file> <out_dir> [--ic NAME] [--steps N] [--stages] [--no-dump]\n");
     return 2;
   }
   g_out = argv[2];
   string ic;
   int steps = 0;
-  bool stages = false;
+  bool stages = false, nodump = false;
   for (int a = 3; a < argc; a++) {
     if (!strcmp(argv[a], "--ic") && a + 1 < argc) ic = argv[++a];
     else if (!strcmp(argv[a], "--steps") && a + 1 < argc) steps = atoi(argv[++a]);
     else if (!strcmp(argv[a], "--stages")) stages = true;
+    else if (!strcmp(argv[a], "--no-dump")) nodump = true;
     else { fprintf(stderr, "bad argument %s\n", argv[a]); return 2; }
   }
 
@@ -298,7 +300,7 @@ int main(int argc, char** argv)
   S.integral_quantities.setup(run_input.n_integral_quantities > 0 ? run_input.n_integral_quantities : 1);
   for (int i = 0; i < 5; i++) S.norm_residual(i) = 0.0;
 
-  dump_setup(S);
+  if (!nodump) dump_setup(S);
 
   int first_stage = 0;
   if (stages) {
@@ -312,6 +314,8 @@ int main(int argc, char** argv)
   int nf = (S.n_dims == 2) ? 4 : 5;
   vector<double> hist;
   int RK = (S.adv_type == 3) ? 5 : 1;
+  struct timespec t0, t1;
+  clock_gettime(CLOCK_MONOTONIC, &t0);
   for (int s = 0; s < steps; s++) {
     for (int i = (s == 0 ? first_stage : 0); i < RK; i++) {
       CalcResidual(0, i, &S);
@@ -321,7 +325,9 @@ int main(int argc, char** argv)
     CalcNormResidual(&S);
     for (int k = 0; k < nf; k++) hist.push_back(S.norm_residual(k));
   }
-  if (steps > 0) {
+  clock_gettime(CLOCK_MONOTONIC, &t1);
+  printf("step_loop_seconds %.9f\n", (t1.tv_sec - t0.tv_sec) + 1e-9 * (t1.tv_nsec - t0.tv_nsec));
+  if (steps > 0 && !nodump) {
     vector<int> shape; shape.push_back(nf); shape.push_back(steps);
     write_npy("res_norms", hist.data(), "<f8", 8, shape);
     dump_stage(S, "final", "disu_upts0");

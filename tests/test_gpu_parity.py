@@ -103,16 +103,34 @@ def test_residual_matches_oracle_on_perturbed_states(dims, P, n, visc, scheme, j
 
 
 def test_fp32_form_error_is_small_and_stated():
+    """FP32 traces/fluxes/operators, FP64 state, RK register and reductions:
+    the L2 error of the solution against the FP64 path stays below 1e-6
+    relative (the residual itself is only good to ~1e-4 at Mach 0.1, where
+    the flux terms are ~1e3 times larger than the residual)."""
     meta, a = load("hex_tgv_p3_n3")
     s64, s32 = _solver(meta, 0), _solver(meta, 1)
     s64.set_state(a["u0"])
     s32.set_state(a["u0"])
     e_res = rel(s32.residual(), s64.residual())
-    s64.advance(5, 1e-3)
-    s32.advance(5, 1e-3)
+    s64.advance(20, 1e-3)
+    s32.advance(20, 1e-3)
     e_state = rel(s32.get_state(), s64.get_state())
-    assert e_res < 1e-5
+    print("fp32 form: residual rel %.3e, state rel after 20 steps %.3e" % (e_res, e_state))
+    assert e_res < 1e-3
     assert e_state < 1e-6
+
+
+@pytest.mark.parametrize("n", [8, 16])
+def test_tgv_residual_at_scale_matches_oracle(n):
+    """TGV at Mach 0.1, P=3: the flux terms are 1e3-1e4 times larger than the
+    residual, so parity at 1e-12 needs the reference's rounding, not just FP64."""
+    kw = dict(viscous=True, gamma=1.4, prandtl=0.71, mu_inf=1.0 / 1600.0, tau=1.0, pen_fact=0.5)
+    s = H.Solver.box(3, 3, (n, n, n), (0, 0, 0), (2 * np.pi,) * 3, vcjh_scheme=1, **kw)
+    m = O.Mesh.box(3, 3, (n, n, n), (0, 0, 0), (2 * np.pi,) * 3, vcjh_scheme=1)
+    u = O.ic_tgv(m.geometry()["pos_upts"])
+    s.set_state(u)
+    ph = O.physics(viscous=1, gamma=1.4, prandtl=0.71, mu_inf=1.0 / 1600.0, tau=1.0, pen_fact=0.5)
+    assert rel(s.residual(), m.residual(ph, u)) <= TOL_RES
 
 
 def test_errors_are_reported():
