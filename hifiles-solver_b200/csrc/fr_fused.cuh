@@ -156,6 +156,21 @@ __device__ __forceinline__ T deriv_line(const Line<T>& L, const S* s, int sst, i
   return acc;
 }
 
+// Dynamic shared-memory sizes of the stage kernels.
+template <int DIM, int P, int EPB, typename TC>
+constexpr size_t grad_smem_bytes()
+{
+  using S = Shape<DIM, P>;
+  return sizeof(TC) * EPB * S::F * (S::NU + 2 * S::NF + 2 * DIM * S::NU);
+}
+template <int DIM, int P, int EPB, int NT, int VISC, typename TC>
+constexpr size_t flux_smem_bytes()
+{
+  using S = Shape<DIM, P>;
+  return sizeof(double) * (EPB * S::F * S::NU + (NT / 32) * S::F) + sizeof(TC) * EPB * S::F * S::NF +
+         (VISC ? 0 : sizeof(TC) * EPB * DIM * S::F * S::NU);
+}
+
 template <int NT, int ITEMS>
 struct Items {
   static constexpr int N = (ITEMS + NT - 1) / NT;
@@ -202,10 +217,14 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
   using S = Shape<DIM, P>;
   constexpr int NU = S::NU, NF = S::NF, F = S::F, D = DIM;
   constexpr int IF = Items<NT, EPB * NF>::N, IU = Items<NT, EPB * NU>::N;
-  __shared__ TC sU[EPB][F][NU];
-  __shared__ TC sX[EPB][F][NF];          // delta_disu_fpts
-  __shared__ TC sG[EPB][F * D][NU];      // physical gradient, component k + F*d
-  __shared__ TC sFl[EPB][D][F][NU];      // transformed total flux
+  extern __shared__ __align__(16) unsigned char fr_smem[];
+  // sU: solution, sX: delta_disu_fpts, sUf: own solution at the flux points,
+  // sG: physical gradient (component k + F*d), sFl: transformed total flux
+  auto sU = reinterpret_cast<TC (*)[F][NU]>(fr_smem);
+  auto sX = reinterpret_cast<TC (*)[F][NF]>(fr_smem + sizeof(TC) * EPB * F * NU);
+  auto sUf = reinterpret_cast<TC (*)[F][NF]>(fr_smem + sizeof(TC) * EPB * F * (NU + NF));
+  auto sG = reinterpret_cast<TC (*)[F * D][NU]>(fr_smem + sizeof(TC) * EPB * F * (NU + 2 * NF));
+  auto sFl = reinterpret_cast<TC (*)[D][F][NU]>(fr_smem + sizeof(TC) * EPB * F * (NU + 2 * NF + D * NU));
   const long long e0 = (long long)blockIdx.x * EPB;
   const long long NFE = (long long)NF * E;
 
@@ -258,6 +277,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
       TC ul = (psd[it] & 1) ? uo : un, ur = (psd[it] & 1) ? un : uo;
       TC uc = TC(0.5) * (ul + ur) - pen * (ul - ur);
       sX[el][k][f] = uc - uo;
+      sUf[el][k][f] = uo;
     }
   }
   __syncthreads();
@@ -278,12 +298,19 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
       else { fm = d == 0 ? 4 : (d == 1 ? 1 : 0); fp = d == 0 ? 2 : (d == 1 ? 3 : 5); }
       int qm = face_fpt<DIM, P>(fm, abc[0], abc[1], abc[2], am);
       int qp = face_fpt<DIM, P>(fp, abc[0], abc[1], abc[2], ap);
+      const int st = upt_stride<DIM, P>(d), ub = u - i * st;
+      TC Dr[P + 1];
+#pragma unroll
+      for (int m = 0; m <= P; m++) Dr[m] = L.D[i][m];
+      const TC gm = L.gL[am], gpl = L.gR[ap];
 #pragma unroll
       for (int k = 0; k < F; k++) {
-        TC acc = deriv_line<DIM, P, TC, TC>(L, &sU[el][k][0], 1, u, d, i);
-        // opp_5 columns in flux-point order: the lower-numbered face first
-        TC cm = sX[el][k][qm] * L.gL[am], cp = sX[el][k][qp] * L.gR[ap];
-        acc = (fm < fp) ? (acc + cm) + cp : (acc + cp) + cm;
+        // the gradient only feeds the viscous flux: contracted with FMAs
+        TC acc = sU[el][k][ub] * Dr[0];
+#pragma unroll
+        for (int m = 1; m <= P; m++) acc = fr_fma(sU[el][k][ub + m * st], Dr[m], acc);
+        acc = fr_fma(sX[el][k][qm], gm, acc);
+        acc = fr_fma(sX[el][k][qp], gpl, acc);
         gr[k][d] = acc;
       }
     }
@@ -295,8 +322,8 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
       TC m0 = pG[it][0 + D * c] * inv, m1 = pG[it][1 + D * c] * inv, m2 = D == 3 ? pG[it][2 + D * c] * inv : TC(0);
 #pragma unroll
       for (int k = 0; k < F; k++) {
-        TC acc = gr[k][0] * m0 + gr[k][1] * m1;
-        if (D == 3) acc = acc + gr[k][2] * m2;
+        TC acc = fr_fma(gr[k][1], m1, gr[k][0] * m0);
+        if (D == 3) acc = fr_fma(gr[k][2], m2, acc);
         gp[k][c] = acc;
         sG[el][k + F * c][u] = acc;
       }
@@ -306,16 +333,17 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
     for (int k = 0; k < F; k++) q[k] = sU[el][k][u];
     TC fi[F][D], fv[F][D];
     inv_flux<D, TC>(ph, q, fi);
-    vis_flux<D, TC>(ph, q, gp, fv);
+    vis_flux_fast<D, TC>(ph, q, gp, fv);
 #pragma unroll
     for (int k = 0; k < F; k++)
 #pragma unroll
       for (int l = 0; l < D; l++) {
+        // inviscid part in the reference's rounding, viscous part added term by term
         TC acc = pG[it][l] * fi[k][0];
 #pragma unroll
         for (int m = 1; m < D; m++) acc = acc + pG[it][l + D * m] * fi[k][m];
 #pragma unroll
-        for (int m = 0; m < D; m++) acc = acc + pG[it][l + D * m] * fv[k][m];
+        for (int m = 0; m < D; m++) acc = fr_fma(pG[it][l + D * m], fv[k][m], acc);
         sFl[el][l][k][u] = acc;
       }
   }
@@ -330,17 +358,26 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
     if (w >= EPB * NF || e >= E) continue;
     size_t own = f + (size_t)NF * e;
     TC uf[F], gf[F][D], fv[F][D];
-#pragma unroll
-    for (int k = 0; k < F; k++) {
-      uf[k] = line_interp<DIM, P, TC, TC>(L, &sU[el][k][0], 1, f);
-#pragma unroll
-      for (int d = 0; d < D; d++) gf[k][d] = line_interp<DIM, P, TC, TC>(L, &sG[el][k + F * d][0], 1, f);
-    }
-    vis_flux<D, TC>(ph, uf, gf, fv);
-#pragma unroll
-    for (int k = 1; k < F; k++) VF[own + NFE * (k - 1)] = project<D, TC>(fv, k, pn[it]);
     int u0, st, ax; bool plus;
     fpt_line<DIM, P>(f, u0, st, ax, plus);
+    TC Lc[P + 1];
+#pragma unroll
+    for (int m = 0; m <= P; m++) Lc[m] = plus ? L.Lp[m] : L.Lm[m];
+#pragma unroll
+    for (int k = 0; k < F; k++) {
+      uf[k] = sUf[el][k][f];
+#pragma unroll
+      for (int d = 0; d < D; d++) {
+        const TC* s = &sG[el][k + F * d][0];
+        TC acc = s[u0] * Lc[0];
+#pragma unroll
+        for (int m = 1; m <= P; m++) acc = fr_fma(s[u0 + m * st], Lc[m], acc);
+        gf[k][d] = acc;
+      }
+    }
+    vis_flux_fast<D, TC>(ph, uf, gf, fv);
+#pragma unroll
+    for (int k = 1; k < F; k++) VF[own + NFE * (k - 1)] = project<D, TC>(fv, k, pn[it]);
 #pragma unroll
     for (int k = 0; k < F; k++) {
       TC v = line_interp<DIM, P, TC, TC>(L, &sFl[el][ax][k][0], 1, f);
@@ -388,10 +425,16 @@ fr_flux_kernel(double* __restrict__ U, double* __restrict__ REG, const TC* __res
   using S = Shape<DIM, P>;
   constexpr int NU = S::NU, NF = S::NF, F = S::F, D = DIM;
   constexpr int IF = Items<NT, EPB * NF>::N, IU = Items<NT, EPB * NU>::N;
-  __shared__ double sU[EPB][F][NU];
-  __shared__ TC sC[EPB][F][NF];                       // norm_tconf - norm_tdisf
-  __shared__ TC sFl[VISC ? 1 : EPB][D][VISC ? 1 : F][VISC ? 1 : NU];
-  __shared__ double sRed[NT / 32][F];
+  extern __shared__ __align__(16) unsigned char fr_smem[];
+  // sU: solution (FP64), sC: norm_tconf - norm_tdisf, sFl: transformed
+  // inviscid flux (inviscid path only), sRed: norm partial sums
+  constexpr int NFL = VISC ? 1 : EPB * D * F * NU;
+  auto sU = reinterpret_cast<double (*)[F][NU]>(fr_smem);
+  auto sRed = reinterpret_cast<double (*)[F]>(fr_smem + sizeof(double) * EPB * F * NU);
+  auto sC = reinterpret_cast<TC (*)[F][NF]>(fr_smem + sizeof(double) * (EPB * F * NU + (NT / 32) * F));
+  auto sFl = reinterpret_cast<TC (*)[D][F][NU]>(fr_smem + sizeof(double) * (EPB * F * NU + (NT / 32) * F) +
+                                                 sizeof(TC) * EPB * F * NF);
+  (void)NFL;
   const long long e0 = (long long)blockIdx.x * EPB;
   const long long NFE = (long long)NF * E;
 

@@ -101,16 +101,26 @@ struct RunnerT : Runner {
     long long n = E * S::NF;
     fr_trace_kernel<DIM, P, TC><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b.U, (TC*)b.UF[cur], E, L);
   }
+  static void set_smem(const void* k, size_t bytes)
+  {
+    if (bytes > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  }
   void grad(const Bufs& b, int cur, cudaStream_t s) override
   {
-    fr_grad_kernel<DIM, P, EPB, NT, TC><<<flux_blocks(), NT, 0, s>>>(
+    constexpr size_t sm = grad_smem_bytes<DIM, P, EPB, TC>();
+    static bool once = (set_smem((const void*)fr_grad_kernel<DIM, P, EPB, NT, TC>, sm), true);
+    (void)once;
+    fr_grad_kernel<DIM, P, EPB, NT, TC><<<flux_blocks(), NT, sm, s>>>(
         b.U, (const TC*)b.UF[cur], b.mate, b.side, (const TC*)b.JG, (const TC*)b.detj, (const TC*)b.nL, (TC*)b.VF,
         (TC*)b.ND, (TC*)b.DV, E, L, ph);
   }
   template <int VISC, int MODE>
   void flux_t(const Bufs& b, int cur, int stage, double dt, bool want_partial, cudaStream_t s)
   {
-    fr_flux_kernel<DIM, P, EPB, NT, VISC, MODE, TC><<<flux_blocks(), NT, 0, s>>>(
+    constexpr size_t sm = flux_smem_bytes<DIM, P, EPB, NT, VISC, TC>();
+    static bool once = (set_smem((const void*)fr_flux_kernel<DIM, P, EPB, NT, VISC, MODE, TC>, sm), true);
+    (void)once;
+    fr_flux_kernel<DIM, P, EPB, NT, VISC, MODE, TC><<<flux_blocks(), NT, sm, s>>>(
         b.U, b.REG, (const TC*)b.UF[cur], (TC*)b.UF[cur ^ 1], (const TC*)b.VF, (const TC*)b.ND, (const TC*)b.DV,
         b.mate, b.side, (const TC*)b.nL, (const TC*)b.tdA, (const TC*)b.JG, b.detj64, b.DIV,
         want_partial ? b.partial : nullptr, E, L, ph, kRK4A[stage], kRK4B[stage], dt, stage == 0 ? 1 : 0);
