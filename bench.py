@@ -178,8 +178,8 @@ def run_b200(a, rank, world, local):
     value = dof_step * world / (ms * 1e-3)
 
     # --- per-kernel event timing for the roofline (stage by stage, not replayed)
-    ms_grad, ms_flux = s.profile_stage(10, dt)
-    stage_ms = ms_grad + ms_flux
+    ms_grad, ms_face, ms_upd = s.profile_stage(10, dt)
+    stage_ms = ms_grad + ms_face + ms_upd
     pk, pk_src = peaks()
     tc = 4 if a.precision == "fp32" else 8
     b_elem = alg_bytes_per_element(3, P, True, s=8, m=tc, t=tc)
@@ -233,11 +233,11 @@ def run_b200(a, rank, world, local):
                                                     ((E * nu * F * 8 * 2 + E * 96 * F * tc * 2 + E * 96 * 15 * tc +
                                                       E * nu * 10 * tc) / 1e9),
                    "parallelism": "replicas" if world > 1 else "single GPU"},
-        "roofline": {"bound": "hbm", "kernel": "one RK stage = fr_grad_kernel + fr_flux_kernel",
+        "roofline": {"bound": "hbm", "kernel": "one RK stage = fr_grad_kernel + fr_face_kernel + fr_update_kernel",
                      "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / pk["hbm_gbs"], "peak_source": pk_src,
                      "alg_bytes_per_element": b_elem, "traffic": traffic,
-                     "ms_grad": ms_grad, "ms_flux": ms_flux},
+                     "ms_grad": ms_grad, "ms_face": ms_face, "ms_update": ms_upd, "ms_stage": stage_ms},
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
     }
     print(json.dumps(out))

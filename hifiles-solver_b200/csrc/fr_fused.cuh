@@ -3,9 +3,9 @@
 //
 // One RK stage of the reference (CalcResidual, src/solver.cpp:65-225, then
 // eles::AdvanceSolution, src/eles.cpp:1091-1188) runs as
-//   viscous :  fr_grad_kernel  -> fr_flux_kernel
-//   inviscid:                     fr_flux_kernel
-// Both are element-blocked: a CTA owns EPB elements, stages their solution in
+//   viscous :  fr_grad_kernel -> fr_face_kernel -> fr_update_kernel
+//   inviscid:                    fr_face_kernel -> fr_update_kernel
+// The element kernels are element-blocked: a CTA owns EPB elements, stages their solution in
 // shared memory, and applies the reference's operators as 1-D line
 // contractions (every dense operator opp_0..opp_6 of a Gauss-point tensor
 // element has exactly one non-trivial factor per line, so the contraction
@@ -17,6 +17,7 @@
 //                                on the interface's left normal (viscous path)
 //   ND  (n_fpts, n_eles, F)      normal discontinuous flux (norm_tdisf_fpts)
 //   DV  (n_upts, n_eles, F)      divergence of the discontinuous flux
+//   CF  (n_fpts, n_eles, F)      common normal flux times tdA (norm_tconf_fpts)
 // mate[i] is the flat index (fpt + n_fpts*ele) of the matching point across
 // the interface; side[i] bit 0 = this side is the left one, bit 1 = the LDG
 // penalty sign is negative.  Both sides evaluate the common flux with the
@@ -164,7 +165,7 @@ constexpr size_t grad_smem_bytes()
   return sizeof(TC) * EPB * S::F * (S::NU + 2 * S::NF + 2 * DIM * S::NU);
 }
 template <int DIM, int P, int EPB, int NT, int VISC, typename TC>
-constexpr size_t flux_smem_bytes()
+constexpr size_t update_smem_bytes()
 {
   using S = Shape<DIM, P>;
   return sizeof(double) * (EPB * S::F * S::NU + (NT / 32) * S::F) + sizeof(TC) * EPB * S::F * S::NF +
@@ -407,96 +408,105 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
 }
 
 // ---------------------------------------------------------------------------
-// Stage, part 2 (per element): common interface fluxes (Rusanov + LDG from the
-// normal projections), norm_tconf - norm_tdisf, the VCJH correction
-// (calculate_corrected_divergence), and either the residual (MODE 0) or the
-// RK45 stage update with the next stage's traces (MODE 1).  The inviscid path
-// (VISC 0) evaluates the flux, its divergence and its normal component here
-// itself, in the reference's order.
+// Common interface fluxes, once per interface flux point (one thread each):
+// int_inters::calculate_common_invFlux (Rusanov, src/int_inters.cpp:225-354)
+// and, viscous, calculate_common_viscFlux (LDG from the two sides' normal
+// projections VF, src/int_inters.cpp:359-470).  Writes norm_tconf_fpts of
+// both sides: +f_n tdA_l on the left, -f_n tdA_r on the right.
+// face[i] = (left flat index, right flat index) of interface point i;
+// fsign[i] != 0 when the LDG penalty sign is negative there.
+template <int DIM, int VISC, typename TC>
+__global__ void __launch_bounds__(128)
+fr_face_kernel(const int2* __restrict__ face, const unsigned char* __restrict__ fsign, long long nint,
+               const TC* __restrict__ UF, const TC* __restrict__ VF, const TC* __restrict__ nL,
+               const TC* __restrict__ tdA, TC* __restrict__ CF, long long NFE, PhysT<TC> ph)
+{
+  constexpr int F = DIM + 2, D = DIM;
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nint) return;
+  const int2 lr = face[i];
+  const long long a = lr.x, b = lr.y;
+  TC ul[F], ur[F], n[D];
+#pragma unroll
+  for (int k = 0; k < F; k++) { ul[k] = UF[a + NFE * k]; ur[k] = UF[b + NFE * k]; }
+#pragma unroll
+  for (int d = 0; d < D; d++) n[d] = nL[a + NFE * d];
+  const TC tl = tdA[a], tr = tdA[b];
+  TC fn[F];
+  rusanov<D, TC>(ph, ul, ur, n, fn);
+  TC cl[F], cr[F];
+#pragma unroll
+  for (int k = 0; k < F; k++) { cl[k] = fn[k] * tl; cr[k] = -fn[k] * tr; }
+  if (VISC) {
+    TC nn = n[0] * n[0];
+#pragma unroll
+    for (int d = 1; d < D; d++) nn = fr_fma(n[d], n[d], nn);
+    const TC pen = fsign[i] ? -ph.pen_fact : ph.pen_fact;
+#pragma unroll
+    for (int k = 0; k < F; k++) {
+      TC al = k ? VF[a + NFE * (k - 1)] : TC(0), ar = k ? VF[b + NFE * (k - 1)] : TC(0);
+      TC fv = ldg_normal<TC>(al, ar, ul[k], ur[k], pen, ph.tau, nn);
+      cl[k] = cl[k] + fv * tl;
+      cr[k] = cr[k] + (-fv) * tr;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < F; k++) { CF[a + NFE * k] = cl[k]; CF[b + NFE * k] = cr[k]; }
+}
+
+// ---------------------------------------------------------------------------
+// Stage, last part (per element): norm_tconf - norm_tdisf, the VCJH
+// correction (calculate_corrected_divergence, src/eles.cpp:1594-1661), and
+// either the residual (MODE 0) or the RK45 stage update
+// (eles::AdvanceSolution, src/eles.cpp:1155-1178) followed by the next
+// stage's traces (MODE 1).  The inviscid path (VISC 0) evaluates the flux,
+// its divergence and its normal component here itself, in the reference's
+// order; the viscous path takes DV and ND from fr_grad_kernel.
 template <int DIM, int P, int EPB, int NT, int VISC, int MODE, typename TC>
 __global__ void __launch_bounds__(NT)
-fr_flux_kernel(double* __restrict__ U, double* __restrict__ REG, const TC* __restrict__ UF,
-               TC* __restrict__ UFn, const TC* __restrict__ VF, const TC* __restrict__ ND,
-               const TC* __restrict__ DV, const int* __restrict__ mate, const unsigned char* __restrict__ side,
-               const TC* __restrict__ nL, const TC* __restrict__ tdA, const TC* __restrict__ JG,
-               const double* __restrict__ detj, double* __restrict__ DIV, double* __restrict__ partial, long long E,
-               Line<TC> L, PhysT<TC> ph, double rk_a, double rk_b, double dt, int first_stage)
+fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restrict__ UFn, const TC* __restrict__ CF,
+                 const TC* __restrict__ ND, const TC* __restrict__ DV, const TC* __restrict__ JG,
+                 const double* __restrict__ detj, double* __restrict__ DIV, double* __restrict__ partial, long long E,
+                 Line<TC> L, PhysT<TC> ph, double rk_a, double rk_b, double dt, int first_stage)
 {
   using S = Shape<DIM, P>;
   constexpr int NU = S::NU, NF = S::NF, F = S::F, D = DIM;
-  constexpr int IF = Items<NT, EPB * NF>::N, IU = Items<NT, EPB * NU>::N;
   extern __shared__ __align__(16) unsigned char fr_smem[];
-  // sU: solution (FP64), sC: norm_tconf - norm_tdisf, sFl: transformed
-  // inviscid flux (inviscid path only), sRed: norm partial sums
-  constexpr int NFL = VISC ? 1 : EPB * D * F * NU;
+  // sU: solution (FP64), sRed: norm partials, sC: norm_tconf - norm_tdisf,
+  // sFl: transformed inviscid flux (inviscid path only)
   auto sU = reinterpret_cast<double (*)[F][NU]>(fr_smem);
   auto sRed = reinterpret_cast<double (*)[F]>(fr_smem + sizeof(double) * EPB * F * NU);
   auto sC = reinterpret_cast<TC (*)[F][NF]>(fr_smem + sizeof(double) * (EPB * F * NU + (NT / 32) * F));
   auto sFl = reinterpret_cast<TC (*)[D][F][NU]>(fr_smem + sizeof(double) * (EPB * F * NU + (NT / 32) * F) +
                                                  sizeof(TC) * EPB * F * NF);
-  (void)NFL;
   const long long e0 = (long long)blockIdx.x * EPB;
   const long long NFE = (long long)NF * E;
 
-  // --- global gathers first
-  TC pun[IF][F], pn[IF][D], pta[IF], pvo[IF][VISC ? F - 1 : 1], pvn[IF][VISC ? F - 1 : 1], pnd[IF][VISC ? F : 1];
-  unsigned char psd[IF];
-#pragma unroll
-  for (int it = 0; it < IF; it++) {
-    int w = threadIdx.x + it * NT, el = w / NF, f = w - el * NF;
-    long long e = e0 + el;
-    if (w < EPB * NF && e < E) {
-      size_t own = f + (size_t)NF * e;
-      int mt = mate[own];
-      psd[it] = side[own];
-      pta[it] = tdA[own];
-#pragma unroll
-      for (int k = 0; k < F; k++) pun[it][k] = UF[mt + NFE * k];
-#pragma unroll
-      for (int d = 0; d < D; d++) pn[it][d] = nL[own + NFE * d];
-      if (VISC) {
-#pragma unroll
-        for (int k = 0; k < F - 1; k++) { pvo[it][k] = VF[own + NFE * k]; pvn[it][k] = VF[mt + NFE * k]; }
-#pragma unroll
-        for (int k = 0; k < F; k++) pnd[it][k] = ND[own + NFE * k];
-      }
-    }
-  }
-  TC pdv[IU][VISC ? F : 1], pG[IU][VISC ? 1 : D * D];
-  double preg[IU][MODE ? F : 1], pdj[IU];
-#pragma unroll
-  for (int it = 0; it < IU; it++) {
-    int w = threadIdx.x + it * NT, el = w / NU, u = w - el * NU;
-    long long e = e0 + el;
-    if (w < EPB * NU && e < E) {
-      size_t p = u + (size_t)NU * e;
-      pdj[it] = detj[p];
-      if (VISC) {
-#pragma unroll
-        for (int k = 0; k < F; k++) pdv[it][k] = DV[u + (size_t)NU * (e + E * k)];
-      } else {
-#pragma unroll
-        for (int q = 0; q < D * D; q++) pG[it][q] = JG[(size_t)D * D * p + q];
-      }
-      if (MODE == 1 && !first_stage) {
-#pragma unroll
-        for (int k = 0; k < F; k++) preg[it][k] = REG[u + (size_t)NU * (e + E * k)];
-      }
-    }
-  }
   for (int w = threadIdx.x; w < EPB * F * NU; w += NT) {
     int el = w / (F * NU), r = w - el * F * NU, k = r / NU, u = r - k * NU;
     long long e = e0 + el;
     sU[el][k][u] = e < E ? U[u + (size_t)NU * (e + E * k)] : 1.0;
   }
-  __syncthreads();
-
-  if (!VISC) {
+  if (VISC) {
+    for (int w = threadIdx.x; w < EPB * F * NF; w += NT) {
+      int el = w / (F * NF), r = w - el * F * NF, k = r / NF, f = r - k * NF;
+      long long e = e0 + el;
+      if (e < E) {
+        size_t g = f + (size_t)NF * (e + E * k);
+        sC[el][k][f] = CF[g] - ND[g];      // daxpy(-1, norm_tdisf, norm_tconf)
+      }
+    }
+  } else {
+    __syncthreads();
     // transformed inviscid flux at the solution points (evaluate_invFlux, src/eles.cpp:1331-1418)
+    for (int w = threadIdx.x; w < EPB * NU; w += NT) {
+      int el = w / NU, u = w - el * NU;
+      long long e = e0 + el;
+      if (e >= E) continue;
+      const TC* G = JG + (size_t)D * D * (u + (size_t)NU * e);
+      TC g[D * D];
 #pragma unroll
-    for (int it = 0; it < IU; it++) {
-      int w = threadIdx.x + it * NT, el = w / NU, u = w - el * NU;
-      if (w >= EPB * NU || e0 + el >= E) continue;
+      for (int q = 0; q < D * D; q++) g[q] = G[q];
       TC q[F], fi[F][D];
 #pragma unroll
       for (int k = 0; k < F; k++) q[k] = (TC)sU[el][k][u];
@@ -505,52 +515,24 @@ fr_flux_kernel(double* __restrict__ U, double* __restrict__ REG, const TC* __res
       for (int l = 0; l < D; l++)
 #pragma unroll
         for (int k = 0; k < F; k++) {
-          TC acc = pG[it][l] * fi[k][0];
+          TC acc = g[l] * fi[k][0];
 #pragma unroll
-          for (int m = 1; m < D; m++) acc = acc + pG[it][l + D * m] * fi[k][m];
+          for (int m = 1; m < D; m++) acc = acc + g[l + D * m] * fi[k][m];
           sFl[el][l][k][u] = acc;
         }
     }
     __syncthreads();
-  }
-
-  // --- common normal flux minus the discontinuous normal flux at every own flux point
-#pragma unroll
-  for (int it = 0; it < IF; it++) {
-    int w = threadIdx.x + it * NT, el = w / NF, f = w - el * NF;
-    if (w >= EPB * NF || e0 + el >= E) continue;
-    const bool left = psd[it] & 1;
-    TC uo[F];
-#pragma unroll
-    for (int k = 0; k < F; k++) uo[k] = line_interp<DIM, P, TC, double>(L, &sU[el][k][0], 1, f);
-    const TC* ul = left ? uo : pun[it];
-    const TC* ur = left ? pun[it] : uo;
-    TC fn[F];
-    rusanov<D, TC>(ph, ul, ur, pn[it], fn);
-    const TC ta = pta[it];
-    TC c[F];
-#pragma unroll
-    for (int k = 0; k < F; k++) c[k] = left ? fn[k] * ta : -fn[k] * ta;
-    if (VISC) {
-      TC nn = pn[it][0] * pn[it][0];
-#pragma unroll
-      for (int d = 1; d < D; d++) nn = nn + pn[it][d] * pn[it][d];
-      const TC pen = (psd[it] & 2) ? -ph.pen_fact : ph.pen_fact;
-#pragma unroll
-      for (int k = 0; k < F; k++) {
-        TC ao = k ? pvo[it][k - 1] : TC(0), an = k ? pvn[it][k - 1] : TC(0);
-        TC fv = left ? ldg_normal<TC>(ao, an, ul[k], ur[k], pen, ph.tau, nn)
-                     : ldg_normal<TC>(an, ao, ul[k], ur[k], pen, ph.tau, nn);
-        c[k] = c[k] + (left ? fv * ta : -fv * ta);
-        sC[el][k][f] = c[k] - pnd[it][k];
-      }
-    } else {
+    // norm_tconf - norm_tdisf with the normal component extrapolated here (extrapolate_totalFlux)
+    for (int w = threadIdx.x; w < EPB * NF; w += NT) {
+      int el = w / NF, f = w - el * NF;
+      long long e = e0 + el;
+      if (e >= E) continue;
       int u0, st, ax; bool plus;
       fpt_line<DIM, P>(f, u0, st, ax, plus);
 #pragma unroll
       for (int k = 0; k < F; k++) {
         TC v = line_interp<DIM, P, TC, TC>(L, &sFl[el][ax][k][0], 1, f);
-        sC[el][k][f] = c[k] - (plus ? v : -v);
+        sC[el][k][f] = CF[f + (size_t)NF * (e + E * k)] - (plus ? v : -v);
       }
     }
   }
@@ -559,19 +541,19 @@ fr_flux_kernel(double* __restrict__ U, double* __restrict__ REG, const TC* __res
   double red[F];
 #pragma unroll
   for (int k = 0; k < F; k++) red[k] = 0.0;
-#pragma unroll
-  for (int it = 0; it < IU; it++) {
-    int w = threadIdx.x + it * NT, el = w / NU, u = w - el * NU;
+  for (int w = threadIdx.x; w < EPB * NU; w += NT) {
+    int el = w / NU, u = w - el * NU;
     long long e = e0 + el;
-    if (w >= EPB * NU || e >= E) continue;
+    if (e >= E) continue;
     int abc[3];
     upt_abc<DIM, P>(u, abc[0], abc[1], abc[2]);
-    const double dj = pdj[it];
+    const double dj = detj[u + (size_t)NU * e];
 #pragma unroll
     for (int k = 0; k < F; k++) {
+      size_t gi = u + (size_t)NU * (e + E * k);
       TC acc;
       if (VISC) {
-        acc = pdv[it][k];
+        acc = DV[gi];
       } else {
         acc = deriv_line<DIM, P, TC, TC>(L, &sFl[el][0][k][0], 1, u, 0, abc[0]);
 #pragma unroll
@@ -589,13 +571,12 @@ fr_flux_kernel(double* __restrict__ U, double* __restrict__ REG, const TC* __res
         TC cf = face_plus<DIM>(fc) ? L.gR[al] : -L.gL[al];
         acc = acc + sC[el][k][q] * cf;
       }
-      size_t gi = u + (size_t)NU * (e + E * k);
       double R = (double)acc;
       if (MODE == 0) {
         DIV[gi] = R;
       } else {
         double rhs = -R / dj;
-        double res = first_stage ? dt * rhs : rk_a * preg[it][k] + dt * rhs;
+        double res = first_stage ? dt * rhs : rk_a * REG[gi] + dt * rhs;
         REG[gi] = res;
         double un = sU[el][k][u] + rk_b * res;
         U[gi] = un;
@@ -623,11 +604,10 @@ fr_flux_kernel(double* __restrict__ U, double* __restrict__ REG, const TC* __res
       partial[(size_t)blockIdx.x * F + threadIdx.x] = v;
     }
     // traces of the updated state for the next stage
-#pragma unroll
-    for (int it = 0; it < IF; it++) {
-      int w = threadIdx.x + it * NT, el = w / NF, f = w - el * NF;
+    for (int w = threadIdx.x; w < EPB * NF; w += NT) {
+      int el = w / NF, f = w - el * NF;
       long long e = e0 + el;
-      if (w >= EPB * NF || e >= E) continue;
+      if (e >= E) continue;
 #pragma unroll
       for (int k = 0; k < F; k++)
         UFn[f + (size_t)NF * (e + E * k)] = line_interp<DIM, P, TC, double>(L, &sU[el][k][0], 1, f);

@@ -40,8 +40,11 @@ static const double kRK4B[5] = {0.149659021999229, 0.379210312999627, 0.82295502
 
 struct Bufs {
   double *U = nullptr, *REG = nullptr, *DIV = nullptr, *detj64 = nullptr, *partial = nullptr, *norms = nullptr;
-  void *UF[2] = {nullptr, nullptr}, *VF = nullptr, *ND = nullptr, *DV = nullptr, *nL = nullptr, *tdA = nullptr,
-       *JG = nullptr, *detj = nullptr;
+  void *UF[2] = {nullptr, nullptr}, *VF = nullptr, *ND = nullptr, *DV = nullptr, *CF = nullptr, *nL = nullptr,
+       *tdA = nullptr, *JG = nullptr, *detj = nullptr;
+  int2* face = nullptr;
+  unsigned char* fsign = nullptr;
+  long long nint = 0;
   int* mate = nullptr;
   unsigned char* side = nullptr;
 };
@@ -50,7 +53,8 @@ struct Runner {
   virtual ~Runner() {}
   virtual void trace(const Bufs& b, int cur, cudaStream_t s) = 0;
   virtual void grad(const Bufs& b, int cur, cudaStream_t s) = 0;
-  virtual void flux(const Bufs& b, int cur, int mode, int stage, double dt, bool want_partial, cudaStream_t s) = 0;
+  virtual void face(const Bufs& b, int cur, cudaStream_t s) = 0;
+  virtual void update(const Bufs& b, int cur, int mode, int stage, double dt, bool want_partial, cudaStream_t s) = 0;
   virtual void ke(const Bufs& b, double* partial, int nblk, cudaStream_t s) = 0;
   virtual int flux_blocks() const = 0;
   virtual int launches_per_stage() const = 0;
@@ -95,7 +99,7 @@ struct RunnerT : Runner {
     ph = PhysT<TC>::make(p);
   }
   int flux_blocks() const override { return (int)((E + EPB - 1) / EPB); }
-  int launches_per_stage() const override { return visc ? 2 : 1; }
+  int launches_per_stage() const override { return visc ? 3 : 2; }
   void trace(const Bufs& b, int cur, cudaStream_t s) override
   {
     long long n = E * S::NF;
@@ -114,23 +118,33 @@ struct RunnerT : Runner {
         b.U, (const TC*)b.UF[cur], b.mate, b.side, (const TC*)b.JG, (const TC*)b.detj, (const TC*)b.nL, (TC*)b.VF,
         (TC*)b.ND, (TC*)b.DV, E, L, ph);
   }
-  template <int VISC, int MODE>
-  void flux_t(const Bufs& b, int cur, int stage, double dt, bool want_partial, cudaStream_t s)
+  void face(const Bufs& b, int cur, cudaStream_t s) override
   {
-    constexpr size_t sm = flux_smem_bytes<DIM, P, EPB, NT, VISC, TC>();
-    static bool once = (set_smem((const void*)fr_flux_kernel<DIM, P, EPB, NT, VISC, MODE, TC>, sm), true);
-    (void)once;
-    fr_flux_kernel<DIM, P, EPB, NT, VISC, MODE, TC><<<flux_blocks(), NT, sm, s>>>(
-        b.U, b.REG, (const TC*)b.UF[cur], (TC*)b.UF[cur ^ 1], (const TC*)b.VF, (const TC*)b.ND, (const TC*)b.DV,
-        b.mate, b.side, (const TC*)b.nL, (const TC*)b.tdA, (const TC*)b.JG, b.detj64, b.DIV,
-        want_partial ? b.partial : nullptr, E, L, ph, kRK4A[stage], kRK4B[stage], dt, stage == 0 ? 1 : 0);
+    if (b.nint == 0) return;
+    unsigned g = (unsigned)((b.nint + 127) / 128);
+    if (visc)
+      fr_face_kernel<DIM, 1, TC><<<g, 128, 0, s>>>(b.face, b.fsign, b.nint, (const TC*)b.UF[cur], (const TC*)b.VF,
+                                                   (const TC*)b.nL, (const TC*)b.tdA, (TC*)b.CF, E * S::NF, ph);
+    else
+      fr_face_kernel<DIM, 0, TC><<<g, 128, 0, s>>>(b.face, b.fsign, b.nint, (const TC*)b.UF[cur], nullptr,
+                                                   (const TC*)b.nL, (const TC*)b.tdA, (TC*)b.CF, E * S::NF, ph);
   }
-  void flux(const Bufs& b, int cur, int mode, int stage, double dt, bool want_partial, cudaStream_t s) override
+  template <int VISC, int MODE>
+  void update_t(const Bufs& b, int cur, int stage, double dt, bool want_partial, cudaStream_t s)
+  {
+    constexpr size_t sm = update_smem_bytes<DIM, P, EPB, NT, VISC, TC>();
+    static bool once = (set_smem((const void*)fr_update_kernel<DIM, P, EPB, NT, VISC, MODE, TC>, sm), true);
+    (void)once;
+    fr_update_kernel<DIM, P, EPB, NT, VISC, MODE, TC><<<flux_blocks(), NT, sm, s>>>(
+        b.U, b.REG, (TC*)b.UF[cur ^ 1], (const TC*)b.CF, (const TC*)b.ND, (const TC*)b.DV, (const TC*)b.JG, b.detj64,
+        b.DIV, want_partial ? b.partial : nullptr, E, L, ph, kRK4A[stage], kRK4B[stage], dt, stage == 0 ? 1 : 0);
+  }
+  void update(const Bufs& b, int cur, int mode, int stage, double dt, bool want_partial, cudaStream_t s) override
   {
     if (visc) {
-      if (mode == 0) flux_t<1, 0>(b, cur, stage, dt, false, s); else flux_t<1, 1>(b, cur, stage, dt, want_partial, s);
+      if (mode == 0) update_t<1, 0>(b, cur, stage, dt, false, s); else update_t<1, 1>(b, cur, stage, dt, want_partial, s);
     } else {
-      if (mode == 0) flux_t<0, 0>(b, cur, stage, dt, false, s); else flux_t<0, 1>(b, cur, stage, dt, want_partial, s);
+      if (mode == 0) update_t<0, 0>(b, cur, stage, dt, false, s); else update_t<0, 1>(b, cur, stage, dt, want_partial, s);
     }
   }
   void ke(const Bufs& b, double* partial, int nblk, cudaStream_t s) override
@@ -230,6 +244,14 @@ fr_status upload_geometry(fr_solver* s)
     side[i] = (m.is_left[i] ? 1 : 0) | (sgn < 0. ? 2 : 0);
   }
   FR_CUDA(cudaMemcpy(s->b.side, side.data(), side.size(), cudaMemcpyHostToDevice));
+  std::vector<int2> face(m.il.size());
+  std::vector<unsigned char> fsign(m.il.size());
+  for (size_t i = 0; i < face.size(); i++) {
+    face[i] = make_int2(m.il[i], m.ir[i]);
+    fsign[i] = (side[m.il[i]] & 2) ? 1 : 0;
+  }
+  FR_CUDA(cudaMemcpy(s->b.face, face.data(), face.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  FR_CUDA(cudaMemcpy(s->b.fsign, fsign.data(), fsign.size(), cudaMemcpyHostToDevice));
   return FR_OK;
 }
 
@@ -250,8 +272,9 @@ fr_status check_launch(const char* what)
 fr_status stage(fr_solver* s, int st, double dt, bool want_partial, cudaStream_t stream)
 {
   if (s->sch.viscous) { s->run->grad(s->b, s->cur, stream); s->launches++; }
-  s->run->flux(s->b, s->cur, 1, st, dt, want_partial, stream);
-  s->launches++;
+  s->run->face(s->b, s->cur, stream);
+  s->run->update(s->b, s->cur, 1, st, dt, want_partial, stream);
+  s->launches += 2;
   s->cur ^= 1;
   return check_launch("fr stage kernels");
 }
@@ -315,6 +338,10 @@ fr_status fr_solver_create(const fr_mesh_desc* md, const fr_scheme_desc* sd, int
     if ((st = dalloc(s.get(), &p, nf * E * F * tc))) return st; s->b.ND = p;
     if ((st = dalloc(s.get(), &p, nu * E * F * tc))) return st; s->b.DV = p;
   }
+  if ((st = dalloc(s.get(), &p, nf * E * F * tc))) return st; s->b.CF = p;
+  s->b.nint = (long long)m.il.size();
+  if ((st = dalloc(s.get(), &s->b.face, (size_t)s->b.nint))) return st;
+  if ((st = dalloc(s.get(), &s->b.fsign, (size_t)s->b.nint))) return st;
   if ((st = dalloc(s.get(), &p, nf * E * D * tc))) return st; s->b.nL = p;
   if ((st = dalloc(s.get(), &p, nf * E * tc))) return st; s->b.tdA = p;
   if ((st = dalloc(s.get(), &p, D * D * nu * E * tc))) return st; s->b.JG = p;
@@ -436,8 +463,9 @@ fr_status fr_solver_residual(fr_solver* s, double* host_div, void* stream)
   FR_CUDA(cudaSetDevice(s->device));
   cudaStream_t st = STRM(s, stream);
   if (s->sch.viscous) { s->run->grad(s->b, s->cur, st); s->launches++; }
-  s->run->flux(s->b, s->cur, 0, 0, 0.0, false, st);
-  s->launches++;
+  s->run->face(s->b, s->cur, st);
+  s->run->update(s->b, s->cur, 0, 0, 0.0, false, st);
+  s->launches += 2;
   fr_status r = check_launch("fr residual kernels");
   if (r) return r;
   size_t n = (size_t)s->mesh.nu * s->mesh.ne * s->mesh.nfields;
@@ -519,33 +547,35 @@ long long fr_solver_launch_count(const fr_solver* s) { return s ? s->launches : 
 
 void* fr_solver_stream(fr_solver* s) { return s ? (void*)s->own_stream : nullptr; }
 
-fr_status fr_solver_profile_stage(fr_solver* s, int reps, double dt, double* ms_grad, double* ms_flux)
+fr_status fr_solver_profile_stage(fr_solver* s, int reps, double dt, double* ms3)
 {
-  if (!s || reps <= 0 || !ms_grad || !ms_flux) return fail(FR_ERR_ARG, "bad argument");
+  if (!s || reps <= 0 || !ms3) return fail(FR_ERR_ARG, "bad argument");
   FR_CUDA(cudaSetDevice(s->device));
   cudaStream_t st = s->own_stream;
-  cudaEvent_t ev[3];
-  for (int i = 0; i < 3; i++) FR_CUDA(cudaEventCreate(&ev[i]));
-  double tg = 0.0, tf = 0.0;
+  cudaEvent_t ev[4];
+  for (int i = 0; i < 4; i++) FR_CUDA(cudaEventCreate(&ev[i]));
+  double acc[3] = {0, 0, 0};
   for (int r = 0; r < reps; r++) {
     int k = r % 5;
     FR_CUDA(cudaEventRecord(ev[0], st));
     if (s->sch.viscous) { s->run->grad(s->b, s->cur, st); s->launches++; }
     FR_CUDA(cudaEventRecord(ev[1], st));
-    s->run->flux(s->b, s->cur, 1, k, dt, k == 4, st);
-    s->launches++;
-    s->cur ^= 1;
+    s->run->face(s->b, s->cur, st);
     FR_CUDA(cudaEventRecord(ev[2], st));
-    FR_CUDA(cudaEventSynchronize(ev[2]));
-    float a = 0.f, b = 0.f;
-    FR_CUDA(cudaEventElapsedTime(&a, ev[0], ev[1]));
-    FR_CUDA(cudaEventElapsedTime(&b, ev[1], ev[2]));
-    tg += a; tf += b;
+    s->run->update(s->b, s->cur, 1, k, dt, k == 4, st);
+    s->launches += 2;
+    s->cur ^= 1;
+    FR_CUDA(cudaEventRecord(ev[3], st));
+    FR_CUDA(cudaEventSynchronize(ev[3]));
+    for (int i = 0; i < 3; i++) {
+      float ms = 0.f;
+      FR_CUDA(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+      acc[i] += ms;
+    }
   }
-  for (int i = 0; i < 3; i++) cudaEventDestroy(ev[i]);
+  for (int i = 0; i < 4; i++) cudaEventDestroy(ev[i]);
   FR_CUDA(cudaGetLastError());
-  *ms_grad = tg / reps;
-  *ms_flux = tf / reps;
+  for (int i = 0; i < 3; i++) ms3[i] = acc[i] / reps;
   return FR_OK;
 }
 

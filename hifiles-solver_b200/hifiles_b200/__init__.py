@@ -73,7 +73,7 @@ def lib():
         "fr_solver_launch_count": (C.c_longlong, [vp]),
         "fr_solver_stream": (vp, [vp]),
         "fr_solver_sync": (C.c_int, [vp]),
-        "fr_solver_profile_stage": (C.c_int, [vp, C.c_int, C.c_double, dp, dp]),
+        "fr_solver_profile_stage": (C.c_int, [vp, C.c_int, C.c_double, dp]),
         "fr_mesh_geometry": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(SchemeDesc), ip, dp, dp, dp, dp, dp, ip, ip]),
         "fr_line_operators": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, dp]),
     }
@@ -287,7 +287,7 @@ class Solver:
         _check(lib().fr_solver_sync(self.h))
 
     def profile_stage(self, reps, dt):
-        """Mean CUDA-event ms of (gradient kernel, flux/update kernel) over reps stages."""
-        a, b = C.c_double(), C.c_double()
-        _check(lib().fr_solver_profile_stage(self.h, int(reps), float(dt), C.byref(a), C.byref(b)))
-        return a.value, b.value
+        """Mean CUDA-event ms of the (gradient, interface-flux, update) kernels over reps stages."""
+        out = np.zeros(3)
+        _check(lib().fr_solver_profile_stage(self.h, int(reps), float(dt), _dp(out)))
+        return tuple(out)

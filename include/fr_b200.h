@@ -125,10 +125,11 @@ long long fr_solver_launch_count(const fr_solver* s);
 void* fr_solver_stream(fr_solver* s);
 fr_status fr_solver_sync(fr_solver* s);
 
-/* Runs `reps` RK stages one by one (advancing the state) and returns the mean
- * CUDA-event duration of each of the two stage kernels on the solver's stream
- * (ms_grad is 0 for inviscid runs).  For roofline accounting. */
-fr_status fr_solver_profile_stage(fr_solver* s, int reps, double dt, double* ms_grad, double* ms_flux);
+/* Runs `reps` RK stages one by one (advancing the state) and returns in ms3
+ * the mean CUDA-event duration, on the solver's stream, of the three stage
+ * kernels: gradient/flux (0 for inviscid runs), interface fluxes, and
+ * correction + update.  For roofline accounting. */
+fr_status fr_solver_profile_stage(fr_solver* s, int reps, double dt, double* ms3);
 
 /* ------------------------------------------------------------------------
  * Host-only set-up queries (no GPU is touched).
