@@ -142,6 +142,7 @@ def run_b200(a, rank, world, local):
                      precision=1 if a.precision == "fp32" else 0, device=dev)
     u0 = tgv_state(s.geometry()["pos_upts"])
     s.set_state(u0)
+    tiles = s.autotune(5) if not a.no_tune else None
     dt = 1e-3
     E, nu, F = s.n_eles, s.n_upts, s.n_fields
     dof_step = E * nu * F * 5
@@ -232,7 +233,9 @@ def run_b200(a, rank, world, local):
                    "precision": a.precision, "l2": "inputs larger than L2 (working set ~%.2f GB)" %
                                                     ((E * nu * F * 8 * 2 + E * 96 * F * tc * 2 + E * 96 * 15 * tc +
                                                       E * nu * 10 * tc) / 1e9),
-                   "parallelism": "replicas" if world > 1 else "single GPU"},
+                   "parallelism": "replicas" if world > 1 else "single GPU",
+                   "tiles": {"grad_elements_per_cta": tiles[0], "grad_threads": tiles[1],
+                             "update_elements_per_cta": tiles[2], "update_threads": tiles[3]} if tiles else None},
         "roofline": {"bound": "hbm", "kernel": "one RK stage = fr_grad_kernel + fr_face_kernel + fr_update_kernel",
                      "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / pk["hbm_gbs"], "peak_source": pk_src,
@@ -253,6 +256,7 @@ def main():
     ap.add_argument("--n", type=int, default=32)
     ap.add_argument("--order", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true")
     a = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

@@ -157,18 +157,66 @@ __device__ __forceinline__ T deriv_line(const Line<T>& L, const S* s, int sst, i
   return acc;
 }
 
+// Per-block copy of the operator pieces that threads index with their own
+// (divergent) point indices, plus a table with the line of every flux point:
+// code = u0 | stride << 8 | axis << 16 | plus << 18.  Reading these from
+// shared memory avoids both serialised constant-bank loads and divergent
+// branches on the face index.
+template <typename T, int NF>
+struct BlockOps {
+  T D[kMaxN1][kMaxN1];
+  T gL[kMaxN1], gR[kMaxN1];
+  int code[NF];
+};
+
+template <typename T, int NF>
+__host__ __device__ constexpr size_t blockops_bytes()
+{
+  return (sizeof(BlockOps<T, NF>) + 15) / 16 * 16;
+}
+
+template <int DIM, int P, typename T, int NF>
+__device__ __forceinline__ void fill_blockops(BlockOps<T, NF>* B, const Line<T>& L, int tid, int nt)
+{
+  for (int i = tid; i < kMaxN1 * kMaxN1; i += nt) B->D[i / kMaxN1][i % kMaxN1] = L.D[i / kMaxN1][i % kMaxN1];
+  for (int i = tid; i < kMaxN1; i += nt) { B->gL[i] = L.gL[i]; B->gR[i] = L.gR[i]; }
+  for (int f = tid; f < NF; f += nt) {
+    int u0, st, ax; bool plus;
+    fpt_line<DIM, P>(f, u0, st, ax, plus);
+    B->code[f] = u0 | (st << 8) | (ax << 16) | ((plus ? 1 : 0) << 18);
+  }
+}
+
+__device__ __forceinline__ int code_u0(int c) { return c & 255; }
+__device__ __forceinline__ int code_st(int c) { return (c >> 8) & 255; }
+__device__ __forceinline__ int code_ax(int c) { return (c >> 16) & 3; }
+__device__ __forceinline__ bool code_plus(int c) { return (c >> 18) & 1; }
+
+// line_interp with the line taken from a flux-point code
+template <int P, typename T, typename S>
+__device__ __forceinline__ T interp_code(const Line<T>& L, int c, const S* s)
+{
+  const int u0 = code_u0(c), st = code_st(c);
+  const bool plus = code_plus(c);
+  T acc = T(0);
+#pragma unroll
+  for (int m = 0; m <= P; m++) acc = acc + (T)s[u0 + m * st] * (plus ? L.Lp[m] : L.Lm[m]);
+  return acc;
+}
+
 // Dynamic shared-memory sizes of the stage kernels.
 template <int DIM, int P, int EPB, typename TC>
-constexpr size_t grad_smem_bytes()
+__host__ __device__ constexpr size_t grad_smem_bytes()
 {
   using S = Shape<DIM, P>;
-  return sizeof(TC) * EPB * S::F * (S::NU + 2 * S::NF + 2 * DIM * S::NU);
+  return blockops_bytes<TC, S::NF>() + sizeof(TC) * EPB * S::F * (S::NU + 2 * S::NF + 2 * DIM * S::NU);
 }
 template <int DIM, int P, int EPB, int NT, int VISC, typename TC>
-constexpr size_t update_smem_bytes()
+__host__ __device__ constexpr size_t update_smem_bytes()
 {
   using S = Shape<DIM, P>;
-  return sizeof(double) * (EPB * S::F * S::NU + (NT / 32) * S::F) + sizeof(TC) * EPB * S::F * S::NF +
+  return blockops_bytes<TC, S::NF>() + sizeof(double) * (EPB * S::F * S::NU + (NT / 32) * S::F) +
+         sizeof(TC) * EPB * S::F * S::NF +
          (VISC ? 0 : sizeof(TC) * EPB * DIM * S::F * S::NU);
 }
 
@@ -219,13 +267,17 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
   constexpr int NU = S::NU, NF = S::NF, F = S::F, D = DIM;
   constexpr int IF = Items<NT, EPB * NF>::N, IU = Items<NT, EPB * NU>::N;
   extern __shared__ __align__(16) unsigned char fr_smem[];
-  // sU: solution, sX: delta_disu_fpts, sUf: own solution at the flux points,
-  // sG: physical gradient (component k + F*d), sFl: transformed total flux
-  auto sU = reinterpret_cast<TC (*)[F][NU]>(fr_smem);
-  auto sX = reinterpret_cast<TC (*)[F][NF]>(fr_smem + sizeof(TC) * EPB * F * NU);
-  auto sUf = reinterpret_cast<TC (*)[F][NF]>(fr_smem + sizeof(TC) * EPB * F * (NU + NF));
-  auto sG = reinterpret_cast<TC (*)[F * D][NU]>(fr_smem + sizeof(TC) * EPB * F * (NU + 2 * NF));
-  auto sFl = reinterpret_cast<TC (*)[D][F][NU]>(fr_smem + sizeof(TC) * EPB * F * (NU + 2 * NF + D * NU));
+  // B: operator pieces and flux-point line table; sU: solution, sX:
+  // delta_disu_fpts, sUf: own solution at the flux points, sG: physical
+  // gradient (component k + F*d), sFl: transformed total flux
+  auto B = reinterpret_cast<BlockOps<TC, NF>*>(fr_smem);
+  unsigned char* sm0 = fr_smem + blockops_bytes<TC, NF>();
+  auto sU = reinterpret_cast<TC (*)[F][NU]>(sm0);
+  auto sX = reinterpret_cast<TC (*)[F][NF]>(sm0 + sizeof(TC) * EPB * F * NU);
+  auto sUf = reinterpret_cast<TC (*)[F][NF]>(sm0 + sizeof(TC) * EPB * F * (NU + NF));
+  auto sG = reinterpret_cast<TC (*)[F * D][NU]>(sm0 + sizeof(TC) * EPB * F * (NU + 2 * NF));
+  auto sFl = reinterpret_cast<TC (*)[D][F][NU]>(sm0 + sizeof(TC) * EPB * F * (NU + 2 * NF + D * NU));
+  fill_blockops<DIM, P, TC, NF>(B, L, threadIdx.x, NT);
   const long long e0 = (long long)blockIdx.x * EPB;
   const long long NFE = (long long)NF * E;
 
@@ -271,9 +323,10 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
     int w = threadIdx.x + it * NT, el = w / NF, f = w - el * NF;
     if (w >= EPB * NF || e0 + el >= E) continue;
     TC pen = (psd[it] & 2) ? -ph.pen_fact : ph.pen_fact;
+    const int cd = B->code[f];
 #pragma unroll
     for (int k = 0; k < F; k++) {
-      TC uo = line_interp<DIM, P, TC, TC>(L, &sU[el][k][0], 1, f);
+      TC uo = interp_code<P, TC, TC>(L, cd, &sU[el][k][0]);
       TC un = pun[it][k];
       TC ul = (psd[it] & 1) ? uo : un, ur = (psd[it] & 1) ? un : uo;
       TC uc = TC(0.5) * (ul + ur) - pen * (ul - ur);
@@ -302,8 +355,8 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
       const int st = upt_stride<DIM, P>(d), ub = u - i * st;
       TC Dr[P + 1];
 #pragma unroll
-      for (int m = 0; m <= P; m++) Dr[m] = L.D[i][m];
-      const TC gm = L.gL[am], gpl = L.gR[ap];
+      for (int m = 0; m <= P; m++) Dr[m] = B->D[i][m];
+      const TC gm = B->gL[am], gpl = B->gR[ap];
 #pragma unroll
       for (int k = 0; k < F; k++) {
         // the gradient only feeds the viscous flux: contracted with FMAs
@@ -359,8 +412,9 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
     if (w >= EPB * NF || e >= E) continue;
     size_t own = f + (size_t)NF * e;
     TC uf[F], gf[F][D], fv[F][D];
-    int u0, st, ax; bool plus;
-    fpt_line<DIM, P>(f, u0, st, ax, plus);
+    const int cd = B->code[f];
+    const int u0 = code_u0(cd), st = code_st(cd), ax = code_ax(cd);
+    const bool plus = code_plus(cd);
     TC Lc[P + 1];
 #pragma unroll
     for (int m = 0; m <= P; m++) Lc[m] = plus ? L.Lp[m] : L.Lm[m];
@@ -381,7 +435,10 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
     for (int k = 1; k < F; k++) VF[own + NFE * (k - 1)] = project<D, TC>(fv, k, pn[it]);
 #pragma unroll
     for (int k = 0; k < F; k++) {
-      TC v = line_interp<DIM, P, TC, TC>(L, &sFl[el][ax][k][0], 1, f);
+      const TC* s = &sFl[el][ax][k][0];
+      TC v = TC(0);
+#pragma unroll
+      for (int m = 0; m <= P; m++) v = v + s[u0 + m * st] * Lc[m];
       ND[own + NFE * k] = plus ? v : -v;
     }
   }
@@ -393,14 +450,19 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
     if (w >= EPB * NU || e >= E) continue;
     int abc[3];
     upt_abc<DIM, P>(u, abc[0], abc[1], abc[2]);
+    TC Dm[D][P + 1];
+#pragma unroll
+    for (int d = 0; d < D; d++)
+#pragma unroll
+      for (int m = 0; m <= P; m++) Dm[d][m] = B->D[abc[d]][m];
 #pragma unroll
     for (int k = 0; k < F; k++) {
-      TC acc = deriv_line<DIM, P, TC, TC>(L, &sFl[el][0][k][0], 1, u, 0, abc[0]);
+      TC acc = TC(0);
 #pragma unroll
-      for (int d = 1; d < D; d++) {
+      for (int d = 0; d < D; d++) {
         const int st = upt_stride<DIM, P>(d), ub = u - abc[d] * st;
 #pragma unroll
-        for (int m = 0; m <= P; m++) acc = acc + sFl[el][d][k][ub + m * st] * L.D[abc[d]][m];
+        for (int m = 0; m <= P; m++) acc = acc + sFl[el][d][k][ub + m * st] * Dm[d][m];
       }
       DV[u + (size_t)NU * (e + E * k)] = acc;
     }
@@ -472,13 +534,17 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
   using S = Shape<DIM, P>;
   constexpr int NU = S::NU, NF = S::NF, F = S::F, D = DIM;
   extern __shared__ __align__(16) unsigned char fr_smem[];
-  // sU: solution (FP64), sRed: norm partials, sC: norm_tconf - norm_tdisf,
-  // sFl: transformed inviscid flux (inviscid path only)
-  auto sU = reinterpret_cast<double (*)[F][NU]>(fr_smem);
-  auto sRed = reinterpret_cast<double (*)[F]>(fr_smem + sizeof(double) * EPB * F * NU);
-  auto sC = reinterpret_cast<TC (*)[F][NF]>(fr_smem + sizeof(double) * (EPB * F * NU + (NT / 32) * F));
-  auto sFl = reinterpret_cast<TC (*)[D][F][NU]>(fr_smem + sizeof(double) * (EPB * F * NU + (NT / 32) * F) +
+  // B: operator pieces and flux-point line table; sU: solution (FP64), sRed:
+  // norm partials, sC: norm_tconf - norm_tdisf, sFl: transformed inviscid
+  // flux (inviscid path only)
+  auto B = reinterpret_cast<BlockOps<TC, NF>*>(fr_smem);
+  unsigned char* sm0 = fr_smem + blockops_bytes<TC, NF>();
+  auto sU = reinterpret_cast<double (*)[F][NU]>(sm0);
+  auto sRed = reinterpret_cast<double (*)[F]>(sm0 + sizeof(double) * EPB * F * NU);
+  auto sC = reinterpret_cast<TC (*)[F][NF]>(sm0 + sizeof(double) * (EPB * F * NU + (NT / 32) * F));
+  auto sFl = reinterpret_cast<TC (*)[D][F][NU]>(sm0 + sizeof(double) * (EPB * F * NU + (NT / 32) * F) +
                                                  sizeof(TC) * EPB * F * NF);
+  fill_blockops<DIM, P, TC, NF>(B, L, threadIdx.x, NT);
   const long long e0 = (long long)blockIdx.x * EPB;
   const long long NFE = (long long)NF * E;
 
@@ -527,11 +593,11 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
       int el = w / NF, f = w - el * NF;
       long long e = e0 + el;
       if (e >= E) continue;
-      int u0, st, ax; bool plus;
-      fpt_line<DIM, P>(f, u0, st, ax, plus);
+      const int cd = B->code[f];
+      const bool plus = code_plus(cd);
 #pragma unroll
       for (int k = 0; k < F; k++) {
-        TC v = line_interp<DIM, P, TC, TC>(L, &sFl[el][ax][k][0], 1, f);
+        TC v = interp_code<P, TC, TC>(L, cd, &sFl[el][code_ax(cd)][k][0]);
         sC[el][k][f] = CF[f + (size_t)NF * (e + E * k)] - (plus ? v : -v);
       }
     }
@@ -555,12 +621,12 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
       if (VISC) {
         acc = DV[gi];
       } else {
-        acc = deriv_line<DIM, P, TC, TC>(L, &sFl[el][0][k][0], 1, u, 0, abc[0]);
+        acc = TC(0);
 #pragma unroll
-        for (int d = 1; d < D; d++) {
+        for (int d = 0; d < D; d++) {
           const int st = upt_stride<DIM, P>(d), ub = u - abc[d] * st;
 #pragma unroll
-          for (int m = 0; m <= P; m++) acc = acc + sFl[el][d][k][ub + m * st] * L.D[abc[d]][m];
+          for (int m = 0; m <= P; m++) acc = acc + sFl[el][d][k][ub + m * st] * B->D[abc[d]][m];
         }
       }
       // opp_3 row of u: one column per face, in flux-point order
@@ -568,7 +634,7 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
       for (int fc = 0; fc < S::NFACE; fc++) {
         int al;
         int q = face_fpt<DIM, P>(fc, abc[0], abc[1], abc[2], al);
-        TC cf = face_plus<DIM>(fc) ? L.gR[al] : -L.gL[al];
+        TC cf = face_plus<DIM>(fc) ? B->gR[al] : -B->gL[al];
         acc = acc + sC[el][k][q] * cf;
       }
       double R = (double)acc;
@@ -608,9 +674,10 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
       int el = w / NF, f = w - el * NF;
       long long e = e0 + el;
       if (e >= E) continue;
+      const int cd = B->code[f];
 #pragma unroll
       for (int k = 0; k < F; k++)
-        UFn[f + (size_t)NF * (e + E * k)] = line_interp<DIM, P, TC, double>(L, &sU[el][k][0], 1, f);
+        UFn[f + (size_t)NF * (e + E * k)] = interp_code<P, TC, double>(L, cd, &sU[el][k][0]);
     }
   }
 }

@@ -49,6 +49,10 @@ struct Bufs {
   unsigned char* side = nullptr;
 };
 
+struct Tile {
+  int epb, nt;
+};
+
 struct Runner {
   virtual ~Runner() {}
   virtual void trace(const Bufs& b, int cur, cudaStream_t s) = 0;
@@ -56,27 +60,51 @@ struct Runner {
   virtual void face(const Bufs& b, int cur, cudaStream_t s) = 0;
   virtual void update(const Bufs& b, int cur, int mode, int stage, double dt, bool want_partial, cudaStream_t s) = 0;
   virtual void ke(const Bufs& b, double* partial, int nblk, cudaStream_t s) = 0;
-  virtual int flux_blocks() const = 0;
+  virtual int flux_blocks() const = 0;      // blocks of the update kernel (norm partials)
+  virtual int max_flux_blocks() const = 0;  // over all update-kernel tiles
   virtual int launches_per_stage() const = 0;
+  // tile variants of the two element kernels (autotuning)
+  virtual int n_grad_tiles() const = 0;
+  virtual int n_update_tiles() const = 0;
+  virtual Tile grad_tile(int i) const = 0;
+  virtual Tile update_tile(int i) const = 0;
+  virtual void select(int g, int u) = 0;
+  virtual int grad_sel() const = 0;
+  virtual int update_sel() const = 0;
 };
 
-template <int DIM, int P> struct Cfg;     // elements per block, threads per block
-template <> struct Cfg<2, 1> { static constexpr int EPB = 32, NT = 128; };
-template <> struct Cfg<2, 2> { static constexpr int EPB = 16, NT = 128; };
-template <> struct Cfg<2, 3> { static constexpr int EPB = 8, NT = 128; };
-template <> struct Cfg<2, 4> { static constexpr int EPB = 8, NT = 256; };
-template <> struct Cfg<2, 5> { static constexpr int EPB = 4, NT = 160; };
-template <> struct Cfg<3, 1> { static constexpr int EPB = 12, NT = 128; };
-template <> struct Cfg<3, 2> { static constexpr int EPB = 4, NT = 128; };
-template <> struct Cfg<3, 3> { static constexpr int EPB = 2, NT = 128; };
-template <> struct Cfg<3, 4> { static constexpr int EPB = 1, NT = 128; };
+// Compiled tile variants (elements per CTA, threads per CTA) of the gradient
+// and update kernels per (dims, order); the first entry is the default, the
+// autotuner may pick another.
+template <int DIM, int P> struct Tiles;
+#define FR_TILES(D_, P_, G, U) \
+  template <> struct Tiles<D_, P_> { static constexpr Tile grad[] = G; static constexpr Tile upd[] = U; };
+#define T_(...) {__VA_ARGS__}
+FR_TILES(2, 1, T_({32, 128}), T_({32, 128}))
+FR_TILES(2, 2, T_({16, 128}), T_({16, 128}))
+FR_TILES(2, 3, T_({8, 128}, {4, 64}, {16, 256}), T_({8, 128}, {4, 64}, {16, 256}))
+FR_TILES(2, 4, T_({8, 256}), T_({8, 256}))
+FR_TILES(2, 5, T_({4, 160}), T_({4, 160}))
+FR_TILES(3, 1, T_({12, 128}), T_({12, 128}))
+FR_TILES(3, 2, T_({4, 128}, {2, 64}, {8, 256}), T_({4, 128}, {2, 64}, {8, 256}))
+FR_TILES(3, 3, T_({2, 128}, {1, 64}, {1, 96}, {2, 192}, {4, 256}), T_({2, 128}, {1, 64}, {4, 256}, {2, 96}, {4, 128}))
+FR_TILES(3, 4, T_({1, 128}, {1, 160}, {2, 256}), T_({1, 128}, {2, 256}, {1, 160}))
+#undef T_
+#undef FR_TILES
+
+static void set_smem(const void* k, size_t bytes)
+{
+  if (bytes > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
 
 template <int DIM, int P, typename TC>
 struct RunnerT : Runner {
   using S = Shape<DIM, P>;
-  static constexpr int EPB = Cfg<DIM, P>::EPB, NT = Cfg<DIM, P>::NT;
+  static constexpr int NG = sizeof(Tiles<DIM, P>::grad) / sizeof(Tile);
+  static constexpr int NUP = sizeof(Tiles<DIM, P>::upd) / sizeof(Tile);
   long long E;
   int visc;
+  int gsel = 0, usel = 0;
   Line<TC> L;
   Line<double> L64;
   PhysT<TC> ph;
@@ -98,26 +126,50 @@ struct RunnerT : Runner {
     }
     ph = PhysT<TC>::make(p);
   }
-  int flux_blocks() const override { return (int)((E + EPB - 1) / EPB); }
+  int n_grad_tiles() const override { return NG; }
+  int n_update_tiles() const override { return NUP; }
+  Tile grad_tile(int i) const override { return Tiles<DIM, P>::grad[i]; }
+  Tile update_tile(int i) const override { return Tiles<DIM, P>::upd[i]; }
+  void select(int g, int u) override { gsel = g; usel = u; }
+  int grad_sel() const override { return gsel; }
+  int update_sel() const override { return usel; }
+  int flux_blocks() const override
+  {
+    int epb = Tiles<DIM, P>::upd[usel].epb;
+    return (int)((E + epb - 1) / epb);
+  }
+  int max_flux_blocks() const override
+  {
+    int m = 1;
+    for (int i = 0; i < NUP; i++) {
+      int b = (int)((E + Tiles<DIM, P>::upd[i].epb - 1) / Tiles<DIM, P>::upd[i].epb);
+      m = b > m ? b : m;
+    }
+    return m;
+  }
   int launches_per_stage() const override { return visc ? 3 : 2; }
   void trace(const Bufs& b, int cur, cudaStream_t s) override
   {
     long long n = E * S::NF;
     fr_trace_kernel<DIM, P, TC><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b.U, (TC*)b.UF[cur], E, L);
   }
-  static void set_smem(const void* k, size_t bytes)
+
+  template <int I>
+  void grad_i(const Bufs& b, int cur, cudaStream_t s)
   {
-    if (bytes > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if constexpr (I < NG) {
+      if (I != gsel) return grad_i<I + 1>(b, cur, s);
+      constexpr int EPB = Tiles<DIM, P>::grad[I].epb, NT = Tiles<DIM, P>::grad[I].nt;
+      constexpr size_t sm = grad_smem_bytes<DIM, P, EPB, TC>();
+      static bool once = (set_smem((const void*)fr_grad_kernel<DIM, P, EPB, NT, TC>, sm), true);
+      (void)once;
+      fr_grad_kernel<DIM, P, EPB, NT, TC><<<(unsigned)((E + EPB - 1) / EPB), NT, sm, s>>>(
+          b.U, (const TC*)b.UF[cur], b.mate, b.side, (const TC*)b.JG, (const TC*)b.detj, (const TC*)b.nL,
+          (TC*)b.VF, (TC*)b.ND, (TC*)b.DV, E, L, ph);
+    }
   }
-  void grad(const Bufs& b, int cur, cudaStream_t s) override
-  {
-    constexpr size_t sm = grad_smem_bytes<DIM, P, EPB, TC>();
-    static bool once = (set_smem((const void*)fr_grad_kernel<DIM, P, EPB, NT, TC>, sm), true);
-    (void)once;
-    fr_grad_kernel<DIM, P, EPB, NT, TC><<<flux_blocks(), NT, sm, s>>>(
-        b.U, (const TC*)b.UF[cur], b.mate, b.side, (const TC*)b.JG, (const TC*)b.detj, (const TC*)b.nL, (TC*)b.VF,
-        (TC*)b.ND, (TC*)b.DV, E, L, ph);
-  }
+  void grad(const Bufs& b, int cur, cudaStream_t s) override { grad_i<0>(b, cur, s); }
+
   void face(const Bufs& b, int cur, cudaStream_t s) override
   {
     if (b.nint == 0) return;
@@ -129,22 +181,30 @@ struct RunnerT : Runner {
       fr_face_kernel<DIM, 0, TC><<<g, 128, 0, s>>>(b.face, b.fsign, b.nint, (const TC*)b.UF[cur], nullptr,
                                                    (const TC*)b.nL, (const TC*)b.tdA, (TC*)b.CF, E * S::NF, ph);
   }
-  template <int VISC, int MODE>
-  void update_t(const Bufs& b, int cur, int stage, double dt, bool want_partial, cudaStream_t s)
+
+  template <int I, int VISC, int MODE>
+  void update_i(const Bufs& b, int cur, int stage, double dt, bool want_partial, cudaStream_t s)
   {
-    constexpr size_t sm = update_smem_bytes<DIM, P, EPB, NT, VISC, TC>();
-    static bool once = (set_smem((const void*)fr_update_kernel<DIM, P, EPB, NT, VISC, MODE, TC>, sm), true);
-    (void)once;
-    fr_update_kernel<DIM, P, EPB, NT, VISC, MODE, TC><<<flux_blocks(), NT, sm, s>>>(
-        b.U, b.REG, (TC*)b.UF[cur ^ 1], (const TC*)b.CF, (const TC*)b.ND, (const TC*)b.DV, (const TC*)b.JG, b.detj64,
-        b.DIV, want_partial ? b.partial : nullptr, E, L, ph, kRK4A[stage], kRK4B[stage], dt, stage == 0 ? 1 : 0);
+    if constexpr (I < NUP) {
+      if (I != usel) return update_i<I + 1, VISC, MODE>(b, cur, stage, dt, want_partial, s);
+      constexpr int EPB = Tiles<DIM, P>::upd[I].epb, NT = Tiles<DIM, P>::upd[I].nt;
+      constexpr size_t sm = update_smem_bytes<DIM, P, EPB, NT, VISC, TC>();
+      static bool once = (set_smem((const void*)fr_update_kernel<DIM, P, EPB, NT, VISC, MODE, TC>, sm), true);
+      (void)once;
+      fr_update_kernel<DIM, P, EPB, NT, VISC, MODE, TC><<<(unsigned)((E + EPB - 1) / EPB), NT, sm, s>>>(
+          b.U, b.REG, (TC*)b.UF[cur ^ 1], (const TC*)b.CF, (const TC*)b.ND, (const TC*)b.DV, (const TC*)b.JG,
+          b.detj64, b.DIV, want_partial ? b.partial : nullptr, E, L, ph, kRK4A[stage], kRK4B[stage], dt,
+          stage == 0 ? 1 : 0);
+    }
   }
   void update(const Bufs& b, int cur, int mode, int stage, double dt, bool want_partial, cudaStream_t s) override
   {
     if (visc) {
-      if (mode == 0) update_t<1, 0>(b, cur, stage, dt, false, s); else update_t<1, 1>(b, cur, stage, dt, want_partial, s);
+      if (mode == 0) update_i<0, 1, 0>(b, cur, stage, dt, false, s);
+      else update_i<0, 1, 1>(b, cur, stage, dt, want_partial, s);
     } else {
-      if (mode == 0) update_t<0, 0>(b, cur, stage, dt, false, s); else update_t<0, 1>(b, cur, stage, dt, want_partial, s);
+      if (mode == 0) update_i<0, 0, 0>(b, cur, stage, dt, false, s);
+      else update_i<0, 0, 1>(b, cur, stage, dt, want_partial, s);
     }
   }
   void ke(const Bufs& b, double* partial, int nblk, cudaStream_t s) override
@@ -348,7 +408,7 @@ fr_status fr_solver_create(const fr_mesh_desc* md, const fr_scheme_desc* sd, int
   if ((st = dalloc(s.get(), &p, nu * E * tc))) return st; s->b.detj = p;
   if ((st = dalloc(s.get(), &s->b.mate, nf * E))) return st;
   if ((st = dalloc(s.get(), &s->b.side, nf * E))) return st;
-  if ((st = dalloc(s.get(), &s->b.partial, (size_t)s->run->flux_blocks() * F))) return st;
+  if ((st = dalloc(s.get(), &s->b.partial, (size_t)s->run->max_flux_blocks() * F))) return st;
   if ((st = dalloc(s.get(), &s->b.norms, F))) return st;
   s->nblk_ke = 296;
   if ((st = dalloc(s.get(), &s->ke_partial, (size_t)s->nblk_ke))) return st;
@@ -576,6 +636,62 @@ fr_status fr_solver_profile_stage(fr_solver* s, int reps, double dt, double* ms3
   for (int i = 0; i < 4; i++) cudaEventDestroy(ev[i]);
   FR_CUDA(cudaGetLastError());
   for (int i = 0; i < 3; i++) ms3[i] = acc[i] / reps;
+  return FR_OK;
+}
+
+fr_status fr_solver_autotune(fr_solver* s, int reps, int out4[4])
+{
+  if (!s || reps <= 0) return fail(FR_ERR_ARG, "bad argument");
+  FR_CUDA(cudaSetDevice(s->device));
+  cudaStream_t st = s->own_stream;
+  cudaEvent_t a, b;
+  FR_CUDA(cudaEventCreate(&a));
+  FR_CUDA(cudaEventCreate(&b));
+  auto time_it = [&](auto&& launch) -> double {
+    launch();                                  // warm-up (and shared-memory opt-in)
+    cudaEventRecord(a, st);
+    for (int r = 0; r < reps; r++) launch();
+    cudaEventRecord(b, st);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms / reps;
+  };
+  Runner* R = s->run.get();
+  int g0 = R->grad_sel(), u0 = R->update_sel();
+  // the gradient kernel only writes scratch (VF, ND, DV) and the update kernel
+  // in residual mode only writes DIV, so timing them leaves the state as it is
+  int gbest = g0;
+  if (s->sch.viscous) {
+    double best = 1e30;
+    for (int g = 0; g < R->n_grad_tiles(); g++) {
+      R->select(g, u0);
+      double ms = time_it([&] { R->grad(s->b, s->cur, st); s->launches++; });
+      if (ms < best) { best = ms; gbest = g; }
+    }
+    R->select(gbest, u0);
+    R->grad(s->b, s->cur, st);                 // scratch consistent with the current state
+    s->launches++;
+  }
+  int ubest = u0;
+  {
+    double best = 1e30;
+    for (int u = 0; u < R->n_update_tiles(); u++) {
+      R->select(gbest, u);
+      double ms = time_it([&] { R->update(s->b, s->cur, 0, 0, 0.0, false, st); s->launches++; });
+      if (ms < best) { best = ms; ubest = u; }
+    }
+  }
+  R->select(gbest, ubest);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  FR_CUDA(cudaGetLastError());
+  FR_CUDA(cudaStreamSynchronize(st));
+  drop_graphs(s);
+  if (out4) {
+    Tile tg = R->grad_tile(gbest), tu = R->update_tile(ubest);
+    out4[0] = tg.epb; out4[1] = tg.nt; out4[2] = tu.epb; out4[3] = tu.nt;
+  }
   return FR_OK;
 }
 

@@ -74,6 +74,7 @@ def lib():
         "fr_solver_stream": (vp, [vp]),
         "fr_solver_sync": (C.c_int, [vp]),
         "fr_solver_profile_stage": (C.c_int, [vp, C.c_int, C.c_double, dp]),
+        "fr_solver_autotune": (C.c_int, [vp, C.c_int, ip]),
         "fr_mesh_geometry": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(SchemeDesc), ip, dp, dp, dp, dp, dp, ip, ip]),
         "fr_line_operators": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, dp]),
     }
@@ -285,6 +286,12 @@ class Solver:
 
     def sync(self):
         _check(lib().fr_solver_sync(self.h))
+
+    def autotune(self, reps=5):
+        """Pick the fastest compiled tile variants; returns (grad EPB, grad NT, update EPB, update NT)."""
+        out = (C.c_int * 4)()
+        _check(lib().fr_solver_autotune(self.h, int(reps), out))
+        return tuple(out)
 
     def profile_stage(self, reps, dt):
         """Mean CUDA-event ms of the (gradient, interface-flux, update) kernels over reps stages."""

@@ -125,6 +125,14 @@ long long fr_solver_launch_count(const fr_solver* s);
 void* fr_solver_stream(fr_solver* s);
 fr_status fr_solver_sync(fr_solver* s);
 
+/* Autotuner: times every compiled tile variant (elements per CTA, threads per
+ * CTA) of the gradient and update kernels on this solver's mesh, `reps`
+ * launches each, keeps the fastest, and returns the choice as
+ * {grad elements, grad threads, update elements, update threads}.  The state
+ * is not changed.  Results do not depend on the tiles except for the
+ * summation order of the residual norms. */
+fr_status fr_solver_autotune(fr_solver* s, int reps, int out4[4]);
+
 /* Runs `reps` RK stages one by one (advancing the state) and returns in ms3
  * the mean CUDA-event duration, on the solver's stream, of the three stage
  * kernels: gradient/flux (0 for inviscid runs), interface fluxes, and

@@ -157,3 +157,18 @@ def test_errors_are_reported():
     with pytest.raises(H.FrError) as ei:
         s.advance(200, 5.0, norms=True)
     assert ei.value.status == 3
+
+
+def test_autotuned_tiles_give_identical_states():
+    """Tile choice (elements and threads per CTA) changes nothing per element."""
+    meta, a = load("hex_tgv_p3_n3")
+    s1, s2 = _solver(meta), _solver(meta)
+    s1.set_state(a["u0"])
+    s2.set_state(a["u0"])
+    before = s2.get_state()
+    tiles = s2.autotune(2)
+    assert np.array_equal(s2.get_state(), before)
+    assert all(t > 0 for t in tiles)
+    s1.advance(3, 1e-3)
+    s2.advance(3, 1e-3)
+    assert np.array_equal(s1.get_state(), s2.get_state())
