@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libfrb200.so")
 BUILD = os.path.join(HERE, "_build")
 
-SOURCES = ["fr_host.cpp", "fr_solver.cu", "fr_ops.cu"]
+SOURCES = ["fr_host.cpp", "fr_solver.cu", "fr_ops.cu", "fr_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 

@@ -683,7 +683,7 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
 }
 
 // Block sums -> norms (fixed order, one thread per field).
-__global__ void fr_norm_finalize(const double* __restrict__ partial, int nblk, int F, double inv_n,
+static __global__ void fr_norm_finalize(const double* __restrict__ partial, int nblk, int F, double inv_n,
                                  double* __restrict__ out)
 {
   int k = threadIdx.x;

@@ -250,6 +250,47 @@ fr_status fr_op_advance_rk45(int n_upts, int n_fields, int n_eles, int stage, do
                              double* disu_upts_0, double* disu_upts_1, const double* div_tconf_upts,
                              const double* detjac_upts, const double* src_upts, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Residual without device allocation.
+ *
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * when they need a residual: code in the middle of recording work for later
+ * replay, code whose device memory comes from someone else's pool, hosts that
+ * forbid allocation after start-up.  The caller passes every input and the
+ * output; the scratch between the stage kernels (traces, viscous-flux
+ * projections, normal discontinuous flux, divergence, common flux) lives in a
+ * fixed 32 MiB array of device memory inside the library, which every GPU that
+ * loads the library keeps until the process exits.  The first call on a
+ * device looks up that array's device address, so make the first call before
+ * any stream capture.  All calls share the array: calls whose work overlaps on
+ * the GPU (different streams, different host threads) race and must be
+ * serialised by the caller.  Meshes whose scratch would exceed 32 MiB are
+ * rejected with FR_ERR_ARG (hex P=3 Navier-Stokes: ~1950 elements).
+ * Output: div_tconf_upts of one CalcResidual, FP64, identical to
+ * fr_solver_residual on the same mesh and state.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+  int dims, order, n_eles, viscous;   /* quads (P 1..5) or hexes (P 1..4)               */
+  int upts_type, vcjh_scheme;         /* as in fr_scheme_desc (Gauss points only)       */
+  double eta;
+  fr_phys_desc phys;
+  const double* disu_upts;            /* (n_upts, n_eles, F) state                      */
+  const double* JGinv_upts;           /* (D, D, n_upts, n_eles)                         */
+  const double* detjac_upts;          /* (n_upts, n_eles)                               */
+  const double* norm_left;            /* (n_fpts, n_eles, D) unit normal of the
+                                         interface's left side, at both sides' points  */
+  const double* tdA_fpts;             /* (n_fpts, n_eles) own |J^-T n| dA               */
+  const int* mate;                    /* (n_fpts, n_eles) matching point, flat index     */
+  const unsigned char* side;          /* (n_fpts, n_eles) bit0 left side, bit1 negative
+                                         LDG penalty                                    */
+  long long n_int;                    /* interface points                               */
+  const int* face_lr;                 /* (n_int, 2) left/right flat indices, 8-byte aligned */
+  const unsigned char* face_sign;     /* (n_int) nonzero: negative LDG penalty           */
+  double* div_tconf_upts;             /* output (n_upts, n_eles, F)                      */
+} fr_residual_args;
+
+fr_status fr_residual_noalloc(const fr_residual_args* args, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
