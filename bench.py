@@ -106,6 +106,23 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(x, world, device="cpu"):
+    """Max of a per-rank scalar over all ranks (the time of the slowest rank)."""
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_value(dof_per_step_per_rank, ms_per_step_max, world):
+    """Whole-job throughput: every rank advances its own replica, the job takes
+    as long as the slowest rank."""
+    return dof_per_step_per_rank * world / (ms_per_step_max * 1e-3)
+
+
 def peaks():
     try:
         return json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json"))), "measured"
@@ -125,6 +142,18 @@ def cpu_baseline_port(n=12, P=3, steps=2):
     dof = m.n_eles * m.n_upts * m.n_fields * 5 * steps
     return {"value": dof / dt, "unit": "DOF-updates/s", "cores": 1, "kind": "port",
             "sample": "oracle (C restatement), TGV P=3 NS on %d^3 hexes, %d RK45 steps, 1 thread, %.1f s" % (n, steps, dt)}
+
+
+def cpu_baseline(a):
+    """The reference's own CPU code (oracle/_ref) on all host cores, bounded
+    sample; the plain-C oracle on one core if the reference build is absent."""
+    try:
+        import bench_reference
+        r = bench_reference.measure(n=10, P=a.order, steps=2)
+        return {"value": r["value"], "unit": "DOF-updates/s", "cores": r["procs"], "kind": "reference",
+                "sample": r["sample"]}
+    except (FileNotFoundError, RuntimeError, OSError):
+        return cpu_baseline_port()
 
 
 def run_b200(a, rank, world, local):
@@ -152,12 +181,8 @@ def run_b200(a, rank, world, local):
         if world > 1:
             torch.distributed.barrier()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda:%d" % dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+    def rank_max(x):
+        return max_over_ranks(x, world, "cuda:%d" % dev)
 
     # --- device-resident throughput (graph-replayed RK45 steps)
     s.advance(max(a.warmup, 3), dt)
@@ -175,8 +200,8 @@ def run_b200(a, rank, world, local):
     launches = s.launch_count() - l0
     ms = ev0.elapsed_time(ev1) / a.steps
     barrier()
-    ms = max_over_ranks(ms)
-    value = dof_step * world / (ms * 1e-3)
+    ms = rank_max(ms)
+    value = aggregate_value(dof_step, ms, world)
 
     # --- per-kernel event timing for the roofline (stage by stage, not replayed)
     ms_grad, ms_face, ms_upd = s.profile_stage(10, dt)
@@ -210,13 +235,13 @@ def run_b200(a, rank, world, local):
     e1.record(stream)
     e1.synchronize()
     wall = (time.perf_counter() - t0) / e2e_steps
-    e2e_ms = max_over_ranks(max(e0.elapsed_time(e1) / e2e_steps, wall * 1e3))
-    e2e = {"value": dof_step * world / (e2e_ms * 1e-3), "unit": "DOF-updates/s",
+    e2e_ms = rank_max(max(e0.elapsed_time(e1) / e2e_steps, wall * 1e3))
+    e2e = {"value": aggregate_value(dof_step, e2e_ms, world), "unit": "DOF-updates/s",
            "h2d_bytes_per_step": int(u0.size * 8), "d2h_bytes_per_step": int(F * 8),
            "ms_per_step": e2e_ms,
            "path": "Solver.set_state(pinned host state) + Solver.advance(1 step, norms) -> C ABI"}
 
-    cpu = cpu_baseline_port() if (rank == 0 and world == 1 and not a.no_cpu) else None
+    cpu = cpu_baseline(a) if (rank == 0 and world == 1 and not a.no_cpu) else None
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()

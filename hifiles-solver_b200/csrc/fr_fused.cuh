@@ -682,15 +682,23 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
   }
 }
 
-// Block sums -> norms (fixed order, one thread per field).
-static __global__ void fr_norm_finalize(const double* __restrict__ partial, int nblk, int F, double inv_n,
-                                 double* __restrict__ out)
+// Block partial sums -> norms: one CTA of 256 threads per field; thread t
+// sums partials t, t+256, ... in order, then a fixed shared-memory tree.  The
+// order depends only on the number of partials, so results are reproducible.
+static __global__ void __launch_bounds__(256)
+fr_norm_finalize(const double* __restrict__ partial, int nblk, int F, double inv_n, double* __restrict__ out)
 {
-  int k = threadIdx.x;
-  if (k >= F) return;
-  double s = 0.0;
-  for (int b = 0; b < nblk; b++) s += partial[(size_t)b * F + k];
-  out[k] = s * inv_n;
+  __shared__ double s[256];
+  const int k = blockIdx.x;
+  double acc = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += 256) acc += partial[(size_t)b * F + k];
+  s[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[k] = s[0] * inv_n;
 }
 
 // Kinetic energy: per-element quadrature with the point weights, block partials.

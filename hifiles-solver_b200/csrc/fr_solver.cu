@@ -578,7 +578,7 @@ fr_status fr_solver_advance(fr_solver* s, int n_steps, double dt, double* norms_
   if (norms_host) {
     int F = s->mesh.nfields;
     double inv_n = 1.0 / ((double)s->mesh.nu * (double)s->mesh.ne);
-    fr_norm_finalize<<<1, 32, 0, st>>>(s->b.partial, s->run->flux_blocks(), F, inv_n, s->b.norms);
+    fr_norm_finalize<<<F, 256, 0, st>>>(s->b.partial, s->run->flux_blocks(), F, inv_n, s->b.norms);
     s->launches++;
     FR_CUDA(cudaGetLastError());
     FR_CUDA(cudaMemcpyAsync(norms_host, s->b.norms, F * 8, cudaMemcpyDeviceToHost, st));
@@ -595,7 +595,7 @@ fr_status fr_solver_kinetic_energy(fr_solver* s, double* out, void* stream)
   FR_CUDA(cudaSetDevice(s->device));
   cudaStream_t st = STRM(s, stream);
   s->run->ke(s->b, s->ke_partial, s->nblk_ke, st);
-  fr_norm_finalize<<<1, 32, 0, st>>>(s->ke_partial, s->nblk_ke, 1, 1.0, s->ke_out);
+  fr_norm_finalize<<<1, 256, 0, st>>>(s->ke_partial, s->nblk_ke, 1, 1.0, s->ke_out);
   s->launches += 2;
   FR_CUDA(cudaGetLastError());
   FR_CUDA(cudaMemcpyAsync(out, s->ke_out, 8, cudaMemcpyDeviceToHost, st));
