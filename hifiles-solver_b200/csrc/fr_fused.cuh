@@ -205,11 +205,12 @@ __device__ __forceinline__ T interp_code(const Line<T>& L, int c, const S* s)
 }
 
 // Dynamic shared-memory sizes of the stage kernels.
-template <int DIM, int P, int EPB, typename TC>
+template <int DIM, int P, int EPB, typename TC, int LES = 0>
 __host__ __device__ constexpr size_t grad_smem_bytes()
 {
   using S = Shape<DIM, P>;
-  return blockops_bytes<TC, S::NF>() + sizeof(TC) * EPB * S::F * (S::NU + 2 * S::NF + 2 * DIM * S::NU);
+  return blockops_bytes<TC, S::NF>() + sizeof(TC) * EPB * S::F * (S::NU + 2 * S::NF + 2 * DIM * S::NU) +
+         (LES ? sizeof(TC) * EPB * (S::F - 1) * DIM * S::NU : 0);
 }
 template <int DIM, int P, int EPB, int NT, int VISC, typename TC>
 __host__ __device__ constexpr size_t update_smem_bytes()
@@ -255,8 +256,14 @@ __global__ void fr_trace_kernel(const double* __restrict__ U, TC* __restrict__ U
 //   gradient (what calculate_common_viscFlux evaluates for this side), kept
 //   only as its projection on the interface's left normal: VF (F-1 values,
 //   the mass component is zero).
+// With LES = 1 the eddy-viscosity SGS flux joins the viscous flux at the
+// solution points (evaluate_viscFlux, src/eles.cpp:2369-2380); its transformed
+// components (sgsf_upts, src/eles.cpp:2382-2409) are extrapolated to the flux
+// points (evaluate_sgsFlux, src/eles.cpp:3294-3368) and added there to the
+// physical viscous flux before the projection, as calculate_common_viscFlux
+// adds sgsf_fpts (src/int_inters.cpp:415-427).
 // Outputs VF (n_fpts, n_eles, F-1), ND (n_fpts, n_eles, F), DV (n_upts, n_eles, F).
-template <int DIM, int P, int EPB, int NT, typename TC>
+template <int DIM, int P, int EPB, int NT, typename TC, int LES = 0>
 __global__ void __launch_bounds__(NT)
 fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const int* __restrict__ mate,
                const unsigned char* __restrict__ side, const TC* __restrict__ JG, const TC* __restrict__ detj,
@@ -277,6 +284,8 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
   auto sUf = reinterpret_cast<TC (*)[F][NF]>(sm0 + sizeof(TC) * EPB * F * (NU + NF));
   auto sG = reinterpret_cast<TC (*)[F * D][NU]>(sm0 + sizeof(TC) * EPB * F * (NU + 2 * NF));
   auto sFl = reinterpret_cast<TC (*)[D][F][NU]>(sm0 + sizeof(TC) * EPB * F * (NU + 2 * NF + D * NU));
+  // sS (LES): transformed SGS flux, component (k - 1) + (F - 1) * l for fields k >= 1
+  auto sS = reinterpret_cast<TC (*)[(F - 1) * D][NU]>(sm0 + sizeof(TC) * EPB * F * (NU + 2 * NF + 2 * D * NU));
   fill_blockops<DIM, P, TC, NF>(B, L, threadIdx.x, NT);
   const long long e0 = (long long)blockIdx.x * EPB;
   const long long NFE = (long long)NF * E;
@@ -388,6 +397,20 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
     TC fi[F][D], fv[F][D];
     inv_flux<D, TC>(ph, q, fi);
     vis_flux_fast<D, TC>(ph, q, gp, fv);
+    if constexpr (LES != 0) {
+      TC fs[F][D];
+      sgs_flux<D, TC>(ph, q, gp, pdj[it], TC(P + 1), fs);
+#pragma unroll
+      for (int k = 1; k < F; k++)
+#pragma unroll
+        for (int l = 0; l < D; l++) {
+          TC a = pG[it][l] * fs[k][0];
+#pragma unroll
+          for (int m = 1; m < D; m++) a = a + pG[it][l + D * m] * fs[k][m];
+          sS[el][(k - 1) + (F - 1) * l][u] = a;
+          fv[k][l] = fv[k][l] + fs[k][l];
+        }
+    }
 #pragma unroll
     for (int k = 0; k < F; k++)
 #pragma unroll
@@ -431,6 +454,18 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
       }
     }
     vis_flux_fast<D, TC>(ph, uf, gf, fv);
+    if constexpr (LES != 0) {
+#pragma unroll
+      for (int k = 1; k < F; k++)
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+          const TC* s = &sS[el][(k - 1) + (F - 1) * d][0];
+          TC acc = s[u0] * Lc[0];
+#pragma unroll
+          for (int m = 1; m <= P; m++) acc = fr_fma(s[u0 + m * st], Lc[m], acc);
+          fv[k][d] = fv[k][d] + acc;
+        }
+    }
 #pragma unroll
     for (int k = 1; k < F; k++) VF[own + NFE * (k - 1)] = project<D, TC>(fv, k, pn[it]);
 #pragma unroll

@@ -18,16 +18,19 @@ namespace frb {
 
 struct Phys {
   double gamma, prandtl, mu_inf, rt_inf, c_sth, fix_vis, tau, pen_fact;
+  int sgs_model = 1;          // eddy-viscosity LES: 0 Smagorinsky, 1 WALE
+  double filter_ratio = 1.0;  // LES filter width over the element's point spacing
 };
 
 template <typename T>
 struct PhysT {
-  T gamma, gm1, prandtl, mu_inf, rt_inf, c_sth, fix_vis, tau, pen_fact;
+  T gamma, gm1, prandtl, mu_inf, rt_inf, c_sth, fix_vis, tau, pen_fact, filter_ratio;
+  int sgs_model;
   __host__ __device__ static PhysT make(const Phys& p) {
     PhysT q;
     q.gamma = (T)p.gamma; q.gm1 = (T)(p.gamma - 1.0); q.prandtl = (T)p.prandtl; q.mu_inf = (T)p.mu_inf;
     q.rt_inf = (T)p.rt_inf; q.c_sth = (T)p.c_sth; q.fix_vis = (T)p.fix_vis; q.tau = (T)p.tau;
-    q.pen_fact = (T)p.pen_fact;
+    q.pen_fact = (T)p.pen_fact; q.filter_ratio = (T)p.filter_ratio; q.sgs_model = p.sgs_model;
     return q;
   }
 };
@@ -273,6 +276,105 @@ __device__ __forceinline__ void ldg_flux(const PhysT<T>& ph, T pen, const T* ul,
       acc = (l == 0) ? fc * n[0] : acc + fc * n[l];
     }
     fn[k] = acc;
+  }
+}
+
+// Subgrid-scale flux of the eddy-viscosity LES models at a solution point
+// (eles::calc_sgsf_upts with sgs_model 0 = Smagorinsky, Cs = 0.1, or 1 =
+// WALE, Cw = 0.5; no wall model; src/eles.cpp:2456-2778), physical
+// components fs[k][l].  g is the physical gradient g[k][l] = d q_k / d x_l,
+// detjac the Jacobian determinant at the point, n1 = order + 1.
+//
+// Two index choices of the reference are kept as it evaluates them: its
+// "velocity" vector is u_i = q_i / rho for i < D, so u_0 = rho / rho
+// (src/eles.cpp:2483), and its velocity gradient subtracts u_j drho_j
+// (src/eles.cpp:2656).  Both enter only the energy flux through the
+// kinetic-energy gradient (the first also the internal energy); the strain
+// rate and hence the eddy viscosity see the second alone.  The filter width
+// is delta = filter_ratio vol^(1/D) / (order + 1) with vol = 2^D detjac
+// (eles_quads / eles_hexas::calc_ele_vol); the turbulent Prandtl number 0.5.
+// The WALE powers x^2.5, x^1.25, x^1.5 are taken through square roots.
+template <int D, typename T>
+__device__ __forceinline__ void sgs_flux(const PhysT<T>& ph, const T* q, const T (*g)[D], T detjac, T n1,
+                                         T (*fs)[D])
+{
+  constexpr int F = D + 2;
+  const T rho = q[0];
+  T u[D], ke = T(0);
+#pragma unroll
+  for (int i = 0; i < D; i++) {
+    u[i] = q[i] / rho;
+    ke = ke + T(0.5) * (u[i] * u[i]);
+  }
+  const T inte = q[F - 1] / rho - ke;
+  const T vol = detjac * T(D == 3 ? 8 : 4);
+  T root;
+  if (D == 3) root = (T)cbrt(vol);
+  else root = fr_sqrt<T>(vol);
+  const T delta = ph.filter_ratio * root / n1;
+  T du[D][D], de[D];
+#pragma unroll
+  for (int i = 0; i < D; i++) {
+    T dke = ke * g[0][i];
+#pragma unroll
+    for (int j = 0; j < D; j++) {
+      du[i][j] = (g[j + 1][i] - u[j] * g[0][j]) / rho;
+      dke = dke + rho * u[j] * du[i][j];
+    }
+    de[i] = (g[F - 1][i] - dke - g[0][i] * inte) / rho;
+  }
+  T S[D][D], diag = T(0);
+#pragma unroll
+  for (int i = 0; i < D; i++) {
+#pragma unroll
+    for (int j = 0; j < D; j++) S[i][j] = (du[i][j] + du[j][i]) / T(2);
+    diag = diag + S[i][i] / T(3);
+  }
+#pragma unroll
+  for (int i = 0; i < D; i++) S[i][i] = S[i][i] - diag;
+  T mu_t;
+  if (ph.sgs_model == 0) {
+    T s2 = T(0);
+#pragma unroll
+    for (int i = 0; i < D; i++)
+#pragma unroll
+      for (int j = 0; j < D; j++) s2 = s2 + T(2) * S[i][j] * S[i][j];
+    const T Cs = T(0.1);
+    mu_t = rho * Cs * Cs * delta * delta * fr_sqrt<T>(s2);
+  } else {
+    T Sq[D][D], dg = T(0);
+#pragma unroll
+    for (int i = 0; i < D; i++)
+#pragma unroll
+      for (int j = 0; j < D; j++) {
+        T a = T(0);
+#pragma unroll
+        for (int k = 0; k < D; k++) a = a + (du[i][k] * du[k][j] + du[j][k] * du[k][i]) / T(2);
+        Sq[i][j] = a;
+        dg = dg + du[i][j] * du[j][i] / T(3);
+      }
+#pragma unroll
+    for (int i = 0; i < D; i++) Sq[i][i] = Sq[i][i] - dg;
+    T num = T(0), den = T(0);
+#pragma unroll
+    for (int i = 0; i < D; i++)
+#pragma unroll
+      for (int j = 0; j < D; j++) {
+        num = num + Sq[i][j] * Sq[i][j];
+        den = den + S[i][j] * S[i][j];
+      }
+    const T sn = fr_sqrt<T>(num);
+    const T denom = den * den * fr_sqrt<T>(den) + num * fr_sqrt<T>(sn);
+    const T Cs = T(0.5);
+    mu_t = rho * Cs * Cs * delta * delta * (num * sn) / (denom + T(1.e-12));
+  }
+  const T Pr = T(0.5);
+#pragma unroll
+  for (int j = 0; j < D; j++) {
+    fs[0][j] = T(0);
+    fs[F - 1][j] = -ph.gamma * mu_t / Pr * de[j];
+#pragma unroll
+    for (int i = 1; i < F - 1; i++) fs[i][j] = T(-2) * mu_t * S[i - 1][j];
   }
 }
 

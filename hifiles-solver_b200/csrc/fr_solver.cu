@@ -103,12 +103,12 @@ struct RunnerT : Runner {
   static constexpr int NG = sizeof(Tiles<DIM, P>::grad) / sizeof(Tile);
   static constexpr int NUP = sizeof(Tiles<DIM, P>::upd) / sizeof(Tile);
   long long E;
-  int visc;
+  int visc, les;
   int gsel = 0, usel = 0;
   Line<TC> L;
   Line<double> L64;
   PhysT<TC> ph;
-  RunnerT(long long E_, int visc_, const Line1D& l, const Phys& p) : E(E_), visc(visc_)
+  RunnerT(long long E_, int visc_, int les_, const Line1D& l, const Phys& p) : E(E_), visc(visc_), les(les_)
   {
     for (int i = 0; i < kMaxN1; i++) {
       L.Lm[i] = L.Lp[i] = L.gL[i] = L.gR[i] = L.w[i] = TC(0);
@@ -154,21 +154,25 @@ struct RunnerT : Runner {
     fr_trace_kernel<DIM, P, TC><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b.U, (TC*)b.UF[cur], E, L);
   }
 
-  template <int I>
+  template <int I, int LES>
   void grad_i(const Bufs& b, int cur, cudaStream_t s)
   {
     if constexpr (I < NG) {
-      if (I != gsel) return grad_i<I + 1>(b, cur, s);
+      if (I != gsel) return grad_i<I + 1, LES>(b, cur, s);
       constexpr int EPB = Tiles<DIM, P>::grad[I].epb, NT = Tiles<DIM, P>::grad[I].nt;
-      constexpr size_t sm = grad_smem_bytes<DIM, P, EPB, TC>();
-      static bool once = (set_smem((const void*)fr_grad_kernel<DIM, P, EPB, NT, TC>, sm), true);
+      constexpr size_t sm = grad_smem_bytes<DIM, P, EPB, TC, LES>();
+      static bool once = (set_smem((const void*)fr_grad_kernel<DIM, P, EPB, NT, TC, LES>, sm), true);
       (void)once;
-      fr_grad_kernel<DIM, P, EPB, NT, TC><<<(unsigned)((E + EPB - 1) / EPB), NT, sm, s>>>(
+      fr_grad_kernel<DIM, P, EPB, NT, TC, LES><<<(unsigned)((E + EPB - 1) / EPB), NT, sm, s>>>(
           b.U, (const TC*)b.UF[cur], b.mate, b.side, (const TC*)b.JG, (const TC*)b.detj, (const TC*)b.nL,
           (TC*)b.VF, (TC*)b.ND, (TC*)b.DV, E, L, ph);
     }
   }
-  void grad(const Bufs& b, int cur, cudaStream_t s) override { grad_i<0>(b, cur, s); }
+  void grad(const Bufs& b, int cur, cudaStream_t s) override
+  {
+    if (les) grad_i<0, 1>(b, cur, s);
+    else grad_i<0, 0>(b, cur, s);
+  }
 
   void face(const Bufs& b, int cur, cudaStream_t s) override
   {
@@ -214,22 +218,22 @@ struct RunnerT : Runner {
 };
 
 template <typename TC>
-static Runner* make_runner_t(int dims, int P, long long E, int visc, const Line1D& l, const Phys& p)
+static Runner* make_runner_t(int dims, int P, long long E, int visc, int les, const Line1D& l, const Phys& p)
 {
   if (dims == 2) {
     switch (P) {
-      case 1: return new RunnerT<2, 1, TC>(E, visc, l, p);
-      case 2: return new RunnerT<2, 2, TC>(E, visc, l, p);
-      case 3: return new RunnerT<2, 3, TC>(E, visc, l, p);
-      case 4: return new RunnerT<2, 4, TC>(E, visc, l, p);
-      case 5: return new RunnerT<2, 5, TC>(E, visc, l, p);
+      case 1: return new RunnerT<2, 1, TC>(E, visc, les, l, p);
+      case 2: return new RunnerT<2, 2, TC>(E, visc, les, l, p);
+      case 3: return new RunnerT<2, 3, TC>(E, visc, les, l, p);
+      case 4: return new RunnerT<2, 4, TC>(E, visc, les, l, p);
+      case 5: return new RunnerT<2, 5, TC>(E, visc, les, l, p);
     }
   } else {
     switch (P) {
-      case 1: return new RunnerT<3, 1, TC>(E, visc, l, p);
-      case 2: return new RunnerT<3, 2, TC>(E, visc, l, p);
-      case 3: return new RunnerT<3, 3, TC>(E, visc, l, p);
-      case 4: return new RunnerT<3, 4, TC>(E, visc, l, p);
+      case 1: return new RunnerT<3, 1, TC>(E, visc, les, l, p);
+      case 2: return new RunnerT<3, 2, TC>(E, visc, les, l, p);
+      case 3: return new RunnerT<3, 3, TC>(E, visc, les, l, p);
+      case 4: return new RunnerT<3, 4, TC>(E, visc, les, l, p);
     }
   }
   return nullptr;
@@ -370,6 +374,12 @@ fr_status fr_solver_create(const fr_mesh_desc* md, const fr_scheme_desc* sd, int
   int maxP = md->dims == 2 ? 5 : 4;
   if (sd->order < 1 || sd->order > maxP) return fail(FR_ERR_UNSUPPORTED, "order outside the built range");
   if (sd->upts_type != 0) return fail(FR_ERR_UNSUPPORTED, "fused kernels need Gauss solution points");
+  if (sd->les != 0) {
+    if (sd->les != 1 || !sd->viscous) return fail(FR_ERR_ARG, "les must be 0 or 1, and 1 needs viscous = 1");
+    if (sd->sgs_model != 0 && sd->sgs_model != 1)
+      return fail(FR_ERR_UNSUPPORTED, "only the eddy-viscosity SGS models 0 (Smagorinsky) and 1 (WALE) are built");
+    if (!(sd->filter_ratio > 0.0)) return fail(FR_ERR_ARG, "filter_ratio must be positive");
+  }
   std::unique_ptr<fr_solver> s(new fr_solver());
   s->device = device;
   s->sch = *sd;
@@ -379,9 +389,12 @@ fr_status fr_solver_create(const fr_mesh_desc* md, const fr_scheme_desc* sd, int
   if (!build_mesh(md->dims, s->line, md->n_verts, md->xv, md->n_eles, md->c2v, md->shift, s->mesh, err))
     return fail(FR_ERR_MESH, err);
   FR_CUDA(cudaSetDevice(device));
-  Phys ph{sd->gamma, sd->prandtl, sd->mu_inf, sd->rt_inf, sd->c_sth, sd->fix_vis, sd->tau, sd->pen_fact};
-  Runner* r = sd->precision == 0 ? make_runner_t<double>(md->dims, sd->order, md->n_eles, sd->viscous, s->line, ph)
-                                  : make_runner_t<float>(md->dims, sd->order, md->n_eles, sd->viscous, s->line, ph);
+  Phys ph{sd->gamma, sd->prandtl, sd->mu_inf, sd->rt_inf, sd->c_sth, sd->fix_vis, sd->tau, sd->pen_fact,
+          sd->sgs_model, sd->filter_ratio};
+  const int les = sd->les;
+  Runner* r = sd->precision == 0
+                  ? make_runner_t<double>(md->dims, sd->order, md->n_eles, sd->viscous, les, s->line, ph)
+                  : make_runner_t<float>(md->dims, sd->order, md->n_eles, sd->viscous, les, s->line, ph);
   if (!r) return fail(FR_ERR_UNSUPPORTED, "no kernel for this (dims, order)");
   s->run.reset(r);
   Mesh& m = s->mesh;

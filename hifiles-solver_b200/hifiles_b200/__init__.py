@@ -38,7 +38,8 @@ class SchemeDesc(C.Structure):
     _fields_ = [("order", C.c_int), ("upts_type", C.c_int), ("vcjh_scheme", C.c_int), ("eta", C.c_double),
                 ("viscous", C.c_int), ("riemann", C.c_int), ("precision", C.c_int), ("gamma", C.c_double),
                 ("prandtl", C.c_double), ("mu_inf", C.c_double), ("rt_inf", C.c_double), ("c_sth", C.c_double),
-                ("fix_vis", C.c_double), ("tau", C.c_double), ("pen_fact", C.c_double)]
+                ("fix_vis", C.c_double), ("tau", C.c_double), ("pen_fact", C.c_double), ("les", C.c_int),
+                ("sgs_model", C.c_int), ("filter_ratio", C.c_double)]
 
 
 _LIB = None
@@ -136,13 +137,15 @@ def box_mesh(dims, n, lo, hi, jitter=0.0, seed=0):
 
 
 def _descs(dims, xv, c2v, shift, order, viscous=False, gamma=1.4, prandtl=0.72, mu_inf=0.0, rt_inf=1.0,
-           c_sth=1.0, fix_vis=1.0, tau=1.0, pen_fact=0.5, vcjh_scheme=1, eta=0.0, upts_type=0, precision=0):
+           c_sth=1.0, fix_vis=1.0, tau=1.0, pen_fact=0.5, vcjh_scheme=1, eta=0.0, upts_type=0, precision=0,
+           les=0, sgs_model=1, filter_ratio=1.0):
     xv = np.ascontiguousarray(xv, dtype=np.float64)
     c2v = np.ascontiguousarray(c2v, dtype=np.int32)
     md = MeshDesc(int(dims), xv.shape[0], _dp(xv), c2v.shape[0], c2v.ctypes.data_as(C.POINTER(C.c_int)),
                   (C.c_double * 3)(*(list(shift) + [0.0] * (3 - len(shift)))))
     sd = SchemeDesc(int(order), int(upts_type), int(vcjh_scheme), float(eta), int(bool(viscous)), 0, int(precision),
-                    gamma, prandtl, mu_inf, rt_inf, c_sth, fix_vis, tau, pen_fact)
+                    gamma, prandtl, mu_inf, rt_inf, c_sth, fix_vis, tau, pen_fact, int(les), int(sgs_model),
+                    float(filter_ratio))
     return md, sd, (xv, c2v)
 
 
@@ -178,7 +181,7 @@ class Solver:
 
     def __init__(self, dims, xv, c2v, shift, order, viscous=False, gamma=1.4, prandtl=0.72, mu_inf=0.0,
                  rt_inf=1.0, c_sth=1.0, fix_vis=1.0, tau=1.0, pen_fact=0.5, vcjh_scheme=1, eta=0.0, upts_type=0,
-                 precision=0, device=0):
+                 precision=0, device=0, les=0, sgs_model=1, filter_ratio=1.0):
         L = lib()
         self._xv = np.ascontiguousarray(xv, dtype=np.float64)
         self._c2v = np.ascontiguousarray(c2v, dtype=np.int32)
@@ -186,7 +189,8 @@ class Solver:
                       self._c2v.ctypes.data_as(C.POINTER(C.c_int)),
                       (C.c_double * 3)(*(list(shift) + [0.0] * (3 - len(shift)))))
         sd = SchemeDesc(int(order), int(upts_type), int(vcjh_scheme), float(eta), int(bool(viscous)), 0,
-                        int(precision), gamma, prandtl, mu_inf, rt_inf, c_sth, fix_vis, tau, pen_fact)
+                        int(precision), gamma, prandtl, mu_inf, rt_inf, c_sth, fix_vis, tau, pen_fact, int(les),
+                        int(sgs_model), float(filter_ratio))
         h = C.c_void_p()
         self.h = None
         _check(L.fr_solver_create(C.byref(md), C.byref(sd), int(device), C.byref(h)))

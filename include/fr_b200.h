@@ -72,6 +72,12 @@ typedef struct {
                             with FP64 state, RK register and reductions        */
   double gamma, prandtl, mu_inf, rt_inf, c_sth, fix_vis; /* gas + viscosity law */
   double tau, pen_fact;  /* LDG penalty parameters                             */
+  int les;               /* 1 adds the eddy-viscosity SGS flux (input key LES;
+                            viscous only; eles::calc_sgsf_upts,
+                            src/eles.cpp:2456-2778); 0 none                    */
+  int sgs_model;         /* with les: 0 Smagorinsky, 1 WALE (SGS_model); the
+                            filter-based models 2-4 are not built             */
+  double filter_ratio;   /* with les: filter width over the point spacing     */
 } fr_scheme_desc;
 
 fr_status fr_solver_create(const fr_mesh_desc* mesh, const fr_scheme_desc* scheme, int device,

@@ -42,7 +42,7 @@ struct or_mesh {
   double *detjac, *JG, *tdA, *nrm;
   int nint; int *il, *ir;                       /* interface fpts */
   /* work arrays */
-  double *ufp, *gup, *gfp, *tf, *ntd, *ntc, *ddu;
+  double *ufp, *gup, *gfp, *tf, *ntd, *ntc, *ddu, *sgu, *sgf;
 };
 
 /* ---------------------------------------------------------------- 1-D basis */
@@ -568,6 +568,8 @@ static void alloc_work(or_mesh* m)
   m->ntd = calloc(m->nf * E * F, sizeof(double));
   m->ntc = calloc(m->nf * E * F, sizeof(double));
   m->ddu = calloc(m->nf * E * F, sizeof(double));
+  m->sgu = calloc(m->nu * E * F * D, sizeof(double));
+  m->sgf = calloc(m->nf * E * F * D, sizeof(double));
 }
 
 or_mesh* or_mesh_new(int dims, int order, int n_verts, const double* xv, int n_eles, const int* c2v,
@@ -636,6 +638,7 @@ void or_mesh_free(or_mesh* m)
   free(m->pos_upts); free(m->pos_fpts); free(m->detjac); free(m->JG); free(m->tdA); free(m->nrm);
   free(m->il); free(m->ir);
   free(m->ufp); free(m->gup); free(m->gfp); free(m->tf); free(m->ntd); free(m->ntc); free(m->ddu);
+  free(m->sgu); free(m->sgf);
   free(m);
 }
 
@@ -825,14 +828,81 @@ static void ldg_flux(int D, int F, const double* ul, const double* ur, const dou
   }
 }
 
+/* Eddy-viscosity SGS flux at a solution point: eles::calc_sgsf_upts for
+ * sgs_model 0 (Smagorinsky) and 1 (WALE) without a wall model,
+ * src/eles.cpp:2456-2778.  Kept as the reference computes it, including two
+ * index choices of its own: the "velocity" vector is u(i) = q(i)/rho for
+ * i < D, so its first entry is rho/rho (src/eles.cpp:2483), and du(i,j)
+ * subtracts u(j)*drho(j) (src/eles.cpp:2656).  Both enter the kinetic-energy
+ * gradient of the energy flux; the strain rate sees only the second. */
+static void sgsf(int D, const or_physics* ph, const double* u, const double* gu /* (F,D) [k+F*l] */, double detjac,
+                 int order, double* f /* (F,D) */)
+{
+  int F = D + 2;
+  double uu[3], drho[3], dene[3], dke[3], de[3], dmom[3][3], du[3][3], S[3][3];
+  double ke = 0.0, diag = 0.0, Smod = 0.0, Pr = 0.5, mu_t = 0.0;
+  double rho = u[0];
+  for (int i = 0; i < D; i++) { uu[i] = u[i] / rho; ke += 0.5 * pow(uu[i], 2); }
+  double inte = u[F - 1] / rho - ke;
+  for (int k = 0; k < F * D; k++) f[k] = 0.0;
+  double vol = detjac * (D == 3 ? 8. : 4.);                     /* calc_ele_vol */
+  double delta = ph->filter_ratio * pow(vol, 1. / D) / (order + 1.);
+  for (int i = 0; i < D; i++) {
+    drho[i] = gu[0 + F * i];
+    dene[i] = gu[(F - 1) + F * i];
+    for (int j = 1; j < F - 1; j++) dmom[i][j - 1] = gu[j + F * i];
+  }
+  for (int i = 0; i < D; i++) {
+    dke[i] = ke * drho[i];
+    for (int j = 0; j < D; j++) {
+      du[i][j] = (dmom[i][j] - uu[j] * drho[j]) / rho;
+      dke[i] += rho * uu[j] * du[i][j];
+    }
+    de[i] = (dene[i] - dke[i] - drho[i] * inte) / rho;
+  }
+  for (int i = 0; i < D; i++) {
+    for (int j = 0; j < D; j++) S[i][j] = (du[i][j] + du[j][i]) / 2.0;
+    diag += S[i][i] / 3.0;
+  }
+  for (int i = 0; i < D; i++) S[i][i] -= diag;
+  for (int i = 0; i < D; i++)
+    for (int j = 0; j < D; j++) Smod += 2.0 * S[i][j] * S[i][j];
+  Smod = sqrt(Smod);
+  if (ph->sgs_model == 0) {
+    double Cs = 0.1;
+    mu_t = rho * Cs * Cs * delta * delta * Smod;
+  } else {
+    double Cs = 0.5, num = 0.0, denom = 0.0, eps = 1.e-12, Sq[3][3];
+    diag = 0.0;
+    for (int i = 0; i < D; i++)
+      for (int j = 0; j < D; j++) {
+        Sq[i][j] = 0.0;
+        for (int k = 0; k < D; ++k) Sq[i][j] += (du[i][k] * du[k][j] + du[j][k] * du[k][i]) / 2.0;
+        diag += du[i][j] * du[j][i] / 3.0;
+      }
+    for (int i = 0; i < D; i++) Sq[i][i] -= diag;
+    for (int i = 0; i < D; i++)
+      for (int j = 0; j < D; j++) { num += Sq[i][j] * Sq[i][j]; denom += S[i][j] * S[i][j]; }
+    denom = pow(denom, 2.5) + pow(num, 1.25);
+    num = pow(num, 1.5);
+    mu_t = rho * Cs * Cs * delta * delta * num / (denom + eps);
+  }
+  for (int j = 0; j < D; j++) {
+    f[0 + F * j] = 0.0;
+    f[(F - 1) + F * j] = -1.0 * ph->gamma * mu_t / Pr * de[j];
+    for (int i = 1; i < F - 1; i++) f[i + F * j] = -2.0 * mu_t * S[i - 1][j];
+  }
+}
+
 /* --------------------------------------------------------------- residual */
 
 void or_stage_offsets(const or_mesh* m, long long* off)
 {
   long long E = m->ne, F = m->nfields, D = m->dims, nu = m->nu, nf = m->nf;
-  long long sz[7] = {nf * E * F, nu * E * F * D, nf * E * F * D, nu * E * F * D, nf * E * F, nf * E * F, nf * E * F};
+  long long sz[9] = {nf * E * F, nu * E * F * D, nf * E * F * D, nu * E * F * D, nf * E * F, nf * E * F, nf * E * F,
+                     nu * E * F * D, nf * E * F * D};
   off[0] = 0;
-  for (int i = 0; i < 7; i++) off[i + 1] = off[i] + sz[i];
+  for (int i = 0; i < 9; i++) off[i + 1] = off[i] + sz[i];
 }
 
 void or_residual(or_mesh* m, const or_physics* ph, const double* u, double* div, double* stages)
@@ -920,11 +990,27 @@ void or_residual(or_mesh* m, const or_physics* ph, const double* u, double* div,
         }
         visf(D, ph, q, gq, f);
         const double* J = m->JG + (size_t)D * D * (j + nu * e);
+        if (ph->les) {
+          /* evaluate_viscFlux with LES, src/eles.cpp:2369-2409 */
+          double sf[15];
+          sgsf(D, ph, q, gq, m->detjac[j + nu * e], m->order, sf);
+          for (int k = 0; k < F; k++)
+            for (int l = 0; l < D; l++) f[k + F * l] += sf[k + F * l];
+          for (int k = 0; k < F; k++)
+            for (int l = 0; l < D; l++) {
+              double s = 0.0;
+              for (int mm = 0; mm < D; mm++) s += J[l + D * mm] * sf[k + F * mm];
+              m->sgu[j + nu * (e + E * (k + (size_t)F * l))] = s;
+            }
+        }
         for (int k = 0; k < F; k++)
           for (int l = 0; l < D; l++)
             for (int mm = 0; mm < D; mm++)
               m->tf[j + nu * (e + E * (k + (size_t)F * l))] += J[l + D * mm] * f[k + F * mm];
       }
+    /* evaluate_sgsFlux, src/eles.cpp:3294-3368 */
+    if (ph->les)
+      for (int d = 0; d < D; d++) op_apply(&m->opp0, m->sgu + (size_t)nu * EF * d, m->sgf + (size_t)nf * EF * d, EF, 0);
   }
   /* extrapolate_totalFlux, src/eles.cpp:1423-1512 */
   for (int d = 0; d < D; d++) op_apply(&m->opp1[d], m->tf + (size_t)nu * EF * d, m->ntd, EF, d > 0);
@@ -943,6 +1029,12 @@ void or_residual(or_mesh* m, const or_physics* ph, const double* u, double* div,
         }
       }
       visf(D, ph, ul, gl, fl); visf(D, ph, ur, gr, fr);
+      if (ph->les)      /* src/int_inters.cpp:411-423: the extrapolated SGS flux joins the viscous flux */
+        for (int d = 0; d < D; d++)
+          for (int k = 0; k < F; k++) {
+            fl[k + F * d] += m->sgf[a + (size_t)nf * E * (k + (size_t)F * d)];
+            fr[k + F * d] += m->sgf[b + (size_t)nf * E * (k + (size_t)F * d)];
+          }
       for (int d = 0; d < D; d++) n[d] = m->nrm[a + (size_t)nf * E * d];
       ldg_flux(D, F, ul, ur, fl, fr, n, ph->tau, ph->pen_fact, fn);
       for (int k = 0; k < F; k++) {
@@ -962,6 +1054,10 @@ void or_residual(or_mesh* m, const or_physics* ph, const double* u, double* div,
     memcpy(stages + off[3], m->tf, sizeof(double) * nu * EF * D);
     memcpy(stages + off[4], m->ntd, sizeof(double) * nf * EF);
     memcpy(stages + off[5], m->ntc, sizeof(double) * nf * EF);
+    if (ph->les) {
+      memcpy(stages + off[7], m->sgu, sizeof(double) * nu * EF * D);
+      memcpy(stages + off[8], m->sgf, sizeof(double) * nf * EF * D);
+    }
   }
   /* calculate_corrected_divergence, src/eles.cpp:1594-1661 */
   for (size_t i = 0; i < (size_t)nf * EF; i++) m->ntc[i] += -1.0 * m->ntd[i];

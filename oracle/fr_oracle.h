@@ -30,6 +30,9 @@ typedef struct {
   double gamma, prandtl; /* gas constants                                  */
   double mu_inf, rt_inf, c_sth, fix_vis; /* viscosity law (flux.cpp:326-330) */
   double tau, pen_fact;  /* LDG penalties (inters.cpp:550-678)             */
+  int les;               /* 0 none, 1 eddy-viscosity LES (input key LES)   */
+  int sgs_model;         /* 0 Smagorinsky, 1 WALE (input key SGS_model)    */
+  double filter_ratio;   /* input key filter_ratio                         */
 } or_physics;
 
 /* Generic conforming mesh of one element type (4-node quads or 8-node hexes,
@@ -70,6 +73,10 @@ void or_set_interfaces(or_mesh* m, int n_int_fpts, const int* left_idx, const in
  * Column-major, (rows, cols) returned through shape. */
 int or_get_operator(const or_mesh* m, int which, int dim, double* out, int* shape2);
 
+/* With les != 0 the stage arrays gain sgsf_upts (n_upts, n_eles, F, D) and
+ * sgsf_fpts (n_fpts, n_eles, F, D) at offsets 7 and 8 (or_stage_offsets
+ * then returns 10 offsets). */
+
 /* One evaluation of CalcResidual (src/solver.cpp:65-225):
  * div_tconf_upts = full FR residual (before division by detjac).
  * stages (optional, may be NULL): receives intermediate arrays in this order
@@ -78,7 +85,7 @@ int or_get_operator(const or_mesh* m, int which, int dim, double* out, int* shap
  *   delta_disu_fpts
  * each at the offsets returned by or_stage_offsets. */
 void or_residual(or_mesh* m, const or_physics* ph, const double* u, double* div, double* stages);
-void or_stage_offsets(const or_mesh* m, long long* off8);
+void or_stage_offsets(const or_mesh* m, long long* off10);
 
 /* n_steps low-storage RK45 steps (src/eles.cpp:1091-1188), in place on u
  * (stage register reg must hold zeros on the first call).  If norms != NULL it

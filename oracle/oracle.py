@@ -61,12 +61,14 @@ def lib():
 class Physics(C.Structure):
     _fields_ = [("viscous", C.c_int), ("gamma", C.c_double), ("prandtl", C.c_double),
                 ("mu_inf", C.c_double), ("rt_inf", C.c_double), ("c_sth", C.c_double),
-                ("fix_vis", C.c_double), ("tau", C.c_double), ("pen_fact", C.c_double)]
+                ("fix_vis", C.c_double), ("tau", C.c_double), ("pen_fact", C.c_double),
+                ("les", C.c_int), ("sgs_model", C.c_int), ("filter_ratio", C.c_double)]
 
 
 def physics(viscous=0, gamma=1.4, prandtl=0.72, mu_inf=0.0, rt_inf=1.0, c_sth=1.0, fix_vis=1.0,
-            tau=1.0, pen_fact=0.5):
-    return Physics(int(viscous), gamma, prandtl, mu_inf, rt_inf, c_sth, fix_vis, tau, pen_fact)
+            tau=1.0, pen_fact=0.5, les=0, sgs_model=1, filter_ratio=1.0):
+    return Physics(int(viscous), gamma, prandtl, mu_inf, rt_inf, c_sth, fix_vis, tau, pen_fact, int(les),
+                   int(sgs_model), float(filter_ratio))
 
 
 def _dp(a):
@@ -158,14 +160,15 @@ class Mesh:
         div = np.zeros(self.state_shape(), order="F")
         st = None
         if stages:
-            off = (C.c_longlong * 8)()
+            off = (C.c_longlong * 10)()
             lib().or_stage_offsets(self.h, off)
-            st = np.zeros(off[7], dtype=np.float64)
+            st = np.zeros(off[9], dtype=np.float64)
             lib().or_residual(self.h, C.byref(ph), _dp(u), _dp(div), _dp(st))
             E, nu, nf, F, D = self.n_eles, self.n_upts, self.n_fpts, self.n_fields, self.dims
-            shapes = [(nf, E, F), (nu, E, F, D), (nf, E, F, D), (nu, E, F, D), (nf, E, F), (nf, E, F), (nf, E, F)]
+            shapes = [(nf, E, F), (nu, E, F, D), (nf, E, F, D), (nu, E, F, D), (nf, E, F), (nf, E, F), (nf, E, F),
+                      (nu, E, F, D), (nf, E, F, D)]
             names = ["disu_fpts", "grad_disu_upts", "grad_disu_fpts", "tdisf_upts", "norm_tdisf_fpts",
-                     "norm_tconf_fpts", "delta_disu_fpts"]
+                     "norm_tconf_fpts", "delta_disu_fpts", "sgsf_upts", "sgsf_fpts"]
             st = {n: st[off[i]:off[i + 1]].reshape(s, order="F") for i, (n, s) in enumerate(zip(names, shapes))}
             return div, st
         lib().or_residual(self.h, C.byref(ph), _dp(u), _dp(div), None)

@@ -227,11 +227,14 @@ static void dump_stage(solution& S, const char* tag, const char* what)
     else if (W == "div_tconf_upts") dump(P + W, e->div_tconf_upts(0), 3);
     else if (W == "disu_upts0") dump(P + W, e->disu_upts(0), 3);
     else if (W == "disu_upts1") dump(P + W, e->disu_upts(1), 3);
+    else if (W == "sgsf_upts") dump(P + W, e->sgsf_upts, 4);
+    else if (W == "sgsf_fpts") dump(P + W, e->sgsf_fpts, 4);
   }
 }
 
 // Stage 0 of CalcResidual, operator by operator (src/solver.cpp:65-225 for a
-// single rank with no LES, no shock capturing, no body force, no SA source).
+// single rank with no shock capturing, no body force, no SA source; LES with
+// an eddy-viscosity model, which needs no calc_sgs_terms, src/solver.cpp:72-76).
 static void staged_residual(solution& S)
 {
   int n = S.n_ele_types;
@@ -254,6 +257,11 @@ static void staged_residual(solution& S)
     dump_stage(S, "s06", "grad_disu_fpts");
     for (int i = 0; i < n; i++) S.mesh_eles(i)->evaluate_viscFlux(0);
     dump_stage(S, "s07", "tdisf_upts");
+  }
+  if (run_input.LES) {
+    dump_stage(S, "s07", "sgsf_upts");
+    for (int i = 0; i < n; i++) S.mesh_eles(i)->evaluate_sgsFlux();
+    dump_stage(S, "s07", "sgsf_fpts");
   }
   for (int i = 0; i < n; i++) S.mesh_eles(i)->extrapolate_totalFlux();
   dump_stage(S, "s08", "norm_tdisf_fpts");

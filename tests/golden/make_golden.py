@@ -191,6 +191,13 @@ CASES = [
          ic="tgv_mach01", vcjh=1, jitter=0.0, steps=3, dt=1e-3, stages=False),
     dict(name="hex_euler_p3_n3", dims=3, order=3, n=(3, 3, 3), lo=(0, 0, 0), hi=(2 * np.pi,) * 3, viscous=0,
          ic="tgv_mach01", vcjh=1, jitter=0.0, steps=3, dt=1e-3, stages=True),
+    # eddy-viscosity LES (input keys LES 1, SGS_model 1 = WALE / 0 = Smagorinsky)
+    dict(name="hex_wale_p3_n3_jit", dims=3, order=3, n=(3, 3, 3), lo=(0, 0, 0), hi=(2 * np.pi,) * 3, viscous=1,
+         ic="tgv_mach01", vcjh=1, jitter=0.1, steps=5, dt=1e-3, stages=True, les=1, sgs=1, filter_ratio=1.0),
+    dict(name="hex_smag_p2_n3", dims=3, order=2, n=(3, 3, 3), lo=(0, 0, 0), hi=(2 * np.pi,) * 3, viscous=1,
+         ic="tgv_mach01", vcjh=2, jitter=0.0, steps=3, dt=1e-3, stages=True, les=1, sgs=0, filter_ratio=2.0),
+    dict(name="quad_wale_p3_n6_jit", dims=2, order=3, n=(6, 6), lo=(-5, -5), hi=(5, 5), viscous=1,
+         ic="vortex_u1v0", vcjh=1, jitter=0.15, steps=5, dt=1e-3, stages=True, les=1, sgs=1, filter_ratio=1.0),
 ]
 
 
@@ -211,6 +218,9 @@ def run_case(ref, c, work):
         "prandtl": 0.71, "Mach_free_stream": 0.1, "Re_free_stream": 1600.0, "gamma": 1.4, "fix_vis": 1,
         "res_norm_type": 1,
     }
+    if c.get("les"):
+        vals.update({"LES": 1, "filter_type": 0, "filter_ratio": "%.17g" % c["filter_ratio"],
+                     "SGS_model": c["sgs"], "wall_model": 0, "wall_layer_thickness": 0.0})
     write_input(os.path.join(d, "input"), os.path.join(ref, TGV_INPUT), vals)
     out = os.path.join(d, "out")
     os.makedirs(out, exist_ok=True)
@@ -246,7 +256,8 @@ def main():
         assert dpos < 1e-12, (c["name"], dpos)
         ph = O.physics(viscous=c["viscous"], gamma=par["gamma"], prandtl=par["prandtl"], mu_inf=par["mu_inf"],
                        rt_inf=par["rt_inf"], c_sth=par["c_sth"], fix_vis=par["fix_vis"], tau=par["tau"],
-                       pen_fact=par["pen_fact"])
+                       pen_fact=par["pen_fact"], les=c.get("les", 0), sgs_model=c.get("sgs", 1),
+                       filter_ratio=c.get("filter_ratio", 1.0))
         u0 = arr[T + "disu_upts_init"]
         pins = {}
         pins["metrics_detjac"] = rel(g["detjac_upts"], arr[T + "detjac_upts"])
@@ -276,6 +287,10 @@ def main():
                 fx["grad_disu_upts0"] = arr[T + "s05_grad_disu_upts"]
                 fx["grad_disu_fpts0"] = arr[T + "s06_grad_disu_fpts"]
                 fx["delta_disu_fpts0"] = arr[T + "s04_delta_disu_fpts"]
+            if c.get("les"):
+                pins["sgsf_upts"] = rel(st["sgsf_upts"], arr[T + "s07_sgsf_upts"])
+                pins["sgsf_fpts"] = rel(st["sgsf_fpts"], arr[T + "s07_sgsf_fpts"])
+                fx["sgsf_upts0"] = arr[T + "s07_sgsf_upts"]
         else:
             div = m.residual(ph, u0)
             fx["div0"] = div  # not dumped by the harness in this mode: the pinned oracle's value
@@ -288,6 +303,7 @@ def main():
         meta = {k: (list(v) if isinstance(v, tuple) else v) for k, v in c.items()}
         meta["physics"] = {k: par[k] for k in ("gamma", "prandtl", "mu_inf", "rt_inf", "c_sth", "fix_vis", "tau",
                                                  "pen_fact")}
+        meta["physics"].update(les=c.get("les", 0), sgs_model=c.get("sgs", 1), filter_ratio=c.get("filter_ratio", 1.0))
         meta["pins"] = pins
         meta["seed"] = 12345
         np.savez_compressed(os.path.join(HERE, c["name"] + ".npz"), meta=json.dumps(meta),

@@ -6,8 +6,10 @@ import os
 import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+# eddy-viscosity LES cases (WALE and Smagorinsky SGS flux)
+LES_CASES = ["hex_wale_p3_n3_jit", "hex_smag_p2_n3", "quad_wale_p3_n6_jit"]
 CASES = ["quad_vortex_p3_n6", "quad_vortex_p2_n5_jit", "quad_vortex_p3_n20", "hex_tgv_p3_n3",
-         "hex_tgv_p2_n3_jit", "hex_tgv_p4_n2", "hex_euler_p3_n3"]
+         "hex_tgv_p2_n3_jit", "hex_tgv_p4_n2", "hex_euler_p3_n3"] + LES_CASES
 
 
 def load(name):

@@ -4,8 +4,10 @@ against the reference's regression known-answer values, and against the CPU
 oracle on states the fixtures do not cover.
 
 Tolerance: normwise relative error ||x - x_ref||_2 / ||x_ref||_2 <= 1e-12 for
-one residual evaluation in FP64 (the path contracts products into FMAs and
-splits the correction sum, so it is not bit-identical)."""
+one residual evaluation in FP64.  The inviscid fluxes, their extrapolation,
+divergence and correction round as the reference does; the viscous terms
+(damped by 1/Re) contract products into FMAs, so the path is close to, but
+not, bit-identical."""
 import json
 import os
 
