@@ -1,0 +1,220 @@
+// fr_runner.cuh -- the per-(dims, order, precision) launchers of the fused
+// stage kernels behind fr_solver: compiled tile variants, the kernel-choice
+// state the autotuner sets, and the launch of each stage kernel.  Each
+// (dims, order, precision) runner is compiled in one of the fr_runner_*.cu
+// translation units so the instantiations build in parallel.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "fr_fused.cuh"
+#include "fr_host.hpp"
+
+namespace frb {
+
+// RK45 coefficients (Carpenter-Kennedy low-storage, eles::AdvanceSolution,
+// src/eles.cpp:1093-1113).
+static const double kRK4A[5] = {0.0, -0.417890474499852, -1.192151694642677, -1.697784692471528,
+                                -1.514183444257156};
+static const double kRK4B[5] = {0.149659021999229, 0.379210312999627, 0.822955029386982, 0.699450455949122,
+                                0.153057247968152};
+
+struct Bufs {
+  double *U = nullptr, *REG = nullptr, *DIV = nullptr, *detj64 = nullptr, *partial = nullptr, *norms = nullptr;
+  void *UF[2] = {nullptr, nullptr}, *VF = nullptr, *ND = nullptr, *DV = nullptr, *CF = nullptr, *nL = nullptr,
+       *tdA = nullptr, *JG = nullptr, *detj = nullptr;
+  int2* face = nullptr;
+  unsigned char* fsign = nullptr;
+  long long nint = 0;
+  int* mate = nullptr;
+  unsigned char* side = nullptr;
+};
+
+struct Tile {
+  int epb, nt;
+};
+
+struct Runner {
+  virtual ~Runner() {}
+  virtual void trace(const Bufs& b, int cur, cudaStream_t s) = 0;
+  virtual void grad(const Bufs& b, int cur, cudaStream_t s) = 0;
+  virtual void face(const Bufs& b, int cur, cudaStream_t s) = 0;
+  virtual void update(const Bufs& b, int cur, int mode, int stage, double dt, bool want_partial, cudaStream_t s) = 0;
+  virtual void ke(const Bufs& b, double* partial, int nblk, cudaStream_t s) = 0;
+  virtual int flux_blocks() const = 0;      // blocks of the update kernel (norm partials)
+  virtual int max_flux_blocks() const = 0;  // over all update-kernel tiles
+  virtual int launches_per_stage() const = 0;
+  // tile variants of the two element kernels (autotuning)
+  virtual int n_grad_tiles() const = 0;
+  virtual int n_update_tiles() const = 0;
+  virtual Tile grad_tile(int i) const = 0;
+  virtual Tile update_tile(int i) const = 0;
+  virtual void select(int g, int u) = 0;
+  virtual int grad_sel() const = 0;
+  virtual int update_sel() const = 0;
+};
+
+// Compiled tile variants (elements per CTA, threads per CTA) of the gradient
+// and update kernels per (dims, order); the first entry is the default, the
+// autotuner may pick another.
+template <int DIM, int P> struct Tiles;
+#define FR_TILES(D_, P_, G, U) \
+  template <> struct Tiles<D_, P_> { static constexpr Tile grad[] = G; static constexpr Tile upd[] = U; };
+#define T_(...) {__VA_ARGS__}
+FR_TILES(2, 1, T_({32, 128}), T_({32, 128}))
+FR_TILES(2, 2, T_({16, 128}), T_({16, 128}))
+FR_TILES(2, 3, T_({8, 128}, {4, 64}, {16, 256}), T_({8, 128}, {4, 64}, {16, 256}))
+FR_TILES(2, 4, T_({8, 256}), T_({8, 256}))
+FR_TILES(2, 5, T_({4, 160}), T_({4, 160}))
+FR_TILES(3, 1, T_({12, 128}), T_({12, 128}))
+FR_TILES(3, 2, T_({4, 128}, {2, 64}, {8, 256}), T_({4, 128}, {2, 64}, {8, 256}))
+FR_TILES(3, 3, T_({2, 128}, {1, 64}, {1, 96}, {2, 192}, {4, 256}), T_({2, 128}, {1, 64}, {4, 256}, {2, 96}, {4, 128}))
+FR_TILES(3, 4, T_({1, 128}, {1, 160}, {2, 256}), T_({1, 128}, {2, 256}, {1, 160}))
+#undef T_
+#undef FR_TILES
+
+static void set_smem(const void* k, size_t bytes)
+{
+  if (bytes > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <int DIM, int P, typename TC>
+struct RunnerT : Runner {
+  using S = Shape<DIM, P>;
+  static constexpr int NG = sizeof(Tiles<DIM, P>::grad) / sizeof(Tile);
+  static constexpr int NUP = sizeof(Tiles<DIM, P>::upd) / sizeof(Tile);
+  long long E;
+  int visc, les;
+  int gsel = 0, usel = 0;
+  Line<TC> L;
+  Line<double> L64;
+  PhysT<TC> ph;
+  RunnerT(long long E_, int visc_, int les_, const Line1D& l, const Phys& p) : E(E_), visc(visc_), les(les_)
+  {
+    for (int i = 0; i < kMaxN1; i++) {
+      L.Lm[i] = L.Lp[i] = L.gL[i] = L.gR[i] = L.w[i] = TC(0);
+      for (int j = 0; j < kMaxN1; j++) L.D[i][j] = TC(0);
+    }
+    for (int i = 0; i <= P; i++) {
+      L.Lm[i] = (TC)l.Lm[i]; L.Lp[i] = (TC)l.Lp[i]; L.gL[i] = (TC)l.gL[i]; L.gR[i] = (TC)l.gR[i];
+      L.w[i] = (TC)l.w[i];
+      for (int j = 0; j <= P; j++) L.D[i][j] = (TC)l.D[i][j];
+    }
+    for (int i = 0; i < kMaxN1; i++) {
+      L64.Lm[i] = i <= P ? l.Lm[i] : 0; L64.Lp[i] = i <= P ? l.Lp[i] : 0; L64.gL[i] = i <= P ? l.gL[i] : 0;
+      L64.gR[i] = i <= P ? l.gR[i] : 0; L64.w[i] = i <= P ? l.w[i] : 0;
+      for (int j = 0; j < kMaxN1; j++) L64.D[i][j] = (i <= P && j <= P) ? l.D[i][j] : 0;
+    }
+    ph = PhysT<TC>::make(p);
+  }
+  int n_grad_tiles() const override { return NG; }
+  int n_update_tiles() const override { return NUP; }
+  Tile grad_tile(int i) const override { return Tiles<DIM, P>::grad[i]; }
+  Tile update_tile(int i) const override { return Tiles<DIM, P>::upd[i]; }
+  void select(int g, int u) override { gsel = g; usel = u; }
+  int grad_sel() const override { return gsel; }
+  int update_sel() const override { return usel; }
+  int flux_blocks() const override
+  {
+    int epb = Tiles<DIM, P>::upd[usel].epb;
+    return (int)((E + epb - 1) / epb);
+  }
+  int max_flux_blocks() const override
+  {
+    int m = 1;
+    for (int i = 0; i < NUP; i++) {
+      int b = (int)((E + Tiles<DIM, P>::upd[i].epb - 1) / Tiles<DIM, P>::upd[i].epb);
+      m = b > m ? b : m;
+    }
+    return m;
+  }
+  int launches_per_stage() const override { return visc ? 3 : 2; }
+  void trace(const Bufs& b, int cur, cudaStream_t s) override
+  {
+    long long n = E * S::NF;
+    fr_trace_kernel<DIM, P, TC><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b.U, (TC*)b.UF[cur], E, L);
+  }
+
+  template <int I, int LES>
+  void grad_i(const Bufs& b, int cur, cudaStream_t s)
+  {
+    if constexpr (I < NG) {
+      if (I != gsel) return grad_i<I + 1, LES>(b, cur, s);
+      constexpr int EPB = Tiles<DIM, P>::grad[I].epb, NT = Tiles<DIM, P>::grad[I].nt;
+      constexpr size_t sm = grad_smem_bytes<DIM, P, EPB, TC, LES>();
+      static bool once = (set_smem((const void*)fr_grad_kernel<DIM, P, EPB, NT, TC, LES>, sm), true);
+      (void)once;
+      fr_grad_kernel<DIM, P, EPB, NT, TC, LES><<<(unsigned)((E + EPB - 1) / EPB), NT, sm, s>>>(
+          b.U, (const TC*)b.UF[cur], b.mate, b.side, (const TC*)b.JG, (const TC*)b.detj, (const TC*)b.nL,
+          (TC*)b.VF, (TC*)b.ND, (TC*)b.DV, E, L, ph);
+    }
+  }
+  void grad(const Bufs& b, int cur, cudaStream_t s) override
+  {
+    if (les) grad_i<0, 1>(b, cur, s);
+    else grad_i<0, 0>(b, cur, s);
+  }
+
+  void face(const Bufs& b, int cur, cudaStream_t s) override
+  {
+    if (b.nint == 0) return;
+    unsigned g = (unsigned)((b.nint + 127) / 128);
+    if (visc)
+      fr_face_kernel<DIM, 1, TC><<<g, 128, 0, s>>>(b.face, b.fsign, b.nint, (const TC*)b.UF[cur], (const TC*)b.VF,
+                                                   (const TC*)b.nL, (const TC*)b.tdA, (TC*)b.CF, E * S::NF, ph);
+    else
+      fr_face_kernel<DIM, 0, TC><<<g, 128, 0, s>>>(b.face, b.fsign, b.nint, (const TC*)b.UF[cur], nullptr,
+                                                   (const TC*)b.nL, (const TC*)b.tdA, (TC*)b.CF, E * S::NF, ph);
+  }
+
+  template <int I, int VISC, int MODE>
+  void update_i(const Bufs& b, int cur, int stage, double dt, bool want_partial, cudaStream_t s)
+  {
+    if constexpr (I < NUP) {
+      if (I != usel) return update_i<I + 1, VISC, MODE>(b, cur, stage, dt, want_partial, s);
+      constexpr int EPB = Tiles<DIM, P>::upd[I].epb, NT = Tiles<DIM, P>::upd[I].nt;
+      constexpr size_t sm = update_smem_bytes<DIM, P, EPB, NT, VISC, TC>();
+      static bool once = (set_smem((const void*)fr_update_kernel<DIM, P, EPB, NT, VISC, MODE, TC>, sm), true);
+      (void)once;
+      fr_update_kernel<DIM, P, EPB, NT, VISC, MODE, TC><<<(unsigned)((E + EPB - 1) / EPB), NT, sm, s>>>(
+          b.U, b.REG, (TC*)b.UF[cur ^ 1], (const TC*)b.CF, (const TC*)b.ND, (const TC*)b.DV, (const TC*)b.JG,
+          b.detj64, b.DIV, want_partial ? b.partial : nullptr, E, L, ph, kRK4A[stage], kRK4B[stage], dt,
+          stage == 0 ? 1 : 0);
+    }
+  }
+  void update(const Bufs& b, int cur, int mode, int stage, double dt, bool want_partial, cudaStream_t s) override
+  {
+    if (visc) {
+      if (mode == 0) update_i<0, 1, 0>(b, cur, stage, dt, false, s);
+      else update_i<0, 1, 1>(b, cur, stage, dt, want_partial, s);
+    } else {
+      if (mode == 0) update_i<0, 0, 0>(b, cur, stage, dt, false, s);
+      else update_i<0, 0, 1>(b, cur, stage, dt, want_partial, s);
+    }
+  }
+  void ke(const Bufs& b, double* partial, int nblk, cudaStream_t s) override
+  {
+    fr_ke_kernel<DIM, P><<<nblk, 256, 0, s>>>(b.U, b.detj64, E, L64, partial);
+  }
+};
+
+// One factory per (dims, order, precision), defined by FR_RUNNER in the
+// fr_runner_*.cu translation units.
+#define FR_RUNNER_NAME(D_, P_, T_) make_runner_##D_##_##P_##_##T_
+#define FR_RUNNER(D_, P_, T_)                                                                          \
+  Runner* FR_RUNNER_NAME(D_, P_, T_)(long long E, int visc, int les, const Line1D& l, const Phys& p) \
+  {                                                                                                    \
+    return new RunnerT<D_, P_, T_>(E, visc, les, l, p);                                                \
+  }
+#define FR_RUNNER_DECL(D_, P_, T_) \
+  Runner* FR_RUNNER_NAME(D_, P_, T_)(long long E, int visc, int les, const Line1D& l, const Phys& p);
+FR_RUNNER_DECL(2, 1, double) FR_RUNNER_DECL(2, 2, double) FR_RUNNER_DECL(2, 3, double)
+FR_RUNNER_DECL(2, 4, double) FR_RUNNER_DECL(2, 5, double)
+FR_RUNNER_DECL(3, 1, double) FR_RUNNER_DECL(3, 2, double) FR_RUNNER_DECL(3, 3, double)
+FR_RUNNER_DECL(3, 4, double)
+FR_RUNNER_DECL(2, 1, float) FR_RUNNER_DECL(2, 2, float) FR_RUNNER_DECL(2, 3, float)
+FR_RUNNER_DECL(2, 4, float) FR_RUNNER_DECL(2, 5, float)
+FR_RUNNER_DECL(3, 1, float) FR_RUNNER_DECL(3, 2, float) FR_RUNNER_DECL(3, 3, float)
+FR_RUNNER_DECL(3, 4, float)
+
+}  // namespace frb
