@@ -205,13 +205,9 @@ __device__ __forceinline__ T interp_code(const Line<T>& L, int c, const S* s)
 }
 
 // Dynamic shared-memory sizes of the stage kernels.
+template <int DIM, int P> struct GradPlan;
 template <int DIM, int P, int EPB, typename TC, int LES = 0>
-__host__ __device__ constexpr size_t grad_smem_bytes()
-{
-  using S = Shape<DIM, P>;
-  return blockops_bytes<TC, S::NF>() + sizeof(TC) * EPB * S::F * (S::NU + 2 * S::NF + 2 * DIM * S::NU) +
-         (LES ? sizeof(TC) * EPB * (S::F - 1) * DIM * S::NU : 0);
-}
+__host__ __device__ constexpr size_t grad_smem_bytes();
 template <int DIM, int P, int EPB, int NT, int VISC, typename TC>
 __host__ __device__ constexpr size_t update_smem_bytes()
 {
@@ -244,6 +240,73 @@ __global__ void fr_trace_kernel(const double* __restrict__ U, TC* __restrict__ U
 }
 
 // ---------------------------------------------------------------------------
+// Asynchronous global -> shared copies (cp.async, sm_80 and later; no
+// multicast).  Each thread copies its own elements; cp_async_wait_all plus a
+// block barrier makes them visible to the block.
+template <int N>
+__device__ __forceinline__ void cp_async(void* dst, const void* src)
+{
+  static_assert(N == 4 || N == 8 || N == 16, "cp.async copies 4, 8 or 16 bytes");
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(src), "n"(N) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// N contiguous shared values, 16 bytes per load where N allows (s 16-byte aligned)
+template <int N, typename T>
+__device__ __forceinline__ void lds_line(const T* s, T (&v)[N])
+{
+  if constexpr (sizeof(T) == 8 && N % 2 == 0) {
+#pragma unroll
+    for (int i = 0; i < N; i += 2) {
+      const double2 q = *reinterpret_cast<const double2*>(s + i);
+      v[i] = q.x; v[i + 1] = q.y;
+    }
+  } else if constexpr (sizeof(T) == 4 && N % 4 == 0) {
+#pragma unroll
+    for (int i = 0; i < N; i += 4) {
+      const float4 q = *reinterpret_cast<const float4*>(s + i);
+      v[i] = q.x; v[i + 1] = q.y; v[i + 2] = q.z; v[i + 3] = q.w;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < N; i++) v[i] = s[i];
+  }
+}
+
+// Shared-memory plan of fr_grad_kernel, per element, in units of TC:
+//   sU  [F][NU]      solution
+//   sX  [F][NF]      neighbour traces, then (in place) delta_disu_fpts
+//   sUf [F][NF]      own solution at the flux points
+//   sM  [R3N]        metrics JGinv (NU x D*D, the reference's per-element
+//                    order) and detJ (NU) for the solution-point phase, then
+//                    the left normals [D][NF] for the flux-point phase
+//   sG  [F*D][NU]    physical gradient (component k + F*d)
+//   sFl [D][F][NU]   transformed total flux
+//   sS  [(F-1)*D][NU] transformed SGS flux (LES only)
+// Every region size is rounded up to 4 words, so each region, and each
+// element's block, starts on a 16-byte boundary whatever the point counts.
+template <int DIM, int P>
+struct GradPlan {
+  using S = Shape<DIM, P>;
+  __host__ __device__ static constexpr int r4(int n) { return (n + 3) / 4 * 4; }
+  static constexpr int R3N = (DIM * DIM + 1) * S::NU > DIM * S::NF ? (DIM * DIM + 1) * S::NU : DIM * S::NF;
+  static constexpr int oX = r4(S::F * S::NU);
+  static constexpr int oUf = oX + r4(S::F * S::NF);
+  static constexpr int oM = oUf + r4(S::F * S::NF);
+  static constexpr int oG = oM + r4(R3N);
+  static constexpr int oFl = oG + r4(S::F * DIM * S::NU);
+  static constexpr int oS = oFl + r4(S::F * DIM * S::NU);
+  __host__ __device__ static constexpr int size(int les) { return oS + (les ? r4((S::F - 1) * DIM * S::NU) : 0); }
+};
+
+template <int DIM, int P, int EPB, typename TC, int LES>
+__host__ __device__ constexpr size_t grad_smem_bytes()
+{
+  return blockops_bytes<TC, Shape<DIM, P>::NF>() + sizeof(TC) * EPB * GradPlan<DIM, P>::size(LES);
+}
+
 // Viscous stage, part 1 (per element):
 //   LDG common solution at every own flux point (the delta_disu_fpts of
 //   int_inters::calculate_common_invFlux, src/int_inters.cpp:331-350)
@@ -262,85 +325,96 @@ __global__ void fr_trace_kernel(const double* __restrict__ U, TC* __restrict__ U
 // points (evaluate_sgsFlux, src/eles.cpp:3294-3368) and added there to the
 // physical viscous flux before the projection, as calculate_common_viscFlux
 // adds sgsf_fpts (src/int_inters.cpp:415-427).
+// Inputs reach shared memory through cp.async, so no register holds a
+// prefetched value across the phases; the left normals are fetched while the
+// divergence is computed.  MINB is the CTAs per SM the registers are sized
+// for; VEC = 0 keeps every global read element-sized (inputs only 8-byte
+// aligned), VEC = 1 uses 16-byte copies where the per-element runs allow.
 // Outputs VF (n_fpts, n_eles, F-1), ND (n_fpts, n_eles, F), DV (n_upts, n_eles, F).
-template <int DIM, int P, int EPB, int NT, typename TC, int LES = 0>
-__global__ void __launch_bounds__(NT)
+template <int DIM, int P, int EPB, int NT, typename TC, int LES = 0, int MINB = 1, int VEC = 1>
+__global__ void __launch_bounds__(NT, MINB)
 fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const int* __restrict__ mate,
                const unsigned char* __restrict__ side, const TC* __restrict__ JG, const TC* __restrict__ detj,
                const TC* __restrict__ nL, TC* __restrict__ VF, TC* __restrict__ ND, TC* __restrict__ DV,
                long long E, Line<TC> L, PhysT<TC> ph)
 {
   using S = Shape<DIM, P>;
-  constexpr int NU = S::NU, NF = S::NF, F = S::F, D = DIM;
+  using G = GradPlan<DIM, P>;
+  constexpr int NU = S::NU, NF = S::NF, F = S::F, D = DIM, DD = DIM * DIM;
   constexpr int IF = Items<NT, EPB * NF>::N, IU = Items<NT, EPB * NU>::N;
+  constexpr int PE = G::size(LES);      // shared TC words per element
   extern __shared__ __align__(16) unsigned char fr_smem[];
-  // B: operator pieces and flux-point line table; sU: solution, sX:
-  // delta_disu_fpts, sUf: own solution at the flux points, sG: physical
-  // gradient (component k + F*d), sFl: transformed total flux
   auto B = reinterpret_cast<BlockOps<TC, NF>*>(fr_smem);
-  unsigned char* sm0 = fr_smem + blockops_bytes<TC, NF>();
-  auto sU = reinterpret_cast<TC (*)[F][NU]>(sm0);
-  auto sX = reinterpret_cast<TC (*)[F][NF]>(sm0 + sizeof(TC) * EPB * F * NU);
-  auto sUf = reinterpret_cast<TC (*)[F][NF]>(sm0 + sizeof(TC) * EPB * F * (NU + NF));
-  auto sG = reinterpret_cast<TC (*)[F * D][NU]>(sm0 + sizeof(TC) * EPB * F * (NU + 2 * NF));
-  auto sFl = reinterpret_cast<TC (*)[D][F][NU]>(sm0 + sizeof(TC) * EPB * F * (NU + 2 * NF + D * NU));
-  // sS (LES): transformed SGS flux, component (k - 1) + (F - 1) * l for fields k >= 1
-  auto sS = reinterpret_cast<TC (*)[(F - 1) * D][NU]>(sm0 + sizeof(TC) * EPB * F * (NU + 2 * NF + 2 * D * NU));
+  TC* sm = reinterpret_cast<TC*>(fr_smem + blockops_bytes<TC, NF>());
+#define FR_SU(el, k, u) sm[(el) * PE + (k) * NU + (u)]
+#define FR_SX(el, k, f) sm[(el) * PE + G::oX + (k) * NF + (f)]
+#define FR_SUF(el, k, f) sm[(el) * PE + G::oUf + (k) * NF + (f)]
+#define FR_SM(el, i) sm[(el) * PE + G::oM + (i)]
+#define FR_SG(el, c, u) sm[(el) * PE + G::oG + (c) * NU + (u)]
+#define FR_SFL(el, l, k, u) sm[(el) * PE + G::oFl + ((l) * F + (k)) * NU + (u)]
+#define FR_SS(el, c, u) sm[(el) * PE + G::oS + (c) * NU + (u)]
   fill_blockops<DIM, P, TC, NF>(B, L, threadIdx.x, NT);
   const long long e0 = (long long)blockIdx.x * EPB;
   const long long NFE = (long long)NF * E;
+  const int nval = (int)(E - e0 < EPB ? E - e0 : EPB);
 
-  // --- issue every global gather of the block up front
-  TC pun[IF][F], pn[IF][D];
+  // --- inputs to shared memory: state, metrics, neighbour traces.  16-byte
+  // copies where the per-element runs are whole 16-byte units (global bases
+  // 16-byte aligned), element-sized otherwise.
+  constexpr int VU = (VEC && sizeof(TC) == 8 && NU % 2 == 0) ? 2 : 1;
+  constexpr int VJ = (VEC && (DD * NU * sizeof(TC)) % 16 == 0) ? 16 / sizeof(TC) : 1;
+  constexpr int VD = (VEC && (NU * sizeof(TC)) % 16 == 0) ? 16 / sizeof(TC) : 1;
+  for (int w = threadIdx.x; w < EPB * F * NU / VU; w += NT) {
+    int el = w / (F * NU / VU), r = w * VU - el * F * NU, k = r / NU, u = r - k * NU;
+    if (el < nval) {
+      const double* src = U + u + (size_t)NU * (e0 + el + E * k);
+      if constexpr (sizeof(TC) == 8) cp_async<8 * VU>(&FR_SU(el, k, u), src);
+      else FR_SU(el, k, u) = (TC)*src;
+    } else {
+#pragma unroll
+      for (int v = 0; v < VU; v++) FR_SU(el, k, u + v) = TC(1);
+    }
+  }
+  for (int w = threadIdx.x; w < nval * DD * NU / VJ; w += NT) {
+    int el = (w * VJ) / (DD * NU), r = w * VJ - el * DD * NU;
+    cp_async<sizeof(TC) * VJ>(&FR_SM(el, r), JG + (size_t)DD * NU * e0 + (size_t)w * VJ);
+  }
+  for (int w = threadIdx.x; w < nval * NU / VD; w += NT) {
+    int el = (w * VD) / NU, u = w * VD - el * NU;
+    cp_async<sizeof(TC) * VD>(&FR_SM(el, DD * NU + u), detj + (size_t)NU * e0 + (size_t)w * VD);
+  }
   unsigned char psd[IF];
 #pragma unroll
   for (int it = 0; it < IF; it++) {
     int w = threadIdx.x + it * NT, el = w / NF, f = w - el * NF;
-    long long e = e0 + el;
-    if (w < EPB * NF && e < E) {
-      size_t own = f + (size_t)NF * e;
+    psd[it] = 0;
+    if (w < EPB * NF && el < nval) {
+      size_t own = f + (size_t)NF * (e0 + el);
       int mt = mate[own];
       psd[it] = side[own];
 #pragma unroll
-      for (int k = 0; k < F; k++) pun[it][k] = UF[mt + NFE * k];
-#pragma unroll
-      for (int d = 0; d < D; d++) pn[it][d] = nL[own + NFE * d];
+      for (int k = 0; k < F; k++) cp_async<sizeof(TC)>(&FR_SX(el, k, f), UF + mt + NFE * k);
     }
   }
-  TC pG[IU][D * D], pdj[IU];
-#pragma unroll
-  for (int it = 0; it < IU; it++) {
-    int w = threadIdx.x + it * NT, el = w / NU, u = w - el * NU;
-    long long e = e0 + el;
-    if (w < EPB * NU && e < E) {
-      const TC* G = JG + (size_t)D * D * (u + (size_t)NU * e);
-#pragma unroll
-      for (int q = 0; q < D * D; q++) pG[it][q] = G[q];
-      pdj[it] = detj[u + (size_t)NU * e];
-    }
-  }
-  for (int w = threadIdx.x; w < EPB * F * NU; w += NT) {
-    int el = w / (F * NU), r = w - el * F * NU, k = r / NU, u = r - k * NU;
-    long long e = e0 + el;
-    sU[el][k][u] = e < E ? (TC)U[u + (size_t)NU * (e + E * k)] : TC(1);
-  }
+  cp_async_commit();
+  cp_async_wait_all();
   __syncthreads();
 
-  // --- LDG common solution u_c = (uL+uR)/2 - beta (uL-uR); delta = u_c - u_own
+  // --- LDG common solution u_c = (uL+uR)/2 - beta (uL-uR); delta = u_c - u_own (in place)
 #pragma unroll
   for (int it = 0; it < IF; it++) {
     int w = threadIdx.x + it * NT, el = w / NF, f = w - el * NF;
-    if (w >= EPB * NF || e0 + el >= E) continue;
+    if (w >= EPB * NF || el >= nval) continue;
     TC pen = (psd[it] & 2) ? -ph.pen_fact : ph.pen_fact;
     const int cd = B->code[f];
 #pragma unroll
     for (int k = 0; k < F; k++) {
-      TC uo = interp_code<P, TC, TC>(L, cd, &sU[el][k][0]);
-      TC un = pun[it][k];
+      TC uo = interp_code<P, TC, TC>(L, cd, &FR_SU(el, k, 0));
+      TC un = FR_SX(el, k, f);
       TC ul = (psd[it] & 1) ? uo : un, ur = (psd[it] & 1) ? un : uo;
       TC uc = TC(0.5) * (ul + ur) - pen * (ul - ur);
-      sX[el][k][f] = uc - uo;
-      sUf[el][k][f] = uo;
+      FR_SX(el, k, f) = uc - uo;
+      FR_SUF(el, k, f) = uo;
     }
   }
   __syncthreads();
@@ -349,7 +423,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
 #pragma unroll
   for (int it = 0; it < IU; it++) {
     int w = threadIdx.x + it * NT, el = w / NU, u = w - el * NU;
-    if (w >= EPB * NU || e0 + el >= E) continue;
+    if (w >= EPB * NU || el >= nval) continue;
     int abc[3];
     upt_abc<DIM, P>(u, abc[0], abc[1], abc[2]);
     TC gr[F][D];
@@ -369,45 +443,55 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
 #pragma unroll
       for (int k = 0; k < F; k++) {
         // the gradient only feeds the viscous flux: contracted with FMAs
-        TC acc = sU[el][k][ub] * Dr[0];
+        TC v[P + 1];
+        if (d == 0) lds_line<P + 1, TC>(&FR_SU(el, k, ub), v);
+        else {
 #pragma unroll
-        for (int m = 1; m <= P; m++) acc = fr_fma(sU[el][k][ub + m * st], Dr[m], acc);
-        acc = fr_fma(sX[el][k][qm], gm, acc);
-        acc = fr_fma(sX[el][k][qp], gpl, acc);
+          for (int m = 0; m <= P; m++) v[m] = FR_SU(el, k, ub + m * st);
+        }
+        TC acc = v[0] * Dr[0];
+#pragma unroll
+        for (int m = 1; m <= P; m++) acc = fr_fma(v[m], Dr[m], acc);
+        acc = fr_fma(FR_SX(el, k, qm), gm, acc);
+        acc = fr_fma(FR_SX(el, k, qp), gpl, acc);
         gr[k][d] = acc;
       }
     }
+    TC g[DD];
+#pragma unroll
+    for (int q = 0; q < DD; q++) g[q] = FR_SM(el, DD * u + q);
+    const TC dj = FR_SM(el, DD * NU + u);
     // physical gradient: d/dx_c = sum_r (JGinv(r,c)/detJ) d/dr (src/eles.cpp:1822-1878)
-    TC inv = TC(1.0) / pdj[it];
+    TC inv = TC(1.0) / dj;
     TC gp[F][D];
 #pragma unroll
     for (int c = 0; c < D; c++) {
-      TC m0 = pG[it][0 + D * c] * inv, m1 = pG[it][1 + D * c] * inv, m2 = D == 3 ? pG[it][2 + D * c] * inv : TC(0);
+      TC m0 = g[0 + D * c] * inv, m1 = g[1 + D * c] * inv, m2 = D == 3 ? g[2 + D * c] * inv : TC(0);
 #pragma unroll
       for (int k = 0; k < F; k++) {
         TC acc = fr_fma(gr[k][1], m1, gr[k][0] * m0);
         if (D == 3) acc = fr_fma(gr[k][2], m2, acc);
         gp[k][c] = acc;
-        sG[el][k + F * c][u] = acc;
+        FR_SG(el, k + F * c, u) = acc;
       }
     }
     TC q[F];
 #pragma unroll
-    for (int k = 0; k < F; k++) q[k] = sU[el][k][u];
+    for (int k = 0; k < F; k++) q[k] = FR_SU(el, k, u);
     TC fi[F][D], fv[F][D];
     inv_flux<D, TC>(ph, q, fi);
     vis_flux_fast<D, TC>(ph, q, gp, fv);
     if constexpr (LES != 0) {
       TC fs[F][D];
-      sgs_flux<D, TC>(ph, q, gp, pdj[it], TC(P + 1), fs);
+      sgs_flux<D, TC>(ph, q, gp, dj, TC(P + 1), fs);
 #pragma unroll
       for (int k = 1; k < F; k++)
 #pragma unroll
         for (int l = 0; l < D; l++) {
-          TC a = pG[it][l] * fs[k][0];
+          TC a = g[l] * fs[k][0];
 #pragma unroll
-          for (int m = 1; m < D; m++) a = a + pG[it][l + D * m] * fs[k][m];
-          sS[el][(k - 1) + (F - 1) * l][u] = a;
+          for (int m = 1; m < D; m++) a = a + g[l + D * m] * fs[k][m];
+          FR_SS(el, (k - 1) + (F - 1) * l, u) = a;
           fv[k][l] = fv[k][l] + fs[k][l];
         }
     }
@@ -416,73 +500,28 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
 #pragma unroll
       for (int l = 0; l < D; l++) {
         // inviscid part in the reference's rounding, viscous part added term by term
-        TC acc = pG[it][l] * fi[k][0];
+        TC acc = g[l] * fi[k][0];
 #pragma unroll
-        for (int m = 1; m < D; m++) acc = acc + pG[it][l + D * m] * fi[k][m];
+        for (int m = 1; m < D; m++) acc = acc + g[l + D * m] * fi[k][m];
 #pragma unroll
-        for (int m = 0; m < D; m++) acc = fr_fma(pG[it][l + D * m], fv[k][m], acc);
-        sFl[el][l][k][u] = acc;
+        for (int m = 0; m < D; m++) acc = fr_fma(g[l + D * m], fv[k][m], acc);
+        FR_SFL(el, l, k, u) = acc;
       }
   }
   __syncthreads();
 
-  // --- flux points: own viscous flux projected on the left normal, and the
-  //     discontinuous normal flux
-#pragma unroll
-  for (int it = 0; it < IF; it++) {
-    int w = threadIdx.x + it * NT, el = w / NF, f = w - el * NF;
-    long long e = e0 + el;
-    if (w >= EPB * NF || e >= E) continue;
-    size_t own = f + (size_t)NF * e;
-    TC uf[F], gf[F][D], fv[F][D];
-    const int cd = B->code[f];
-    const int u0 = code_u0(cd), st = code_st(cd), ax = code_ax(cd);
-    const bool plus = code_plus(cd);
-    TC Lc[P + 1];
-#pragma unroll
-    for (int m = 0; m <= P; m++) Lc[m] = plus ? L.Lp[m] : L.Lm[m];
-#pragma unroll
-    for (int k = 0; k < F; k++) {
-      uf[k] = sUf[el][k][f];
-#pragma unroll
-      for (int d = 0; d < D; d++) {
-        const TC* s = &sG[el][k + F * d][0];
-        TC acc = s[u0] * Lc[0];
-#pragma unroll
-        for (int m = 1; m <= P; m++) acc = fr_fma(s[u0 + m * st], Lc[m], acc);
-        gf[k][d] = acc;
-      }
-    }
-    vis_flux_fast<D, TC>(ph, uf, gf, fv);
-    if constexpr (LES != 0) {
-#pragma unroll
-      for (int k = 1; k < F; k++)
-#pragma unroll
-        for (int d = 0; d < D; d++) {
-          const TC* s = &sS[el][(k - 1) + (F - 1) * d][0];
-          TC acc = s[u0] * Lc[0];
-#pragma unroll
-          for (int m = 1; m <= P; m++) acc = fr_fma(s[u0 + m * st], Lc[m], acc);
-          fv[k][d] = fv[k][d] + acc;
-        }
-    }
-#pragma unroll
-    for (int k = 1; k < F; k++) VF[own + NFE * (k - 1)] = project<D, TC>(fv, k, pn[it]);
-#pragma unroll
-    for (int k = 0; k < F; k++) {
-      const TC* s = &sFl[el][ax][k][0];
-      TC v = TC(0);
-#pragma unroll
-      for (int m = 0; m <= P; m++) v = v + s[u0 + m * st] * Lc[m];
-      ND[own + NFE * k] = plus ? v : -v;
-    }
+  // --- left normals into the metric region, fetched while the divergence runs
+  for (int w = threadIdx.x; w < nval * D * NF; w += NT) {
+    int el = w / (D * NF), r = w - el * D * NF, d = r / NF, f = r - d * NF;
+    cp_async<sizeof(TC)>(&FR_SM(el, r), nL + f + (size_t)NF * (e0 + el) + NFE * d);
   }
+  cp_async_commit();
+
   // --- divergence of the total discontinuous flux
 #pragma unroll
   for (int it = 0; it < IU; it++) {
     int w = threadIdx.x + it * NT, el = w / NU, u = w - el * NU;
-    long long e = e0 + el;
-    if (w >= EPB * NU || e >= E) continue;
+    if (w >= EPB * NU || el >= nval) continue;
     int abc[3];
     upt_abc<DIM, P>(u, abc[0], abc[1], abc[2]);
     TC Dm[D][P + 1];
@@ -496,12 +535,80 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
 #pragma unroll
       for (int d = 0; d < D; d++) {
         const int st = upt_stride<DIM, P>(d), ub = u - abc[d] * st;
+        TC v[P + 1];
+        if (d == 0) lds_line<P + 1, TC>(&FR_SFL(el, d, k, ub), v);
+        else {
 #pragma unroll
-        for (int m = 0; m <= P; m++) acc = acc + sFl[el][d][k][ub + m * st] * Dm[d][m];
+          for (int m = 0; m <= P; m++) v[m] = FR_SFL(el, d, k, ub + m * st);
+        }
+#pragma unroll
+        for (int m = 0; m <= P; m++) acc = acc + v[m] * Dm[d][m];
       }
-      DV[u + (size_t)NU * (e + E * k)] = acc;
+      DV[u + (size_t)NU * (e0 + el + E * k)] = acc;
     }
   }
+  cp_async_wait_all();
+  __syncthreads();
+
+  // --- flux points: own viscous flux projected on the left normal, and the
+  //     discontinuous normal flux
+#pragma unroll
+  for (int it = 0; it < IF; it++) {
+    int w = threadIdx.x + it * NT, el = w / NF, f = w - el * NF;
+    if (w >= EPB * NF || el >= nval) continue;
+    size_t own = f + (size_t)NF * (e0 + el);
+    TC uf[F], gf[F][D], fv[F][D], n[D];
+    const int cd = B->code[f];
+    const int u0 = code_u0(cd), st = code_st(cd), ax = code_ax(cd);
+    const bool plus = code_plus(cd);
+    TC Lc[P + 1];
+#pragma unroll
+    for (int m = 0; m <= P; m++) Lc[m] = plus ? L.Lp[m] : L.Lm[m];
+#pragma unroll
+    for (int k = 0; k < F; k++) {
+      uf[k] = FR_SUF(el, k, f);
+#pragma unroll
+      for (int d = 0; d < D; d++) {
+        const TC* s = &FR_SG(el, k + F * d, 0);
+        TC acc = s[u0] * Lc[0];
+#pragma unroll
+        for (int m = 1; m <= P; m++) acc = fr_fma(s[u0 + m * st], Lc[m], acc);
+        gf[k][d] = acc;
+      }
+    }
+    vis_flux_fast<D, TC>(ph, uf, gf, fv);
+    if constexpr (LES != 0) {
+#pragma unroll
+      for (int k = 1; k < F; k++)
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+          const TC* s = &FR_SS(el, (k - 1) + (F - 1) * d, 0);
+          TC acc = s[u0] * Lc[0];
+#pragma unroll
+          for (int m = 1; m <= P; m++) acc = fr_fma(s[u0 + m * st], Lc[m], acc);
+          fv[k][d] = fv[k][d] + acc;
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < D; d++) n[d] = FR_SM(el, d * NF + f);
+#pragma unroll
+    for (int k = 1; k < F; k++) VF[own + NFE * (k - 1)] = project<D, TC>(fv, k, n);
+#pragma unroll
+    for (int k = 0; k < F; k++) {
+      const TC* s = &FR_SFL(el, ax, k, 0);
+      TC v = TC(0);
+#pragma unroll
+      for (int m = 0; m <= P; m++) v = v + s[u0 + m * st] * Lc[m];
+      ND[own + NFE * k] = plus ? v : -v;
+    }
+  }
+#undef FR_SU
+#undef FR_SX
+#undef FR_SUF
+#undef FR_SM
+#undef FR_SG
+#undef FR_SFL
+#undef FR_SS
 }
 
 // ---------------------------------------------------------------------------
@@ -583,6 +690,25 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
   const long long e0 = (long long)blockIdx.x * EPB;
   const long long NFE = (long long)NF * E;
 
+  // per-point inputs of this thread's solution points, requested before the
+  // block-wide loads so that all of them are in flight together
+  constexpr int IU = Items<NT, EPB * NU>::N;
+  TC pdv[IU][F];
+  double preg[IU][F], pdj[IU];
+#pragma unroll
+  for (int it = 0; it < IU; it++) {
+    int w = threadIdx.x + it * NT, el = w / NU, u = w - el * NU;
+    long long e = e0 + el;
+    if (w < EPB * NU && e < E) {
+      if (MODE == 1) pdj[it] = detj[u + (size_t)NU * e];
+#pragma unroll
+      for (int k = 0; k < F; k++) {
+        size_t gi = u + (size_t)NU * (e + E * k);
+        if (VISC) pdv[it][k] = DV[gi];
+        if (MODE == 1) preg[it][k] = first_stage ? 0.0 : REG[gi];
+      }
+    }
+  }
   for (int w = threadIdx.x; w < EPB * F * NU; w += NT) {
     int el = w / (F * NU), r = w - el * F * NU, k = r / NU, u = r - k * NU;
     long long e = e0 + el;
@@ -642,19 +768,19 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
   double red[F];
 #pragma unroll
   for (int k = 0; k < F; k++) red[k] = 0.0;
-  for (int w = threadIdx.x; w < EPB * NU; w += NT) {
-    int el = w / NU, u = w - el * NU;
+#pragma unroll
+  for (int it = 0; it < IU; it++) {
+    int w = threadIdx.x + it * NT, el = w / NU, u = w - el * NU;
     long long e = e0 + el;
-    if (e >= E) continue;
+    if (w >= EPB * NU || e >= E) continue;
     int abc[3];
     upt_abc<DIM, P>(u, abc[0], abc[1], abc[2]);
-    const double dj = detj[u + (size_t)NU * e];
 #pragma unroll
     for (int k = 0; k < F; k++) {
       size_t gi = u + (size_t)NU * (e + E * k);
       TC acc;
       if (VISC) {
-        acc = DV[gi];
+        acc = pdv[it][k];
       } else {
         acc = TC(0);
 #pragma unroll
@@ -676,8 +802,8 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
       if (MODE == 0) {
         DIV[gi] = R;
       } else {
-        double rhs = -R / dj;
-        double res = first_stage ? dt * rhs : rk_a * REG[gi] + dt * rhs;
+        double rhs = -R / pdj[it];
+        double res = first_stage ? dt * rhs : rk_a * preg[it][k] + dt * rhs;
         REG[gi] = res;
         double un = sU[el][k][u] + rk_b * res;
         U[gi] = un;

@@ -124,9 +124,9 @@ fr_status run(const fr_residual_args* a, double* scratch, cudaStream_t s)
   if (visc) {
     constexpr size_t sm = grad_smem_bytes<DIM, P, EPB, double>();
     if (sm > 48 * 1024)
-      cudaFuncSetAttribute(fr_grad_kernel<DIM, P, EPB, NT, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(fr_grad_kernel<DIM, P, EPB, NT, double, 0, 1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)sm);
-    fr_grad_kernel<DIM, P, EPB, NT, double><<<nblk, NT, sm, s>>>(a->disu_upts, UF, a->mate, a->side, a->JGinv_upts,
+    fr_grad_kernel<DIM, P, EPB, NT, double, 0, 1, 0><<<nblk, NT, sm, s>>>(a->disu_upts, UF, a->mate, a->side, a->JGinv_upts,
                                                                   a->detjac_upts, a->norm_left, VF, ND, DV, E, L, ph);
   }
   if (a->n_int > 0) {

@@ -31,7 +31,7 @@ struct Bufs {
 };
 
 struct Tile {
-  int epb, nt;
+  int epb, nt, minb;   // elements per CTA, threads per CTA, CTAs per SM the registers are sized for (0: any)
 };
 
 struct Runner {
@@ -68,7 +68,7 @@ FR_TILES(2, 4, T_({8, 256}), T_({8, 256}))
 FR_TILES(2, 5, T_({4, 160}), T_({4, 160}))
 FR_TILES(3, 1, T_({12, 128}), T_({12, 128}))
 FR_TILES(3, 2, T_({4, 128}, {2, 64}, {8, 256}), T_({4, 128}, {2, 64}, {8, 256}))
-FR_TILES(3, 3, T_({2, 128}, {1, 64}, {1, 96}, {2, 192}, {4, 256}), T_({2, 128}, {1, 64}, {4, 256}, {2, 96}, {4, 128}))
+FR_TILES(3, 3, T_({2, 128, 4}, {1, 64, 8}, {2, 192, 2}, {2, 128, 3}, {1, 96, 0}, {4, 256, 2}), T_({2, 128}, {1, 64}, {4, 256}, {2, 96}, {4, 128}))
 FR_TILES(3, 4, T_({1, 128}, {1, 160}, {2, 256}), T_({1, 128}, {2, 256}, {1, 160}))
 #undef T_
 #undef FR_TILES
@@ -141,10 +141,11 @@ struct RunnerT : Runner {
     if constexpr (I < NG) {
       if (I != gsel) return grad_i<I + 1, LES>(b, cur, s);
       constexpr int EPB = Tiles<DIM, P>::grad[I].epb, NT = Tiles<DIM, P>::grad[I].nt;
+      constexpr int MINB = Tiles<DIM, P>::grad[I].minb > 0 ? Tiles<DIM, P>::grad[I].minb : 1;
       constexpr size_t sm = grad_smem_bytes<DIM, P, EPB, TC, LES>();
-      static bool once = (set_smem((const void*)fr_grad_kernel<DIM, P, EPB, NT, TC, LES>, sm), true);
+      static bool once = (set_smem((const void*)fr_grad_kernel<DIM, P, EPB, NT, TC, LES, MINB>, sm), true);
       (void)once;
-      fr_grad_kernel<DIM, P, EPB, NT, TC, LES><<<(unsigned)((E + EPB - 1) / EPB), NT, sm, s>>>(
+      fr_grad_kernel<DIM, P, EPB, NT, TC, LES, MINB><<<(unsigned)((E + EPB - 1) / EPB), NT, sm, s>>>(
           b.U, (const TC*)b.UF[cur], b.mate, b.side, (const TC*)b.JG, (const TC*)b.detj, (const TC*)b.nL,
           (TC*)b.VF, (TC*)b.ND, (TC*)b.DV, E, L, ph);
     }
