@@ -330,13 +330,15 @@ __host__ __device__ constexpr size_t grad_smem_bytes()
 // divergence is computed.  MINB is the CTAs per SM the registers are sized
 // for; VEC = 0 keeps every global read element-sized (inputs only 8-byte
 // aligned), VEC = 1 uses 16-byte copies where the per-element runs allow.
-// Outputs VF (n_fpts, n_eles, F-1), ND (n_fpts, n_eles, F), DV (n_upts, n_eles, F).
+// Outputs VF (n_fpts, n_eles, F-1), ND (n_fpts, n_eles, F), DV (n_upts, n_eles, F),
+// and, when GRAD is not null, the corrected physical gradient
+// grad_disu_upts (n_upts, n_eles, F, D).
 template <int DIM, int P, int EPB, int NT, typename TC, int LES = 0, int MINB = 1, int VEC = 1>
 __global__ void __launch_bounds__(NT, MINB)
 fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const int* __restrict__ mate,
                const unsigned char* __restrict__ side, const TC* __restrict__ JG, const TC* __restrict__ detj,
                const TC* __restrict__ nL, TC* __restrict__ VF, TC* __restrict__ ND, TC* __restrict__ DV,
-               long long E, Line<TC> L, PhysT<TC> ph)
+               long long E, Line<TC> L, PhysT<TC> ph, TC* __restrict__ GRAD)
 {
   using S = Shape<DIM, P>;
   using G = GradPlan<DIM, P>;
@@ -473,6 +475,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
         if (D == 3) acc = fr_fma(gr[k][2], m2, acc);
         gp[k][c] = acc;
         FR_SG(el, k + F * c, u) = acc;
+        if (GRAD) GRAD[u + (size_t)NU * (e0 + el + E * (k + (long long)F * c))] = acc;
       }
     }
     TC q[F];

@@ -14,23 +14,28 @@
 
 #include <cuda_runtime.h>
 
+#include "fr_mlp.cuh"
+
 namespace frb {
 
 struct Phys {
   double gamma, prandtl, mu_inf, rt_inf, c_sth, fix_vis, tau, pen_fact;
-  int sgs_model = 1;          // eddy-viscosity LES: 0 Smagorinsky, 1 WALE
+  int sgs_model = 1;          // eddy-viscosity LES: 0 Smagorinsky, 1 WALE, 5 learned (fr_mlp.cuh)
   double filter_ratio = 1.0;  // LES filter width over the element's point spacing
+  const float* mlp = nullptr; // device parameters of the learned closure (sgs_model 5)
 };
 
 template <typename T>
 struct PhysT {
   T gamma, gm1, prandtl, mu_inf, rt_inf, c_sth, fix_vis, tau, pen_fact, filter_ratio;
   int sgs_model;
+  const float* mlp;
   __host__ __device__ static PhysT make(const Phys& p) {
     PhysT q;
     q.gamma = (T)p.gamma; q.gm1 = (T)(p.gamma - 1.0); q.prandtl = (T)p.prandtl; q.mu_inf = (T)p.mu_inf;
     q.rt_inf = (T)p.rt_inf; q.c_sth = (T)p.c_sth; q.fix_vis = (T)p.fix_vis; q.tau = (T)p.tau;
     q.pen_fact = (T)p.pen_fact; q.filter_ratio = (T)p.filter_ratio; q.sgs_model = p.sgs_model;
+    q.mlp = p.mlp;
     return q;
   }
 };
@@ -284,6 +289,7 @@ __device__ __forceinline__ void ldg_flux(const PhysT<T>& ph, T pen, const T* ul,
 // WALE, Cw = 0.5; no wall model; src/eles.cpp:2456-2778), physical
 // components fs[k][l].  g is the physical gradient g[k][l] = d q_k / d x_l,
 // detjac the Jacobian determinant at the point, n1 = order + 1.
+// sgs_model 5 is the learned closure of fr_mlp.cuh (no reference counterpart).
 //
 // Two index choices of the reference are kept as it evaluates them: its
 // "velocity" vector is u_i = q_i / rho for i < D, so u_0 = rho / rho
@@ -298,6 +304,10 @@ template <int D, typename T>
 __device__ __forceinline__ void sgs_flux(const PhysT<T>& ph, const T* q, const T (*g)[D], T detjac, T n1,
                                          T (*fs)[D])
 {
+  if (ph.sgs_model == 5) {
+    sgs_flux_learned<D, T>(ph.mlp, ph.gamma, q, g, detjac, n1, ph.filter_ratio, fs);
+    return;
+  }
   constexpr int F = D + 2;
   const T rho = q[0];
   T u[D], ke = T(0);

@@ -22,7 +22,7 @@ static const double kRK4B[5] = {0.149659021999229, 0.379210312999627, 0.82295502
 struct Bufs {
   double *U = nullptr, *REG = nullptr, *DIV = nullptr, *detj64 = nullptr, *partial = nullptr, *norms = nullptr;
   void *UF[2] = {nullptr, nullptr}, *VF = nullptr, *ND = nullptr, *DV = nullptr, *CF = nullptr, *nL = nullptr,
-       *tdA = nullptr, *JG = nullptr, *detj = nullptr;
+       *tdA = nullptr, *JG = nullptr, *detj = nullptr, *GRAD = nullptr;
   int2* face = nullptr;
   unsigned char* fsign = nullptr;
   long long nint = 0;
@@ -147,7 +147,7 @@ struct RunnerT : Runner {
       (void)once;
       fr_grad_kernel<DIM, P, EPB, NT, TC, LES, MINB><<<(unsigned)((E + EPB - 1) / EPB), NT, sm, s>>>(
           b.U, (const TC*)b.UF[cur], b.mate, b.side, (const TC*)b.JG, (const TC*)b.detj, (const TC*)b.nL,
-          (TC*)b.VF, (TC*)b.ND, (TC*)b.DV, E, L, ph);
+          (TC*)b.VF, (TC*)b.ND, (TC*)b.DV, E, L, ph, (TC*)b.GRAD);
     }
   }
   void grad(const Bufs& b, int cur, cudaStream_t s) override

@@ -17,6 +17,10 @@ namespace frb {
 
 thread_local std::string g_err;
 
+cudaError_t launch_sgs_inputs(int dims, int tc_size, const double* U, const void* G, const double* detj, long long npts,
+                              int nu, long long E, int order, double filter_ratio, float* X, cudaStream_t st);
+void mlp_default_params(float* w);
+
 static fr_status fail(fr_status s, const std::string& msg)
 {
   g_err = msg;
@@ -63,6 +67,9 @@ struct fr_solver {
   int nblk_ke = 0;
   double* ke_partial = nullptr;
   double* ke_out = nullptr;
+  float* mlp = nullptr;             // learned-closure parameters (sgs_model 5)
+  void* grad_buf = nullptr;         // gradient output of fr_solver_gradient (allocated on first use)
+  float* feat_buf = nullptr;        // closure inputs of fr_solver_sgs_features (allocated on first use)
   std::vector<void*> allocs;
 };
 
@@ -180,8 +187,9 @@ fr_status fr_solver_create(const fr_mesh_desc* md, const fr_scheme_desc* sd, int
   if (sd->upts_type != 0) return fail(FR_ERR_UNSUPPORTED, "fused kernels need Gauss solution points");
   if (sd->les != 0) {
     if (sd->les != 1 || !sd->viscous) return fail(FR_ERR_ARG, "les must be 0 or 1, and 1 needs viscous = 1");
-    if (sd->sgs_model != 0 && sd->sgs_model != 1)
-      return fail(FR_ERR_UNSUPPORTED, "only the eddy-viscosity SGS models 0 (Smagorinsky) and 1 (WALE) are built");
+    if (sd->sgs_model != 0 && sd->sgs_model != 1 && sd->sgs_model != 5)
+      return fail(FR_ERR_UNSUPPORTED,
+                  "SGS models built: 0 (Smagorinsky), 1 (WALE) and 5 (learned); the filter-based models are not");
     if (!(sd->filter_ratio > 0.0)) return fail(FR_ERR_ARG, "filter_ratio must be positive");
   }
   std::unique_ptr<fr_solver> s(new fr_solver());
@@ -193,8 +201,16 @@ fr_status fr_solver_create(const fr_mesh_desc* md, const fr_scheme_desc* sd, int
   if (!build_mesh(md->dims, s->line, md->n_verts, md->xv, md->n_eles, md->c2v, md->shift, s->mesh, err))
     return fail(FR_ERR_MESH, err);
   FR_CUDA(cudaSetDevice(device));
+  if (sd->les && sd->sgs_model == 5) {
+    // the learned closure starts switched off (c ~ 2e-9) until parameters are set
+    fr_status st0 = dalloc(s.get(), &s->mlp, (size_t)kMlpN);
+    if (st0) return st0;
+    std::vector<float> w0(kMlpN);
+    mlp_default_params(w0.data());
+    FR_CUDA(cudaMemcpy(s->mlp, w0.data(), sizeof(float) * kMlpN, cudaMemcpyHostToDevice));
+  }
   Phys ph{sd->gamma, sd->prandtl, sd->mu_inf, sd->rt_inf, sd->c_sth, sd->fix_vis, sd->tau, sd->pen_fact,
-          sd->sgs_model, sd->filter_ratio};
+          sd->sgs_model, sd->filter_ratio, s->mlp};
   const int les = sd->les;
   Runner* r = make_runner(md->dims, sd->order, (int)s->tc_size, md->n_eles, sd->viscous, les, s->line, ph);
   if (!r) return fail(FR_ERR_UNSUPPORTED, "no kernel for this (dims, order)");
@@ -561,3 +577,69 @@ fr_status fr_solver_sync(fr_solver* s)
 }
 
 }  // extern "C"
+
+fr_status fr_solver_gradient(fr_solver* s, double* host_grad, void* stream)
+{
+  if (!s || !host_grad) return fail(FR_ERR_ARG, "null argument");
+  if (!s->sch.viscous) return fail(FR_ERR_UNSUPPORTED, "the gradient is evaluated on the viscous path only");
+  FR_CUDA(cudaSetDevice(s->device));
+  cudaStream_t st = STRM(s, stream);
+  const Mesh& m = s->mesh;
+  const size_t n = (size_t)m.nu * m.ne * m.nfields * m.dims;
+  if (!s->grad_buf) {
+    char* p;
+    fr_status r = dalloc(s, &p, n * s->tc_size);
+    if (r) return r;
+    s->grad_buf = p;
+  }
+  Bufs b = s->b;
+  b.GRAD = s->grad_buf;
+  s->run->grad(b, s->cur, st);
+  s->launches++;
+  fr_status r = check_launch("fr gradient kernel");
+  if (r) return r;
+  if (s->tc_size == 8) {
+    FR_CUDA(cudaMemcpyAsync(host_grad, s->grad_buf, n * 8, cudaMemcpyDeviceToHost, st));
+    FR_CUDA(cudaStreamSynchronize(st));
+  } else {
+    std::vector<float> f(n);
+    FR_CUDA(cudaMemcpyAsync(f.data(), s->grad_buf, n * 4, cudaMemcpyDeviceToHost, st));
+    FR_CUDA(cudaStreamSynchronize(st));
+    for (size_t i = 0; i < n; i++) host_grad[i] = f[i];
+  }
+  return FR_OK;
+}
+
+fr_status fr_solver_sgs_features(fr_solver* s, float* host_x, void* stream)
+{
+  if (!s || !host_x) return fail(FR_ERR_ARG, "null argument");
+  if (!s->sch.viscous) return fail(FR_ERR_UNSUPPORTED, "the closure inputs need the viscous path");
+  const Mesh& m = s->mesh;
+  const size_t npts = (size_t)m.nu * m.ne;
+  std::vector<double> tmp((size_t)npts * m.nfields * m.dims);
+  fr_status r = fr_solver_gradient(s, tmp.data(), stream);   // leaves the gradient in grad_buf
+  if (r) return r;
+  cudaStream_t st = STRM(s, stream);
+  if (!s->feat_buf) {
+    r = dalloc(s, &s->feat_buf, npts * kMlpIn);
+    if (r) return r;
+  }
+  const double fr = s->sch.les ? s->sch.filter_ratio : 1.0;
+  FR_CUDA(launch_sgs_inputs(m.dims, (int)s->tc_size, s->b.U, s->grad_buf, s->b.detj64, (long long)npts, m.nu,
+                            (long long)m.ne, s->sch.order, fr, s->feat_buf, st));
+  s->launches++;
+  FR_CUDA(cudaMemcpyAsync(host_x, s->feat_buf, npts * kMlpIn * sizeof(float), cudaMemcpyDeviceToHost, st));
+  FR_CUDA(cudaStreamSynchronize(st));
+  return FR_OK;
+}
+
+fr_status fr_solver_set_sgs_mlp(fr_solver* s, const float* host_w)
+{
+  if (!s || !host_w) return fail(FR_ERR_ARG, "null argument");
+  if (!s->mlp) return fail(FR_ERR_ARG, "the solver was not created with les = 1, sgs_model = 5");
+  for (int p = 0; p < kMlpN; p++)
+    if (!std::isfinite(host_w[p])) return fail(FR_ERR_NONFINITE, "non-finite closure parameter");
+  FR_CUDA(cudaSetDevice(s->device));
+  FR_CUDA(cudaMemcpy(s->mlp, host_w, sizeof(float) * kMlpN, cudaMemcpyHostToDevice));
+  return FR_OK;
+}

@@ -78,6 +78,15 @@ def lib():
         "fr_solver_autotune": (C.c_int, [vp, C.c_int, ip]),
         "fr_mesh_geometry": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(SchemeDesc), ip, dp, dp, dp, dp, dp, ip, ip]),
         "fr_line_operators": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, dp]),
+        "fr_solver_gradient": (C.c_int, [vp, dp, vp]),
+        "fr_solver_sgs_features": (C.c_int, [vp, C.POINTER(C.c_float), vp]),
+        "fr_solver_set_sgs_mlp": (C.c_int, [vp, C.POINTER(C.c_float)]),
+        "fr_mlp_n_params": (C.c_int, []),
+        "fr_mlp_n_trained": (C.c_int, []),
+        "fr_mlp_scratch_floats": (C.c_longlong, [C.c_longlong]),
+        "fr_mlp_forward": (C.c_int, [vp, vp, C.c_longlong, vp, vp]),
+        "fr_mlp_loss_grad": (C.c_int, [vp, vp, vp, C.c_longlong, vp, vp, vp, C.c_longlong, vp]),
+        "fr_mlp_adam": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_float, vp]),
     }
     for name, (res, args) in sigs.items():
         f = getattr(L, name)
@@ -277,6 +286,25 @@ class Solver:
         _check(lib().fr_solver_advance(self.h, int(n_steps), float(dt), _dp(out) if norms else None, stream))
         return out
 
+    def gradient(self, stream=None):
+        """Corrected physical gradient grad_disu_upts (n_upts, n_eles, n_fields, n_dims)."""
+        g = np.zeros((self.n_upts, self.n_eles, self.n_fields, self.dims), order="F")
+        _check(lib().fr_solver_gradient(self.h, _dp(g), stream))
+        return g
+
+    def sgs_features(self, stream=None):
+        """Inputs of the learned closure at every solution point, (n_upts * n_eles, 6) float32."""
+        x = np.zeros((self.n_upts * self.n_eles, 6), dtype=np.float32)
+        _check(lib().fr_solver_sgs_features(self.h, x.ctypes.data_as(C.POINTER(C.c_float)), stream))
+        return x
+
+    def set_sgs_mlp(self, w):
+        """Parameters of the learned closure (solvers made with les=1, sgs_model=5)."""
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        if w.size != mlp_n_params():
+            raise ValueError("expected %d parameters" % mlp_n_params())
+        _check(lib().fr_solver_set_sgs_mlp(self.h, w.ctypes.data_as(C.POINTER(C.c_float))))
+
     def kinetic_energy(self, stream=None):
         v = C.c_double()
         _check(lib().fr_solver_kinetic_energy(self.h, C.byref(v), stream))
@@ -302,3 +330,30 @@ class Solver:
         out = np.zeros(3)
         _check(lib().fr_solver_profile_stage(self.h, int(reps), float(dt), _dp(out)))
         return tuple(out)
+
+
+# ---------------------------------------------------------------- learned closure kernels
+# Device arrays are passed as integer addresses (e.g. torch's data_ptr()).
+
+def mlp_n_params():
+    return int(lib().fr_mlp_n_params())
+
+
+def mlp_n_trained():
+    return int(lib().fr_mlp_n_trained())
+
+
+def mlp_scratch_floats(n):
+    return int(lib().fr_mlp_scratch_floats(int(n)))
+
+
+def mlp_forward(d_w, d_x, n, d_out, stream=None):
+    _check(lib().fr_mlp_forward(d_w, d_x, int(n), d_out, stream))
+
+
+def mlp_loss_grad(d_w, d_x, d_y, n, d_grad, d_loss, d_scratch, scratch_floats, stream=None):
+    _check(lib().fr_mlp_loss_grad(d_w, d_x, d_y, int(n), d_grad, d_loss, d_scratch, int(scratch_floats), stream))
+
+
+def mlp_adam(d_w, d_grad, d_m, d_v, step, lr, stream=None):
+    _check(lib().fr_mlp_adam(d_w, d_grad, d_m, d_v, int(step), float(lr), stream))

@@ -75,8 +75,9 @@ typedef struct {
   int les;               /* 1 adds the eddy-viscosity SGS flux (input key LES;
                             viscous only; eles::calc_sgsf_upts,
                             src/eles.cpp:2456-2778); 0 none                    */
-  int sgs_model;         /* with les: 0 Smagorinsky, 1 WALE (SGS_model); the
-                            filter-based models 2-4 are not built             */
+  int sgs_model;         /* with les: 0 Smagorinsky, 1 WALE (SGS_model), 5 the
+                            learned closure below; the filter-based models
+                            2-4 are not built                                 */
   double filter_ratio;   /* with les: filter width over the point spacing     */
 } fr_scheme_desc;
 
@@ -144,6 +145,43 @@ fr_status fr_solver_autotune(fr_solver* s, int reps, int out4[4]);
  * kernels: gradient/flux (0 for inviscid runs), interface fluxes, and
  * correction + update.  For roofline accounting. */
 fr_status fr_solver_profile_stage(fr_solver* s, int reps, double dt, double* ms3);
+
+/* Corrected physical gradient of the current state, grad_disu_upts after
+ * eles::correct_gradient (src/eles.cpp:1770-1968), to host memory in the
+ * layout (n_upts, n_eles, n_fields, n_dims).  Viscous solvers only. */
+fr_status fr_solver_gradient(fr_solver* s, double* host_grad, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Learned SGS closure (sgs_model 5).  No counterpart in the reference, whose
+ * eddy-viscosity models are Smagorinsky and WALE (eles::calc_sgsf_upts,
+ * src/eles.cpp:2456-2778); it uses the same flux with
+ * mu_t = rho Delta^2 |S| c, where c >= 0 comes from a 6-64-64-1 perceptron
+ * (tanh, tanh, softplus; FP32) of five invariants of the resolved velocity
+ * gradient and log Delta.  Parameter vector: W1[64][6], b1[64], W2[64][64],
+ * b2[64], w3[64], b3 (trained), then xmean[6], xscale[6] (input
+ * normalisation (x - xmean) * xscale).
+ * ---------------------------------------------------------------------- */
+int fr_mlp_n_params(void);       /* 4685 floats in all */
+int fr_mlp_n_trained(void);      /* 4673 trained ones (the leading part) */
+
+/* Closure inputs at every solution point of the current state, host memory
+ * (n_upts * n_eles, 6) floats, point index upt + n_upts * ele. */
+fr_status fr_solver_sgs_features(fr_solver* s, float* host_x, void* stream);
+/* Copies a parameter vector into a solver created with les = 1,
+ * sgs_model = 5 (such a solver starts with the closure off, c ~ 2e-9). */
+fr_status fr_solver_set_sgs_mlp(fr_solver* s, const float* host_w);
+
+/* Training kernels on device arrays: x (n, 6), c* = y (n), w, grad, m, v
+ * (fr_mlp_n_params() / fr_mlp_n_trained() floats).  loss_grad gives the
+ * gradient of (1/n) sum (c(x) - y)^2 over the trained parameters and the
+ * loss; it needs fr_mlp_scratch_floats(n) floats of caller scratch and is
+ * deterministic.  adam applies one Adam step (beta 0.9 / 0.999, eps 1e-8;
+ * step counts from 1). */
+long long fr_mlp_scratch_floats(long long n);
+fr_status fr_mlp_forward(const float* d_w, const float* d_x, long long n, float* d_out, void* stream);
+fr_status fr_mlp_loss_grad(const float* d_w, const float* d_x, const float* d_y, long long n, float* d_grad,
+                           float* d_loss, float* d_scratch, long long scratch_floats, void* stream);
+fr_status fr_mlp_adam(float* d_w, const float* d_grad, float* d_m, float* d_v, int step, float lr, void* stream);
 
 /* ------------------------------------------------------------------------
  * Host-only set-up queries (no GPU is touched).

@@ -828,6 +828,85 @@ static void ldg_flux(int D, int F, const double* ul, const double* ur, const dou
   }
 }
 
+/* Learned closure (sgs_model 5; no reference counterpart): a 6-64-64-1
+ * perceptron, tanh/tanh/softplus, in float, gives c >= 0 of
+ * mu_t = rho Delta^2 |S| c from the invariants of the resolved velocity
+ * gradient (A_ij = d u_i / d x_j, S its deviatoric symmetric part, W its
+ * antisymmetric part, a2 = sum A_ij^2):
+ *   x = (tr S^2/a2, tr W^2/a2, tr S^3/a2^1.5, tr S W^2/a2^1.5, tr S^2 W^2/a2^2, log Delta).
+ * Parameter layout: W1[64][6] b1[64] W2[64][64] b2[64] w3[64] b3 xmean[6] xscale[6]. */
+enum { MLP_IN = 6, MLP_H = 64, MLP_W1 = 0, MLP_B1 = 384, MLP_W2 = 448, MLP_B2 = 4544, MLP_W3 = 4608,
+       MLP_B3 = 4672, MLP_XM = 4673, MLP_XS = 4679 };
+
+static float mlp_eval_c(const float* w, const float* xr)
+{
+  float x[MLP_IN], h1[MLP_H];
+  for (int k = 0; k < MLP_IN; k++) x[k] = (xr[k] - w[MLP_XM + k]) * w[MLP_XS + k];
+  for (int i = 0; i < MLP_H; i++) {
+    float a = w[MLP_B1 + i];
+    for (int k = 0; k < MLP_IN; k++) a = fmaf(w[MLP_W1 + i * MLP_IN + k], x[k], a);
+    h1[i] = tanhf(a);
+  }
+  float o = w[MLP_B3];
+  for (int j = 0; j < MLP_H; j++) {
+    float a = w[MLP_B2 + j];
+    for (int i = 0; i < MLP_H; i++) a = fmaf(w[MLP_W2 + j * MLP_H + i], h1[i], a);
+    o = fmaf(w[MLP_W3 + j], tanhf(a), o);
+  }
+  return o > 20.f ? o : log1pf(expf(o));
+}
+
+static void sgsf_learned(int D, const or_physics* ph, const double* q, const double* g, double detjac, int order,
+                         double* f)
+{
+  int F = D + 2;
+  double rho = q[0], u[3], ke = 0.0, A[3][3], S[3][3], W[3][3], de[3], tr = 0.0, a2 = 0.0;
+  for (int i = 0; i < D; i++) { u[i] = q[i + 1] / rho; ke = ke + 0.5 * u[i] * u[i]; }
+  double inte = q[F - 1] / rho - ke;
+  for (int i = 0; i < D; i++)
+    for (int j = 0; j < D; j++) A[i][j] = (g[(i + 1) + F * j] - u[i] * g[0 + F * j]) / rho;
+  for (int j = 0; j < D; j++) {
+    double ud = 0.0;
+    for (int i = 0; i < D; i++) ud = ud + u[i] * A[i][j];
+    de[j] = (g[(F - 1) + F * j] - ke * g[0 + F * j] - rho * ud - g[0 + F * j] * inte) / rho;
+  }
+  for (int i = 0; i < D; i++) tr = tr + A[i][i];
+  for (int i = 0; i < D; i++)
+    for (int j = 0; j < D; j++) {
+      S[i][j] = 0.5 * (A[i][j] + A[j][i]) - (i == j ? tr / 3.0 : 0.0);
+      W[i][j] = 0.5 * (A[i][j] - A[j][i]);
+      a2 = a2 + A[i][j] * A[i][j];
+    }
+  a2 = a2 + 1e-30;
+  double S2[3][3], W2[3][3], trS2 = 0, trW2 = 0, trS3 = 0, trSW2 = 0, trS2W2 = 0;
+  for (int i = 0; i < D; i++)
+    for (int j = 0; j < D; j++) {
+      double s = 0, w = 0;
+      for (int k = 0; k < D; k++) { s = s + S[i][k] * S[k][j]; w = w + W[i][k] * W[k][j]; }
+      S2[i][j] = s; W2[i][j] = w;
+    }
+  for (int i = 0; i < D; i++)
+    for (int j = 0; j < D; j++) {
+      trS2 = trS2 + S[i][j] * S[j][i];
+      trW2 = trW2 + W[i][j] * W[j][i];
+      trS3 = trS3 + S2[i][j] * S[j][i];
+      trSW2 = trSW2 + S[i][j] * W2[j][i];
+      trS2W2 = trS2W2 + S2[i][j] * W2[j][i];
+    }
+  double ra = 1.0 / a2, ra15 = ra / sqrt(a2);
+  double vol = detjac * (D == 3 ? 8. : 4.);
+  double delta = ph->filter_ratio * (D == 3 ? cbrt(vol) : sqrt(vol)) / (order + 1.);
+  float x[MLP_IN] = {(float)(trS2 * ra), (float)(trW2 * ra), (float)(trS3 * ra15), (float)(trSW2 * ra15),
+                     (float)(trS2W2 * ra * ra), (float)log(delta)};
+  double c = (double)mlp_eval_c(ph->mlp, x);
+  double mu_t = rho * delta * delta * sqrt(2.0 * trS2) * c;
+  for (int j = 0; j < D; j++) {
+    f[0 + F * j] = 0.0;
+    f[(F - 1) + F * j] = -ph->gamma * mu_t / 0.5 * de[j];
+    for (int i = 1; i < F - 1; i++) f[i + F * j] = -2.0 * mu_t * S[i - 1][j];
+  }
+}
+
 /* Eddy-viscosity SGS flux at a solution point: eles::calc_sgsf_upts for
  * sgs_model 0 (Smagorinsky) and 1 (WALE) without a wall model,
  * src/eles.cpp:2456-2778.  Kept as the reference computes it, including two
@@ -838,6 +917,10 @@ static void ldg_flux(int D, int F, const double* ul, const double* ur, const dou
 static void sgsf(int D, const or_physics* ph, const double* u, const double* gu /* (F,D) [k+F*l] */, double detjac,
                  int order, double* f /* (F,D) */)
 {
+  if (ph->sgs_model == 5) {
+    sgsf_learned(D, ph, u, gu, detjac, order, f);
+    return;
+  }
   int F = D + 2;
   double uu[3], drho[3], dene[3], dke[3], de[3], dmom[3][3], du[3][3], S[3][3];
   double ke = 0.0, diag = 0.0, Smod = 0.0, Pr = 0.5, mu_t = 0.0;

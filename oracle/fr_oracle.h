@@ -33,6 +33,8 @@ typedef struct {
   int les;               /* 0 none, 1 eddy-viscosity LES (input key LES)   */
   int sgs_model;         /* 0 Smagorinsky, 1 WALE (input key SGS_model)    */
   double filter_ratio;   /* input key filter_ratio                         */
+  const float* mlp;      /* sgs_model 5: parameters of the learned closure
+                            (no reference counterpart; layout in mlp.py)    */
 } or_physics;
 
 /* Generic conforming mesh of one element type (4-node quads or 8-node hexes,
