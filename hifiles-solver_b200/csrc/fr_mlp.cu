@@ -2,8 +2,9 @@
 // (parameter layout and the per-point model in fr_mlp.cuh), and the kernel
 // that evaluates the closure's inputs from a solver's state and gradient.
 //
-// Training step on a batch of N samples (x_n, c*_n):
-//   loss = (1/N) sum_n (c(x_n) - c*_n)^2
+// Training step on a batch of N samples (x_n, c*_n, weight s_n; s_n = 1 when
+// no weights are given):
+//   loss = (1/N) sum_n s_n (c(x_n) - c*_n)^2
 // fr_mlp_loss_grad_kernel: one CTA per tile of 128 samples; forward pass with
 // the activations kept in shared memory, then the backward pass as
 // tile-local sums over the samples in a fixed order -> one partial gradient
@@ -45,7 +46,8 @@ __global__ void __launch_bounds__(256) fr_mlp_forward_kernel(const float* __rest
 
 __global__ void __launch_bounds__(kTile) fr_mlp_loss_grad_kernel(const float* __restrict__ w,
                                                                  const float* __restrict__ X,
-                                                                 const float* __restrict__ Y, long long n,
+                                                                 const float* __restrict__ Y,
+                                                                 const float* __restrict__ SW, long long n,
                                                                  float inv_n, float* __restrict__ partial)
 {
   // activations sample-minor ([unit][sample]) so that a warp's 32 samples
@@ -82,9 +84,10 @@ __global__ void __launch_bounds__(kTile) fr_mlp_loss_grad_kernel(const float* __
   }
   const float c = mlp_softplus(o);
   const float r = live ? c - Y[s] : 0.f;
+  const float sw = (live && SW) ? SW[s] : 1.f;
   const float sig = 1.f / (1.f + expf(-o));
-  sDo[t] = 2.f * r * sig * inv_n;       // d loss / d o
-  sLoss[t] = r * r;
+  sDo[t] = 2.f * sw * r * sig * inv_n;  // d loss / d o
+  sLoss[t] = sw * r * r;
   __syncthreads();
 
   float* P = partial + (size_t)blockIdx.x * (kMlpTrain + 1);
@@ -241,8 +244,8 @@ fr_status fr_mlp_forward(const float* w, const float* x, long long n, float* out
   return e == cudaSuccess ? FR_OK : mlp_fail(FR_ERR_CUDA, cudaGetErrorString(e));
 }
 
-fr_status fr_mlp_loss_grad(const float* w, const float* x, const float* y, long long n, float* grad, float* loss,
-                           float* scratch, long long scratch_floats, void* stream)
+fr_status fr_mlp_loss_grad(const float* w, const float* x, const float* y, const float* sw, long long n, float* grad,
+                           float* loss, float* scratch, long long scratch_floats, void* stream)
 {
   if (!w || !x || !y || !grad || !scratch || n <= 0) return mlp_fail(FR_ERR_ARG, "bad argument");
   if (scratch_floats < fr_mlp_scratch_floats(n))
@@ -254,7 +257,7 @@ fr_status fr_mlp_loss_grad(const float* w, const float* x, const float* y, long 
   static bool once = (cudaFuncSetAttribute(fr_mlp_loss_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)kGradSmem), true);
   (void)once;
-  fr_mlp_loss_grad_kernel<<<(unsigned)nblk, kTile, kGradSmem, st>>>(w, x, y, n, inv_n, scratch);
+  fr_mlp_loss_grad_kernel<<<(unsigned)nblk, kTile, kGradSmem, st>>>(w, x, y, sw, n, inv_n, scratch);
   fr_mlp_reduce_kernel<<<(kMlpTrain + 1 + 255) / 256, 256, 0, st>>>(scratch, (int)nblk, inv_n, grad, loss);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? FR_OK : mlp_fail(FR_ERR_CUDA, cudaGetErrorString(e));

@@ -85,7 +85,7 @@ def lib():
         "fr_mlp_n_trained": (C.c_int, []),
         "fr_mlp_scratch_floats": (C.c_longlong, [C.c_longlong]),
         "fr_mlp_forward": (C.c_int, [vp, vp, C.c_longlong, vp, vp]),
-        "fr_mlp_loss_grad": (C.c_int, [vp, vp, vp, C.c_longlong, vp, vp, vp, C.c_longlong, vp]),
+        "fr_mlp_loss_grad": (C.c_int, [vp, vp, vp, vp, C.c_longlong, vp, vp, vp, C.c_longlong, vp]),
         "fr_mlp_adam": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_float, vp]),
     }
     for name, (res, args) in sigs.items():
@@ -118,9 +118,9 @@ def box_mesh(dims, n, lo, hi, jitter=0.0, seed=0):
     nv = vx * vy * vz
     mask = (1 << 64) - 1
     A, B = 6364136223846793005, 1442695040888963407
-    rnd = np.empty((nv, dims))
+    rnd = np.zeros((nv, dims))
     s = (int(seed) * A + B) & mask
-    for v in range(nv):
+    for v in range(nv if jitter > 0 else 0):
         for d in range(dims):
             s = (s * A + B) & mask
             rnd[v, d] = ((s >> 11) * (1.0 / 9007199254740992.0)) * 2.0 - 1.0
@@ -351,8 +351,9 @@ def mlp_forward(d_w, d_x, n, d_out, stream=None):
     _check(lib().fr_mlp_forward(d_w, d_x, int(n), d_out, stream))
 
 
-def mlp_loss_grad(d_w, d_x, d_y, n, d_grad, d_loss, d_scratch, scratch_floats, stream=None):
-    _check(lib().fr_mlp_loss_grad(d_w, d_x, d_y, int(n), d_grad, d_loss, d_scratch, int(scratch_floats), stream))
+def mlp_loss_grad(d_w, d_x, d_y, n, d_grad, d_loss, d_scratch, scratch_floats, d_sw=None, stream=None):
+    _check(lib().fr_mlp_loss_grad(d_w, d_x, d_y, d_sw, int(n), d_grad, d_loss, d_scratch, int(scratch_floats),
+                                  stream))
 
 
 def mlp_adam(d_w, d_grad, d_m, d_v, step, lr, stream=None):

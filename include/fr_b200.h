@@ -171,16 +171,17 @@ fr_status fr_solver_sgs_features(fr_solver* s, float* host_x, void* stream);
  * sgs_model = 5 (such a solver starts with the closure off, c ~ 2e-9). */
 fr_status fr_solver_set_sgs_mlp(fr_solver* s, const float* host_w);
 
-/* Training kernels on device arrays: x (n, 6), c* = y (n), w, grad, m, v
- * (fr_mlp_n_params() / fr_mlp_n_trained() floats).  loss_grad gives the
- * gradient of (1/n) sum (c(x) - y)^2 over the trained parameters and the
- * loss; it needs fr_mlp_scratch_floats(n) floats of caller scratch and is
+/* Training kernels on device arrays: x (n, 6), c* = y (n), sample weights
+ * sw (n, or NULL for all ones), w, grad, m, v (fr_mlp_n_params() /
+ * fr_mlp_n_trained() floats).  loss_grad gives the gradient of
+ * (1/n) sum sw (c(x) - y)^2 over the trained parameters and the loss; it
+ * needs fr_mlp_scratch_floats(n) floats of caller scratch and is
  * deterministic.  adam applies one Adam step (beta 0.9 / 0.999, eps 1e-8;
  * step counts from 1). */
 long long fr_mlp_scratch_floats(long long n);
 fr_status fr_mlp_forward(const float* d_w, const float* d_x, long long n, float* d_out, void* stream);
-fr_status fr_mlp_loss_grad(const float* d_w, const float* d_x, const float* d_y, long long n, float* d_grad,
-                           float* d_loss, float* d_scratch, long long scratch_floats, void* stream);
+fr_status fr_mlp_loss_grad(const float* d_w, const float* d_x, const float* d_y, const float* d_sw, long long n,
+                           float* d_grad, float* d_loss, float* d_scratch, long long scratch_floats, void* stream);
 fr_status fr_mlp_adam(float* d_w, const float* d_grad, float* d_m, float* d_v, int step, float lr, void* stream);
 
 /* ------------------------------------------------------------------------

@@ -56,8 +56,8 @@ def forward(w, X):
     return _softplus(h2 @ w3 + b3)
 
 
-def loss_grad(w, X, Y):
-    """(loss, gradient over the 4673 trained parameters) of mean (c - y)^2."""
+def loss_grad(w, X, Y, sw=None):
+    """(loss, gradient over the 4673 trained parameters) of mean sw (c - y)^2."""
     w1, b1, w2, b2, w3, b3, xm, xs = unpack(w)
     X = np.asarray(X, dtype=np.float64)
     Y = np.asarray(Y, dtype=np.float64)
@@ -67,7 +67,8 @@ def loss_grad(w, X, Y):
     h2 = np.tanh(h1 @ w2.T + b2)
     o = h2 @ w3 + b3
     r = _softplus(o) - Y
-    do = 2.0 * r / (1.0 + np.exp(-o)) / n
+    sw = np.ones(n) if sw is None else np.asarray(sw, dtype=np.float64)
+    do = 2.0 * sw * r / (1.0 + np.exp(-o)) / n
     g = np.zeros(NTRAIN)
     g[W3:B3] = do @ h2
     g[B3] = do.sum()
@@ -77,7 +78,7 @@ def loss_grad(w, X, Y):
     da1 = (da2 @ w2) * (1.0 - h1 * h1)
     g[W1:B1] = (da1.T @ xn).ravel()
     g[B1:W2] = da1.sum(axis=0)
-    return float((r * r).mean()), g
+    return float((sw * r * r).mean()), g
 
 
 def inputs(q, g, detjac, order, filter_ratio):

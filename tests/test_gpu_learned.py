@@ -71,6 +71,15 @@ def test_loss_gradient_kernel_matches_numpy_and_is_deterministic():
     for a, b in ((M.W1, M.B1), (M.W2, M.B2), (M.W3, M.B3)):
         assert rel(grads[0][a:b], g_ref[a:b]) < 1e-4
     assert np.array_equal(grads[0], grads[1])
+    # per-sample weights
+    sw = np.random.default_rng(8).uniform(0.0, 3.0, n).astype(np.float32)
+    dsw = _dev(sw)
+    H.mlp_loss_grad(dw.data_ptr(), dx.data_ptr(), dy.data_ptr(), n, g.data_ptr(), loss.data_ptr(),
+                    scratch.data_ptr(), ns, d_sw=dsw.data_ptr())
+    torch.cuda.synchronize()
+    l_ref, g_ref = M.loss_grad(w, X, Y, sw)
+    assert abs(loss.item() - l_ref) <= 1e-5 * l_ref
+    assert rel(g.cpu().numpy(), g_ref) < 1e-4
 
 
 def test_adam_kernel_matches_numpy():

@@ -1,0 +1,36 @@
+"""What the learned SGS closure gains: the whole pipeline of
+hifiles_b200.learned_sgs at small scale (fine 32^3 hexes P=3 solved without a
+model, projected onto 8^3 P=3; decaying isotropic turbulence, u_rms 1,
+Mach 0.1, mu 1e-3), trained on the GPU with the library's kernels on two
+snapshots and judged on a third, held out, and by coarse runs from the
+filtered initial field against the filtered fine solution.
+
+Measured on a B200 (seed 1): relative L2 error of the SGS dissipation
+tau^d:S, a priori -- closure 0.98, WALE 2.5, no model 1.0; mean relative
+error of the resolved kinetic energy over three times, a posteriori --
+closure 3.0 %, WALE 19.5 %, no model 0.4 %.  The closure beats the WALE
+fallback on both counts and the no-model baseline a priori; at this
+resolution the scheme's own dissipation (no model) tracks the filtered
+fine kinetic energy most closely, which this test records rather than
+hides."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+pytest.importorskip("torch")
+
+from hifiles_b200 import learned_sgs as L  # noqa: E402
+
+
+def test_learned_closure_gains_over_wale_and_no_model_a_priori():
+    r = L.run_experiment(nf=32, nc=8, P=3, mu=1e-3, dt=1e-3, epochs=40, seed=1, log=lambda *_: None)
+    ap, post = r["a_priori"], r["a_posteriori"]
+    print({k: v for k, v in ap.items()}, {k: v["mean_rel_ke_error"] for k, v in post.items()})
+    assert r["loss_history"][-1] < r["loss_history"][0]
+    # a priori, held-out snapshot: better than the method without a model and than WALE
+    assert ap["learned"]["rel_l2_error"] < ap["none"]["rel_l2_error"]
+    assert ap["learned"]["rel_l2_error"] < ap["wale"]["rel_l2_error"]
+    assert ap["learned"]["corr"] > ap["wale"]["corr"]
+    # a posteriori: closer to the filtered fine kinetic energy than WALE
+    assert post["learned"]["mean_rel_ke_error"] < post["wale"]["mean_rel_ke_error"]
+    assert all(np.isfinite(v["mean_rel_ke_error"]) for v in post.values())
