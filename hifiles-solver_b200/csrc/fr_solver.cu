@@ -643,3 +643,25 @@ fr_status fr_solver_set_sgs_mlp(fr_solver* s, const float* host_w)
   FR_CUDA(cudaMemcpy(s->mlp, host_w, sizeof(float) * kMlpN, cudaMemcpyHostToDevice));
   return FR_OK;
 }
+
+fr_status fr_solver_write_restart(fr_solver* s, const char* path, double time)
+{
+  if (!s || !path) return fail(FR_ERR_ARG, "null argument");
+  const Mesh& m = s->mesh;
+  std::vector<double> u((size_t)m.nu * m.ne * m.nfields);
+  fr_status r = fr_solver_get_state(s, u.data(), nullptr);
+  if (r) return r;
+  fr_restart_block b{m.dims == 2 ? 1 : 4, s->sch.order, m.nu, (int)m.ne, m.nfields, s->line.loc, nullptr, u.data()};
+  return fr_restart_write(path, time, &b, 1);
+}
+
+fr_status fr_solver_read_restart(fr_solver* s, const char* path, double* time_out)
+{
+  if (!s || !path) return fail(FR_ERR_ARG, "null argument");
+  const Mesh& m = s->mesh;
+  std::vector<double> u((size_t)m.nu * m.ne * m.nfields);
+  fr_status r = fr_restart_read(path, m.dims == 2 ? 1 : 4, s->sch.order, s->sch.upts_type, (int)m.ne, m.nfields,
+                                nullptr, u.data(), time_out);
+  if (r) return r;
+  return fr_solver_set_state(s, u.data(), nullptr);
+}

@@ -79,6 +79,10 @@ def lib():
         "fr_mesh_geometry": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(SchemeDesc), ip, dp, dp, dp, dp, dp, ip, ip]),
         "fr_line_operators": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, dp]),
         "fr_solver_gradient": (C.c_int, [vp, dp, vp]),
+        "fr_restart_write": (C.c_int, [C.c_char_p, C.c_double, vp, C.c_int]),
+        "fr_restart_read": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp, dp, dp]),
+        "fr_solver_write_restart": (C.c_int, [vp, C.c_char_p, C.c_double]),
+        "fr_solver_read_restart": (C.c_int, [vp, C.c_char_p, dp]),
         "fr_solver_sgs_features": (C.c_int, [vp, C.POINTER(C.c_float), vp]),
         "fr_solver_set_sgs_mlp": (C.c_int, [vp, C.POINTER(C.c_float)]),
         "fr_mlp_n_params": (C.c_int, []),
@@ -286,6 +290,17 @@ class Solver:
         _check(lib().fr_solver_advance(self.h, int(n_steps), float(dt), _dp(out) if norms else None, stream))
         return out
 
+    def write_restart(self, path, time=0.0):
+        """The state as a restart file in the reference's format."""
+        _check(lib().fr_solver_write_restart(self.h, str(path).encode(), float(time)))
+
+    def read_restart(self, path):
+        """Sets the state from a restart file (any order of the same element
+        type); returns the file's time."""
+        t = C.c_double()
+        _check(lib().fr_solver_read_restart(self.h, str(path).encode(), C.byref(t)))
+        return t.value
+
     def gradient(self, stream=None):
         """Corrected physical gradient grad_disu_upts (n_upts, n_eles, n_fields, n_dims)."""
         g = np.zeros((self.n_upts, self.n_eles, self.n_fields, self.dims), order="F")
@@ -358,3 +373,35 @@ def mlp_loss_grad(d_w, d_x, d_y, n, d_grad, d_loss, d_scratch, scratch_floats, d
 
 def mlp_adam(d_w, d_grad, d_m, d_v, step, lr, stream=None):
     _check(lib().fr_mlp_adam(d_w, d_grad, d_m, d_v, int(step), float(lr), stream))
+
+
+# ---------------------------------------------------------------- restart files (host only)
+
+class RestartBlock(C.Structure):
+    _fields_ = [("ele_type", C.c_int), ("order", C.c_int), ("n_upts", C.c_int), ("n_eles", C.c_int),
+                ("n_fields", C.c_int), ("loc_1d", C.POINTER(C.c_double)), ("ele2global", C.POINTER(C.c_int)),
+                ("disu_upts", C.POINTER(C.c_double))]
+
+
+def restart_write(path, time, blocks):
+    """blocks: list of dicts(ele_type, order, loc_1d, disu_upts (n_upts, n_eles, F), ele2global=None)."""
+    keep, arr = [], (RestartBlock * len(blocks))()
+    for i, b in enumerate(blocks):
+        u = np.asfortranarray(b["disu_upts"], dtype=np.float64)
+        loc = np.ascontiguousarray(b["loc_1d"], dtype=np.float64)
+        g = None if b.get("ele2global") is None else np.ascontiguousarray(b["ele2global"], dtype=np.int32)
+        keep += [u, loc, g]
+        arr[i] = RestartBlock(int(b["ele_type"]), int(b["order"]), u.shape[0], u.shape[1], u.shape[2], _dp(loc),
+                              None if g is None else g.ctypes.data_as(C.POINTER(C.c_int)), _dp(u))
+    _check(lib().fr_restart_write(str(path).encode(), float(time), arr, len(blocks)))
+
+
+def restart_read(path, ele_type, order, n_eles, n_fields, upts_type=0, ele2global=None):
+    """(disu_upts (n_upts, n_eles, F), time) of one element type's block."""
+    dims = 2 if ele_type == 1 else 3
+    u = np.zeros(((order + 1) ** dims, n_eles, n_fields), order="F")
+    g = None if ele2global is None else np.ascontiguousarray(ele2global, dtype=np.int32)
+    t = C.c_double()
+    _check(lib().fr_restart_read(str(path).encode(), int(ele_type), int(order), int(upts_type), int(n_eles),
+                                 int(n_fields), None if g is None else g.ctypes.data, _dp(u), C.byref(t)))
+    return u, t.value

@@ -152,6 +152,35 @@ fr_status fr_solver_profile_stage(fr_solver* s, int reps, double dt, double* ms3
 fr_status fr_solver_gradient(fr_solver* s, double* host_grad, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Restart files in the reference's text format (write_restart,
+ * src/output.cpp:1057-1107; read_restart, src/solver.cpp:390-445).  Host
+ * memory only; no GPU is touched by fr_restart_*.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+  int ele_type;            /* reference codes: 1 quads, 4 hexes                */
+  int order;               /* polynomial order of the block                    */
+  int n_upts, n_eles, n_fields;
+  const double* loc_1d;    /* order + 1 solution-point locations in 1-D        */
+  const int* ele2global;   /* global element ids (NULL: 0 .. n_eles-1)         */
+  const double* disu_upts; /* (n_upts, n_eles, n_fields)                       */
+} fr_restart_block;
+
+/* Writes a restart file exactly as the reference does (%.15g numbers,
+ * eles::write_restart_info / write_restart_data, src/eles_hexas.cpp:882-900,
+ * src/eles.cpp:697-722); blocks with no elements are left out. */
+fr_status fr_restart_write(const char* path, double time, const fr_restart_block* blocks, int n_blocks);
+/* Reads the block of one element type into disu_upts (n_upts, n_eles,
+ * n_fields) of a solver of the given order and point family, interpolating
+ * from the file's order when it differs (eles::set_opp_r,
+ * src/eles.cpp:4135-4153).  Elements are matched by global id; every
+ * element must be present.  time_out may be NULL. */
+fr_status fr_restart_read(const char* path, int ele_type, int order, int upts_type, int n_eles, int n_fields,
+                          const int* ele2global, double* disu_upts, double* time_out);
+/* The solver's state to / from a restart file (global ids 0 .. n_eles-1). */
+fr_status fr_solver_write_restart(fr_solver* s, const char* path, double time);
+fr_status fr_solver_read_restart(fr_solver* s, const char* path, double* time_out);
+
+/* ------------------------------------------------------------------------
  * Learned SGS closure (sgs_model 5).  No counterpart in the reference, whose
  * eddy-viscosity models are Smagorinsky and WALE (eles::calc_sgsf_upts,
  * src/eles.cpp:2456-2778); it uses the same flux with

@@ -279,18 +279,21 @@ static void staged_residual(solution& S)
 int main(int argc, char** argv)
 {
   if (argc < 3) {
-    fprintf(stderr, "usage: ref_harness <input_file> <out_dir> [--ic NAME] [--steps N] [--stages] [--no-dump]\n");
+    fprintf(stderr, "usage: ref_harness <input_file> <out_dir> [--ic NAME] [--steps N] [--stages] [--no-dump]"
+                    " [--write-restart N]\n");
     return 2;
   }
   g_out = argv[2];
   string ic;
   int steps = 0;
   bool stages = false, nodump = false;
+  int restart_out = -1;
   for (int a = 3; a < argc; a++) {
     if (!strcmp(argv[a], "--ic") && a + 1 < argc) ic = argv[++a];
     else if (!strcmp(argv[a], "--steps") && a + 1 < argc) steps = atoi(argv[++a]);
     else if (!strcmp(argv[a], "--stages")) stages = true;
     else if (!strcmp(argv[a], "--no-dump")) nodump = true;
+    else if (!strcmp(argv[a], "--write-restart") && a + 1 < argc) restart_out = atoi(argv[++a]);
     else { fprintf(stderr, "bad argument %s\n", argv[a]); return 2; }
   }
 
@@ -340,6 +343,11 @@ int main(int argc, char** argv)
     write_npy("res_norms", hist.data(), "<f8", 8, shape);
     dump_stage(S, "final", "disu_upts0");
     dump_stage(S, "final", "div_tconf_upts");
+  }
+  if (restart_out >= 0) {
+    // Rest_<N>_p0000.dat in the working directory (src/output.cpp:1057-1107)
+    run_input.restart_mesh_out = 0;
+    write_restart(restart_out, &S);
   }
   printf("ref_harness done\n");
   return 0;

@@ -178,7 +178,7 @@ def rel(a, b):
 CASES = [
     # name, dims, order, n, lo, hi, viscous, ic, vcjh, jitter, steps, dt, stages
     dict(name="quad_vortex_p3_n6", dims=2, order=3, n=(6, 6), lo=(-5, -5), hi=(5, 5), viscous=0,
-         ic="vortex_u1v0", vcjh=1, jitter=0.0, steps=20, dt=1e-3, stages=True),
+         ic="vortex_u1v0", vcjh=1, jitter=0.0, steps=20, dt=1e-3, stages=True, restart_out=True),
     dict(name="quad_vortex_p2_n5_jit", dims=2, order=2, n=(5, 5), lo=(-5, -5), hi=(5, 5), viscous=0,
          ic="vortex_u1v0", vcjh=2, jitter=0.15, steps=10, dt=1e-3, stages=True),
     dict(name="quad_vortex_p3_n20", dims=2, order=3, n=(20, 20), lo=(-5, -5), hi=(5, 5), viscous=0,
@@ -186,7 +186,7 @@ CASES = [
     dict(name="hex_tgv_p3_n3", dims=3, order=3, n=(3, 3, 3), lo=(0, 0, 0), hi=(2 * np.pi,) * 3, viscous=1,
          ic="tgv_mach01", vcjh=1, jitter=0.0, steps=5, dt=1e-3, stages=True),
     dict(name="hex_tgv_p2_n3_jit", dims=3, order=2, n=(3, 3, 3), lo=(0, 0, 0), hi=(2 * np.pi,) * 3, viscous=1,
-         ic="tgv_mach01", vcjh=2, jitter=0.1, steps=5, dt=1e-3, stages=True),
+         ic="tgv_mach01", vcjh=2, jitter=0.1, steps=5, dt=1e-3, stages=True, restart_out=True),
     dict(name="hex_tgv_p4_n2", dims=3, order=4, n=(2, 2, 2), lo=(0, 0, 0), hi=(2 * np.pi,) * 3, viscous=1,
          ic="tgv_mach01", vcjh=1, jitter=0.0, steps=3, dt=1e-3, stages=False),
     dict(name="hex_euler_p3_n3", dims=3, order=3, n=(3, 3, 3), lo=(0, 0, 0), hi=(2 * np.pi,) * 3, viscous=0,
@@ -227,12 +227,56 @@ def run_case(ref, c, work):
     args = [HARNESS, "input", out, "--ic", c["ic"], "--steps", str(c["steps"])]
     if c["stages"]:
         args.append("--stages")
+    if c.get("restart_out"):
+        args += ["--write-restart", str(c["steps"])]
     env = dict(os.environ, HIFILES_HOME=os.path.join(REPO, "oracle", "_ref"))
     r = subprocess.run(args, cwd=d, env=env, capture_output=True, text=True)
     if r.returncode != 0:
         print(r.stdout[-2000:], r.stderr[-2000:])
         raise RuntimeError("harness failed for " + c["name"])
+    if c.get("restart_out"):
+        # the reference's own restart file, kept verbatim as a fixture
+        src = os.path.join(d, "Rest_%09d_p%04d.dat" % (c["steps"], 0))
+        with open(src) as fi, open(os.path.join(HERE, "rest_" + c["name"] + ".dat"), "w") as fo:
+            fo.write(fi.read())
     return load_npy_dir(out)
+
+
+def restart_read_fixture(ref, work):
+    """The reference reading a restart file written by this library's writer
+    (fr_restart_write) at another order: the TGV P=2 jittered case's final
+    state, written as order 2, read by the reference set up at order 3
+    (read_restart + eles::set_opp_r interpolation) -> its disu_upts(0)."""
+    sys.path.insert(0, os.path.join(REPO, "hifiles-solver_b200"))
+    import hifiles_b200 as H
+    meta, fx = None, np.load(os.path.join(HERE, "hex_tgv_p2_n3_jit.npz"))
+    meta = json.loads(str(fx["meta"]))
+    u2 = np.asfortranarray(fx["uN"])
+    d = os.path.join(work, "restart_read")
+    os.makedirs(d, exist_ok=True)
+    H.restart_write(os.path.join(d, "Rest_%09d_p%04d.dat" % (7, 0)), 0.005,
+                    [dict(ele_type=4, order=2, loc_1d=O.points_1d(2), disu_upts=u2)])
+    xv, c2v = box_vertices(3, meta["n"], meta["lo"], meta["hi"], meta["jitter"], seed=12345)
+    write_gambit(os.path.join(d, "mesh.neu"), 3, xv, c2v, meta["n"])
+    L = [meta["hi"][i] - meta["lo"][i] for i in range(3)]
+    vals = {"equation": 0, "viscous": 1, "order": 3, "dt_type": 0, "dt": 1e-3, "n_steps": 1, "adv_type": 3,
+            "mesh_file": "mesh.neu", "dx_cyclic": "%.17g" % L[0], "dy_cyclic": "%.17g" % L[1],
+            "dz_cyclic": "%.17g" % L[2], "monitor_res_freq": 100000, "plot_freq": 100000,
+            "restart_dump_freq": 100000, "upts_type_hexa": 0, "vcjh_scheme_hexa": 2, "prandtl": 0.71,
+            "Mach_free_stream": 0.1, "Re_free_stream": 1600.0, "gamma": 1.4, "fix_vis": 1, "ic_form": 7,
+            "restart_flag": 1, "restart_iter": 7, "n_restart_files": 1}
+    write_input(os.path.join(d, "input"), os.path.join(ref, TGV_INPUT), vals)
+    out = os.path.join(d, "out")
+    os.makedirs(out, exist_ok=True)
+    env = dict(os.environ, HIFILES_HOME=os.path.join(REPO, "oracle", "_ref"))
+    r = subprocess.run([HARNESS, "input", out, "--steps", "0"], cwd=d, env=env, capture_output=True, text=True)
+    if r.returncode != 0:
+        print(r.stdout[-2000:], r.stderr[-2000:])
+        raise RuntimeError("harness failed reading a restart file")
+    arr, _ = load_npy_dir(out)
+    np.savez_compressed(os.path.join(HERE, "rest_read_p2_to_p3.npz"), u_p2=u2,
+                        u_p3_ref=np.asfortranarray(arr["t4_disu_upts_init"]), time=0.005)
+    print("restart read fixture: reference P3 state from our P2 file, shape", arr["t4_disu_upts_init"].shape)
 
 
 def main():
@@ -346,6 +390,7 @@ def main():
     with open(os.path.join(HERE, "summary.json"), "w") as f:
         json.dump({"pins": summary, "kat_oracle": kat["oracle_vals"], "points_1d_mismatches": mism}, f, indent=1)
     print("kat", kat["oracle_vals"], "point-table mismatches", mism)
+    restart_read_fixture(a.ref, work)
 
 
 if __name__ == "__main__":

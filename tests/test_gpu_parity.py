@@ -174,3 +174,16 @@ def test_autotuned_tiles_give_identical_states():
     s1.advance(3, 1e-3)
     s2.advance(3, 1e-3)
     assert np.array_equal(s1.get_state(), s2.get_state())
+
+
+def test_solver_restart_round_trip_with_reference_file(tmp_path):
+    """Solver state from the reference's own restart file, stepped on, and
+    written back in the same format."""
+    meta, a = load("quad_vortex_p3_n6")
+    s = _solver(meta)
+    t = s.read_restart(os.path.join(GOLDEN, "rest_quad_vortex_p3_n6.dat"))
+    assert abs(t - 0.02) < 1e-12
+    assert rel(s.get_state(), a["uN"]) <= 1e-14
+    out = tmp_path / "Rest.dat"
+    s.write_restart(out, t)
+    assert out.read_bytes() == open(os.path.join(GOLDEN, "rest_quad_vortex_p3_n6.dat"), "rb").read()
