@@ -621,8 +621,9 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
 // projections VF, src/int_inters.cpp:359-470).  Writes norm_tconf_fpts of
 // both sides: +f_n tdA_l on the left, -f_n tdA_r on the right.
 // face[i] = (left flat index, right flat index) of interface point i;
-// fsign[i] != 0 when the LDG penalty sign is negative there.
-template <int DIM, int VISC, typename TC>
+// fsign[i] != 0 when the LDG penalty sign is negative there.  RIEMANN is the
+// reference's riemann_solve_type: 0 Rusanov, 2 Roe (2-D).
+template <int DIM, int VISC, typename TC, int RIEMANN = 0>
 __global__ void __launch_bounds__(128)
 fr_face_kernel(const int2* __restrict__ face, const unsigned char* __restrict__ fsign, long long nint,
                const TC* __restrict__ UF, const TC* __restrict__ VF, const TC* __restrict__ nL,
@@ -640,7 +641,8 @@ fr_face_kernel(const int2* __restrict__ face, const unsigned char* __restrict__ 
   for (int d = 0; d < D; d++) n[d] = nL[a + NFE * d];
   const TC tl = tdA[a], tr = tdA[b];
   TC fn[F];
-  rusanov<D, TC>(ph, ul, ur, n, fn);
+  if constexpr (RIEMANN == 2 && DIM == 2) roe<TC>(ph, ul, ur, n, fn);
+  else rusanov<D, TC>(ph, ul, ur, n, fn);
   TC cl[F], cr[F];
 #pragma unroll
   for (int k = 0; k < F; k++) { cl[k] = fn[k] * tl; cr[k] = -fn[k] * tr; }

@@ -231,6 +231,59 @@ __device__ __forceinline__ void rusanov(const PhysT<T>& ph, const T* ul, const T
   }
 }
 
+// Roe common normal flux with the entropy fix of inters::roe_flux,
+// src/inters.cpp:390-508, static mesh (v_g = 0).  2-D only, as in the
+// reference ("Roe not implemented in 3D").
+template <typename T>
+__device__ __forceinline__ void roe(const PhysT<T>& ph, const T* ul, const T* ur, const T* n, T* fn)
+{
+  const T g = ph.gamma, gm1 = g - T(1.0);
+  const T vl0 = ul[1] / ul[0], vl1 = ul[2] / ul[0], vr0 = ur[1] / ur[0], vr1 = ur[2] / ur[0];
+  const T pl = gm1 * (ul[3] - (T(0.5) * ul[0] * ((vl0 * vl0) + (vl1 * vl1))));
+  const T pr = gm1 * (ur[3] - (T(0.5) * ur[0] * ((vr0 * vr0) + (vr1 * vr1))));
+  const T hl = (ul[3] + pl) / ul[0], hr = (ur[3] + pr) / ur[0];
+  const T sq = fr_sqrt<T>(ur[0] / ul[0]);
+  const T rr = T(1.) / (sq + T(1.));
+  const T um0 = rr * (vl0 + sq * vr0), um1 = rr * (vl1 + sq * vr1);
+  const T hm = rr * (hl + sq * hr);
+  T usq = T(0.);
+  usq = usq + T(0.5) * um0 * um0;
+  usq = usq + T(0.5) * um1 * um1;
+  const T am2 = gm1 * (hm - usq);
+  const T am = fr_sqrt<T>(am2);
+  T unm = T(0.), vgn = T(0.), rl = T(0.), rrn = T(0.);
+  unm = unm + um0 * n[0]; unm = unm + um1 * n[1];
+  vgn = vgn + T(0.0) * n[0]; vgn = vgn + T(0.0) * n[1];
+  rl = rl + ul[1] * n[0]; rl = rl + ul[2] * n[1];
+  rrn = rrn + ur[1] * n[0]; rrn = rrn + ur[2] * n[1];
+  T f0 = rl + rrn;
+  T f1 = rl * vl0 + rrn * vr0 + (pl + pr) * n[0];
+  T f2 = rl * vl1 + rrn * vr1 + (pl + pr) * n[1];
+  T f3 = rl * hl + rrn * hr;
+  const T du0 = ur[0] - ul[0], du1 = ur[1] - ul[1], du2 = ur[2] - ul[2], du3 = ur[3] - ul[3];
+  T l0 = fr_abs<T>(unm - vgn), lP = fr_abs<T>(unm - vgn + am), lM = fr_abs<T>(unm - vgn - am);
+  const T eps = T(0.5) * (fr_abs<T>(rl / ul[0] - rrn / ur[0]) +
+                          fr_abs<T>(fr_sqrt<T>(g * pl / ul[0]) - fr_sqrt<T>(g * pr / ur[0])));
+  if (l0 < T(2.) * eps) l0 = T(0.25) * l0 * l0 / eps + eps;
+  if (lP < T(2.) * eps) lP = T(0.25) * lP * lP / eps + eps;
+  if (lM < T(2.) * eps) lM = T(0.25) * lM * lM / eps + eps;
+  const T a2 = T(0.5) * (lP + lM) - l0;
+  const T a3 = T(0.5) * (lP - lM) / am;
+  const T a1 = a2 * gm1 / am2;
+  const T a4 = a3 * gm1;
+  const T a5 = usq * du0 - um0 * du1 - um1 * du2 + du3;
+  const T a6 = unm * du0 - n[0] * du1 - n[1] * du2;
+  const T aL1 = a1 * a5 - a3 * a6, bL1 = a4 * a5 - a2 * a6;
+  f0 = f0 - (l0 * du0 + aL1);
+  f1 = f1 - (l0 * du1 + aL1 * um0 + bL1 * n[0]);
+  f2 = f2 - (l0 * du2 + aL1 * um1 + bL1 * n[1]);
+  f3 = f3 - (l0 * du3 + aL1 * hm + bL1 * unm);
+  fn[0] = T(0.5) * f0 - T(0.5) * vgn * (ur[0] + ul[0]);
+  fn[1] = T(0.5) * f1 - T(0.5) * vgn * (ur[1] + ul[1]);
+  fn[2] = T(0.5) * f2 - T(0.5) * vgn * (ur[2] + ul[2]);
+  fn[3] = T(0.5) * f3 - T(0.5) * vgn * (ur[3] + ul[3]);
+}
+
 // Sign of the LDG penalty: one fixed direction per interface point, taken
 // from the left normal (src/inters.cpp:555-564, 651-660).
 template <int D, typename T>

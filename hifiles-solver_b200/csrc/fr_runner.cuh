@@ -44,6 +44,7 @@ struct Runner {
   virtual int flux_blocks() const = 0;      // blocks of the update kernel (norm partials)
   virtual int max_flux_blocks() const = 0;  // over all update-kernel tiles
   virtual int launches_per_stage() const = 0;
+  virtual void set_riemann(int rs) = 0;
   // tile variants of the two element kernels (autotuning)
   virtual int n_grad_tiles() const = 0;
   virtual int n_update_tiles() const = 0;
@@ -84,7 +85,7 @@ struct RunnerT : Runner {
   static constexpr int NG = sizeof(Tiles<DIM, P>::grad) / sizeof(Tile);
   static constexpr int NUP = sizeof(Tiles<DIM, P>::upd) / sizeof(Tile);
   long long E;
-  int visc, les;
+  int visc, les, riemann = 0;
   int gsel = 0, usel = 0;
   Line<TC> L;
   Line<double> L64;
@@ -129,6 +130,7 @@ struct RunnerT : Runner {
     return m;
   }
   int launches_per_stage() const override { return visc ? 3 : 2; }
+  void set_riemann(int rs) override { riemann = rs; }
   void trace(const Bufs& b, int cur, cudaStream_t s) override
   {
     long long n = E * S::NF;
@@ -156,16 +158,24 @@ struct RunnerT : Runner {
     else grad_i<0, 0>(b, cur, s);
   }
 
+  template <int VISC, int RS>
+  void face_t(const Bufs& b, int cur, cudaStream_t s)
+  {
+    unsigned g = (unsigned)((b.nint + 127) / 128);
+    fr_face_kernel<DIM, VISC, TC, RS><<<g, 128, 0, s>>>(b.face, b.fsign, b.nint, (const TC*)b.UF[cur],
+                                                         VISC ? (const TC*)b.VF : nullptr, (const TC*)b.nL,
+                                                         (const TC*)b.tdA, (TC*)b.CF, E * S::NF, ph);
+  }
   void face(const Bufs& b, int cur, cudaStream_t s) override
   {
     if (b.nint == 0) return;
-    unsigned g = (unsigned)((b.nint + 127) / 128);
-    if (visc)
-      fr_face_kernel<DIM, 1, TC><<<g, 128, 0, s>>>(b.face, b.fsign, b.nint, (const TC*)b.UF[cur], (const TC*)b.VF,
-                                                   (const TC*)b.nL, (const TC*)b.tdA, (TC*)b.CF, E * S::NF, ph);
-    else
-      fr_face_kernel<DIM, 0, TC><<<g, 128, 0, s>>>(b.face, b.fsign, b.nint, (const TC*)b.UF[cur], nullptr,
-                                                   (const TC*)b.nL, (const TC*)b.tdA, (TC*)b.CF, E * S::NF, ph);
+    if (DIM == 2 && riemann == 2) {
+      if (visc) face_t<1, 2>(b, cur, s);
+      else face_t<0, 2>(b, cur, s);
+    } else {
+      if (visc) face_t<1, 0>(b, cur, s);
+      else face_t<0, 0>(b, cur, s);
+    }
   }
 
   template <int I, int VISC, int MODE>

@@ -180,7 +180,8 @@ fr_status fr_solver_create(const fr_mesh_desc* md, const fr_scheme_desc* sd, int
   if (!md || !sd || !out) return fail(FR_ERR_ARG, "null argument");
   *out = nullptr;
   if (md->dims != 2 && md->dims != 3) return fail(FR_ERR_ARG, "dims must be 2 or 3");
-  if (sd->riemann != 0) return fail(FR_ERR_UNSUPPORTED, "only the Rusanov common flux is built");
+  if (sd->riemann != 0 && !(sd->riemann == 2 && md->dims == 2))
+    return fail(FR_ERR_UNSUPPORTED, "common fluxes built: Rusanov (0), and Roe (2) in 2-D as in the reference");
   if (sd->precision != 0 && sd->precision != 1) return fail(FR_ERR_ARG, "precision must be 0 or 1");
   int maxP = md->dims == 2 ? 5 : 4;
   if (sd->order < 1 || sd->order > maxP) return fail(FR_ERR_UNSUPPORTED, "order outside the built range");
@@ -214,6 +215,7 @@ fr_status fr_solver_create(const fr_mesh_desc* md, const fr_scheme_desc* sd, int
   const int les = sd->les;
   Runner* r = make_runner(md->dims, sd->order, (int)s->tc_size, md->n_eles, sd->viscous, les, s->line, ph);
   if (!r) return fail(FR_ERR_UNSUPPORTED, "no kernel for this (dims, order)");
+  r->set_riemann(sd->riemann);
   s->run.reset(r);
   Mesh& m = s->mesh;
   size_t E = m.ne, F = m.nfields, D = m.dims, nu = m.nu, nf = m.nf, tc = s->tc_size;

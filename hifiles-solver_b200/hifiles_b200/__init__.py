@@ -151,12 +151,13 @@ def box_mesh(dims, n, lo, hi, jitter=0.0, seed=0):
 
 def _descs(dims, xv, c2v, shift, order, viscous=False, gamma=1.4, prandtl=0.72, mu_inf=0.0, rt_inf=1.0,
            c_sth=1.0, fix_vis=1.0, tau=1.0, pen_fact=0.5, vcjh_scheme=1, eta=0.0, upts_type=0, precision=0,
-           les=0, sgs_model=1, filter_ratio=1.0):
+           les=0, sgs_model=1, filter_ratio=1.0, riemann=0):
     xv = np.ascontiguousarray(xv, dtype=np.float64)
     c2v = np.ascontiguousarray(c2v, dtype=np.int32)
     md = MeshDesc(int(dims), xv.shape[0], _dp(xv), c2v.shape[0], c2v.ctypes.data_as(C.POINTER(C.c_int)),
                   (C.c_double * 3)(*(list(shift) + [0.0] * (3 - len(shift)))))
-    sd = SchemeDesc(int(order), int(upts_type), int(vcjh_scheme), float(eta), int(bool(viscous)), 0, int(precision),
+    sd = SchemeDesc(int(order), int(upts_type), int(vcjh_scheme), float(eta), int(bool(viscous)), int(riemann),
+                    int(precision),
                     gamma, prandtl, mu_inf, rt_inf, c_sth, fix_vis, tau, pen_fact, int(les), int(sgs_model),
                     float(filter_ratio))
     return md, sd, (xv, c2v)
@@ -194,14 +195,14 @@ class Solver:
 
     def __init__(self, dims, xv, c2v, shift, order, viscous=False, gamma=1.4, prandtl=0.72, mu_inf=0.0,
                  rt_inf=1.0, c_sth=1.0, fix_vis=1.0, tau=1.0, pen_fact=0.5, vcjh_scheme=1, eta=0.0, upts_type=0,
-                 precision=0, device=0, les=0, sgs_model=1, filter_ratio=1.0):
+                 precision=0, device=0, les=0, sgs_model=1, filter_ratio=1.0, riemann=0):
         L = lib()
         self._xv = np.ascontiguousarray(xv, dtype=np.float64)
         self._c2v = np.ascontiguousarray(c2v, dtype=np.int32)
         md = MeshDesc(int(dims), self._xv.shape[0], _dp(self._xv), self._c2v.shape[0],
                       self._c2v.ctypes.data_as(C.POINTER(C.c_int)),
                       (C.c_double * 3)(*(list(shift) + [0.0] * (3 - len(shift)))))
-        sd = SchemeDesc(int(order), int(upts_type), int(vcjh_scheme), float(eta), int(bool(viscous)), 0,
+        sd = SchemeDesc(int(order), int(upts_type), int(vcjh_scheme), float(eta), int(bool(viscous)), int(riemann),
                         int(precision), gamma, prandtl, mu_inf, rt_inf, c_sth, fix_vis, tau, pen_fact, int(les),
                         int(sgs_model), float(filter_ratio))
         h = C.c_void_p()

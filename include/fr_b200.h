@@ -67,7 +67,8 @@ typedef struct {
   int vcjh_scheme;       /* 0 VCJH with eta, 1 DG, 2 SD, 3 Hu, 4 c_+           */
   double eta;            /* used when vcjh_scheme == 0                         */
   int viscous;           /* 0 Euler, 1 Navier-Stokes                           */
-  int riemann;           /* 0 Rusanov (riemann_solve_type 0)                   */
+  int riemann;           /* riemann_solve_type: 0 Rusanov; 2 Roe (2-D only, as
+                            in the reference, src/inters.cpp:390-508)          */
   int precision;         /* 0 FP64 throughout; 1 FP32 traces/fluxes/operators
                             with FP64 state, RK register and reductions        */
   double gamma, prandtl, mu_inf, rt_inf, c_sth, fix_vis; /* gas + viscosity law */

@@ -797,6 +797,48 @@ static void rusanov(int D, int F, double g, const double* ul, const double* ur, 
   for (int k = 0; k < F; k++) fn[k] = 0.5 * ((fnl[k] + fnr[k]) - eig * (ur[k] - ul[k]));
 }
 
+/* inters::roe_flux, src/inters.cpp:390-508, in 2-D (the reference stops with
+ * "Roe not implemented in 3D"); static mesh, v_g = 0 */
+static void roe(double g, const double* ul, const double* ur, const double* n, double* fn)
+{
+  double vl[2] = {ul[1] / ul[0], ul[2] / ul[0]}, vr[2] = {ur[1] / ur[0], ur[2] / ur[0]};
+  double pl = (g - 1.0) * (ul[3] - (0.5 * ul[0] * ((vl[0] * vl[0]) + (vl[1] * vl[1]))));
+  double pr = (g - 1.0) * (ur[3] - (0.5 * ur[0] * ((vr[0] * vr[0]) + (vr[1] * vr[1]))));
+  double hl = (ul[3] + pl) / ul[0], hr = (ur[3] + pr) / ur[0];
+  double sq = sqrt(ur[0] / ul[0]);
+  double rr = 1. / (sq + 1.);
+  double um[2], usq = 0., unm = 0., vgn = 0., rl = 0., rrn = 0., du[4];
+  for (int i = 0; i < 2; i++) um[i] = rr * (vl[i] + sq * vr[i]);
+  double hm = rr * (hl + sq * hr);
+  for (int i = 0; i < 2; i++) usq += 0.5 * um[i] * um[i];
+  double am2 = (g - 1.) * (hm - usq);
+  double am = sqrt(am2);
+  for (int i = 0; i < 2; i++) { unm += um[i] * n[i]; vgn += 0.0 * n[i]; }
+  for (int i = 0; i < 2; i++) { rl += ul[i + 1] * n[i]; rrn += ur[i + 1] * n[i]; }
+  fn[0] = rl + rrn;
+  fn[1] = rl * vl[0] + rrn * vr[0] + (pl + pr) * n[0];
+  fn[2] = rl * vl[1] + rrn * vr[1] + (pl + pr) * n[1];
+  fn[3] = rl * hl + rrn * hr;
+  for (int i = 0; i < 4; i++) du[i] = ur[i] - ul[i];
+  double l0 = fabs(unm - vgn), lP = fabs(unm - vgn + am), lM = fabs(unm - vgn - am);
+  double eps = 0.5 * (fabs(rl / ul[0] - rrn / ur[0]) + fabs(sqrt(g * pl / ul[0]) - sqrt(g * pr / ur[0])));
+  if (l0 < 2. * eps) l0 = 0.25 * l0 * l0 / eps + eps;
+  if (lP < 2. * eps) lP = 0.25 * lP * lP / eps + eps;
+  if (lM < 2. * eps) lM = 0.25 * lM * lM / eps + eps;
+  double a2 = 0.5 * (lP + lM) - l0;
+  double a3 = 0.5 * (lP - lM) / am;
+  double a1 = a2 * (g - 1.) / am2;
+  double a4 = a3 * (g - 1.);
+  double a5 = usq * du[0] - um[0] * du[1] - um[1] * du[2] + du[3];
+  double a6 = unm * du[0] - n[0] * du[1] - n[1] * du[2];
+  double aL1 = a1 * a5 - a3 * a6, bL1 = a4 * a5 - a2 * a6;
+  fn[0] = fn[0] - (l0 * du[0] + aL1);
+  fn[1] = fn[1] - (l0 * du[1] + aL1 * um[0] + bL1 * n[0]);
+  fn[2] = fn[2] - (l0 * du[2] + aL1 * um[1] + bL1 * n[1]);
+  fn[3] = fn[3] - (l0 * du[3] + aL1 * hm + bL1 * unm);
+  for (int i = 0; i < 4; i++) fn[i] = 0.5 * fn[i] - 0.5 * vgn * (ur[i] + ul[i]);
+}
+
 /* sign switch shared by ldg_flux and ldg_solution, src/inters.cpp:555-564, 651-660 */
 static double ldg_beta(int D, double pen, const double* n)
 {
@@ -1020,7 +1062,8 @@ void or_residual(or_mesh* m, const or_physics* ph, const double* u, double* div,
     double ul[5], ur[5], n[3], fn[5];
     for (int k = 0; k < F; k++) { ul[k] = m->ufp[a + (size_t)nf * E * k]; ur[k] = m->ufp[b + (size_t)nf * E * k]; }
     for (int d = 0; d < D; d++) n[d] = m->nrm[a + (size_t)nf * E * d];
-    rusanov(D, F, g, ul, ur, n, fn);
+    if (ph->riemann == 2 && D == 2) roe(g, ul, ur, n, fn);
+    else rusanov(D, F, g, ul, ur, n, fn);
     double tl = m->tdA[a], tr = m->tdA[b];
     for (int k = 0; k < F; k++) {
       m->ntc[a + (size_t)nf * E * k] = fn[k] * tl;

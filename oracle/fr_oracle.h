@@ -35,6 +35,7 @@ typedef struct {
   double filter_ratio;   /* input key filter_ratio                         */
   const float* mlp;      /* sgs_model 5: parameters of the learned closure
                             (no reference counterpart; layout in mlp.py)    */
+  int riemann;           /* riemann_solve_type: 0 Rusanov, 2 Roe (2-D only) */
 } or_physics;
 
 /* Generic conforming mesh of one element type (4-node quads or 8-node hexes,

@@ -63,11 +63,11 @@ class Physics(C.Structure):
                 ("mu_inf", C.c_double), ("rt_inf", C.c_double), ("c_sth", C.c_double),
                 ("fix_vis", C.c_double), ("tau", C.c_double), ("pen_fact", C.c_double),
                 ("les", C.c_int), ("sgs_model", C.c_int), ("filter_ratio", C.c_double),
-                ("mlp", C.POINTER(C.c_float))]
+                ("mlp", C.POINTER(C.c_float)), ("riemann", C.c_int)]
 
 
 def physics(viscous=0, gamma=1.4, prandtl=0.72, mu_inf=0.0, rt_inf=1.0, c_sth=1.0, fix_vis=1.0,
-            tau=1.0, pen_fact=0.5, les=0, sgs_model=1, filter_ratio=1.0, mlp=None):
+            tau=1.0, pen_fact=0.5, les=0, sgs_model=1, filter_ratio=1.0, mlp=None, riemann=0):
     """mlp: float32 parameter vector of the learned closure (sgs_model 5); the
     returned structure keeps a reference to it."""
     ptr = None
@@ -75,7 +75,7 @@ def physics(viscous=0, gamma=1.4, prandtl=0.72, mu_inf=0.0, rt_inf=1.0, c_sth=1.
         mlp = np.ascontiguousarray(mlp, dtype=np.float32)
         ptr = mlp.ctypes.data_as(C.POINTER(C.c_float))
     ph = Physics(int(viscous), gamma, prandtl, mu_inf, rt_inf, c_sth, fix_vis, tau, pen_fact, int(les),
-                 int(sgs_model), float(filter_ratio), ptr)
+                 int(sgs_model), float(filter_ratio), ptr, int(riemann))
     ph._keep = mlp
     return ph
 

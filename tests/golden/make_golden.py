@@ -198,6 +198,11 @@ CASES = [
          ic="tgv_mach01", vcjh=2, jitter=0.0, steps=3, dt=1e-3, stages=True, les=1, sgs=0, filter_ratio=2.0),
     dict(name="quad_wale_p3_n6_jit", dims=2, order=3, n=(6, 6), lo=(-5, -5), hi=(5, 5), viscous=1,
          ic="vortex_u1v0", vcjh=1, jitter=0.15, steps=5, dt=1e-3, stages=True, les=1, sgs=1, filter_ratio=1.0),
+    # Roe common flux (riemann_solve_type 2; 2-D only in the reference)
+    dict(name="quad_vortex_roe_p3_n6_jit", dims=2, order=3, n=(6, 6), lo=(-5, -5), hi=(5, 5), viscous=0,
+         ic="vortex_u1v0", vcjh=1, jitter=0.15, steps=10, dt=1e-3, stages=True, riemann=2),
+    dict(name="quad_ns_roe_p2_n5", dims=2, order=2, n=(5, 5), lo=(-5, -5), hi=(5, 5), viscous=1,
+         ic="vortex_u1v0", vcjh=2, jitter=0.0, steps=5, dt=1e-3, stages=True, riemann=2),
 ]
 
 
@@ -218,6 +223,7 @@ def run_case(ref, c, work):
         "prandtl": 0.71, "Mach_free_stream": 0.1, "Re_free_stream": 1600.0, "gamma": 1.4, "fix_vis": 1,
         "res_norm_type": 1,
     }
+    vals["riemann_solve_type"] = c.get("riemann", 0)
     if c.get("les"):
         vals.update({"LES": 1, "filter_type": 0, "filter_ratio": "%.17g" % c["filter_ratio"],
                      "SGS_model": c["sgs"], "wall_model": 0, "wall_layer_thickness": 0.0})
@@ -301,7 +307,7 @@ def main():
         ph = O.physics(viscous=c["viscous"], gamma=par["gamma"], prandtl=par["prandtl"], mu_inf=par["mu_inf"],
                        rt_inf=par["rt_inf"], c_sth=par["c_sth"], fix_vis=par["fix_vis"], tau=par["tau"],
                        pen_fact=par["pen_fact"], les=c.get("les", 0), sgs_model=c.get("sgs", 1),
-                       filter_ratio=c.get("filter_ratio", 1.0))
+                       filter_ratio=c.get("filter_ratio", 1.0), riemann=c.get("riemann", 0))
         u0 = arr[T + "disu_upts_init"]
         pins = {}
         pins["metrics_detjac"] = rel(g["detjac_upts"], arr[T + "detjac_upts"])
@@ -347,7 +353,8 @@ def main():
         meta = {k: (list(v) if isinstance(v, tuple) else v) for k, v in c.items()}
         meta["physics"] = {k: par[k] for k in ("gamma", "prandtl", "mu_inf", "rt_inf", "c_sth", "fix_vis", "tau",
                                                  "pen_fact")}
-        meta["physics"].update(les=c.get("les", 0), sgs_model=c.get("sgs", 1), filter_ratio=c.get("filter_ratio", 1.0))
+        meta["physics"].update(les=c.get("les", 0), sgs_model=c.get("sgs", 1), filter_ratio=c.get("filter_ratio", 1.0),
+                               riemann=c.get("riemann", 0))
         meta["pins"] = pins
         meta["seed"] = 12345
         np.savez_compressed(os.path.join(HERE, c["name"] + ".npz"), meta=json.dumps(meta),

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from golden_util import CASES, GOLDEN, LES_CASES, load, rel
+from golden_util import CASES, GOLDEN, LES_CASES, ROE_CASES, load, rel
 
 
 def _mesh(meta):
@@ -46,7 +46,7 @@ def test_oracle_steps_match_reference(case):
     assert rel(nrm, a["norms"]) <= 1e-12
 
 
-@pytest.mark.parametrize("case", ["quad_vortex_p3_n6", "hex_tgv_p3_n3", "hex_tgv_p2_n3_jit"] + LES_CASES)
+@pytest.mark.parametrize("case", ["quad_vortex_p3_n6", "hex_tgv_p3_n3", "hex_tgv_p2_n3_jit"] + LES_CASES + ROE_CASES)
 def test_oracle_stage_arrays_match_reference(case):
     meta, a = load(case)
     m = _mesh(meta)
