@@ -41,6 +41,8 @@ struct or_mesh {
   double *pos_upts, *pos_fpts;                  /* (n, E, D) */
   double *detjac, *JG, *tdA, *nrm;
   int nint; int *il, *ir;                       /* interface fpts */
+  int nb; int* bf; unsigned char* bt;           /* boundary fpts: flat index, boundary type */
+  int* bct;                                     /* (E, nface) boundary type per face, 0 = matched */
   /* work arrays */
   double *ufp, *gup, *gfp, *tf, *ntd, *ntc, *ddu, *sgu, *sgf;
 };
@@ -492,9 +494,23 @@ static int build_interfaces(or_mesh* m, const double* shift)
   }
   double tol = 1e-6 * h;
   facerec* fr = malloc((size_t)E * nface * sizeof(facerec));
+  int nrec = 0, nbf = 0;
+  for (int e = 0; e < E; e++)
+    for (int fc = 0; fc < nface; fc++)
+      if (m->bct && m->bct[(size_t)e * nface + fc] > 0) nbf++;
+  m->nb = nbf * nfpf;
+  m->bf = malloc(sizeof(int) * (m->nb + 1)); m->bt = malloc(m->nb + 1);
+  nbf = 0;
   for (int e = 0; e < E; e++)
     for (int fc = 0; fc < nface; fc++) {
-      facerec* r = fr + (size_t)e * nface + fc;
+      if (m->bct && m->bct[(size_t)e * nface + fc] > 0) {   /* boundary face: its points in face order */
+        for (int q = 0; q < nfpf; q++) {
+          m->bf[nbf] = fc * nfpf + q + nf * e;
+          m->bt[nbf++] = (unsigned char)m->bct[(size_t)e * nface + fc];
+        }
+        continue;
+      }
+      facerec* r = fr + nrec++;
       r->e = e; r->face = fc;
       for (int d = 0; d < D; d++) {
         double s = 0;
@@ -504,13 +520,13 @@ static int build_interfaces(or_mesh* m, const double* shift)
       }
     }
   g_dims = D;
-  qsort(fr, (size_t)E * nface, sizeof(facerec), cmp_face);
-  int nint = E * nface / 2;
+  qsort(fr, (size_t)nrec, sizeof(facerec), cmp_face);
+  int nint = nrec / 2;
   m->nint = nint * nfpf;
-  m->il = malloc(sizeof(int) * m->nint); m->ir = malloc(sizeof(int) * m->nint);
+  m->il = malloc(sizeof(int) * (m->nint + 1)); m->ir = malloc(sizeof(int) * (m->nint + 1));
   int k = 0;
-  for (int i = 0; i < E * nface; i += 2) {
-    if (i + 1 >= E * nface || cmp_face(fr + i, fr + i + 1) != 0) { fprintf(stderr, "oracle: unmatched face\n"); free(fr); return -1; }
+  for (int i = 0; i < nrec; i += 2) {
+    if (i + 1 >= nrec || cmp_face(fr + i, fr + i + 1) != 0) { fprintf(stderr, "oracle: unmatched face\n"); free(fr); return -1; }
     facerec *a = fr + i, *b = fr + i + 1;
     if (b->e < a->e || (b->e == a->e && b->face < a->face)) { facerec* t = a; a = b; b = t; }
     for (int q = 0; q < nfpf; q++) {
@@ -575,12 +591,22 @@ static void alloc_work(or_mesh* m)
 or_mesh* or_mesh_new(int dims, int order, int n_verts, const double* xv, int n_eles, const int* c2v,
                      const double* shift, int upts_type, int vcjh_scheme, double eta)
 {
+  return or_mesh_new_bc(dims, order, n_verts, xv, n_eles, c2v, shift, NULL, upts_type, vcjh_scheme, eta);
+}
+
+or_mesh* or_mesh_new_bc(int dims, int order, int n_verts, const double* xv, int n_eles, const int* c2v,
+                        const double* shift, const int* bctype, int upts_type, int vcjh_scheme, double eta)
+{
   or_mesh* m = mesh_core(dims, order, upts_type, vcjh_scheme, eta);
   if (!m) return NULL;
   int nsp = 1 << dims;
   m->nv = n_verts; m->ne = n_eles;
   m->xv = malloc(sizeof(double) * dims * n_verts); memcpy(m->xv, xv, sizeof(double) * dims * n_verts);
   m->c2v = malloc(sizeof(int) * nsp * n_eles); memcpy(m->c2v, c2v, sizeof(int) * nsp * n_eles);
+  if (bctype) {
+    m->bct = malloc(sizeof(int) * 2 * dims * n_eles);
+    memcpy(m->bct, bctype, sizeof(int) * 2 * dims * n_eles);
+  }
   if (build_metrics(m) || build_interfaces(m, shift)) { or_mesh_free(m); return NULL; }
   alloc_work(m);
   return m;
@@ -588,6 +614,12 @@ or_mesh* or_mesh_new(int dims, int order, int n_verts, const double* xv, int n_e
 
 or_mesh* or_box_new(int dims, int order, const int* n, const double* lo, const double* hi,
                     double jitter, unsigned long long seed, int upts_type, int vcjh_scheme, double eta)
+{
+  return or_box_new_bc(dims, order, n, lo, hi, jitter, seed, NULL, upts_type, vcjh_scheme, eta);
+}
+
+or_mesh* or_box_new_bc(int dims, int order, const int* n, const double* lo, const double* hi, double jitter,
+                       unsigned long long seed, const int* side_bc, int upts_type, int vcjh_scheme, double eta)
 {
   int nx = n[0], ny = n[1], nz = dims == 3 ? n[2] : 1;
   int vx = nx + 1, vy = ny + 1, vz = dims == 3 ? nz + 1 : 1;
@@ -622,8 +654,32 @@ or_mesh* or_box_new(int dims, int order, const int* n, const double* lo, const d
       }
   double shift[3] = {0, 0, 0};
   for (int d = 0; d < dims; d++) shift[d] = hi[d] - lo[d];
-  or_mesh* m = or_mesh_new(dims, order, nv, xv, ne, c2v, shift, upts_type, vcjh_scheme, eta);
-  free(xv); free(c2v);
+  int* bct = NULL;
+  if (side_bc) {
+    /* local face of each box side: quads y- 0, x+ 1, y+ 2, x- 3; hexes z- 0,
+     * y- 1, x+ 2, y+ 3, x- 4, z+ 5 (the reference's face numbering) */
+    static const int q_face[4] = {3, 1, 0, 2}, h_face[6] = {4, 2, 1, 3, 0, 5};
+    int nface = 2 * dims;
+    bct = calloc((size_t)ne * nface, sizeof(int));
+    for (int d = 0; d < dims; d++)
+      if (side_bc[2 * d] > 0 || side_bc[2 * d + 1] > 0) shift[d] = 0.0;
+    for (int k = 0; k < nz; k++)
+      for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) {
+          int e = i + nx * (j + ny * k), ijk[3] = {i, j, k}, nn[3] = {nx, ny, nz};
+          for (int d = 0; d < dims; d++)
+            for (int sd = 0; sd < 2; sd++) {
+              int bc = side_bc[2 * d + sd];
+              if (bc <= 0) continue;
+              if ((sd == 0 && ijk[d] == 0) || (sd == 1 && ijk[d] == nn[d] - 1)) {
+                int fc = dims == 2 ? q_face[2 * d + sd] : h_face[2 * d + sd];
+                bct[(size_t)e * nface + fc] = bc;
+              }
+            }
+        }
+  }
+  or_mesh* m = or_mesh_new_bc(dims, order, nv, xv, ne, c2v, shift, bct, upts_type, vcjh_scheme, eta);
+  free(xv); free(c2v); free(bct);
   return m;
 }
 
@@ -636,10 +692,17 @@ void or_mesh_free(or_mesh* m)
   for (int d = 0; d < 3; d++) { op_free(&m->opp1[d]); op_free(&m->opp2[d]); op_free(&m->opp5[d]); }
   free(m->loc_upts); free(m->tloc_fpts); free(m->tnorm_fpts); free(m->xv); free(m->c2v);
   free(m->pos_upts); free(m->pos_fpts); free(m->detjac); free(m->JG); free(m->tdA); free(m->nrm);
-  free(m->il); free(m->ir);
+  free(m->il); free(m->ir); free(m->bf); free(m->bt); free(m->bct);
   free(m->ufp); free(m->gup); free(m->gfp); free(m->tf); free(m->ntd); free(m->ntc); free(m->ddu);
   free(m->sgu); free(m->sgf);
   free(m);
+}
+
+int or_n_boundary(const or_mesh* m) { return m->nb; }
+
+void or_get_boundary(const or_mesh* m, int* fpt_idx, int* type)
+{
+  for (int i = 0; i < m->nb; i++) { fpt_idx[i] = m->bf[i]; type[i] = m->bt[i]; }
 }
 
 void or_sizes(const or_mesh* m, int* o)
@@ -675,7 +738,7 @@ void or_set_geometry(or_mesh* m, const double* detjac, const double* JG, const d
 
 void or_set_interfaces(or_mesh* m, int n, const int* l, const int* r)
 {
-  free(m->il); free(m->ir);
+  free(m->il); free(m->ir); free(m->bf); free(m->bt); free(m->bct);
   m->nint = n;
   m->il = malloc(sizeof(int) * n); m->ir = malloc(sizeof(int) * n);
   memcpy(m->il, l, sizeof(int) * n); memcpy(m->ir, r, sizeof(int) * n);
@@ -837,6 +900,175 @@ static void roe(double g, const double* ul, const double* ur, const double* n, d
   fn[2] = fn[2] - (l0 * du[2] + aL1 * um[1] + bL1 * n[1]);
   fn[3] = fn[3] - (l0 * du[3] + aL1 * hm + bL1 * unm);
   for (int i = 0; i < 4; i++) fn[i] = 0.5 * fn[i] - 0.5 * vgn * (ur[i] + ul[i]);
+}
+
+/* Ghost state of a boundary flux point: bdy_inters::set_inv_boundary_conditions
+ * for the Navier-Stokes/Euler types, src/bdy_inters.cpp:391-860, static mesh
+ * (grid velocity v_g = 0), no turbulence model. */
+static void bc_ghost(int D, int type, const double* ul, const double* n, const or_physics* ph, double* ur)
+{
+  const double g = ph->gamma, R_ref = ph->R_ref;
+  const double* P = ph->bdy;
+  const double rho_bound = P[0], *v_bound = P + 1, p_bound = P[4], *v_wall = P + 5, T_wall = P[8];
+  const double vg[3] = {0.0, 0.0, 0.0};
+  double rho_l = ul[0], v_l[3], e_l = ul[D + 1], v_sq = 0., p_l, rho_r = 0, v_r[3] = {0, 0, 0}, e_r = 0, p_r, T_r, vn_l;
+  for (int i = 0; i < D; i++) v_l[i] = ul[i + 1] / ul[0];
+  for (int i = 0; i < D; i++) v_sq += (v_l[i] * v_l[i]);
+  p_l = (g - 1.0) * (e_l - 0.5 * rho_l * v_sq);
+  if (type == 1) {                           /* sub_in_simp */
+    rho_r = rho_bound;
+    for (int i = 0; i < D; i++) v_r[i] = v_bound[i];
+    p_r = p_l;
+    v_sq = 0.; for (int i = 0; i < D; i++) v_sq += (v_r[i] * v_r[i]);
+    e_r = (p_r / (g - 1.0)) + 0.5 * rho_r * v_sq;
+  } else if (type == 2) {                    /* sub_out_simp */
+    rho_r = rho_l;
+    for (int i = 0; i < D; i++) v_r[i] = v_l[i];
+    p_r = p_bound;
+    v_sq = 0.; for (int i = 0; i < D; i++) v_sq += (v_r[i] * v_r[i]);
+    e_r = (p_r / (g - 1.0)) + 0.5 * rho_r * v_sq;
+  } else if (type == 3) {                    /* sub_in_char */
+    double p_total_bound = P[9], T_total_bound = P[10];
+    const double* nfs = P + 11;
+    vn_l = 0.; for (int i = 0; i < D; i++) vn_l += v_l[i] * n[i];
+    double c_l = sqrt(g * p_l / rho_l);
+    double R_plus = vn_l + 2.0 * c_l / (g - 1.0);
+    double h_total = g * R_ref / (g - 1.0) * T_total_bound;
+    v_sq = 0.; for (int i = 0; i < D; i++) v_sq += v_l[i] * v_l[i];
+    double c_total_sq = (g - 1.0) * (h_total - (e_l / rho_l + p_l / rho_l) + 0.5 * v_sq) + c_l * c_l;
+    double alpha = 0.; for (int i = 0; i < D; i++) alpha += n[i] * nfs[i];
+    double aa = 1.0 + 0.5 * (g - 1.0) * alpha * alpha;
+    double bb = -(g - 1.0) * alpha * R_plus;
+    double cc = 0.5 * (g - 1.0) * R_plus * R_plus - 2.0 * c_total_sq / (g - 1.0);
+    double dd = bb * bb - 4.0 * aa * cc;
+    dd = sqrt(fmax(dd, 0.0));
+    double V_r = (-bb + dd) / (2.0 * aa);
+    V_r = fmax(V_r, 0.0);
+    v_sq = V_r * V_r;
+    double c_r_sq = c_total_sq - 0.5 * (g - 1.0) * v_sq;
+    double Mach_sq = v_sq / (c_r_sq);
+    Mach_sq = fmin(Mach_sq, 1.0);
+    v_sq = Mach_sq * c_r_sq;
+    V_r = sqrt(v_sq);
+    c_r_sq = c_total_sq - 0.5 * (g - 1.0) * v_sq;
+    for (int i = 0; i < D; i++) v_r[i] = V_r * nfs[i];
+    T_r = c_r_sq / (g * R_ref);
+    p_r = p_total_bound * pow(T_r / T_total_bound, g / (g - 1.0));
+    rho_r = p_r / (R_ref * T_r);
+    e_r = (p_r / (g - 1.0)) + 0.5 * rho_r * v_sq;
+  } else if (type == 4) {                    /* sub_out_char */
+    vn_l = 0.; for (int i = 0; i < D; i++) vn_l += v_l[i] * n[i];
+    double c_l = sqrt(g * p_l / rho_l);
+    double R_plus = vn_l + 2.0 * c_l / (g - 1.0);
+    double s = p_l / pow(rho_l, g);
+    p_r = p_bound;
+    rho_r = pow(p_r / s, 1.0 / g);
+    double c_r = sqrt(g * p_r / rho_r);
+    double vn_r = R_plus - 2.0 * c_r / (g - 1.0);
+    v_sq = 0.;
+    for (int i = 0; i < D; i++) { v_r[i] = v_l[i] + (vn_r - vn_l) * n[i]; v_sq += (v_r[i] * v_r[i]); }
+    e_r = (p_r / (g - 1.0)) + 0.5 * rho_r * v_sq;
+  } else if (type == 5) {                    /* sup_in */
+    rho_r = rho_bound;
+    for (int i = 0; i < D; i++) v_r[i] = v_bound[i];
+    p_r = p_bound;
+    v_sq = 0.; for (int i = 0; i < D; i++) v_sq += (v_r[i] * v_r[i]);
+    e_r = (p_r / (g - 1.0)) + 0.5 * rho_r * v_sq;
+  } else if (type == 6) {                    /* sup_out */
+    rho_r = rho_l;
+    for (int i = 0; i < D; i++) v_r[i] = v_l[i];
+    e_r = e_l;
+  } else if (type == 7) {                    /* slip_wall */
+    rho_r = rho_l;
+    vn_l = 0.; for (int i = 0; i < D; i++) vn_l += (v_l[i] - vg[i]) * n[i];
+    for (int i = 0; i < D; i++) v_r[i] = v_l[i] - 2.0 * vn_l * n[i];
+    e_r = e_l;
+  } else if (type == 11 || type == 13) {     /* isotherm_fix, isotherm_move */
+    p_r = p_l;
+    T_r = T_wall;
+    rho_r = p_r / (R_ref * T_r);
+    for (int i = 0; i < D; i++) v_r[i] = type == 11 ? vg[i] : v_wall[i] + vg[i];
+    v_sq = 0.; for (int i = 0; i < D; i++) v_sq += (v_r[i] * v_r[i]);
+    e_r = (p_r / (g - 1.0)) + 0.5 * rho_r * v_sq;
+  } else if (type == 12 || type == 14) {     /* adiabat_fix, adiabat_move */
+    rho_r = rho_l;
+    p_r = p_l;
+    for (int i = 0; i < D; i++) v_r[i] = type == 12 ? vg[i] : v_wall[i] + vg[i];
+    v_sq = 0.; for (int i = 0; i < D; i++) v_sq += (v_r[i] * v_r[i]);
+    e_r = (p_r / (g - 1.0)) + 0.5 * rho_r * v_sq;
+  } else if (type == 15) {                   /* char */
+    vn_l = 0.; for (int i = 0; i < D; i++) vn_l += v_l[i] * n[i];
+    double vn_bound = 0; for (int i = 0; i < D; i++) vn_bound += v_bound[i] * n[i];
+    double r_plus = vn_l + 2. / (g - 1.) * sqrt(g * p_l / rho_l);
+    double r_minus = vn_bound - 2. / (g - 1.) * sqrt(g * p_bound / rho_bound);
+    double c_star = 0.25 * (g - 1.) * (r_plus - r_minus);
+    double vn_star = 0.5 * (r_plus + r_minus);
+    if (vn_l < 0) {
+      double one_over_s = pow(rho_bound, g) / p_bound;
+      v_sq = 0.; for (int i = 0; i < D; i++) v_sq += v_bound[i] * v_bound[i];
+      double h_free_stream = g / (g - 1.) * p_bound / rho_bound + 0.5 * v_sq;
+      rho_r = pow(1. / g * (one_over_s * c_star * c_star), 1. / (g - 1.));
+      for (int i = 0; i < D; i++) v_r[i] = vn_star * n[i] + (v_bound[i] - vn_bound * n[i]);
+      p_r = rho_r / g * c_star * c_star;
+      e_r = rho_r * h_free_stream - p_r;
+    } else {
+      double one_over_s = pow(rho_l, g) / p_l;
+      rho_r = pow(1. / g * (one_over_s * c_star * c_star), 1. / (g - 1.));
+      for (int i = 0; i < D; i++) v_r[i] = vn_star * n[i] + (v_l[i] - vn_l * n[i]);
+      p_r = rho_r / g * c_star * c_star;
+      v_sq = 0.; for (int i = 0; i < D; i++) v_sq += (v_r[i] * v_r[i]);
+      e_r = (p_r / (g - 1.0)) + 0.5 * rho_r * v_sq;
+    }
+  } else if (type == 16) {                   /* slip_wall_dual */
+    rho_r = rho_l;
+    vn_l = 0.; for (int i = 0; i < D; i++) vn_l += v_l[i] * n[i];
+    for (int i = 0; i < D; i++) v_r[i] = v_l[i] - vn_l * n[i];
+    e_r = e_l;
+  }
+  ur[0] = rho_r;
+  for (int i = 0; i < D; i++) ur[i + 1] = rho_r * v_r[i];
+  ur[D + 1] = e_r;
+}
+
+/* bdy_inters::set_vis_boundary_conditions for the adiabatic walls (12, 14):
+ * the energy gradient of the ghost side is replaced so that the wall has no
+ * temperature gradient, src/bdy_inters.cpp:1062-1113.  g: (F, D), [k + F*d]. */
+static void bc_vis_gradient(int D, const or_physics* ph, const double* ul, const double* ur, double* g)
+{
+  int F = D + 2;
+  double v_sq = 0., gv[9];
+  for (int i = 0; i < D; i++) v_sq += (ul[i + 1] * ul[i + 1]);
+  double p_l = (ph->gamma - 1.0) * (ul[D + 1] - 0.5 * v_sq / ul[0]);
+  double p_r = p_l;
+  double inte = p_r / ((ph->gamma - 1.0) * ur[0]);
+  for (int j = 0; j < D; j++)
+    for (int i = 0; i < D; i++)
+      gv[j * D + i] = (g[(j + 1) + F * i] - g[0 + F * i] * ur[j + 1] / ur[0]) / ur[0];
+  for (int i = 0; i < D; i++) {
+    if (D == 2)
+      g[3 + F * i] = inte * g[0 + F * i] + 0.5 * ((ur[1] * ur[1] + ur[2] * ur[2]) / (ur[0] * ur[0])) * g[0 + F * i] +
+                     ur[0] * ((ur[1] / ur[0]) * gv[0 * D + i] + (ur[2] / ur[0]) * gv[1 * D + i]);
+    else
+      g[4 + F * i] = inte * g[0 + F * i] +
+                     0.5 * ((ur[1] * ur[1] + ur[2] * ur[2] + ur[3] * ur[3]) / (ur[0] * ur[0])) * g[0 + F * i] +
+                     ur[0] * ((ur[1] / ur[0]) * gv[0 * D + i] + (ur[2] / ur[0]) * gv[1 * D + i] +
+                              (ur[3] / ur[0]) * gv[2 * D + i]);
+  }
+}
+
+/* inters::ldg_flux with flux_spec 1 (Dirichlet: own flux) or 2 (von Neumann:
+ * ghost flux), src/inters.cpp:589-622, then the normal component. */
+static void ldg_flux_bdy(int D, int F, int spec, const double* ul, const double* ur, const double* fl,
+                         const double* fr, const double* n, double tau, double* fn)
+{
+  double fc[15];
+  const double* f = spec == 1 ? fl : fr;
+  for (int k = 0; k < F; k++)
+    for (int d = 0; d < D; d++) fc[k + F * d] = f[k + F * d] + tau * n[d] * (ul[k] - ur[k]);
+  for (int k = 0; k < F; k++) {
+    fn[k] = fc[k + F * 0] * n[0];
+    for (int l = 1; l < D; l++) fn[k] += fc[k + F * l] * n[l];
+  }
 }
 
 /* sign switch shared by ldg_flux and ldg_solution, src/inters.cpp:555-564, 651-660 */
@@ -1079,6 +1311,33 @@ void or_residual(or_mesh* m, const or_physics* ph, const double* u, double* div,
     }
     (void)ea; (void)eb;
   }
+  /* bdy_inters::evaluate_boundaryConditions_invFlux, src/bdy_inters.cpp:245-389 */
+  for (int i = 0; i < m->nb; i++) {
+    long a = m->bf[i];
+    int type = m->bt[i];
+    double ul[5], ur[5], n[3], fn[5], fl[15], fr[15];
+    for (int k = 0; k < F; k++) ul[k] = m->ufp[a + (size_t)nf * E * k];
+    for (int d = 0; d < D; d++) n[d] = m->nrm[a + (size_t)nf * E * d];
+    bc_ghost(D, type, ul, n, ph, ur);
+    invf(D, g, ul, fl); invf(D, g, ur, fr);
+    if (type == 16) {                        /* right_flux of the own flux, src/inters.cpp:299-308 */
+      for (int k = 0; k < F; k++) { fn[k] = 0.; for (int l = 0; l < D; l++) fn[k] += fl[k + F * l] * n[l]; }
+    } else if (ph->riemann == 2 && D == 2) {
+      roe(g, ul, ur, n, fn);
+    } else {                                 /* convective_flux_boundary, src/inters.cpp:368-387 */
+      for (int k = 0; k < F; k++) {
+        double a1 = 0., b1 = 0.;
+        for (int l = 0; l < D; l++) { a1 += fl[k + F * l] * n[l]; b1 += fr[k + F * l] * n[l]; }
+        fn[k] = 0.5 * (a1 + b1);
+      }
+    }
+    for (int k = 0; k < F; k++) m->ntc[a + (size_t)nf * E * k] = fn[k] * m->tdA[a];
+    if (ph->viscous)                         /* ldg_solution, flux_spec 1 or 2: u_c = (u_r + u_l)/2 */
+      for (int k = 0; k < F; k++) {
+        double uc = 0.5 * (ur[k] + ul[k]);
+        m->ddu[a + (size_t)nf * E * k] = (uc - ul[k]);
+      }
+  }
   if (ph->viscous) {
     /* correct_gradient, src/eles.cpp:1770-1968 */
     for (int d = 0; d < D; d++) op_apply(&m->opp5[d], m->ddu, m->gup + (size_t)nu * EF * d, EF, 1);
@@ -1168,9 +1427,33 @@ void or_residual(or_mesh* m, const or_physics* ph, const double* u, double* div,
         m->ntc[b + (size_t)nf * E * k] += -fn[k] * m->tdA[b];
       }
     }
+    /* bdy_inters::evaluate_boundaryConditions_viscFlux, src/bdy_inters.cpp:905-1057 */
+    for (int i = 0; i < m->nb; i++) {
+      long a = m->bf[i];
+      int type = m->bt[i], spec = (type == 12 || type == 14) ? 2 : 1;
+      double ul[5], ur[5], gl[15], gr[15], fl[15] = {0}, fr[15] = {0}, n[3], fn[5];
+      for (int k = 0; k < F; k++) {
+        ul[k] = m->ufp[a + (size_t)nf * E * k];
+        for (int d = 0; d < D; d++) gl[k + F * d] = m->gfp[a + (size_t)nf * E * (k + (size_t)F * d)];
+      }
+      for (int d = 0; d < D; d++) n[d] = m->nrm[a + (size_t)nf * E * d];
+      bc_ghost(D, type, ul, n, ph, ur);
+      if (spec == 2) {
+        for (int q = 0; q < F * D; q++) gr[q] = gl[q];
+        bc_vis_gradient(D, ph, ul, ur, gr);
+        visf(D, ph, ur, gr, fr);
+      } else {
+        visf(D, ph, ul, gl, fl);
+      }
+      if (ph->les)
+        for (int d = 0; d < D; d++)
+          for (int k = 0; k < F; k++) fl[k + F * d] += m->sgf[a + (size_t)nf * E * (k + (size_t)F * d)];
+      ldg_flux_bdy(D, F, spec, ul, ur, fl, fr, n, ph->tau, fn);
+      for (int k = 0; k < F; k++) m->ntc[a + (size_t)nf * E * k] += fn[k] * m->tdA[a];
+    }
   }
   if (stages) {
-    long long off[8]; or_stage_offsets(m, off);
+    long long off[10]; or_stage_offsets(m, off);
     memcpy(stages + off[0], m->ufp, sizeof(double) * nf * EF);
     if (ph->viscous) {
       memcpy(stages + off[1], m->gup, sizeof(double) * nu * EF * D);

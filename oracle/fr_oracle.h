@@ -36,6 +36,11 @@ typedef struct {
   const float* mlp;      /* sgs_model 5: parameters of the learned closure
                             (no reference counterpart; layout in mlp.py)    */
   int riemann;           /* riemann_solve_type: 0 Rusanov, 2 Roe (2-D only) */
+  double bdy[14];        /* boundary parameters in bdy_inters::set_bdy_params
+                            order (src/bdy_inters.cpp:78-110): rho_bound,
+                            v_bound[3], p_bound, v_wall[3], T_wall,
+                            p_total_bound, T_total_bound, n_free_stream[3]   */
+  double R_ref;          /* gas constant in reference units                 */
 } or_physics;
 
 /* Generic conforming mesh of one element type (4-node quads or 8-node hexes,
@@ -54,6 +59,21 @@ or_mesh* or_mesh_new(int dims, int order, int n_verts, const double* xv /* (n_ve
  * +-jitter*h (a 64-bit LCG, so the same seed gives the same mesh everywhere). */
 or_mesh* or_box_new(int dims, int order, const int* n, const double* lo, const double* hi,
                     double jitter, unsigned long long seed, int upts_type, int vcjh_scheme, double eta);
+
+/* Variants with boundaries.  bctype (n_eles, 2*dims): reference boundary
+ * type of each local face (src/geometry.cpp:121-148: 1 sub_in_simp,
+ * 2 sub_out_simp, 3 sub_in_char, 4 sub_out_char, 5 sup_in, 6 sup_out,
+ * 7 slip_wall, 11 isotherm_fix, 12 adiabat_fix, 13 isotherm_move,
+ * 14 adiabat_move, 15 char, 16 slip_wall_dual), 0 = matched with another
+ * face.  side_bc (2*dims): type of the box sides x-, x+, y-, y+, z-, z+;
+ * 0 = periodic pair. */
+or_mesh* or_mesh_new_bc(int dims, int order, int n_verts, const double* xv, int n_eles, const int* c2v,
+                        const double* shift, const int* bctype, int upts_type, int vcjh_scheme, double eta);
+or_mesh* or_box_new_bc(int dims, int order, const int* n, const double* lo, const double* hi, double jitter,
+                       unsigned long long seed, const int* side_bc, int upts_type, int vcjh_scheme, double eta);
+/* Number of boundary flux points; their flat indices (fpt + n_fpts*ele) and types. */
+int or_n_boundary(const or_mesh* m);
+void or_get_boundary(const or_mesh* m, int* fpt_idx, int* type);
 
 void or_mesh_free(or_mesh* m);
 

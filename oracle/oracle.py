@@ -28,6 +28,12 @@ def _lib():
     P = C.c_void_p
     dp = C.POINTER(C.c_double)
     ip = C.POINTER(C.c_int)
+    lib.or_box_new_bc.restype = P
+    lib.or_box_new_bc.argtypes = [C.c_int, C.c_int, ip, dp, dp, C.c_double, C.c_ulonglong, ip, C.c_int, C.c_int,
+                                  C.c_double]
+    lib.or_n_boundary.restype = C.c_int
+    lib.or_n_boundary.argtypes = [P]
+    lib.or_get_boundary.argtypes = [P, ip, ip]
     lib.or_box_new.restype = P
     lib.or_box_new.argtypes = [C.c_int, C.c_int, ip, dp, dp, C.c_double, C.c_ulonglong, C.c_int, C.c_int, C.c_double]
     lib.or_mesh_new.restype = P
@@ -63,11 +69,12 @@ class Physics(C.Structure):
                 ("mu_inf", C.c_double), ("rt_inf", C.c_double), ("c_sth", C.c_double),
                 ("fix_vis", C.c_double), ("tau", C.c_double), ("pen_fact", C.c_double),
                 ("les", C.c_int), ("sgs_model", C.c_int), ("filter_ratio", C.c_double),
-                ("mlp", C.POINTER(C.c_float)), ("riemann", C.c_int)]
+                ("mlp", C.POINTER(C.c_float)), ("riemann", C.c_int), ("bdy", C.c_double * 14),
+                ("R_ref", C.c_double)]
 
 
 def physics(viscous=0, gamma=1.4, prandtl=0.72, mu_inf=0.0, rt_inf=1.0, c_sth=1.0, fix_vis=1.0,
-            tau=1.0, pen_fact=0.5, les=0, sgs_model=1, filter_ratio=1.0, mlp=None, riemann=0):
+            tau=1.0, pen_fact=0.5, les=0, sgs_model=1, filter_ratio=1.0, mlp=None, riemann=0, bdy=None, R_ref=1.0):
     """mlp: float32 parameter vector of the learned closure (sgs_model 5); the
     returned structure keeps a reference to it."""
     ptr = None
@@ -75,7 +82,8 @@ def physics(viscous=0, gamma=1.4, prandtl=0.72, mu_inf=0.0, rt_inf=1.0, c_sth=1.
         mlp = np.ascontiguousarray(mlp, dtype=np.float32)
         ptr = mlp.ctypes.data_as(C.POINTER(C.c_float))
     ph = Physics(int(viscous), gamma, prandtl, mu_inf, rt_inf, c_sth, fix_vis, tau, pen_fact, int(les),
-                 int(sgs_model), float(filter_ratio), ptr, int(riemann))
+                 int(sgs_model), float(filter_ratio), ptr, int(riemann),
+                 (C.c_double * 14)(*(list(bdy) if bdy is not None else [0.0] * 14)), float(R_ref))
     ph._keep = mlp
     return ph
 
@@ -106,12 +114,26 @@ class Mesh:
         self.n_eles, self.n_upts, self.n_fpts, self.n_fields, self.dims, self.n_int = list(s)
 
     @classmethod
-    def box(cls, dims, order, n, lo, hi, jitter=0.0, seed=0, upts_type=0, vcjh_scheme=1, eta=0.0):
+    def box(cls, dims, order, n, lo, hi, jitter=0.0, seed=0, upts_type=0, vcjh_scheme=1, eta=0.0, side_bc=None):
+        """side_bc: boundary type of the sides x-, x+, y-, y+(, z-, z+); 0 = periodic."""
         n = np.ascontiguousarray(list(n) + [1] * (3 - len(n)), dtype=np.int32)
         lo = np.ascontiguousarray(list(lo) + [0.0] * (3 - len(lo)), dtype=np.float64)
         hi = np.ascontiguousarray(list(hi) + [0.0] * (3 - len(hi)), dtype=np.float64)
+        if side_bc is not None:
+            sb = np.ascontiguousarray(side_bc, dtype=np.int32)
+            return cls(lib().or_box_new_bc(dims, order, _ip(n), _dp(lo), _dp(hi), float(jitter), int(seed), _ip(sb),
+                                           upts_type, vcjh_scheme, float(eta)))
         return cls(lib().or_box_new(dims, order, _ip(n), _dp(lo), _dp(hi), float(jitter), int(seed),
                                     upts_type, vcjh_scheme, float(eta)))
+
+    def boundary(self):
+        """(flat flux-point index, boundary type) of every boundary flux point."""
+        nb = lib().or_n_boundary(self.h)
+        i = np.zeros(nb, dtype=np.int32)
+        t = np.zeros(nb, dtype=np.int32)
+        if nb:
+            lib().or_get_boundary(self.h, _ip(i), _ip(t))
+        return i, t
 
     @classmethod
     def from_vertices(cls, dims, order, xv, c2v, shift, upts_type=0, vcjh_scheme=1, eta=0.0):

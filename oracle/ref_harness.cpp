@@ -118,6 +118,20 @@ static void apply_ic(const string& ic, solution& S)
           double u = sin(x) * cos(y) * cos(z), v = -cos(x) * sin(y) * cos(z);
           q[0] = rho; q[1] = rho * u; q[2] = rho * v; q[3] = 0.0;
           q[4] = p / (gamma - 1.0) + 0.5 * rho * (u * u + v * v);
+        } else if (ic == "channel_mach01") {
+          // smooth non-uniform flow at the Mach 0.1 free stream of the
+          // non-dimensionalisation (rho = 1, u = 1, p = 1/(gamma M^2))
+          double M = 0.1, p0 = 1.0 / (gamma * M * M);
+          double rho = 1.0 + 0.05 * sin(x) * cos(y);
+          double u = 1.0 + 0.1 * sin(y), v = 0.1 * cos(x), w = 0.05 * sin(x + y + z);
+          double p = p0 * (1.0 + 0.01 * cos(x + y));
+          if (e->n_dims == 2) {
+            q[0] = rho; q[1] = rho * u; q[2] = rho * v;
+            q[3] = p / (gamma - 1.0) + 0.5 * rho * (u * u + v * v);
+          } else {
+            q[0] = rho; q[1] = rho * u; q[2] = rho * v; q[3] = rho * w;
+            q[4] = p / (gamma - 1.0) + 0.5 * rho * (u * u + v * v + w * w);
+          }
         } else {
           fprintf(stderr, "unknown --ic %s\n", ic.c_str()); exit(2);
         }
@@ -153,6 +167,9 @@ static void dump_setup(solution& S)
           run_input.gamma, run_input.mu_inf, run_input.prandtl, run_input.rt_inf,
           run_input.c_sth, run_input.fix_vis, run_input.tau, run_input.pen_fact,
           run_input.dt, run_input.viscous, run_input.order, S.n_dims, run_input.prandtl_t);
+  fprintf(f, "R_ref %.17g\n", run_input.R_ref);
+  if (S.n_bdy_inter_types > 0)
+    for (int i = 0; i < 14; i++) fprintf(f, "bdy%d %.17g\n", i, S.mesh_bdy_inters(0).bdy_params(i));
   for (int t = 0; t < S.n_ele_types; t++) {
     eles* e = S.mesh_eles(t);
     fprintf(f, "type %d ele_type %d n_eles %d n_upts %d n_fpts %d\n", t, e->ele_type,

@@ -84,15 +84,23 @@ def box_vertices(dims, n, lo, hi, jitter=0.0, seed=0):
     return xv, c2v
 
 
-def write_gambit(path, dims, xv, c2v, n):
+BC_NAMES = {1: "sub_in_simp", 2: "sub_out_simp", 3: "sub_in_char", 4: "sub_out_char", 5: "sup_in", 6: "sup_out",
+            7: "slip_wall", 11: "isotherm_fix", 12: "adiabat_fix", 13: "isotherm_move", 14: "adiabat_move",
+            15: "char", 16: "slip_wall_dual"}
+
+
+def write_gambit(path, dims, xv, c2v, n, side_bc=None):
     """Gambit neutral file.  Node order is chosen so that the reference's local
     axes (xi, eta, zeta) equal physical (x, y, z): the hex reader stores Gambit
     nodes 0..7 in c2v slots (0,2,4,6,1,3,5,7) (src/geometry.cpp:1840-1843) and
     the quad reader stores them in slots (0,1,3,2) (src/geometry.cpp:1800-1803)."""
     ne = c2v.shape[0]
+    side_bc = list(side_bc) if side_bc is not None else [0] * (2 * dims)
+    names = ["Cyclic" if b == 0 else BC_NAMES[b] for b in side_bc]
+    groups = sorted(set(names), key=names.index)
     lines = ["        CONTROL INFO 2.3.16", "** GAMBIT NEUTRAL FILE", "box", "PROGRAM:  fixture", "",
              "     NUMNP     NELEM     NGRPS    NBSETS     NDFCD     NDFVL",
-             "%10d%10d%10d%10d%10d%10d" % (xv.shape[0], ne, 1, 1, dims, dims),
+             "%10d%10d%10d%10d%10d%10d" % (xv.shape[0], ne, 1, len(groups), dims, dims),
              "ENDOFSECTION", "   NODAL COORDINATES 2.3.16"]
     for v in range(xv.shape[0]):
         lines.append("%10d " % (v + 1) + " ".join("%.17e" % c for c in xv[v]))
@@ -114,8 +122,7 @@ def write_gambit(path, dims, xv, c2v, n):
     ids = [str(e + 1) for e in range(ne)]
     for i in range(0, ne, 10):
         lines.append(" ".join("%7s" % x for x in ids[i:i + 10]))
-    lines += ["ENDOFSECTION", " BOUNDARY CONDITIONS 2.3.16"]
-    bnd = []
+    bnd = {g: [] for g in groups}
     nx, ny = n[0], n[1]
     nz = n[2] if dims == 3 else 1
     for k in range(nz):
@@ -123,20 +130,22 @@ def write_gambit(path, dims, xv, c2v, n):
             for i in range(nx):
                 e = i + nx * (j + ny * k) + 1
                 if dims == 3:   # Gambit hex faces: x- 5, x+ 6, y- 4, y+ 2, z- 1, z+ 3
-                    if i == 0: bnd.append((e, 4, 5))
-                    if i == nx - 1: bnd.append((e, 4, 6))
-                    if j == 0: bnd.append((e, 4, 4))
-                    if j == ny - 1: bnd.append((e, 4, 2))
-                    if k == 0: bnd.append((e, 4, 1))
-                    if k == nz - 1: bnd.append((e, 4, 3))
+                    if i == 0: bnd[names[0]].append((e, 4, 5))
+                    if i == nx - 1: bnd[names[1]].append((e, 4, 6))
+                    if j == 0: bnd[names[2]].append((e, 4, 4))
+                    if j == ny - 1: bnd[names[3]].append((e, 4, 2))
+                    if k == 0: bnd[names[4]].append((e, 4, 1))
+                    if k == nz - 1: bnd[names[5]].append((e, 4, 3))
                 else:           # Gambit quad faces: y- 1, x+ 2, y+ 3, x- 4
-                    if j == 0: bnd.append((e, 2, 1))
-                    if i == nx - 1: bnd.append((e, 2, 2))
-                    if j == ny - 1: bnd.append((e, 2, 3))
-                    if i == 0: bnd.append((e, 2, 4))
-    lines.append("%32s%8d%8d%8d%8d" % ("Cyclic", 1, len(bnd), 0, 6))
-    for b in bnd:
-        lines.append("%10d%5d%5d" % b)
+                    if j == 0: bnd[names[2]].append((e, 2, 1))
+                    if i == nx - 1: bnd[names[1]].append((e, 2, 2))
+                    if j == ny - 1: bnd[names[3]].append((e, 2, 3))
+                    if i == 0: bnd[names[0]].append((e, 2, 4))
+    for gi, g in enumerate(groups):
+        lines += ["ENDOFSECTION", " BOUNDARY CONDITIONS 2.3.16"]
+        lines.append("%32s%8d%8d%8d%8d" % (g, 1, len(bnd[g]), 0, 6))
+        for b in bnd[g]:
+            lines.append("%10d%5d%5d" % b)
     lines.append("ENDOFSECTION")
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
@@ -203,6 +212,19 @@ CASES = [
          ic="vortex_u1v0", vcjh=1, jitter=0.15, steps=10, dt=1e-3, stages=True, riemann=2),
     dict(name="quad_ns_roe_p2_n5", dims=2, order=2, n=(5, 5), lo=(-5, -5), hi=(5, 5), viscous=1,
          ic="vortex_u1v0", vcjh=2, jitter=0.0, steps=5, dt=1e-3, stages=True, riemann=2),
+    # boundary conditions (side types x-, x+, y-, y+, z-, z+; 0 = periodic)
+    dict(name="quad_bc_euler_p3", dims=2, order=3, n=(5, 4), lo=(-5, -5), hi=(5, 5), viscous=0,
+         ic="vortex_u1v0", vcjh=1, jitter=0.1, steps=10, dt=1e-3, stages=True, side_bc=(15, 4, 7, 16)),
+    dict(name="quad_bc_euler2_p2", dims=2, order=2, n=(4, 5), lo=(-5, -5), hi=(5, 5), viscous=0,
+         ic="vortex_u1v0", vcjh=2, jitter=0.1, steps=10, dt=1e-3, stages=True, side_bc=(1, 2, 5, 6)),
+    dict(name="quad_bc_roe_p3", dims=2, order=3, n=(4, 4), lo=(-5, -5), hi=(5, 5), viscous=0,
+         ic="vortex_u1v0", vcjh=1, jitter=0.1, steps=10, dt=1e-3, stages=True, side_bc=(15, 4, 7, 16), riemann=2),
+    dict(name="quad_ns_bc_p3", dims=2, order=3, n=(5, 4), lo=(0, 0), hi=(2 * np.pi, 2 * np.pi), viscous=1,
+         ic="channel_mach01", vcjh=1, jitter=0.1, steps=5, dt=1e-3, stages=True, side_bc=(3, 4, 13, 14)),
+    dict(name="hex_channel_p2", dims=3, order=2, n=(4, 3, 3), lo=(0, 0, 0), hi=(2 * np.pi,) * 3, viscous=1,
+         ic="channel_mach01", vcjh=1, jitter=0.1, steps=5, dt=1e-3, stages=True, side_bc=(0, 0, 11, 12, 0, 0)),
+    dict(name="hex_channel_char_p3", dims=3, order=3, n=(3, 2, 2), lo=(0, 0, 0), hi=(2 * np.pi,) * 3, viscous=1,
+         ic="channel_mach01", vcjh=1, jitter=0.0, steps=3, dt=1e-3, stages=True, side_bc=(15, 15, 11, 7, 0, 0)),
 ]
 
 
@@ -210,8 +232,11 @@ def run_case(ref, c, work):
     d = os.path.join(work, c["name"])
     os.makedirs(d, exist_ok=True)
     xv, c2v = box_vertices(c["dims"], c["n"], c["lo"], c["hi"], c["jitter"], seed=12345)
-    write_gambit(os.path.join(d, "mesh.neu"), c["dims"], xv, c2v, c["n"])
+    write_gambit(os.path.join(d, "mesh.neu"), c["dims"], xv, c2v, c["n"], c.get("side_bc"))
     L = [c["hi"][i] - c["lo"][i] for i in range(c["dims"])]
+    # the cyclic lengths stay the box lengths in every direction, walls too:
+    # with a zero length check_cyclic (src/geometry.cpp:3634-3664) matches a
+    # periodic face with itself and flips the orientation of the real pairs
     vals = {
         "equation": 0, "viscous": c["viscous"], "riemann_solve_type": 0, "vis_riemann_solve_type": 0,
         "ic_form": 7 if c["ic"].startswith("tgv") else 1, "order": c["order"], "dt_type": 0, "dt": c["dt"],
@@ -224,6 +249,11 @@ def run_case(ref, c, work):
         "res_norm_type": 1,
     }
     vals["riemann_solve_type"] = c.get("riemann", 0)
+    if c.get("side_bc"):
+        # free stream along x; inviscid runs take the boundary state as given
+        vals.update({"nx_free_stream": 1.0, "ny_free_stream": 0.0, "nz_free_stream": 0.0, "Mach_wall": 0.05,
+                     "nx_wall": 1.0, "ny_wall": 0.0, "nz_wall": 0.0, "rho_bound": 1.0, "u_bound": 1.0,
+                     "v_bound": 0.0, "w_bound": 0.0, "p_bound": 1.0, "T_wall": 300.0, "T_free_stream": 300.0})
     if c.get("les"):
         vals.update({"LES": 1, "filter_type": 0, "filter_ratio": "%.17g" % c["filter_ratio"],
                      "SGS_model": c["sgs"], "wall_model": 0, "wall_layer_thickness": 0.0})
@@ -299,7 +329,8 @@ def main():
         et = 1 if c["dims"] == 2 else 4
         T = "t%d_" % et
         m = O.Mesh.box(c["dims"], c["order"], c["n"], c["lo"], c["hi"], jitter=c["jitter"], seed=12345,
-                       vcjh_scheme=c["vcjh"])
+                       vcjh_scheme=c["vcjh"], side_bc=c.get("side_bc"))
+        bdy = [par.get("bdy%d" % i, 0.0) for i in range(14)]
         g = m.geometry()
         # 3. ordering check: the reference's solution points sit where ours do
         dpos = np.abs(arr[T + "pos_upts"] - g["pos_upts"]).max()
@@ -307,7 +338,8 @@ def main():
         ph = O.physics(viscous=c["viscous"], gamma=par["gamma"], prandtl=par["prandtl"], mu_inf=par["mu_inf"],
                        rt_inf=par["rt_inf"], c_sth=par["c_sth"], fix_vis=par["fix_vis"], tau=par["tau"],
                        pen_fact=par["pen_fact"], les=c.get("les", 0), sgs_model=c.get("sgs", 1),
-                       filter_ratio=c.get("filter_ratio", 1.0), riemann=c.get("riemann", 0))
+                       filter_ratio=c.get("filter_ratio", 1.0), riemann=c.get("riemann", 0), bdy=bdy,
+                       R_ref=par.get("R_ref", 1.0))
         u0 = arr[T + "disu_upts_init"]
         pins = {}
         pins["metrics_detjac"] = rel(g["detjac_upts"], arr[T + "detjac_upts"])
@@ -355,6 +387,8 @@ def main():
                                                  "pen_fact")}
         meta["physics"].update(les=c.get("les", 0), sgs_model=c.get("sgs", 1), filter_ratio=c.get("filter_ratio", 1.0),
                                riemann=c.get("riemann", 0))
+        if c.get("side_bc"):
+            meta["physics"].update(bdy=bdy, R_ref=par.get("R_ref", 1.0))
         meta["pins"] = pins
         meta["seed"] = 12345
         np.savez_compressed(os.path.join(HERE, c["name"] + ".npz"), meta=json.dumps(meta),

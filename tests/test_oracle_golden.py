@@ -10,12 +10,12 @@ import numpy as np
 import pytest
 
 import oracle as O
-from golden_util import CASES, GOLDEN, LES_CASES, ROE_CASES, load, rel
+from golden_util import BC_CASES, CASES, GOLDEN, LES_CASES, ROE_CASES, load, rel
 
 
 def _mesh(meta):
     return O.Mesh.box(meta["dims"], meta["order"], meta["n"], meta["lo"], meta["hi"], jitter=meta["jitter"],
-                      seed=meta["seed"], vcjh_scheme=meta["vcjh"])
+                      seed=meta["seed"], vcjh_scheme=meta["vcjh"], side_bc=meta.get("side_bc"))
 
 
 def _phys(meta):
@@ -29,7 +29,7 @@ def test_point_tables_match_reference():
             assert O.points_1d(int(p), 0 if kind == "gauss" else 1).tolist() == vals, (kind, p)
 
 
-@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("case", CASES + BC_CASES)
 def test_oracle_residual_matches_reference(case):
     meta, a = load(case)
     m = _mesh(meta)
@@ -37,7 +37,7 @@ def test_oracle_residual_matches_reference(case):
     assert rel(div, a["div0"]) <= 1e-14
 
 
-@pytest.mark.parametrize("case", [c for c in CASES if c != "quad_vortex_p3_n20"])
+@pytest.mark.parametrize("case", [c for c in CASES if c != "quad_vortex_p3_n20"] + BC_CASES)
 def test_oracle_steps_match_reference(case):
     meta, a = load(case)
     m = _mesh(meta)
@@ -46,7 +46,7 @@ def test_oracle_steps_match_reference(case):
     assert rel(nrm, a["norms"]) <= 1e-12
 
 
-@pytest.mark.parametrize("case", ["quad_vortex_p3_n6", "hex_tgv_p3_n3", "hex_tgv_p2_n3_jit"] + LES_CASES + ROE_CASES)
+@pytest.mark.parametrize("case", ["quad_vortex_p3_n6", "hex_tgv_p3_n3", "hex_tgv_p2_n3_jit"] + LES_CASES + ROE_CASES + BC_CASES)
 def test_oracle_stage_arrays_match_reference(case):
     meta, a = load(case)
     m = _mesh(meta)
