@@ -331,14 +331,16 @@ __host__ __device__ constexpr size_t grad_smem_bytes()
 // for; VEC = 0 keeps every global read element-sized (inputs only 8-byte
 // aligned), VEC = 1 uses 16-byte copies where the per-element runs allow.
 // Outputs VF (n_fpts, n_eles, F-1), ND (n_fpts, n_eles, F), DV (n_upts, n_eles, F),
-// and, when GRAD is not null, the corrected physical gradient
+// BV (n_boundary_points, F) the viscous normal flux at boundary points (side
+// bits 2.. hold the boundary type, mate = -1 - position in the boundary
+// list), and, when GRAD is not null, the corrected physical gradient
 // grad_disu_upts (n_upts, n_eles, F, D).
 template <int DIM, int P, int EPB, int NT, typename TC, int LES = 0, int MINB = 1, int VEC = 1>
 __global__ void __launch_bounds__(NT, MINB)
 fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const int* __restrict__ mate,
                const unsigned char* __restrict__ side, const TC* __restrict__ JG, const TC* __restrict__ detj,
                const TC* __restrict__ nL, TC* __restrict__ VF, TC* __restrict__ ND, TC* __restrict__ DV,
-               long long E, Line<TC> L, PhysT<TC> ph, TC* __restrict__ GRAD)
+               long long E, Line<TC> L, PhysT<TC> ph, TC* __restrict__ GRAD, TC* __restrict__ BV)
 {
   using S = Shape<DIM, P>;
   using G = GradPlan<DIM, P>;
@@ -394,8 +396,10 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
       size_t own = f + (size_t)NF * (e0 + el);
       int mt = mate[own];
       psd[it] = side[own];
+      if (mt >= 0) {                 // boundary points (mate < 0) have no neighbour trace
 #pragma unroll
-      for (int k = 0; k < F; k++) cp_async<sizeof(TC)>(&FR_SX(el, k, f), UF + mt + NFE * k);
+        for (int k = 0; k < F; k++) cp_async<sizeof(TC)>(&FR_SX(el, k, f), UF + mt + NFE * k);
+      }
     }
   }
   cp_async_commit();
@@ -407,8 +411,27 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
   for (int it = 0; it < IF; it++) {
     int w = threadIdx.x + it * NT, el = w / NF, f = w - el * NF;
     if (w >= EPB * NF || el >= nval) continue;
-    TC pen = (psd[it] & 2) ? -ph.pen_fact : ph.pen_fact;
     const int cd = B->code[f];
+    if (psd[it] >> 2) {
+      // boundary point: ghost state from the boundary condition, then
+      // ldg_solution with flux_spec 1 or 2, u_c = (u_r + u_l)/2
+      // (bdy_inters::evaluate_boundaryConditions_invFlux, src/bdy_inters.cpp:245-389)
+      TC uo[F], ug[F], nb[D];
+#pragma unroll
+      for (int k = 0; k < F; k++) uo[k] = interp_code<P, TC, TC>(L, cd, &FR_SU(el, k, 0));
+      const size_t own = f + (size_t)NF * (e0 + el);
+#pragma unroll
+      for (int d = 0; d < D; d++) nb[d] = nL[own + NFE * d];
+      bc_ghost<D, TC>(ph, psd[it] >> 2, uo, nb, ug);
+#pragma unroll
+      for (int k = 0; k < F; k++) {
+        TC uc = TC(0.5) * (ug[k] + uo[k]);
+        FR_SX(el, k, f) = uc - uo[k];
+        FR_SUF(el, k, f) = uo[k];
+      }
+      continue;
+    }
+    TC pen = (psd[it] & 2) ? -ph.pen_fact : ph.pen_fact;
 #pragma unroll
     for (int k = 0; k < F; k++) {
       TC uo = interp_code<P, TC, TC>(L, cd, &FR_SU(el, k, 0));
@@ -594,8 +617,35 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
     }
 #pragma unroll
     for (int d = 0; d < D; d++) n[d] = FR_SM(el, d * NF + f);
+    const int btype = psd[it] >> 2;
+    if (btype) {
+      // viscous normal flux of a boundary point, bdy_inters::evaluate_boundaryConditions_viscFlux
+      // (src/bdy_inters.cpp:905-1057): own flux (flux_spec 1) or the ghost
+      // side's with the adiabatic-wall energy gradient (flux_spec 2, types
+      // 12 and 14), plus tau n (u_l - u_r), on the normal
+      TC ug[F];
+      bc_ghost<D, TC>(ph, btype, uf, n, ug);
+      if (btype == 12 || btype == 14) {
+        TC gr[F][D];
 #pragma unroll
-    for (int k = 1; k < F; k++) VF[own + NFE * (k - 1)] = project<D, TC>(fv, k, n);
+        for (int k = 0; k < F; k++)
+#pragma unroll
+          for (int d = 0; d < D; d++) gr[k][d] = gf[k][d];
+        bc_vis_gradient<D, TC>(ph, uf, ug, gr);
+        vis_flux_fast<D, TC>(ph, ug, gr, fv);
+      }
+      const long long j = -1 - (long long)mate[own];
+#pragma unroll
+      for (int k = 0; k < F; k++) {
+        TC fnk = (fv[k][0] + ph.tau * n[0] * (uf[k] - ug[k])) * n[0];
+#pragma unroll
+        for (int d = 1; d < D; d++) fnk = fnk + (fv[k][d] + ph.tau * n[d] * (uf[k] - ug[k])) * n[d];
+        BV[j * F + k] = fnk;
+      }
+    } else {
+#pragma unroll
+      for (int k = 1; k < F; k++) VF[own + NFE * (k - 1)] = project<D, TC>(fv, k, n);
+    }
 #pragma unroll
     for (int k = 0; k < F; k++) {
       const TC* s = &FR_SFL(el, ax, k, 0);
@@ -623,15 +673,63 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
 // face[i] = (left flat index, right flat index) of interface point i;
 // fsign[i] != 0 when the LDG penalty sign is negative there.  RIEMANN is the
 // reference's riemann_solve_type: 0 Rusanov, 2 Roe (2-D).
+// Threads past nint take the boundary points: ghost state, inviscid common
+// flux of bdy_inters::evaluate_boundaryConditions_invFlux (central flux of the
+// two states, convective_flux_boundary, src/inters.cpp:368-387; Roe in 2-D
+// with RIEMANN 2; the own flux for slip_wall_dual, right_flux,
+// src/inters.cpp:299-308), plus the viscous part BV from the gradient kernel.
 template <int DIM, int VISC, typename TC, int RIEMANN = 0>
 __global__ void __launch_bounds__(128)
 fr_face_kernel(const int2* __restrict__ face, const unsigned char* __restrict__ fsign, long long nint,
                const TC* __restrict__ UF, const TC* __restrict__ VF, const TC* __restrict__ nL,
-               const TC* __restrict__ tdA, TC* __restrict__ CF, long long NFE, PhysT<TC> ph)
+               const TC* __restrict__ tdA, TC* __restrict__ CF, long long NFE, PhysT<TC> ph,
+               long long nbdy = 0, const int* __restrict__ bf = nullptr, const unsigned char* __restrict__ bt = nullptr,
+               const TC* __restrict__ BV = nullptr)
 {
   constexpr int F = DIM + 2, D = DIM;
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nint) return;
+  if (i >= nint) {
+    const long long j = i - nint;
+    if (j >= nbdy) return;
+    const long long a = bf[j];
+    const int type = bt[j];
+    TC ul[F], ug[F], n[D], fn[F];
+#pragma unroll
+    for (int k = 0; k < F; k++) ul[k] = UF[a + NFE * k];
+#pragma unroll
+    for (int d = 0; d < D; d++) n[d] = nL[a + NFE * d];
+    bc_ghost<D, TC>(ph, type, ul, n, ug);
+    TC fl[F][D], fr[F][D];
+    inv_flux<D, TC>(ph, ul, fl);
+    inv_flux<D, TC>(ph, ug, fr);
+    if (type == 16) {
+#pragma unroll
+      for (int k = 0; k < F; k++) {
+        TC s = fl[k][0] * n[0];
+#pragma unroll
+        for (int l = 1; l < D; l++) s = s + fl[k][l] * n[l];
+        fn[k] = s;
+      }
+    } else if (RIEMANN == 2 && DIM == 2) {
+      roe<TC>(ph, ul, ug, n, fn);
+    } else {
+#pragma unroll
+      for (int k = 0; k < F; k++) {
+        TC s = fl[k][0] * n[0], q = fr[k][0] * n[0];
+#pragma unroll
+        for (int l = 1; l < D; l++) { s = s + fl[k][l] * n[l]; q = q + fr[k][l] * n[l]; }
+        fn[k] = TC(0.5) * (s + q);
+      }
+    }
+    const TC tl = tdA[a];
+#pragma unroll
+    for (int k = 0; k < F; k++) {
+      TC c = fn[k] * tl;
+      if (VISC) c = c + BV[j * F + k] * tl;
+      CF[a + NFE * k] = c;
+    }
+    return;
+  }
   const int2 lr = face[i];
   const long long a = lr.x, b = lr.y;
   TC ul[F], ur[F], n[D];

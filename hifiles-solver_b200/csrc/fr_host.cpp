@@ -349,13 +349,22 @@ double wrap_coord(double c, double L, double lo)
 }
 }  // namespace
 
+constexpr int kUnwired = -2147483647 - 1;
+
 void finish_wiring(Mesh& m)
 {
   size_t E = m.ne;
   int D = m.dims, nf = m.nf;
-  m.mate.assign((size_t)nf * E, -1);
+  m.mate.assign((size_t)nf * E, kUnwired);
   m.is_left.assign((size_t)nf * E, 0);
   m.nL.assign((size_t)nf * E * D, 0.0);
+  for (size_t j = 0; j < m.bf.size(); j++) {   // boundary points: own side is the left one
+    long long a = m.bf[j];
+    m.mate[a] = -1 - (int)j;
+    m.is_left[a] = 1;
+    size_t ea = a / nf, fa = a % nf;
+    for (int d = 0; d < D; d++) m.nL[fa + nf * (ea + E * d)] = m.nrm[fa + nf * (ea + E * d)];
+  }
   for (size_t i = 0; i < m.il.size(); i++) {
     long long a = m.il[i], b = m.ir[i];
     m.mate[a] = (int)b; m.mate[b] = (int)a;
@@ -375,7 +384,7 @@ void finish_wiring(Mesh& m)
 // the left side.  This takes the place of CompConnectivity, the cyclic-face
 // search and the rotation look-up table of the reference
 // (src/geometry.cpp:2412-2720, 3489-3666; src/inters.cpp:187-296).
-static bool wire(Mesh& m, const double* shift, std::string& err)
+static bool wire(Mesh& m, const double* shift, const int* bctype, std::string& err)
 {
   int D = m.dims, nf = m.nf, nface = m.nface, nfpf = m.nfpf;
   size_t E = m.ne;
@@ -398,10 +407,19 @@ static bool wire(Mesh& m, const double* shift, std::string& err)
   };
   std::unordered_map<Key, long long, KeyHash> open;
   open.reserve(E * nface);
-  m.il.clear(); m.ir.clear();
+  m.il.clear(); m.ir.clear(); m.bf.clear(); m.bt.clear();
   m.il.reserve(E * nf / 2); m.ir.reserve(E * nf / 2);
   for (size_t e = 0; e < E; e++)
     for (int fc = 0; fc < nface; fc++) {
+      const int bc = bctype ? bctype[e * nface + fc] : 0;
+      if (bc != 0) {
+        if (!((bc >= 1 && bc <= 7) || (bc >= 11 && bc <= 16))) { err = "unknown boundary type"; return false; }
+        for (int q = 0; q < nfpf; q++) {
+          m.bf.push_back((int)(fc * nfpf + q + nf * e));
+          m.bt.push_back((unsigned char)bc);
+        }
+        continue;
+      }
       Key k{{0, 0, 0}};
       for (int d = 0; d < D; d++) {
         double s = 0;
@@ -430,15 +448,15 @@ static bool wire(Mesh& m, const double* shift, std::string& err)
         m.ir.push_back((int)(best + nf * e));
       }
     }
-  if (!open.empty()) { err = "unmatched faces (boundary conditions are not part of this path)"; return false; }
+  if (!open.empty()) { err = "unmatched faces without a boundary type"; return false; }
   finish_wiring(m);
   for (size_t i = 0; i < m.mate.size(); i++)
-    if (m.mate[i] < 0) { err = "flux points of a face pair do not map one to one"; return false; }
+    if (m.mate[i] == kUnwired) { err = "flux points of a face pair do not map one to one"; return false; }
   return true;
 }
 
 bool build_mesh(int dims, const Line1D& L, long long nv, const double* xv, long long ne, const int* c2v,
-                const double* shift, Mesh& m, std::string& err)
+                const double* shift, const int* bctype, Mesh& m, std::string& err)
 {
   if (dims != 2 && dims != 3) { err = "dims must be 2 or 3"; return false; }
   if (ne <= 0 || nv <= 0 || !xv || !c2v) { err = "empty mesh"; return false; }
@@ -454,7 +472,7 @@ bool build_mesh(int dims, const Line1D& L, long long nv, const double* xv, long 
   for (size_t i = 0; i < m.c2v.size(); i++)
     if (m.c2v[i] < 0 || m.c2v[i] >= nv) { err = "vertex index out of range"; return false; }
   if (!compute_metrics(m, L, err)) return false;
-  return wire(m, shift, err);
+  return wire(m, shift, bctype, err);
 }
 
 }  // namespace frb

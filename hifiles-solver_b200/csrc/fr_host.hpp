@@ -61,14 +61,20 @@ struct Mesh {
   std::vector<int> mate;                    // (nf, ne)
   std::vector<unsigned char> is_left;       // (nf, ne)
   std::vector<double> nL;                   // (nf, ne, dims)
+  // boundary flux points (faces given a boundary type): flat index, type;
+  // their mate is -1 - (position in this list)
+  std::vector<int> bf;
+  std::vector<unsigned char> bt;
 };
 
 // Local point sets (reference orderings) of the element type.
 void element_points(int dims, const Line1D& L, std::vector<double>& loc_upts, std::vector<double>& tloc_fpts,
                     std::vector<double>& tnorm_fpts);
 
+// bctype (ne, 2*dims) or null: reference boundary type of each local face
+// (0 = matched with another face).
 bool build_mesh(int dims, const Line1D& L, long long nv, const double* xv, long long ne, const int* c2v,
-                const double* shift, Mesh& m, std::string& err);
+                const double* shift, const int* bctype, Mesh& m, std::string& err);
 
 // Recompute the per-fpt interface data (mate, is_left, nL) after the metrics
 // were replaced.

@@ -127,7 +127,7 @@ fr_status run(const fr_residual_args* a, double* scratch, cudaStream_t s)
       cudaFuncSetAttribute(fr_grad_kernel<DIM, P, EPB, NT, double, 0, 1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)sm);
     fr_grad_kernel<DIM, P, EPB, NT, double, 0, 1, 0><<<nblk, NT, sm, s>>>(a->disu_upts, UF, a->mate, a->side, a->JGinv_upts,
-                                                                  a->detjac_upts, a->norm_left, VF, ND, DV, E, L, ph, nullptr);
+                                                                  a->detjac_upts, a->norm_left, VF, ND, DV, E, L, ph, nullptr, nullptr);
   }
   if (a->n_int > 0) {
     unsigned g = (unsigned)((a->n_int + 127) / 128);

@@ -23,6 +23,8 @@ struct Phys {
   int sgs_model = 1;          // eddy-viscosity LES: 0 Smagorinsky, 1 WALE, 5 learned (fr_mlp.cuh)
   double filter_ratio = 1.0;  // LES filter width over the element's point spacing
   const float* mlp = nullptr; // device parameters of the learned closure (sgs_model 5)
+  double bdy[14] = {};        // boundary values (bdy_inters::set_bdy_params order)
+  double R_ref = 1.0;
 };
 
 template <typename T>
@@ -30,12 +32,15 @@ struct PhysT {
   T gamma, gm1, prandtl, mu_inf, rt_inf, c_sth, fix_vis, tau, pen_fact, filter_ratio;
   int sgs_model;
   const float* mlp;
+  T bdy[14], R_ref;
   __host__ __device__ static PhysT make(const Phys& p) {
     PhysT q;
     q.gamma = (T)p.gamma; q.gm1 = (T)(p.gamma - 1.0); q.prandtl = (T)p.prandtl; q.mu_inf = (T)p.mu_inf;
     q.rt_inf = (T)p.rt_inf; q.c_sth = (T)p.c_sth; q.fix_vis = (T)p.fix_vis; q.tau = (T)p.tau;
     q.pen_fact = (T)p.pen_fact; q.filter_ratio = (T)p.filter_ratio; q.sgs_model = p.sgs_model;
     q.mlp = p.mlp;
+    for (int i = 0; i < 14; i++) q.bdy[i] = (T)p.bdy[i];
+    q.R_ref = (T)p.R_ref;
     return q;
   }
 };
@@ -282,6 +287,220 @@ __device__ __forceinline__ void roe(const PhysT<T>& ph, const T* ul, const T* ur
   fn[1] = T(0.5) * f1 - T(0.5) * vgn * (ur[1] + ul[1]);
   fn[2] = T(0.5) * f2 - T(0.5) * vgn * (ur[2] + ul[2]);
   fn[3] = T(0.5) * f3 - T(0.5) * vgn * (ur[3] + ul[3]);
+}
+
+template <typename T> __device__ __forceinline__ T fr_pow(T x, T y);
+template <> __device__ __forceinline__ double fr_pow<double>(double x, double y) { return pow(x, y); }
+template <> __device__ __forceinline__ float fr_pow<float>(float x, float y) { return powf(x, y); }
+
+// Ghost state of a boundary flux point: bdy_inters::set_inv_boundary_conditions
+// for the Euler/Navier-Stokes types, src/bdy_inters.cpp:391-860; static mesh
+// (grid velocity 0), no turbulence model.  Types (get_bc_number,
+// src/geometry.cpp:121-148): 1 sub_in_simp, 2 sub_out_simp, 3 sub_in_char,
+// 4 sub_out_char, 5 sup_in, 6 sup_out, 7 slip_wall, 11 isotherm_fix,
+// 12 adiabat_fix, 13 isotherm_move, 14 adiabat_move, 15 char,
+// 16 slip_wall_dual.  ph.bdy holds rho_bound, v_bound[3], p_bound,
+// v_wall[3], T_wall, p_total_bound, T_total_bound, n_free_stream[3].
+template <int D, typename T>
+__device__ __forceinline__ void bc_ghost(const PhysT<T>& ph, int type, const T* ul, const T* n, T* ur)
+{
+  const T g = ph.gamma, R_ref = ph.R_ref;
+  const T rho_bound = ph.bdy[0], p_bound = ph.bdy[4], T_wall = ph.bdy[8];
+  const T rho_l = ul[0], e_l = ul[D + 1];
+  T v_l[D], v_r[D], v_sq = T(0.), rho_r = T(0), e_r = T(0), p_r, vn_l;
+#pragma unroll
+  for (int i = 0; i < D; i++) { v_l[i] = ul[i + 1] / ul[0]; v_r[i] = T(0); }
+#pragma unroll
+  for (int i = 0; i < D; i++) v_sq = v_sq + (v_l[i] * v_l[i]);
+  const T p_l = (g - T(1.0)) * (e_l - T(0.5) * rho_l * v_sq);
+  auto energy = [&](void) {
+    T s = T(0.);
+#pragma unroll
+    for (int i = 0; i < D; i++) s = s + (v_r[i] * v_r[i]);
+    e_r = (p_r / (g - T(1.0))) + T(0.5) * rho_r * s;
+  };
+  switch (type) {
+    case 1:                                   // sub_in_simp
+      rho_r = rho_bound;
+#pragma unroll
+      for (int i = 0; i < D; i++) v_r[i] = ph.bdy[1 + i];
+      p_r = p_l;
+      energy();
+      break;
+    case 2:                                   // sub_out_simp
+      rho_r = rho_l;
+#pragma unroll
+      for (int i = 0; i < D; i++) v_r[i] = v_l[i];
+      p_r = p_bound;
+      energy();
+      break;
+    case 3: {                                 // sub_in_char
+      const T p_total_bound = ph.bdy[9], T_total_bound = ph.bdy[10];
+      vn_l = T(0.);
+#pragma unroll
+      for (int i = 0; i < D; i++) vn_l = vn_l + v_l[i] * n[i];
+      const T c_l = fr_sqrt<T>(g * p_l / rho_l);
+      const T R_plus = vn_l + T(2.0) * c_l / (g - T(1.0));
+      const T h_total = g * R_ref / (g - T(1.0)) * T_total_bound;
+      T vs = T(0.);
+#pragma unroll
+      for (int i = 0; i < D; i++) vs = vs + v_l[i] * v_l[i];
+      const T c_total_sq = (g - T(1.0)) * (h_total - (e_l / rho_l + p_l / rho_l) + T(0.5) * vs) + c_l * c_l;
+      T alpha = T(0.);
+#pragma unroll
+      for (int i = 0; i < D; i++) alpha = alpha + n[i] * ph.bdy[11 + i];
+      const T aa = T(1.0) + T(0.5) * (g - T(1.0)) * alpha * alpha;
+      const T bb = -(g - T(1.0)) * alpha * R_plus;
+      const T cc = T(0.5) * (g - T(1.0)) * R_plus * R_plus - T(2.0) * c_total_sq / (g - T(1.0));
+      T dd = bb * bb - T(4.0) * aa * cc;
+      dd = fr_sqrt<T>(dd > T(0.0) ? dd : T(0.0));
+      T V_r = (-bb + dd) / (T(2.0) * aa);
+      V_r = V_r > T(0.0) ? V_r : T(0.0);
+      vs = V_r * V_r;
+      T c_r_sq = c_total_sq - T(0.5) * (g - T(1.0)) * vs;
+      T Mach_sq = vs / (c_r_sq);
+      Mach_sq = Mach_sq < T(1.0) ? Mach_sq : T(1.0);
+      vs = Mach_sq * c_r_sq;
+      V_r = fr_sqrt<T>(vs);
+      c_r_sq = c_total_sq - T(0.5) * (g - T(1.0)) * vs;
+#pragma unroll
+      for (int i = 0; i < D; i++) v_r[i] = V_r * ph.bdy[11 + i];
+      const T T_r = c_r_sq / (g * R_ref);
+      p_r = p_total_bound * fr_pow<T>(T_r / T_total_bound, g / (g - T(1.0)));
+      rho_r = p_r / (R_ref * T_r);
+      e_r = (p_r / (g - T(1.0))) + T(0.5) * rho_r * vs;
+      break;
+    }
+    case 4: {                                 // sub_out_char
+      vn_l = T(0.);
+#pragma unroll
+      for (int i = 0; i < D; i++) vn_l = vn_l + v_l[i] * n[i];
+      const T c_l = fr_sqrt<T>(g * p_l / rho_l);
+      const T R_plus = vn_l + T(2.0) * c_l / (g - T(1.0));
+      const T s = p_l / fr_pow<T>(rho_l, g);
+      p_r = p_bound;
+      rho_r = fr_pow<T>(p_r / s, T(1.0) / g);
+      const T c_r = fr_sqrt<T>(g * p_r / rho_r);
+      const T vn_r = R_plus - T(2.0) * c_r / (g - T(1.0));
+      T vs = T(0.);
+#pragma unroll
+      for (int i = 0; i < D; i++) {
+        v_r[i] = v_l[i] + (vn_r - vn_l) * n[i];
+        vs = vs + (v_r[i] * v_r[i]);
+      }
+      e_r = (p_r / (g - T(1.0))) + T(0.5) * rho_r * vs;
+      break;
+    }
+    case 5:                                   // sup_in
+      rho_r = rho_bound;
+#pragma unroll
+      for (int i = 0; i < D; i++) v_r[i] = ph.bdy[1 + i];
+      p_r = p_bound;
+      energy();
+      break;
+    case 6:                                   // sup_out
+      rho_r = rho_l;
+#pragma unroll
+      for (int i = 0; i < D; i++) v_r[i] = v_l[i];
+      e_r = e_l;
+      break;
+    case 7:                                   // slip_wall
+      rho_r = rho_l;
+      vn_l = T(0.);
+#pragma unroll
+      for (int i = 0; i < D; i++) vn_l = vn_l + (v_l[i] - T(0.0)) * n[i];
+#pragma unroll
+      for (int i = 0; i < D; i++) v_r[i] = v_l[i] - T(2.0) * vn_l * n[i];
+      e_r = e_l;
+      break;
+    case 11: case 13:                         // isotherm_fix, isotherm_move
+      p_r = p_l;
+      rho_r = p_r / (R_ref * T_wall);
+#pragma unroll
+      for (int i = 0; i < D; i++) v_r[i] = type == 11 ? T(0.0) : ph.bdy[5 + i] + T(0.0);
+      energy();
+      break;
+    case 12: case 14:                         // adiabat_fix, adiabat_move
+      rho_r = rho_l;
+      p_r = p_l;
+#pragma unroll
+      for (int i = 0; i < D; i++) v_r[i] = type == 12 ? T(0.0) : ph.bdy[5 + i] + T(0.0);
+      energy();
+      break;
+    case 15: {                                // char
+      vn_l = T(0.);
+#pragma unroll
+      for (int i = 0; i < D; i++) vn_l = vn_l + v_l[i] * n[i];
+      T vn_bound = T(0);
+#pragma unroll
+      for (int i = 0; i < D; i++) vn_bound = vn_bound + ph.bdy[1 + i] * n[i];
+      const T r_plus = vn_l + T(2.) / (g - T(1.)) * fr_sqrt<T>(g * p_l / rho_l);
+      const T r_minus = vn_bound - T(2.) / (g - T(1.)) * fr_sqrt<T>(g * p_bound / rho_bound);
+      const T c_star = T(0.25) * (g - T(1.)) * (r_plus - r_minus);
+      const T vn_star = T(0.5) * (r_plus + r_minus);
+      if (vn_l < T(0)) {
+        const T one_over_s = fr_pow<T>(rho_bound, g) / p_bound;
+        T vs = T(0.);
+#pragma unroll
+        for (int i = 0; i < D; i++) vs = vs + ph.bdy[1 + i] * ph.bdy[1 + i];
+        const T h_free_stream = g / (g - T(1.)) * p_bound / rho_bound + T(0.5) * vs;
+        rho_r = fr_pow<T>(T(1.) / g * (one_over_s * c_star * c_star), T(1.) / (g - T(1.)));
+#pragma unroll
+        for (int i = 0; i < D; i++) v_r[i] = vn_star * n[i] + (ph.bdy[1 + i] - vn_bound * n[i]);
+        p_r = rho_r / g * c_star * c_star;
+        e_r = rho_r * h_free_stream - p_r;
+      } else {
+        const T one_over_s = fr_pow<T>(rho_l, g) / p_l;
+        rho_r = fr_pow<T>(T(1.) / g * (one_over_s * c_star * c_star), T(1.) / (g - T(1.)));
+#pragma unroll
+        for (int i = 0; i < D; i++) v_r[i] = vn_star * n[i] + (v_l[i] - vn_l * n[i]);
+        p_r = rho_r / g * c_star * c_star;
+        energy();
+      }
+      break;
+    }
+    default:                                  // 16 slip_wall_dual
+      rho_r = rho_l;
+      vn_l = T(0.);
+#pragma unroll
+      for (int i = 0; i < D; i++) vn_l = vn_l + v_l[i] * n[i];
+#pragma unroll
+      for (int i = 0; i < D; i++) v_r[i] = v_l[i] - vn_l * n[i];
+      e_r = e_l;
+      break;
+  }
+  ur[0] = rho_r;
+#pragma unroll
+  for (int i = 0; i < D; i++) ur[i + 1] = rho_r * v_r[i];
+  ur[D + 1] = e_r;
+}
+
+// Energy gradient of the ghost side at adiabatic walls (12, 14): no
+// temperature gradient, bdy_inters::set_vis_boundary_conditions,
+// src/bdy_inters.cpp:1062-1113.  g[k][d]: copy of the own gradient, changed in place.
+template <int D, typename T>
+__device__ __forceinline__ void bc_vis_gradient(const PhysT<T>& ph, const T* ul, const T* ur, T (*g)[D])
+{
+  T v_sq = T(0.);
+#pragma unroll
+  for (int i = 0; i < D; i++) v_sq = v_sq + (ul[i + 1] * ul[i + 1]);
+  const T p_l = (ph.gamma - T(1.0)) * (ul[D + 1] - T(0.5) * v_sq / ul[0]);
+  const T inte = p_l / ((ph.gamma - T(1.0)) * ur[0]);
+  T gv[D][D];
+#pragma unroll
+  for (int j = 0; j < D; j++)
+#pragma unroll
+    for (int i = 0; i < D; i++) gv[j][i] = (g[j + 1][i] - g[0][i] * ur[j + 1] / ur[0]) / ur[0];
+  T ke = ur[1] * ur[1];
+#pragma unroll
+  for (int j = 1; j < D; j++) ke = ke + ur[j + 1] * ur[j + 1];
+#pragma unroll
+  for (int i = 0; i < D; i++) {
+    T w = (ur[1] / ur[0]) * gv[0][i];
+#pragma unroll
+    for (int j = 1; j < D; j++) w = w + (ur[j + 1] / ur[0]) * gv[j][i];
+    g[D + 1][i] = inte * g[0][i] + T(0.5) * (ke / (ur[0] * ur[0])) * g[0][i] + ur[0] * w;
+  }
 }
 
 // Sign of the LDG penalty: one fixed direction per interface point, taken

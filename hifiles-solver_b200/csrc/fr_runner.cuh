@@ -26,6 +26,10 @@ struct Bufs {
   int2* face = nullptr;
   unsigned char* fsign = nullptr;
   long long nint = 0;
+  long long nbdy = 0;              // boundary flux points
+  int* bf = nullptr;               // their flat indices
+  unsigned char* bt = nullptr;     // their boundary types
+  void* BV = nullptr;              // viscous boundary normal flux (nbdy, F), from the gradient kernel
   int* mate = nullptr;
   unsigned char* side = nullptr;
 };
@@ -149,7 +153,7 @@ struct RunnerT : Runner {
       (void)once;
       fr_grad_kernel<DIM, P, EPB, NT, TC, LES, MINB><<<(unsigned)((E + EPB - 1) / EPB), NT, sm, s>>>(
           b.U, (const TC*)b.UF[cur], b.mate, b.side, (const TC*)b.JG, (const TC*)b.detj, (const TC*)b.nL,
-          (TC*)b.VF, (TC*)b.ND, (TC*)b.DV, E, L, ph, (TC*)b.GRAD);
+          (TC*)b.VF, (TC*)b.ND, (TC*)b.DV, E, L, ph, (TC*)b.GRAD, (TC*)b.BV);
     }
   }
   void grad(const Bufs& b, int cur, cudaStream_t s) override
@@ -161,14 +165,15 @@ struct RunnerT : Runner {
   template <int VISC, int RS>
   void face_t(const Bufs& b, int cur, cudaStream_t s)
   {
-    unsigned g = (unsigned)((b.nint + 127) / 128);
+    unsigned g = (unsigned)((b.nint + b.nbdy + 127) / 128);
     fr_face_kernel<DIM, VISC, TC, RS><<<g, 128, 0, s>>>(b.face, b.fsign, b.nint, (const TC*)b.UF[cur],
                                                          VISC ? (const TC*)b.VF : nullptr, (const TC*)b.nL,
-                                                         (const TC*)b.tdA, (TC*)b.CF, E * S::NF, ph);
+                                                         (const TC*)b.tdA, (TC*)b.CF, E * S::NF, ph, b.nbdy, b.bf,
+                                                         b.bt, VISC ? (const TC*)b.BV : nullptr);
   }
   void face(const Bufs& b, int cur, cudaStream_t s) override
   {
-    if (b.nint == 0) return;
+    if (b.nint + b.nbdy == 0) return;
     if (DIM == 2 && riemann == 2) {
       if (visc) face_t<1, 2>(b, cur, s);
       else face_t<0, 2>(b, cur, s);

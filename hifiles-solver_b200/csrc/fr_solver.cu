@@ -118,6 +118,7 @@ fr_status upload_geometry(fr_solver* s)
     double sgn = m.dims == 2 ? (n[0] + n[1]) : (n[0] + n[1] + std::sqrt(2.) * n[2]);
     side[i] = (m.is_left[i] ? 1 : 0) | (sgn < 0. ? 2 : 0);
   }
+  for (size_t j = 0; j < m.bf.size(); j++) side[m.bf[j]] = (unsigned char)(1 | (m.bt[j] << 2));
   FR_CUDA(cudaMemcpy(s->b.side, side.data(), side.size(), cudaMemcpyHostToDevice));
   std::vector<int2> face(m.il.size());
   std::vector<unsigned char> fsign(m.il.size());
@@ -127,6 +128,10 @@ fr_status upload_geometry(fr_solver* s)
   }
   FR_CUDA(cudaMemcpy(s->b.face, face.data(), face.size() * sizeof(int2), cudaMemcpyHostToDevice));
   FR_CUDA(cudaMemcpy(s->b.fsign, fsign.data(), fsign.size(), cudaMemcpyHostToDevice));
+  if (s->b.nbdy > 0) {
+    FR_CUDA(cudaMemcpy(s->b.bf, m.bf.data(), m.bf.size() * sizeof(int), cudaMemcpyHostToDevice));
+    FR_CUDA(cudaMemcpy(s->b.bt, m.bt.data(), m.bt.size(), cudaMemcpyHostToDevice));
+  }
   return FR_OK;
 }
 
@@ -199,7 +204,7 @@ fr_status fr_solver_create(const fr_mesh_desc* md, const fr_scheme_desc* sd, int
   s->tc_size = sd->precision == 1 ? 4 : 8;
   std::string err;
   if (!make_line(sd->order, sd->upts_type, sd->vcjh_scheme, sd->eta, s->line, err)) return fail(FR_ERR_ARG, err);
-  if (!build_mesh(md->dims, s->line, md->n_verts, md->xv, md->n_eles, md->c2v, md->shift, s->mesh, err))
+  if (!build_mesh(md->dims, s->line, md->n_verts, md->xv, md->n_eles, md->c2v, md->shift, md->bctype, s->mesh, err))
     return fail(FR_ERR_MESH, err);
   FR_CUDA(cudaSetDevice(device));
   if (sd->les && sd->sgs_model == 5) {
@@ -212,6 +217,8 @@ fr_status fr_solver_create(const fr_mesh_desc* md, const fr_scheme_desc* sd, int
   }
   Phys ph{sd->gamma, sd->prandtl, sd->mu_inf, sd->rt_inf, sd->c_sth, sd->fix_vis, sd->tau, sd->pen_fact,
           sd->sgs_model, sd->filter_ratio, s->mlp};
+  for (int i = 0; i < 14; i++) ph.bdy[i] = sd->bdy[i];
+  ph.R_ref = sd->R_ref;
   const int les = sd->les;
   Runner* r = make_runner(md->dims, sd->order, (int)s->tc_size, md->n_eles, sd->viscous, les, s->line, ph);
   if (!r) return fail(FR_ERR_UNSUPPORTED, "no kernel for this (dims, order)");
@@ -233,6 +240,12 @@ fr_status fr_solver_create(const fr_mesh_desc* md, const fr_scheme_desc* sd, int
   }
   if ((st = dalloc(s.get(), &p, nf * E * F * tc))) return st; s->b.CF = p;
   s->b.nint = (long long)m.il.size();
+  s->b.nbdy = (long long)m.bf.size();
+  if (s->b.nbdy > 0) {
+    if ((st = dalloc(s.get(), &s->b.bf, (size_t)s->b.nbdy))) return st;
+    if ((st = dalloc(s.get(), &s->b.bt, (size_t)s->b.nbdy))) return st;
+    if (sd->viscous) { if ((st = dalloc(s.get(), &p, (size_t)s->b.nbdy * F * tc))) return st; s->b.BV = p; }
+  }
   if ((st = dalloc(s.get(), &s->b.face, (size_t)s->b.nint))) return st;
   if ((st = dalloc(s.get(), &s->b.fsign, (size_t)s->b.nint))) return st;
   if ((st = dalloc(s.get(), &p, nf * E * D * tc))) return st; s->b.nL = p;
@@ -537,7 +550,7 @@ fr_status fr_mesh_geometry(const fr_mesh_desc* md, const fr_scheme_desc* sd, int
   Mesh m;
   std::string err;
   if (!make_line(sd->order, sd->upts_type, sd->vcjh_scheme, sd->eta, line, err)) return fail(FR_ERR_ARG, err);
-  if (!build_mesh(md->dims, line, md->n_verts, md->xv, md->n_eles, md->c2v, md->shift, m, err))
+  if (!build_mesh(md->dims, line, md->n_verts, md->xv, md->n_eles, md->c2v, md->shift, md->bctype, m, err))
     return fail(FR_ERR_MESH, err);
   out6[0] = (int)m.ne; out6[1] = m.nu; out6[2] = m.nf; out6[3] = m.nfields; out6[4] = m.dims;
   out6[5] = (int)m.il.size();

@@ -31,7 +31,7 @@ class FrError(RuntimeError):
 
 class MeshDesc(C.Structure):
     _fields_ = [("dims", C.c_int), ("n_verts", C.c_int), ("xv", C.POINTER(C.c_double)), ("n_eles", C.c_int),
-                ("c2v", C.POINTER(C.c_int)), ("shift", C.c_double * 3)]
+                ("c2v", C.POINTER(C.c_int)), ("shift", C.c_double * 3), ("bctype", C.POINTER(C.c_int))]
 
 
 class SchemeDesc(C.Structure):
@@ -39,7 +39,30 @@ class SchemeDesc(C.Structure):
                 ("viscous", C.c_int), ("riemann", C.c_int), ("precision", C.c_int), ("gamma", C.c_double),
                 ("prandtl", C.c_double), ("mu_inf", C.c_double), ("rt_inf", C.c_double), ("c_sth", C.c_double),
                 ("fix_vis", C.c_double), ("tau", C.c_double), ("pen_fact", C.c_double), ("les", C.c_int),
-                ("sgs_model", C.c_int), ("filter_ratio", C.c_double)]
+                ("sgs_model", C.c_int), ("filter_ratio", C.c_double), ("bdy", C.c_double * 14), ("R_ref", C.c_double)]
+
+
+# local face of each box side (x-, x+, y-, y+, z-, z+) in the reference's numbering
+_QUAD_SIDE_FACE = (3, 1, 0, 2)
+_HEX_SIDE_FACE = (4, 2, 1, 3, 0, 5)
+
+
+def box_bctype(dims, n, side_bc):
+    """(n_eles, 2*dims) boundary type per local face of a box mesh whose sides
+    x-, x+, y-, y+(, z-, z+) carry the types side_bc (0 = periodic)."""
+    nx, ny = int(n[0]), int(n[1])
+    nz = int(n[2]) if dims == 3 else 1
+    bct = np.zeros((nx * ny * nz, 2 * dims), dtype=np.int32)
+    ijk = np.indices((nz, ny, nx)).reshape(3, -1)[::-1]          # i, j, k with i fastest
+    nn = (nx, ny, nz)
+    side_face = _QUAD_SIDE_FACE if dims == 2 else _HEX_SIDE_FACE
+    for d in range(dims):
+        for sd in range(2):
+            b = int(side_bc[2 * d + sd])
+            if b:
+                sel = ijk[d] == (0 if sd == 0 else nn[d] - 1)
+                bct[sel, side_face[2 * d + sd]] = b
+    return bct
 
 
 _LIB = None
@@ -149,18 +172,24 @@ def box_mesh(dims, n, lo, hi, jitter=0.0, seed=0):
     return xv, c2v
 
 
+def _bdy(bdy):
+    return (C.c_double * 14)(*(list(bdy) if bdy is not None else [0.0] * 14))
+
+
 def _descs(dims, xv, c2v, shift, order, viscous=False, gamma=1.4, prandtl=0.72, mu_inf=0.0, rt_inf=1.0,
            c_sth=1.0, fix_vis=1.0, tau=1.0, pen_fact=0.5, vcjh_scheme=1, eta=0.0, upts_type=0, precision=0,
-           les=0, sgs_model=1, filter_ratio=1.0, riemann=0):
+           les=0, sgs_model=1, filter_ratio=1.0, riemann=0, bctype=None, bdy=None, R_ref=1.0):
     xv = np.ascontiguousarray(xv, dtype=np.float64)
     c2v = np.ascontiguousarray(c2v, dtype=np.int32)
+    bct = None if bctype is None else np.ascontiguousarray(bctype, dtype=np.int32)
     md = MeshDesc(int(dims), xv.shape[0], _dp(xv), c2v.shape[0], c2v.ctypes.data_as(C.POINTER(C.c_int)),
-                  (C.c_double * 3)(*(list(shift) + [0.0] * (3 - len(shift)))))
+                  (C.c_double * 3)(*(list(shift) + [0.0] * (3 - len(shift)))),
+                  None if bct is None else bct.ctypes.data_as(C.POINTER(C.c_int)))
     sd = SchemeDesc(int(order), int(upts_type), int(vcjh_scheme), float(eta), int(bool(viscous)), int(riemann),
                     int(precision),
                     gamma, prandtl, mu_inf, rt_inf, c_sth, fix_vis, tau, pen_fact, int(les), int(sgs_model),
-                    float(filter_ratio))
-    return md, sd, (xv, c2v)
+                    float(filter_ratio), _bdy(bdy), float(R_ref))
+    return md, sd, (xv, c2v, bct)
 
 
 def mesh_geometry(dims, xv, c2v, shift, order, **kw):
@@ -195,16 +224,19 @@ class Solver:
 
     def __init__(self, dims, xv, c2v, shift, order, viscous=False, gamma=1.4, prandtl=0.72, mu_inf=0.0,
                  rt_inf=1.0, c_sth=1.0, fix_vis=1.0, tau=1.0, pen_fact=0.5, vcjh_scheme=1, eta=0.0, upts_type=0,
-                 precision=0, device=0, les=0, sgs_model=1, filter_ratio=1.0, riemann=0):
+                 precision=0, device=0, les=0, sgs_model=1, filter_ratio=1.0, riemann=0, bctype=None, bdy=None,
+                 R_ref=1.0):
         L = lib()
         self._xv = np.ascontiguousarray(xv, dtype=np.float64)
         self._c2v = np.ascontiguousarray(c2v, dtype=np.int32)
+        self._bct = None if bctype is None else np.ascontiguousarray(bctype, dtype=np.int32)
         md = MeshDesc(int(dims), self._xv.shape[0], _dp(self._xv), self._c2v.shape[0],
                       self._c2v.ctypes.data_as(C.POINTER(C.c_int)),
-                      (C.c_double * 3)(*(list(shift) + [0.0] * (3 - len(shift)))))
+                      (C.c_double * 3)(*(list(shift) + [0.0] * (3 - len(shift)))),
+                      None if self._bct is None else self._bct.ctypes.data_as(C.POINTER(C.c_int)))
         sd = SchemeDesc(int(order), int(upts_type), int(vcjh_scheme), float(eta), int(bool(viscous)), int(riemann),
                         int(precision), gamma, prandtl, mu_inf, rt_inf, c_sth, fix_vis, tau, pen_fact, int(les),
-                        int(sgs_model), float(filter_ratio))
+                        int(sgs_model), float(filter_ratio), _bdy(bdy), float(R_ref))
         h = C.c_void_p()
         self.h = None
         _check(L.fr_solver_create(C.byref(md), C.byref(sd), int(device), C.byref(h)))
@@ -216,9 +248,14 @@ class Solver:
         self.precision = precision
 
     @classmethod
-    def box(cls, dims, order, n, lo, hi, jitter=0.0, seed=0, **kw):
+    def box(cls, dims, order, n, lo, hi, jitter=0.0, seed=0, side_bc=None, **kw):
+        """Structured box; side_bc: boundary types of the sides x-, x+, y-, y+(,
+        z-, z+), 0 = periodic (the default for every side)."""
         xv, c2v = box_mesh(dims, n, lo, hi, jitter, seed)
         shift = [hi[d] - lo[d] for d in range(dims)]
+        if side_bc is not None:
+            shift = [0.0 if (side_bc[2 * d] or side_bc[2 * d + 1]) else shift[d] for d in range(dims)]
+            kw["bctype"] = box_bctype(dims, n, side_bc)
         return cls(dims, xv, c2v, shift, order, **kw)
 
     def close(self):

@@ -59,6 +59,16 @@ typedef struct {
                             sits at reference corner (a, b, c) in {0,1}^dims    */
   double shift[3];       /* periodic translation per axis (dx/dy/dz_cyclic of
                             the reference input), 0 = not periodic             */
+  const int* bctype;     /* (n_eles, 2*dims) boundary type of each local
+                            face in the reference's face numbering (quads:
+                            y- 0, x+ 1, y+ 2, x- 3; hexes: z- 0, y- 1, x+ 2,
+                            y+ 3, x- 4, z+ 5), get_bc_number codes
+                            (src/geometry.cpp:121-148): 1 sub_in_simp,
+                            2 sub_out_simp, 3 sub_in_char, 4 sub_out_char,
+                            5 sup_in, 6 sup_out, 7 slip_wall, 11 isotherm_fix,
+                            12 adiabat_fix, 13 isotherm_move, 14 adiabat_move,
+                            15 char, 16 slip_wall_dual; 0 = matched with
+                            another face.  NULL: every face is matched.       */
 } fr_mesh_desc;
 
 typedef struct {
@@ -80,6 +90,12 @@ typedef struct {
                             learned closure below; the filter-based models
                             2-4 are not built                                 */
   double filter_ratio;   /* with les: filter width over the point spacing     */
+  double bdy[14];        /* boundary values in bdy_inters::set_bdy_params
+                            order (src/bdy_inters.cpp:78-110): rho_bound,
+                            v_bound[3], p_bound, v_wall[3], T_wall,
+                            p_total_bound, T_total_bound, n_free_stream[3]   */
+  double R_ref;          /* gas constant in reference units (isothermal walls,
+                            characteristic inflow)                            */
 } fr_scheme_desc;
 
 fr_status fr_solver_create(const fr_mesh_desc* mesh, const fr_scheme_desc* scheme, int device,

@@ -16,7 +16,7 @@ import pytest
 
 import hifiles_b200 as H
 import oracle as O
-from golden_util import CASES, GOLDEN, load, rel
+from golden_util import BC_CASES, CASES, GOLDEN, load, rel
 
 pytestmark = pytest.mark.gpu
 
@@ -27,10 +27,10 @@ def _solver(meta, precision=0):
     ph = meta["physics"]
     return H.Solver.box(meta["dims"], meta["order"], meta["n"], meta["lo"], meta["hi"], jitter=meta["jitter"],
                         seed=meta["seed"], viscous=bool(meta["viscous"]), vcjh_scheme=meta["vcjh"],
-                        precision=precision, **ph)
+                        precision=precision, side_bc=meta.get("side_bc"), **ph)
 
 
-@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("case", CASES + BC_CASES)
 def test_residual_matches_reference(case):
     meta, a = load(case)
     s = _solver(meta)
@@ -39,7 +39,7 @@ def test_residual_matches_reference(case):
     assert rel(div, a["div0"]) <= TOL_RES
 
 
-@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("case", CASES + BC_CASES)
 def test_rk45_steps_match_reference(case):
     meta, a = load(case)
     s = _solver(meta)
