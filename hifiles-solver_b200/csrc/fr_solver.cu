@@ -161,6 +161,10 @@ fr_status stage(fr_solver* s, int st, double dt, bool want_partial, cudaStream_t
 
 }  // namespace
 
+static fr_status create_with_mesh(Mesh&& mesh, const Line1D& line, const fr_scheme_desc* sd, int device,
+                                  fr_solver** out);
+static fr_status validate_scheme(int dims, const fr_scheme_desc* sd);
+
 extern "C" {
 
 const char* fr_status_string(fr_status s)
@@ -184,11 +188,26 @@ fr_status fr_solver_create(const fr_mesh_desc* md, const fr_scheme_desc* sd, int
   g_err.clear();
   if (!md || !sd || !out) return fail(FR_ERR_ARG, "null argument");
   *out = nullptr;
-  if (md->dims != 2 && md->dims != 3) return fail(FR_ERR_ARG, "dims must be 2 or 3");
-  if (sd->riemann != 0 && !(sd->riemann == 2 && md->dims == 2))
+  fr_status v = validate_scheme(md->dims, sd);
+  if (v) return v;
+  Line1D line;
+  std::string err;
+  if (!make_line(sd->order, sd->upts_type, sd->vcjh_scheme, sd->eta, line, err)) return fail(FR_ERR_ARG, err);
+  Mesh mesh;
+  if (!build_mesh(md->dims, line, md->n_verts, md->xv, md->n_eles, md->c2v, md->shift, md->bctype, mesh, err))
+    return fail(FR_ERR_MESH, err);
+  return create_with_mesh(std::move(mesh), line, sd, device, out);
+}
+
+}  // extern "C"
+
+static fr_status validate_scheme(int dims, const fr_scheme_desc* sd)
+{
+  if (dims != 2 && dims != 3) return fail(FR_ERR_ARG, "dims must be 2 or 3");
+  if (sd->riemann != 0 && !(sd->riemann == 2 && dims == 2))
     return fail(FR_ERR_UNSUPPORTED, "common fluxes built: Rusanov (0), and Roe (2) in 2-D as in the reference");
   if (sd->precision != 0 && sd->precision != 1) return fail(FR_ERR_ARG, "precision must be 0 or 1");
-  int maxP = md->dims == 2 ? 5 : 4;
+  int maxP = dims == 2 ? 5 : 4;
   if (sd->order < 1 || sd->order > maxP) return fail(FR_ERR_UNSUPPORTED, "order outside the built range");
   if (sd->upts_type != 0) return fail(FR_ERR_UNSUPPORTED, "fused kernels need Gauss solution points");
   if (sd->les != 0) {
@@ -198,14 +217,20 @@ fr_status fr_solver_create(const fr_mesh_desc* md, const fr_scheme_desc* sd, int
                   "SGS models built: 0 (Smagorinsky), 1 (WALE) and 5 (learned); the filter-based models are not");
     if (!(sd->filter_ratio > 0.0)) return fail(FR_ERR_ARG, "filter_ratio must be positive");
   }
+  return FR_OK;
+}
+
+// Everything of fr_solver_create after the mesh is wired (also used for the
+// merged meshes of a batch).
+static fr_status create_with_mesh(Mesh&& mesh, const Line1D& line, const fr_scheme_desc* sd, int device,
+                                  fr_solver** out)
+{
   std::unique_ptr<fr_solver> s(new fr_solver());
   s->device = device;
   s->sch = *sd;
   s->tc_size = sd->precision == 1 ? 4 : 8;
-  std::string err;
-  if (!make_line(sd->order, sd->upts_type, sd->vcjh_scheme, sd->eta, s->line, err)) return fail(FR_ERR_ARG, err);
-  if (!build_mesh(md->dims, s->line, md->n_verts, md->xv, md->n_eles, md->c2v, md->shift, md->bctype, s->mesh, err))
-    return fail(FR_ERR_MESH, err);
+  s->line = line;
+  s->mesh = std::move(mesh);
   FR_CUDA(cudaSetDevice(device));
   if (sd->les && sd->sgs_model == 5) {
     // the learned closure starts switched off (c ~ 2e-9) until parameters are set
@@ -220,7 +245,7 @@ fr_status fr_solver_create(const fr_mesh_desc* md, const fr_scheme_desc* sd, int
   for (int i = 0; i < 14; i++) ph.bdy[i] = sd->bdy[i];
   ph.R_ref = sd->R_ref;
   const int les = sd->les;
-  Runner* r = make_runner(md->dims, sd->order, (int)s->tc_size, md->n_eles, sd->viscous, les, s->line, ph);
+  Runner* r = make_runner(s->mesh.dims, sd->order, (int)s->tc_size, s->mesh.ne, sd->viscous, les, s->line, ph);
   if (!r) return fail(FR_ERR_UNSUPPORTED, "no kernel for this (dims, order)");
   r->set_riemann(sd->riemann);
   s->run.reset(r);
@@ -266,6 +291,8 @@ fr_status fr_solver_create(const fr_mesh_desc* md, const fr_scheme_desc* sd, int
   *out = s.release();
   return FR_OK;
 }
+
+extern "C" {
 
 fr_status fr_solver_destroy(fr_solver* s)
 {
@@ -680,3 +707,279 @@ fr_status fr_solver_read_restart(fr_solver* s, const char* path, double* time_ou
   if (r) return r;
   return fr_solver_set_state(s, u.data(), nullptr);
 }
+
+// ---------------------------------------------------------------------------
+// Batches of independent meshes.  Instances with the same element type,
+// order and scheme are merged into one mesh (elements, flux-point indices and
+// boundary lists offset; each instance keeps its own periodic wiring), so a
+// group is one solver: one launch per stage kernel over all its instances.
+// A step of the whole batch (every group, five stages) is one CUDA graph.
+
+namespace {
+
+template <typename V>
+void cat_blocks(V& out, const std::vector<const V*>& parts, const std::vector<size_t>& per_elem, int nblocks)
+{
+  // arrays laid out (n, ne, blocks): per block, the instances' runs one after the other
+  out.clear();
+  for (int d = 0; d < nblocks; d++)
+    for (size_t i = 0; i < parts.size(); i++) {
+      const V& a = *parts[i];
+      size_t len = a.size() / nblocks;
+      out.insert(out.end(), a.begin() + d * len, a.begin() + (d + 1) * len);
+    }
+  (void)per_elem;
+}
+
+bool merge_meshes(std::vector<Mesh>& parts, Mesh& m, std::string& err)
+{
+  const Mesh& p0 = parts[0];
+  m = Mesh();
+  m.dims = p0.dims; m.P = p0.P; m.n1 = p0.n1; m.nu = p0.nu; m.nf = p0.nf; m.nface = p0.nface;
+  m.nfpf = p0.nfpf; m.nfields = p0.nfields;
+  long long ne = 0, nv = 0, nb = 0;
+  for (auto& p : parts) ne += p.ne;
+  if ((double)m.nf * (double)ne >= 2147483647.0) { err = "batch group too large for 32-bit flux-point indices"; return false; }
+  m.ne = ne;
+  const int D = m.dims, ns = 1 << D, nf = m.nf;
+  std::vector<const std::vector<double>*> pu, pf, dj, jg, ta, nr, nl;
+  std::vector<const std::vector<unsigned char>*> il;
+  for (auto& p : parts) {
+    pu.push_back(&p.pos_upts); pf.push_back(&p.pos_fpts); dj.push_back(&p.detjac); jg.push_back(&p.JG);
+    ta.push_back(&p.tdA); nr.push_back(&p.nrm); nl.push_back(&p.nL); il.push_back(&p.is_left);
+  }
+  std::vector<size_t> none;
+  cat_blocks(m.pos_upts, pu, none, D);
+  cat_blocks(m.pos_fpts, pf, none, D);
+  cat_blocks(m.detjac, dj, none, 1);
+  cat_blocks(m.JG, jg, none, 1);
+  cat_blocks(m.tdA, ta, none, 1);
+  cat_blocks(m.nrm, nr, none, D);
+  cat_blocks(m.nL, nl, none, D);
+  cat_blocks(m.is_left, il, none, 1);
+  long long eoff = 0;
+  for (auto& p : parts) {
+    const long long fo = (long long)nf * eoff;
+    m.xv.insert(m.xv.end(), p.xv.begin(), p.xv.end());
+    for (int v : p.c2v) m.c2v.push_back((int)(v + nv));
+    for (size_t i = 0; i < p.il.size(); i++) { m.il.push_back((int)(p.il[i] + fo)); m.ir.push_back((int)(p.ir[i] + fo)); }
+    for (int q : p.mate) m.mate.push_back(q >= 0 ? (int)(q + fo) : (int)(q - nb));
+    for (size_t j = 0; j < p.bf.size(); j++) { m.bf.push_back((int)(p.bf[j] + fo)); m.bt.push_back(p.bt[j]); }
+    nv += (long long)(p.xv.size() / D);
+    nb += (long long)p.bf.size();
+    eoff += p.ne;
+  }
+  (void)ns;
+  return true;
+}
+
+bool same_scheme(const fr_scheme_desc& a, const fr_scheme_desc& b)
+{
+  if (a.order != b.order || a.upts_type != b.upts_type || a.vcjh_scheme != b.vcjh_scheme || a.eta != b.eta ||
+      a.viscous != b.viscous || a.riemann != b.riemann || a.precision != b.precision || a.gamma != b.gamma ||
+      a.prandtl != b.prandtl || a.mu_inf != b.mu_inf || a.rt_inf != b.rt_inf || a.c_sth != b.c_sth ||
+      a.fix_vis != b.fix_vis || a.tau != b.tau || a.pen_fact != b.pen_fact || a.les != b.les ||
+      a.sgs_model != b.sgs_model || a.filter_ratio != b.filter_ratio || a.R_ref != b.R_ref)
+    return false;
+  for (int i = 0; i < 14; i++)
+    if (a.bdy[i] != b.bdy[i]) return false;
+  return true;
+}
+
+}  // namespace
+
+struct fr_batch {
+  int device = 0;
+  std::vector<fr_solver*> groups;
+  std::vector<int> inst_group;            // instance -> group
+  std::vector<long long> inst_eoff, inst_ne;
+  std::vector<char> dirty;                // group state written since its traces were made
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  double graph_dt[2] = {0, 0};
+  long long launches = 0;
+};
+
+extern "C" {
+
+fr_status fr_batch_destroy(fr_batch* b)
+{
+  if (!b) return FR_OK;
+  cudaSetDevice(b->device);
+  for (int i = 0; i < 2; i++)
+    if (b->graph[i]) cudaGraphExecDestroy(b->graph[i]);
+  if (b->stream) { cudaStreamSynchronize(b->stream); cudaStreamDestroy(b->stream); }
+  for (fr_solver* s : b->groups) fr_solver_destroy(s);
+  delete b;
+  return FR_OK;
+}
+
+fr_status fr_batch_create(const fr_mesh_desc* meshes, const fr_scheme_desc* schemes, int n, int device,
+                          fr_batch** out)
+{
+  g_err.clear();
+  if (!meshes || !schemes || !out || n < 1) return fail(FR_ERR_ARG, "bad argument");
+  *out = nullptr;
+  std::unique_ptr<fr_batch, fr_status (*)(fr_batch*)> b(new fr_batch(), fr_batch_destroy);
+  b->device = device;
+  b->inst_group.assign(n, -1);
+  b->inst_eoff.assign(n, 0);
+  b->inst_ne.assign(n, 0);
+  std::vector<int> done(n, 0);
+  for (int i = 0; i < n; i++) {
+    if (done[i]) continue;
+    std::vector<int> members;
+    for (int j = i; j < n; j++)
+      if (!done[j] && meshes[j].dims == meshes[i].dims && same_scheme(schemes[j], schemes[i])) {
+        members.push_back(j);
+        done[j] = 1;
+      }
+    const fr_scheme_desc* sd = &schemes[i];
+    fr_status v = validate_scheme(meshes[i].dims, sd);
+    if (v) return v;
+    Line1D line;
+    std::string err;
+    if (!make_line(sd->order, sd->upts_type, sd->vcjh_scheme, sd->eta, line, err)) return fail(FR_ERR_ARG, err);
+    std::vector<Mesh> parts(members.size());
+    long long eoff = 0;
+    for (size_t q = 0; q < members.size(); q++) {
+      const fr_mesh_desc* md = &meshes[members[q]];
+      if (!build_mesh(md->dims, line, md->n_verts, md->xv, md->n_eles, md->c2v, md->shift, md->bctype, parts[q],
+                      err))
+        return fail(FR_ERR_MESH, "instance " + std::to_string(members[q]) + ": " + err);
+      b->inst_group[members[q]] = (int)b->groups.size();
+      b->inst_eoff[members[q]] = eoff;
+      b->inst_ne[members[q]] = parts[q].ne;
+      eoff += parts[q].ne;
+    }
+    Mesh merged;
+    if (!merge_meshes(parts, merged, err)) return fail(FR_ERR_MESH, err);
+    parts.clear();
+    fr_solver* s = nullptr;
+    // validation of the scheme (orders, models) is fr_solver_create's: run it on the first instance's shape
+    fr_status st = create_with_mesh(std::move(merged), line, sd, device, &s);
+    if (st) return st;
+    b->groups.push_back(s);
+  }
+  b->dirty.assign(b->groups.size(), 1);
+  FR_CUDA(cudaSetDevice(device));
+  FR_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  *out = b.release();
+  return FR_OK;
+}
+
+int fr_batch_n_groups(const fr_batch* b) { return b ? (int)b->groups.size() : 0; }
+
+fr_status fr_batch_group(fr_batch* b, int g, fr_solver** out)
+{
+  if (!b || !out || g < 0 || g >= (int)b->groups.size()) return fail(FR_ERR_ARG, "bad group");
+  *out = b->groups[g];
+  return FR_OK;
+}
+
+fr_status fr_batch_instance(const fr_batch* b, int i, int out4[4])
+{
+  if (!b || !out4 || i < 0 || i >= (int)b->inst_group.size()) return fail(FR_ERR_ARG, "bad instance");
+  const fr_solver* s = b->groups[b->inst_group[i]];
+  out4[0] = b->inst_group[i];
+  out4[1] = (int)b->inst_eoff[i];
+  out4[2] = (int)b->inst_ne[i];
+  out4[3] = s->mesh.nu;
+  return FR_OK;
+}
+
+fr_status fr_batch_set_state(fr_batch* b, int i, const double* host_u)
+{
+  if (!b || !host_u || i < 0 || i >= (int)b->inst_group.size()) return fail(FR_ERR_ARG, "bad argument");
+  const int g = b->inst_group[i];
+  fr_solver* s = b->groups[g];
+  const size_t nu = s->mesh.nu, E = s->mesh.ne, F = s->mesh.nfields, ne = b->inst_ne[i], eo = b->inst_eoff[i];
+  for (size_t q = 0; q < nu * ne * F; q++)
+    if (!std::isfinite(host_u[q])) return fail(FR_ERR_NONFINITE, "non-finite state");
+  FR_CUDA(cudaSetDevice(b->device));
+  for (size_t k = 0; k < F; k++) {
+    FR_CUDA(cudaMemcpyAsync(s->b.U + nu * (eo + E * k), host_u + nu * ne * k, nu * ne * 8, cudaMemcpyHostToDevice,
+                            b->stream));
+    FR_CUDA(cudaMemsetAsync(s->b.REG + nu * (eo + E * k), 0, nu * ne * 8, b->stream));
+  }
+  FR_CUDA(cudaStreamSynchronize(b->stream));
+  b->dirty[g] = 1;
+  return FR_OK;
+}
+
+fr_status fr_batch_get_state(fr_batch* b, int i, double* host_u)
+{
+  if (!b || !host_u || i < 0 || i >= (int)b->inst_group.size()) return fail(FR_ERR_ARG, "bad argument");
+  fr_solver* s = b->groups[b->inst_group[i]];
+  const size_t nu = s->mesh.nu, E = s->mesh.ne, F = s->mesh.nfields, ne = b->inst_ne[i], eo = b->inst_eoff[i];
+  FR_CUDA(cudaSetDevice(b->device));
+  for (size_t k = 0; k < F; k++)
+    FR_CUDA(cudaMemcpyAsync(host_u + nu * ne * k, s->b.U + nu * (eo + E * k), nu * ne * 8, cudaMemcpyDeviceToHost,
+                            b->stream));
+  FR_CUDA(cudaStreamSynchronize(b->stream));
+  return FR_OK;
+}
+
+fr_status fr_batch_autotune(fr_batch* b, int reps)
+{
+  if (!b) return fail(FR_ERR_ARG, "null batch");
+  int t[4];
+  for (size_t g = 0; g < b->groups.size(); g++) {
+    fr_status st = fr_solver_state_updated(b->groups[g], b->stream);
+    if (st) return st;
+    b->dirty[g] = 0;
+    st = fr_solver_autotune(b->groups[g], reps, t);
+    if (st) return st;
+  }
+  for (int i = 0; i < 2; i++)
+    if (b->graph[i]) { cudaGraphExecDestroy(b->graph[i]); b->graph[i] = nullptr; }
+  return FR_OK;
+}
+
+fr_status fr_batch_advance(fr_batch* b, int n_steps, double dt, void* stream)
+{
+  if (!b || n_steps < 0) return fail(FR_ERR_ARG, "bad argument");
+  if (!(dt > 0) || !std::isfinite(dt)) return fail(FR_ERR_ARG, "dt must be positive");
+  FR_CUDA(cudaSetDevice(b->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
+  for (size_t g = 0; g < b->groups.size(); g++)
+    if (b->dirty[g]) {
+      fr_status r = fr_solver_state_updated(b->groups[g], st);
+      if (r) return r;
+      b->dirty[g] = 0;
+    }
+  const int c0 = b->groups[0]->cur;
+  for (fr_solver* s : b->groups)
+    if (s->cur != c0) return fail(FR_ERR_ARG, "groups out of step");
+  long long per_step = 0;
+  for (fr_solver* s : b->groups) per_step += 5 * s->run->launches_per_stage();
+  for (int i = 0; i < n_steps; i++) {
+    const int c = b->groups[0]->cur;
+    if (!b->graph[c] || b->graph_dt[c] != dt) {
+      if (b->graph[c]) { cudaGraphExecDestroy(b->graph[c]); b->graph[c] = nullptr; }
+      cudaGraph_t gr;
+      FR_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      for (int k = 0; k < 5; k++)
+        for (fr_solver* s : b->groups) {
+          long long l0 = s->launches;
+          stage(s, k, dt, k == 4, st);
+          s->launches = l0;
+        }
+      for (fr_solver* s : b->groups) s->cur = c;
+      FR_CUDA(cudaStreamEndCapture(st, &gr));
+      cudaError_t e = cudaGraphInstantiate(&b->graph[c], gr, 0);
+      cudaGraphDestroy(gr);
+      if (e != cudaSuccess) return fail(FR_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+      b->graph_dt[c] = dt;
+    }
+    FR_CUDA(cudaGraphLaunch(b->graph[c], st));
+    b->launches += per_step;
+    for (fr_solver* s : b->groups) s->cur ^= 1;
+  }
+  return FR_OK;
+}
+
+long long fr_batch_launch_count(const fr_batch* b) { return b ? b->launches : 0; }
+void* fr_batch_stream(fr_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+}  // extern "C"

@@ -102,6 +102,17 @@ def lib():
         "fr_mesh_geometry": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(SchemeDesc), ip, dp, dp, dp, dp, dp, ip, ip]),
         "fr_line_operators": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, dp]),
         "fr_solver_gradient": (C.c_int, [vp, dp, vp]),
+        "fr_batch_create": (C.c_int, [vp, vp, C.c_int, C.c_int, C.POINTER(vp)]),
+        "fr_batch_destroy": (C.c_int, [vp]),
+        "fr_batch_n_groups": (C.c_int, [vp]),
+        "fr_batch_group": (C.c_int, [vp, C.c_int, C.POINTER(vp)]),
+        "fr_batch_instance": (C.c_int, [vp, C.c_int, ip]),
+        "fr_batch_set_state": (C.c_int, [vp, C.c_int, dp]),
+        "fr_batch_get_state": (C.c_int, [vp, C.c_int, dp]),
+        "fr_batch_autotune": (C.c_int, [vp, C.c_int]),
+        "fr_batch_advance": (C.c_int, [vp, C.c_int, C.c_double, vp]),
+        "fr_batch_launch_count": (C.c_longlong, [vp]),
+        "fr_batch_stream": (vp, [vp]),
         "fr_restart_write": (C.c_int, [C.c_char_p, C.c_double, vp, C.c_int]),
         "fr_restart_read": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp, dp, dp]),
         "fr_solver_write_restart": (C.c_int, [vp, C.c_char_p, C.c_double]),
@@ -443,3 +454,81 @@ def restart_read(path, ele_type, order, n_eles, n_fields, upts_type=0, ele2globa
     _check(lib().fr_restart_read(str(path).encode(), int(ele_type), int(order), int(upts_type), int(n_eles),
                                  int(n_fields), None if g is None else g.ctypes.data, _dp(u), C.byref(t)))
     return u, t.value
+
+
+# ---------------------------------------------------------------- batches
+
+class Batch:
+    """Independent meshes advanced together: instances with the same dims and
+    scheme are merged into one group (one launch per stage kernel), and a
+    step of all groups is one CUDA graph.  instances: list of dicts with the
+    Solver.box arguments (dims, order, n, lo, hi, jitter, seed, side_bc and
+    the scheme keywords)."""
+
+    def __init__(self, instances, device=0):
+        L = lib()
+        n = len(instances)
+        mds, sds = (MeshDesc * n)(), (SchemeDesc * n)()
+        self._keep = []
+        for i, inst in enumerate(instances):
+            kw = dict(inst)
+            dims, order, nn, lo, hi = kw.pop("dims"), kw.pop("order"), kw.pop("n"), kw.pop("lo"), kw.pop("hi")
+            xv, c2v = box_mesh(dims, nn, lo, hi, kw.pop("jitter", 0.0), kw.pop("seed", 0))
+            shift = [hi[d] - lo[d] for d in range(dims)]
+            side_bc = kw.pop("side_bc", None)
+            if side_bc is not None:
+                shift = [0.0 if (side_bc[2 * d] or side_bc[2 * d + 1]) else shift[d] for d in range(dims)]
+                kw["bctype"] = box_bctype(dims, nn, side_bc)
+            md, sd, keep = _descs(dims, xv, c2v, shift, order, **kw)
+            mds[i], sds[i] = md, sd
+            self._keep.append(keep)
+        h = C.c_void_p()
+        self.h = None
+        _check(L.fr_batch_create(mds, sds, n, int(device), C.byref(h)))
+        self.h = h
+        self.n = n
+        self.shapes = []
+        for i in range(n):
+            o = (C.c_int * 4)()
+            _check(L.fr_batch_instance(self.h, i, o))
+            inst = instances[i]
+            self.shapes.append((o[3], o[2], inst["dims"] + 2))
+        self.n_groups = int(L.fr_batch_n_groups(self.h))
+
+    def close(self):
+        if self.h is not None:
+            lib().fr_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, i, u):
+        u = np.asfortranarray(u, dtype=np.float64)
+        if u.shape != self.shapes[i]:
+            raise ValueError("state of instance %d must have shape %s" % (i, self.shapes[i]))
+        _check(lib().fr_batch_set_state(self.h, int(i), _dp(u)))
+
+    def get_state(self, i):
+        u = np.zeros(self.shapes[i], order="F")
+        _check(lib().fr_batch_get_state(self.h, int(i), _dp(u)))
+        return u
+
+    def autotune(self, reps=3):
+        _check(lib().fr_batch_autotune(self.h, int(reps)))
+
+    def advance(self, n_steps, dt, stream=None):
+        _check(lib().fr_batch_advance(self.h, int(n_steps), float(dt), stream))
+
+    def launch_count(self):
+        return int(lib().fr_batch_launch_count(self.h))
+
+    def stream(self):
+        return lib().fr_batch_stream(self.h)
+
+    def dof(self):
+        """Degrees of freedom of the whole batch (sum of n_upts * n_eles * n_fields)."""
+        return int(sum(a * b * c for a, b, c in self.shapes))

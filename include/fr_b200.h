@@ -169,6 +169,32 @@ fr_status fr_solver_profile_stage(fr_solver* s, int reps, double dt, double* ms3
 fr_status fr_solver_gradient(fr_solver* s, double* host_grad, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Batches of independent meshes (no reference counterpart: the reference
+ * runs one mesh per process).  Instances with the same dims and scheme form a
+ * group whose meshes are merged (each keeps its own periodic wiring), so a
+ * group advances with one launch per stage kernel; fr_batch_advance runs a
+ * whole RK45 step of every group as one CUDA graph.  All instances share dt.
+ * ---------------------------------------------------------------------- */
+typedef struct fr_batch fr_batch;
+fr_status fr_batch_create(const fr_mesh_desc* meshes, const fr_scheme_desc* schemes, int n_instances, int device,
+                          fr_batch** out);
+fr_status fr_batch_destroy(fr_batch* b);
+int fr_batch_n_groups(const fr_batch* b);
+/* The solver object of group g (owned by the batch; for queries, autotuning,
+ * kinetic energy of the whole group). */
+fr_status fr_batch_group(fr_batch* b, int g, fr_solver** out);
+/* group, first element in the group, n_eles, n_upts of instance i */
+fr_status fr_batch_instance(const fr_batch* b, int i, int out4[4]);
+/* State of one instance, host memory (n_upts, n_eles_i, n_fields); setting
+ * it zeroes its RK register. */
+fr_status fr_batch_set_state(fr_batch* b, int i, const double* host_u);
+fr_status fr_batch_get_state(fr_batch* b, int i, double* host_u);
+fr_status fr_batch_autotune(fr_batch* b, int reps);
+fr_status fr_batch_advance(fr_batch* b, int n_steps, double dt, void* stream);
+long long fr_batch_launch_count(const fr_batch* b);
+void* fr_batch_stream(fr_batch* b);
+
+/* ------------------------------------------------------------------------
  * Restart files in the reference's text format (write_restart,
  * src/output.cpp:1057-1107; read_restart, src/solver.cpp:390-445).  Host
  * memory only; no GPU is touched by fr_restart_*.
