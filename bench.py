@@ -156,6 +156,101 @@ def cpu_baseline(a):
         return cpu_baseline_port()
 
 
+BATCH_SEED, BATCH_N = 2024, 64
+
+
+def batch_instances(precision):
+    """The batched configuration: 64 periodic TGV instances (NS, Mach 0.1,
+    Re 1600) with seeded sizes n^3, n in [8, 24], and orders P in [2, 4]."""
+    rng = np.random.default_rng(BATCH_SEED)
+    L = 2 * np.pi
+    out = []
+    for _ in range(BATCH_N):
+        n, P = int(rng.integers(8, 25)), int(rng.integers(2, 5))
+        out.append(dict(dims=3, order=P, n=(n, n, n), lo=(0, 0, 0), hi=(L, L, L), viscous=True, vcjh_scheme=1,
+                        gamma=GAMMA, prandtl=PR, mu_inf=1.0 / RE, tau=1.0, pen_fact=0.5, precision=precision))
+    return out
+
+
+def box_upts(n, P, L):
+    """Solution-point positions (n_upts, n_eles, 3) of the uniform periodic
+    box of n^3 hexes: element i + n (j + n k), point a + (P+1)(b + (P+1) c)."""
+    import hifiles_b200 as H
+    loc = H.line_operators(P)["loc"]
+    h = L / n
+    x1 = ((np.arange(n)[:, None] + 0.5 * (loc[None, :] + 1.0)) * h)        # [cell, point]
+    i, j, k = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    e_i, e_j, e_k = i.transpose(2, 1, 0).ravel(), j.transpose(2, 1, 0).ravel(), k.transpose(2, 1, 0).ravel()
+    a, b, c = np.meshgrid(np.arange(P + 1), np.arange(P + 1), np.arange(P + 1), indexing="ij")
+    pa, pb, pc = a.transpose(2, 1, 0).ravel(), b.transpose(2, 1, 0).ravel(), c.transpose(2, 1, 0).ravel()
+    pos = np.empty(((P + 1) ** 3, n ** 3, 3), order="F")
+    pos[:, :, 0] = x1[e_i[None, :], pa[:, None]]
+    pos[:, :, 1] = x1[e_j[None, :], pb[:, None]]
+    pos[:, :, 2] = x1[e_k[None, :], pc[:, None]]
+    return pos
+
+
+def _time_steps(advance, stream, steps):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    advance(steps)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def measure_forms(a, dev, fp64_value, s64, u0):
+    """The precision and batching forms beside the FP64 headline: the FP32
+    form on the same workload with its L2 error against the FP64 path after 20
+    steps, and the 64-instance batch in FP64 and FP32 (one CUDA graph per
+    step, autotuned tiles per group)."""
+    import torch
+    import hifiles_b200 as H
+    n, P, L = a.n, a.order, 2 * np.pi
+    dt, steps = 1e-3, max(5, min(a.steps, 20))
+    s32 = H.Solver.box(3, P, (n, n, n), (0, 0, 0), (L, L, L), viscous=True, vcjh_scheme=1, gamma=GAMMA, prandtl=PR,
+                       mu_inf=1.0 / RE, rt_inf=1.0, c_sth=1.0, fix_vis=1.0, tau=1.0, pen_fact=0.5, precision=1,
+                       device=dev)
+    s32.set_state(u0)
+    s32.autotune(3)
+    st32 = torch.cuda.ExternalStream(s32.stream(), device=dev)
+    s32.advance(3, dt)
+    ms32 = _time_steps(lambda k: s32.advance(k, dt), st32, steps)
+    dof_step = s32.n_eles * s32.n_upts * s32.n_fields * 5
+    s64.set_state(u0)
+    s32.set_state(u0)
+    s64.advance(20, dt)
+    s32.advance(20, dt)
+    u64, u32 = s64.get_state(), s32.get_state()
+    l2 = float(np.linalg.norm(u32 - u64) / np.linalg.norm(u64))
+    s32.close()
+    out = {"fp32": {"value": dof_step / (ms32 * 1e-3), "ms_per_step": ms32, "l2_rel_vs_fp64_after_20_steps": l2,
+                    "ratio_to_fp64": dof_step / (ms32 * 1e-3) / fp64_value}}
+    for prec, name in ((0, "batched_fp64"), (1, "batched_fp32")):
+        insts = batch_instances(prec)
+        t0 = time.perf_counter()
+        b = H.Batch(insts, device=dev)
+        setup_s = time.perf_counter() - t0
+        states = []
+        for i, inst in enumerate(insts):
+            b.set_state(i, tgv_state(box_upts(inst["n"][0], inst["order"], L)))
+        b.autotune(2)
+        stb = torch.cuda.ExternalStream(b.stream(), device=dev)
+        b.advance(3, dt)
+        l0 = b.launch_count()
+        msb = _time_steps(lambda k: b.advance(k, dt), stb, steps)
+        launches_per_step = (b.launch_count() - l0) // steps
+        v = b.dof() * 5 / (msb * 1e-3)
+        out[name] = {"value": v, "ms_per_step": msb, "ratio_to_fp64": v / fp64_value, "groups": b.n_groups,
+                     "launches_per_step": launches_per_step, "graphs_per_step": 1, "setup_s": setup_s}
+        b.close()
+    out["batch"] = ("%d periodic TGV instances (NS, Mach 0.1, Re 1600), sizes n^3 with n in [8, 24] and P in "
+                    "[2, 4] drawn with seed %d; DOF-updates per RK stage over all instances" % (BATCH_N, BATCH_SEED))
+    return out
+
+
 def run_b200(a, rank, world, local):
     import torch
     import hifiles_b200 as H
@@ -241,6 +336,7 @@ def run_b200(a, rank, world, local):
            "ms_per_step": e2e_ms,
            "path": "Solver.set_state(pinned host state) + Solver.advance(1 step, norms) -> C ABI"}
 
+    forms = measure_forms(a, dev, value / world, s, u0) if (world == 1 and not a.no_forms) else None
     cpu = cpu_baseline(a) if (rank == 0 and world == 1 and not a.no_cpu) else None
     if world > 1:
         torch.distributed.barrier()
@@ -267,6 +363,7 @@ def run_b200(a, rank, world, local):
                      "alg_bytes_per_element": b_elem, "traffic": traffic,
                      "ms_grad": ms_grad, "ms_face": ms_face, "ms_update": ms_upd, "ms_stage": stage_ms},
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
+        "forms": forms,
     }
     print(json.dumps(out))
 
@@ -282,6 +379,7 @@ def main():
     ap.add_argument("--order", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the FP32 and batched forms")
     a = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
