@@ -20,6 +20,9 @@ thread_local std::string g_err;
 cudaError_t launch_sgs_inputs(int dims, int tc_size, const double* U, const void* G, const double* detj, long long npts,
                               int nu, long long E, int order, double filter_ratio, float* X, cudaStream_t st);
 void mlp_default_params(float* w);
+cudaError_t launch_diagnostics(int dims, int tc_size, const double* U, const void* G, const double* detj,
+                               const double* W, long long npts, int nu, double gamma, double* partial, int nblk,
+                               double* out, cudaStream_t st);
 
 static fr_status fail(fr_status s, const std::string& msg)
 {
@@ -70,6 +73,7 @@ struct fr_solver {
   float* mlp = nullptr;             // learned-closure parameters (sgs_model 5)
   void* grad_buf = nullptr;         // gradient output of fr_solver_gradient (allocated on first use)
   float* feat_buf = nullptr;        // closure inputs of fr_solver_sgs_features (allocated on first use)
+  double *diag_w = nullptr, *diag_partial = nullptr, *diag_out = nullptr;   // integral diagnostics
   std::vector<void*> allocs;
 };
 
@@ -652,6 +656,43 @@ fr_status fr_solver_gradient(fr_solver* s, double* host_grad, void* stream)
   return FR_OK;
 }
 
+fr_status fr_solver_integral_quantities(fr_solver* s, double out5[5], void* stream)
+{
+  if (!s || !out5) return fail(FR_ERR_ARG, "null argument");
+  if (!s->sch.viscous) return fail(FR_ERR_UNSUPPORTED, "the integral quantities need the gradient: viscous path only");
+  FR_CUDA(cudaSetDevice(s->device));
+  cudaStream_t st = STRM(s, stream);
+  const Mesh& m = s->mesh;
+  const int nblk = 296;
+  fr_status r;
+  if (!s->diag_w) {
+    std::vector<double> w((size_t)m.nu);
+    for (int u = 0; u < m.nu; u++) {
+      int a = u % m.n1, b = (u / m.n1) % m.n1, c = m.dims == 3 ? u / (m.n1 * m.n1) : 0;
+      w[u] = s->line.w[a] * s->line.w[b] * (m.dims == 3 ? s->line.w[c] : 1.0);
+    }
+    if ((r = dalloc(s, &s->diag_w, (size_t)m.nu))) return r;
+    if ((r = dalloc(s, &s->diag_partial, (size_t)nblk * 5))) return r;
+    if ((r = dalloc(s, &s->diag_out, 5))) return r;
+    FR_CUDA(cudaMemcpy(s->diag_w, w.data(), w.size() * 8, cudaMemcpyHostToDevice));
+  }
+  const size_t n = (size_t)m.nu * m.ne * m.nfields * m.dims;
+  if (!s->grad_buf) {
+    char* p;
+    if ((r = dalloc(s, &p, n * s->tc_size))) return r;
+    s->grad_buf = p;
+  }
+  Bufs b = s->b;
+  b.GRAD = s->grad_buf;
+  s->run->grad(b, s->cur, st);
+  FR_CUDA(launch_diagnostics(m.dims, (int)s->tc_size, s->b.U, s->grad_buf, s->b.detj64, s->diag_w,
+                             (long long)m.nu * m.ne, m.nu, s->sch.gamma, s->diag_partial, nblk, s->diag_out, st));
+  s->launches += 3;
+  FR_CUDA(cudaMemcpyAsync(out5, s->diag_out, 5 * 8, cudaMemcpyDeviceToHost, st));
+  FR_CUDA(cudaStreamSynchronize(st));
+  return FR_OK;
+}
+
 fr_status fr_solver_sgs_features(fr_solver* s, float* host_x, void* stream)
 {
   if (!s || !host_x) return fail(FR_ERR_ARG, "null argument");
@@ -983,3 +1024,13 @@ long long fr_batch_launch_count(const fr_batch* b) { return b ? b->launches : 0;
 void* fr_batch_stream(fr_batch* b) { return b ? (void*)b->stream : nullptr; }
 
 }  // extern "C"
+
+extern "C" fr_status fr_solver_write_vtu(fr_solver* s, const char* path)
+{
+  if (!s || !path) return fail(FR_ERR_ARG, "null argument");
+  const Mesh& m = s->mesh;
+  std::vector<double> u((size_t)m.nu * m.ne * m.nfields);
+  fr_status r = fr_solver_get_state(s, u.data(), nullptr);
+  if (r) return r;
+  return fr_vtu_write(path, m.dims, s->sch.order, (int)m.ne, m.pos_upts.data(), u.data(), s->sch.gamma);
+}

@@ -102,6 +102,9 @@ def lib():
         "fr_mesh_geometry": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(SchemeDesc), ip, dp, dp, dp, dp, dp, ip, ip]),
         "fr_line_operators": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, dp]),
         "fr_solver_gradient": (C.c_int, [vp, dp, vp]),
+        "fr_solver_integral_quantities": (C.c_int, [vp, dp, vp]),
+        "fr_vtu_write": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, dp, dp, C.c_double]),
+        "fr_solver_write_vtu": (C.c_int, [vp, C.c_char_p]),
         "fr_batch_create": (C.c_int, [vp, vp, C.c_int, C.c_int, C.POINTER(vp)]),
         "fr_batch_destroy": (C.c_int, [vp]),
         "fr_batch_n_groups": (C.c_int, [vp]),
@@ -350,6 +353,18 @@ class Solver:
         _check(lib().fr_solver_read_restart(self.h, str(path).encode(), C.byref(t)))
         return t.value
 
+    def write_vtu(self, path):
+        """The current state as a .vtu file (solution points, sub-cells per element)."""
+        _check(lib().fr_solver_write_vtu(self.h, str(path).encode()))
+
+    def integral_quantities(self, stream=None):
+        """kinetic energy, enstrophy, pressure dilatation, strain colon product,
+        deviatoric strain colon product of the current state (viscous solvers)."""
+        out = np.zeros(5)
+        _check(lib().fr_solver_integral_quantities(self.h, _dp(out), stream))
+        return dict(zip(("kineticenergy", "vorticity", "pressuredilatation", "straincolonproduct",
+                         "devstraincolonproduct"), out.tolist()))
+
     def gradient(self, stream=None):
         """Corrected physical gradient grad_disu_upts (n_upts, n_eles, n_fields, n_dims)."""
         g = np.zeros((self.n_upts, self.n_eles, self.n_fields, self.dims), order="F")
@@ -532,3 +547,10 @@ class Batch:
     def dof(self):
         """Degrees of freedom of the whole batch (sum of n_upts * n_eles * n_fields)."""
         return int(sum(a * b * c for a, b, c in self.shapes))
+
+
+def vtu_write(path, dims, order, pos_upts, disu_upts, gamma=1.4):
+    """Host-only .vtu writer (see fr_vtu_write)."""
+    pos = np.asfortranarray(pos_upts, dtype=np.float64)
+    u = np.asfortranarray(disu_upts, dtype=np.float64)
+    _check(lib().fr_vtu_write(str(path).encode(), int(dims), int(order), u.shape[1], _dp(pos), _dp(u), float(gamma)))

@@ -168,6 +168,15 @@ fr_status fr_solver_profile_stage(fr_solver* s, int reps, double dt, double* ms3
  * layout (n_upts, n_eles, n_fields, n_dims).  Viscous solvers only. */
 fr_status fr_solver_gradient(fr_solver* s, double* host_grad, void* stream);
 
+/* Integral diagnostics of the current state on the device, the quantities of
+ * eles::CalcIntegralQuantities (src/eles.cpp:6503-6641): out5 = kinetic
+ * energy, enstrophy (rho |curl u|^2 / 2, the reference's "vorticity"),
+ * pressure dilatation, strain colon product, deviatoric strain colon
+ * product, each integrated with the tensor Gauss rule of the solution points
+ * (the reference interpolates to a separate volume cubature rule).  Viscous
+ * solvers only (the corrected gradient comes from the gradient kernel). */
+fr_status fr_solver_integral_quantities(fr_solver* s, double out5[5], void* stream);
+
 /* ------------------------------------------------------------------------
  * Batches of independent meshes (no reference counterpart: the reference
  * runs one mesh per process).  Instances with the same dims and scheme form a
@@ -219,6 +228,16 @@ fr_status fr_restart_write(const char* path, double time, const fr_restart_block
  * element must be present.  time_out may be NULL. */
 fr_status fr_restart_read(const char* path, int ele_type, int order, int upts_type, int n_eles, int n_fields,
                           const int* ele2global, double* disu_upts, double* time_out);
+/* A solution as a VTK unstructured grid (.vtu, inline base64 binary), the
+ * role of the reference's Paraview output (src/output.cpp:580-1055): points
+ * are the solution points (pos_upts, (n_upts, n_eles, dims)), each element is
+ * cut into order^dims sub-cells joining neighbouring points, point data
+ * Density, Velocity, Pressure, Energy (float32).  Host memory only. */
+fr_status fr_vtu_write(const char* path, int dims, int order, int n_eles, const double* pos_upts,
+                       const double* disu_upts, double gamma);
+/* The solver's current state as such a file (one device-to-host copy). */
+fr_status fr_solver_write_vtu(fr_solver* s, const char* path);
+
 /* The solver's state to / from a restart file (global ids 0 .. n_eles-1). */
 fr_status fr_solver_write_restart(fr_solver* s, const char* path, double time);
 fr_status fr_solver_read_restart(fr_solver* s, const char* path, double* time_out);
