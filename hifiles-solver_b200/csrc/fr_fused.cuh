@@ -208,14 +208,9 @@ __device__ __forceinline__ T interp_code(const Line<T>& L, int c, const S* s)
 template <int DIM, int P> struct GradPlan;
 template <int DIM, int P, int EPB, typename TC, int LES = 0>
 __host__ __device__ constexpr size_t grad_smem_bytes();
-template <int DIM, int P, int EPB, int NT, int VISC, typename TC>
-__host__ __device__ constexpr size_t update_smem_bytes()
-{
-  using S = Shape<DIM, P>;
-  return blockops_bytes<TC, S::NF>() + sizeof(double) * (EPB * S::F * S::NU + (NT / 32) * S::F) +
-         sizeof(TC) * EPB * S::F * S::NF +
-         (VISC ? 0 : sizeof(TC) * EPB * DIM * S::F * S::NU);
-}
+template <int DIM, int P, int EPB, int NT, int VISC, int MODE, typename TC> struct UpdPlan;
+template <int DIM, int P, int EPB, int NT, int VISC, int MODE, typename TC>
+__host__ __device__ constexpr size_t update_smem_bytes();
 
 template <int NT, int ITEMS>
 struct Items {
@@ -769,7 +764,45 @@ fr_face_kernel(const int2* __restrict__ face, const unsigned char* __restrict__ 
 // stage's traces (MODE 1).  The inviscid path (VISC 0) evaluates the flux,
 // its divergence and its normal component here itself, in the reference's
 // order; the viscous path takes DV and ND from fr_grad_kernel.
+// Shared-memory plan of fr_update_kernel (byte offsets, every region
+// rounded up to 16 bytes): state and RK register (FP64), detJ (FP64), common
+// normal flux CF (overwritten in place by norm_tconf - norm_tdisf), ND and DV
+// (viscous path), transformed flux and JGinv (inviscid path), norm partials.
 template <int DIM, int P, int EPB, int NT, int VISC, int MODE, typename TC>
+struct UpdPlan {
+  using S = Shape<DIM, P>;
+  __host__ __device__ static constexpr size_t r16(size_t b) { return (b + 15) / 16 * 16; }
+  static constexpr size_t bU = r16(sizeof(double) * EPB * S::F * S::NU);
+  static constexpr size_t bREG = MODE == 1 ? bU : 0;
+  static constexpr size_t bDJ = MODE == 1 ? r16(sizeof(double) * EPB * S::NU) : 0;
+  static constexpr size_t bCF = r16(sizeof(TC) * EPB * S::F * S::NF);
+  static constexpr size_t bND = VISC ? bCF : 0;
+  static constexpr size_t bDV = VISC ? r16(sizeof(TC) * EPB * S::F * S::NU) : 0;
+  static constexpr size_t bFL = VISC ? 0 : r16(sizeof(TC) * EPB * DIM * S::F * S::NU);
+  static constexpr size_t bJ = VISC ? 0 : r16(sizeof(TC) * EPB * DIM * DIM * S::NU);
+  static constexpr size_t bRED = r16(sizeof(double) * (NT / 32) * S::F);
+  static constexpr size_t oU = 0, oREG = oU + bU, oDJ = oREG + bREG, oCF = oDJ + bDJ, oND = oCF + bCF,
+                          oDV = oND + bND, oFL = oDV + bDV, oJ = oFL + bFL, oRED = oJ + bJ, total = oRED + bRED;
+};
+
+template <int DIM, int P, int EPB, int NT, int VISC, int MODE, typename TC>
+__host__ __device__ constexpr size_t update_smem_bytes()
+{
+  return blockops_bytes<TC, Shape<DIM, P>::NF>() + UpdPlan<DIM, P, EPB, NT, VISC, MODE, TC>::total;
+}
+
+// Stage, last part (per element): norm_tconf - norm_tdisf, the VCJH
+// correction (calculate_corrected_divergence, src/eles.cpp:1594-1661), and
+// either the residual (MODE 0) or the RK45 stage update
+// (eles::AdvanceSolution, src/eles.cpp:1155-1178) followed by the next
+// stage's traces (MODE 1).  The inviscid path (VISC 0) evaluates the flux,
+// its divergence and its normal component here itself, in the reference's
+// order; the viscous path takes DV and ND from fr_grad_kernel.  Every
+// per-element input reaches shared memory through cp.async (16-byte copies
+// where the element runs allow, VEC = 1; element-sized with VEC = 0 for
+// inputs only 8-byte aligned), so all of a block's loads are in flight
+// together.
+template <int DIM, int P, int EPB, int NT, int VISC, int MODE, typename TC, int VEC = 1>
 __global__ void __launch_bounds__(NT)
 fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restrict__ UFn, const TC* __restrict__ CF,
                  const TC* __restrict__ ND, const TC* __restrict__ DV, const TC* __restrict__ JG,
@@ -777,66 +810,73 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
                  Line<TC> L, PhysT<TC> ph, double rk_a, double rk_b, double dt, int first_stage)
 {
   using S = Shape<DIM, P>;
-  constexpr int NU = S::NU, NF = S::NF, F = S::F, D = DIM;
+  using Q = UpdPlan<DIM, P, EPB, NT, VISC, MODE, TC>;
+  constexpr int NU = S::NU, NF = S::NF, F = S::F, D = DIM, DD = DIM * DIM;
   extern __shared__ __align__(16) unsigned char fr_smem[];
-  // B: operator pieces and flux-point line table; sU: solution (FP64), sRed:
-  // norm partials, sC: norm_tconf - norm_tdisf, sFl: transformed inviscid
-  // flux (inviscid path only)
   auto B = reinterpret_cast<BlockOps<TC, NF>*>(fr_smem);
   unsigned char* sm0 = fr_smem + blockops_bytes<TC, NF>();
-  auto sU = reinterpret_cast<double (*)[F][NU]>(sm0);
-  auto sRed = reinterpret_cast<double (*)[F]>(sm0 + sizeof(double) * EPB * F * NU);
-  auto sC = reinterpret_cast<TC (*)[F][NF]>(sm0 + sizeof(double) * (EPB * F * NU + (NT / 32) * F));
-  auto sFl = reinterpret_cast<TC (*)[D][F][NU]>(sm0 + sizeof(double) * (EPB * F * NU + (NT / 32) * F) +
-                                                 sizeof(TC) * EPB * F * NF);
+  auto sU = reinterpret_cast<double (*)[F][NU]>(sm0 + Q::oU);
+  auto sREG = reinterpret_cast<double (*)[F][NU]>(sm0 + Q::oREG);
+  auto sDJ = reinterpret_cast<double (*)[NU]>(sm0 + Q::oDJ);
+  auto sC = reinterpret_cast<TC (*)[F][NF]>(sm0 + Q::oCF);
+  auto sND = reinterpret_cast<TC (*)[F][NF]>(sm0 + Q::oND);
+  auto sDV = reinterpret_cast<TC (*)[F][NU]>(sm0 + Q::oDV);
+  auto sFl = reinterpret_cast<TC (*)[D][F][NU]>(sm0 + Q::oFL);
+  auto sJ = reinterpret_cast<TC (*)[DD * NU]>(sm0 + Q::oJ);
+  auto sRed = reinterpret_cast<double (*)[F]>(sm0 + Q::oRED);
   fill_blockops<DIM, P, TC, NF>(B, L, threadIdx.x, NT);
   const long long e0 = (long long)blockIdx.x * EPB;
-  const long long NFE = (long long)NF * E;
+  const int nval = (int)(E - e0 < EPB ? E - e0 : EPB);
 
-  // per-point inputs of this thread's solution points, requested before the
-  // block-wide loads so that all of them are in flight together
-  constexpr int IU = Items<NT, EPB * NU>::N;
-  TC pdv[IU][F];
-  double preg[IU][F], pdj[IU];
-#pragma unroll
-  for (int it = 0; it < IU; it++) {
-    int w = threadIdx.x + it * NT, el = w / NU, u = w - el * NU;
-    long long e = e0 + el;
-    if (w < EPB * NU && e < E) {
-      if (MODE == 1) pdj[it] = detj[u + (size_t)NU * e];
-#pragma unroll
-      for (int k = 0; k < F; k++) {
-        size_t gi = u + (size_t)NU * (e + E * k);
-        if (VISC) pdv[it][k] = DV[gi];
-        if (MODE == 1) preg[it][k] = first_stage ? 0.0 : REG[gi];
-      }
+  // --- inputs to shared memory
+  constexpr int V8 = (VEC && NU % 2 == 0) ? 2 : 1;                                   // doubles per copy
+  constexpr int VF = (VEC && (NF * sizeof(TC)) % 16 == 0) ? 16 / sizeof(TC) : 1;     // flux-point runs
+  constexpr int VN = (VEC && (NU * sizeof(TC)) % 16 == 0) ? 16 / sizeof(TC) : 1;     // point runs
+  constexpr int VJ = (VEC && (DD * NU * sizeof(TC)) % 16 == 0) ? 16 / sizeof(TC) : 1;
+  const bool want_reg = MODE == 1 && !first_stage;
+  for (int w = threadIdx.x; w < nval * F * NU / V8; w += NT) {
+    int el = w / (F * NU / V8), r = w * V8 - el * F * NU, k = r / NU, u = r - k * NU;
+    size_t g = u + (size_t)NU * (e0 + el + E * k);
+    cp_async<8 * V8>(&sU[el][k][u], U + g);
+    if (want_reg) cp_async<8 * V8>(&sREG[el][k][u], REG + g);
+  }
+  if (MODE == 1)
+    for (int w = threadIdx.x; w < nval * NU / V8; w += NT) {
+      int el = (w * V8) / NU, u = w * V8 - el * NU;
+      cp_async<8 * V8>(&sDJ[el][u], detj + (size_t)NU * e0 + (size_t)w * V8);
     }
+  for (int w = threadIdx.x; w < nval * F * NF / VF; w += NT) {
+    int el = w / (F * NF / VF), r = w * VF - el * F * NF, k = r / NF, f = r - k * NF;
+    size_t g = f + (size_t)NF * (e0 + el + E * k);
+    cp_async<sizeof(TC) * VF>(&sC[el][k][f], CF + g);
+    if (VISC) cp_async<sizeof(TC) * VF>(&sND[el][k][f], ND + g);
   }
-  for (int w = threadIdx.x; w < EPB * F * NU; w += NT) {
-    int el = w / (F * NU), r = w - el * F * NU, k = r / NU, u = r - k * NU;
-    long long e = e0 + el;
-    sU[el][k][u] = e < E ? U[u + (size_t)NU * (e + E * k)] : 1.0;
-  }
+  if (VISC)
+    for (int w = threadIdx.x; w < nval * F * NU / VN; w += NT) {
+      int el = w / (F * NU / VN), r = w * VN - el * F * NU, k = r / NU, u = r - k * NU;
+      cp_async<sizeof(TC) * VN>(&sDV[el][k][u], DV + u + (size_t)NU * (e0 + el + E * k));
+    }
+  else
+    for (int w = threadIdx.x; w < nval * DD * NU / VJ; w += NT) {
+      int el = (w * VJ) / (DD * NU), r = w * VJ - el * DD * NU;
+      cp_async<sizeof(TC) * VJ>(&sJ[el][r], JG + (size_t)DD * NU * e0 + (size_t)w * VJ);
+    }
+  cp_async_commit();
+  cp_async_wait_all();
+  __syncthreads();
+
   if (VISC) {
-    for (int w = threadIdx.x; w < EPB * F * NF; w += NT) {
+    for (int w = threadIdx.x; w < nval * F * NF; w += NT) {
       int el = w / (F * NF), r = w - el * F * NF, k = r / NF, f = r - k * NF;
-      long long e = e0 + el;
-      if (e < E) {
-        size_t g = f + (size_t)NF * (e + E * k);
-        sC[el][k][f] = CF[g] - ND[g];      // daxpy(-1, norm_tdisf, norm_tconf)
-      }
+      sC[el][k][f] = sC[el][k][f] - sND[el][k][f];      // daxpy(-1, norm_tdisf, norm_tconf)
     }
   } else {
-    __syncthreads();
     // transformed inviscid flux at the solution points (evaluate_invFlux, src/eles.cpp:1331-1418)
-    for (int w = threadIdx.x; w < EPB * NU; w += NT) {
+    for (int w = threadIdx.x; w < nval * NU; w += NT) {
       int el = w / NU, u = w - el * NU;
-      long long e = e0 + el;
-      if (e >= E) continue;
-      const TC* G = JG + (size_t)D * D * (u + (size_t)NU * e);
-      TC g[D * D];
+      TC g[DD];
 #pragma unroll
-      for (int q = 0; q < D * D; q++) g[q] = G[q];
+      for (int q = 0; q < DD; q++) g[q] = sJ[el][DD * u + q];
       TC q[F], fi[F][D];
 #pragma unroll
       for (int k = 0; k < F; k++) q[k] = (TC)sU[el][k][u];
@@ -853,16 +893,14 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
     }
     __syncthreads();
     // norm_tconf - norm_tdisf with the normal component extrapolated here (extrapolate_totalFlux)
-    for (int w = threadIdx.x; w < EPB * NF; w += NT) {
+    for (int w = threadIdx.x; w < nval * NF; w += NT) {
       int el = w / NF, f = w - el * NF;
-      long long e = e0 + el;
-      if (e >= E) continue;
       const int cd = B->code[f];
       const bool plus = code_plus(cd);
 #pragma unroll
       for (int k = 0; k < F; k++) {
         TC v = interp_code<P, TC, TC>(L, cd, &sFl[el][code_ax(cd)][k][0]);
-        sC[el][k][f] = CF[f + (size_t)NF * (e + E * k)] - (plus ? v : -v);
+        sC[el][k][f] = sC[el][k][f] - (plus ? v : -v);
       }
     }
   }
@@ -871,11 +909,12 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
   double red[F];
 #pragma unroll
   for (int k = 0; k < F; k++) red[k] = 0.0;
+  constexpr int IU = Items<NT, EPB * NU>::N;
 #pragma unroll
   for (int it = 0; it < IU; it++) {
     int w = threadIdx.x + it * NT, el = w / NU, u = w - el * NU;
-    long long e = e0 + el;
-    if (w >= EPB * NU || e >= E) continue;
+    if (w >= EPB * NU || el >= nval) continue;
+    const long long e = e0 + el;
     int abc[3];
     upt_abc<DIM, P>(u, abc[0], abc[1], abc[2]);
 #pragma unroll
@@ -883,7 +922,7 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
       size_t gi = u + (size_t)NU * (e + E * k);
       TC acc;
       if (VISC) {
-        acc = pdv[it][k];
+        acc = sDV[el][k][u];
       } else {
         acc = TC(0);
 #pragma unroll
@@ -905,8 +944,8 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
       if (MODE == 0) {
         DIV[gi] = R;
       } else {
-        double rhs = -R / pdj[it];
-        double res = first_stage ? dt * rhs : rk_a * preg[it][k] + dt * rhs;
+        double rhs = -R / sDJ[el][u];
+        double res = first_stage ? dt * rhs : rk_a * sREG[el][k][u] + dt * rhs;
         REG[gi] = res;
         double un = sU[el][k][u] + rk_b * res;
         U[gi] = un;
@@ -934,10 +973,9 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
       partial[(size_t)blockIdx.x * F + threadIdx.x] = v;
     }
     // traces of the updated state for the next stage
-    for (int w = threadIdx.x; w < EPB * NF; w += NT) {
+    for (int w = threadIdx.x; w < nval * NF; w += NT) {
       int el = w / NF, f = w - el * NF;
       long long e = e0 + el;
-      if (e >= E) continue;
       const int cd = B->code[f];
 #pragma unroll
       for (int k = 0; k < F; k++)

@@ -140,19 +140,19 @@ fr_status run(const fr_residual_args* a, double* scratch, cudaStream_t s)
                                                        a->tdA_fpts, CF, NFE, ph);
   }
   if (visc) {
-    constexpr size_t sm = update_smem_bytes<DIM, P, EPB, NT, 1, double>();
+    constexpr size_t sm = update_smem_bytes<DIM, P, EPB, NT, 1, 0, double>();
     if (sm > 48 * 1024)
-      cudaFuncSetAttribute(fr_update_kernel<DIM, P, EPB, NT, 1, 0, double>,
+      cudaFuncSetAttribute(fr_update_kernel<DIM, P, EPB, NT, 1, 0, double, 0>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    fr_update_kernel<DIM, P, EPB, NT, 1, 0, double><<<nblk, NT, sm, s>>>(
+    fr_update_kernel<DIM, P, EPB, NT, 1, 0, double, 0><<<nblk, NT, sm, s>>>(
         const_cast<double*>(a->disu_upts), nullptr, nullptr, CF, ND, DV, a->JGinv_upts, a->detjac_upts, a->div_tconf_upts, nullptr, E, L, ph,
         0.0, 0.0, 0.0, 0);
   } else {
-    constexpr size_t sm = update_smem_bytes<DIM, P, EPB, NT, 0, double>();
+    constexpr size_t sm = update_smem_bytes<DIM, P, EPB, NT, 0, 0, double>();
     if (sm > 48 * 1024)
-      cudaFuncSetAttribute(fr_update_kernel<DIM, P, EPB, NT, 0, 0, double>,
+      cudaFuncSetAttribute(fr_update_kernel<DIM, P, EPB, NT, 0, 0, double, 0>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    fr_update_kernel<DIM, P, EPB, NT, 0, 0, double><<<nblk, NT, sm, s>>>(
+    fr_update_kernel<DIM, P, EPB, NT, 0, 0, double, 0><<<nblk, NT, sm, s>>>(
         const_cast<double*>(a->disu_upts), nullptr, nullptr, CF, nullptr, nullptr, a->JGinv_upts, a->detjac_upts,
         a->div_tconf_upts, nullptr, E, L, ph, 0.0, 0.0, 0.0, 0);
   }

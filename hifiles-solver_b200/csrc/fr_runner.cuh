@@ -189,7 +189,7 @@ struct RunnerT : Runner {
     if constexpr (I < NUP) {
       if (I != usel) return update_i<I + 1, VISC, MODE>(b, cur, stage, dt, want_partial, s);
       constexpr int EPB = Tiles<DIM, P>::upd[I].epb, NT = Tiles<DIM, P>::upd[I].nt;
-      constexpr size_t sm = update_smem_bytes<DIM, P, EPB, NT, VISC, TC>();
+      constexpr size_t sm = update_smem_bytes<DIM, P, EPB, NT, VISC, MODE, TC>();
       static bool once = (set_smem((const void*)fr_update_kernel<DIM, P, EPB, NT, VISC, MODE, TC>, sm), true);
       (void)once;
       fr_update_kernel<DIM, P, EPB, NT, VISC, MODE, TC><<<(unsigned)((E + EPB - 1) / EPB), NT, sm, s>>>(
