@@ -917,6 +917,16 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
     const long long e = e0 + el;
     int abc[3];
     upt_abc<DIM, P>(u, abc[0], abc[1], abc[2]);
+    // opp_3 row of u: one column per face, in flux-point order (the same for every field)
+    int qf[S::NFACE];
+    TC cf[S::NFACE];
+#pragma unroll
+    for (int fc = 0; fc < S::NFACE; fc++) {
+      int al;
+      qf[fc] = face_fpt<DIM, P>(fc, abc[0], abc[1], abc[2], al);
+      cf[fc] = face_plus<DIM>(fc) ? B->gR[al] : -B->gL[al];
+    }
+    const double dj = MODE == 1 ? sDJ[el][u] : 1.0;
 #pragma unroll
     for (int k = 0; k < F; k++) {
       size_t gi = u + (size_t)NU * (e + E * k);
@@ -932,19 +942,13 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
           for (int m = 0; m <= P; m++) acc = acc + sFl[el][d][k][ub + m * st] * B->D[abc[d]][m];
         }
       }
-      // opp_3 row of u: one column per face, in flux-point order
 #pragma unroll
-      for (int fc = 0; fc < S::NFACE; fc++) {
-        int al;
-        int q = face_fpt<DIM, P>(fc, abc[0], abc[1], abc[2], al);
-        TC cf = face_plus<DIM>(fc) ? B->gR[al] : -B->gL[al];
-        acc = acc + sC[el][k][q] * cf;
-      }
+      for (int fc = 0; fc < S::NFACE; fc++) acc = acc + sC[el][k][qf[fc]] * cf[fc];
       double R = (double)acc;
       if (MODE == 0) {
         DIV[gi] = R;
       } else {
-        double rhs = -R / sDJ[el][u];
+        double rhs = -R / dj;
         double res = first_stage ? dt * rhs : rk_a * sREG[el][k][u] + dt * rhs;
         REG[gi] = res;
         double un = sU[el][k][u] + rk_b * res;
