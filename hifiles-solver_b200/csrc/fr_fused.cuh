@@ -270,6 +270,66 @@ __device__ __forceinline__ void lds_line(const T* s, T (&v)[N])
   }
 }
 
+// Shared-memory slot of solution point u in the gradient kernel's per-field
+// point arrays.  Hexahedra of P = 3 in FP64 store point (a, b, c) at
+// 16 c + 4 ((b + c) & 3) + ((a + c) & 3): every z-plane stays one 128-byte
+// row, and the 16 points of any face plane (c, b or a fixed) fall in 16
+// distinct 8-byte bank pairs, so the flux-point phases -- one thread per
+// flux point, 16 threads per face, reading the line through their point --
+// and the line reads of the solution-point phases are free of bank
+// conflicts.  Other shapes, and 4-byte values (32 per bank row), keep the
+// natural order.
+template <int DIM, int P, typename TC>
+__device__ __forceinline__ int swz(int u)
+{
+  if constexpr (DIM == 3 && P == 3 && sizeof(TC) == 8) return (u & 48) | ((((u >> 2) + (u >> 4)) & 3) << 2) | ((u + (u >> 4)) & 3);
+  else return u;
+}
+
+// Boundary points of the gradient kernel, out of line so that the hot loop
+// bodies stay compact (most meshes have few or no boundary points).
+// LDG common solution of a boundary point: ghost state from the boundary
+// condition, then ldg_solution with flux_spec 1 or 2, u_c = (u_r + u_l)/2
+// (bdy_inters::evaluate_boundaryConditions_invFlux, src/bdy_inters.cpp:245-389);
+// writes delta = u_c - u_own and u_own at stride st.
+template <int D, typename TC>
+__device__ __noinline__ void ldg_boundary(PhysT<TC> ph, int type, const TC* uo, const TC* nb, TC* dx, TC* uf, int st)
+{
+  constexpr int F = D + 2;
+  TC ug[F];
+  bc_ghost<D, TC>(ph, type, uo, nb, ug);
+  for (int k = 0; k < F; k++) {
+    TC uc = TC(0.5) * (ug[k] + uo[k]);
+    dx[k * st] = uc - uo[k];
+    uf[k * st] = uo[k];
+  }
+}
+
+// Viscous normal flux of a boundary point, bdy_inters::evaluate_boundaryConditions_viscFlux
+// (src/bdy_inters.cpp:905-1057): own flux fv (flux_spec 1) or the ghost
+// side's with the adiabatic-wall energy gradient (flux_spec 2, types 12 and
+// 14), plus tau n (u_l - u_r), on the normal.  gf is the own gradient.
+template <int D, typename TC>
+__device__ __noinline__ void vis_boundary(PhysT<TC> ph, int type, const TC* uf, TC (*gf)[D], const TC* n,
+                                          TC (*fv)[D], TC* bv)
+{
+  constexpr int F = D + 2;
+  TC ug[F];
+  bc_ghost<D, TC>(ph, type, uf, n, ug);
+  if (type == 12 || type == 14) {
+    TC gr[F][D];
+    for (int k = 0; k < F; k++)
+      for (int d = 0; d < D; d++) gr[k][d] = gf[k][d];
+    bc_vis_gradient<D, TC>(ph, uf, ug, gr);
+    vis_flux_fast<D, TC>(ph, ug, gr, fv);
+  }
+  for (int k = 0; k < F; k++) {
+    TC fnk = (fv[k][0] + ph.tau * n[0] * (uf[k] - ug[k])) * n[0];
+    for (int d = 1; d < D; d++) fnk = fnk + (fv[k][d] + ph.tau * n[d] * (uf[k] - ug[k])) * n[d];
+    bv[k] = fnk;
+  }
+}
+
 // Shared-memory plan of fr_grad_kernel, per element, in units of TC:
 //   sU  [F][NU]      solution
 //   sX  [F][NF]      neighbour traces, then (in place) delta_disu_fpts
@@ -360,18 +420,23 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
   // --- inputs to shared memory: state, metrics, neighbour traces.  16-byte
   // copies where the per-element runs are whole 16-byte units (global bases
   // 16-byte aligned), element-sized otherwise.
-  constexpr int VU = (VEC && sizeof(TC) == 8 && NU % 2 == 0) ? 2 : 1;
+  constexpr bool SWZ = DIM == 3 && P == 3 && sizeof(TC) == 8;
+  constexpr int VU = (VEC && !SWZ && sizeof(TC) == 8 && NU % 2 == 0) ? 2 : 1;
   constexpr int VJ = (VEC && (DD * NU * sizeof(TC)) % 16 == 0) ? 16 / sizeof(TC) : 1;
   constexpr int VD = (VEC && (NU * sizeof(TC)) % 16 == 0) ? 16 / sizeof(TC) : 1;
   for (int w = threadIdx.x; w < EPB * F * NU / VU; w += NT) {
     int el = w / (F * NU / VU), r = w * VU - el * F * NU, k = r / NU, u = r - k * NU;
     if (el < nval) {
       const double* src = U + u + (size_t)NU * (e0 + el + E * k);
-      if constexpr (sizeof(TC) == 8) cp_async<8 * VU>(&FR_SU(el, k, u), src);
-      else FR_SU(el, k, u) = (TC)*src;
+      const int su = swz<DIM, P, TC>(u);
+      if constexpr (sizeof(TC) == 8) cp_async<8 * VU>(&FR_SU(el, k, su), src);
+      else FR_SU(el, k, su) = (TC)*src;
     } else {
 #pragma unroll
-      for (int v = 0; v < VU; v++) FR_SU(el, k, u + v) = TC(1);
+      for (int v = 0; v < VU; v++) {
+        const int su = swz<DIM, P, TC>(u + v);
+        FR_SU(el, k, su) = TC(1);
+      }
     }
   }
   for (int w = threadIdx.x; w < nval * DD * NU / VJ; w += NT) {
@@ -407,29 +472,34 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
     int w = threadIdx.x + it * NT, el = w / NF, f = w - el * NF;
     if (w >= EPB * NF || el >= nval) continue;
     const int cd = B->code[f];
-    if (psd[it] >> 2) {
-      // boundary point: ghost state from the boundary condition, then
-      // ldg_solution with flux_spec 1 or 2, u_c = (u_r + u_l)/2
-      // (bdy_inters::evaluate_boundaryConditions_invFlux, src/bdy_inters.cpp:245-389)
-      TC uo[F], ug[F], nb[D];
+    int sl[P + 1];
+    TC Lc[P + 1];
 #pragma unroll
-      for (int k = 0; k < F; k++) uo[k] = interp_code<P, TC, TC>(L, cd, &FR_SU(el, k, 0));
+    for (int m = 0; m <= P; m++) {
+      sl[m] = swz<DIM, P, TC>(code_u0(cd) + m * code_st(cd));
+      Lc[m] = code_plus(cd) ? L.Lp[m] : L.Lm[m];
+    }
+    // the reference's opp_0 row of f in column order, (((0 + t0) + t1) + ...)
+    auto trace = [&](int k) {
+      TC acc = TC(0);
+#pragma unroll
+      for (int m = 0; m <= P; m++) acc = acc + FR_SU(el, k, sl[m]) * Lc[m];
+      return acc;
+    };
+    if (psd[it] >> 2) {
+      TC uo[F], nb[D];
+#pragma unroll
+      for (int k = 0; k < F; k++) uo[k] = trace(k);
       const size_t own = f + (size_t)NF * (e0 + el);
 #pragma unroll
       for (int d = 0; d < D; d++) nb[d] = nL[own + NFE * d];
-      bc_ghost<D, TC>(ph, psd[it] >> 2, uo, nb, ug);
-#pragma unroll
-      for (int k = 0; k < F; k++) {
-        TC uc = TC(0.5) * (ug[k] + uo[k]);
-        FR_SX(el, k, f) = uc - uo[k];
-        FR_SUF(el, k, f) = uo[k];
-      }
+      ldg_boundary<D, TC>(ph, psd[it] >> 2, uo, nb, &FR_SX(el, 0, f), &FR_SUF(el, 0, f), NF);
       continue;
     }
     TC pen = (psd[it] & 2) ? -ph.pen_fact : ph.pen_fact;
 #pragma unroll
     for (int k = 0; k < F; k++) {
-      TC uo = interp_code<P, TC, TC>(L, cd, &FR_SU(el, k, 0));
+      TC uo = trace(k);
       TC un = FR_SX(el, k, f);
       TC ul = (psd[it] & 1) ? uo : un, ur = (psd[it] & 1) ? un : uo;
       TC uc = TC(0.5) * (ul + ur) - pen * (ul - ur);
@@ -457,17 +527,21 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
       int qp = face_fpt<DIM, P>(fp, abc[0], abc[1], abc[2], ap);
       const int st = upt_stride<DIM, P>(d), ub = u - i * st;
       TC Dr[P + 1];
+      int sl[P + 1];
 #pragma unroll
-      for (int m = 0; m <= P; m++) Dr[m] = B->D[i][m];
+      for (int m = 0; m <= P; m++) {
+        Dr[m] = B->D[i][m];
+        sl[m] = swz<DIM, P, TC>(ub + m * st);
+      }
       const TC gm = B->gL[am], gpl = B->gR[ap];
 #pragma unroll
       for (int k = 0; k < F; k++) {
         // the gradient only feeds the viscous flux: contracted with FMAs
         TC v[P + 1];
-        if (d == 0) lds_line<P + 1, TC>(&FR_SU(el, k, ub), v);
+        if (!SWZ && d == 0) lds_line<P + 1, TC>(&FR_SU(el, k, ub), v);
         else {
 #pragma unroll
-          for (int m = 0; m <= P; m++) v[m] = FR_SU(el, k, ub + m * st);
+          for (int m = 0; m <= P; m++) v[m] = FR_SU(el, k, sl[m]);
         }
         TC acc = v[0] * Dr[0];
 #pragma unroll
@@ -477,6 +551,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
         gr[k][d] = acc;
       }
     }
+    const int su = swz<DIM, P, TC>(u);
     TC g[DD];
 #pragma unroll
     for (int q = 0; q < DD; q++) g[q] = FR_SM(el, DD * u + q);
@@ -492,13 +567,13 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
         TC acc = fr_fma(gr[k][1], m1, gr[k][0] * m0);
         if (D == 3) acc = fr_fma(gr[k][2], m2, acc);
         gp[k][c] = acc;
-        FR_SG(el, k + F * c, u) = acc;
+        FR_SG(el, k + F * c, su) = acc;
         if (GRAD) GRAD[u + (size_t)NU * (e0 + el + E * (k + (long long)F * c))] = acc;
       }
     }
     TC q[F];
 #pragma unroll
-    for (int k = 0; k < F; k++) q[k] = FR_SU(el, k, u);
+    for (int k = 0; k < F; k++) q[k] = FR_SU(el, k, su);
     TC fi[F][D], fv[F][D];
     inv_flux<D, TC>(ph, q, fi);
     vis_flux_fast<D, TC>(ph, q, gp, fv);
@@ -512,7 +587,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
           TC a = g[l] * fs[k][0];
 #pragma unroll
           for (int m = 1; m < D; m++) a = a + g[l + D * m] * fs[k][m];
-          FR_SS(el, (k - 1) + (F - 1) * l, u) = a;
+          FR_SS(el, (k - 1) + (F - 1) * l, su) = a;
           fv[k][l] = fv[k][l] + fs[k][l];
         }
     }
@@ -526,7 +601,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
         for (int m = 1; m < D; m++) acc = acc + g[l + D * m] * fi[k][m];
 #pragma unroll
         for (int m = 0; m < D; m++) acc = fr_fma(g[l + D * m], fv[k][m], acc);
-        FR_SFL(el, l, k, u) = acc;
+        FR_SFL(el, l, k, su) = acc;
       }
   }
   __syncthreads();
@@ -551,16 +626,22 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
 #pragma unroll
       for (int m = 0; m <= P; m++) Dm[d][m] = B->D[abc[d]][m];
 #pragma unroll
+    int sl[D][P + 1];
+#pragma unroll
+    for (int d = 0; d < D; d++)
+#pragma unroll
+      for (int m = 0; m <= P; m++) sl[d][m] = swz<DIM, P, TC>(u - abc[d] * upt_stride<DIM, P>(d) + m * upt_stride<DIM, P>(d));
+#pragma unroll
     for (int k = 0; k < F; k++) {
       TC acc = TC(0);
 #pragma unroll
       for (int d = 0; d < D; d++) {
         const int st = upt_stride<DIM, P>(d), ub = u - abc[d] * st;
         TC v[P + 1];
-        if (d == 0) lds_line<P + 1, TC>(&FR_SFL(el, d, k, ub), v);
+        if (!SWZ && d == 0) lds_line<P + 1, TC>(&FR_SFL(el, d, k, ub), v);
         else {
 #pragma unroll
-          for (int m = 0; m <= P; m++) v[m] = FR_SFL(el, d, k, ub + m * st);
+          for (int m = 0; m <= P; m++) v[m] = FR_SFL(el, d, k, sl[d][m]);
         }
 #pragma unroll
         for (int m = 0; m <= P; m++) acc = acc + v[m] * Dm[d][m];
@@ -583,17 +664,21 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
     const int u0 = code_u0(cd), st = code_st(cd), ax = code_ax(cd);
     const bool plus = code_plus(cd);
     TC Lc[P + 1];
+    int sl[P + 1];
 #pragma unroll
-    for (int m = 0; m <= P; m++) Lc[m] = plus ? L.Lp[m] : L.Lm[m];
+    for (int m = 0; m <= P; m++) {
+      Lc[m] = plus ? L.Lp[m] : L.Lm[m];
+      sl[m] = swz<DIM, P, TC>(u0 + m * st);
+    }
 #pragma unroll
     for (int k = 0; k < F; k++) {
       uf[k] = FR_SUF(el, k, f);
 #pragma unroll
       for (int d = 0; d < D; d++) {
         const TC* s = &FR_SG(el, k + F * d, 0);
-        TC acc = s[u0] * Lc[0];
+        TC acc = s[sl[0]] * Lc[0];
 #pragma unroll
-        for (int m = 1; m <= P; m++) acc = fr_fma(s[u0 + m * st], Lc[m], acc);
+        for (int m = 1; m <= P; m++) acc = fr_fma(s[sl[m]], Lc[m], acc);
         gf[k][d] = acc;
       }
     }
@@ -604,9 +689,9 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
 #pragma unroll
         for (int d = 0; d < D; d++) {
           const TC* s = &FR_SS(el, (k - 1) + (F - 1) * d, 0);
-          TC acc = s[u0] * Lc[0];
+          TC acc = s[sl[0]] * Lc[0];
 #pragma unroll
-          for (int m = 1; m <= P; m++) acc = fr_fma(s[u0 + m * st], Lc[m], acc);
+          for (int m = 1; m <= P; m++) acc = fr_fma(s[sl[m]], Lc[m], acc);
           fv[k][d] = fv[k][d] + acc;
         }
     }
@@ -614,29 +699,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
     for (int d = 0; d < D; d++) n[d] = FR_SM(el, d * NF + f);
     const int btype = psd[it] >> 2;
     if (btype) {
-      // viscous normal flux of a boundary point, bdy_inters::evaluate_boundaryConditions_viscFlux
-      // (src/bdy_inters.cpp:905-1057): own flux (flux_spec 1) or the ghost
-      // side's with the adiabatic-wall energy gradient (flux_spec 2, types
-      // 12 and 14), plus tau n (u_l - u_r), on the normal
-      TC ug[F];
-      bc_ghost<D, TC>(ph, btype, uf, n, ug);
-      if (btype == 12 || btype == 14) {
-        TC gr[F][D];
-#pragma unroll
-        for (int k = 0; k < F; k++)
-#pragma unroll
-          for (int d = 0; d < D; d++) gr[k][d] = gf[k][d];
-        bc_vis_gradient<D, TC>(ph, uf, ug, gr);
-        vis_flux_fast<D, TC>(ph, ug, gr, fv);
-      }
-      const long long j = -1 - (long long)mate[own];
-#pragma unroll
-      for (int k = 0; k < F; k++) {
-        TC fnk = (fv[k][0] + ph.tau * n[0] * (uf[k] - ug[k])) * n[0];
-#pragma unroll
-        for (int d = 1; d < D; d++) fnk = fnk + (fv[k][d] + ph.tau * n[d] * (uf[k] - ug[k])) * n[d];
-        BV[j * F + k] = fnk;
-      }
+      vis_boundary<D, TC>(ph, btype, uf, gf, n, fv, &BV[(-1 - (long long)mate[own]) * F]);
     } else {
 #pragma unroll
       for (int k = 1; k < F; k++) VF[own + NFE * (k - 1)] = project<D, TC>(fv, k, n);
@@ -646,7 +709,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
       const TC* s = &FR_SFL(el, ax, k, 0);
       TC v = TC(0);
 #pragma unroll
-      for (int m = 0; m <= P; m++) v = v + s[u0 + m * st] * Lc[m];
+      for (int m = 0; m <= P; m++) v = v + s[sl[m]] * Lc[m];
       ND[own + NFE * k] = plus ? v : -v;
     }
   }
