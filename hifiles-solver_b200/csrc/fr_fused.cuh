@@ -287,47 +287,57 @@ __device__ __forceinline__ int swz(int u)
 }
 
 // Boundary points of the gradient kernel, out of line so that the hot loop
-// bodies stay compact (most meshes have few or no boundary points).
+// bodies stay compact (most meshes have few or no boundary points).  The
+// inputs travel by value, so no array of the calling thread has its address
+// taken.
+template <int D, typename TC>
+struct BdyPoint {
+  TC u[D + 2], n[D], g[D + 2][D], fv[D + 2][D];
+};
+
 // LDG common solution of a boundary point: ghost state from the boundary
 // condition, then ldg_solution with flux_spec 1 or 2, u_c = (u_r + u_l)/2
 // (bdy_inters::evaluate_boundaryConditions_invFlux, src/bdy_inters.cpp:245-389);
 // writes delta = u_c - u_own and u_own at stride st.
 template <int D, typename TC>
-__device__ __noinline__ void ldg_boundary(PhysT<TC> ph, int type, const TC* uo, const TC* nb, TC* dx, TC* uf, int st)
+__device__ __noinline__ void ldg_boundary(PhysT<TC> ph, int type, BdyPoint<D, TC> q, TC* dx, TC* uf, int st)
 {
   constexpr int F = D + 2;
   TC ug[F];
-  bc_ghost<D, TC>(ph, type, uo, nb, ug);
+  bc_ghost<D, TC>(ph, type, q.u, q.n, ug);
   for (int k = 0; k < F; k++) {
-    TC uc = TC(0.5) * (ug[k] + uo[k]);
-    dx[k * st] = uc - uo[k];
-    uf[k * st] = uo[k];
+    TC uc = TC(0.5) * (ug[k] + q.u[k]);
+    dx[k * st] = uc - q.u[k];
+    uf[k * st] = q.u[k];
   }
 }
 
 // Viscous normal flux of a boundary point, bdy_inters::evaluate_boundaryConditions_viscFlux
-// (src/bdy_inters.cpp:905-1057): own flux fv (flux_spec 1) or the ghost
+// (src/bdy_inters.cpp:905-1057): own flux q.fv (flux_spec 1) or the ghost
 // side's with the adiabatic-wall energy gradient (flux_spec 2, types 12 and
-// 14), plus tau n (u_l - u_r), on the normal.  gf is the own gradient.
+// 14), plus tau n (u_l - u_r), on the normal.  q.g is the own gradient.
 template <int D, typename TC>
-__device__ __noinline__ void vis_boundary(PhysT<TC> ph, int type, const TC* uf, TC (*gf)[D], const TC* n,
-                                          TC (*fv)[D], TC* bv)
+__device__ __noinline__ void vis_boundary(PhysT<TC> ph, int type, BdyPoint<D, TC> q, TC* bv)
 {
   constexpr int F = D + 2;
   TC ug[F];
-  bc_ghost<D, TC>(ph, type, uf, n, ug);
+  bc_ghost<D, TC>(ph, type, q.u, q.n, ug);
   if (type == 12 || type == 14) {
-    TC gr[F][D];
-    for (int k = 0; k < F; k++)
-      for (int d = 0; d < D; d++) gr[k][d] = gf[k][d];
-    bc_vis_gradient<D, TC>(ph, uf, ug, gr);
-    vis_flux_fast<D, TC>(ph, ug, gr, fv);
+    bc_vis_gradient<D, TC>(ph, q.u, ug, q.g);
+    vis_flux_fast<D, TC>(ph, ug, q.g, q.fv);
   }
   for (int k = 0; k < F; k++) {
-    TC fnk = (fv[k][0] + ph.tau * n[0] * (uf[k] - ug[k])) * n[0];
-    for (int d = 1; d < D; d++) fnk = fnk + (fv[k][d] + ph.tau * n[d] * (uf[k] - ug[k])) * n[d];
+    TC fnk = (q.fv[k][0] + ph.tau * q.n[0] * (q.u[k] - ug[k])) * q.n[0];
+    for (int d = 1; d < D; d++) fnk = fnk + (q.fv[k][d] + ph.tau * q.n[d] * (q.u[k] - ug[k])) * q.n[d];
     bv[k] = fnk;
   }
+}
+
+// side bytes of the block's flux points, after the operator copy
+template <int EPB, int NF>
+__host__ __device__ constexpr size_t grad_side_bytes()
+{
+  return (EPB * NF + 15) / 16 * 16;
 }
 
 // Shared-memory plan of fr_grad_kernel, per element, in units of TC:
@@ -359,7 +369,8 @@ struct GradPlan {
 template <int DIM, int P, int EPB, typename TC, int LES>
 __host__ __device__ constexpr size_t grad_smem_bytes()
 {
-  return blockops_bytes<TC, Shape<DIM, P>::NF>() + sizeof(TC) * EPB * GradPlan<DIM, P>::size(LES);
+  return blockops_bytes<TC, Shape<DIM, P>::NF>() + grad_side_bytes<EPB, Shape<DIM, P>::NF>() +
+         sizeof(TC) * EPB * GradPlan<DIM, P>::size(LES);
 }
 
 // Viscous stage, part 1 (per element):
@@ -404,7 +415,8 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
   constexpr int PE = G::size(LES);      // shared TC words per element
   extern __shared__ __align__(16) unsigned char fr_smem[];
   auto B = reinterpret_cast<BlockOps<TC, NF>*>(fr_smem);
-  TC* sm = reinterpret_cast<TC*>(fr_smem + blockops_bytes<TC, NF>());
+  unsigned char* sSide = fr_smem + blockops_bytes<TC, NF>();
+  TC* sm = reinterpret_cast<TC*>(fr_smem + blockops_bytes<TC, NF>() + grad_side_bytes<EPB, NF>());
 #define FR_SU(el, k, u) sm[(el) * PE + (k) * NU + (u)]
 #define FR_SX(el, k, f) sm[(el) * PE + G::oX + (k) * NF + (f)]
 #define FR_SUF(el, k, f) sm[(el) * PE + G::oUf + (k) * NF + (f)]
@@ -456,6 +468,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
       size_t own = f + (size_t)NF * (e0 + el);
       int mt = mate[own];
       psd[it] = side[own];
+      sSide[w] = psd[it];
       if (mt >= 0) {                 // boundary points (mate < 0) have no neighbour trace
 #pragma unroll
         for (int k = 0; k < F; k++) cp_async<sizeof(TC)>(&FR_SX(el, k, f), UF + mt + NFE * k);
@@ -487,13 +500,13 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
       return acc;
     };
     if (psd[it] >> 2) {
-      TC uo[F], nb[D];
+      BdyPoint<D, TC> q;
 #pragma unroll
-      for (int k = 0; k < F; k++) uo[k] = trace(k);
+      for (int k = 0; k < F; k++) q.u[k] = trace(k);
       const size_t own = f + (size_t)NF * (e0 + el);
 #pragma unroll
-      for (int d = 0; d < D; d++) nb[d] = nL[own + NFE * d];
-      ldg_boundary<D, TC>(ph, psd[it] >> 2, uo, nb, &FR_SX(el, 0, f), &FR_SUF(el, 0, f), NF);
+      for (int d = 0; d < D; d++) q.n[d] = nL[own + NFE * d];
+      ldg_boundary<D, TC>(ph, psd[it] >> 2, q, &FR_SX(el, 0, f), &FR_SUF(el, 0, f), NF);
       continue;
     }
     TC pen = (psd[it] & 2) ? -ph.pen_fact : ph.pen_fact;
@@ -652,65 +665,178 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
   cp_async_wait_all();
   __syncthreads();
 
-  // --- flux points: own viscous flux projected on the left normal, and the
-  //     discontinuous normal flux
+  if constexpr (SWZ) {
+    // --- flux points, one line of solution points per task: the corrected
+    // gradient (and SGS flux) and the transformed flux along the line are read
+    // once and extrapolated to the flux points at both ends; each end then gets
+    // its own viscous flux projected on the left normal (VF, or BV at a
+    // boundary point) and its discontinuous normal flux ND.
+    constexpr int NLN = NU / (P + 1);               // lines per axis
+    constexpr int IL = Items<NT, EPB * D * NLN>::N;
 #pragma unroll
-  for (int it = 0; it < IF; it++) {
-    int w = threadIdx.x + it * NT, el = w / NF, f = w - el * NF;
-    if (w >= EPB * NF || el >= nval) continue;
-    size_t own = f + (size_t)NF * (e0 + el);
-    TC uf[F], gf[F][D], fv[F][D], n[D];
-    const int cd = B->code[f];
-    const int u0 = code_u0(cd), st = code_st(cd), ax = code_ax(cd);
-    const bool plus = code_plus(cd);
-    TC Lc[P + 1];
-    int sl[P + 1];
-#pragma unroll
-    for (int m = 0; m <= P; m++) {
-      Lc[m] = plus ? L.Lp[m] : L.Lm[m];
-      sl[m] = swz<DIM, P, TC>(u0 + m * st);
-    }
-#pragma unroll
-    for (int k = 0; k < F; k++) {
-      uf[k] = FR_SUF(el, k, f);
-#pragma unroll
-      for (int d = 0; d < D; d++) {
-        const TC* s = &FR_SG(el, k + F * d, 0);
-        TC acc = s[sl[0]] * Lc[0];
-#pragma unroll
-        for (int m = 1; m <= P; m++) acc = fr_fma(s[sl[m]], Lc[m], acc);
-        gf[k][d] = acc;
+    for (int it = 0; it < IL; it++) {
+      const int w = threadIdx.x + it * NT, el = w / (D * NLN), r = w - el * (D * NLN), ax = r / NLN, j = r - ax * NLN;
+      if (w >= EPB * D * NLN || el >= nval) continue;
+      int a = 0, b = 0, c = 0;
+      if (DIM == 2) {
+        if (ax == 0) b = j; else a = j;
+      } else {
+        const int j0 = j % (P + 1), j1 = j / (P + 1);
+        if (ax == 0) { b = j0; c = j1; } else if (ax == 1) { a = j0; c = j1; } else { a = j0; b = j1; }
       }
-    }
-    vis_flux_fast<D, TC>(ph, uf, gf, fv);
-    if constexpr (LES != 0) {
+      const int st = upt_stride<DIM, P>(ax), ub = a + (P + 1) * (b + (P + 1) * c);
+      const int fcm = DIM == 2 ? (ax == 0 ? 3 : 0) : (ax == 0 ? 4 : (ax == 1 ? 1 : 0));
+      const int fcp = DIM == 2 ? (ax == 0 ? 1 : 2) : (ax == 0 ? 2 : (ax == 1 ? 3 : 5));
+      int al;
+      const int fe[2] = {face_fpt<DIM, P>(fcm, a, b, c, al), face_fpt<DIM, P>(fcp, a, b, c, al)};
+      int sl[P + 1];
 #pragma unroll
-      for (int k = 1; k < F; k++)
+      for (int m = 0; m <= P; m++) sl[m] = swz<DIM, P, TC>(ub + m * st);
+      // the own corrected gradient at both ends, opp_6 rows in column order with FMAs
+      TC ge[2][F][D];
+#pragma unroll
+      for (int k = 0; k < F; k++)
 #pragma unroll
         for (int d = 0; d < D; d++) {
-          const TC* s = &FR_SS(el, (k - 1) + (F - 1) * d, 0);
+          const TC* s = &FR_SG(el, k + F * d, 0);
+          TC v[P + 1];
+#pragma unroll
+          for (int m = 0; m <= P; m++) v[m] = s[sl[m]];
+          TC am = v[0] * L.Lm[0], ap = v[0] * L.Lp[0];
+#pragma unroll
+          for (int m = 1; m <= P; m++) {
+            am = fr_fma(v[m], L.Lm[m], am);
+            ap = fr_fma(v[m], L.Lp[m], ap);
+          }
+          ge[0][k][d] = am;
+          ge[1][k][d] = ap;
+        }
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const int f = fe[e];
+        const size_t own = f + (size_t)NF * (e0 + el);
+        TC uf[F], fv[F][D], n[D];
+#pragma unroll
+        for (int k = 0; k < F; k++) uf[k] = FR_SUF(el, k, f);
+        vis_flux_fast<D, TC>(ph, uf, ge[e], fv);
+        if constexpr (LES != 0) {
+#pragma unroll
+          for (int k = 1; k < F; k++)
+#pragma unroll
+            for (int d = 0; d < D; d++) {
+              const TC* s = &FR_SS(el, (k - 1) + (F - 1) * d, 0);
+              const TC* Lc = e ? L.Lp : L.Lm;
+              TC acc = s[sl[0]] * Lc[0];
+#pragma unroll
+              for (int m = 1; m <= P; m++) acc = fr_fma(s[sl[m]], Lc[m], acc);
+              fv[k][d] = fv[k][d] + acc;
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < D; d++) n[d] = FR_SM(el, d * NF + f);
+        const int btype = sSide[el * NF + f] >> 2;
+        if (btype) {
+          BdyPoint<D, TC> q;
+#pragma unroll
+          for (int k = 0; k < F; k++) {
+            q.u[k] = uf[k];
+#pragma unroll
+            for (int d = 0; d < D; d++) { q.g[k][d] = ge[e][k][d]; q.fv[k][d] = fv[k][d]; }
+          }
+#pragma unroll
+          for (int d = 0; d < D; d++) q.n[d] = n[d];
+          vis_boundary<D, TC>(ph, btype, q, &BV[(-1 - (long long)mate[own]) * F]);
+        } else {
+#pragma unroll
+          for (int k = 1; k < F; k++) VF[own + NFE * (k - 1)] = project<D, TC>(fv, k, n);
+        }
+      }
+      // the discontinuous normal flux at both ends, opp_1 rows in column order
+      const size_t om = fe[0] + (size_t)NF * (e0 + el), op = fe[1] + (size_t)NF * (e0 + el);
+#pragma unroll
+      for (int k = 0; k < F; k++) {
+        const TC* s = &FR_SFL(el, ax, k, 0);
+        TC vm = TC(0), vp = TC(0);
+#pragma unroll
+        for (int m = 0; m <= P; m++) {
+          const TC x = s[sl[m]];
+          vm = vm + x * L.Lm[m];
+          vp = vp + x * L.Lp[m];
+        }
+        ND[om + NFE * k] = -vm;
+        ND[op + NFE * k] = vp;
+      }
+    }
+  } else {
+    // --- flux points, one thread per flux point: own viscous flux projected on
+    //     the left normal, and the discontinuous normal flux
+#pragma unroll
+    for (int it = 0; it < IF; it++) {
+      int w = threadIdx.x + it * NT, el = w / NF, f = w - el * NF;
+      if (w >= EPB * NF || el >= nval) continue;
+      size_t own = f + (size_t)NF * (e0 + el);
+      TC uf[F], gf[F][D], fv[F][D], n[D];
+      const int cd = B->code[f];
+      const int u0 = code_u0(cd), st = code_st(cd), ax = code_ax(cd);
+      const bool plus = code_plus(cd);
+      TC Lc[P + 1];
+      int sl[P + 1];
+#pragma unroll
+      for (int m = 0; m <= P; m++) {
+        Lc[m] = plus ? L.Lp[m] : L.Lm[m];
+        sl[m] = swz<DIM, P, TC>(u0 + m * st);
+      }
+#pragma unroll
+      for (int k = 0; k < F; k++) {
+        uf[k] = FR_SUF(el, k, f);
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+          const TC* s = &FR_SG(el, k + F * d, 0);
           TC acc = s[sl[0]] * Lc[0];
 #pragma unroll
           for (int m = 1; m <= P; m++) acc = fr_fma(s[sl[m]], Lc[m], acc);
-          fv[k][d] = fv[k][d] + acc;
+          gf[k][d] = acc;
         }
-    }
+      }
+      vis_flux_fast<D, TC>(ph, uf, gf, fv);
+      if constexpr (LES != 0) {
 #pragma unroll
-    for (int d = 0; d < D; d++) n[d] = FR_SM(el, d * NF + f);
-    const int btype = psd[it] >> 2;
-    if (btype) {
-      vis_boundary<D, TC>(ph, btype, uf, gf, n, fv, &BV[(-1 - (long long)mate[own]) * F]);
-    } else {
+        for (int k = 1; k < F; k++)
 #pragma unroll
-      for (int k = 1; k < F; k++) VF[own + NFE * (k - 1)] = project<D, TC>(fv, k, n);
-    }
+          for (int d = 0; d < D; d++) {
+            const TC* s = &FR_SS(el, (k - 1) + (F - 1) * d, 0);
+            TC acc = s[sl[0]] * Lc[0];
 #pragma unroll
-    for (int k = 0; k < F; k++) {
-      const TC* s = &FR_SFL(el, ax, k, 0);
-      TC v = TC(0);
+            for (int m = 1; m <= P; m++) acc = fr_fma(s[sl[m]], Lc[m], acc);
+            fv[k][d] = fv[k][d] + acc;
+          }
+      }
 #pragma unroll
-      for (int m = 0; m <= P; m++) v = v + s[sl[m]] * Lc[m];
-      ND[own + NFE * k] = plus ? v : -v;
+      for (int d = 0; d < D; d++) n[d] = FR_SM(el, d * NF + f);
+      const int btype = psd[it] >> 2;
+      if (btype) {
+        BdyPoint<D, TC> q;
+#pragma unroll
+        for (int k = 0; k < F; k++) {
+          q.u[k] = uf[k];
+#pragma unroll
+          for (int d = 0; d < D; d++) { q.g[k][d] = gf[k][d]; q.fv[k][d] = fv[k][d]; }
+        }
+#pragma unroll
+        for (int d = 0; d < D; d++) q.n[d] = n[d];
+        vis_boundary<D, TC>(ph, btype, q, &BV[(-1 - (long long)mate[own]) * F]);
+      } else {
+#pragma unroll
+        for (int k = 1; k < F; k++) VF[own + NFE * (k - 1)] = project<D, TC>(fv, k, n);
+      }
+#pragma unroll
+      for (int k = 0; k < F; k++) {
+        const TC* s = &FR_SFL(el, ax, k, 0);
+        TC v = TC(0);
+#pragma unroll
+        for (int m = 0; m <= P; m++) v = v + s[sl[m]] * Lc[m];
+        ND[own + NFE * k] = plus ? v : -v;
+      }
     }
   }
 #undef FR_SU
