@@ -280,9 +280,14 @@ __device__ __forceinline__ void lds_line(const T* s, T (&v)[N])
 // conflicts.  Other shapes, and 4-byte values (32 per bank row), keep the
 // natural order.
 template <int DIM, int P, typename TC>
+__host__ __device__ constexpr bool swz_on()
+{
+  return DIM == 3 && P == 3 && sizeof(TC) == 8;
+}
+template <int DIM, int P, typename TC>
 __device__ __forceinline__ int swz(int u)
 {
-  if constexpr (DIM == 3 && P == 3 && sizeof(TC) == 8) return (u & 48) | ((((u >> 2) + (u >> 4)) & 3) << 2) | ((u + (u >> 4)) & 3);
+  if constexpr (swz_on<DIM, P, TC>()) return (u & 48) | ((((u >> 2) + (u >> 4)) & 3) << 2) | ((u + (u >> 4)) & 3);
   else return u;
 }
 
@@ -432,7 +437,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
   // --- inputs to shared memory: state, metrics, neighbour traces.  16-byte
   // copies where the per-element runs are whole 16-byte units (global bases
   // 16-byte aligned), element-sized otherwise.
-  constexpr bool SWZ = DIM == 3 && P == 3 && sizeof(TC) == 8;
+  constexpr bool SWZ = swz_on<DIM, P, TC>();
   constexpr int VU = (VEC && !SWZ && sizeof(TC) == 8 && NU % 2 == 0) ? 2 : 1;
   constexpr int VJ = (VEC && (DD * NU * sizeof(TC)) % 16 == 0) ? 16 / sizeof(TC) : 1;
   constexpr int VD = (VEC && (NU * sizeof(TC)) % 16 == 0) ? 16 / sizeof(TC) : 1;
@@ -1022,13 +1027,21 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
   constexpr int VF = (VEC && (NF * sizeof(TC)) % 16 == 0) ? 16 / sizeof(TC) : 1;     // flux-point runs
   constexpr int VN = (VEC && (NU * sizeof(TC)) % 16 == 0) ? 16 / sizeof(TC) : 1;     // point runs
   constexpr int VJ = (VEC && (DD * NU * sizeof(TC)) % 16 == 0) ? 16 / sizeof(TC) : 1;
+  // the state is kept in the bank-conflict-free point order of swz (read
+  // along lines for the next stage's traces), so its copies are element-sized
+  // where that order is not the natural one
+  constexpr bool SWU = swz_on<DIM, P, double>();
+  constexpr int V8U = SWU ? 1 : V8;
   const bool want_reg = MODE == 1 && !first_stage;
-  for (int w = threadIdx.x; w < nval * F * NU / V8; w += NT) {
-    int el = w / (F * NU / V8), r = w * V8 - el * F * NU, k = r / NU, u = r - k * NU;
-    size_t g = u + (size_t)NU * (e0 + el + E * k);
-    cp_async<8 * V8>(&sU[el][k][u], U + g);
-    if (want_reg) cp_async<8 * V8>(&sREG[el][k][u], REG + g);
+  for (int w = threadIdx.x; w < nval * F * NU / V8U; w += NT) {
+    int el = w / (F * NU / V8U), r = w * V8U - el * F * NU, k = r / NU, u = r - k * NU;
+    cp_async<8 * V8U>(&sU[el][k][swz<DIM, P, double>(u)], U + u + (size_t)NU * (e0 + el + E * k));
   }
+  if (want_reg)
+    for (int w = threadIdx.x; w < nval * F * NU / V8; w += NT) {
+      int el = w / (F * NU / V8), r = w * V8 - el * F * NU, k = r / NU, u = r - k * NU;
+      cp_async<8 * V8>(&sREG[el][k][u], REG + u + (size_t)NU * (e0 + el + E * k));
+    }
   if (MODE == 1)
     for (int w = threadIdx.x; w < nval * NU / V8; w += NT) {
       int el = (w * V8) / NU, u = w * V8 - el * NU;
@@ -1068,7 +1081,7 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
       for (int q = 0; q < DD; q++) g[q] = sJ[el][DD * u + q];
       TC q[F], fi[F][D];
 #pragma unroll
-      for (int k = 0; k < F; k++) q[k] = (TC)sU[el][k][u];
+      for (int k = 0; k < F; k++) q[k] = (TC)sU[el][k][swz<DIM, P, double>(u)];
       inv_flux<D, TC>(ph, q, fi);
 #pragma unroll
       for (int l = 0; l < D; l++)
@@ -1140,9 +1153,10 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
         double rhs = -R / dj;
         double res = first_stage ? dt * rhs : rk_a * sREG[el][k][u] + dt * rhs;
         REG[gi] = res;
-        double un = sU[el][k][u] + rk_b * res;
+        const int su = swz<DIM, P, double>(u);
+        double un = sU[el][k][su] + rk_b * res;
         U[gi] = un;
-        sU[el][k][u] = un;
+        sU[el][k][su] = un;
         red[k] += fabs(rhs);
       }
     }
@@ -1170,9 +1184,21 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
       int el = w / NF, f = w - el * NF;
       long long e = e0 + el;
       const int cd = B->code[f];
+      int sl[P + 1];
+      TC Lc[P + 1];
 #pragma unroll
-      for (int k = 0; k < F; k++)
-        UFn[f + (size_t)NF * (e + E * k)] = interp_code<P, TC, double>(L, cd, &sU[el][k][0]);
+      for (int m = 0; m <= P; m++) {
+        sl[m] = swz<DIM, P, double>(code_u0(cd) + m * code_st(cd));
+        Lc[m] = code_plus(cd) ? L.Lp[m] : L.Lm[m];
+      }
+      // the opp_0 row of f in column order, (((0 + t0) + t1) + ...)
+#pragma unroll
+      for (int k = 0; k < F; k++) {
+        TC acc = TC(0);
+#pragma unroll
+        for (int m = 0; m <= P; m++) acc = acc + (TC)sU[el][k][sl[m]] * Lc[m];
+        UFn[f + (size_t)NF * (e + E * k)] = acc;
+      }
     }
   }
 }
