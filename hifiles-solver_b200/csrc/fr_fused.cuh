@@ -320,11 +320,13 @@ __device__ __noinline__ void ldg_boundary(PhysT<TC> ph, int type, BdyPoint<D, TC
 // Viscous normal flux of a boundary point, bdy_inters::evaluate_boundaryConditions_viscFlux
 // (src/bdy_inters.cpp:905-1057): own flux q.fv (flux_spec 1) or the ghost
 // side's with the adiabatic-wall energy gradient (flux_spec 2, types 12 and
-// 14), plus tau n (u_l - u_r), on the normal.  q.g is the own gradient.
-template <int D, typename TC>
+// 14), plus tau n (u_l - u_r), on the normal.  q.g is the own gradient; with
+// HAVE_FV = false the own flux is evaluated here from q.u and q.g.
+template <int D, typename TC, bool HAVE_FV = true>
 __device__ __noinline__ void vis_boundary(PhysT<TC> ph, int type, BdyPoint<D, TC> q, TC* bv)
 {
   constexpr int F = D + 2;
+  if (!HAVE_FV) vis_flux_fast<D, TC>(ph, q.u, q.g, q.fv);
   TC ug[F];
   bc_ghost<D, TC>(ph, type, q.u, q.n, ug);
   if (type == 12 || type == 14) {
@@ -720,11 +722,34 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
       for (int e = 0; e < 2; e++) {
         const int f = fe[e];
         const size_t own = f + (size_t)NF * (e0 + el);
-        TC uf[F], fv[F][D], n[D];
+        TC uf[F], n[D];
 #pragma unroll
         for (int k = 0; k < F; k++) uf[k] = FR_SUF(el, k, f);
-        vis_flux_fast<D, TC>(ph, uf, ge[e], fv);
-        if constexpr (LES != 0) {
+#pragma unroll
+        for (int d = 0; d < D; d++) n[d] = FR_SM(el, d * NF + f);
+        const int btype = sSide[el * NF + f] >> 2;
+        if constexpr (LES == 0) {
+          // the projection is accumulated as the flux is formed (no full flux held)
+          if (btype) {
+            BdyPoint<D, TC> q;
+#pragma unroll
+            for (int k = 0; k < F; k++) {
+              q.u[k] = uf[k];
+#pragma unroll
+              for (int d = 0; d < D; d++) q.g[k][d] = ge[e][k][d];
+            }
+#pragma unroll
+            for (int d = 0; d < D; d++) q.n[d] = n[d];
+            vis_boundary<D, TC, false>(ph, btype, q, &BV[(-1 - (long long)mate[own]) * F]);
+          } else {
+            TC pr[F - 1];
+            vis_flux_proj<D, TC>(ph, uf, ge[e], n, pr);
+#pragma unroll
+            for (int k = 1; k < F; k++) VF[own + NFE * (k - 1)] = pr[k - 1];
+          }
+        } else {
+          TC fv[F][D];
+          vis_flux_fast<D, TC>(ph, uf, ge[e], fv);
 #pragma unroll
           for (int k = 1; k < F; k++)
 #pragma unroll
@@ -736,24 +761,21 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
               for (int m = 1; m <= P; m++) acc = fr_fma(s[sl[m]], Lc[m], acc);
               fv[k][d] = fv[k][d] + acc;
             }
-        }
+          if (btype) {
+            BdyPoint<D, TC> q;
 #pragma unroll
-        for (int d = 0; d < D; d++) n[d] = FR_SM(el, d * NF + f);
-        const int btype = sSide[el * NF + f] >> 2;
-        if (btype) {
-          BdyPoint<D, TC> q;
+            for (int k = 0; k < F; k++) {
+              q.u[k] = uf[k];
 #pragma unroll
-          for (int k = 0; k < F; k++) {
-            q.u[k] = uf[k];
+              for (int d = 0; d < D; d++) { q.g[k][d] = ge[e][k][d]; q.fv[k][d] = fv[k][d]; }
+            }
 #pragma unroll
-            for (int d = 0; d < D; d++) { q.g[k][d] = ge[e][k][d]; q.fv[k][d] = fv[k][d]; }
+            for (int d = 0; d < D; d++) q.n[d] = n[d];
+            vis_boundary<D, TC>(ph, btype, q, &BV[(-1 - (long long)mate[own]) * F]);
+          } else {
+#pragma unroll
+            for (int k = 1; k < F; k++) VF[own + NFE * (k - 1)] = project<D, TC>(fv, k, n);
           }
-#pragma unroll
-          for (int d = 0; d < D; d++) q.n[d] = n[d];
-          vis_boundary<D, TC>(ph, btype, q, &BV[(-1 - (long long)mate[own]) * F]);
-        } else {
-#pragma unroll
-          for (int k = 1; k < F; k++) VF[own + NFE * (k - 1)] = project<D, TC>(fv, k, n);
         }
       }
       // the discontinuous normal flux at both ends, opp_1 rows in column order
@@ -780,7 +802,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
       int w = threadIdx.x + it * NT, el = w / NF, f = w - el * NF;
       if (w >= EPB * NF || el >= nval) continue;
       size_t own = f + (size_t)NF * (e0 + el);
-      TC uf[F], gf[F][D], fv[F][D], n[D];
+      TC uf[F], gf[F][D], n[D];
       const int cd = B->code[f];
       const int u0 = code_u0(cd), st = code_st(cd), ax = code_ax(cd);
       const bool plus = code_plus(cd);
@@ -803,8 +825,31 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
           gf[k][d] = acc;
         }
       }
-      vis_flux_fast<D, TC>(ph, uf, gf, fv);
-      if constexpr (LES != 0) {
+#pragma unroll
+      for (int d = 0; d < D; d++) n[d] = FR_SM(el, d * NF + f);
+      const int btype = psd[it] >> 2;
+      if constexpr (LES == 0) {
+        // the projection is accumulated as the flux is formed (no full flux held)
+        if (btype) {
+          BdyPoint<D, TC> q;
+#pragma unroll
+          for (int k = 0; k < F; k++) {
+            q.u[k] = uf[k];
+#pragma unroll
+            for (int d = 0; d < D; d++) q.g[k][d] = gf[k][d];
+          }
+#pragma unroll
+          for (int d = 0; d < D; d++) q.n[d] = n[d];
+          vis_boundary<D, TC, false>(ph, btype, q, &BV[(-1 - (long long)mate[own]) * F]);
+        } else {
+          TC pr[F - 1];
+          vis_flux_proj<D, TC>(ph, uf, gf, n, pr);
+#pragma unroll
+          for (int k = 1; k < F; k++) VF[own + NFE * (k - 1)] = pr[k - 1];
+        }
+      } else {
+        TC fv[F][D];
+        vis_flux_fast<D, TC>(ph, uf, gf, fv);
 #pragma unroll
         for (int k = 1; k < F; k++)
 #pragma unroll
@@ -815,24 +860,21 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
             for (int m = 1; m <= P; m++) acc = fr_fma(s[sl[m]], Lc[m], acc);
             fv[k][d] = fv[k][d] + acc;
           }
-      }
+        if (btype) {
+          BdyPoint<D, TC> q;
 #pragma unroll
-      for (int d = 0; d < D; d++) n[d] = FR_SM(el, d * NF + f);
-      const int btype = psd[it] >> 2;
-      if (btype) {
-        BdyPoint<D, TC> q;
+          for (int k = 0; k < F; k++) {
+            q.u[k] = uf[k];
 #pragma unroll
-        for (int k = 0; k < F; k++) {
-          q.u[k] = uf[k];
+            for (int d = 0; d < D; d++) { q.g[k][d] = gf[k][d]; q.fv[k][d] = fv[k][d]; }
+          }
 #pragma unroll
-          for (int d = 0; d < D; d++) { q.g[k][d] = gf[k][d]; q.fv[k][d] = fv[k][d]; }
+          for (int d = 0; d < D; d++) q.n[d] = n[d];
+          vis_boundary<D, TC>(ph, btype, q, &BV[(-1 - (long long)mate[own]) * F]);
+        } else {
+#pragma unroll
+          for (int k = 1; k < F; k++) VF[own + NFE * (k - 1)] = project<D, TC>(fv, k, n);
         }
-#pragma unroll
-        for (int d = 0; d < D; d++) q.n[d] = n[d];
-        vis_boundary<D, TC>(ph, btype, q, &BV[(-1 - (long long)mate[own]) * F]);
-      } else {
-#pragma unroll
-        for (int k = 1; k < F; k++) VF[own + NFE * (k - 1)] = project<D, TC>(fv, k, n);
       }
 #pragma unroll
       for (int k = 0; k < F; k++) {
@@ -851,6 +893,54 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
 #undef FR_SG
 #undef FR_SFL
 #undef FR_SS
+}
+
+// Boundary point j of the interface kernel (flat own index bf[j], type
+// bt[j]), out of line so that the interior path keeps few registers.
+template <int DIM, int VISC, typename TC, int RIEMANN>
+__device__ __noinline__ void face_boundary(PhysT<TC> ph, long long j, const TC* __restrict__ UF,
+                                           const TC* __restrict__ nL, const TC* __restrict__ tdA, TC* __restrict__ CF,
+                                           long long NFE, const int* __restrict__ bf,
+                                           const unsigned char* __restrict__ bt, const TC* __restrict__ BV)
+{
+  constexpr int F = DIM + 2, D = DIM;
+  const long long a = bf[j];
+  const int type = bt[j];
+  TC ul[F], ug[F], n[D], fn[F];
+#pragma unroll
+  for (int k = 0; k < F; k++) ul[k] = UF[a + NFE * k];
+#pragma unroll
+  for (int d = 0; d < D; d++) n[d] = nL[a + NFE * d];
+  bc_ghost<D, TC>(ph, type, ul, n, ug);
+  TC fl[F][D], fr[F][D];
+  inv_flux<D, TC>(ph, ul, fl);
+  inv_flux<D, TC>(ph, ug, fr);
+  if (type == 16) {
+#pragma unroll
+    for (int k = 0; k < F; k++) {
+      TC s = fl[k][0] * n[0];
+#pragma unroll
+      for (int l = 1; l < D; l++) s = s + fl[k][l] * n[l];
+      fn[k] = s;
+    }
+  } else if (RIEMANN == 2 && DIM == 2) {
+    roe<TC>(ph, ul, ug, n, fn);
+  } else {
+#pragma unroll
+    for (int k = 0; k < F; k++) {
+      TC s = fl[k][0] * n[0], q = fr[k][0] * n[0];
+#pragma unroll
+      for (int l = 1; l < D; l++) { s = s + fl[k][l] * n[l]; q = q + fr[k][l] * n[l]; }
+      fn[k] = TC(0.5) * (s + q);
+    }
+  }
+  const TC tl = tdA[a];
+#pragma unroll
+  for (int k = 0; k < F; k++) {
+    TC c = fn[k] * tl;
+    if (VISC) c = c + BV[j * F + k] * tl;
+    CF[a + NFE * k] = c;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -878,45 +968,7 @@ fr_face_kernel(const int2* __restrict__ face, const unsigned char* __restrict__ 
   constexpr int F = DIM + 2, D = DIM;
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nint) {
-    const long long j = i - nint;
-    if (j >= nbdy) return;
-    const long long a = bf[j];
-    const int type = bt[j];
-    TC ul[F], ug[F], n[D], fn[F];
-#pragma unroll
-    for (int k = 0; k < F; k++) ul[k] = UF[a + NFE * k];
-#pragma unroll
-    for (int d = 0; d < D; d++) n[d] = nL[a + NFE * d];
-    bc_ghost<D, TC>(ph, type, ul, n, ug);
-    TC fl[F][D], fr[F][D];
-    inv_flux<D, TC>(ph, ul, fl);
-    inv_flux<D, TC>(ph, ug, fr);
-    if (type == 16) {
-#pragma unroll
-      for (int k = 0; k < F; k++) {
-        TC s = fl[k][0] * n[0];
-#pragma unroll
-        for (int l = 1; l < D; l++) s = s + fl[k][l] * n[l];
-        fn[k] = s;
-      }
-    } else if (RIEMANN == 2 && DIM == 2) {
-      roe<TC>(ph, ul, ug, n, fn);
-    } else {
-#pragma unroll
-      for (int k = 0; k < F; k++) {
-        TC s = fl[k][0] * n[0], q = fr[k][0] * n[0];
-#pragma unroll
-        for (int l = 1; l < D; l++) { s = s + fl[k][l] * n[l]; q = q + fr[k][l] * n[l]; }
-        fn[k] = TC(0.5) * (s + q);
-      }
-    }
-    const TC tl = tdA[a];
-#pragma unroll
-    for (int k = 0; k < F; k++) {
-      TC c = fn[k] * tl;
-      if (VISC) c = c + BV[j * F + k] * tl;
-      CF[a + NFE * k] = c;
-    }
+    if (i - nint < nbdy) face_boundary<DIM, VISC, TC, RIEMANN>(ph, i - nint, UF, nL, tdA, CF, NFE, bf, bt, BV);
     return;
   }
   const int2 lr = face[i];

@@ -146,12 +146,14 @@ __device__ __forceinline__ void vis_flux(const PhysT<T>& ph, const T* u, T (*g)[
 __device__ __forceinline__ double fr_fma(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ float fr_fma(float a, float b, float c) { return fmaf(a, b, c); }
 
+// Shared part of the viscous flux: velocity v, stress tau and the heat-flux
+// term q[l] = (mu gamma / Pr) de/dx_l of calc_visf_3d (src/flux.cpp:263-431).
 template <int D, typename T>
-__device__ __forceinline__ void vis_flux_fast(const PhysT<T>& ph, const T* u, T (*g)[D], T (*f)[D])
+__device__ __forceinline__ void vis_core(const PhysT<T>& ph, const T* u, T (*g)[D], T (&v)[D], T (&tau)[D][D],
+                                         T (&q)[D])
 {
   constexpr int F = D + 2;
   const T rho = u[0], ri = T(1) / rho;
-  T v[D];
 #pragma unroll
   for (int l = 0; l < D; l++) v[l] = u[l + 1] * ri;
   T ke = v[0] * v[0];
@@ -185,22 +187,52 @@ __device__ __forceinline__ void vis_flux_fast(const PhysT<T>& ph, const T* u, T 
   for (int l = 1; l < D; l++) dsum = dsum + dv[l][l];
   const T diag = dsum * T(1.0 / 3.0);
   const T kg = mu / ph.prandtl * ph.gamma, mu2 = T(2) * mu;
-  T tau[D][D];
 #pragma unroll
   for (int m = 0; m < D; m++)
 #pragma unroll
     for (int l = 0; l < D; l++)
       tau[m][l] = (m == l) ? mu2 * (dv[m][m] - diag) : mu * (dv[m][l] + dv[l][m]);
 #pragma unroll
+  for (int l = 0; l < D; l++) q[l] = kg * de[l];
+}
+
+template <int D, typename T>
+__device__ __forceinline__ void vis_flux_fast(const PhysT<T>& ph, const T* u, T (*g)[D], T (*f)[D])
+{
+  constexpr int F = D + 2;
+  T v[D], tau[D][D], q[D];
+  vis_core<D, T>(ph, u, g, v, tau, q);
+#pragma unroll
   for (int l = 0; l < D; l++) {
     f[0][l] = T(0);
-    T w = kg * de[l];
+    T w = q[l];
 #pragma unroll
     for (int m = 0; m < D; m++) {
       f[m + 1][l] = -tau[m][l];
       w = fr_fma(v[m], tau[m][l], w);
     }
     f[F - 1][l] = -w;
+  }
+}
+
+// The viscous flux projected on n, pr[k - 1] = project(f, k, n) for the
+// components k = 1 .. F-1, without holding all of f.
+template <int D, typename T>
+__device__ __forceinline__ void vis_flux_proj(const PhysT<T>& ph, const T* u, T (*g)[D], const T* n, T* pr)
+{
+  T v[D], tau[D][D], q[D];
+  vis_core<D, T>(ph, u, g, v, tau, q);
+#pragma unroll
+  for (int l = 0; l < D; l++) {
+    T w = q[l];
+#pragma unroll
+    for (int m = 0; m < D; m++) {
+      const T fm = -tau[m][l];
+      pr[m] = l == 0 ? fm * n[0] : fr_fma(fm, n[l], pr[m]);
+      w = fr_fma(v[m], tau[m][l], w);
+    }
+    const T fe = -w;
+    pr[D] = l == 0 ? fe * n[0] : fr_fma(fe, n[l], pr[D]);
   }
 }
 
