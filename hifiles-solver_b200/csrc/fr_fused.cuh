@@ -408,7 +408,7 @@ __host__ __device__ constexpr size_t grad_smem_bytes()
 // bits 2.. hold the boundary type, mate = -1 - position in the boundary
 // list), and, when GRAD is not null, the corrected physical gradient
 // grad_disu_upts (n_upts, n_eles, F, D).
-template <int DIM, int P, int EPB, int NT, typename TC, int LES = 0, int MINB = 1, int VEC = 1>
+template <int DIM, int P, int EPB, int NT, typename TC, int LES = 0, int MINB = 1, int VEC = 1, int PERS = 0>
 __global__ void __launch_bounds__(NT, MINB)
 fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const int* __restrict__ mate,
                const unsigned char* __restrict__ side, const TC* __restrict__ JG, const TC* __restrict__ detj,
@@ -432,59 +432,95 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
 #define FR_SFL(el, l, k, u) sm[(el) * PE + G::oFl + ((l) * F + (k)) * NU + (u)]
 #define FR_SS(el, c, u) sm[(el) * PE + G::oS + (c) * NU + (u)]
   fill_blockops<DIM, P, TC, NF>(B, L, threadIdx.x, NT);
-  const long long e0 = (long long)blockIdx.x * EPB;
   const long long NFE = (long long)NF * E;
-  const int nval = (int)(E - e0 < EPB ? E - e0 : EPB);
+  const long long nblk = (E + EPB - 1) / EPB;
 
   // --- inputs to shared memory: state, metrics, neighbour traces.  16-byte
   // copies where the per-element runs are whole 16-byte units (global bases
-  // 16-byte aligned), element-sized otherwise.
+  // 16-byte aligned), element-sized otherwise.  With PERS = 1 a block walks
+  // over element blocks blockIdx.x, + gridDim.x, ...; the next block's state,
+  // metrics and neighbour traces are fetched into their regions as soon as
+  // the current block no longer reads them (after the solution-point phase),
+  // so the copies overlap the divergence and flux-point phases, and the left
+  // normals are read from global memory at the flux points.
   constexpr bool SWZ = swz_on<DIM, P, TC>();
   constexpr int VU = (VEC && !SWZ && sizeof(TC) == 8 && NU % 2 == 0) ? 2 : 1;
   constexpr int VJ = (VEC && (DD * NU * sizeof(TC)) % 16 == 0) ? 16 / sizeof(TC) : 1;
   constexpr int VD = (VEC && (NU * sizeof(TC)) % 16 == 0) ? 16 / sizeof(TC) : 1;
-  for (int w = threadIdx.x; w < EPB * F * NU / VU; w += NT) {
-    int el = w / (F * NU / VU), r = w * VU - el * F * NU, k = r / NU, u = r - k * NU;
-    if (el < nval) {
-      const double* src = U + u + (size_t)NU * (e0 + el + E * k);
-      const int su = swz<DIM, P, TC>(u);
-      if constexpr (sizeof(TC) == 8) cp_async<8 * VU>(&FR_SU(el, k, su), src);
-      else FR_SU(el, k, su) = (TC)*src;
-    } else {
+  // state (FP64 form: asynchronous; FP32 form: loaded and rounded here)
+  auto stage_state = [&](long long eb, int nv) {
+    for (int w = threadIdx.x; w < EPB * F * NU / VU; w += NT) {
+      int el = w / (F * NU / VU), r = w * VU - el * F * NU, k = r / NU, u = r - k * NU;
+      if (el < nv) {
+        const double* src = U + u + (size_t)NU * (eb + el + E * k);
+        const int su = swz<DIM, P, TC>(u);
+        if constexpr (sizeof(TC) == 8) cp_async<8 * VU>(&FR_SU(el, k, su), src);
+        else FR_SU(el, k, su) = (TC)*src;
+      } else {
 #pragma unroll
-      for (int v = 0; v < VU; v++) {
-        const int su = swz<DIM, P, TC>(u + v);
-        FR_SU(el, k, su) = TC(1);
+        for (int v = 0; v < VU; v++) {
+          const int su = swz<DIM, P, TC>(u + v);
+          FR_SU(el, k, su) = TC(1);
+        }
       }
     }
-  }
-  for (int w = threadIdx.x; w < nval * DD * NU / VJ; w += NT) {
-    int el = (w * VJ) / (DD * NU), r = w * VJ - el * DD * NU;
-    cp_async<sizeof(TC) * VJ>(&FR_SM(el, r), JG + (size_t)DD * NU * e0 + (size_t)w * VJ);
-  }
-  for (int w = threadIdx.x; w < nval * NU / VD; w += NT) {
-    int el = (w * VD) / NU, u = w * VD - el * NU;
-    cp_async<sizeof(TC) * VD>(&FR_SM(el, DD * NU + u), detj + (size_t)NU * e0 + (size_t)w * VD);
-  }
+  };
+  auto stage_metrics = [&](long long eb, int nv) {
+    for (int w = threadIdx.x; w < nv * DD * NU / VJ; w += NT) {
+      int el = (w * VJ) / (DD * NU), r = w * VJ - el * DD * NU;
+      cp_async<sizeof(TC) * VJ>(&FR_SM(el, r), JG + (size_t)DD * NU * eb + (size_t)w * VJ);
+    }
+    for (int w = threadIdx.x; w < nv * NU / VD; w += NT) {
+      int el = (w * VD) / NU, u = w * VD - el * NU;
+      cp_async<sizeof(TC) * VD>(&FR_SM(el, DD * NU + u), detj + (size_t)NU * eb + (size_t)w * VD);
+    }
+  };
+  // wiring of the thread's flux points: mate index and side byte
+  auto load_wiring = [&](long long eb, int nv, int (&mt)[IF], unsigned char (&sd)[IF]) {
+#pragma unroll
+    for (int it = 0; it < IF; it++) {
+      int w = threadIdx.x + it * NT, el = w / NF, f = w - el * NF;
+      mt[it] = -1;
+      sd[it] = 0;
+      if (w < EPB * NF && el < nv) {
+        size_t own = f + (size_t)NF * (eb + el);
+        mt[it] = mate[own];
+        sd[it] = side[own];
+      }
+    }
+  };
+  // neighbour traces (boundary points, mate < 0, have none)
+  auto stage_traces = [&](const int (&mt)[IF]) {
+#pragma unroll
+    for (int it = 0; it < IF; it++) {
+      int w = threadIdx.x + it * NT, el = w / NF, f = w - el * NF;
+      if (mt[it] >= 0) {
+#pragma unroll
+        for (int k = 0; k < F; k++) cp_async<sizeof(TC)>(&FR_SX(el, k, f), UF + mt[it] + NFE * k);
+      }
+    }
+  };
+
+  long long blk = blockIdx.x;
+  int nval = (int)(E - blk * EPB < EPB ? E - blk * EPB : EPB);
   unsigned char psd[IF];
-#pragma unroll
-  for (int it = 0; it < IF; it++) {
-    int w = threadIdx.x + it * NT, el = w / NF, f = w - el * NF;
-    psd[it] = 0;
-    if (w < EPB * NF && el < nval) {
-      size_t own = f + (size_t)NF * (e0 + el);
-      int mt = mate[own];
-      psd[it] = side[own];
-      sSide[w] = psd[it];
-      if (mt >= 0) {                 // boundary points (mate < 0) have no neighbour trace
-#pragma unroll
-        for (int k = 0; k < F; k++) cp_async<sizeof(TC)>(&FR_SX(el, k, f), UF + mt + NFE * k);
-      }
-    }
+  {
+    int mt[IF];
+    stage_state(blk * EPB, nval);
+    stage_metrics(blk * EPB, nval);
+    load_wiring(blk * EPB, nval, mt, psd);
+    stage_traces(mt);
+    cp_async_commit();
   }
-  cp_async_commit();
+  for (;;) {
+  const long long e0 = blk * EPB;
   cp_async_wait_all();
   __syncthreads();
+#pragma unroll
+  for (int it = 0; it < IF; it++) {
+    const int w = threadIdx.x + it * NT;
+    if (w < EPB * NF) sSide[w] = psd[it];
+  }
 
   // --- LDG common solution u_c = (uL+uR)/2 - beta (uL-uR); delta = u_c - u_own (in place)
 #pragma unroll
@@ -626,11 +662,23 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
   }
   __syncthreads();
 
-  // --- left normals into the metric region, fetched while the divergence runs
-  for (int w = threadIdx.x; w < nval * D * NF; w += NT) {
-    int el = w / (D * NF), r = w - el * D * NF, d = r / NF, f = r - d * NF;
-    cp_async<sizeof(TC)>(&FR_SM(el, r), nL + f + (size_t)NF * (e0 + el) + NFE * d);
+  // --- the next block's state, metrics and wiring (PERS), or the left
+  // normals into the metric region, fetched while the divergence runs
+  const long long nb = blk + gridDim.x;
+  const bool more = PERS && nb < nblk;
+  const int nvn = more ? (int)(E - nb * EPB < EPB ? E - nb * EPB : EPB) : 0;
+  int mtn[IF];
+  unsigned char psn[IF];
+  if (more) {
+    if constexpr (sizeof(TC) == 8) stage_state(nb * EPB, nvn);
+    stage_metrics(nb * EPB, nvn);
+    load_wiring(nb * EPB, nvn, mtn, psn);
   }
+  if (!PERS)
+    for (int w = threadIdx.x; w < nval * D * NF; w += NT) {
+      int el = w / (D * NF), r = w - el * D * NF, d = r / NF, f = r - d * NF;
+      cp_async<sizeof(TC)>(&FR_SM(el, r), nL + f + (size_t)NF * (e0 + el) + NFE * d);
+    }
   cp_async_commit();
 
   // --- divergence of the total discontinuous flux
@@ -645,7 +693,6 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
     for (int d = 0; d < D; d++)
 #pragma unroll
       for (int m = 0; m <= P; m++) Dm[d][m] = B->D[abc[d]][m];
-#pragma unroll
     int sl[D][P + 1];
 #pragma unroll
     for (int d = 0; d < D; d++)
@@ -669,7 +716,11 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
       DV[u + (size_t)NU * (e0 + el + E * k)] = acc;
     }
   }
-  cp_async_wait_all();
+  if (more) {
+    stage_traces(mtn);
+    cp_async_commit();
+  }
+  if (!PERS) cp_async_wait_all();
   __syncthreads();
 
   if constexpr (SWZ) {
@@ -726,7 +777,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
 #pragma unroll
         for (int k = 0; k < F; k++) uf[k] = FR_SUF(el, k, f);
 #pragma unroll
-        for (int d = 0; d < D; d++) n[d] = FR_SM(el, d * NF + f);
+        for (int d = 0; d < D; d++) n[d] = PERS ? nL[own + NFE * d] : FR_SM(el, d * NF + f);
         const int btype = sSide[el * NF + f] >> 2;
         if constexpr (LES == 0) {
           // the projection is accumulated as the flux is formed (no full flux held)
@@ -826,7 +877,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
         }
       }
 #pragma unroll
-      for (int d = 0; d < D; d++) n[d] = FR_SM(el, d * NF + f);
+      for (int d = 0; d < D; d++) n[d] = PERS ? nL[own + NFE * d] : FR_SM(el, d * NF + f);
       const int btype = psd[it] >> 2;
       if constexpr (LES == 0) {
         // the projection is accumulated as the flux is formed (no full flux held)
@@ -885,6 +936,13 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
         ND[own + NFE * k] = plus ? v : -v;
       }
     }
+  }
+  if (!more) break;
+  blk = nb;
+  nval = nvn;
+#pragma unroll
+  for (int it = 0; it < IF; it++) psd[it] = psn[it];
+  if constexpr (sizeof(TC) != 8) stage_state(blk * EPB, nval);   // the state region is free after the solution-point phase
   }
 #undef FR_SU
 #undef FR_SX

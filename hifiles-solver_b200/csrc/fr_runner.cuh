@@ -36,6 +36,7 @@ struct Bufs {
 
 struct Tile {
   int epb, nt, minb;   // elements per CTA, threads per CTA, CTAs per SM the registers are sized for (0: any)
+  int pers = 0;        // gradient kernel only: 1 = persistent blocks that prefetch their next element block
 };
 
 struct Runner {
@@ -73,7 +74,8 @@ FR_TILES(2, 4, T_({8, 256}), T_({8, 256}))
 FR_TILES(2, 5, T_({4, 160}), T_({4, 160}))
 FR_TILES(3, 1, T_({12, 128}), T_({12, 128}))
 FR_TILES(3, 2, T_({4, 128}, {2, 64}, {8, 256}), T_({4, 128}, {2, 64}, {8, 256}))
-FR_TILES(3, 3, T_({2, 128, 4}, {1, 64, 8}, {2, 192, 2}, {2, 128, 3}, {1, 96, 0}, {4, 256, 2}, {1, 96, 5}, {1, 96, 6}), T_({2, 128}, {1, 64}, {4, 256}, {2, 96}, {4, 128}))
+FR_TILES(3, 3, T_({2, 128, 4}, {1, 64, 8}, {2, 192, 2}, {2, 128, 3}, {1, 96, 0}, {4, 256, 2}, {1, 96, 5}, {1, 96, 6},
+                  {1, 64, 8, 1}, {2, 128, 3, 1}), T_({2, 128}, {1, 64}, {4, 256}, {2, 96}, {4, 128}))
 FR_TILES(3, 4, T_({1, 128}, {1, 160}, {2, 256}), T_({1, 128}, {2, 256}, {1, 160}))
 #undef T_
 #undef FR_TILES
@@ -148,10 +150,24 @@ struct RunnerT : Runner {
       if (I != gsel) return grad_i<I + 1, LES>(b, cur, s);
       constexpr int EPB = Tiles<DIM, P>::grad[I].epb, NT = Tiles<DIM, P>::grad[I].nt;
       constexpr int MINB = Tiles<DIM, P>::grad[I].minb > 0 ? Tiles<DIM, P>::grad[I].minb : 1;
+      constexpr int PERS = Tiles<DIM, P>::grad[I].pers;
       constexpr size_t sm = grad_smem_bytes<DIM, P, EPB, TC, LES>();
-      static bool once = (set_smem((const void*)fr_grad_kernel<DIM, P, EPB, NT, TC, LES, MINB>, sm), true);
+      const void* kfn = (const void*)fr_grad_kernel<DIM, P, EPB, NT, TC, LES, MINB, 1, PERS>;
+      static bool once = (set_smem(kfn, sm), true);
       (void)once;
-      fr_grad_kernel<DIM, P, EPB, NT, TC, LES, MINB><<<(unsigned)((E + EPB - 1) / EPB), NT, sm, s>>>(
+      long long grid = (E + EPB - 1) / EPB;
+      if (PERS) {
+        // persistent blocks: as many as are resident at once
+        static int resident = [&] {
+          int dev = 0, sms = 0, per = 0;
+          cudaGetDevice(&dev);
+          cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kfn, NT, sm);
+          return (per > 0 ? per : 1) * (sms > 0 ? sms : 1);
+        }();
+        grid = grid < resident ? grid : resident;
+      }
+      fr_grad_kernel<DIM, P, EPB, NT, TC, LES, MINB, 1, PERS><<<(unsigned)grid, NT, sm, s>>>(
           b.U, (const TC*)b.UF[cur], b.mate, b.side, (const TC*)b.JG, (const TC*)b.detj, (const TC*)b.nL,
           (TC*)b.VF, (TC*)b.ND, (TC*)b.DV, E, L, ph, (TC*)b.GRAD, (TC*)b.BV);
     }

@@ -572,6 +572,36 @@ fr_status fr_solver_autotune(fr_solver* s, int reps, int out4[4])
   return FR_OK;
 }
 
+fr_status fr_solver_tile_count(const fr_solver* s, int out2[2])
+{
+  if (!s || !out2) return fail(FR_ERR_ARG, "bad argument");
+  out2[0] = s->run->n_grad_tiles();
+  out2[1] = s->run->n_update_tiles();
+  return FR_OK;
+}
+
+fr_status fr_solver_tile_info(const fr_solver* s, int kind, int i, int out4[4])
+{
+  if (!s || !out4 || (kind != 0 && kind != 1)) return fail(FR_ERR_ARG, "bad argument");
+  const int n = kind == 0 ? s->run->n_grad_tiles() : s->run->n_update_tiles();
+  if (i < 0 || i >= n) return fail(FR_ERR_ARG, "tile index out of range");
+  const Tile t = kind == 0 ? s->run->grad_tile(i) : s->run->update_tile(i);
+  out4[0] = t.epb; out4[1] = t.nt; out4[2] = t.minb; out4[3] = t.pers;
+  return FR_OK;
+}
+
+fr_status fr_solver_select_tiles(fr_solver* s, int g, int u)
+{
+  if (!s) return fail(FR_ERR_ARG, "bad argument");
+  if (g < 0 || g >= s->run->n_grad_tiles() || u < 0 || u >= s->run->n_update_tiles())
+    return fail(FR_ERR_ARG, "tile index out of range");
+  FR_CUDA(cudaSetDevice(s->device));
+  FR_CUDA(cudaStreamSynchronize(s->own_stream));
+  s->run->select(g, u);
+  drop_graphs(s);
+  return FR_OK;
+}
+
 fr_status fr_mesh_geometry(const fr_mesh_desc* md, const fr_scheme_desc* sd, int out6[6], double* pos_upts,
                            double* detjac, double* JG, double* tdA, double* nrm, int* left_idx, int* right_idx)
 {

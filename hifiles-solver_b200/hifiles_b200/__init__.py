@@ -99,6 +99,9 @@ def lib():
         "fr_solver_sync": (C.c_int, [vp]),
         "fr_solver_profile_stage": (C.c_int, [vp, C.c_int, C.c_double, dp]),
         "fr_solver_autotune": (C.c_int, [vp, C.c_int, ip]),
+        "fr_solver_tile_count": (C.c_int, [vp, ip]),
+        "fr_solver_tile_info": (C.c_int, [vp, C.c_int, C.c_int, ip]),
+        "fr_solver_select_tiles": (C.c_int, [vp, C.c_int, C.c_int]),
         "fr_mesh_geometry": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(SchemeDesc), ip, dp, dp, dp, dp, dp, ip, ip]),
         "fr_line_operators": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, dp]),
         "fr_solver_gradient": (C.c_int, [vp, dp, vp]),
@@ -403,6 +406,22 @@ class Solver:
         out = (C.c_int * 4)()
         _check(lib().fr_solver_autotune(self.h, int(reps), out))
         return tuple(out)
+
+    def tile_count(self):
+        """(gradient variants, update variants) compiled for this solver's shape."""
+        out = (C.c_int * 2)()
+        _check(lib().fr_solver_tile_count(self.h, out))
+        return tuple(out)
+
+    def tile_info(self, kind, i):
+        """(elements, threads, CTAs per SM, persistent) of gradient (kind 0) or update (kind 1) variant i."""
+        out = (C.c_int * 4)()
+        _check(lib().fr_solver_tile_info(self.h, int(kind), int(i), out))
+        return tuple(out)
+
+    def select_tiles(self, g, u):
+        """Use gradient variant g and update variant u (as the autotuner would)."""
+        _check(lib().fr_solver_select_tiles(self.h, int(g), int(u)))
 
     def profile_stage(self, reps, dt):
         """Mean CUDA-event ms of the (gradient, interface-flux, update) kernels over reps stages."""

@@ -157,6 +157,17 @@ fr_status fr_solver_sync(fr_solver* s);
  * summation order of the residual norms. */
 fr_status fr_solver_autotune(fr_solver* s, int reps, int out4[4]);
 
+/* The compiled tile variants by index, as the autotuner walks them:
+ * fr_solver_tile_count returns {gradient variants, update variants};
+ * fr_solver_tile_info returns {elements, threads, CTAs per SM the registers
+ * are sized for, persistent} of gradient variant i (kind 0) or update variant
+ * i (kind 1); fr_solver_select_tiles makes variants g and u the ones used.
+ * Results do not depend on the choice (except the summation order of the
+ * residual norms). */
+fr_status fr_solver_tile_count(const fr_solver* s, int out2[2]);
+fr_status fr_solver_tile_info(const fr_solver* s, int kind, int i, int out4[4]);
+fr_status fr_solver_select_tiles(fr_solver* s, int g, int u);
+
 /* Runs `reps` RK stages one by one (advancing the state) and returns in ms3
  * the mean CUDA-event duration, on the solver's stream, of the three stage
  * kernels: gradient/flux (0 for inviscid runs), interface fluxes, and
