@@ -18,6 +18,7 @@ max over ranks.  `--impl reference` times the reference's own CPU code
 (oracle/_ref, built from the reference sources) on the host cores.
 """
 import argparse
+import re
 import json
 import os
 import subprocess
@@ -305,11 +306,14 @@ def run_b200(a, rank, world, local):
     tc = 4 if a.precision == "fp32" else 8
     b_elem = alg_bytes_per_element(3, P, True, s=8, m=tc, t=tc)
     achieved = b_elem * E / (stage_ms * 1e-3) / 1e9
+    # measured DRAM bytes of one stage (the three kernels), from the ncu
+    # capture summarised in profiles/ (a line "DRAM bytes per element per stage: N")
     traffic = None
-    tr_path = os.path.join(REPO, "profiles", "traffic_tgv_p%d_%s.json" % (P, a.precision))
+    tr_path = os.path.join(REPO, "profiles", "dram_tgv%d_p%d_%s.md" % (n, P, a.precision))
     if os.path.exists(tr_path):
-        tr = json.load(open(tr_path))
-        traffic = tr["bytes_per_element_per_stage"] * E
+        m = re.search(r"DRAM bytes per element per stage:\s*(\d+)", open(tr_path).read())
+        if m:
+            traffic = int(m.group(1)) * E
 
     # --- end to end through the public API with host buffers
     pinned = torch.empty(u0.size, dtype=torch.float64, pin_memory=True)
