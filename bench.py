@@ -249,7 +249,64 @@ def measure_forms(a, dev, fp64_value, s64, u0):
         b.close()
     out["batch"] = ("%d periodic TGV instances (NS, Mach 0.1, Re 1600), sizes n^3 with n in [8, 24] and P in "
                     "[2, 4] drawn with seed %d; DOF-updates per RK stage over all instances" % (BATCH_N, BATCH_SEED))
+    out["operator_path"] = measure_operator_path(a, dev, s64, u0)
     return out
+
+
+def measure_operator_path(a, dev, s64, u0):
+    """The reference's residual as per-operator calls (dense opp_0 .. opp_6
+    over all elements, pointer-table interface kernels): FP64 operator products
+    on the CUDA cores against the BF16 3-term split products on the tensor
+    cores, same workload, with the L2 error of the BF16 form after 20 steps,
+    and the extrapolation product alone (opp_0 U) in both precisions."""
+    import ctypes
+    import torch
+    from hifiles_b200 import seam
+    dt, steps = 1e-3, 3
+    phys = dict(gamma=GAMMA, prandtl=PR, mu_inf=1.0 / RE, rt_inf=1.0, c_sth=1.0, fix_vis=1.0, tau=1.0, pen_fact=0.5)
+    op = seam.OperatorStage(s64, phys, a.order, vcjh_scheme=1)
+    dof_step = op.E * op.nu * op.F * 5
+    res = {}
+    modes = ((0, "fp64"), (1, "bf16x3"), (2, "bf16x6"))
+    for mode, name in modes:
+        op.set_state(u0)
+        op.advance(1, dt, gemm_precision=mode)
+        ms = _time_steps(lambda k: op.advance(k, dt, gemm_precision=mode), op.stream, steps)
+        res[name] = {"value": dof_step / (ms * 1e-3), "ms_per_step": ms}
+    op.set_state(u0)
+    op.advance(20, dt, gemm_precision=0)
+    u_ref = op.get_state()
+    for mode, name in modes[1:]:
+        op.set_state(u0)
+        op.advance(20, dt, gemm_precision=mode)
+        u_tc = op.get_state()
+        res[name]["l2_rel_vs_fp64_after_20_steps"] = float(np.linalg.norm(u_tc - u_ref) / np.linalg.norm(u_ref))
+        res[name]["l2_rel_of_change_after_20_steps"] = float(np.linalg.norm(u_tc - u_ref) /
+                                                             np.linalg.norm(u_ref - u0))
+    # the extrapolation product opp_0 U alone (HBM-bound: U read, U_f written, FP64)
+    L = op.L
+    m, k, ncols = op.nf, op.nu, op.F * op.E
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for mode, name in modes:
+        L.fr_op_set_gemm_precision(mode)
+        for it in range(4):
+            if it == 1:
+                e0.record(op.stream)
+            L.fr_op_extrapolate_solution(m, k, op.F, op.E, op._ops["opp_0"].data_ptr(), op.u.data_ptr(),
+                                         op.ufp.data_ptr(), ctypes.c_void_p(op.stream.cuda_stream))
+        e1.record(op.stream)
+        e1.synchronize()
+        L.fr_op_set_gemm_precision(0)
+        t = e0.elapsed_time(e1) / 3 * 1e-3
+        bytes_ = 8.0 * (k + m) * ncols
+        flops = 2.0 * m * k * ncols * (1, 3, 6)[mode]
+        res[name]["opp_0_product"] = {"ms": t * 1e3, "GB/s": bytes_ / t / 1e9, "TFLOP/s": flops / t / 1e12}
+    res["workload"] = ("same TGV mesh and state; one step = 5 RK stages of CalcResidual through the fr_op_* "
+                       "entry points; operator products in FP64 on the CUDA cores, or BF16x3 / BF16x6 split "
+                       "products on the tcgen05 tensor cores with FP32 accumulation")
+    del op
+    torch.cuda.empty_cache()
+    return res
 
 
 def run_b200(a, rank, world, local):

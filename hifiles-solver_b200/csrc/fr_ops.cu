@@ -14,6 +14,10 @@
 
 namespace frb {
 extern thread_local std::string g_err;
+// BF16 3-term split operator product on the tensor cores (fr_tc_gemm.cu)
+fr_status gemm_bf16x3(int m, int k, long long ncols, const double* A, const double* B, double* C, int beta,
+                      cudaStream_t s, int terms);
+fr_status gemm_bf16x3_check(cudaStream_t s);
 }
 using namespace frb;
 
@@ -71,11 +75,17 @@ dense_apply_kernel(int m, int k, long long ncols, const double* __restrict__ A, 
   for (int i = threadIdx.x; i < nc * m; i += kDenseThreads) Ct[i] = sC[i];
 }
 
+// Precision of the operator products of this seam: 0 = FP64 (dense_apply_kernel),
+// 1 = BF16x3 and 2 = BF16x6 split products on the tensor cores, FP32
+// accumulation (fr_tc_gemm.cu).
+static int g_gemm_mode = 0;
+
 fr_status dense_apply(int m, int k, long long ncols, const double* A, const double* B, double* Cm, int beta,
                       cudaStream_t s)
 {
   if (m <= 0 || k <= 0 || ncols < 0 || !A || !B || !Cm) return op_fail(FR_ERR_ARG, "bad operator arguments");
   if (ncols == 0) return FR_OK;
+  if (g_gemm_mode) return gemm_bf16x3(m, k, ncols, A, B, Cm, beta, s, g_gemm_mode == 2 ? 6 : 3);
   size_t smem = ((size_t)k * kTileCols + (size_t)kTileCols * m) * sizeof(double);
   if (smem > 220 * 1024) return op_fail(FR_ERR_UNSUPPORTED, "operator too large for one column tile");
   if (smem > 48 * 1024) {
@@ -276,6 +286,23 @@ bool dims_ok(int d, int F) { return (d == 2 && F == 4) || (d == 3 && F == 5); }
 #define ST(stream) ((cudaStream_t)(stream))
 
 extern "C" {
+
+fr_status fr_op_set_gemm_precision(int mode)
+{
+  if (mode < 0 || mode > 2)
+    return op_fail(FR_ERR_ARG, "GEMM precision: 0 (FP64), 1 (BF16x3) or 2 (BF16x6 tensor cores)");
+  g_gemm_mode = mode;
+  return FR_OK;
+}
+
+int fr_op_gemm_precision(void) { return g_gemm_mode; }
+
+fr_status fr_op_check(void* stream)
+{
+  cudaError_t e = cudaStreamSynchronize(ST(stream));
+  if (e != cudaSuccess) return op_fail(FR_ERR_CUDA, cudaGetErrorString(e));
+  return gemm_bf16x3_check(ST(stream));
+}
 
 fr_status fr_op_extrapolate_solution(int n_fpts, int n_upts, int n_fields, int n_eles, const double* opp_0,
                                      const double* disu_upts, double* disu_fpts, void* stream)

@@ -1,0 +1,353 @@
+// fr_tc_gemm.cu -- the dense operator product of the per-operator seam,
+// C = A B (+ C), on the fifth-generation tensor cores in BF16 with a 3-term
+// split and FP32 accumulation: the GEMM precision form of the reference's
+// cublasDgemm('N','N', m, ncols, k, 1, opp, m, B, k, beta, C, m) calls
+// (eles::extrapolate_solution, calculate_gradient, ... , src/eles.cpp).
+//
+// Split: x = x0 + x1 + x2 with x0 = bf16(x), x1 = bf16(x - x0),
+// x2 = bf16(x - x0 - x1).  TERMS = 3 (BF16x3) keeps x0y0 + x0y1 + x1y0, about
+// 16 bits; TERMS = 6 (BF16x6) adds x0y2 + x1y1 + x2y0, about 24 bits (FP32
+// level).  Either is one GEMM over K' = TERMS KP:
+//   BF16x3:  A' = [A0 | A0 | A1],            B' = [B0 ; B1 ; B0]
+//   BF16x6:  A' = [A0 | A0 | A1 | A0 | A1 | A2],  B' = [B0 ; B1 ; B0 ; B2 ; B1 ; B0]
+// KP is k rounded up to 16 (zeros), M = 128 rows (m <= 128, zero rows), N = 64
+// columns per tile.  Inputs and outputs stay FP64 in HBM.
+//
+// One block of 128 threads per tile pass, persistent over column tiles:
+// the threads stage A' once and B' per tile into shared memory in the
+// K-major, no-swizzle canonical layout (8 x 16-byte core matrices), one
+// thread issues the K'/16 tcgen05.mma instructions into a TMEM accumulator
+// (128 lanes x 64 columns) and commits them to an mbarrier; the four warps
+// read their 32 lanes back with tcgen05.ld and write C.  Every mbarrier wait
+// is bounded: on expiry the kernel sets the error flag, waits once more
+// (bounded) for its MMAs, frees its TMEM and returns.
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "fr_b200.h"
+
+namespace frb {
+extern thread_local std::string g_err;
+
+namespace {
+
+constexpr int kTM = 128;          // rows of the MMA tile (operator rows, zero-padded)
+constexpr int kTN = 64;           // columns per tile
+constexpr int kThreads = 128;
+constexpr uint32_t kTmemCols = 64;
+constexpr long long kWaitLimit = 1LL << 20;   // x 1 us suspend hint: about a second
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor, K-major, no swizzle (layout type 0),
+// descriptor version 1; offsets in bytes (16-byte units in the descriptor)
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
+{
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+// instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
+// K-major, N >> 3 at bit 17, M >> 4 at bit 24
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTN >> 3) << 17) |
+                            ((uint32_t)(kTM >> 4) << 24);
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate)
+{
+  asm volatile(
+      "{\n\t"
+      ".reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
+      "}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar)
+{
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity)
+{
+  uint32_t ok;
+  asm volatile(
+      "{\n\t"
+      ".reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t"
+      "}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(1000u)
+      : "memory");
+  return ok != 0;
+}
+
+// bounded wait on an mbarrier phase; false when the limit ran out
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+{
+  for (long long i = 0; i < kWaitLimit; i++)
+    if (mbar_try(bar, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
+{
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// 8 values -> 16-byte chunks of their three BF16 parts (x0 + x1 + x2 = x to
+// about 24 bits; each residual is formed in FP64)
+__device__ __forceinline__ void split8(const double (&x)[8], uint4 (&q)[3])
+{
+  uint32_t w[3][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    uint32_t lo16[3], hi16[3];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      double r = x[2 * i + h];
+#pragma unroll
+      for (int t = 0; t < 3; t++) {
+        const __nv_bfloat16 b = __double2bfloat16(r);
+        r -= (double)__bfloat162float(b);
+        (h ? hi16 : lo16)[t] = __bfloat16_as_ushort(b);
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < 3; t++) w[t][i] = lo16[t] | (hi16[t] << 16);
+  }
+#pragma unroll
+  for (int t = 0; t < 3; t++) q[t] = make_uint4(w[t][0], w[t][1], w[t][2], w[t][3]);
+}
+
+// part of A' (a = 1) or B' (a = 0) in K-copy j of the split product
+template <int TERMS>
+__device__ __forceinline__ int part_of(int j, int a)
+{
+  // BF16x3: A 0 0 1, B 0 1 0; BF16x6: A 0 0 1 0 1 2, B 0 1 0 2 1 0
+  constexpr int PA[6] = {0, 0, 1, 0, 1, 2}, PB[6] = {0, 1, 0, 2, 1, 0};
+  return a ? PA[j] : PB[j];
+}
+
+// byte offset of 16-byte chunk (row, kchunk) of a K-major tile of R rows
+__device__ __forceinline__ uint32_t chunk_off(int row, int kc, int R)
+{
+  return (uint32_t)((kc * (R / 8) + row / 8) * 128 + (row % 8) * 16);
+}
+
+template <int TERMS>
+__global__ void __launch_bounds__(kThreads)
+fr_gemm_bf16x3_kernel(int m, int k, int KP, long long ncols, const double* __restrict__ A,
+                      const double* __restrict__ B, double* __restrict__ C, int beta, int* __restrict__ err)
+{
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const int KC = KP / 8;                   // 16-byte chunks of one copy of K
+  const int KQ = TERMS * KC;               // chunks of K'
+  unsigned char* sA = sm;                  // kTM x K' bf16
+  unsigned char* sB = sm + (size_t)kTM * KQ * 16;   // kTN x K' bf16
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_slot;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // A' once: rows r (fastest) x chunks c of A
+  for (int w = tid; w < kTM * KC; w += kThreads) {
+    const int r = w % kTM, c = w / kTM;
+    double x[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int kk = 8 * c + i;
+      x[i] = (r < m && kk < k) ? __ldg(A + r + (size_t)m * kk) : 0.0;
+    }
+    uint4 q[3];
+    split8(x, q);
+#pragma unroll
+    for (int j = 0; j < TERMS; j++) *reinterpret_cast<uint4*>(sA + chunk_off(r, j * KC + c, kTM)) = q[part_of<TERMS>(j, 1)];
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = tmem_slot;
+  const long long ntiles = (ncols + kTN - 1) / kTN;
+  uint32_t parity = 0;
+  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const long long j0 = t * kTN;
+    // B' for columns j0 ..: columns n (fastest) x chunks c
+    for (int w = tid; w < kTN * KC; w += kThreads) {
+      const int n = w % kTN, c = w / kTN;
+      const long long j = j0 + n;
+      double x[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        const int kk = 8 * c + i;
+        x[i] = (j < ncols && kk < k) ? __ldg(B + (size_t)j * k + kk) : 0.0;
+      }
+      uint4 q[3];
+      split8(x, q);
+#pragma unroll
+      for (int jj = 0; jj < TERMS; jj++)
+        *reinterpret_cast<uint4*>(sB + chunk_off(n, jj * KC + c, kTN)) = q[part_of<TERMS>(jj, 0)];
+    }
+    // generic-proxy writes -> visible to the tensor cores' reads
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    fence_before();
+    __syncthreads();
+    fence_after();
+    if (tid == 0) {
+      const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+      for (int s = 0; s < KQ / 2; s++) {
+        const uint64_t ad = umma_desc(a0 + (uint32_t)(2 * s) * (kTM / 8) * 128, (kTM / 8) * 128, 128);
+        const uint64_t bd = umma_desc(b0 + (uint32_t)(2 * s) * (kTN / 8) * 128, (kTN / 8) * 128, 128);
+        mma_bf16(tmem, ad, bd, s > 0 ? 1u : 0u);
+      }
+      mma_commit(&bar);
+    }
+    // every thread waits (bounded); the block leaves together if any ran out
+    if (!__syncthreads_and(mbar_wait(&bar, parity) ? 1 : 0)) {
+      if (tid == 0) atomicExch(err, 1);
+      mbar_wait(&bar, parity);             // the MMAs may still be running
+      break;
+    }
+    parity ^= 1u;
+    fence_after();
+    // accumulator rows 32 warp .. +31 -> C
+    const int r = 32 * warp + lane;
+#pragma unroll
+    for (int h = 0; h < kTN / 32; h++) {
+      float v[32];
+      tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(32 * h), v);
+      if (r < m) {
+#pragma unroll
+        for (int i = 0; i < 32; i++) {
+          const long long j = j0 + 32 * h + i;
+          if (j < ncols) {
+            double* c = C + r + (size_t)m * j;
+            *c = beta ? *c + (double)v[i] : (double)v[i];
+          }
+        }
+      }
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+}
+
+int* g_gemm_err = nullptr;
+
+}  // namespace
+
+// Shared memory of one block: the A' and B' tiles.
+static size_t gemm_split_smem(int k, int terms)
+{
+  const int KP = (k + 15) / 16 * 16;
+  return (size_t)(kTM + kTN) * terms * KP * 2;
+}
+
+// terms = 3 (BF16x3): operators up to 128 x 128; terms = 6 (BF16x6): up to 128 x 96
+bool gemm_split_supported(int m, int k, int terms)
+{
+  return m >= 1 && m <= kTM && k >= 1 && k <= (terms == 6 ? 96 : 128);
+}
+
+fr_status gemm_bf16x3(int m, int k, long long ncols, const double* A, const double* B, double* C, int beta,
+                      cudaStream_t s, int terms)
+{
+  if (terms != 3 && terms != 6) {
+    g_err = "split products have 3 or 6 terms";
+    return FR_ERR_ARG;
+  }
+  if (!gemm_split_supported(m, k, terms)) {
+    g_err = terms == 6 ? "BF16x6 operator product: operators up to 128 x 96"
+                       : "BF16x3 operator product: operators up to 128 x 128";
+    return FR_ERR_UNSUPPORTED;
+  }
+  if (ncols == 0) return FR_OK;
+  if (!g_gemm_err) {
+    cudaError_t e = cudaMalloc(&g_gemm_err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(g_gemm_err, 0, sizeof(int));
+    if (e != cudaSuccess) {
+      g_err = cudaGetErrorString(e);
+      return FR_ERR_CUDA;
+    }
+  }
+  const size_t smem = gemm_split_smem(k, terms);
+  const void* kfn = terms == 6 ? (const void*)fr_gemm_bf16x3_kernel<6> : (const void*)fr_gemm_bf16x3_kernel<3>;
+  cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) {
+    g_err = cudaGetErrorString(e);
+    return FR_ERR_CUDA;
+  }
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kfn, kThreads, smem);
+  const long long ntiles = (ncols + kTN - 1) / kTN;
+  long long grid = (long long)(per > 0 ? per : 1) * (sms > 0 ? sms : 1);
+  if (grid > ntiles) grid = ntiles;
+  if (terms == 6)
+    fr_gemm_bf16x3_kernel<6><<<(unsigned)grid, kThreads, smem, s>>>(m, k, (k + 15) / 16 * 16, ncols, A, B, C, beta,
+                                                                     g_gemm_err);
+  else
+    fr_gemm_bf16x3_kernel<3><<<(unsigned)grid, kThreads, smem, s>>>(m, k, (k + 15) / 16 * 16, ncols, A, B, C, beta,
+                                                                     g_gemm_err);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    g_err = std::string("fr_gemm_bf16x3_kernel: ") + cudaGetErrorString(e);
+    return FR_ERR_CUDA;
+  }
+  return FR_OK;
+}
+
+// FR_ERR_TIMEOUT if a tensor-core product gave up waiting for its MMAs since
+// the last check (the flag is cleared); synchronises the stream.
+fr_status gemm_bf16x3_check(cudaStream_t s)
+{
+  if (!g_gemm_err) return FR_OK;
+  int v = 0;
+  cudaError_t e = cudaMemcpyAsync(&v, g_gemm_err, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    g_err = cudaGetErrorString(e);
+    return FR_ERR_CUDA;
+  }
+  if (v) {
+    cudaMemsetAsync(g_gemm_err, 0, sizeof(int), s);
+    g_err = "tensor-core operator product: MMA completion wait ran out";
+    return FR_ERR_TIMEOUT;
+  }
+  return FR_OK;
+}
+
+}  // namespace frb

@@ -263,6 +263,7 @@ class Solver:
         self.n_eles, self.n_upts, self.n_fpts, self.n_fields, self.dims, self.n_int = list(sz)
         self.viscous = bool(viscous)
         self.precision = precision
+        self.device = int(device)
 
     @classmethod
     def box(cls, dims, order, n, lo, hi, jitter=0.0, seed=0, side_bc=None, **kw):

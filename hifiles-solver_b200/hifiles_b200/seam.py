@@ -1,0 +1,224 @@
+"""The reference's residual as a sequence of per-operator calls.
+
+`OperatorStage` runs CalcResidual (src/solver.cpp:65-225) and
+eles::AdvanceSolution (src/eles.cpp:1091-1188) for one element type through
+the fr_op_* entry points of include/fr_b200.h: the dense operators
+opp_0 .. opp_6 applied to all elements (the reference's cublasDgemm calls),
+the pointwise flux kernels, and the interface kernels over tables of
+pointers (int_inters' disu_fpts_l / _r ... pointer arrays).  The operator
+products run in FP64 (0) or as BF16 split products on the tensor cores,
+BF16x3 (1) or BF16x6 (2) (`fr_op_set_gemm_precision`); `gemm_precision`
+selects it per call.
+
+The dense operators are built from the library's 1-D factors (`fr_line_operators`):
+for Gauss solution points every row of opp_0 .. opp_6 has one non-zero 1-D
+factor per line, so the Kronecker construction below reproduces the
+reference's matrices (eles::set_opp_0 .. set_opp_6, src/eles.cpp:3620-4052)
+entry for entry.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _check, lib, line_operators
+
+_VP = C.c_void_p
+
+
+class PhysDesc(C.Structure):
+    """fr_phys_desc of include/fr_b200.h."""
+    _fields_ = [(n, C.c_double) for n in ("gamma", "prandtl", "mu_inf", "rt_inf", "c_sth", "fix_vis", "tau",
+                                          "pen_fact")]
+
+
+def _face_lines(dims, P):
+    """Per flux point: (fixed coordinates, axis, plus) of the line of solution
+    points through it, in the reference's flux-point order (quads
+    src/eles_quads.cpp:259-300, hexes src/eles_hexas.cpp:262-324)."""
+    n = P + 1
+    nfpf = n ** (dims - 1)
+    out = []
+    for f in range(2 * dims * nfpf):
+        fc, r = divmod(f, nfpf)
+        if dims == 2:
+            j = r
+            out.append({0: ((j, None), 1, 0), 1: ((None, j), 0, 1), 2: ((P - j, None), 1, 1),
+                        3: ((None, P - j), 0, 0)}[fc])
+        else:
+            j, k = divmod(r, n)
+            out.append({0: ((P - k, j, None), 2, 0), 1: ((k, None, j), 1, 0), 2: ((None, k, j), 0, 1),
+                        3: ((P - k, None, j), 1, 1), 4: ((None, P - k, j), 0, 0), 5: ((k, j, None), 2, 1)}[fc])
+    return out
+
+
+def dense_operators(dims, P, upts_type=0, vcjh_scheme=1, eta=0.0):
+    """opp_0 (nf x nu), opp_1[d] (nf x nu), opp_2[d] = opp_4[d] (nu x nu),
+    opp_3 (nu x nf), opp_5[d] (nu x nf), opp_6 = opp_0, column-major float64."""
+    L = line_operators(P, upts_type, vcjh_scheme, eta)
+    n = P + 1
+    nu = n ** dims
+    lines = _face_lines(dims, P)
+    nf = len(lines)
+
+    def abc(u):
+        return (u % n, (u // n) % n, u // (n * n)) if dims == 3 else (u % n, u // n, 0)
+
+    o0 = np.zeros((nf, nu))
+    o3 = np.zeros((nu, nf))
+    nrm = np.zeros((nf, dims))            # reference-element unit normal of each flux point
+    for f, (fixed, ax, plus) in enumerate(lines):
+        nrm[f, ax] = 1.0 if plus else -1.0
+        for u in range(nu):
+            c = abc(u)
+            if all(fixed[d] is None or fixed[d] == c[d] for d in range(dims)):
+                o0[f, u] = (L["Lp"] if plus else L["Lm"])[c[ax]]
+                o3[u, f] = L["gR"][c[ax]] if plus else -L["gL"][c[ax]]
+    o2 = []
+    for d in range(dims):
+        Dm = np.zeros((nu, nu))
+        for k in range(nu):
+            ck = abc(k)
+            for u in range(nu):
+                cu = abc(u)
+                if all(cu[e] == ck[e] for e in range(dims) if e != d):
+                    Dm[k, u] = L["D"][ck[d], cu[d]]
+        o2.append(Dm)
+    o1 = [o0 * nrm[:, d][:, None] for d in range(dims)]
+    o5 = [o3 * nrm[:, d][None, :] for d in range(dims)]
+    F = lambda a: np.asfortranarray(a)  # noqa: E731
+    return dict(opp_0=F(o0), opp_1=[F(a) for a in o1], opp_2=[F(a) for a in o2], opp_3=F(o3),
+                opp_4=[F(a) for a in o2], opp_5=[F(a) for a in o5], opp_6=F(o0))
+
+
+def _bind(L):
+    i, vp = C.c_int, _VP
+    sig = {
+        "fr_op_extrapolate_solution": [i, i, i, i, vp, vp, vp, vp],
+        "fr_op_evaluate_invFlux": [i, i, i, i, vp, vp, vp, vp, vp],
+        "fr_op_calculate_gradient": [i, i, i, i, vp, vp, vp, vp],
+        "fr_op_correct_gradient": [i, i, i, i, i, vp, vp, vp, vp, vp, vp],
+        "fr_op_extrapolate_corrected_gradient": [i, i, i, i, i, vp, vp, vp, vp],
+        "fr_op_evaluate_viscFlux": [i, i, i, i, vp, vp, vp, vp, vp, vp],
+        "fr_op_extrapolate_totalFlux": [i, i, i, i, i, vp, vp, vp, vp],
+        "fr_op_calculate_divergence": [i, i, i, i, vp, vp, vp, vp],
+        "fr_op_calculate_corrected_divergence": [i, i, i, i, vp, vp, vp, vp, vp],
+        "fr_op_int_inters_common_invFlux": [i, i, i, i] + [vp] * 9 + [vp, i, vp],
+        "fr_op_int_inters_common_viscFlux": [i, i, i, i] + [vp] * 9 + [vp, vp],
+        "fr_op_advance_rk45": [i, i, i, i, C.c_double, C.c_double, vp, vp, vp, vp, vp, vp],
+        "fr_op_set_gemm_precision": [i],
+        "fr_op_check": [vp],
+    }
+    for name, args in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = C.c_int
+    L.fr_op_gemm_precision.restype = C.c_int
+    return L
+
+
+class OperatorStage:
+    """One element type of a periodic mesh, advanced through the per-operator
+    entry points.  `solver` (a hifiles_b200.Solver of the same scheme) supplies
+    the metrics and the interface wiring; the state lives here as a torch
+    tensor of layout (n_upts, n_eles, n_fields)."""
+
+    def __init__(self, solver, physics, order, vcjh_scheme=1, eta=0.0, upts_type=0, viscous=True):
+        import torch
+        self.torch = torch
+        self.L = _bind(lib())
+        s = solver
+        self.E, self.nu, self.nf, self.F, self.D = s.n_eles, s.n_upts, s.n_fpts, s.n_fields, s.dims
+        self.visc = bool(viscous)
+        E, nu, nf, F, D = self.E, self.nu, self.nf, self.F, self.D
+        dev = "cuda:%d" % s.device
+        z = lambda n: torch.zeros(n, dtype=torch.float64, device=dev)  # noqa: E731
+        t = lambda a: torch.from_numpy(np.asfortranarray(a).ravel(order="F")).to(dev)  # noqa: E731
+        ops = dense_operators(D, order, upts_type, vcjh_scheme, eta)
+        self._ops = {k: (t(v) if not isinstance(v, list) else [t(a) for a in v]) for k, v in ops.items()}
+        self._tabs = {k: (C.c_void_p * D)(*[a.data_ptr() for a in self._ops[k]])
+                      for k in ("opp_1", "opp_2", "opp_4", "opp_5")}
+        g = s.geometry()
+        self.JG, self.dj, self.tdA, self.nrm = (t(g[k]) for k in ("JGinv_upts", "detjac_upts", "tdA_fpts",
+                                                                   "norm_fpts"))
+        self.u, self.reg, self.div = z(nu * E * F), z(nu * E * F), z(nu * E * F)
+        self.ufp, self.ntc, self.ntd, self.ddu = z(nf * E * F), z(nf * E * F), z(nf * E * F), z(nf * E * F)
+        self.tf, self.gup, self.gfp = z(nu * E * F * D), z(nu * E * F * D), z(nf * E * F * D)
+        il, ir = s.interfaces()
+        il, ir = il.astype(np.int64), ir.astype(np.int64)
+        self.ni = len(il)
+        fk = np.arange(F)[None, :] * (nf * E)
+        gk = (np.arange(F)[:, None] + F * np.arange(D)[None, :]).ravel(order="F")[None, :] * (nf * E)
+
+        def table(base, offsets):
+            a = base.data_ptr() + 8 * np.asarray(offsets, dtype=np.int64).ravel(order="F")
+            return torch.from_numpy(a.astype(np.int64)).to(dev)
+
+        self._pt = dict(ul=table(self.ufp, il[:, None] + fk), ur=table(self.ufp, ir[:, None] + fk),
+                        tl=table(self.ntc, il[:, None] + fk), tr=table(self.ntc, ir[:, None] + fk),
+                        dl=table(self.ddu, il[:, None] + fk), dr=table(self.ddu, ir[:, None] + fk),
+                        al=table(self.tdA, il), ar=table(self.tdA, ir),
+                        n=table(self.nrm, il[:, None] + np.arange(D)[None, :] * (nf * E)),
+                        gl=table(self.gfp, il[:, None] + gk), gr=table(self.gfp, ir[:, None] + gk))
+        self.ph = PhysDesc(**physics)
+        self.stream = torch.cuda.current_stream(dev)
+
+    # -- state
+    def set_state(self, u):
+        self.u.copy_(self.torch.from_numpy(np.asfortranarray(u).ravel(order="F")))
+
+    def get_state(self):
+        self.torch.cuda.synchronize()
+        return self.u.cpu().numpy().reshape((self.nu, self.E, self.F), order="F")
+
+    def _ok(self, st):
+        if st != 0:
+            raise RuntimeError(lib().fr_last_error().decode())
+
+    def residual(self, gemm_precision=0):
+        """div_tconf_upts of the current state (CalcResidual)."""
+        L, P = self.L, (lambda a: a.data_ptr())
+        E, nu, nf, F, D = self.E, self.nu, self.nf, self.F, self.D
+        sp = C.c_void_p(self.stream.cuda_stream)
+        ph = C.byref(self.ph)
+        pt = {k: P(v) for k, v in self._pt.items()}
+        self._ok(L.fr_op_set_gemm_precision(int(gemm_precision)))
+        try:
+            self._ok(L.fr_op_extrapolate_solution(nf, nu, F, E, P(self._ops["opp_0"]), P(self.u), P(self.ufp), sp))
+            if self.visc:
+                self._ok(L.fr_op_calculate_gradient(nu, D, F, E, C.cast(self._tabs["opp_4"], _VP), P(self.u),
+                                                    P(self.gup), sp))
+            self._ok(L.fr_op_evaluate_invFlux(nu, D, F, E, P(self.u), P(self.JG), P(self.tf), ph, sp))
+            self._ok(L.fr_op_int_inters_common_invFlux(1, D, F, self.ni, pt["ul"], pt["ur"], pt["tl"], pt["tr"],
+                                                       pt["al"], pt["ar"], pt["n"], pt["dl"], pt["dr"], ph,
+                                                       int(self.visc), sp))
+            if self.visc:
+                self._ok(L.fr_op_correct_gradient(nu, nf, D, F, E, C.cast(self._tabs["opp_5"], _VP), P(self.ddu),
+                                                  P(self.JG), P(self.dj), P(self.gup), sp))
+                self._ok(L.fr_op_extrapolate_corrected_gradient(nf, nu, D, F, E, P(self._ops["opp_6"]),
+                                                                P(self.gup), P(self.gfp), sp))
+                self._ok(L.fr_op_evaluate_viscFlux(nu, D, F, E, P(self.u), P(self.gup), P(self.JG), P(self.tf),
+                                                   ph, sp))
+            self._ok(L.fr_op_extrapolate_totalFlux(nf, nu, D, F, E, C.cast(self._tabs["opp_1"], _VP), P(self.tf),
+                                                   P(self.ntd), sp))
+            self._ok(L.fr_op_calculate_divergence(nu, D, F, E, C.cast(self._tabs["opp_2"], _VP), P(self.tf),
+                                                  P(self.div), sp))
+            if self.visc:
+                self._ok(L.fr_op_int_inters_common_viscFlux(1, D, F, self.ni, pt["ul"], pt["ur"], pt["gl"],
+                                                            pt["gr"], pt["tl"], pt["tr"], pt["al"], pt["ar"],
+                                                            pt["n"], ph, sp))
+            self._ok(L.fr_op_calculate_corrected_divergence(nu, nf, F, E, P(self._ops["opp_3"]), P(self.ntd),
+                                                            P(self.ntc), P(self.div), sp))
+        finally:
+            L.fr_op_set_gemm_precision(0)
+        return self.div
+
+    def advance(self, n_steps, dt, gemm_precision=0):
+        """n_steps RK45 steps (5 stages each) through the operator seam."""
+        L, P = self.L, (lambda a: a.data_ptr())
+        sp = C.c_void_p(self.stream.cuda_stream)
+        for _ in range(n_steps):
+            for k in range(5):
+                self.residual(gemm_precision)
+                self._ok(L.fr_op_advance_rk45(self.nu, self.F, self.E, k, float(dt), 0.0, P(self.u), P(self.reg),
+                                              P(self.div), P(self.dj), None, sp))
+        self._ok(L.fr_op_check(sp))

@@ -397,6 +397,24 @@ fr_status fr_op_advance_rk45(int n_upts, int n_fields, int n_eles, int stage, do
                              double* disu_upts_0, double* disu_upts_1, const double* div_tconf_upts,
                              const double* detjac_upts, const double* src_upts, void* stream);
 
+/* Precision of the operator products (opp_0 .. opp_6 applied to all
+ * elements, the reference's cublasDgemm calls) of the fr_op_* entry points,
+ * process-wide like the reference's run_input:
+ *   0  FP64 on the CUDA cores (default; parity with the reference),
+ *   1  BF16x3: x = x0 + x1 + x2 in BF16, products x0y0 + x0y1 + x1y0 (about
+ *      16 bits) on the tcgen05 tensor cores, FP32 accumulation, FP64 inputs
+ *      and outputs; operators up to 128 x 128 (quads up to P = 10, hexes up
+ *      to P = 3),
+ *   2  BF16x6: the same plus x0y2 + x1y1 + x2y0 (about 24 bits); operators
+ *      up to 128 x 96 (hexes up to P = 3);
+ * larger operators return FR_ERR_UNSUPPORTED.
+ * Pointwise kernels stay FP64.  fr_op_check synchronises the stream and
+ * returns FR_ERR_TIMEOUT if a tensor-core product gave up waiting for its
+ * MMAs since the last check. */
+fr_status fr_op_set_gemm_precision(int mode);
+int fr_op_gemm_precision(void);
+fr_status fr_op_check(void* stream);
+
 /* ------------------------------------------------------------------------
  * Residual without device allocation.
  *

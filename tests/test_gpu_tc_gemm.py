@@ -1,0 +1,146 @@
+"""The tensor-core form of the per-operator path: the operator product in
+BF16 with a 3-term split (tcgen05, FP32 accumulation) against FP64, and a
+whole RK45 step through the per-operator entry points against the fused
+solver."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+import hifiles_b200 as H
+from hifiles_b200 import seam
+
+pytestmark = pytest.mark.gpu
+
+VP = C.c_void_p
+GAMMA, MACH, RE, PR = 1.4, 0.1, 1600.0, 0.71
+
+
+def _lib():
+    L = seam._bind(H.lib())
+    return L
+
+
+def _dev(a):
+    return torch.from_numpy(np.asfortranarray(a).ravel(order="F").copy()).cuda()
+
+
+def _host(t, shape):
+    torch.cuda.synchronize()
+    return t.cpu().numpy().reshape(shape, order="F")
+
+
+def _product(L, A, B, mode):
+    m, k = A.shape
+    n = B.shape[1]
+    dA, dB = _dev(A), _dev(B)
+    dC = torch.zeros(m * n, dtype=torch.float64, device="cuda")
+    assert L.fr_op_set_gemm_precision(mode) == 0
+    try:
+        st = L.fr_op_extrapolate_solution(m, k, 1, n, dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), None)
+        assert st == 0, H.lib().fr_last_error().decode()
+        assert L.fr_op_check(None) == 0, H.lib().fr_last_error().decode()
+    finally:
+        L.fr_op_set_gemm_precision(0)
+    return _host(dC, (m, n))
+
+
+@pytest.mark.parametrize("m,k,n", [(96, 64, 5 * 1000 + 3), (64, 96, 777), (128, 128, 64 * 40), (16, 16, 100),
+                                   (1, 1, 5), (64, 64, 64)])
+def test_bf16x3_product_against_fp64(m, k, n):
+    rng = np.random.default_rng(7 + m + k)
+    A = rng.standard_normal((m, k))
+    B = rng.standard_normal((k, n))
+    ref = A @ B
+    L = _lib()
+    c64 = _product(L, A, B, 0)
+    assert np.abs(c64 - ref).max() <= 1e-12 * np.abs(ref).max() * max(1, k)
+    c3 = _product(L, A, B, 1)
+    err = np.linalg.norm(c3 - ref) / np.linalg.norm(ref)
+    # x0 + x1 keeps ~16 bits of each operand: a few 1e-6 relative
+    assert 1e-9 < err < 3e-5, err
+    if k <= 96:
+        c6 = _product(L, A, B, 2)
+        err6 = np.linalg.norm(c6 - ref) / np.linalg.norm(ref)
+        # x0 + x1 + x2 keeps ~24 bits; the FP32 accumulation over the 6 k
+        # products (about 1e-6 relative on random data) is then the limit
+        assert err6 < 2e-6 and err6 < err / 4, (err6, err)
+
+
+def test_bf16x3_accumulates_into_c():
+    """beta = 1 (div += opp_3 (norm_tconf - norm_tdisf)) in the tensor-core form."""
+    rng = np.random.default_rng(3)
+    nu, nf, F, E = 64, 96, 5, 300
+    A = rng.standard_normal((nu, nf))
+    ntd, ntc, div = (rng.standard_normal((nf, F * E)), rng.standard_normal((nf, F * E)),
+                     rng.standard_normal((nu, F * E)))
+    ref = div + A @ (ntc - ntd)
+    L = _lib()
+    dA, d_ntd, d_ntc, d_div = _dev(A), _dev(ntd), _dev(ntc), _dev(div)
+    assert L.fr_op_set_gemm_precision(1) == 0
+    try:
+        assert L.fr_op_calculate_corrected_divergence(nu, nf, F, E, dA.data_ptr(), d_ntd.data_ptr(), d_ntc.data_ptr(),
+                                                      d_div.data_ptr(), None) == 0
+        assert L.fr_op_check(None) == 0
+    finally:
+        L.fr_op_set_gemm_precision(0)
+    out = _host(d_div, (nu, F * E))
+    assert np.linalg.norm(out - ref) / np.linalg.norm(ref) < 3e-5
+
+
+def test_bf16x3_rejects_operators_beyond_one_tile():
+    L = _lib()
+    A = np.ones((150, 125))
+    B = np.ones((125, 10))
+    dA, dB = _dev(A), _dev(B)
+    dC = torch.zeros(150 * 10, dtype=torch.float64, device="cuda")
+    assert L.fr_op_set_gemm_precision(1) == 0
+    try:
+        st = L.fr_op_extrapolate_solution(150, 125, 1, 10, dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), None)
+    finally:
+        L.fr_op_set_gemm_precision(0)
+    assert st == 5
+    dB2 = _dev(np.ones((100, 10)))
+    assert L.fr_op_set_gemm_precision(2) == 0
+    try:
+        st = L.fr_op_extrapolate_solution(64, 100, 1, 10, dA.data_ptr(), dB2.data_ptr(), dC.data_ptr(), None)
+    finally:
+        L.fr_op_set_gemm_precision(0)
+    assert st == 5
+    assert L.fr_op_set_gemm_precision(3) == 1
+
+
+def _tgv(pos):
+    x, y, z = pos[..., 0], pos[..., 1], pos[..., 2]
+    p = 1.0 / (GAMMA * MACH * MACH) + (np.cos(2 * x) + np.cos(2 * y)) * (np.cos(2 * z) + 2.0) / 16.0
+    u = np.sin(x) * np.cos(y) * np.cos(z)
+    v = -np.cos(x) * np.sin(y) * np.cos(z)
+    return np.asfortranarray(np.stack([np.ones_like(x), u, v, np.zeros_like(x),
+                                       p / (GAMMA - 1.0) + 0.5 * (u * u + v * v)], axis=-1))
+
+
+def test_operator_path_step_matches_fused_solver_and_bf16x3_error_is_small():
+    L2 = 2 * np.pi
+    phys = dict(gamma=GAMMA, prandtl=PR, mu_inf=1.0 / RE, rt_inf=1.0, c_sth=1.0, fix_vis=1.0, tau=1.0, pen_fact=0.5)
+    s = H.Solver.box(3, 3, (4, 4, 4), (0, 0, 0), (L2, L2, L2), viscous=True, vcjh_scheme=1, **phys)
+    u0 = _tgv(s.geometry()["pos_upts"])
+    s.set_state(u0)
+    s.advance(2, 1e-3)
+    fused = s.get_state()
+    op = seam.OperatorStage(s, phys, 3, vcjh_scheme=1)
+    op.set_state(u0)
+    op.advance(2, 1e-3)
+    u64 = op.get_state()
+    assert np.linalg.norm(u64 - fused) / np.linalg.norm(fused) < 1e-13
+    op.set_state(u0)
+    op.advance(2, 1e-3, gemm_precision=1)
+    u3 = op.get_state()
+    err = np.linalg.norm(u3 - u64) / np.linalg.norm(u64)
+    # ~16-bit operands: the state (energy ~178 at p0 = 1/(gamma M^2)) carries
+    # a few 1e-6 relative error into every product of a stage
+    assert 1e-12 < err < 1e-5, err
+    op.set_state(u0)
+    op.advance(2, 1e-3, gemm_precision=2)
+    err6 = np.linalg.norm(op.get_state() - u64) / np.linalg.norm(u64)
+    assert err6 < 1e-7 and err6 < err / 10, (err6, err)
