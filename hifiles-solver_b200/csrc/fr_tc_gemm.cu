@@ -309,10 +309,15 @@ fr_status gemm_bf16x3(int m, int k, long long ncols, const double* A, const doub
     g_err = cudaGetErrorString(e);
     return FR_ERR_CUDA;
   }
-  int dev = 0, sms = 0, per = 0;
+  cudaFuncSetAttribute(kfn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  int dev = 0, sms = 0, per = 0, smem_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kfn, kThreads, smem);
+  // blocks that fit by shared memory (1 kB static and 1 kB reserved per block)
+  const int by_smem = smem_sm > 0 ? (int)((size_t)smem_sm / (smem + 2048)) : 1;
+  if (by_smem > per) per = by_smem;
   const long long ntiles = (ncols + kTN - 1) / kTN;
   long long grid = (long long)(per > 0 ? per : 1) * (sms > 0 ? sms : 1);
   if (grid > ntiles) grid = ntiles;

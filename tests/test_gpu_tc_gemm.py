@@ -47,7 +47,7 @@ def _product(L, A, B, mode):
 
 
 @pytest.mark.parametrize("m,k,n", [(96, 64, 5 * 1000 + 3), (64, 96, 777), (128, 128, 64 * 40), (16, 16, 100),
-                                   (1, 1, 5), (64, 64, 64)])
+                                   (1, 1, 5), (64, 64, 64), (96, 64, 5 * 32 ** 3)])
 def test_bf16x3_product_against_fp64(m, k, n):
     rng = np.random.default_rng(7 + m + k)
     A = rng.standard_normal((m, k))
