@@ -250,6 +250,40 @@ def measure_forms(a, dev, fp64_value, s64, u0):
     out["batch"] = ("%d periodic TGV instances (NS, Mach 0.1, Re 1600), sizes n^3 with n in [8, 24] and P in "
                     "[2, 4] drawn with seed %d; DOF-updates per RK stage over all instances" % (BATCH_N, BATCH_SEED))
     out["operator_path"] = measure_operator_path(a, dev, s64, u0)
+    out["tgv64_p4"] = measure_tgv64_p4(dev)
+    return out
+
+
+def measure_tgv64_p4(dev, n=64, P=4, steps=100, dt=2e-4):
+    """The precision sweep on TGV 64^3 hexes at P = 4 (32.8 M points x 5
+    fields, 1.3 GB per FP64 state): FP64 and FP32 forms of the fused path,
+    DOF-updates/s, and the L2 error of FP32 against FP64 after 100 steps."""
+    import torch
+    import hifiles_b200 as H
+    L = 2 * np.pi
+    kw = dict(viscous=True, vcjh_scheme=1, gamma=GAMMA, prandtl=PR, mu_inf=1.0 / RE, rt_inf=1.0, c_sth=1.0,
+              fix_vis=1.0, tau=1.0, pen_fact=0.5, device=dev)
+    out, states = {}, {}
+    for prec, name in ((0, "fp64"), (1, "fp32")):
+        s = H.Solver.box(3, P, (n, n, n), (0, 0, 0), (L, L, L), precision=prec, **kw)
+        u0 = tgv_state(s.geometry()["pos_upts"])
+        s.set_state(u0)
+        s.autotune(3)
+        st = torch.cuda.ExternalStream(s.stream(), device=dev)
+        s.advance(3, dt)
+        ms = _time_steps(lambda k: s.advance(k, dt), st, 10)
+        out[name] = {"value": s.n_eles * s.n_upts * s.n_fields * 5 / (ms * 1e-3), "ms_per_step": ms}
+        s.set_state(u0)
+        s.advance(steps, dt)
+        states[name] = s.get_state()
+        s.close()
+        del s
+        torch.cuda.empty_cache()
+    out["fp32"]["ratio_to_fp64"] = out["fp32"]["value"] / out["fp64"]["value"]
+    out["fp32"]["l2_rel_vs_fp64_after_%d_steps" % steps] = float(
+        np.linalg.norm(states["fp32"] - states["fp64"]) / np.linalg.norm(states["fp64"]))
+    out["workload"] = ("TGV %d^3 hex P=%d NS (Re 1600, Mach 0.1), dt %g; BF16 split products need operators up to "
+                       "128 x 128 and P = 4 hexes have 150 x 125, so this size has no tensor-core row" % (n, P, dt))
     return out
 
 
