@@ -282,8 +282,33 @@ def measure_tgv64_p4(dev, n=64, P=4, steps=100, dt=2e-4):
     out["fp32"]["ratio_to_fp64"] = out["fp32"]["value"] / out["fp64"]["value"]
     out["fp32"]["l2_rel_vs_fp64_after_%d_steps" % steps] = float(
         np.linalg.norm(states["fp32"] - states["fp64"]) / np.linalg.norm(states["fp64"]))
-    out["workload"] = ("TGV %d^3 hex P=%d NS (Re 1600, Mach 0.1), dt %g; BF16 split products need operators up to "
-                       "128 x 128 and P = 4 hexes have 150 x 125, so this size has no tensor-core row" % (n, P, dt))
+    del states
+    # BF16x3 operator products on the tensor cores, through the per-operator path
+    from hifiles_b200 import seam
+    s = H.Solver.box(3, P, (n, n, n), (0, 0, 0), (L, L, L), precision=0, **kw)
+    u0 = tgv_state(s.geometry()["pos_upts"])
+    phys = dict(gamma=GAMMA, prandtl=PR, mu_inf=1.0 / RE, rt_inf=1.0, c_sth=1.0, fix_vis=1.0, tau=1.0, pen_fact=0.5)
+    op = seam.OperatorStage(s, phys, P, vcjh_scheme=1)
+    op.set_state(u0)
+    op.advance(1, dt, gemm_precision=1)
+    ms = _time_steps(lambda k: op.advance(k, dt, gemm_precision=1), op.stream, 2)
+    nb = 20
+    op.set_state(u0)
+    op.advance(nb, dt, gemm_precision=1)
+    u_tc = op.get_state()
+    del op
+    torch.cuda.empty_cache()
+    s.set_state(u0)
+    s.advance(nb, dt)
+    u_ref = s.get_state()
+    s.close()
+    out["bf16x3_operator_path"] = {"value": s.n_eles * s.n_upts * s.n_fields * 5 / (ms * 1e-3), "ms_per_step": ms,
+                                   "l2_rel_vs_fp64_after_%d_steps" % nb:
+                                   float(np.linalg.norm(u_tc - u_ref) / np.linalg.norm(u_ref))}
+    out["workload"] = ("TGV %d^3 hex P=%d NS (Re 1600, Mach 0.1), dt %g; fused path in FP64 and FP32; BF16x3 "
+                       "split operator products on the tensor cores through the per-operator path (its P = 4 "
+                       "operators, up to 150 x 150, take two 128-row MMA tiles); BF16x6 does not fit one block's "
+                       "shared memory at P = 4" % (n, P, dt))
     return out
 
 

@@ -10,15 +10,18 @@
 // level).  Either is one GEMM over K' = TERMS KP:
 //   BF16x3:  A' = [A0 | A0 | A1],            B' = [B0 ; B1 ; B0]
 //   BF16x6:  A' = [A0 | A0 | A1 | A0 | A1 | A2],  B' = [B0 ; B1 ; B0 ; B2 ; B1 ; B0]
-// KP is k rounded up to 16 (zeros), M = 128 rows (m <= 128, zero rows), N = 64
-// columns per tile.  Inputs and outputs stay FP64 in HBM.
+// KP is k rounded up to 16 (zeros); MT = 1 or 2 MMA tiles of 128 rows cover
+// the operator's m <= 256 rows (zero rows beyond m); TN = 64 or 32 columns
+// per tile, the larger that fits shared memory.  Inputs and outputs stay FP64
+// in HBM.
 //
 // One block of 128 threads per tile pass, persistent over column tiles:
 // the threads stage A' once and B' per tile into shared memory in the
 // K-major, no-swizzle canonical layout (8 x 16-byte core matrices), one
-// thread issues the K'/16 tcgen05.mma instructions into a TMEM accumulator
-// (128 lanes x 64 columns) and commits them to an mbarrier; the four warps
-// read their 32 lanes back with tcgen05.ld and write C.  Every mbarrier wait
+// thread issues the MT K'/16 tcgen05.mma instructions into MT TMEM
+// accumulators (128 lanes x TN columns each) and commits them to an
+// mbarrier; the four warps read their 32 lanes of each back with tcgen05.ld
+// and write C.  Every mbarrier wait
 // is bounded: on expiry the kernel sets the error flag, waits once more
 // (bounded) for its MMAs, frees its TMEM and returns.
 #include <cuda_runtime.h>
@@ -34,10 +37,9 @@ extern thread_local std::string g_err;
 
 namespace {
 
-constexpr int kTM = 128;          // rows of the MMA tile (operator rows, zero-padded)
-constexpr int kTN = 64;           // columns per tile
+constexpr int kTM = 128;          // rows of one MMA tile (operator rows, zero-padded)
 constexpr int kThreads = 128;
-constexpr uint32_t kTmemCols = 64;
+constexpr uint32_t kTmemCols = 64;    // MT x TN accumulator columns (64 in both shapes)
 constexpr long long kWaitLimit = 1LL << 20;   // x 1 us suspend hint: about a second
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -52,11 +54,16 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint3
 
 // instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
 // K-major, N >> 3 at bit 17, M >> 4 at bit 24
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTN >> 3) << 17) |
-                            ((uint32_t)(kTM >> 4) << 24);
+template <int TN>
+__host__ __device__ constexpr uint32_t idesc_bf16()
+{
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(kTM >> 4) << 24);
+}
 
+template <int TN>
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate)
 {
+  constexpr uint32_t kIdesc = idesc_bf16<TN>();
   asm volatile(
       "{\n\t"
       ".reg .pred p;\n\t"
@@ -154,16 +161,18 @@ __device__ __forceinline__ uint32_t chunk_off(int row, int kc, int R)
   return (uint32_t)((kc * (R / 8) + row / 8) * 128 + (row % 8) * 16);
 }
 
-template <int TERMS>
+template <int TERMS, int MT, int TN>
 __global__ void __launch_bounds__(kThreads)
 fr_gemm_bf16x3_kernel(int m, int k, int KP, long long ncols, const double* __restrict__ A,
                       const double* __restrict__ B, double* __restrict__ C, int beta, int* __restrict__ err)
 {
+  static_assert(MT * TN == (int)kTmemCols, "accumulator columns");
+  constexpr int RA = MT * kTM;             // rows of A'
   extern __shared__ __align__(1024) unsigned char sm[];
   const int KC = KP / 8;                   // 16-byte chunks of one copy of K
   const int KQ = TERMS * KC;               // chunks of K'
-  unsigned char* sA = sm;                  // kTM x K' bf16
-  unsigned char* sB = sm + (size_t)kTM * KQ * 16;   // kTN x K' bf16
+  unsigned char* sA = sm;                  // RA x K' bf16 (MT tiles of kTM rows)
+  unsigned char* sB = sm + (size_t)RA * KQ * 16;    // TN x K' bf16
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tmem_slot;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -177,9 +186,9 @@ fr_gemm_bf16x3_kernel(int m, int k, int KP, long long ncols, const double* __res
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar)));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  // A' once: rows r (fastest) x chunks c of A
-  for (int w = tid; w < kTM * KC; w += kThreads) {
-    const int r = w % kTM, c = w / kTM;
+  // A' once: rows r (fastest) x chunks c of A; tile mt holds rows 128 mt ..
+  for (int w = tid; w < RA * KC; w += kThreads) {
+    const int r = w % RA, c = w / RA, mt = r / kTM, rr = r % kTM;
     double x[8];
 #pragma unroll
     for (int i = 0; i < 8; i++) {
@@ -188,20 +197,21 @@ fr_gemm_bf16x3_kernel(int m, int k, int KP, long long ncols, const double* __res
     }
     uint4 q[3];
     split8(x, q);
+    unsigned char* tA = sA + (size_t)mt * kTM * KQ * 16;
 #pragma unroll
-    for (int j = 0; j < TERMS; j++) *reinterpret_cast<uint4*>(sA + chunk_off(r, j * KC + c, kTM)) = q[part_of<TERMS>(j, 1)];
+    for (int j = 0; j < TERMS; j++) *reinterpret_cast<uint4*>(tA + chunk_off(rr, j * KC + c, kTM)) = q[part_of<TERMS>(j, 1)];
   }
   fence_before();
   __syncthreads();
   fence_after();
   const uint32_t tmem = tmem_slot;
-  const long long ntiles = (ncols + kTN - 1) / kTN;
+  const long long ntiles = (ncols + TN - 1) / TN;
   uint32_t parity = 0;
   for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const long long j0 = t * kTN;
+    const long long j0 = t * TN;
     // B' for columns j0 ..: columns n (fastest) x chunks c
-    for (int w = tid; w < kTN * KC; w += kThreads) {
-      const int n = w % kTN, c = w / kTN;
+    for (int w = tid; w < TN * KC; w += kThreads) {
+      const int n = w % TN, c = w / TN;
       const long long j = j0 + n;
       double x[8];
 #pragma unroll
@@ -213,7 +223,7 @@ fr_gemm_bf16x3_kernel(int m, int k, int KP, long long ncols, const double* __res
       split8(x, q);
 #pragma unroll
       for (int jj = 0; jj < TERMS; jj++)
-        *reinterpret_cast<uint4*>(sB + chunk_off(n, jj * KC + c, kTN)) = q[part_of<TERMS>(jj, 0)];
+        *reinterpret_cast<uint4*>(sB + chunk_off(n, jj * KC + c, TN)) = q[part_of<TERMS>(jj, 0)];
     }
     // generic-proxy writes -> visible to the tensor cores' reads
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -221,11 +231,15 @@ fr_gemm_bf16x3_kernel(int m, int k, int KP, long long ncols, const double* __res
     __syncthreads();
     fence_after();
     if (tid == 0) {
-      const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+      const uint32_t b0 = smem_u32(sB);
       for (int s = 0; s < KQ / 2; s++) {
-        const uint64_t ad = umma_desc(a0 + (uint32_t)(2 * s) * (kTM / 8) * 128, (kTM / 8) * 128, 128);
-        const uint64_t bd = umma_desc(b0 + (uint32_t)(2 * s) * (kTN / 8) * 128, (kTN / 8) * 128, 128);
-        mma_bf16(tmem, ad, bd, s > 0 ? 1u : 0u);
+        const uint64_t bd = umma_desc(b0 + (uint32_t)(2 * s) * (TN / 8) * 128, (TN / 8) * 128, 128);
+#pragma unroll
+        for (int mt = 0; mt < MT; mt++) {
+          const uint32_t a0 = smem_u32(sA + (size_t)mt * kTM * KQ * 16);
+          const uint64_t ad = umma_desc(a0 + (uint32_t)(2 * s) * (kTM / 8) * 128, (kTM / 8) * 128, 128);
+          mma_bf16<TN>(tmem + (uint32_t)(mt * TN), ad, bd, s > 0 ? 1u : 0u);
+        }
       }
       mma_commit(&bar);
     }
@@ -237,19 +251,22 @@ fr_gemm_bf16x3_kernel(int m, int k, int KP, long long ncols, const double* __res
     }
     parity ^= 1u;
     fence_after();
-    // accumulator rows 32 warp .. +31 -> C
-    const int r = 32 * warp + lane;
+    // accumulator mt, lanes 32 warp .. +31 -> rows 128 mt + 32 warp + lane of C
 #pragma unroll
-    for (int h = 0; h < kTN / 32; h++) {
-      float v[32];
-      tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(32 * h), v);
-      if (r < m) {
+    for (int mt = 0; mt < MT; mt++) {
+      const int r = mt * kTM + 32 * warp + lane;
 #pragma unroll
-        for (int i = 0; i < 32; i++) {
-          const long long j = j0 + 32 * h + i;
-          if (j < ncols) {
-            double* c = C + r + (size_t)m * j;
-            *c = beta ? *c + (double)v[i] : (double)v[i];
+      for (int h = 0; h < TN / 32; h++) {
+        float v[32];
+        tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(mt * TN + 32 * h), v);
+        if (r < m) {
+#pragma unroll
+          for (int i = 0; i < 32; i++) {
+            const long long j = j0 + 32 * h + i;
+            if (j < ncols) {
+              double* c = C + r + (size_t)m * j;
+              *c = beta ? *c + (double)v[i] : (double)v[i];
+            }
           }
         }
       }
@@ -268,42 +285,37 @@ int* g_gemm_err = nullptr;
 
 }  // namespace
 
-// Shared memory of one block: the A' and B' tiles.
-static size_t gemm_split_smem(int k, int terms)
+// Shared memory of one block: the A' tiles (mt of 128 rows) and the B' tile.
+static size_t gemm_split_smem(int k, int terms, int mt, int tn)
 {
   const int KP = (k + 15) / 16 * 16;
-  return (size_t)(kTM + kTN) * terms * KP * 2;
+  return (size_t)(mt * kTM + tn) * terms * KP * 2;
 }
 
-// terms = 3 (BF16x3): operators up to 128 x 128; terms = 6 (BF16x6): up to 128 x 96
+// dynamic shared memory a block may use (227 kB less the 1 kB static part)
+static constexpr size_t kSmemMax = 232448 - 1024;
+
+// tile shape for an m x k operator: {MT, TN}, or {0, 0} when none fits
+static void gemm_split_shape(int m, int k, int terms, int& mt, int& tn)
+{
+  mt = m <= kTM ? 1 : (m <= 2 * kTM ? 2 : 0);
+  tn = mt == 1 ? 64 : 32;
+  if (mt == 0 || k < 1 || gemm_split_smem(k, terms, mt, tn) > kSmemMax) mt = tn = 0;
+}
+
 bool gemm_split_supported(int m, int k, int terms)
 {
-  return m >= 1 && m <= kTM && k >= 1 && k <= (terms == 6 ? 96 : 128);
+  int mt, tn;
+  gemm_split_shape(m, k, terms, mt, tn);
+  return m >= 1 && mt > 0;
 }
 
-fr_status gemm_bf16x3(int m, int k, long long ncols, const double* A, const double* B, double* C, int beta,
-                      cudaStream_t s, int terms)
+template <int TERMS, int MT, int TN>
+static fr_status launch_split(int m, int k, long long ncols, const double* A, const double* B, double* C, int beta,
+                              cudaStream_t s)
 {
-  if (terms != 3 && terms != 6) {
-    g_err = "split products have 3 or 6 terms";
-    return FR_ERR_ARG;
-  }
-  if (!gemm_split_supported(m, k, terms)) {
-    g_err = terms == 6 ? "BF16x6 operator product: operators up to 128 x 96"
-                       : "BF16x3 operator product: operators up to 128 x 128";
-    return FR_ERR_UNSUPPORTED;
-  }
-  if (ncols == 0) return FR_OK;
-  if (!g_gemm_err) {
-    cudaError_t e = cudaMalloc(&g_gemm_err, sizeof(int));
-    if (e == cudaSuccess) e = cudaMemset(g_gemm_err, 0, sizeof(int));
-    if (e != cudaSuccess) {
-      g_err = cudaGetErrorString(e);
-      return FR_ERR_CUDA;
-    }
-  }
-  const size_t smem = gemm_split_smem(k, terms);
-  const void* kfn = terms == 6 ? (const void*)fr_gemm_bf16x3_kernel<6> : (const void*)fr_gemm_bf16x3_kernel<3>;
+  const size_t smem = gemm_split_smem(k, TERMS, MT, TN);
+  const void* kfn = (const void*)fr_gemm_bf16x3_kernel<TERMS, MT, TN>;
   cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) {
     g_err = cudaGetErrorString(e);
@@ -318,21 +330,47 @@ fr_status gemm_bf16x3(int m, int k, long long ncols, const double* A, const doub
   // blocks that fit by shared memory (1 kB static and 1 kB reserved per block)
   const int by_smem = smem_sm > 0 ? (int)((size_t)smem_sm / (smem + 2048)) : 1;
   if (by_smem > per) per = by_smem;
-  const long long ntiles = (ncols + kTN - 1) / kTN;
+  const long long ntiles = (ncols + TN - 1) / TN;
   long long grid = (long long)(per > 0 ? per : 1) * (sms > 0 ? sms : 1);
   if (grid > ntiles) grid = ntiles;
-  if (terms == 6)
-    fr_gemm_bf16x3_kernel<6><<<(unsigned)grid, kThreads, smem, s>>>(m, k, (k + 15) / 16 * 16, ncols, A, B, C, beta,
-                                                                     g_gemm_err);
-  else
-    fr_gemm_bf16x3_kernel<3><<<(unsigned)grid, kThreads, smem, s>>>(m, k, (k + 15) / 16 * 16, ncols, A, B, C, beta,
-                                                                     g_gemm_err);
+  fr_gemm_bf16x3_kernel<TERMS, MT, TN><<<(unsigned)grid, kThreads, smem, s>>>(m, k, (k + 15) / 16 * 16, ncols, A, B,
+                                                                              C, beta, g_gemm_err);
   e = cudaGetLastError();
   if (e != cudaSuccess) {
     g_err = std::string("fr_gemm_bf16x3_kernel: ") + cudaGetErrorString(e);
     return FR_ERR_CUDA;
   }
   return FR_OK;
+}
+
+fr_status gemm_bf16x3(int m, int k, long long ncols, const double* A, const double* B, double* C, int beta,
+                      cudaStream_t s, int terms)
+{
+  if (terms != 3 && terms != 6) {
+    g_err = "split products have 3 or 6 terms";
+    return FR_ERR_ARG;
+  }
+  int mt, tn;
+  gemm_split_shape(m, k, terms, mt, tn);
+  if (m < 1 || mt == 0) {
+    g_err = std::string(terms == 6 ? "BF16x6" : "BF16x3") + " operator product: " + std::to_string(m) + " x " +
+            std::to_string(k) + " does not fit one block's shared memory";
+    return FR_ERR_UNSUPPORTED;
+  }
+  if (ncols == 0) return FR_OK;
+  if (!g_gemm_err) {
+    cudaError_t e = cudaMalloc(&g_gemm_err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(g_gemm_err, 0, sizeof(int));
+    if (e != cudaSuccess) {
+      g_err = cudaGetErrorString(e);
+      return FR_ERR_CUDA;
+    }
+  }
+  if (terms == 3)
+    return mt == 1 ? launch_split<3, 1, 64>(m, k, ncols, A, B, C, beta, s)
+                   : launch_split<3, 2, 32>(m, k, ncols, A, B, C, beta, s);
+  return mt == 1 ? launch_split<6, 1, 64>(m, k, ncols, A, B, C, beta, s)
+                 : launch_split<6, 2, 32>(m, k, ncols, A, B, C, beta, s);
 }
 
 // FR_ERR_TIMEOUT if a tensor-core product gave up waiting for its MMAs since

@@ -47,7 +47,8 @@ def _product(L, A, B, mode):
 
 
 @pytest.mark.parametrize("m,k,n", [(96, 64, 5 * 1000 + 3), (64, 96, 777), (128, 128, 64 * 40), (16, 16, 100),
-                                   (1, 1, 5), (64, 64, 64), (96, 64, 5 * 32 ** 3)])
+                                   (1, 1, 5), (64, 64, 64), (96, 64, 5 * 32 ** 3), (150, 125, 5 * 200 + 7),
+                                   (125, 150, 333), (256, 128, 96)])
 def test_bf16x3_product_against_fp64(m, k, n):
     rng = np.random.default_rng(7 + m + k)
     A = rng.standard_normal((m, k))
@@ -60,7 +61,7 @@ def test_bf16x3_product_against_fp64(m, k, n):
     err = np.linalg.norm(c3 - ref) / np.linalg.norm(ref)
     # x0 + x1 keeps ~16 bits of each operand: a few 1e-6 relative
     assert 1e-9 < err < 3e-5, err
-    if k <= 96:
+    if (m <= 128 and k <= 96) or k <= 64:
         c6 = _product(L, A, B, 2)
         err6 = np.linalg.norm(c6 - ref) / np.linalg.norm(ref)
         # x0 + x1 + x2 keeps ~24 bits; the FP32 accumulation over the 6 k
@@ -89,25 +90,18 @@ def test_bf16x3_accumulates_into_c():
     assert np.linalg.norm(out - ref) / np.linalg.norm(ref) < 3e-5
 
 
-def test_bf16x3_rejects_operators_beyond_one_tile():
+def test_split_products_reject_operators_beyond_shared_memory():
     L = _lib()
-    A = np.ones((150, 125))
-    B = np.ones((125, 10))
-    dA, dB = _dev(A), _dev(B)
-    dC = torch.zeros(150 * 10, dtype=torch.float64, device="cuda")
-    assert L.fr_op_set_gemm_precision(1) == 0
-    try:
-        st = L.fr_op_extrapolate_solution(150, 125, 1, 10, dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), None)
-    finally:
-        L.fr_op_set_gemm_precision(0)
-    assert st == 5
-    dB2 = _dev(np.ones((100, 10)))
-    assert L.fr_op_set_gemm_precision(2) == 0
-    try:
-        st = L.fr_op_extrapolate_solution(64, 100, 1, 10, dA.data_ptr(), dB2.data_ptr(), dC.data_ptr(), None)
-    finally:
-        L.fr_op_set_gemm_precision(0)
-    assert st == 5
+    big = torch.zeros(300 * 300, dtype=torch.float64, device="cuda")
+    col = torch.zeros(300 * 10, dtype=torch.float64, device="cuda")
+    out = torch.zeros(300 * 10, dtype=torch.float64, device="cuda")
+    for mode, (m, k) in ((1, (300, 64)), (1, (200, 160)), (2, (150, 125)), (2, (64, 100))):
+        assert L.fr_op_set_gemm_precision(mode) == 0
+        try:
+            st = L.fr_op_extrapolate_solution(m, k, 1, 10, big.data_ptr(), col.data_ptr(), out.data_ptr(), None)
+        finally:
+            L.fr_op_set_gemm_precision(0)
+        assert st == 5, (mode, m, k)
     assert L.fr_op_set_gemm_precision(3) == 1
 
 
