@@ -205,8 +205,8 @@ __device__ __forceinline__ T interp_code(const Line<T>& L, int c, const S* s)
 }
 
 // Dynamic shared-memory sizes of the stage kernels.
-template <int DIM, int P> struct GradPlan;
-template <int DIM, int P, int EPB, typename TC, int LES = 0>
+template <int DIM, int P, bool ALIAS> struct GradPlan;
+template <int DIM, int P, int EPB, typename TC, int LES = 0, bool ALIAS = false>
 __host__ __device__ constexpr size_t grad_smem_bytes();
 template <int DIM, int P, int EPB, int NT, int VISC, int MODE, typename TC> struct UpdPlan;
 template <int DIM, int P, int EPB, int NT, int VISC, int MODE, typename TC>
@@ -359,25 +359,42 @@ __host__ __device__ constexpr size_t grad_side_bytes()
 //   sS  [(F-1)*D][NU] transformed SGS flux (LES only)
 // Every region size is rounded up to 4 words, so each region, and each
 // element's block, starts on a 16-byte boundary whatever the point counts.
-template <int DIM, int P>
+// With ALIAS the transformed flux sFl takes the place of sX and the metrics
+// (both dead once every thread has finished its solution-point reads; the
+// kernel puts a barrier there) and the left normals go to sU (dead after the
+// solution-point phase): 25 % less shared memory per element.  oN is where
+// the left normals [D][NF] live for the flux-point phase.
+template <int DIM, int P, bool ALIAS>
 struct GradPlan {
   using S = Shape<DIM, P>;
   __host__ __device__ static constexpr int r4(int n) { return (n + 3) / 4 * 4; }
-  static constexpr int R3N = (DIM * DIM + 1) * S::NU > DIM * S::NF ? (DIM * DIM + 1) * S::NU : DIM * S::NF;
+  static constexpr int NM = (DIM * DIM + 1) * S::NU;        // metrics
+  static constexpr int R3N = ALIAS ? NM : (NM > DIM * S::NF ? NM : DIM * S::NF);
   static constexpr int oX = r4(S::F * S::NU);
-  static constexpr int oUf = oX + r4(S::F * S::NF);
-  static constexpr int oM = oUf + r4(S::F * S::NF);
-  static constexpr int oG = oM + r4(R3N);
-  static constexpr int oFl = oG + r4(S::F * DIM * S::NU);
-  static constexpr int oS = oFl + r4(S::F * DIM * S::NU);
+  static constexpr int oUf = ALIAS ? oX + r4(S::F * S::NF) + r4(R3N) : oX + r4(S::F * S::NF);
+  static constexpr int oM = ALIAS ? oX + r4(S::F * S::NF) : oUf + r4(S::F * S::NF);
+  static constexpr int oG = ALIAS ? oUf + r4(S::F * S::NF) : oM + r4(R3N);
+  static constexpr int oFl = ALIAS ? oX : oG + r4(S::F * DIM * S::NU);
+  static constexpr int oS = ALIAS ? oG + r4(S::F * DIM * S::NU) : oFl + r4(S::F * DIM * S::NU);
+  static constexpr int oN = ALIAS ? 0 : oM;
+  static_assert(!ALIAS || (S::F * DIM * S::NU <= oUf - oX && DIM * S::NF <= oX), "aliased regions too small");
   __host__ __device__ static constexpr int size(int les) { return oS + (les ? r4((S::F - 1) * DIM * S::NU) : 0); }
 };
 
-template <int DIM, int P, int EPB, typename TC, int LES>
+template <int DIM, int P, int EPB, typename TC, int LES, bool ALIAS>
 __host__ __device__ constexpr size_t grad_smem_bytes()
 {
   return blockops_bytes<TC, Shape<DIM, P>::NF>() + grad_side_bytes<EPB, Shape<DIM, P>::NF>() +
-         sizeof(TC) * EPB * GradPlan<DIM, P>::size(LES);
+         sizeof(TC) * EPB * GradPlan<DIM, P, ALIAS>::size(LES);
+}
+
+// Whether an instantiation of fr_grad_kernel uses the aliased shared-memory
+// plan: the FP64 hex P = 3 layout, no LES, not persistent, one solution
+// point per thread (the in-phase barrier needs every thread's reads done).
+template <int DIM, int P, int EPB, int NT, typename TC, int LES, int PERS>
+__host__ __device__ constexpr bool grad_alias()
+{
+  return swz_on<DIM, P, TC>() && LES == 0 && PERS == 0 && Items<NT, EPB * Shape<DIM, P>::NU>::N == 1;
 }
 
 // Viscous stage, part 1 (per element):
@@ -416,7 +433,8 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
                long long E, Line<TC> L, PhysT<TC> ph, TC* __restrict__ GRAD, TC* __restrict__ BV)
 {
   using S = Shape<DIM, P>;
-  using G = GradPlan<DIM, P>;
+  constexpr bool ALIAS = grad_alias<DIM, P, EPB, NT, TC, LES, PERS>();
+  using G = GradPlan<DIM, P, ALIAS>;
   constexpr int NU = S::NU, NF = S::NF, F = S::F, D = DIM, DD = DIM * DIM;
   constexpr int IF = Items<NT, EPB * NF>::N, IU = Items<NT, EPB * NU>::N;
   constexpr int PE = G::size(LES);      // shared TC words per element
@@ -431,6 +449,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
 #define FR_SG(el, c, u) sm[(el) * PE + G::oG + (c) * NU + (u)]
 #define FR_SFL(el, l, k, u) sm[(el) * PE + G::oFl + ((l) * F + (k)) * NU + (u)]
 #define FR_SS(el, c, u) sm[(el) * PE + G::oS + (c) * NU + (u)]
+#define FR_SN(el, i) sm[(el) * PE + G::oN + (i)]
   fill_blockops<DIM, P, TC, NF>(B, L, threadIdx.x, NT);
   const long long NFE = (long long)NF * E;
   const long long nblk = (E + EPB - 1) / EPB;
@@ -569,7 +588,9 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
 #pragma unroll
   for (int it = 0; it < IU; it++) {
     int w = threadIdx.x + it * NT, el = w / NU, u = w - el * NU;
-    if (w >= EPB * NU || el >= nval) continue;
+    const bool valid = w < EPB * NU && el < nval;
+    if (!ALIAS && !valid) continue;
+    if (!valid) el = u = 0;                  // reads in bounds, results unused
     int abc[3];
     upt_abc<DIM, P>(u, abc[0], abc[1], abc[2]);
     TC gr[F][D];
@@ -623,13 +644,20 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
         TC acc = fr_fma(gr[k][1], m1, gr[k][0] * m0);
         if (D == 3) acc = fr_fma(gr[k][2], m2, acc);
         gp[k][c] = acc;
-        FR_SG(el, k + F * c, su) = acc;
-        if (GRAD) GRAD[u + (size_t)NU * (e0 + el + E * (k + (long long)F * c))] = acc;
+        if (valid) {
+          FR_SG(el, k + F * c, su) = acc;
+          if (GRAD) GRAD[u + (size_t)NU * (e0 + el + E * (k + (long long)F * c))] = acc;
+        }
       }
     }
     TC q[F];
 #pragma unroll
     for (int k = 0; k < F; k++) q[k] = FR_SU(el, k, su);
+    if constexpr (ALIAS) {
+      // sFl overwrites the neighbour traces and metrics: every thread's reads first
+      __syncthreads();
+      if (!valid) continue;
+    }
     TC fi[F][D], fv[F][D];
     inv_flux<D, TC>(ph, q, fi);
     vis_flux_fast<D, TC>(ph, q, gp, fv);
@@ -677,7 +705,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
   if (!PERS)
     for (int w = threadIdx.x; w < nval * D * NF; w += NT) {
       int el = w / (D * NF), r = w - el * D * NF, d = r / NF, f = r - d * NF;
-      cp_async<sizeof(TC)>(&FR_SM(el, r), nL + f + (size_t)NF * (e0 + el) + NFE * d);
+      cp_async<sizeof(TC)>(&FR_SN(el, r), nL + f + (size_t)NF * (e0 + el) + NFE * d);
     }
   cp_async_commit();
 
@@ -777,7 +805,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
 #pragma unroll
         for (int k = 0; k < F; k++) uf[k] = FR_SUF(el, k, f);
 #pragma unroll
-        for (int d = 0; d < D; d++) n[d] = PERS ? nL[own + NFE * d] : FR_SM(el, d * NF + f);
+        for (int d = 0; d < D; d++) n[d] = PERS ? nL[own + NFE * d] : FR_SN(el, d * NF + f);
         const int btype = sSide[el * NF + f] >> 2;
         if constexpr (LES == 0) {
           // the projection is accumulated as the flux is formed (no full flux held)
@@ -877,7 +905,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
         }
       }
 #pragma unroll
-      for (int d = 0; d < D; d++) n[d] = PERS ? nL[own + NFE * d] : FR_SM(el, d * NF + f);
+      for (int d = 0; d < D; d++) n[d] = PERS ? nL[own + NFE * d] : FR_SN(el, d * NF + f);
       const int btype = psd[it] >> 2;
       if constexpr (LES == 0) {
         // the projection is accumulated as the flux is formed (no full flux held)
@@ -951,6 +979,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
 #undef FR_SG
 #undef FR_SFL
 #undef FR_SS
+#undef FR_SN
 }
 
 // Boundary point j of the interface kernel (flat own index bf[j], type

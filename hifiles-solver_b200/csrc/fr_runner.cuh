@@ -151,7 +151,7 @@ struct RunnerT : Runner {
       constexpr int EPB = Tiles<DIM, P>::grad[I].epb, NT = Tiles<DIM, P>::grad[I].nt;
       constexpr int MINB = Tiles<DIM, P>::grad[I].minb > 0 ? Tiles<DIM, P>::grad[I].minb : 1;
       constexpr int PERS = Tiles<DIM, P>::grad[I].pers;
-      constexpr size_t sm = grad_smem_bytes<DIM, P, EPB, TC, LES>();
+      constexpr size_t sm = grad_smem_bytes<DIM, P, EPB, TC, LES, grad_alias<DIM, P, EPB, NT, TC, LES, PERS>()>();
       const void* kfn = (const void*)fr_grad_kernel<DIM, P, EPB, NT, TC, LES, MINB, 1, PERS>;
       static bool once = (set_smem(kfn, sm), true);
       (void)once;
