@@ -1058,14 +1058,42 @@ fr_face_kernel(const int2* __restrict__ face, const unsigned char* __restrict__ 
     if (i - nint < nbdy) face_boundary<DIM, VISC, TC, RIEMANN>(ph, i - nint, UF, nL, tdA, CF, NFE, bf, bt, BV);
     return;
   }
+  // FP64: the point's inputs reach shared memory through cp.async (one
+  // column per thread, field-major: no bank conflicts, no barrier), so they
+  // are all in flight at once without holding registers; FP32 reads them
+  // directly
+  constexpr bool STAGE = sizeof(TC) == 8;
+  constexpr int NV = 2 * F + D + 2 + (VISC ? 2 * (F - 1) : 0);
+  __shared__ TC sv[STAGE ? NV : 1][STAGE ? 128 : 1];
+  const int t = threadIdx.x;
   const int2 lr = face[i];
   const long long a = lr.x, b = lr.y;
+  auto in = [&](int j, const TC* src) -> TC { return STAGE ? sv[j][t] : *src; };
+  if constexpr (STAGE) {
+    int j = 0;
+#pragma unroll
+    for (int k = 0; k < F; k++) cp_async<sizeof(TC)>(&sv[j++][t], UF + a + NFE * k);
+#pragma unroll
+    for (int k = 0; k < F; k++) cp_async<sizeof(TC)>(&sv[j++][t], UF + b + NFE * k);
+#pragma unroll
+    for (int d = 0; d < D; d++) cp_async<sizeof(TC)>(&sv[j++][t], nL + a + NFE * d);
+    cp_async<sizeof(TC)>(&sv[j++][t], tdA + a);
+    cp_async<sizeof(TC)>(&sv[j++][t], tdA + b);
+    if (VISC) {
+#pragma unroll
+      for (int k = 1; k < F; k++) cp_async<sizeof(TC)>(&sv[j++][t], VF + a + NFE * (k - 1));
+#pragma unroll
+      for (int k = 1; k < F; k++) cp_async<sizeof(TC)>(&sv[j++][t], VF + b + NFE * (k - 1));
+    }
+    cp_async_commit();
+    cp_async_wait_all();
+  }
   TC ul[F], ur[F], n[D];
 #pragma unroll
-  for (int k = 0; k < F; k++) { ul[k] = UF[a + NFE * k]; ur[k] = UF[b + NFE * k]; }
+  for (int k = 0; k < F; k++) { ul[k] = in(k, UF + a + NFE * k); ur[k] = in(F + k, UF + b + NFE * k); }
 #pragma unroll
-  for (int d = 0; d < D; d++) n[d] = nL[a + NFE * d];
-  const TC tl = tdA[a], tr = tdA[b];
+  for (int d = 0; d < D; d++) n[d] = in(2 * F + d, nL + a + NFE * d);
+  const TC tl = in(2 * F + D, tdA + a), tr = in(2 * F + D + 1, tdA + b);
   TC fn[F];
   if constexpr (RIEMANN == 2 && DIM == 2) roe<TC>(ph, ul, ur, n, fn);
   else rusanov<D, TC>(ph, ul, ur, n, fn);
@@ -1079,7 +1107,8 @@ fr_face_kernel(const int2* __restrict__ face, const unsigned char* __restrict__ 
     const TC pen = fsign[i] ? -ph.pen_fact : ph.pen_fact;
 #pragma unroll
     for (int k = 0; k < F; k++) {
-      TC al = k ? VF[a + NFE * (k - 1)] : TC(0), ar = k ? VF[b + NFE * (k - 1)] : TC(0);
+      TC al = k ? in(2 * F + D + 2 + (k - 1), VF + a + NFE * (k - 1)) : TC(0);
+      TC ar = k ? in(2 * F + D + 2 + (F - 1) + (k - 1), VF + b + NFE * (k - 1)) : TC(0);
       TC fv = ldg_normal<TC>(al, ar, ul[k], ur[k], pen, ph.tau, nn);
       cl[k] = cl[k] + fv * tl;
       cr[k] = cr[k] + (-fv) * tr;
