@@ -289,26 +289,27 @@ def measure_tgv64_p4(dev, n=64, P=4, steps=100, dt=2e-4):
     u0 = tgv_state(s.geometry()["pos_upts"])
     phys = dict(gamma=GAMMA, prandtl=PR, mu_inf=1.0 / RE, rt_inf=1.0, c_sth=1.0, fix_vis=1.0, tau=1.0, pen_fact=0.5)
     op = seam.OperatorStage(s, phys, P, vcjh_scheme=1)
-    op.set_state(u0)
-    op.advance(1, dt, gemm_precision=1)
-    ms = _time_steps(lambda k: op.advance(k, dt, gemm_precision=1), op.stream, 2)
     nb = 20
-    op.set_state(u0)
-    op.advance(nb, dt, gemm_precision=1)
-    u_tc = op.get_state()
+    u_tc = {}
+    for mode, name in ((1, "bf16x3_operator_path"), (2, "bf16x6_operator_path")):
+        op.set_state(u0)
+        op.advance(1, dt, gemm_precision=mode)
+        ms = _time_steps(lambda k: op.advance(k, dt, gemm_precision=mode), op.stream, 2)
+        out[name] = {"value": s.n_eles * s.n_upts * s.n_fields * 5 / (ms * 1e-3), "ms_per_step": ms}
+        op.set_state(u0)
+        op.advance(nb, dt, gemm_precision=mode)
+        u_tc[name] = op.get_state()
     del op
     torch.cuda.empty_cache()
     s.set_state(u0)
     s.advance(nb, dt)
     u_ref = s.get_state()
     s.close()
-    out["bf16x3_operator_path"] = {"value": s.n_eles * s.n_upts * s.n_fields * 5 / (ms * 1e-3), "ms_per_step": ms,
-                                   "l2_rel_vs_fp64_after_%d_steps" % nb:
-                                   float(np.linalg.norm(u_tc - u_ref) / np.linalg.norm(u_ref))}
-    out["workload"] = ("TGV %d^3 hex P=%d NS (Re 1600, Mach 0.1), dt %g; fused path in FP64 and FP32; BF16x3 "
-                       "split operator products on the tensor cores through the per-operator path (its P = 4 "
-                       "operators, up to 150 x 150, take two 128-row MMA tiles); BF16x6 does not fit one block's "
-                       "shared memory at P = 4" % (n, P, dt))
+    for name, u in u_tc.items():
+        out[name]["l2_rel_vs_fp64_after_%d_steps" % nb] = float(np.linalg.norm(u - u_ref) / np.linalg.norm(u_ref))
+    out["workload"] = ("TGV %d^3 hex P=%d NS (Re 1600, Mach 0.1), dt %g; fused path in FP64 and FP32; BF16x3 and "
+                       "BF16x6 split operator products on the tensor cores through the per-operator path (its "
+                       "P = 4 operators, up to 150 x 150, take two 128-row MMA tiles)" % (n, P, dt))
     return out
 
 

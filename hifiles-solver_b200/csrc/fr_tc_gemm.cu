@@ -7,9 +7,11 @@
 // Split: x = x0 + x1 + x2 with x0 = bf16(x), x1 = bf16(x - x0),
 // x2 = bf16(x - x0 - x1).  TERMS = 3 (BF16x3) keeps x0y0 + x0y1 + x1y0, about
 // 16 bits; TERMS = 6 (BF16x6) adds x0y2 + x1y1 + x2y0, about 24 bits (FP32
-// level).  Either is one GEMM over K' = TERMS KP:
+// level).  Either is one accumulation over K' = TERMS KP:
 //   BF16x3:  A' = [A0 | A0 | A1],            B' = [B0 ; B1 ; B0]
 //   BF16x6:  A' = [A0 | A0 | A1 | A0 | A1 | A2],  B' = [B0 ; B1 ; B0 ; B2 ; B1 ; B0]
+// Shared memory holds each distinct part once (2 or 3 of A and of B); the
+// descriptors of each K-copy point at its parts.
 // KP is k rounded up to 16 (zeros); MT = 1 or 2 MMA tiles of 128 rows cover
 // the operator's m <= 256 rows (zero rows beyond m); TN = 64 or 32 columns
 // per tile, the larger that fits shared memory.  Inputs and outputs stay FP64
@@ -147,13 +149,15 @@ __device__ __forceinline__ void split8(const double (&x)[8], uint4 (&q)[3])
 }
 
 // part of A' (a = 1) or B' (a = 0) in K-copy j of the split product
-template <int TERMS>
-__device__ __forceinline__ int part_of(int j, int a)
+__host__ __device__ constexpr int part_of(int j, int a)
 {
   // BF16x3: A 0 0 1, B 0 1 0; BF16x6: A 0 0 1 0 1 2, B 0 1 0 2 1 0
   constexpr int PA[6] = {0, 0, 1, 0, 1, 2}, PB[6] = {0, 1, 0, 2, 1, 0};
   return a ? PA[j] : PB[j];
 }
+
+// distinct parts kept of each operand: 2 (BF16x3) or 3 (BF16x6)
+__host__ __device__ constexpr int n_parts(int terms) { return terms == 6 ? 3 : 2; }
 
 // byte offset of 16-byte chunk (row, kchunk) of a K-major tile of R rows
 __device__ __forceinline__ uint32_t chunk_off(int row, int kc, int R)
@@ -168,11 +172,12 @@ fr_gemm_bf16x3_kernel(int m, int k, int KP, long long ncols, const double* __res
 {
   static_assert(MT * TN == (int)kTmemCols, "accumulator columns");
   constexpr int RA = MT * kTM;             // rows of A'
+  constexpr int NP = n_parts(TERMS);
   extern __shared__ __align__(1024) unsigned char sm[];
-  const int KC = KP / 8;                   // 16-byte chunks of one copy of K
-  const int KQ = TERMS * KC;               // chunks of K'
-  unsigned char* sA = sm;                  // RA x K' bf16 (MT tiles of kTM rows)
-  unsigned char* sB = sm + (size_t)RA * KQ * 16;    // TN x K' bf16
+  const int KC = KP / 8;                   // 16-byte chunks of one part (KP values)
+  const size_t tileA = (size_t)kTM * KC * 16, partA = (size_t)MT * tileA, partB = (size_t)TN * KC * 16;
+  unsigned char* sA = sm;                  // NP parts x MT tiles of kTM x KP bf16
+  unsigned char* sB = sm + NP * partA;     // NP parts of TN x KP bf16
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tmem_slot;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -197,9 +202,9 @@ fr_gemm_bf16x3_kernel(int m, int k, int KP, long long ncols, const double* __res
     }
     uint4 q[3];
     split8(x, q);
-    unsigned char* tA = sA + (size_t)mt * kTM * KQ * 16;
 #pragma unroll
-    for (int j = 0; j < TERMS; j++) *reinterpret_cast<uint4*>(tA + chunk_off(rr, j * KC + c, kTM)) = q[part_of<TERMS>(j, 1)];
+    for (int pp = 0; pp < NP; pp++)
+      *reinterpret_cast<uint4*>(sA + pp * partA + mt * tileA + chunk_off(rr, c, kTM)) = q[pp];
   }
   fence_before();
   __syncthreads();
@@ -222,8 +227,7 @@ fr_gemm_bf16x3_kernel(int m, int k, int KP, long long ncols, const double* __res
       uint4 q[3];
       split8(x, q);
 #pragma unroll
-      for (int jj = 0; jj < TERMS; jj++)
-        *reinterpret_cast<uint4*>(sB + chunk_off(n, jj * KC + c, TN)) = q[part_of<TERMS>(jj, 0)];
+      for (int pp = 0; pp < NP; pp++) *reinterpret_cast<uint4*>(sB + pp * partB + chunk_off(n, c, TN)) = q[pp];
     }
     // generic-proxy writes -> visible to the tensor cores' reads
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -231,14 +235,18 @@ fr_gemm_bf16x3_kernel(int m, int k, int KP, long long ncols, const double* __res
     __syncthreads();
     fence_after();
     if (tid == 0) {
-      const uint32_t b0 = smem_u32(sB);
-      for (int s = 0; s < KQ / 2; s++) {
-        const uint64_t bd = umma_desc(b0 + (uint32_t)(2 * s) * (TN / 8) * 128, (TN / 8) * 128, 128);
+      // K-copy j multiplies A part part_of(j, 1) with B part part_of(j, 0)
 #pragma unroll
-        for (int mt = 0; mt < MT; mt++) {
-          const uint32_t a0 = smem_u32(sA + (size_t)mt * kTM * KQ * 16);
-          const uint64_t ad = umma_desc(a0 + (uint32_t)(2 * s) * (kTM / 8) * 128, (kTM / 8) * 128, 128);
-          mma_bf16<TN>(tmem + (uint32_t)(mt * TN), ad, bd, s > 0 ? 1u : 0u);
+      for (int j = 0; j < TERMS; j++) {
+        const uint32_t b0 = smem_u32(sB + part_of(j, 0) * partB);
+        for (int s = 0; s < KC / 2; s++) {
+          const uint64_t bd = umma_desc(b0 + (uint32_t)(2 * s) * (TN / 8) * 128, (TN / 8) * 128, 128);
+#pragma unroll
+          for (int mt = 0; mt < MT; mt++) {
+            const uint32_t a0 = smem_u32(sA + part_of(j, 1) * partA + mt * tileA);
+            const uint64_t ad = umma_desc(a0 + (uint32_t)(2 * s) * (kTM / 8) * 128, (kTM / 8) * 128, 128);
+            mma_bf16<TN>(tmem + (uint32_t)(mt * TN), ad, bd, (j > 0 || s > 0) ? 1u : 0u);
+          }
         }
       }
       mma_commit(&bar);
@@ -285,11 +293,12 @@ int* g_gemm_err = nullptr;
 
 }  // namespace
 
-// Shared memory of one block: the A' tiles (mt of 128 rows) and the B' tile.
+// Shared memory of one block: the distinct parts of A (mt tiles of 128 rows)
+// and of the B tile.
 static size_t gemm_split_smem(int k, int terms, int mt, int tn)
 {
   const int KP = (k + 15) / 16 * 16;
-  return (size_t)(mt * kTM + tn) * terms * KP * 2;
+  return (size_t)(mt * kTM + tn) * n_parts(terms) * KP * 2;
 }
 
 // dynamic shared memory a block may use (227 kB less the 1 kB static part)

@@ -61,12 +61,13 @@ def test_bf16x3_product_against_fp64(m, k, n):
     err = np.linalg.norm(c3 - ref) / np.linalg.norm(ref)
     # x0 + x1 keeps ~16 bits of each operand: a few 1e-6 relative
     assert 1e-9 < err < 3e-5, err
-    if (m <= 128 and k <= 96) or k <= 64:
+    if (m <= 128 and k <= 192) or k <= 128:
         c6 = _product(L, A, B, 2)
         err6 = np.linalg.norm(c6 - ref) / np.linalg.norm(ref)
         # x0 + x1 + x2 keeps ~24 bits; the FP32 accumulation over the 6 k
-        # products (about 1e-6 relative on random data) is then the limit
-        assert err6 < 2e-6 and err6 < err / 4, (err6, err)
+        # products (about 1e-6 relative on random data, more for long k) is
+        # then the limit
+        assert err6 < 3e-6 and err6 < err / 2, (err6, err)
 
 
 def test_bf16x3_accumulates_into_c():
@@ -95,7 +96,7 @@ def test_split_products_reject_operators_beyond_shared_memory():
     big = torch.zeros(300 * 300, dtype=torch.float64, device="cuda")
     col = torch.zeros(300 * 10, dtype=torch.float64, device="cuda")
     out = torch.zeros(300 * 10, dtype=torch.float64, device="cuda")
-    for mode, (m, k) in ((1, (300, 64)), (1, (200, 160)), (2, (150, 125)), (2, (64, 100))):
+    for mode, (m, k) in ((1, (300, 64)), (1, (200, 200)), (2, (150, 140)), (2, (64, 200))):
         assert L.fr_op_set_gemm_precision(mode) == 0
         try:
             st = L.fr_op_extrapolate_solution(m, k, 1, 10, big.data_ptr(), col.data_ptr(), out.data_ptr(), None)
