@@ -75,7 +75,7 @@ FR_TILES(2, 5, T_({4, 160}), T_({4, 160}))
 FR_TILES(3, 1, T_({12, 128}), T_({12, 128}))
 FR_TILES(3, 2, T_({4, 128}, {2, 64}, {8, 256}), T_({4, 128}, {2, 64}, {8, 256}))
 FR_TILES(3, 3, T_({2, 128, 4}, {1, 64, 8}, {2, 192, 2}, {2, 128, 3}, {1, 96, 0}, {4, 256, 2}, {1, 96, 5}, {1, 96, 6},
-                  {1, 64, 8, 1}, {2, 128, 3, 1}), T_({2, 128}, {1, 64}, {4, 256}, {2, 96}, {4, 128}))
+                  {1, 64, 8, 1}, {2, 128, 3, 1}, {1, 96, 10}), T_({2, 128}, {1, 64}, {4, 256}, {2, 96}, {4, 128}))
 FR_TILES(3, 4, T_({1, 128}, {1, 160}, {2, 256}), T_({1, 128}, {2, 256}, {1, 160}))
 #undef T_
 #undef FR_TILES
