@@ -8,6 +8,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "fr_b200.h"
@@ -74,6 +75,12 @@ struct fr_solver {
   void* grad_buf = nullptr;         // gradient output of fr_solver_gradient (allocated on first use)
   float* feat_buf = nullptr;        // closure inputs of fr_solver_sgs_features (allocated on first use)
   double *diag_w = nullptr, *diag_partial = nullptr, *diag_out = nullptr;   // integral diagnostics
+  // asynchronous state upload (fr_solver_set_state_async): a device staging
+  // copy of the state, filled on its own stream while earlier steps run
+  double* staging = nullptr;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_staged = nullptr, ev_consumed = nullptr;
+  bool staged = false;
   std::vector<void*> allocs;
 };
 
@@ -304,6 +311,9 @@ fr_status fr_solver_destroy(fr_solver* s)
   cudaSetDevice(s->device);
   drop_graphs(s);
   if (s->own_stream) { cudaStreamSynchronize(s->own_stream); cudaStreamDestroy(s->own_stream); }
+  if (s->copy_stream) { cudaStreamSynchronize(s->copy_stream); cudaStreamDestroy(s->copy_stream); }
+  if (s->ev_staged) cudaEventDestroy(s->ev_staged);
+  if (s->ev_consumed) cudaEventDestroy(s->ev_consumed);
   for (void* p : s->allocs) cudaFree(p);
   delete s;
   return FR_OK;
@@ -371,17 +381,78 @@ fr_status fr_solver_state_updated(fr_solver* s, void* stream)
   return check_launch("fr_trace_kernel");
 }
 
+// Every density positive and finite; large arrays are split over host threads.
+static bool densities_ok(const double* rho, size_t n)
+{
+  auto scan = [rho](size_t a, size_t b) {
+    bool ok = true;
+    for (size_t i = a; i < b; i++) ok &= (rho[i] > 0) && std::isfinite(rho[i]);
+    return ok;
+  };
+  unsigned nt = std::thread::hardware_concurrency();
+  nt = nt < 1 ? 1 : (nt > 16 ? 16 : nt);
+  if (n < (size_t)1 << 18 || nt == 1) return scan(0, n);
+  std::vector<std::thread> pool;
+  std::vector<char> ok(nt, 1);
+  const size_t chunk = (n + nt - 1) / nt;
+  for (unsigned t = 0; t < nt; t++) {
+    const size_t a = t * chunk, b = a + chunk < n ? a + chunk : n;
+    pool.emplace_back([&, t, a, b] { ok[t] = a < b ? scan(a, b) : 1; });
+  }
+  for (auto& th : pool) th.join();
+  for (char c : ok)
+    if (!c) return false;
+  return true;
+}
+
 fr_status fr_solver_set_state(fr_solver* s, const double* host_u, void* stream)
 {
   if (!s || !host_u) return fail(FR_ERR_ARG, "null argument");
   FR_CUDA(cudaSetDevice(s->device));
   size_t n = (size_t)s->mesh.nu * s->mesh.ne * s->mesh.nfields;
-  for (size_t i = 0; i < (size_t)s->mesh.nu * s->mesh.ne; i++)
-    if (!(host_u[i] > 0) || !std::isfinite(host_u[i])) return fail(FR_ERR_NONFINITE, "density must be positive and finite");
+  if (!densities_ok(host_u, (size_t)s->mesh.nu * s->mesh.ne))
+    return fail(FR_ERR_NONFINITE, "density must be positive and finite");
   cudaStream_t st = STRM(s, stream);
   FR_CUDA(cudaMemcpyAsync(s->b.U, host_u, n * 8, cudaMemcpyHostToDevice, st));
   FR_CUDA(cudaMemsetAsync(s->b.REG, 0, n * 8, st));
   return fr_solver_state_updated(s, stream);
+}
+
+fr_status fr_solver_set_state_async(fr_solver* s, const double* host_u)
+{
+  if (!s || !host_u) return fail(FR_ERR_ARG, "null argument");
+  FR_CUDA(cudaSetDevice(s->device));
+  size_t n = (size_t)s->mesh.nu * s->mesh.ne * s->mesh.nfields;
+  if (!densities_ok(host_u, (size_t)s->mesh.nu * s->mesh.ne))
+    return fail(FR_ERR_NONFINITE, "density must be positive and finite");
+  if (!s->staging) {
+    fr_status r = dalloc(s, &s->staging, n);
+    if (r) return r;
+    FR_CUDA(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+    FR_CUDA(cudaEventCreateWithFlags(&s->ev_staged, cudaEventDisableTiming));
+    FR_CUDA(cudaEventCreateWithFlags(&s->ev_consumed, cudaEventDisableTiming));
+    FR_CUDA(cudaEventRecord(s->ev_consumed, s->copy_stream));
+  }
+  if (s->staged) return fail(FR_ERR_ARG, "a staged state has not been taken by an advance yet");
+  // the staging buffer is free once the step that took the previous state has copied it
+  FR_CUDA(cudaStreamWaitEvent(s->copy_stream, s->ev_consumed, 0));
+  FR_CUDA(cudaMemcpyAsync(s->staging, host_u, n * 8, cudaMemcpyHostToDevice, s->copy_stream));
+  FR_CUDA(cudaEventRecord(s->ev_staged, s->copy_stream));
+  s->staged = true;
+  return FR_OK;
+}
+
+// The staged state (if any) becomes the current state, in stream order.
+static fr_status take_staged(fr_solver* s, cudaStream_t st)
+{
+  if (!s->staged) return FR_OK;
+  size_t n = (size_t)s->mesh.nu * s->mesh.ne * s->mesh.nfields;
+  FR_CUDA(cudaStreamWaitEvent(st, s->ev_staged, 0));
+  FR_CUDA(cudaMemcpyAsync(s->b.U, s->staging, n * 8, cudaMemcpyDeviceToDevice, st));
+  FR_CUDA(cudaEventRecord(s->ev_consumed, st));
+  FR_CUDA(cudaMemsetAsync(s->b.REG, 0, n * 8, st));
+  s->staged = false;
+  return fr_solver_state_updated(s, st);
 }
 
 fr_status fr_solver_get_state(fr_solver* s, double* host_u, void* stream)
@@ -418,12 +489,28 @@ fr_status fr_solver_rk_stage(fr_solver* s, int st, double dt, void* stream)
   return stage(s, st, dt, st == 4, STRM(s, stream));
 }
 
+static fr_status advance_impl(fr_solver* s, int n_steps, double dt, double* norms_host, void* stream, bool wait);
+
 fr_status fr_solver_advance(fr_solver* s, int n_steps, double dt, double* norms_host, void* stream)
+{
+  return advance_impl(s, n_steps, dt, norms_host, stream, true);
+}
+
+fr_status fr_solver_advance_async(fr_solver* s, int n_steps, double dt, double* norms_host, void* stream)
+{
+  return advance_impl(s, n_steps, dt, norms_host, stream, false);
+}
+
+static fr_status advance_impl(fr_solver* s, int n_steps, double dt, double* norms_host, void* stream, bool wait)
 {
   if (!s || n_steps < 0) return fail(FR_ERR_ARG, "bad argument");
   if (!(dt > 0) || !std::isfinite(dt)) return fail(FR_ERR_ARG, "dt must be positive");
   FR_CUDA(cudaSetDevice(s->device));
   cudaStream_t st = STRM(s, stream);
+  {
+    fr_status r = take_staged(s, st);
+    if (r) return r;
+  }
   bool capture_ok = true;
   for (int i = 0; i < n_steps; i++) {
     int c = s->cur;
@@ -459,6 +546,7 @@ fr_status fr_solver_advance(fr_solver* s, int n_steps, double dt, double* norms_
     s->launches++;
     FR_CUDA(cudaGetLastError());
     FR_CUDA(cudaMemcpyAsync(norms_host, s->b.norms, F * 8, cudaMemcpyDeviceToHost, st));
+    if (!wait) return FR_OK;
     FR_CUDA(cudaStreamSynchronize(st));
     for (int k = 0; k < F; k++)
       if (!std::isfinite(norms_host[k])) return fail(FR_ERR_NONFINITE, "NaN/Inf in the residual");

@@ -87,12 +87,14 @@ def lib():
         "fr_solver_get_interfaces": (C.c_int, [vp, ip, ip]),
         "fr_solver_set_geometry": (C.c_int, [vp, dp, dp, dp, dp]),
         "fr_solver_set_state": (C.c_int, [vp, dp, vp]),
+        "fr_solver_set_state_async": (C.c_int, [vp, dp]),
         "fr_solver_get_state": (C.c_int, [vp, dp, vp]),
         "fr_solver_state_ptrs": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp)]),
         "fr_solver_state_updated": (C.c_int, [vp, vp]),
         "fr_solver_residual": (C.c_int, [vp, dp, vp]),
         "fr_solver_rk_stage": (C.c_int, [vp, C.c_int, C.c_double, vp]),
         "fr_solver_advance": (C.c_int, [vp, C.c_int, C.c_double, dp, vp]),
+        "fr_solver_advance_async": (C.c_int, [vp, C.c_int, C.c_double, dp, vp]),
         "fr_solver_kinetic_energy": (C.c_int, [vp, dp, vp]),
         "fr_solver_launch_count": (C.c_longlong, [vp]),
         "fr_solver_stream": (vp, [vp]),
@@ -317,6 +319,23 @@ class Solver:
         if u.shape != self.state_shape:
             raise ValueError("state shape %s != %s" % (u.shape, self.state_shape))
         _check(lib().fr_solver_set_state(self.h, _dp(u), stream))
+
+    def set_state_async(self, u):
+        """Stage a state for the next advance (fr_solver_set_state_async): u must
+        be a Fortran-ordered float64 array, ideally in pinned memory, left
+        unchanged until that advance has run."""
+        if not (isinstance(u, np.ndarray) and u.dtype == np.float64 and u.flags.f_contiguous):
+            raise ValueError("set_state_async needs a Fortran-ordered float64 array")
+        if u.shape != self.state_shape:
+            raise ValueError("state shape %s != %s" % (u.shape, self.state_shape))
+        _check(lib().fr_solver_set_state_async(self.h, _dp(u)))
+        self._staged_host = u
+
+    def advance_async(self, n_steps, dt, norms_out=None, stream=None):
+        """advance without waiting; norms_out (float64, n_fields, pinned memory
+        for an asynchronous copy) holds the L1 norms once the stream is synced."""
+        _check(lib().fr_solver_advance_async(self.h, int(n_steps), float(dt),
+                                             _dp(norms_out) if norms_out is not None else None, stream))
 
     def get_state(self, stream=None):
         u = np.zeros(self.state_shape, order="F")

@@ -117,6 +117,15 @@ fr_status fr_solver_set_geometry(fr_solver* s, const double* detjac_upts, const 
 /* State transfer (disu_upts(0)), host memory, layout (n_upts, n_eles, n_fields).
  * set_state zeroes the RK register (disu_upts(1)), like InitSolution. */
 fr_status fr_solver_set_state(fr_solver* s, const double* host_u, void* stream);
+
+/* Asynchronous state upload for pipelined hosts: validates the densities
+ * (as fr_solver_set_state), then copies host_u -- pinned host memory that
+ * must stay unchanged until the copy is done -- into a device staging buffer
+ * on the solver's copy stream, overlapping steps already queued.  The next
+ * fr_solver_advance / fr_solver_advance_async takes it as the current state
+ * (RK register cleared, traces rebuilt) in stream order.  One state can be
+ * staged at a time (FR_ERR_ARG otherwise).  No counterpart in the reference. */
+fr_status fr_solver_set_state_async(fr_solver* s, const double* host_u);
 fr_status fr_solver_get_state(fr_solver* s, double* host_u, void* stream);
 /* Device pointers of the resident state and RK register (owned by the solver). */
 fr_status fr_solver_state_ptrs(fr_solver* s, double** d_u, double** d_reg);
@@ -137,6 +146,11 @@ fr_status fr_solver_rk_stage(fr_solver* s, int stage, double dt, void* stream);
  * src/output.cpp:1452-1523, res_norm_type 1).  Graph-replayed after the first
  * call with the same dt. */
 fr_status fr_solver_advance(fr_solver* s, int n_steps, double dt, double* norms_host, void* stream);
+
+/* fr_solver_advance without waiting: the norms (if requested) are copied to
+ * norms_host asynchronously -- valid, and not yet checked for NaN/Inf, once
+ * the stream is synchronised (fr_solver_sync). */
+fr_status fr_solver_advance_async(fr_solver* s, int n_steps, double dt, double* norms_host, void* stream);
 
 /* Volume integral of 0.5 rho |v|^2 (solution-point Gauss quadrature), FP64. */
 fr_status fr_solver_kinetic_energy(fr_solver* s, double* out_host, void* stream);
