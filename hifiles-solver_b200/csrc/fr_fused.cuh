@@ -419,7 +419,12 @@ __host__ __device__ constexpr bool grad_alias()
 // prefetched value across the phases; the left normals are fetched while the
 // divergence is computed.  MINB is the CTAs per SM the registers are sized
 // for; VEC = 0 keeps every global read element-sized (inputs only 8-byte
-// aligned), VEC = 1 uses 16-byte copies where the per-element runs allow.
+// aligned), VEC = 1 uses 16-byte copies where the per-element runs allow;
+// PERS = 1 makes the blocks persistent (see the input staging below).
+// Hexahedra of P = 3 in FP64 keep their per-point arrays in the order of swz
+// (bank-conflict-free line reads), run the flux-point phase one line of
+// solution points per task (both end flux points from one read), and, with
+// one point per thread, use the aliased shared-memory plan of GradPlan.
 // Outputs VF (n_fpts, n_eles, F-1), ND (n_fpts, n_eles, F), DV (n_upts, n_eles, F),
 // BV (n_boundary_points, F) the viscous normal flux at boundary points (side
 // bits 2.. hold the boundary type, mate = -1 - position in the boundary
@@ -1044,6 +1049,7 @@ __device__ __noinline__ void face_boundary(PhysT<TC> ph, long long j, const TC* 
 // two states, convective_flux_boundary, src/inters.cpp:368-387; Roe in 2-D
 // with RIEMANN 2; the own flux for slip_wall_dual, right_flux,
 // src/inters.cpp:299-308), plus the viscous part BV from the gradient kernel.
+// Blocks of exactly 128 threads (one shared staging column per thread).
 template <int DIM, int VISC, typename TC, int RIEMANN = 0>
 __global__ void __launch_bounds__(128)
 fr_face_kernel(const int2* __restrict__ face, const unsigned char* __restrict__ fsign, long long nint,
