@@ -1,0 +1,266 @@
+#!/usr/bin/env python3
+"""Golden fixtures of mixed-element meshes (tets, prisms, hexes), made by
+running the reference itself.
+
+TEST INFRASTRUCTURE ONLY.  Runs where the reference sources are available and
+oracle/_ref/ref_harness is built (`make -C oracle ref`).  For every case it
+
+  1. writes a jittered periodic box of mixed elements as a Gambit neutral file
+     (element reader src/geometry.cpp:1706-1880: linear tets = Gambit type 6,
+     linear prisms = type 5, hexes = type 4; face numbers of the boundary
+     reader src/geometry.cpp:1236-1290),
+  2. runs the unmodified reference objects through ref_harness, which dumps
+     every element type's operators opp_0..opp_6 (eles_tets / eles_pris /
+     eles_hexas set-up), metrics, the interface wiring of every interface type
+     (triangular and quadrilateral faces), the intermediate arrays of one
+     CalcResidual and the state after N RK45 steps,
+  3. stores a compact .npz per case.
+
+The per-operator entry points take exactly these operators and tables, as the
+reference's own per-type methods would pass them; tests/test_gpu_mixed.py runs
+the stage through them and compares with the reference's arrays.
+
+Meshes (a conforming mix of the three types needs pyramids, which the
+reference has no element for, so hexes and tets never share a face):
+  * "pritet": prism layers at the bottom and top of y (each x-z cell square
+    split along its (0,0)-(1,1) diagonal into two triangles, extruded in y)
+    and a core of six tets per cell (Kuhn split along the main diagonal, whose
+    y-faces carry the same diagonal), periodic in x, y and z;
+  * "hexpri": hexes for the first half of the x cells and y-extruded prisms
+    for the second half (hex and prism meet on quadrilateral faces), periodic.
+Interior vertices move by a seeded jitter of up to `jitter` cell sizes.
+
+Usage:  python tests/golden/make_mixed.py [--ref /root/reference]
+"""
+import argparse
+import itertools
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.abspath(os.path.join(HERE, "..", ".."))
+sys.path.insert(0, HERE)
+import make_golden as G  # noqa: E402
+
+# reference local faces (src/geometry.cpp:3075-3290) and the Gambit face
+# number the boundary reader maps to each (inverse of src/geometry.cpp:1255-1282)
+TET_FACES = [(1, 2, 3), (0, 3, 2), (0, 1, 3), (0, 2, 1)]
+TET_GAMBIT = {0: 3, 1: 4, 2: 2, 3: 1}
+PRI_FACES = [(0, 2, 1), (3, 4, 5), (0, 1, 4, 3), (1, 2, 5, 4), (2, 0, 3, 5)]
+PRI_GAMBIT = {0: 4, 1: 5, 2: 1, 3: 2, 4: 3}
+# hex: Gambit node g = ag + 2 bg + 4 cg is tensor node (a, b, c) = (cg, ag, bg)
+HEX_ORDER = [((g >> 2) & 1) + 2 * (g & 1) + 4 * ((g >> 1) & 1) for g in range(8)]
+
+
+def _vol(xv, t):
+    a, b, c, d = (xv[v] for v in t)
+    return float(np.dot(np.cross(b - a, c - a), d - a))
+
+
+def mixed_cells(kind, n, lo, hi, jitter, seed):
+    """Vertices and elements [(gambit_type, vertex ids), ...] of a mixed box,
+    plus per element its boundary faces [(side, gambit_face)]."""
+    xv, c2v = G.box_vertices(3, n, lo, hi, jitter, seed=seed)
+    nx, ny, nz = n
+    vx, vy = nx + 1, ny + 1
+
+    def vid(i, j, k):
+        return i + vx * (j + vy * k)
+
+    def ijk(v):
+        return v % vx, (v // vx) % vy, v // (vx * vy)
+
+    eles = []
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                c = lambda a, b, cc: vid(i + a, j + b, k + cc)  # noqa: E731
+                if kind == "pritet":
+                    use = "pri" if j in (0, ny - 1) else "tet"
+                else:
+                    use = "hex" if i < nx // 2 else "pri"
+                if use == "hex":
+                    e = c2v[i + nx * (j + ny * k)]
+                    eles.append((4, [int(e[HEX_ORDER[g]]) for g in range(8)]))
+                elif use == "pri":
+                    # triangles in (x, z): (00, 11, 10) and (00, 01, 11); node 0->1
+                    # x node 0->2 along +y gives a positive volume
+                    for tri in (((0, 0), (1, 1), (1, 0)), ((0, 0), (0, 1), (1, 1))):
+                        bot = [c(a, 0, cc) for a, cc in tri]
+                        top = [c(a, 1, cc) for a, cc in tri]
+                        eles.append((5, bot + top))
+                else:
+                    for perm in itertools.permutations(range(3)):
+                        p = [0, 0, 0]
+                        path = [tuple(p)]
+                        for ax in perm:
+                            p[ax] = 1
+                            path.append(tuple(p))
+                        t = [c(*q) for q in (path[0], path[1], path[2], path[3])]
+                        if _vol(xv, t) < 0:
+                            t = [t[0], t[2], t[1], t[3]]
+                        eles.append((6, t))
+    # orientation and boundary faces
+    out = []
+    for gt, vs in eles:
+        if gt == 6:
+            assert _vol(xv, vs) > 0
+            faces = [(f, TET_GAMBIT[f], [vs[q] for q in TET_FACES[f]]) for f in range(4)]
+        elif gt == 5:
+            assert _vol(xv, [vs[0], vs[1], vs[2], vs[3]]) > 0
+            faces = [(f, PRI_GAMBIT[f], [vs[q] for q in PRI_FACES[f]]) for f in range(5)]
+        else:
+            faces = None
+        bf = []
+        if faces is None:
+            I = [ijk(v) for v in vs]
+            for side, code in ((0, 5), (1, 6), (2, 4), (3, 2), (4, 1), (5, 3)):
+                ax, hi_side = side // 2, side % 2
+                lim = n[ax] if hi_side else 0
+                if sum(1 for q in I if q[ax] == lim) == 4:
+                    bf.append((side, code))
+        else:
+            for f, code, fv in faces:
+                I = [ijk(v) for v in fv]
+                for side in range(6):
+                    ax, hi_side = side // 2, side % 2
+                    lim = n[ax] if hi_side else 0
+                    if all(q[ax] == lim for q in I):
+                        bf.append((side, code))
+        out.append((gt, vs, bf))
+    return xv, out
+
+
+def write_mixed_gambit(path, xv, eles, side_bc=None):
+    side_bc = list(side_bc) if side_bc is not None else [0] * 6
+    names = ["Cyclic" if b == 0 else G.BC_NAMES[b] for b in side_bc]
+    groups = sorted(set(names), key=names.index)
+    ne = len(eles)
+    lines = ["        CONTROL INFO 2.3.16", "** GAMBIT NEUTRAL FILE", "mixed", "PROGRAM:  fixture", "",
+             "     NUMNP     NELEM     NGRPS    NBSETS     NDFCD     NDFVL",
+             "%10d%10d%10d%10d%10d%10d" % (xv.shape[0], ne, 1, len(groups), 3, 3),
+             "ENDOFSECTION", "   NODAL COORDINATES 2.3.16"]
+    for v in range(xv.shape[0]):
+        lines.append("%10d " % (v + 1) + " ".join("%.17e" % c for c in xv[v]))
+    lines += ["ENDOFSECTION", "      ELEMENTS/CELLS 2.3.16"]
+    for e, (gt, vs, _) in enumerate(eles):
+        nodes = [v + 1 for v in vs]
+        lines.append("%8d %2d %2d " % (e + 1, gt, len(nodes)) + " ".join("%8d" % x for x in nodes[:7]))
+        if len(nodes) > 7:
+            lines.append("               " + " ".join("%8d" % x for x in nodes[7:]))
+    lines += ["ENDOFSECTION", "       ELEMENT GROUP 2.3.16",
+              "GROUP:          1 ELEMENTS: %10d MATERIAL:          2 NFLAGS:          1" % ne,
+              "                           fluid", "       0"]
+    ids = [str(e + 1) for e in range(ne)]
+    for i in range(0, ne, 10):
+        lines.append(" ".join("%7s" % x for x in ids[i:i + 10]))
+    bnd = {g: [] for g in groups}
+    for e, (gt, _, bf) in enumerate(eles):
+        for side, code in bf:
+            bnd[names[side]].append((e + 1, gt, code))
+    for g in groups:
+        lines += ["ENDOFSECTION", " BOUNDARY CONDITIONS 2.3.16"]
+        lines.append("%32s%8d%8d%8d%8d" % (g, 1, len(bnd[g]), 0, 6))
+        for b in bnd[g]:
+            lines.append("%10d%5d%5d" % b)
+    lines.append("ENDOFSECTION")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
+CASES = [
+    # tet_upts: upts_type_tet (0 interior quadrature points, 1 alpha-optimised nodes)
+    dict(name="mixed_pritet_p3", kind="pritet", order=3, n=(2, 3, 2), jitter=0.1, steps=3, dt=1e-3, tet_upts=0),
+    dict(name="mixed_pritet_p2", kind="pritet", order=2, n=(2, 4, 2), jitter=0.15, steps=3, dt=1e-3, tet_upts=1),
+    dict(name="mixed_hexpri_p3", kind="hexpri", order=3, n=(4, 2, 2), jitter=0.1, steps=3, dt=1e-3, tet_upts=0),
+]
+
+# arrays kept per element type (prefix t<ele_type>_ in the harness output)
+SETUP = ["opp_0", "opp_3", "opp_6", "detjac_upts", "JGinv_upts", "tdA_fpts", "norm_fpts", "disu_upts_init"]
+STAGES = ["s01_disu_fpts", "s04_delta_disu_fpts", "s05_grad_disu_upts", "s06_grad_disu_fpts", "s07_tdisf_upts",
+          "s08_norm_tdisf_fpts", "s09_div_tconf_upts", "s10_norm_tconf_fpts", "s11_div_tconf_upts",
+          "s12_disu_upts0", "final_disu_upts0"]
+
+
+def run_case(ref, c, work):
+    d = os.path.join(work, c["name"])
+    os.makedirs(d, exist_ok=True)
+    lo, hi = (0.0, 0.0, 0.0), (2 * np.pi,) * 3
+    xv, eles = mixed_cells(c["kind"], c["n"], lo, hi, c["jitter"], seed=12345)
+    write_mixed_gambit(os.path.join(d, "mesh.neu"), xv, eles)
+    L = [hi[i] - lo[i] for i in range(3)]
+    vals = {
+        "equation": 0, "viscous": 1, "riemann_solve_type": 0, "vis_riemann_solve_type": 0, "ic_form": 7,
+        "order": c["order"], "dt_type": 0, "dt": c["dt"], "n_steps": c["steps"], "adv_type": 3, "tau": 1.0,
+        "pen_fact": 0.5, "mesh_file": "mesh.neu", "dx_cyclic": "%.17g" % L[0], "dy_cyclic": "%.17g" % L[1],
+        "dz_cyclic": "%.17g" % L[2], "monitor_res_freq": 100000, "plot_freq": 100000, "restart_dump_freq": 100000,
+        "upts_type_hexa": 0, "vcjh_scheme_hexa": 1, "upts_type_tet": c["tet_upts"], "fpts_type_tet": 0, "vcjh_scheme_tet": 2,
+        "upts_type_pri_tri": 0, "upts_type_pri_1d": 0, "vcjh_scheme_pri_1d": 1, "vcjh_scheme_tri": 1,
+        "prandtl": 0.71, "Mach_free_stream": 0.1, "Re_free_stream": 1600.0, "gamma": 1.4, "fix_vis": 1,
+        "res_norm_type": 1,
+    }
+    G.write_input(os.path.join(d, "input"), os.path.join(ref, G.TGV_INPUT), vals)
+    out = os.path.join(d, "out")
+    os.makedirs(out, exist_ok=True)
+    env = dict(os.environ, HIFILES_HOME=os.path.join(REPO, "oracle", "_ref"))
+    args = [G.HARNESS, "input", out, "--ic", "tgv_mach01", "--steps", str(c["steps"]), "--stages"]
+    r = subprocess.run(args, cwd=d, env=env, capture_output=True, text=True)
+    if r.returncode != 0:
+        print(r.stdout[-3000:], r.stderr[-3000:])
+        raise RuntimeError("harness failed for " + c["name"])
+    arr, par = G.load_npy_dir(out)
+    types = []
+    for line in open(os.path.join(out, "params.txt")):
+        p = line.split()
+        if p[0] == "type" and int(p[5]) > 0:
+            types.append(dict(index=int(p[1]), ele_type=int(p[3]), n_eles=int(p[5]), n_upts=int(p[7]),
+                              n_fpts=int(p[9])))
+    return arr, par, types, eles
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--work", default=None)
+    a = ap.parse_args()
+    if not os.path.exists(G.HARNESS):
+        subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "REF=" + a.ref, "ref"], check=True)
+    work = a.work or tempfile.mkdtemp(prefix="fr_mixed_")
+    for c in CASES:
+        arr, par, types, eles = run_case(a.ref, c, work)
+        fx = {}
+        for t in types:
+            T = "t%d_" % t["ele_type"]
+            for k in SETUP:
+                fx[T + k] = arr[T + k]
+            for w in (1, 2, 4, 5):
+                for dd in range(3):
+                    fx[T + "opp_%d_%d" % (w, dd)] = arr[T + "opp_%d_%d" % (w, dd)]
+            for k in STAGES:
+                fx[T + k] = arr[T + k]
+        inters = []
+        for it in range(8):
+            key = "int_inters_%d" % it
+            if key in arr:
+                fx[key] = arr[key]
+                inters.append(dict(index=it, n_fpts=int(arr[key].shape[1]), n_inters=int(arr[key].shape[2])))
+        fx["res_norms"] = arr["res_norms"]
+        meta = dict(c)
+        meta["n"] = list(c["n"])
+        meta["types"] = types
+        meta["inters"] = inters
+        meta["physics"] = {k: par[k] for k in ("gamma", "prandtl", "mu_inf", "rt_inf", "c_sth", "fix_vis", "tau",
+                                                 "pen_fact")}
+        meta["element_counts"] = {str(gt): sum(1 for e in eles if e[0] == gt) for gt in (4, 5, 6)}
+        np.savez_compressed(os.path.join(HERE, c["name"] + ".npz"), meta=json.dumps(meta),
+                            **{k: np.asfortranarray(v) for k, v in fx.items()})
+        print(c["name"], json.dumps({"types": types, "inters": inters}))
+
+
+if __name__ == "__main__":
+    main()

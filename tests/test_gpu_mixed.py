@@ -1,0 +1,208 @@
+"""Mixed-element meshes (tets, prisms, hexes) through the per-operator entry
+points, against the reference's own arrays.
+
+The fixtures (tests/golden/mixed_*.npz, made by tests/golden/make_mixed.py
+from runs of the reference itself) hold what the reference's per-type classes
+pass across the seam: every element type's dense operators opp_0..opp_6
+(eles_tets, eles_pris, eles_hexas set-up), its metrics, and the wiring of the
+triangular and quadrilateral interfaces, decoded from int_inters' pointer
+tables (src/int_inters.cpp:95-178).  The GPU test runs CalcResidual
+(src/solver.cpp:65-225) one operator at a time, element type by element type
+and interface type by interface type as the reference does, then three RK45
+steps, and compares every intermediate array and the final state.
+
+The CPU tests check the fixtures themselves: the wiring pairs every flux
+point of the periodic mesh exactly once, and the dumped arrays obey the
+linear operator relations they are defined by."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from golden_util import load, rel
+
+MIXED = ["mixed_pritet_p3", "mixed_pritet_p2", "mixed_hexpri_p3"]
+RK4B = [0.149659021999229, 0.379210312999627, 0.822955029386982, 0.699450455949122, 0.153057247968152]
+
+
+def _types(meta):
+    return {t["index"]: t for t in meta["types"]}
+
+
+@pytest.mark.parametrize("case", MIXED)
+def test_mixed_wiring_pairs_every_flux_point_once(case):
+    meta, a = load(case)
+    ty = _types(meta)
+    seen = {i: np.zeros((t["n_fpts"], t["n_eles"]), dtype=np.int64) for i, t in ty.items()}
+    for it in meta["inters"]:
+        w = a["int_inters_%d" % it["index"]].reshape(6, -1)
+        for s in (0, 3):
+            for tt, e, f in zip(w[s], w[s + 1], w[s + 2]):
+                seen[int(tt)][f, e] += 1
+        # both sides of an interface point sit at the same place: same state
+        # trace in the reference's extrapolated solution
+        for k in range(w.shape[1]):
+            tl, el, fl, tr, er, fr = (int(x) for x in w[:, k])
+            ul = a["t%d_s01_disu_fpts" % ty[tl]["ele_type"]][fl, el, 0]
+            ur = a["t%d_s01_disu_fpts" % ty[tr]["ele_type"]][fr, er, 0]
+            assert abs(ul - ur) < 0.05 * abs(ul)
+    for i, s in seen.items():
+        assert (s == 1).all(), (case, ty[i]["ele_type"])
+
+
+@pytest.mark.parametrize("case", MIXED)
+def test_mixed_fixture_operator_relations(case):
+    meta, a = load(case)
+    for t in meta["types"]:
+        T = "t%d_" % t["ele_type"]
+        u0 = a[T + "disu_upts_init"]
+        nu, E, F = u0.shape
+        # extrapolation: disu_fpts = opp_0 u
+        got = np.einsum("fu,uek->fek", a[T + "opp_0"], u0)
+        assert rel(got, a[T + "s01_disu_fpts"]) < 1e-14
+        # divergence: div = sum_d opp_2[d] tdisf[d]; corrected: += opp_3 (norm_tconf - norm_tdisf)
+        div = sum(np.einsum("vu,uek->vek", a[T + "opp_2_%d" % d], a[T + "s07_tdisf_upts"][..., d]) for d in range(3))
+        assert rel(div, a[T + "s09_div_tconf_upts"]) < 1e-13
+        jump = a[T + "s10_norm_tconf_fpts"] - a[T + "s08_norm_tdisf_fpts"]
+        corr = a[T + "s09_div_tconf_upts"] + np.einsum("uf,fek->uek", a[T + "opp_3"], jump)
+        assert rel(corr, a[T + "s11_div_tconf_upts"]) < 1e-12
+        # RK45 stage 0 from a zero register: u1 = u0 + b_0 dt (-div / detJ)
+        res = meta["dt"] * (-a[T + "s11_div_tconf_upts"] / a[T + "detjac_upts"][:, :, None])
+        assert rel(a[T + "s12_disu_upts0"], u0 + RK4B[0] * res) < 1e-15
+
+
+# ------------------------------------------------------------------ GPU path
+
+def _seam():
+    import hifiles_b200 as H
+    import test_gpu_ops as T
+    return H, T, T._bind(H.lib())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", MIXED)
+def test_mixed_mesh_through_the_operator_seam_matches_the_reference(case):
+    torch = pytest.importorskip("torch")
+    H, T, L = _seam()
+    meta, a = load(case)
+    VP = C.c_void_p
+    ty = _types(meta)
+    ph = T.PhysDesc(**meta["physics"])
+    D, F = 3, 5
+    P = lambda t: t.data_ptr()  # noqa: E731
+    dev = T._dev
+    S = {}
+    for i, t in ty.items():
+        X = "t%d_" % t["ele_type"]
+        nu, nf, E = t["n_upts"], t["n_fpts"], t["n_eles"]
+        s = dict(nu=nu, nf=nf, E=E, X=X)
+        s["opp0"], s["opp3"], s["opp6"] = (dev(a[X + k]) for k in ("opp_0", "opp_3", "opp_6"))
+        for w in (1, 2, 4, 5):
+            s["opp%d" % w] = [dev(a[X + "opp_%d_%d" % (w, d)]) for d in range(D)]
+            s["opp%d_ptrs" % w] = (VP * D)(*[P(x) for x in s["opp%d" % w]])
+        s["JG"], s["dj"], s["tdA"], s["nrm"] = (dev(a[X + k]) for k in ("JGinv_upts", "detjac_upts", "tdA_fpts",
+                                                                         "norm_fpts"))
+        s["u"] = dev(a[X + "disu_upts_init"])
+        s["reg"] = torch.zeros_like(s["u"])
+        z = lambda n: torch.zeros(n, dtype=torch.float64, device="cuda")  # noqa: E731
+        s["ufp"], s["ntc"], s["ntd"], s["ddu"] = z(nf * E * F), z(nf * E * F), z(nf * E * F), z(nf * E * F)
+        s["tf"], s["gup"], s["gfp"] = z(nu * E * F * D), z(nu * E * F * D), z(nf * E * F * D)
+        s["div"] = z(nu * E * F)
+        S[i] = s
+
+    def table(w, side, arr, comps):
+        """int_inters-style device table: for every (fpt, inter) of one side and
+        every component c, the address of arr[fpt, ele, c] of that side's type."""
+        tt, e, f = (w[side + q].reshape(-1, order="F").astype(np.int64) for q in range(3))
+        rows = np.zeros((tt.size, comps), dtype=np.int64)
+        for i, s in S.items():
+            m = tt == i
+            if not m.any():
+                continue
+            base = s[arr].data_ptr()
+            slot = f[m] + s["nf"] * e[m]
+            rows[m] = base + 8 * (slot[:, None] + s["nf"] * s["E"] * np.arange(comps)[None, :])
+        return torch.from_numpy(np.asfortranarray(rows).ravel(order="F").copy()).cuda()
+
+    inters = []
+    for it in meta["inters"]:
+        w = a["int_inters_%d" % it["index"]]
+        tb = dict(nfpi=it["n_fpts"], ni=it["n_inters"])
+        for side, sfx in ((0, "l"), (3, "r")):
+            tb["u" + sfx] = table(w, side, "ufp", F)
+            tb["t" + sfx] = table(w, side, "ntc", F)
+            tb["d" + sfx] = table(w, side, "ddu", F)
+            tb["g" + sfx] = table(w, side, "gfp", F * D)
+            tb["a" + sfx] = table(w, side, "tdA", 1)
+        tb["n"] = table(w, 0, "nrm", D)
+        inters.append(tb)
+
+    def ok(st):
+        assert st == 0, H.lib().fr_last_error().decode()
+
+    def residual():
+        for s in S.values():
+            ok(L.fr_op_extrapolate_solution(s["nf"], s["nu"], F, s["E"], P(s["opp0"]), P(s["u"]), P(s["ufp"]), None))
+            ok(L.fr_op_calculate_gradient(s["nu"], D, F, s["E"], C.cast(s["opp4_ptrs"], VP), P(s["u"]), P(s["gup"]),
+                                          None))
+            ok(L.fr_op_evaluate_invFlux(s["nu"], D, F, s["E"], P(s["u"]), P(s["JG"]), P(s["tf"]), C.byref(ph), None))
+        for tb in inters:
+            ok(L.fr_op_int_inters_common_invFlux(tb["nfpi"], D, F, tb["ni"], P(tb["ul"]), P(tb["ur"]), P(tb["tl"]),
+                                                 P(tb["tr"]), P(tb["al"]), P(tb["ar"]), P(tb["n"]), P(tb["dl"]),
+                                                 P(tb["dr"]), C.byref(ph), 1, None))
+        for s in S.values():
+            ok(L.fr_op_correct_gradient(s["nu"], s["nf"], D, F, s["E"], C.cast(s["opp5_ptrs"], VP), P(s["ddu"]),
+                                        P(s["JG"]), P(s["dj"]), P(s["gup"]), None))
+            ok(L.fr_op_extrapolate_corrected_gradient(s["nf"], s["nu"], D, F, s["E"], P(s["opp6"]), P(s["gup"]),
+                                                      P(s["gfp"]), None))
+            ok(L.fr_op_evaluate_viscFlux(s["nu"], D, F, s["E"], P(s["u"]), P(s["gup"]), P(s["JG"]), P(s["tf"]),
+                                         C.byref(ph), None))
+            ok(L.fr_op_extrapolate_totalFlux(s["nf"], s["nu"], D, F, s["E"], C.cast(s["opp1_ptrs"], VP), P(s["tf"]),
+                                             P(s["ntd"]), None))
+            ok(L.fr_op_calculate_divergence(s["nu"], D, F, s["E"], C.cast(s["opp2_ptrs"], VP), P(s["tf"]),
+                                            P(s["div"]), None))
+        for tb in inters:
+            ok(L.fr_op_int_inters_common_viscFlux(tb["nfpi"], D, F, tb["ni"], P(tb["ul"]), P(tb["ur"]), P(tb["gl"]),
+                                                  P(tb["gr"]), P(tb["tl"]), P(tb["tr"]), P(tb["al"]), P(tb["ar"]),
+                                                  P(tb["n"]), C.byref(ph), None))
+        snap = {i: T._host(s["ntc"], (s["nf"], s["E"], F)) for i, s in S.items()}
+        for s in S.values():
+            ok(L.fr_op_calculate_corrected_divergence(s["nu"], s["nf"], F, s["E"], P(s["opp3"]), P(s["ntd"]),
+                                                      P(s["ntc"]), P(s["div"]), None))
+        return snap
+
+    def advance(stage):
+        for s in S.values():
+            ok(L.fr_op_advance_rk45(s["nu"], F, s["E"], stage, meta["dt"], 0.0, P(s["u"]), P(s["reg"]), P(s["div"]),
+                                    P(s["dj"]), None, None))
+
+    ntc_visc = residual()
+    torch.cuda.synchronize()
+    tol = 1e-12
+    for i, s in S.items():
+        X, nu, nf, E = s["X"], s["nu"], s["nf"], s["E"]
+        assert rel(T._host(s["ufp"], (nf, E, F)), a[X + "s01_disu_fpts"]) <= tol
+        assert rel(T._host(s["ddu"], (nf, E, F)), a[X + "s04_delta_disu_fpts"]) <= tol
+        assert rel(T._host(s["gup"], (nu, E, F, D)), a[X + "s05_grad_disu_upts"]) <= tol
+        assert rel(T._host(s["gfp"], (nf, E, F, D)), a[X + "s06_grad_disu_fpts"]) <= tol
+        assert rel(T._host(s["tf"], (nu, E, F, D)), a[X + "s07_tdisf_upts"]) <= tol
+        assert rel(T._host(s["ntd"], (nf, E, F)), a[X + "s08_norm_tdisf_fpts"]) <= tol
+        assert rel(ntc_visc[i], a[X + "s10_norm_tconf_fpts"]) <= tol
+        assert rel(T._host(s["div"], (nu, E, F)), a[X + "s11_div_tconf_upts"]) <= tol
+    advance(0)
+    torch.cuda.synchronize()
+    for s in S.values():
+        assert rel(T._host(s["u"], (s["nu"], s["E"], F)), a[s["X"] + "s12_disu_upts0"]) <= 1e-14
+    # the rest of three RK45 steps (src/HiFiLES.cpp:159-183)
+    for step in range(meta["steps"]):
+        for stage in range(1 if step == 0 else 0, 5):
+            residual()
+            advance(stage)
+    torch.cuda.synchronize()
+    for s in S.values():
+        X = s["X"]
+        u = T._host(s["u"], (s["nu"], s["E"], F))
+        u0 = a[X + "disu_upts_init"]
+        assert rel(u, a[X + "final_disu_upts0"]) <= 1e-14
+        # the change over three steps, not only the state, agrees
+        assert rel(u - u0, a[X + "final_disu_upts0"] - u0) <= 1e-10
