@@ -271,6 +271,113 @@ __global__ void common_vis_kernel(int nfpi, int ni, double* const* __restrict__ 
   for (int k = 0; k < F; k++) { *tl_p[t + n * k] += fn[k] * tal; *tr_p[t + n * k] += -fn[k] * tar; }
 }
 
+// --------------------------------------------------------- boundary kernels
+// Tables follow bdy_inters (src/bdy_inters.cpp:111-203): only the owning
+// (left) side; boundary_type[i] is the type of boundary interface i and
+// bdy_params the 14 boundary values of bdy_inters::set_bdy_params
+// (src/bdy_inters.cpp:78-108), both in device memory as the reference keeps
+// them.  The ghost state, the central boundary flux and the viscous wall flux
+// are the ones of the fused interface kernel's boundary points.
+
+__device__ __forceinline__ void load_bdy(PhysT<double>& ph, const double* __restrict__ bp)
+{
+#pragma unroll
+  for (int i = 0; i < 14; i++) ph.bdy[i] = bp[i];
+}
+
+// bdy_inters::evaluate_boundaryConditions_invFlux (src/bdy_inters.cpp:245-389):
+// norm_tconf_l = f_n tdA with f_n the central flux of own and ghost state
+// (the own flux alone at dual-consistent slip walls, Roe in 2-D when asked),
+// and, viscous, the LDG common solution delta_l = (u_ghost + u_l)/2 - u_l.
+template <int D>
+__global__ void bdy_inv_kernel(int nfpi, int ni, double* const* __restrict__ ul_p, double* const* __restrict__ tl_p,
+                               double* const* __restrict__ al_p, double* const* __restrict__ n_p,
+                               double* const* __restrict__ dl_p, const int* __restrict__ btype,
+                               const double* __restrict__ bp, PhysT<double> ph, int riemann, int viscous)
+{
+  constexpr int F = D + 2;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)nfpi * ni;
+  if (t >= n) return;
+  load_bdy(ph, bp);
+  const int type = btype[t / nfpi];
+  double ul[F], ug[F], nn[D], fn[F], fl[F][D], fr[F][D];
+#pragma unroll
+  for (int k = 0; k < F; k++) ul[k] = *ul_p[t + n * k];
+#pragma unroll
+  for (int d = 0; d < D; d++) nn[d] = *n_p[t + n * d];
+  bc_ghost<D, double>(ph, type, ul, nn, ug);
+  inv_flux<D, double>(ph, ul, fl);
+  inv_flux<D, double>(ph, ug, fr);
+  if (type == 16) {
+#pragma unroll
+    for (int k = 0; k < F; k++) {
+      double s = fl[k][0] * nn[0];
+#pragma unroll
+      for (int l = 1; l < D; l++) s = s + fl[k][l] * nn[l];
+      fn[k] = s;
+    }
+  } else if (D == 2 && riemann == 2) {
+    roe<double>(ph, ul, ug, nn, fn);
+  } else {
+#pragma unroll
+    for (int k = 0; k < F; k++) {
+      double s = fl[k][0] * nn[0], q = fr[k][0] * nn[0];
+#pragma unroll
+      for (int l = 1; l < D; l++) { s = s + fl[k][l] * nn[l]; q = q + fr[k][l] * nn[l]; }
+      fn[k] = 0.5 * (s + q);
+    }
+  }
+  const double tal = *al_p[t];
+#pragma unroll
+  for (int k = 0; k < F; k++) *tl_p[t + n * k] = fn[k] * tal;
+  if (viscous) {
+#pragma unroll
+    for (int k = 0; k < F; k++) *dl_p[t + n * k] = 0.5 * (ug[k] + ul[k]) - ul[k];
+  }
+}
+
+// bdy_inters::evaluate_boundaryConditions_viscFlux (src/bdy_inters.cpp:905-1057):
+// norm_tconf_l += (f_v + tau n (u_l - u_ghost)) . n tdA, f_v the own viscous
+// flux, or the ghost side's with no wall-normal temperature gradient at
+// adiabatic walls (types 12 and 14).
+template <int D>
+__global__ void bdy_vis_kernel(int nfpi, int ni, double* const* __restrict__ ul_p, double* const* __restrict__ gl_p,
+                               double* const* __restrict__ tl_p, double* const* __restrict__ al_p,
+                               double* const* __restrict__ n_p, const int* __restrict__ btype,
+                               const double* __restrict__ bp, PhysT<double> ph)
+{
+  constexpr int F = D + 2;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)nfpi * ni;
+  if (t >= n) return;
+  load_bdy(ph, bp);
+  const int type = btype[t / nfpi];
+  double ul[F], ug[F], nn[D], g[F][D], fv[F][D];
+#pragma unroll
+  for (int k = 0; k < F; k++) {
+    ul[k] = *ul_p[t + n * k];
+#pragma unroll
+    for (int d = 0; d < D; d++) g[k][d] = *gl_p[t + n * (k + (long long)F * d)];
+  }
+#pragma unroll
+  for (int d = 0; d < D; d++) nn[d] = *n_p[t + n * d];
+  vis_flux_fast<D, double>(ph, ul, g, fv);
+  bc_ghost<D, double>(ph, type, ul, nn, ug);
+  if (type == 12 || type == 14) {
+    bc_vis_gradient<D, double>(ph, ul, ug, g);
+    vis_flux_fast<D, double>(ph, ug, g, fv);
+  }
+  const double tal = *al_p[t];
+#pragma unroll
+  for (int k = 0; k < F; k++) {
+    double fnk = (fv[k][0] + ph.tau * nn[0] * (ul[k] - ug[k])) * nn[0];
+#pragma unroll
+    for (int d = 1; d < D; d++) fnk = fnk + (fv[k][d] + ph.tau * nn[d] * (ul[k] - ug[k])) * nn[d];
+    *tl_p[t + n * k] += fnk * tal;
+  }
+}
+
 inline unsigned grid_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
 PhysT<double> phys_of(const fr_phys_desc* p)
@@ -454,6 +561,55 @@ fr_status fr_op_int_inters_common_viscFlux(int n_fpts_per_inter, int n_dims, int
   else
     common_vis_kernel<3><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_fpts_per_inter, n_inters, disu_fpts_l, disu_fpts_r, grad_disu_fpts_l, grad_disu_fpts_r, norm_tconf_fpts_l, norm_tconf_fpts_r, tdA_fpts_l, tdA_fpts_r, norm_fpts, phys_of(phys));
   return launched("common_vis_kernel");
+}
+
+fr_status fr_op_bdy_inters_common_invFlux(int n_fpts_per_inter, int n_dims, int n_fields, int n_inters,
+                                          double* const* disu_fpts_l, double* const* norm_tconf_fpts_l,
+                                          double* const* tdA_fpts_l, double* const* norm_fpts,
+                                          const int* boundary_type, const double* bdy_params,
+                                          double* const* delta_disu_fpts_l, const fr_phys_desc* phys, double R_ref,
+                                          int riemann_solve_type, int viscous, void* stream)
+{
+  if (!phys || !dims_ok(n_dims, n_fields) || n_fpts_per_inter < 0 || n_inters < 0)
+    return op_fail(FR_ERR_ARG, "bad arguments");
+  if (riemann_solve_type != 0 && riemann_solve_type != 2)
+    return op_fail(FR_ERR_UNSUPPORTED, "boundary fluxes: riemann_solve_type 0 (Rusanov) or 2 (Roe, 2-D)");
+  if (riemann_solve_type == 2 && n_dims != 2) return op_fail(FR_ERR_UNSUPPORTED, "Roe flux is 2-D only");
+  long long n = (long long)n_fpts_per_inter * n_inters;
+  if (n == 0) return FR_OK;
+  if (!disu_fpts_l || !norm_tconf_fpts_l || !tdA_fpts_l || !norm_fpts || !boundary_type || !bdy_params ||
+      (viscous && !delta_disu_fpts_l))
+    return op_fail(FR_ERR_ARG, "missing boundary table");
+  PhysT<double> ph = phys_of(phys);
+  ph.R_ref = R_ref;
+  if (n_dims == 2)
+    bdy_inv_kernel<2><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_fpts_per_inter, n_inters, disu_fpts_l, norm_tconf_fpts_l, tdA_fpts_l, norm_fpts, delta_disu_fpts_l, boundary_type, bdy_params, ph, riemann_solve_type, viscous);
+  else
+    bdy_inv_kernel<3><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_fpts_per_inter, n_inters, disu_fpts_l, norm_tconf_fpts_l, tdA_fpts_l, norm_fpts, delta_disu_fpts_l, boundary_type, bdy_params, ph, riemann_solve_type, viscous);
+  return launched("bdy_inv_kernel");
+}
+
+fr_status fr_op_bdy_inters_common_viscFlux(int n_fpts_per_inter, int n_dims, int n_fields, int n_inters,
+                                           double* const* disu_fpts_l, double* const* grad_disu_fpts_l,
+                                           double* const* norm_tconf_fpts_l, double* const* tdA_fpts_l,
+                                           double* const* norm_fpts, const int* boundary_type,
+                                           const double* bdy_params, const fr_phys_desc* phys, double R_ref,
+                                           void* stream)
+{
+  if (!phys || !dims_ok(n_dims, n_fields) || n_fpts_per_inter < 0 || n_inters < 0)
+    return op_fail(FR_ERR_ARG, "bad arguments");
+  long long n = (long long)n_fpts_per_inter * n_inters;
+  if (n == 0) return FR_OK;
+  if (!disu_fpts_l || !grad_disu_fpts_l || !norm_tconf_fpts_l || !tdA_fpts_l || !norm_fpts || !boundary_type ||
+      !bdy_params)
+    return op_fail(FR_ERR_ARG, "missing boundary table");
+  PhysT<double> ph = phys_of(phys);
+  ph.R_ref = R_ref;
+  if (n_dims == 2)
+    bdy_vis_kernel<2><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_fpts_per_inter, n_inters, disu_fpts_l, grad_disu_fpts_l, norm_tconf_fpts_l, tdA_fpts_l, norm_fpts, boundary_type, bdy_params, ph);
+  else
+    bdy_vis_kernel<3><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_fpts_per_inter, n_inters, disu_fpts_l, grad_disu_fpts_l, norm_tconf_fpts_l, tdA_fpts_l, norm_fpts, boundary_type, bdy_params, ph);
+  return launched("bdy_vis_kernel");
 }
 
 fr_status fr_op_advance_rk45(int n_upts, int n_fields, int n_eles, int stage, double dt, double const_src,

@@ -403,6 +403,35 @@ fr_status fr_op_int_inters_common_viscFlux(int n_fpts_per_inter, int n_dims, int
                                            double* const* tdA_fpts_l, double* const* tdA_fpts_r,
                                            double* const* norm_fpts, const fr_phys_desc* phys, void* stream);
 
+/* bdy_inters::evaluate_boundaryConditions_invFlux, include/bdy_inters.h:70;
+ * replaces evaluate_boundaryConditions_invFlux_gpu_kernel_wrapper,
+ * include/cuda_kernels.h:42 (static mesh, Euler/Navier-Stokes).  Tables as
+ * bdy_inters keeps them (src/bdy_inters.cpp:111-203): (n_fpts_per_inter,
+ * n_inters, n_fields) / (.., n_dims) device arrays of device pointers into the
+ * owning elements' flux-point arrays; boundary_type (n_inters) and the 14
+ * bdy_params of bdy_inters::set_bdy_params are device arrays.  Boundary types
+ * 1-7 and 11-16 (get_bc_number, src/geometry.cpp:121-148); riemann_solve_type
+ * 0 (central flux of own and ghost state) or 2 (Roe, 2-D).  Writes
+ * norm_tconf_fpts_l = f_n tdA and, with viscous != 0, the LDG common solution
+ * into delta_disu_fpts_l. */
+fr_status fr_op_bdy_inters_common_invFlux(int n_fpts_per_inter, int n_dims, int n_fields, int n_inters,
+                                          double* const* disu_fpts_l, double* const* norm_tconf_fpts_l,
+                                          double* const* tdA_fpts_l, double* const* norm_fpts,
+                                          const int* boundary_type, const double* bdy_params,
+                                          double* const* delta_disu_fpts_l, const fr_phys_desc* phys, double R_ref,
+                                          int riemann_solve_type, int viscous, void* stream);
+
+/* bdy_inters::evaluate_boundaryConditions_viscFlux, include/bdy_inters.h:76;
+ * replaces evaluate_boundaryConditions_viscFlux_gpu_kernel_wrapper,
+ * include/cuda_kernels.h:59 (no LES, no turbulence model):
+ * norm_tconf_fpts_l += (f_v + tau n (u_l - u_ghost)) . n tdA. */
+fr_status fr_op_bdy_inters_common_viscFlux(int n_fpts_per_inter, int n_dims, int n_fields, int n_inters,
+                                           double* const* disu_fpts_l, double* const* grad_disu_fpts_l,
+                                           double* const* norm_tconf_fpts_l, double* const* tdA_fpts_l,
+                                           double* const* norm_fpts, const int* boundary_type,
+                                           const double* bdy_params, const fr_phys_desc* phys, double R_ref,
+                                           void* stream);
+
 /* eles::AdvanceSolution(stage, adv_type 3), include/eles.h:157; replaces
  * RK45_update_kernel_wrapper, include/cuda_kernels.h:30 (fixed dt):
  * res = a_s res + dt (-div/detjac + const_src + src); u += b_s res.

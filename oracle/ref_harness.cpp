@@ -225,6 +225,25 @@ static void dump_setup(solution& S)
     vector<int> shape; shape.push_back(6); shape.push_back(I.n_fpts_per_inter); shape.push_back(I.n_inters);
     dump_ints(b, v, shape);
   }
+
+  // boundary interfaces: (type, ele, fpt) of the owning side of every
+  // boundary flux point and the interface's boundary type
+  // (bdy_inters::set_boundary, src/bdy_inters.cpp:111-203).
+  for (int it = 0; it < S.n_bdy_inter_types; it++) {
+    bdy_inters& B = S.mesh_bdy_inters(it);
+    if (B.n_inters == 0) continue;
+    vector<int> v;
+    for (int i = 0; i < B.n_inters; i++)
+      for (int j = 0; j < B.n_fpts_per_inter; j++) {
+        int tl, el, fl;
+        locate(S, B.disu_fpts_l(j, i, 0), false, tl, el, fl);
+        int row[4] = {tl, el, fl, B.boundary_type(i)};
+        v.insert(v.end(), row, row + 4);
+      }
+    char b[32]; snprintf(b, sizeof b, "bdy_inters_%d", it);
+    vector<int> shape; shape.push_back(4); shape.push_back(B.n_fpts_per_inter); shape.push_back(B.n_inters);
+    dump_ints(b, v, shape);
+  }
 }
 
 static void dump_stage(solution& S, const char* tag, const char* what)

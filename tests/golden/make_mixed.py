@@ -178,6 +178,12 @@ CASES = [
     dict(name="mixed_pritet_p3", kind="pritet", order=3, n=(2, 3, 2), jitter=0.1, steps=3, dt=1e-3, tet_upts=0),
     dict(name="mixed_pritet_p2", kind="pritet", order=2, n=(2, 4, 2), jitter=0.15, steps=3, dt=1e-3, tet_upts=1),
     dict(name="mixed_hexpri_p3", kind="hexpri", order=3, n=(4, 2, 2), jitter=0.1, steps=3, dt=1e-3, tet_upts=0),
+    # channel: isothermal wall at y = 0, adiabatic wall at y = 2 pi, on the
+    # prisms' triangular faces; periodic in x and z
+    dict(name="mixed_channel_p2", kind="pritet", order=2, n=(3, 4, 2), jitter=0.15, steps=3, dt=1e-3, tet_upts=0,
+         side_bc=(0, 0, 11, 12, 0, 0), ic="channel_mach01"),
+    dict(name="mixed_channel_p3", kind="pritet", order=3, n=(2, 3, 2), jitter=0.1, steps=2, dt=1e-3, tet_upts=1,
+         side_bc=(0, 0, 11, 12, 0, 0), ic="channel_mach01"),
 ]
 
 # arrays kept per element type (prefix t<ele_type>_ in the harness output)
@@ -192,7 +198,7 @@ def run_case(ref, c, work):
     os.makedirs(d, exist_ok=True)
     lo, hi = (0.0, 0.0, 0.0), (2 * np.pi,) * 3
     xv, eles = mixed_cells(c["kind"], c["n"], lo, hi, c["jitter"], seed=12345)
-    write_mixed_gambit(os.path.join(d, "mesh.neu"), xv, eles)
+    write_mixed_gambit(os.path.join(d, "mesh.neu"), xv, eles, c.get("side_bc"))
     L = [hi[i] - lo[i] for i in range(3)]
     vals = {
         "equation": 0, "viscous": 1, "riemann_solve_type": 0, "vis_riemann_solve_type": 0, "ic_form": 7,
@@ -204,11 +210,16 @@ def run_case(ref, c, work):
         "prandtl": 0.71, "Mach_free_stream": 0.1, "Re_free_stream": 1600.0, "gamma": 1.4, "fix_vis": 1,
         "res_norm_type": 1,
     }
+    if c.get("side_bc"):
+        # free stream along x, wall temperature = free-stream temperature
+        vals.update({"nx_free_stream": 1.0, "ny_free_stream": 0.0, "nz_free_stream": 0.0, "Mach_wall": 0.0,
+                     "nx_wall": 1.0, "ny_wall": 0.0, "nz_wall": 0.0, "rho_bound": 1.0, "u_bound": 1.0,
+                     "v_bound": 0.0, "w_bound": 0.0, "p_bound": 1.0, "T_wall": 300.0, "T_free_stream": 300.0})
     G.write_input(os.path.join(d, "input"), os.path.join(ref, G.TGV_INPUT), vals)
     out = os.path.join(d, "out")
     os.makedirs(out, exist_ok=True)
     env = dict(os.environ, HIFILES_HOME=os.path.join(REPO, "oracle", "_ref"))
-    args = [G.HARNESS, "input", out, "--ic", "tgv_mach01", "--steps", str(c["steps"]), "--stages"]
+    args = [G.HARNESS, "input", out, "--ic", c.get("ic", "tgv_mach01"), "--steps", str(c["steps"]), "--stages"]
     r = subprocess.run(args, cwd=d, env=env, capture_output=True, text=True)
     if r.returncode != 0:
         print(r.stdout[-3000:], r.stderr[-3000:])
@@ -249,11 +260,22 @@ def main():
             if key in arr:
                 fx[key] = arr[key]
                 inters.append(dict(index=it, n_fpts=int(arr[key].shape[1]), n_inters=int(arr[key].shape[2])))
+        bdys = []
+        for it in range(8):
+            key = "bdy_inters_%d" % it
+            if key in arr:
+                fx[key] = arr[key]
+                bdys.append(dict(index=it, n_fpts=int(arr[key].shape[1]), n_inters=int(arr[key].shape[2])))
         fx["res_norms"] = arr["res_norms"]
         meta = dict(c)
         meta["n"] = list(c["n"])
         meta["types"] = types
         meta["inters"] = inters
+        meta["bdy_inters"] = bdys
+        meta["bdy"] = [par.get("bdy%d" % i, 0.0) for i in range(14)]
+        meta["R_ref"] = par.get("R_ref", 1.0)
+        if c.get("side_bc"):
+            meta["side_bc"] = list(c["side_bc"])
         meta["physics"] = {k: par[k] for k in ("gamma", "prandtl", "mu_inf", "rt_inf", "c_sth", "fix_vis", "tau",
                                                  "pen_fact")}
         meta["element_counts"] = {str(gt): sum(1 for e in eles if e[0] == gt) for gt in (4, 5, 6)}
