@@ -251,7 +251,61 @@ def measure_forms(a, dev, fp64_value, s64, u0):
                     "[2, 4] drawn with seed %d; DOF-updates per RK stage over all instances" % (BATCH_N, BATCH_SEED))
     out["operator_path"] = measure_operator_path(a, dev, s64, u0)
     out["tgv64_p4"] = measure_tgv64_p4(dev)
+    out["mixed_channel"] = {name: measure_mixed_channel(name) for name in ("mixed_channel_p2", "mixed_channel_p3")}
     return out
+
+
+def measure_mixed_channel(case, target_dofs=10_000_000, steps=2, err_steps=10):
+    """The mixed tet/prism channel (isothermal and adiabatic walls on the
+    prisms' triangular faces, jittered vertices, periodic in x and z) through
+    the per-operator entry points: operators, metrics and wiring as the
+    reference's eles_tets / eles_pris / bdy_inters set them up (the committed
+    fixture of one small channel), tiled into independent copies up to
+    about 10 M DOFs.  FP64 operator products on the CUDA cores against BF16x3
+    and BF16x6 split products on the tensor cores, with their L2 error
+    against FP64 after `err_steps` steps."""
+    import json as _json
+    import torch
+    from hifiles_b200 import seam
+    z = np.load(os.path.join(REPO, "tests", "golden", case + ".npz"))
+    meta = _json.loads(str(z["meta"]))
+    arrs = {k: np.asfortranarray(z[k]) for k in z.files if k != "meta"}
+    types, ints, bdys = seam.mixed_mesh_inputs(meta, arrs)
+    dofs_one = sum(t["u"].size for t in types.values())
+    copies = max(1, target_dofs // dofs_one)
+    tt, ti, tb = seam.tile_mixed_mesh(types, ints, bdys, copies)
+    m = seam.MixedOperatorMesh(tt, ti, meta["physics"], tb, meta["bdy"], meta["R_ref"])
+    u0 = {i: m.S[i]["u"].clone() for i in m.S}
+
+    def reset():
+        for i, s in m.S.items():
+            s["u"].copy_(u0[i])
+            s["reg"].zero_()
+
+    dt = meta["dt"]
+    res = {}
+    for mode, name in ((0, "fp64"), (1, "bf16x3"), (2, "bf16x6")):
+        reset()
+        m.advance(1, dt, gemm_precision=mode)
+        ms = _time_steps(lambda k: m.advance(k, dt, gemm_precision=mode), m.stream, steps)
+        res[name] = {"value": m.dofs * 5 / (ms * 1e-3), "ms_per_step": ms}
+    reset()
+    m.advance(err_steps, dt, gemm_precision=0)
+    ref = {i: s["u"].clone() for i, s in m.S.items()}
+    for mode, name in ((1, "bf16x3"), (2, "bf16x6")):
+        reset()
+        m.advance(err_steps, dt, gemm_precision=mode)
+        num = sum(float(torch.linalg.vector_norm(s["u"] - ref[i]) ** 2) for i, s in m.S.items())
+        den = sum(float(torch.linalg.vector_norm(ref[i]) ** 2) for i in m.S)
+        res[name]["l2_rel_vs_fp64_after_%d_steps" % err_steps] = (num / den) ** 0.5
+    cnt = meta["element_counts"]
+    res["workload"] = ("%d copies of a %s channel of order %d (%s tets, %s prisms per copy; isothermal wall at y = 0, "
+                       "adiabatic at y = 2 pi), %d DOFs; one step = 5 RK stages of CalcResidual through the fr_op_* "
+                       "entry points" % (copies, "x".join(str(v) for v in meta["n"]), meta["order"], cnt["6"],
+                                         cnt["5"], m.dofs))
+    del m
+    torch.cuda.empty_cache()
+    return res
 
 
 def measure_tgv64_p4(dev, n=64, P=4, steps=100, dt=2e-4):

@@ -37,42 +37,84 @@ fr_status launched(const char* what)
 }
 
 constexpr int kTileCols = 32;
+constexpr int kTileStride = kTileCols + 1;  // staged B rows padded: the column-major copy-in is conflict-free
 constexpr int kDenseThreads = 256;
 
 // C(:, j) = beta*C(:, j) + A * B(:, j) for all ncols columns, A (m x k) column
 // major, B (k x ncols) and C (m x ncols) with leading dimensions k and m (the
 // reference's cublasDgemm('N','N', m, ncols, k, 1, A, m, B, k, beta, C, m)).
-// A column tile of B and C is staged through shared memory so both global
-// streams are contiguous; A is read through the read-only cache (every lane
-// of a warp reads the same entry).  Summation runs over l in increasing order.
+// A tile of 32 columns of B and C is staged through shared memory so both
+// global streams are contiguous.  Each thread keeps an RM x 4 register tile:
+// rows r0 + 32 i (i < RM; r0 = lane, then lane + 32 RM ... while rows remain)
+// and columns warp + 8 j (j < 4), so per term l a
+// warp reads 4 broadcast entries of B from shared memory and RM coalesced
+// 32-row slices of A's column l (read-only cache), for 4 RM fused
+// multiply-adds.  Every output is one fma chain over l in increasing order.
+template <int RM>
 __global__ void __launch_bounds__(kDenseThreads)
 dense_apply_kernel(int m, int k, long long ncols, const double* __restrict__ A, const double* __restrict__ B,
                    double* __restrict__ Cm, int beta)
 {
   extern __shared__ double sm[];
-  double* sB = sm;                         // [k][kTileCols]
-  double* sC = sm + (size_t)k * kTileCols; // [kTileCols][m]
-  long long c0 = (long long)blockIdx.x * kTileCols;
-  int nc = (int)min((long long)kTileCols, ncols - c0);
+  double* sB = sm;                           // [k][kTileStride]
+  double* sC = sm + (size_t)k * kTileStride; // [kTileCols][m]
+  const long long c0 = (long long)blockIdx.x * kTileCols;
+  const int nc = (int)min((long long)kTileCols, ncols - c0);
   const double* Bt = B + (size_t)c0 * k;
   for (int i = threadIdx.x; i < nc * k; i += kDenseThreads) {
     int c = i / k, l = i - c * k;
-    sB[l * kTileCols + c] = Bt[i];
+    sB[l * kTileStride + c] = Bt[i];
   }
   double* Ct = Cm + (size_t)c0 * m;
   if (beta)
     for (int i = threadIdx.x; i < nc * m; i += kDenseThreads) sC[i] = Ct[i];
   __syncthreads();
-  int c = threadIdx.x % kTileCols;
-  for (int r = threadIdx.x / kTileCols; r < m; r += kDenseThreads / kTileCols) {
-    if (c < nc) {
-      double acc = beta ? sC[c * m + r] : 0.0;
-      for (int l = 0; l < k; l++) acc = fma(sB[l * kTileCols + c], __ldg(A + r + (size_t)m * l), acc);
-      sC[c * m + r] = acc;
+  const int lane = threadIdx.x & 31, wc = threadIdx.x >> 5;
+  // row passes of 32 RM rows (one pass for m <= 32 RM)
+  for (int r0 = lane; r0 < m; r0 += 32 * RM) {
+    double acc[RM][4];
+#pragma unroll
+    for (int i = 0; i < RM; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int r = r0 + 32 * i, c = wc + 8 * j;
+        acc[i][j] = (beta && r < m && c < nc) ? sC[c * m + r] : 0.0;
+      }
+    const double* Ar = A + r0;
+    for (int l = 0; l < k; l++) {
+      double b[4], a[RM];
+#pragma unroll
+      for (int j = 0; j < 4; j++) b[j] = sB[l * kTileStride + wc + 8 * j];
+#pragma unroll
+      for (int i = 0; i < RM; i++) a[i] = (r0 + 32 * i < m) ? __ldg(Ar + 32 * i + (size_t)m * l) : 0.0;
+#pragma unroll
+      for (int i = 0; i < RM; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = fma(b[j], a[i], acc[i][j]);
     }
+#pragma unroll
+    for (int i = 0; i < RM; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int r = r0 + 32 * i, c = wc + 8 * j;
+        if (r < m && c < nc) sC[c * m + r] = acc[i][j];
+      }
   }
   __syncthreads();
   for (int i = threadIdx.x; i < nc * m; i += kDenseThreads) Ct[i] = sC[i];
+}
+
+template <int RM>
+fr_status dense_launch(int m, int k, long long ncols, const double* A, const double* B, double* Cm, int beta,
+                       cudaStream_t s, size_t smem, unsigned blocks)
+{
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(dense_apply_kernel<RM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return op_fail(FR_ERR_CUDA, cudaGetErrorString(e));
+  }
+  dense_apply_kernel<RM><<<blocks, kDenseThreads, smem, s>>>(m, k, ncols, A, B, Cm, beta);
+  return launched("dense_apply_kernel");
 }
 
 // Precision of the operator products of this seam: 0 = FP64 (dense_apply_kernel),
@@ -86,16 +128,21 @@ fr_status dense_apply(int m, int k, long long ncols, const double* A, const doub
   if (m <= 0 || k <= 0 || ncols < 0 || !A || !B || !Cm) return op_fail(FR_ERR_ARG, "bad operator arguments");
   if (ncols == 0) return FR_OK;
   if (g_gemm_mode) return gemm_bf16x3(m, k, ncols, A, B, Cm, beta, s, g_gemm_mode == 2 ? 6 : 3);
-  size_t smem = ((size_t)k * kTileCols + (size_t)kTileCols * m) * sizeof(double);
+  size_t smem = ((size_t)k * kTileStride + (size_t)kTileCols * m) * sizeof(double);
   if (smem > 220 * 1024) return op_fail(FR_ERR_UNSUPPORTED, "operator too large for one column tile");
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(dense_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return op_fail(FR_ERR_CUDA, cudaGetErrorString(e));
-  }
   long long blocks = (ncols + kTileCols - 1) / kTileCols;
   if (blocks > 2147483647LL) return op_fail(FR_ERR_ARG, "too many columns");
-  dense_apply_kernel<<<(unsigned)blocks, kDenseThreads, smem, s>>>(m, k, ncols, A, B, Cm, beta);
-  return launched("dense_apply_kernel");
+  const unsigned nb = (unsigned)blocks;
+  switch ((m + 31) / 32) {
+    case 1: return dense_launch<1>(m, k, ncols, A, B, Cm, beta, s, smem, nb);
+    case 2: return dense_launch<2>(m, k, ncols, A, B, Cm, beta, s, smem, nb);
+    case 3: return dense_launch<3>(m, k, ncols, A, B, Cm, beta, s, smem, nb);
+    case 4: return dense_launch<4>(m, k, ncols, A, B, Cm, beta, s, smem, nb);
+    case 5: return dense_launch<5>(m, k, ncols, A, B, Cm, beta, s, smem, nb);
+    case 6: return dense_launch<6>(m, k, ncols, A, B, Cm, beta, s, smem, nb);
+    case 7: return dense_launch<7>(m, k, ncols, A, B, Cm, beta, s, smem, nb);
+    default: return dense_launch<8>(m, k, ncols, A, B, Cm, beta, s, smem, nb);
+  }
 }
 
 // ------------------------------------------------------------ pointwise kernels

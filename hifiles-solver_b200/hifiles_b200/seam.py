@@ -222,3 +222,216 @@ class OperatorStage:
                 self._ok(L.fr_op_advance_rk45(self.nu, self.F, self.E, k, float(dt), 0.0, P(self.u), P(self.reg),
                                               P(self.div), P(self.dj), None, sp))
         self._ok(L.fr_op_check(sp))
+
+
+def _bind_bdy(L):
+    i, vp = C.c_int, _VP
+    L.fr_op_bdy_inters_common_invFlux.argtypes = [i, i, i, i] + [vp] * 7 + [vp, C.c_double, i, i, vp]
+    L.fr_op_bdy_inters_common_viscFlux.argtypes = [i, i, i, i] + [vp] * 7 + [vp, C.c_double, vp]
+    L.fr_op_bdy_inters_common_invFlux.restype = C.c_int
+    L.fr_op_bdy_inters_common_viscFlux.restype = C.c_int
+    return L
+
+
+class MixedOperatorMesh:
+    """A mesh of several element types (tets, prisms, hexes, ...) advanced
+    through the per-operator entry points, in the order of CalcResidual
+    (src/solver.cpp:65-225): every element type for each element step, every
+    interface type for each interface step.
+
+    `types` maps the caller's element-type index to a dict with that type's
+    dense operators as the caller's classes build them (opp_0, opp_3, opp_6;
+    lists of n_dims matrices opp_1, opp_2, opp_4, opp_5), its metrics
+    (JGinv_upts, detjac_upts, tdA_fpts, norm_fpts) and its state u
+    (n_upts, n_eles, n_fields).  `int_inters` lists int32 arrays
+    (6, n_fpts_per_inter, n_inters) of (type, element, flux point) of the left
+    and right side of every interface point (int_inters' pointer tables,
+    src/int_inters.cpp:95-178, as indices); `bdy_inters` lists
+    (4, n_fpts_per_inter, n_inters) arrays of the owning side's triple and the
+    boundary type (bdy_inters, src/bdy_inters.cpp:111-203), whose boundary
+    values `bdy` (14, bdy_inters::set_bdy_params order) and gas constant
+    `R_ref` apply.  Navier-Stokes; the state lives on the device."""
+
+    def __init__(self, types, int_inters, physics, bdy_inters=(), bdy=None, R_ref=1.0, device=0):
+        import torch
+        self.torch = torch
+        self.L = _bind_bdy(_bind(lib()))
+        dev = "cuda:%d" % device
+        self.dev = dev
+        D = 3
+        F = 5
+        self.D, self.F = D, F
+        t = lambda a: torch.from_numpy(np.asfortranarray(a, dtype=np.float64).ravel(order="F").copy()).to(dev)  # noqa
+        z = lambda n: torch.zeros(n, dtype=torch.float64, device=dev)  # noqa: E731
+        self.S = {}
+        for i, ty in types.items():
+            nu, E, _ = ty["u"].shape
+            nf = ty["opp_0"].shape[0]
+            s = dict(nu=nu, nf=nf, E=E)
+            for k in ("opp_0", "opp_3", "opp_6"):
+                s[k] = t(ty[k])
+            for k in ("opp_1", "opp_2", "opp_4", "opp_5"):
+                s[k] = [t(a) for a in ty[k]]
+                s[k + "_tab"] = (C.c_void_p * D)(*[a.data_ptr() for a in s[k]])
+            s["JG"], s["dj"], s["tdA"], s["nrm"] = (t(ty[k]) for k in ("JGinv_upts", "detjac_upts", "tdA_fpts",
+                                                                         "norm_fpts"))
+            s["u"], s["reg"], s["div"] = t(ty["u"]), z(nu * E * F), z(nu * E * F)
+            s["ufp"], s["ntc"], s["ntd"], s["ddu"] = z(nf * E * F), z(nf * E * F), z(nf * E * F), z(nf * E * F)
+            s["tf"], s["gup"], s["gfp"] = z(nu * E * F * D), z(nu * E * F * D), z(nf * E * F * D)
+            self.S[i] = s
+
+        def table(w, side, arr, comps):
+            tt, e, f = (np.asarray(w[side + q]).reshape(-1, order="F").astype(np.int64) for q in range(3))
+            rows = np.zeros((tt.size, comps), dtype=np.int64)
+            for i, s in self.S.items():
+                m = tt == i
+                if m.any():
+                    slot = f[m] + s["nf"] * e[m]
+                    rows[m] = s[arr].data_ptr() + 8 * (slot[:, None] + s["nf"] * s["E"] * np.arange(comps)[None, :])
+            return torch.from_numpy(np.asfortranarray(rows).ravel(order="F").copy()).to(dev)
+
+        self.inters = []
+        for w in int_inters:
+            tb = dict(nfpi=int(w.shape[1]), ni=int(w.shape[2]))
+            for side, sx in ((0, "l"), (3, "r")):
+                tb["u" + sx], tb["t" + sx] = table(w, side, "ufp", F), table(w, side, "ntc", F)
+                tb["d" + sx], tb["g" + sx] = table(w, side, "ddu", F), table(w, side, "gfp", F * D)
+                tb["a" + sx] = table(w, side, "tdA", 1)
+            tb["n"] = table(w, 0, "nrm", D)
+            self.inters.append(tb)
+        self.bdys = []
+        for w in bdy_inters:
+            tb = dict(nfpi=int(w.shape[1]), ni=int(w.shape[2]))
+            tb["ul"], tb["tl"], tb["dl"] = table(w, 0, "ufp", F), table(w, 0, "ntc", F), table(w, 0, "ddu", F)
+            tb["gl"], tb["al"], tb["n"] = table(w, 0, "gfp", F * D), table(w, 0, "tdA", 1), table(w, 0, "nrm", D)
+            tb["type"] = torch.from_numpy(np.ascontiguousarray(np.asarray(w)[3, 0, :]).astype(np.int32)).to(dev)
+            self.bdys.append(tb)
+        self.bdy = torch.tensor(list(bdy) if bdy is not None else [0.0] * 14, dtype=torch.float64, device=dev)
+        self.R_ref = float(R_ref)
+        self.ph = PhysDesc(**physics)
+        self.stream = torch.cuda.current_stream(dev)
+
+    @property
+    def dofs(self):
+        """Solution DOFs (points x fields) over all element types."""
+        return sum(s["nu"] * s["E"] * self.F for s in self.S.values())
+
+    def get_state(self, i):
+        self.torch.cuda.synchronize()
+        s = self.S[i]
+        return s["u"].cpu().numpy().reshape((s["nu"], s["E"], self.F), order="F")
+
+    def _ok(self, st):
+        if st != 0:
+            raise RuntimeError(lib().fr_last_error().decode())
+
+    def residual(self, gemm_precision=0):
+        """div_tconf_upts of every element type (CalcResidual)."""
+        L, P, ok, D, F = self.L, (lambda a: a.data_ptr()), self._ok, self.D, self.F
+        sp = C.c_void_p(self.stream.cuda_stream)
+        ph = C.byref(self.ph)
+        cast = lambda tab: C.cast(tab, _VP)  # noqa: E731
+        ok(L.fr_op_set_gemm_precision(int(gemm_precision)))
+        try:
+            for s in self.S.values():
+                nu, nf, E = s["nu"], s["nf"], s["E"]
+                ok(L.fr_op_extrapolate_solution(nf, nu, F, E, P(s["opp_0"]), P(s["u"]), P(s["ufp"]), sp))
+                ok(L.fr_op_calculate_gradient(nu, D, F, E, cast(s["opp_4_tab"]), P(s["u"]), P(s["gup"]), sp))
+                ok(L.fr_op_evaluate_invFlux(nu, D, F, E, P(s["u"]), P(s["JG"]), P(s["tf"]), ph, sp))
+            for tb in self.inters:
+                ok(L.fr_op_int_inters_common_invFlux(tb["nfpi"], D, F, tb["ni"], P(tb["ul"]), P(tb["ur"]),
+                                                     P(tb["tl"]), P(tb["tr"]), P(tb["al"]), P(tb["ar"]), P(tb["n"]),
+                                                     P(tb["dl"]), P(tb["dr"]), ph, 1, sp))
+            for tb in self.bdys:
+                ok(L.fr_op_bdy_inters_common_invFlux(tb["nfpi"], D, F, tb["ni"], P(tb["ul"]), P(tb["tl"]),
+                                                     P(tb["al"]), P(tb["n"]), P(tb["type"]), P(self.bdy),
+                                                     P(tb["dl"]), ph, self.R_ref, 0, 1, sp))
+            for s in self.S.values():
+                nu, nf, E = s["nu"], s["nf"], s["E"]
+                ok(L.fr_op_correct_gradient(nu, nf, D, F, E, cast(s["opp_5_tab"]), P(s["ddu"]), P(s["JG"]),
+                                            P(s["dj"]), P(s["gup"]), sp))
+                ok(L.fr_op_extrapolate_corrected_gradient(nf, nu, D, F, E, P(s["opp_6"]), P(s["gup"]), P(s["gfp"]),
+                                                          sp))
+                ok(L.fr_op_evaluate_viscFlux(nu, D, F, E, P(s["u"]), P(s["gup"]), P(s["JG"]), P(s["tf"]), ph, sp))
+                ok(L.fr_op_extrapolate_totalFlux(nf, nu, D, F, E, cast(s["opp_1_tab"]), P(s["tf"]), P(s["ntd"]), sp))
+                ok(L.fr_op_calculate_divergence(nu, D, F, E, cast(s["opp_2_tab"]), P(s["tf"]), P(s["div"]), sp))
+            for tb in self.inters:
+                ok(L.fr_op_int_inters_common_viscFlux(tb["nfpi"], D, F, tb["ni"], P(tb["ul"]), P(tb["ur"]),
+                                                      P(tb["gl"]), P(tb["gr"]), P(tb["tl"]), P(tb["tr"]),
+                                                      P(tb["al"]), P(tb["ar"]), P(tb["n"]), ph, sp))
+            for tb in self.bdys:
+                ok(L.fr_op_bdy_inters_common_viscFlux(tb["nfpi"], D, F, tb["ni"], P(tb["ul"]), P(tb["gl"]),
+                                                      P(tb["tl"]), P(tb["al"]), P(tb["n"]), P(tb["type"]),
+                                                      P(self.bdy), ph, self.R_ref, sp))
+            for s in self.S.values():
+                ok(L.fr_op_calculate_corrected_divergence(s["nu"], s["nf"], F, s["E"], P(s["opp_3"]), P(s["ntd"]),
+                                                          P(s["ntc"]), P(s["div"]), sp))
+        finally:
+            L.fr_op_set_gemm_precision(0)
+
+    def advance(self, n_steps, dt, gemm_precision=0):
+        """n_steps RK45 steps (5 stages each), eles::AdvanceSolution per type."""
+        L, P = self.L, (lambda a: a.data_ptr())
+        sp = C.c_void_p(self.stream.cuda_stream)
+        for _ in range(n_steps):
+            for k in range(5):
+                self.residual(gemm_precision)
+                for s in self.S.values():
+                    self._ok(L.fr_op_advance_rk45(s["nu"], self.F, s["E"], k, float(dt), 0.0, P(s["u"]),
+                                                  P(s["reg"]), P(s["div"]), P(s["dj"]), None, sp))
+        self._ok(L.fr_op_check(sp))
+
+
+def tile_mixed_mesh(types, int_inters, bdy_inters, copies):
+    """`copies` independent copies of a mixed mesh (element axis tiled, every
+    copy's interfaces wired to its own elements), for throughput runs on a
+    mesh whose operators and metrics come from one small set-up."""
+    out = {}
+    for i, ty in types.items():
+        E = ty["u"].shape[1]
+        o = {k: ty[k] for k in ("opp_0", "opp_1", "opp_2", "opp_3", "opp_4", "opp_5", "opp_6")}
+        o["JGinv_upts"] = np.tile(ty["JGinv_upts"], (1, 1, 1, copies))
+        o["detjac_upts"] = np.tile(ty["detjac_upts"], (1, copies))
+        o["tdA_fpts"] = np.tile(ty["tdA_fpts"], (1, copies))
+        o["norm_fpts"] = np.tile(ty["norm_fpts"], (1, copies, 1))
+        o["u"] = np.tile(ty["u"], (1, copies, 1))
+        o["_E"] = E
+        out[i] = o
+
+    def shift(w, sides):
+        w = np.asarray(w)
+        parts = []
+        for c in range(copies):
+            x = w.copy()
+            for s in sides:
+                for i, o in out.items():
+                    m = x[s] == i
+                    x[s + 1][m] += c * o["_E"]
+            parts.append(x)
+        return np.concatenate(parts, axis=2)
+
+    ints = [shift(w, (0, 3)) for w in int_inters]
+    bdys = [shift(w, (0,)) for w in bdy_inters]
+    for o in out.values():
+        del o["_E"]
+    return out, ints, bdys
+
+
+def mixed_mesh_inputs(meta, arrays, state_key="disu_upts_init"):
+    """(types, int_inters, bdy_inters) for MixedOperatorMesh from arrays named
+    as the reference's objects dump them: per element type with ele_type et,
+    t<et>_opp_0, t<et>_opp_<w>_<d>, t<et>_JGinv_upts ... t<et>_<state_key>;
+    int_inters_<k> / bdy_inters_<k> wiring; `meta` lists the element types
+    ({"index", "ele_type"}), interface and boundary types ({"index"})."""
+    types = {}
+    for t in meta["types"]:
+        X = "t%d_" % t["ele_type"]
+        ty = {k: arrays[X + k] for k in ("opp_0", "opp_3", "opp_6", "JGinv_upts", "detjac_upts", "tdA_fpts",
+                                         "norm_fpts")}
+        for w in (1, 2, 4, 5):
+            ty["opp_%d" % w] = [arrays[X + "opp_%d_%d" % (w, d)] for d in range(3)]
+        ty["u"] = arrays[X + state_key]
+        types[t["index"]] = ty
+    ints = [arrays["int_inters_%d" % it["index"]] for it in meta["inters"]]
+    bdys = [arrays["bdy_inters_%d" % it["index"]] for it in meta.get("bdy_inters", [])]
+    return types, ints, bdys

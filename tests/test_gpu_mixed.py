@@ -242,3 +242,51 @@ def test_mixed_mesh_through_the_operator_seam_matches_the_reference(case):
         assert rel(u, a[X + "final_disu_upts0"]) <= 1e-14
         # the change over three steps, not only the state, agrees
         assert rel(u - u0, a[X + "final_disu_upts0"] - u0) <= 1e-10
+
+
+@pytest.mark.parametrize("case", ["mixed_channel_p2", "mixed_hexpri_p3"])
+def test_tiled_mixed_mesh_wires_each_copy_to_itself(case):
+    import hifiles_b200.seam as SM
+    meta, a = load(case)
+    types, ints, bdys = SM.mixed_mesh_inputs(meta, a)
+    K = 3
+    tt, ti, tb = SM.tile_mixed_mesh(types, ints, bdys, K)
+    for i, ty in types.items():
+        E = ty["u"].shape[1]
+        assert tt[i]["u"].shape[1] == K * E
+        assert np.array_equal(tt[i]["JGinv_upts"][..., E:2 * E], ty["JGinv_upts"])
+    for w, w3 in zip(ints + bdys, ti + tb):
+        ni = w.shape[2]
+        assert w3.shape[2] == K * ni
+        for c in range(K):
+            blk = w3[:, :, c * ni:(c + 1) * ni]
+            for s in ((0, 3) if w.shape[0] == 6 else (0,)):
+                assert np.array_equal(blk[s], w[s]) and np.array_equal(blk[s + 2], w[s + 2])
+                for i, ty in types.items():
+                    m = w[s] == i
+                    assert np.array_equal(blk[s + 1][m], w[s + 1][m] + c * ty["u"].shape[1])
+
+
+@pytest.mark.gpu
+def test_mixed_mesh_driver_matches_the_reference_and_its_copies():
+    """The package driver used for throughput runs (seam.MixedOperatorMesh):
+    the reference's final state of the wall channel, and every copy of a tiled
+    mesh bit for bit equal to the single mesh."""
+    import hifiles_b200.seam as SM
+    meta, a = load("mixed_channel_p2")
+    types, ints, bdys = SM.mixed_mesh_inputs(meta, a)
+    m = SM.MixedOperatorMesh(types, ints, meta["physics"], bdys, meta["bdy"], meta["R_ref"])
+    m.advance(meta["steps"], meta["dt"])
+    one = {}
+    for t in meta["types"]:
+        one[t["index"]] = m.get_state(t["index"])
+        assert rel(one[t["index"]], a["t%d_final_disu_upts0" % t["ele_type"]]) <= 1e-14
+    K = 3
+    tt, ti, tb = SM.tile_mixed_mesh(types, ints, bdys, K)
+    m3 = SM.MixedOperatorMesh(tt, ti, meta["physics"], tb, meta["bdy"], meta["R_ref"])
+    m3.advance(meta["steps"], meta["dt"])
+    for i, u1 in one.items():
+        u3 = m3.get_state(i)
+        E = u1.shape[1]
+        for c in range(K):
+            assert np.array_equal(u3[:, c * E:(c + 1) * E], u1)
