@@ -49,8 +49,11 @@ constexpr int kDenseThreads = 256;
 // and columns warp + 8 j (j < 4), so per term l a
 // warp reads 4 broadcast entries of B from shared memory and RM coalesced
 // 32-row slices of A's column l (read-only cache), for 4 RM fused
-// multiply-adds.  Every output is one fma chain over l in increasing order.
-template <int RM>
+// multiply-adds.  With SA (operators of up to kSmallOp entries) A itself is
+// copied to shared memory first and read from there.  Every output is one fma
+// chain over l in increasing order.
+constexpr int kSmallOp = 4096;
+template <int RM, bool SA>
 __global__ void __launch_bounds__(kDenseThreads)
 dense_apply_kernel(int m, int k, long long ncols, const double* __restrict__ A, const double* __restrict__ B,
                    double* __restrict__ Cm, int beta)
@@ -58,6 +61,9 @@ dense_apply_kernel(int m, int k, long long ncols, const double* __restrict__ A, 
   extern __shared__ double sm[];
   double* sB = sm;                           // [k][kTileStride]
   double* sC = sm + (size_t)k * kTileStride; // [kTileCols][m]
+  double* sA = sC + (size_t)kTileCols * m;   // [k][m] when SA
+  if (SA)
+    for (int i = threadIdx.x; i < m * k; i += kDenseThreads) sA[i] = __ldg(A + i);
   const long long c0 = (long long)blockIdx.x * kTileCols;
   const int nc = (int)min((long long)kTileCols, ncols - c0);
   const double* Bt = B + (size_t)c0 * k;
@@ -80,13 +86,14 @@ dense_apply_kernel(int m, int k, long long ncols, const double* __restrict__ A, 
         const int r = r0 + 32 * i, c = wc + 8 * j;
         acc[i][j] = (beta && r < m && c < nc) ? sC[c * m + r] : 0.0;
       }
-    const double* Ar = A + r0;
+    const double* Ar = (SA ? sA : A) + r0;
     for (int l = 0; l < k; l++) {
       double b[4], a[RM];
 #pragma unroll
       for (int j = 0; j < 4; j++) b[j] = sB[l * kTileStride + wc + 8 * j];
 #pragma unroll
-      for (int i = 0; i < RM; i++) a[i] = (r0 + 32 * i < m) ? __ldg(Ar + 32 * i + (size_t)m * l) : 0.0;
+      for (int i = 0; i < RM; i++)
+        a[i] = (r0 + 32 * i < m) ? (SA ? Ar[32 * i + (size_t)m * l] : __ldg(Ar + 32 * i + (size_t)m * l)) : 0.0;
 #pragma unroll
       for (int i = 0; i < RM; i++)
 #pragma unroll
@@ -108,12 +115,14 @@ template <int RM>
 fr_status dense_launch(int m, int k, long long ncols, const double* A, const double* B, double* Cm, int beta,
                        cudaStream_t s, size_t smem, unsigned blocks)
 {
+  const bool sa = (long long)m * k <= kSmallOp && smem + (size_t)m * k * sizeof(double) <= 220 * 1024;
+  if (sa) smem += (size_t)m * k * sizeof(double);
+  auto kern = sa ? dense_apply_kernel<RM, true> : dense_apply_kernel<RM, false>;
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(dense_apply_kernel<RM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return op_fail(FR_ERR_CUDA, cudaGetErrorString(e));
   }
-  dense_apply_kernel<RM><<<blocks, kDenseThreads, smem, s>>>(m, k, ncols, A, B, Cm, beta);
+  kern<<<blocks, kDenseThreads, smem, s>>>(m, k, ncols, A, B, Cm, beta);
   return launched("dense_apply_kernel");
 }
 
