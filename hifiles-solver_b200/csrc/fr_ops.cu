@@ -39,90 +39,125 @@ fr_status launched(const char* what)
 constexpr int kTileCols = 32;
 constexpr int kTileStride = kTileCols + 1;  // staged B rows padded: the column-major copy-in is conflict-free
 constexpr int kDenseThreads = 256;
+constexpr int kMaxOps = 3;
+constexpr int kSmallOps = 8192;             // operator entries (all nd) staged in shared memory
+constexpr size_t kDenseSmem = 220 * 1024;
+constexpr size_t kStageSmem = 64 * 1024;    // operators are staged while a block stays within this
 
-// C(:, j) = beta*C(:, j) + A * B(:, j) for all ncols columns, A (m x k) column
-// major, B (k x ncols) and C (m x ncols) with leading dimensions k and m (the
-// reference's cublasDgemm('N','N', m, ncols, k, 1, A, m, B, k, beta, C, m)).
-// A tile of 32 columns of B and C is staged through shared memory so both
-// global streams are contiguous.  Each thread keeps an RM x 4 register tile:
-// rows r0 + 32 i (i < RM; r0 = lane, then lane + 32 RM ... while rows remain)
-// and columns warp + 8 j (j < 4), so per term l a
-// warp reads 4 broadcast entries of B from shared memory and RM coalesced
-// 32-row slices of A's column l (read-only cache), for 4 RM fused
-// multiply-adds.  With SA (operators of up to kSmallOp entries) A itself is
-// copied to shared memory first and read from there.  Every output is one fma
-// chain over l in increasing order.
-constexpr int kSmallOp = 4096;
-template <int RM, bool SA>
+struct OpSet {
+  const double* a[kMaxOps];
+  // selected without indexing the parameter array by a run-time value
+  __device__ __forceinline__ const double* get(int d) const { return d == 0 ? a[0] : (d == 1 ? a[1] : a[2]); }
+};
+
+// Dense operator products over all ncols columns, nd <= 3 operators A_d
+// (m x k, column major), the reference's cublasDgemm('N','N', m, ncols, k, 1,
+// A_d, m, B, k, beta, C, m) calls of one method fused into one pass:
+//   FAN = false:  C = beta C + sum_d A_d B_d        (B_d = B + d strideB),
+//                 the d-loop of extrapolate_totalFlux / calculate_divergence
+//                 (beta 1 for d > 0): each output is one fma chain over d, l;
+//   FAN = true:   C_d = beta C_d + A_d B            (C_d = C + d strideC),
+//                 calculate_gradient / correct_gradient: B is read once.
+// A tile of 32 columns of every B_d and C_d is staged through shared memory so
+// all global streams are contiguous.  Each thread keeps an RM x 4 register
+// tile: rows r0 + 32 i (i < RM; r0 = lane, then lane + 32 RM ... while rows
+// remain) and columns warp + 8 j (j < 4), so per term l a warp reads 4
+// broadcast entries of B from shared memory and RM coalesced 32-row slices of
+// A_d's column l, for 4 RM fused multiply-adds.  With SA the operators are
+// copied to shared memory first, otherwise read through the read-only cache.
+// Sums run over d, then l, in increasing order: the result equals nd separate
+// single-operator products bit for bit.
+template <int RM, bool SA, bool FAN>
 __global__ void __launch_bounds__(kDenseThreads)
-dense_apply_kernel(int m, int k, long long ncols, const double* __restrict__ A, const double* __restrict__ B,
-                   double* __restrict__ Cm, int beta)
+dense_apply_kernel(int m, int k, long long ncols, int nd, OpSet ops, const double* __restrict__ B,
+                   long long strideB, double* __restrict__ Cm, long long strideC, int beta)
 {
   extern __shared__ double sm[];
-  double* sB = sm;                           // [k][kTileStride]
-  double* sC = sm + (size_t)k * kTileStride; // [kTileCols][m]
-  double* sA = sC + (size_t)kTileCols * m;   // [k][m] when SA
+  const int nb = FAN ? 1 : nd, ncs = FAN ? nd : 1;
+  double* sB = sm;                                          // [nb][k][kTileStride]
+  double* sC = sB + (size_t)nb * k * kTileStride;           // [ncs][kTileCols][m]
+  double* sA = sC + (size_t)ncs * kTileCols * m;            // [nd][k][m] when SA
   if (SA)
-    for (int i = threadIdx.x; i < m * k; i += kDenseThreads) sA[i] = __ldg(A + i);
+    for (int d = 0; d < nd; d++)
+      for (int i = threadIdx.x; i < m * k; i += kDenseThreads) sA[(size_t)d * m * k + i] = __ldg(ops.get(d) + i);
   const long long c0 = (long long)blockIdx.x * kTileCols;
   const int nc = (int)min((long long)kTileCols, ncols - c0);
-  const double* Bt = B + (size_t)c0 * k;
-  for (int i = threadIdx.x; i < nc * k; i += kDenseThreads) {
-    int c = i / k, l = i - c * k;
-    sB[l * kTileStride + c] = Bt[i];
+  for (int b = 0; b < nb; b++) {
+    const double* Bt = B + b * strideB + (size_t)c0 * k;
+    double* sb = sB + (size_t)b * k * kTileStride;
+    for (int i = threadIdx.x; i < nc * k; i += kDenseThreads) {
+      int c = i / k, l = i - c * k;
+      sb[l * kTileStride + c] = Bt[i];
+    }
   }
-  double* Ct = Cm + (size_t)c0 * m;
   if (beta)
-    for (int i = threadIdx.x; i < nc * m; i += kDenseThreads) sC[i] = Ct[i];
+    for (int t = 0; t < ncs; t++) {
+      const double* Ct = Cm + t * strideC + (size_t)c0 * m;
+      double* sc = sC + (size_t)t * kTileCols * m;
+      for (int i = threadIdx.x; i < nc * m; i += kDenseThreads) sc[i] = Ct[i];
+    }
   __syncthreads();
   const int lane = threadIdx.x & 31, wc = threadIdx.x >> 5;
-  // row passes of 32 RM rows (one pass for m <= 32 RM)
   for (int r0 = lane; r0 < m; r0 += 32 * RM) {
     double acc[RM][4];
+    for (int d = 0; d < nd; d++) {
+      double* sc = sC + (FAN ? (size_t)d * kTileCols * m : 0);
+      if (FAN || d == 0) {
 #pragma unroll
-    for (int i = 0; i < RM; i++)
+        for (int i = 0; i < RM; i++)
 #pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const int r = r0 + 32 * i, c = wc + 8 * j;
-        acc[i][j] = (beta && r < m && c < nc) ? sC[c * m + r] : 0.0;
+          for (int j = 0; j < 4; j++) {
+            const int r = r0 + 32 * i, c = wc + 8 * j;
+            acc[i][j] = (beta && r < m && c < nc) ? sc[c * m + r] : 0.0;
+          }
       }
-    const double* Ar = (SA ? sA : A) + r0;
-    for (int l = 0; l < k; l++) {
-      double b[4], a[RM];
+      const double* sb = sB + (FAN ? 0 : (size_t)d * k * kTileStride);
+      const double* Ar = (SA ? sA + (size_t)d * m * k : ops.get(d)) + r0;
+      for (int l = 0; l < k; l++) {
+        double bv[4], a[RM];
 #pragma unroll
-      for (int j = 0; j < 4; j++) b[j] = sB[l * kTileStride + wc + 8 * j];
+        for (int j = 0; j < 4; j++) bv[j] = sb[l * kTileStride + wc + 8 * j];
 #pragma unroll
-      for (int i = 0; i < RM; i++)
-        a[i] = (r0 + 32 * i < m) ? (SA ? Ar[32 * i + (size_t)m * l] : __ldg(Ar + 32 * i + (size_t)m * l)) : 0.0;
+        for (int i = 0; i < RM; i++)
+          a[i] = (r0 + 32 * i < m) ? (SA ? Ar[32 * i + (size_t)m * l] : __ldg(Ar + 32 * i + (size_t)m * l)) : 0.0;
 #pragma unroll
-      for (int i = 0; i < RM; i++)
+        for (int i = 0; i < RM; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = fma(b[j], a[i], acc[i][j]);
+          for (int j = 0; j < 4; j++) acc[i][j] = fma(bv[j], a[i], acc[i][j]);
+      }
+      if (FAN || d == nd - 1) {
+#pragma unroll
+        for (int i = 0; i < RM; i++)
+#pragma unroll
+          for (int j = 0; j < 4; j++) {
+            const int r = r0 + 32 * i, c = wc + 8 * j;
+            if (r < m && c < nc) sc[c * m + r] = acc[i][j];
+          }
+      }
     }
-#pragma unroll
-    for (int i = 0; i < RM; i++)
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const int r = r0 + 32 * i, c = wc + 8 * j;
-        if (r < m && c < nc) sC[c * m + r] = acc[i][j];
-      }
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < nc * m; i += kDenseThreads) Ct[i] = sC[i];
+  for (int t = 0; t < ncs; t++) {
+    double* Ct = Cm + t * strideC + (size_t)c0 * m;
+    const double* sc = sC + (size_t)t * kTileCols * m;
+    for (int i = threadIdx.x; i < nc * m; i += kDenseThreads) Ct[i] = sc[i];
+  }
 }
 
 template <int RM>
-fr_status dense_launch(int m, int k, long long ncols, const double* A, const double* B, double* Cm, int beta,
-                       cudaStream_t s, size_t smem, unsigned blocks)
+fr_status dense_launch(int m, int k, long long ncols, int nd, const OpSet& ops, const double* B, long long sB,
+                       double* Cm, long long sC, int beta, bool fan, cudaStream_t s, size_t smem, unsigned blocks)
 {
-  const bool sa = (long long)m * k <= kSmallOp && smem + (size_t)m * k * sizeof(double) <= 220 * 1024;
-  if (sa) smem += (size_t)m * k * sizeof(double);
-  auto kern = sa ? dense_apply_kernel<RM, true> : dense_apply_kernel<RM, false>;
+  const size_t a_bytes = (size_t)nd * m * k * sizeof(double);
+  const bool sa = (long long)nd * m * k <= kSmallOps && smem + a_bytes <= kStageSmem;
+  if (sa) smem += a_bytes;
+  auto kern = fan ? (sa ? dense_apply_kernel<RM, true, true> : dense_apply_kernel<RM, false, true>)
+                  : (sa ? dense_apply_kernel<RM, true, false> : dense_apply_kernel<RM, false, false>);
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return op_fail(FR_ERR_CUDA, cudaGetErrorString(e));
   }
-  kern<<<blocks, kDenseThreads, smem, s>>>(m, k, ncols, A, B, Cm, beta);
+  kern<<<blocks, kDenseThreads, smem, s>>>(m, k, ncols, nd, ops, B, sB, Cm, sC, beta);
   return launched("dense_apply_kernel");
 }
 
@@ -131,27 +166,59 @@ fr_status dense_launch(int m, int k, long long ncols, const double* A, const dou
 // accumulation (fr_tc_gemm.cu).
 static int g_gemm_mode = 0;
 
+// nd operator products of one method (see dense_apply_kernel); FAN selects
+// C_d = beta C_d + A_d B, otherwise C = beta C + sum_d A_d B_d.  The tensor-
+// core forms and shapes whose staged tiles exceed shared memory run as nd
+// single products in the same order.
+fr_status dense_apply_nd(int m, int k, long long ncols, int nd, const double* const* A, const double* B,
+                         long long strideB, double* Cm, long long strideC, int beta, bool fan, cudaStream_t s)
+{
+  if (m <= 0 || k <= 0 || ncols < 0 || nd < 1 || nd > kMaxOps || !A || !B || !Cm)
+    return op_fail(FR_ERR_ARG, "bad operator arguments");
+  for (int d = 0; d < nd; d++)
+    if (!A[d]) return op_fail(FR_ERR_ARG, "bad operator arguments");
+  if (ncols == 0) return FR_OK;
+  const int nb = fan ? 1 : nd, ncs = fan ? nd : 1;
+  size_t smem = ((size_t)nb * k * kTileStride + (size_t)ncs * kTileCols * m) * sizeof(double);
+  const size_t a1 = (size_t)m * k * sizeof(double);
+  const size_t smem1 = ((size_t)k * kTileStride + (size_t)kTileCols * m) * sizeof(double);
+  // fused unless one operator could sit in shared memory but all nd cannot:
+  // then nd single products with a staged operator are faster
+  const bool split = nd > 1 && (long long)m * k <= kSmallOps && smem1 + a1 <= kStageSmem &&
+                     !((long long)nd * m * k <= kSmallOps && smem + nd * a1 <= kStageSmem);
+  if (g_gemm_mode || split || (nd > 1 && smem > kDenseSmem)) {
+    for (int d = 0; d < nd; d++) {
+      const double* Bd = B + (fan ? 0 : d * strideB);
+      double* Cd = Cm + (fan ? d * strideC : 0);
+      const int bd = fan ? beta : (d > 0 ? 1 : beta);
+      fr_status st = g_gemm_mode ? gemm_bf16x3(m, k, ncols, A[d], Bd, Cd, bd, s, g_gemm_mode == 2 ? 6 : 3)
+                                 : dense_apply_nd(m, k, ncols, 1, A + d, Bd, 0, Cd, 0, bd, false, s);
+      if (st) return st;
+    }
+    return FR_OK;
+  }
+  if (smem > kDenseSmem) return op_fail(FR_ERR_UNSUPPORTED, "operator too large for one column tile");
+  long long blocks = (ncols + kTileCols - 1) / kTileCols;
+  if (blocks > 2147483647LL) return op_fail(FR_ERR_ARG, "too many columns");
+  const unsigned nbk = (unsigned)blocks;
+  OpSet ops{};
+  for (int d = 0; d < nd; d++) ops.a[d] = A[d];
+  switch ((m + 31) / 32) {
+    case 1: return dense_launch<1>(m, k, ncols, nd, ops, B, strideB, Cm, strideC, beta, fan, s, smem, nbk);
+    case 2: return dense_launch<2>(m, k, ncols, nd, ops, B, strideB, Cm, strideC, beta, fan, s, smem, nbk);
+    case 3: return dense_launch<3>(m, k, ncols, nd, ops, B, strideB, Cm, strideC, beta, fan, s, smem, nbk);
+    case 4: return dense_launch<4>(m, k, ncols, nd, ops, B, strideB, Cm, strideC, beta, fan, s, smem, nbk);
+    case 5: return dense_launch<5>(m, k, ncols, nd, ops, B, strideB, Cm, strideC, beta, fan, s, smem, nbk);
+    case 6: return dense_launch<6>(m, k, ncols, nd, ops, B, strideB, Cm, strideC, beta, fan, s, smem, nbk);
+    case 7: return dense_launch<7>(m, k, ncols, nd, ops, B, strideB, Cm, strideC, beta, fan, s, smem, nbk);
+    default: return dense_launch<8>(m, k, ncols, nd, ops, B, strideB, Cm, strideC, beta, fan, s, smem, nbk);
+  }
+}
+
 fr_status dense_apply(int m, int k, long long ncols, const double* A, const double* B, double* Cm, int beta,
                       cudaStream_t s)
 {
-  if (m <= 0 || k <= 0 || ncols < 0 || !A || !B || !Cm) return op_fail(FR_ERR_ARG, "bad operator arguments");
-  if (ncols == 0) return FR_OK;
-  if (g_gemm_mode) return gemm_bf16x3(m, k, ncols, A, B, Cm, beta, s, g_gemm_mode == 2 ? 6 : 3);
-  size_t smem = ((size_t)k * kTileStride + (size_t)kTileCols * m) * sizeof(double);
-  if (smem > 220 * 1024) return op_fail(FR_ERR_UNSUPPORTED, "operator too large for one column tile");
-  long long blocks = (ncols + kTileCols - 1) / kTileCols;
-  if (blocks > 2147483647LL) return op_fail(FR_ERR_ARG, "too many columns");
-  const unsigned nb = (unsigned)blocks;
-  switch ((m + 31) / 32) {
-    case 1: return dense_launch<1>(m, k, ncols, A, B, Cm, beta, s, smem, nb);
-    case 2: return dense_launch<2>(m, k, ncols, A, B, Cm, beta, s, smem, nb);
-    case 3: return dense_launch<3>(m, k, ncols, A, B, Cm, beta, s, smem, nb);
-    case 4: return dense_launch<4>(m, k, ncols, A, B, Cm, beta, s, smem, nb);
-    case 5: return dense_launch<5>(m, k, ncols, A, B, Cm, beta, s, smem, nb);
-    case 6: return dense_launch<6>(m, k, ncols, A, B, Cm, beta, s, smem, nb);
-    case 7: return dense_launch<7>(m, k, ncols, A, B, Cm, beta, s, smem, nb);
-    default: return dense_launch<8>(m, k, ncols, A, B, Cm, beta, s, smem, nb);
-  }
+  return dense_apply_nd(m, k, ncols, 1, &A, B, 0, Cm, 0, beta, false, s);
 }
 
 // ------------------------------------------------------------ pointwise kernels
@@ -491,12 +558,8 @@ fr_status fr_op_calculate_gradient(int n_upts, int n_dims, int n_fields, int n_e
 {
   if (!opp_4 || n_dims < 2 || n_dims > 3) return op_fail(FR_ERR_ARG, "bad arguments");
   long long cols = (long long)n_fields * n_eles;
-  for (int d = 0; d < n_dims; d++) {
-    fr_status st = dense_apply(n_upts, n_upts, cols, opp_4[d], disu_upts, grad_disu_upts + (size_t)n_upts * cols * d,
-                               0, ST(stream));
-    if (st) return st;
-  }
-  return FR_OK;
+  return dense_apply_nd(n_upts, n_upts, cols, n_dims, opp_4, disu_upts, 0, grad_disu_upts, (long long)n_upts * cols,
+                        0, true, ST(stream));
 }
 
 fr_status fr_op_correct_gradient(int n_upts, int n_fpts, int n_dims, int n_fields, int n_eles,
@@ -505,11 +568,9 @@ fr_status fr_op_correct_gradient(int n_upts, int n_fpts, int n_dims, int n_field
 {
   if (!opp_5 || n_dims < 2 || n_dims > 3 || !JGinv_upts || !detjac_upts) return op_fail(FR_ERR_ARG, "bad arguments");
   long long cols = (long long)n_fields * n_eles;
-  for (int d = 0; d < n_dims; d++) {
-    fr_status st = dense_apply(n_upts, n_fpts, cols, opp_5[d], delta_disu_fpts,
-                               grad_disu_upts + (size_t)n_upts * cols * d, 1, ST(stream));
-    if (st) return st;
-  }
+  fr_status st = dense_apply_nd(n_upts, n_fpts, cols, n_dims, opp_5, delta_disu_fpts, 0, grad_disu_upts,
+                                (long long)n_upts * cols, 1, true, ST(stream));
+  if (st) return st;
   long long n = (long long)n_upts * n_eles;
   if (n_dims == 2) grad_transform_kernel<2><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_upts, n_eles, n_fields, grad_disu_upts, JGinv_upts, detjac_upts);
   else grad_transform_kernel<3><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_upts, n_eles, n_fields, grad_disu_upts, JGinv_upts, detjac_upts);
@@ -546,27 +607,19 @@ fr_status fr_op_extrapolate_totalFlux(int n_fpts, int n_upts, int n_dims, int n_
                                       const double* const* opp_1, const double* tdisf_upts, double* norm_tdisf_fpts,
                                       void* stream)
 {
-  if (!opp_1) return op_fail(FR_ERR_ARG, "bad arguments");
+  if (!opp_1 || n_dims < 1 || n_dims > 3) return op_fail(FR_ERR_ARG, "bad arguments");
   long long cols = (long long)n_fields * n_eles;
-  for (int d = 0; d < n_dims; d++) {
-    fr_status st = dense_apply(n_fpts, n_upts, cols, opp_1[d], tdisf_upts + (size_t)n_upts * cols * d,
-                               norm_tdisf_fpts, d > 0, ST(stream));
-    if (st) return st;
-  }
-  return FR_OK;
+  return dense_apply_nd(n_fpts, n_upts, cols, n_dims, opp_1, tdisf_upts, (long long)n_upts * cols, norm_tdisf_fpts, 0,
+                        0, false, ST(stream));
 }
 
 fr_status fr_op_calculate_divergence(int n_upts, int n_dims, int n_fields, int n_eles, const double* const* opp_2,
                                      const double* tdisf_upts, double* div_tconf_upts, void* stream)
 {
-  if (!opp_2) return op_fail(FR_ERR_ARG, "bad arguments");
+  if (!opp_2 || n_dims < 1 || n_dims > 3) return op_fail(FR_ERR_ARG, "bad arguments");
   long long cols = (long long)n_fields * n_eles;
-  for (int d = 0; d < n_dims; d++) {
-    fr_status st = dense_apply(n_upts, n_upts, cols, opp_2[d], tdisf_upts + (size_t)n_upts * cols * d,
-                               div_tconf_upts, d > 0, ST(stream));
-    if (st) return st;
-  }
-  return FR_OK;
+  return dense_apply_nd(n_upts, n_upts, cols, n_dims, opp_2, tdisf_upts, (long long)n_upts * cols, div_tconf_upts, 0,
+                        0, false, ST(stream));
 }
 
 fr_status fr_op_calculate_corrected_divergence(int n_upts, int n_fpts, int n_fields, int n_eles, const double* opp_3,
