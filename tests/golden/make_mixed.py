@@ -188,7 +188,9 @@ CASES = [
 
 # arrays kept per element type (prefix t<ele_type>_ in the harness output)
 SETUP = ["opp_0", "opp_3", "opp_6", "detjac_upts", "JGinv_upts", "tdA_fpts", "norm_fpts", "disu_upts_init"]
-STAGES = ["s01_disu_fpts", "s04_delta_disu_fpts", "s05_grad_disu_upts", "s06_grad_disu_fpts", "s07_tdisf_upts",
+# s03 / s04 arrays are the final flux and common flux of inviscid runs only
+INVISCID_ONLY = ("s03_tdisf_upts", "s04_norm_tconf_fpts")
+STAGES = ["s01_disu_fpts", "s03_tdisf_upts", "s04_norm_tconf_fpts", "s04_delta_disu_fpts", "s05_grad_disu_upts", "s06_grad_disu_fpts", "s07_tdisf_upts",
           "s08_norm_tdisf_fpts", "s09_div_tconf_upts", "s10_norm_tconf_fpts", "s11_div_tconf_upts",
           "s12_disu_upts0", "final_disu_upts0"]
 
@@ -234,6 +236,57 @@ def run_case(ref, c, work):
     return arr, par, types, eles
 
 
+# 2-D quadrilateral boxes with boundaries on every side (side order x-, x+,
+# y-, y+), run through make_golden's writer and input; they exercise the
+# boundary entry points in 2-D and every boundary type but the moving walls'
+# 3-D forms
+SEAM_2D = [
+    dict(name="seam_quad_bc_euler_p3", dims=2, order=3, n=(5, 4), lo=(-5, -5), hi=(5, 5), viscous=0,
+         ic="vortex_u1v0", vcjh=1, jitter=0.1, steps=3, dt=1e-3, stages=True, side_bc=(15, 4, 7, 16)),
+    dict(name="seam_quad_bc_euler2_p2", dims=2, order=2, n=(4, 5), lo=(-5, -5), hi=(5, 5), viscous=0,
+         ic="vortex_u1v0", vcjh=2, jitter=0.1, steps=3, dt=1e-3, stages=True, side_bc=(1, 2, 5, 6)),
+    dict(name="seam_quad_ns_bc_p3", dims=2, order=3, n=(5, 4), lo=(0, 0), hi=(2 * np.pi, 2 * np.pi), viscous=1,
+         ic="channel_mach01", vcjh=1, jitter=0.1, steps=3, dt=1e-3, stages=True, side_bc=(3, 4, 13, 14)),
+]
+
+
+def pack(out_dir, arr, par, meta):
+    """Fixture arrays of one harness run (every element, interface and boundary type)."""
+    types = []
+    for line in open(os.path.join(out_dir, "params.txt")):
+        p = line.split()
+        if p[0] == "type" and int(p[5]) > 0:
+            types.append(dict(index=int(p[1]), ele_type=int(p[3]), n_eles=int(p[5]), n_upts=int(p[7]),
+                              n_fpts=int(p[9])))
+    D = int(par["n_dims"])
+    fx = {}
+    for t in types:
+        T = "t%d_" % t["ele_type"]
+        for k in SETUP:
+            if T + k in arr:
+                fx[T + k] = arr[T + k]
+        for w in (1, 2, 4, 5):
+            for dd in range(D):
+                if T + "opp_%d_%d" % (w, dd) in arr:
+                    fx[T + "opp_%d_%d" % (w, dd)] = arr[T + "opp_%d_%d" % (w, dd)]
+        for k in STAGES:
+            if T + k in arr and not (meta["viscous"] and k in INVISCID_ONLY):
+                fx[T + k] = arr[T + k]
+    inters, bdys = [], []
+    for it in range(8):
+        for key, lst in (("int_inters_%d" % it, inters), ("bdy_inters_%d" % it, bdys)):
+            if key in arr:
+                fx[key] = arr[key]
+                lst.append(dict(index=it, n_fpts=int(arr[key].shape[1]), n_inters=int(arr[key].shape[2])))
+    fx["res_norms"] = arr["res_norms"]
+    meta = dict(meta)
+    meta.update(types=types, inters=inters, bdy_inters=bdys, dims=D,
+                physics={k: par[k] for k in ("gamma", "prandtl", "mu_inf", "rt_inf", "c_sth", "fix_vis", "tau",
+                                             "pen_fact")},
+                bdy=[par.get("bdy%d" % i, 0.0) for i in range(14)], R_ref=par.get("R_ref", 1.0))
+    return fx, meta
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -242,6 +295,13 @@ def main():
     if not os.path.exists(G.HARNESS):
         subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "REF=" + a.ref, "ref"], check=True)
     work = a.work or tempfile.mkdtemp(prefix="fr_mixed_")
+    for c in SEAM_2D:
+        arr, par = G.run_case(a.ref, c, work)
+        meta = {k: (list(v) if isinstance(v, tuple) else v) for k, v in c.items()}
+        fx, meta = pack(os.path.join(work, c["name"], "out"), arr, par, meta)
+        np.savez_compressed(os.path.join(HERE, c["name"] + ".npz"), meta=json.dumps(meta),
+                            **{k: np.asfortranarray(v) for k, v in fx.items()})
+        print(c["name"], json.dumps({"types": meta["types"], "bdy_inters": meta["bdy_inters"]}))
     for c in CASES:
         arr, par, types, eles = run_case(a.ref, c, work)
         fx = {}
@@ -253,7 +313,8 @@ def main():
                 for dd in range(3):
                     fx[T + "opp_%d_%d" % (w, dd)] = arr[T + "opp_%d_%d" % (w, dd)]
             for k in STAGES:
-                fx[T + k] = arr[T + k]
+                if k not in INVISCID_ONLY:
+                    fx[T + k] = arr[T + k]
         inters = []
         for it in range(8):
             key = "int_inters_%d" % it

@@ -26,6 +26,25 @@ import pytest
 from golden_util import load, rel
 
 MIXED = ["mixed_pritet_p3", "mixed_pritet_p2", "mixed_hexpri_p3", "mixed_channel_p2", "mixed_channel_p3"]
+# 2-D quadrilateral boxes with a boundary on every side: Euler with
+# characteristic / subsonic outflow / slip wall / dual-consistent slip wall and
+# simple in- and outflow / supersonic in- and outflow, Navier-Stokes with
+# characteristic in- and outflow and moving isothermal / adiabatic walls
+SEAM_2D = ["seam_quad_bc_euler_p3", "seam_quad_bc_euler2_p2", "seam_quad_ns_bc_p3"]
+CASES = MIXED + SEAM_2D
+
+
+def _dims(meta):
+    return meta.get("dims", 3)
+
+
+def _visc(meta):
+    return bool(meta.get("viscous", 1))
+
+
+def _keys(meta):
+    """Harness stage arrays of the final transformed flux and common flux."""
+    return ("s07_tdisf_upts", "s10_norm_tconf_fpts") if _visc(meta) else ("s03_tdisf_upts", "s04_norm_tconf_fpts")
 RK4B = [0.149659021999229, 0.379210312999627, 0.822955029386982, 0.699450455949122, 0.153057247968152]
 
 
@@ -33,7 +52,7 @@ def _types(meta):
     return {t["index"]: t for t in meta["types"]}
 
 
-@pytest.mark.parametrize("case", MIXED)
+@pytest.mark.parametrize("case", CASES)
 def test_mixed_wiring_pairs_every_flux_point_once(case):
     meta, a = load(case)
     ty = _types(meta)
@@ -59,9 +78,10 @@ def test_mixed_wiring_pairs_every_flux_point_once(case):
         assert (s == 1).all(), (case, ty[i]["ele_type"])
 
 
-@pytest.mark.parametrize("case", MIXED)
+@pytest.mark.parametrize("case", CASES)
 def test_mixed_fixture_operator_relations(case):
     meta, a = load(case)
+    tf_key, ntc_key = _keys(meta)
     for t in meta["types"]:
         T = "t%d_" % t["ele_type"]
         u0 = a[T + "disu_upts_init"]
@@ -70,9 +90,9 @@ def test_mixed_fixture_operator_relations(case):
         got = np.einsum("fu,uek->fek", a[T + "opp_0"], u0)
         assert rel(got, a[T + "s01_disu_fpts"]) < 1e-14
         # divergence: div = sum_d opp_2[d] tdisf[d]; corrected: += opp_3 (norm_tconf - norm_tdisf)
-        div = sum(np.einsum("vu,uek->vek", a[T + "opp_2_%d" % d], a[T + "s07_tdisf_upts"][..., d]) for d in range(3))
+        div = sum(np.einsum("vu,uek->vek", a[T + "opp_2_%d" % d], a[T + tf_key][..., d]) for d in range(_dims(meta)))
         assert rel(div, a[T + "s09_div_tconf_upts"]) < 1e-13
-        jump = a[T + "s10_norm_tconf_fpts"] - a[T + "s08_norm_tdisf_fpts"]
+        jump = a[T + ntc_key] - a[T + "s08_norm_tdisf_fpts"]
         corr = a[T + "s09_div_tconf_upts"] + np.einsum("uf,fek->uek", a[T + "opp_3"], jump)
         assert rel(corr, a[T + "s11_div_tconf_upts"]) < 1e-12
         # RK45 stage 0 from a zero register: u1 = u0 + b_0 dt (-div / detJ)
@@ -93,7 +113,7 @@ def _seam():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", MIXED)
+@pytest.mark.parametrize("case", CASES)
 def test_mixed_mesh_through_the_operator_seam_matches_the_reference(case):
     torch = pytest.importorskip("torch")
     H, T, L = _seam()
@@ -101,7 +121,10 @@ def test_mixed_mesh_through_the_operator_seam_matches_the_reference(case):
     VP = C.c_void_p
     ty = _types(meta)
     ph = T.PhysDesc(**meta["physics"])
-    D, F = 3, 5
+    D = _dims(meta)
+    F = D + 2
+    visc = _visc(meta)
+    tf_key, ntc_key = _keys(meta)
     P = lambda t: t.data_ptr()  # noqa: E731
     dev = T._dev
     S = {}
@@ -109,8 +132,9 @@ def test_mixed_mesh_through_the_operator_seam_matches_the_reference(case):
         X = "t%d_" % t["ele_type"]
         nu, nf, E = t["n_upts"], t["n_fpts"], t["n_eles"]
         s = dict(nu=nu, nf=nf, E=E, X=X)
-        s["opp0"], s["opp3"], s["opp6"] = (dev(a[X + k]) for k in ("opp_0", "opp_3", "opp_6"))
-        for w in (1, 2, 4, 5):
+        s["opp0"], s["opp3"] = dev(a[X + "opp_0"]), dev(a[X + "opp_3"])
+        s["opp6"] = dev(a[X + "opp_6"]) if visc else None
+        for w in ((1, 2, 4, 5) if visc else (1, 2)):
             s["opp%d" % w] = [dev(a[X + "opp_%d_%d" % (w, d)]) for d in range(D)]
             s["opp%d_ptrs" % w] = (VP * D)(*[P(x) for x in s["opp%d" % w]])
         s["JG"], s["dj"], s["tdA"], s["nrm"] = (dev(a[X + k]) for k in ("JGinv_upts", "detjac_upts", "tdA_fpts",
@@ -166,33 +190,37 @@ def test_mixed_mesh_through_the_operator_seam_matches_the_reference(case):
     def residual():
         for s in S.values():
             ok(L.fr_op_extrapolate_solution(s["nf"], s["nu"], F, s["E"], P(s["opp0"]), P(s["u"]), P(s["ufp"]), None))
-            ok(L.fr_op_calculate_gradient(s["nu"], D, F, s["E"], C.cast(s["opp4_ptrs"], VP), P(s["u"]), P(s["gup"]),
-                                          None))
+            if visc:
+                ok(L.fr_op_calculate_gradient(s["nu"], D, F, s["E"], C.cast(s["opp4_ptrs"], VP), P(s["u"]),
+                                              P(s["gup"]), None))
             ok(L.fr_op_evaluate_invFlux(s["nu"], D, F, s["E"], P(s["u"]), P(s["JG"]), P(s["tf"]), C.byref(ph), None))
         for tb in inters:
             ok(L.fr_op_int_inters_common_invFlux(tb["nfpi"], D, F, tb["ni"], P(tb["ul"]), P(tb["ur"]), P(tb["tl"]),
                                                  P(tb["tr"]), P(tb["al"]), P(tb["ar"]), P(tb["n"]), P(tb["dl"]),
-                                                 P(tb["dr"]), C.byref(ph), 1, None))
+                                                 P(tb["dr"]), C.byref(ph), int(visc), None))
         for tb in bdys:
             ok(L.fr_op_bdy_inters_common_invFlux(tb["nfpi"], D, F, tb["ni"], P(tb["ul"]), P(tb["tl"]), P(tb["al"]),
                                                  P(tb["n"]), P(tb["type"]), P(bdy_params), P(tb["dl"]), C.byref(ph),
-                                                 R_ref, 0, 1, None))
+                                                 R_ref, 0, int(visc), None))
         for s in S.values():
+            if not visc:
+                break
             ok(L.fr_op_correct_gradient(s["nu"], s["nf"], D, F, s["E"], C.cast(s["opp5_ptrs"], VP), P(s["ddu"]),
                                         P(s["JG"]), P(s["dj"]), P(s["gup"]), None))
             ok(L.fr_op_extrapolate_corrected_gradient(s["nf"], s["nu"], D, F, s["E"], P(s["opp6"]), P(s["gup"]),
                                                       P(s["gfp"]), None))
             ok(L.fr_op_evaluate_viscFlux(s["nu"], D, F, s["E"], P(s["u"]), P(s["gup"]), P(s["JG"]), P(s["tf"]),
                                          C.byref(ph), None))
+        for s in S.values():
             ok(L.fr_op_extrapolate_totalFlux(s["nf"], s["nu"], D, F, s["E"], C.cast(s["opp1_ptrs"], VP), P(s["tf"]),
                                              P(s["ntd"]), None))
             ok(L.fr_op_calculate_divergence(s["nu"], D, F, s["E"], C.cast(s["opp2_ptrs"], VP), P(s["tf"]),
                                             P(s["div"]), None))
-        for tb in inters:
+        for tb in (inters if visc else []):
             ok(L.fr_op_int_inters_common_viscFlux(tb["nfpi"], D, F, tb["ni"], P(tb["ul"]), P(tb["ur"]), P(tb["gl"]),
                                                   P(tb["gr"]), P(tb["tl"]), P(tb["tr"]), P(tb["al"]), P(tb["ar"]),
                                                   P(tb["n"]), C.byref(ph), None))
-        for tb in bdys:
+        for tb in (bdys if visc else []):
             ok(L.fr_op_bdy_inters_common_viscFlux(tb["nfpi"], D, F, tb["ni"], P(tb["ul"]), P(tb["gl"]), P(tb["tl"]),
                                                   P(tb["al"]), P(tb["n"]), P(tb["type"]), P(bdy_params), C.byref(ph),
                                                   R_ref, None))
@@ -213,17 +241,18 @@ def test_mixed_mesh_through_the_operator_seam_matches_the_reference(case):
     for i, s in S.items():
         X, nu, nf, E = s["X"], s["nu"], s["nf"], s["E"]
         assert rel(T._host(s["ufp"], (nf, E, F)), a[X + "s01_disu_fpts"]) <= tol
-        # delta = u_common - u_own is a difference of nearly equal traces (on
-        # faces that carry solution points it nearly vanishes): bounded by
-        # 1e-12 of itself plus a few ulps of the traces it is taken from
-        dd = T._host(s["ddu"], (nf, E, F)) - a[X + "s04_delta_disu_fpts"]
-        assert np.linalg.norm(dd) <= (tol * np.linalg.norm(a[X + "s04_delta_disu_fpts"])
-                                      + 4e-16 * np.linalg.norm(a[X + "s01_disu_fpts"]))
-        assert rel(T._host(s["gup"], (nu, E, F, D)), a[X + "s05_grad_disu_upts"]) <= tol
-        assert rel(T._host(s["gfp"], (nf, E, F, D)), a[X + "s06_grad_disu_fpts"]) <= tol
-        assert rel(T._host(s["tf"], (nu, E, F, D)), a[X + "s07_tdisf_upts"]) <= tol
+        if visc:
+            # delta = u_common - u_own is a difference of nearly equal traces
+            # (on faces that carry solution points it nearly vanishes): bounded
+            # by 1e-12 of itself plus a few ulps of the traces it comes from
+            dd = T._host(s["ddu"], (nf, E, F)) - a[X + "s04_delta_disu_fpts"]
+            assert np.linalg.norm(dd) <= (tol * np.linalg.norm(a[X + "s04_delta_disu_fpts"])
+                                          + 4e-16 * np.linalg.norm(a[X + "s01_disu_fpts"]))
+            assert rel(T._host(s["gup"], (nu, E, F, D)), a[X + "s05_grad_disu_upts"]) <= tol
+            assert rel(T._host(s["gfp"], (nf, E, F, D)), a[X + "s06_grad_disu_fpts"]) <= tol
+        assert rel(T._host(s["tf"], (nu, E, F, D)), a[X + tf_key]) <= tol
         assert rel(T._host(s["ntd"], (nf, E, F)), a[X + "s08_norm_tdisf_fpts"]) <= tol
-        assert rel(ntc_visc[i], a[X + "s10_norm_tconf_fpts"]) <= tol
+        assert rel(ntc_visc[i], a[X + ntc_key]) <= tol
         assert rel(T._host(s["div"], (nu, E, F)), a[X + "s11_div_tconf_upts"]) <= tol
     advance(0)
     torch.cuda.synchronize()
