@@ -67,7 +67,7 @@ struct OpSet {
 // copied to shared memory first, otherwise read through the read-only cache.
 // Sums run over d, then l, in increasing order: the result equals nd separate
 // single-operator products bit for bit.
-template <int RM, bool SA, bool FAN>
+template <int RM, bool SA, bool FAN, int LW>
 __global__ void __launch_bounds__(kDenseThreads)
 dense_apply_kernel(int m, int k, long long ncols, int nd, OpSet ops, const double* __restrict__ B,
                    long long strideB, double* __restrict__ Cm, long long strideC, int beta)
@@ -97,40 +97,45 @@ dense_apply_kernel(int m, int k, long long ncols, int nd, OpSet ops, const doubl
       for (int i = threadIdx.x; i < nc * m; i += kDenseThreads) sc[i] = Ct[i];
     }
   __syncthreads();
+  // LW lanes of a warp share a column and take LW consecutive rows; the
+  // 32 / LW lane groups, the 8 warps and RC register columns cover the tile
+  constexpr int RC = LW == 32 ? 4 : 2, CW = 32 / LW;
+  static_assert(CW * 8 * RC == kTileCols, "column tile");
   const int lane = threadIdx.x & 31, wc = threadIdx.x >> 5;
-  for (int r0 = lane; r0 < m; r0 += 32 * RM) {
-    double acc[RM][4];
+  const int cbase = lane / LW + CW * wc;
+  for (int r0 = lane & (LW - 1); r0 < m; r0 += LW * RM) {
+    double acc[RM][RC];
     for (int d = 0; d < nd; d++) {
       double* sc = sC + (FAN ? (size_t)d * kTileCols * m : 0);
       if (FAN || d == 0) {
 #pragma unroll
         for (int i = 0; i < RM; i++)
 #pragma unroll
-          for (int j = 0; j < 4; j++) {
-            const int r = r0 + 32 * i, c = wc + 8 * j;
+          for (int j = 0; j < RC; j++) {
+            const int r = r0 + LW * i, c = cbase + 8 * CW * j;
             acc[i][j] = (beta && r < m && c < nc) ? sc[c * m + r] : 0.0;
           }
       }
       const double* sb = sB + (FAN ? 0 : (size_t)d * k * kTileStride);
       const double* Ar = (SA ? sA + (size_t)d * m * k : ops.get(d)) + r0;
       for (int l = 0; l < k; l++) {
-        double bv[4], a[RM];
+        double bv[RC], a[RM];
 #pragma unroll
-        for (int j = 0; j < 4; j++) bv[j] = sb[l * kTileStride + wc + 8 * j];
-#pragma unroll
-        for (int i = 0; i < RM; i++)
-          a[i] = (r0 + 32 * i < m) ? (SA ? Ar[32 * i + (size_t)m * l] : __ldg(Ar + 32 * i + (size_t)m * l)) : 0.0;
+        for (int j = 0; j < RC; j++) bv[j] = sb[l * kTileStride + cbase + 8 * CW * j];
 #pragma unroll
         for (int i = 0; i < RM; i++)
+          a[i] = (r0 + LW * i < m) ? (SA ? Ar[LW * i + (size_t)m * l] : __ldg(Ar + LW * i + (size_t)m * l)) : 0.0;
 #pragma unroll
-          for (int j = 0; j < 4; j++) acc[i][j] = fma(bv[j], a[i], acc[i][j]);
+        for (int i = 0; i < RM; i++)
+#pragma unroll
+          for (int j = 0; j < RC; j++) acc[i][j] = fma(bv[j], a[i], acc[i][j]);
       }
       if (FAN || d == nd - 1) {
 #pragma unroll
         for (int i = 0; i < RM; i++)
 #pragma unroll
-          for (int j = 0; j < 4; j++) {
-            const int r = r0 + 32 * i, c = wc + 8 * j;
+          for (int j = 0; j < RC; j++) {
+            const int r = r0 + LW * i, c = cbase + 8 * CW * j;
             if (r < m && c < nc) sc[c * m + r] = acc[i][j];
           }
       }
@@ -144,15 +149,15 @@ dense_apply_kernel(int m, int k, long long ncols, int nd, OpSet ops, const doubl
   }
 }
 
-template <int RM>
+template <int RM, int LW = 32>
 fr_status dense_launch(int m, int k, long long ncols, int nd, const OpSet& ops, const double* B, long long sB,
                        double* Cm, long long sC, int beta, bool fan, cudaStream_t s, size_t smem, unsigned blocks)
 {
   const size_t a_bytes = (size_t)nd * m * k * sizeof(double);
   const bool sa = (long long)nd * m * k <= kSmallOps && smem + a_bytes <= kStageSmem;
   if (sa) smem += a_bytes;
-  auto kern = fan ? (sa ? dense_apply_kernel<RM, true, true> : dense_apply_kernel<RM, false, true>)
-                  : (sa ? dense_apply_kernel<RM, true, false> : dense_apply_kernel<RM, false, false>);
+  auto kern = fan ? (sa ? dense_apply_kernel<RM, true, true, LW> : dense_apply_kernel<RM, false, true, LW>)
+                  : (sa ? dense_apply_kernel<RM, true, false, LW> : dense_apply_kernel<RM, false, false, LW>);
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return op_fail(FR_ERR_CUDA, cudaGetErrorString(e));
@@ -203,6 +208,9 @@ fr_status dense_apply_nd(int m, int k, long long ncols, int nd, const double* co
   const unsigned nbk = (unsigned)blocks;
   OpSet ops{};
   for (int d = 0; d < nd; d++) ops.a[d] = A[d];
+  // operators of at most 16 rows: 16 rows per warp, half the padding (for
+  // taller ones the extra operator loads per fma measured slower)
+  if (m <= 16) return dense_launch<1, 16>(m, k, ncols, nd, ops, B, strideB, Cm, strideC, beta, fan, s, smem, nbk);
   switch ((m + 31) / 32) {
     case 1: return dense_launch<1>(m, k, ncols, nd, ops, B, strideB, Cm, strideC, beta, fan, s, smem, nbk);
     case 2: return dense_launch<2>(m, k, ncols, nd, ops, B, strideB, Cm, strideC, beta, fan, s, smem, nbk);
