@@ -345,7 +345,7 @@ __global__ void common_inv_kernel(int nfpi, int ni, double* const* __restrict__ 
                                   double* const* __restrict__ tl_p, double* const* __restrict__ tr_p,
                                   double* const* __restrict__ al_p, double* const* __restrict__ ar_p,
                                   double* const* __restrict__ n_p, double* const* __restrict__ dl_p,
-                                  double* const* __restrict__ dr_p, PhysT<double> ph, int viscous)
+                                  double* const* __restrict__ dr_p, PhysT<double> ph, int riemann, int viscous)
 {
   constexpr int F = D + 2;
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -356,7 +356,8 @@ __global__ void common_inv_kernel(int nfpi, int ni, double* const* __restrict__ 
   for (int k = 0; k < F; k++) { ul[k] = *ul_p[t + n * k]; ur[k] = *ur_p[t + n * k]; }
 #pragma unroll
   for (int d = 0; d < D; d++) nn[d] = *n_p[t + n * d];
-  rusanov<D, double>(ph, ul, ur, nn, fn);
+  if (D == 2 && riemann == 2) roe<double>(ph, ul, ur, nn, fn);
+  else rusanov<D, double>(ph, ul, ur, nn, fn);
   double tal = *al_p[t], tar = *ar_p[t];
 #pragma unroll
   for (int k = 0; k < F; k++) { *tl_p[t + n * k] = fn[k] * tal; *tr_p[t + n * k] = -fn[k] * tar; }
@@ -649,17 +650,20 @@ fr_status fr_op_int_inters_common_invFlux(int n_fpts_per_inter, int n_dims, int 
                                           double* const* norm_tconf_fpts_l, double* const* norm_tconf_fpts_r,
                                           double* const* tdA_fpts_l, double* const* tdA_fpts_r,
                                           double* const* norm_fpts, double* const* delta_disu_fpts_l,
-                                          double* const* delta_disu_fpts_r, const fr_phys_desc* phys, int viscous,
-                                          void* stream)
+                                          double* const* delta_disu_fpts_r, const fr_phys_desc* phys,
+                                          int riemann_solve_type, int viscous, void* stream)
 {
   if (!phys || !dims_ok(n_dims, n_fields)) return op_fail(FR_ERR_ARG, "bad arguments");
+  if (riemann_solve_type != 0 && riemann_solve_type != 2)
+    return op_fail(FR_ERR_UNSUPPORTED, "common flux: riemann_solve_type 0 (Rusanov) or 2 (Roe, 2-D)");
+  if (riemann_solve_type == 2 && n_dims != 2) return op_fail(FR_ERR_UNSUPPORTED, "Roe flux is 2-D only");
   if (viscous && (!delta_disu_fpts_l || !delta_disu_fpts_r)) return op_fail(FR_ERR_ARG, "viscous needs delta tables");
   long long n = (long long)n_fpts_per_inter * n_inters;
   if (n == 0) return FR_OK;
   if (n_dims == 2)
-    common_inv_kernel<2><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_fpts_per_inter, n_inters, disu_fpts_l, disu_fpts_r, norm_tconf_fpts_l, norm_tconf_fpts_r, tdA_fpts_l, tdA_fpts_r, norm_fpts, delta_disu_fpts_l, delta_disu_fpts_r, phys_of(phys), viscous);
+    common_inv_kernel<2><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_fpts_per_inter, n_inters, disu_fpts_l, disu_fpts_r, norm_tconf_fpts_l, norm_tconf_fpts_r, tdA_fpts_l, tdA_fpts_r, norm_fpts, delta_disu_fpts_l, delta_disu_fpts_r, phys_of(phys), riemann_solve_type, viscous);
   else
-    common_inv_kernel<3><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_fpts_per_inter, n_inters, disu_fpts_l, disu_fpts_r, norm_tconf_fpts_l, norm_tconf_fpts_r, tdA_fpts_l, tdA_fpts_r, norm_fpts, delta_disu_fpts_l, delta_disu_fpts_r, phys_of(phys), viscous);
+    common_inv_kernel<3><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_fpts_per_inter, n_inters, disu_fpts_l, disu_fpts_r, norm_tconf_fpts_l, norm_tconf_fpts_r, tdA_fpts_l, tdA_fpts_r, norm_fpts, delta_disu_fpts_l, delta_disu_fpts_r, phys_of(phys), riemann_solve_type, viscous);
   return launched("common_inv_kernel");
 }
 

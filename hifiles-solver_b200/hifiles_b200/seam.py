@@ -102,7 +102,7 @@ def _bind(L):
         "fr_op_extrapolate_totalFlux": [i, i, i, i, i, vp, vp, vp, vp],
         "fr_op_calculate_divergence": [i, i, i, i, vp, vp, vp, vp],
         "fr_op_calculate_corrected_divergence": [i, i, i, i, vp, vp, vp, vp, vp],
-        "fr_op_int_inters_common_invFlux": [i, i, i, i] + [vp] * 9 + [vp, i, vp],
+        "fr_op_int_inters_common_invFlux": [i, i, i, i] + [vp] * 9 + [vp, i, i, vp],
         "fr_op_int_inters_common_viscFlux": [i, i, i, i] + [vp] * 9 + [vp, vp],
         "fr_op_advance_rk45": [i, i, i, i, C.c_double, C.c_double, vp, vp, vp, vp, vp, vp],
         "fr_op_set_gemm_precision": [i],
@@ -189,7 +189,7 @@ class OperatorStage:
                                                     P(self.gup), sp))
             self._ok(L.fr_op_evaluate_invFlux(nu, D, F, E, P(self.u), P(self.JG), P(self.tf), ph, sp))
             self._ok(L.fr_op_int_inters_common_invFlux(1, D, F, self.ni, pt["ul"], pt["ur"], pt["tl"], pt["tr"],
-                                                       pt["al"], pt["ar"], pt["n"], pt["dl"], pt["dr"], ph,
+                                                       pt["al"], pt["ar"], pt["n"], pt["dl"], pt["dr"], ph, 0,
                                                        int(self.visc), sp))
             if self.visc:
                 self._ok(L.fr_op_correct_gradient(nu, nf, D, F, E, C.cast(self._tabs["opp_5"], _VP), P(self.ddu),
@@ -341,7 +341,7 @@ class MixedOperatorMesh:
             for tb in self.inters:
                 ok(L.fr_op_int_inters_common_invFlux(tb["nfpi"], D, F, tb["ni"], P(tb["ul"]), P(tb["ur"]),
                                                      P(tb["tl"]), P(tb["tr"]), P(tb["al"]), P(tb["ar"]), P(tb["n"]),
-                                                     P(tb["dl"]), P(tb["dr"]), ph, 1, sp))
+                                                     P(tb["dl"]), P(tb["dr"]), ph, 0, 1, sp))
             for tb in self.bdys:
                 ok(L.fr_op_bdy_inters_common_invFlux(tb["nfpi"], D, F, tb["ni"], P(tb["ul"]), P(tb["tl"]),
                                                      P(tb["al"]), P(tb["n"]), P(tb["type"]), P(self.bdy),

@@ -383,15 +383,16 @@ fr_status fr_op_calculate_corrected_divergence(int n_upts, int n_fpts, int n_fie
 
 /* int_inters::calculate_common_invFlux, include/int_inters.h:61; replaces
  * calculate_common_invFlux_gpu_kernel_wrapper, include/cuda_kernels.h:39
- * (Rusanov, static mesh; with viscous != 0 also the LDG common solution into
- * delta_disu_fpts_l/_r). */
+ * (static mesh): riemann_solve_type 0 Rusanov or 2 Roe (2-D, as the
+ * reference); with viscous != 0 also the LDG common solution into
+ * delta_disu_fpts_l/_r. */
 fr_status fr_op_int_inters_common_invFlux(int n_fpts_per_inter, int n_dims, int n_fields, int n_inters,
                                           double* const* disu_fpts_l, double* const* disu_fpts_r,
                                           double* const* norm_tconf_fpts_l, double* const* norm_tconf_fpts_r,
                                           double* const* tdA_fpts_l, double* const* tdA_fpts_r,
                                           double* const* norm_fpts, double* const* delta_disu_fpts_l,
-                                          double* const* delta_disu_fpts_r, const fr_phys_desc* phys, int viscous,
-                                          void* stream);
+                                          double* const* delta_disu_fpts_r, const fr_phys_desc* phys,
+                                          int riemann_solve_type, int viscous, void* stream);
 
 /* int_inters::calculate_common_viscFlux, include/int_inters.h:64; replaces
  * calculate_common_viscFlux_gpu_kernel_wrapper, include/cuda_kernels.h:56

@@ -247,6 +247,11 @@ SEAM_2D = [
          ic="vortex_u1v0", vcjh=2, jitter=0.1, steps=3, dt=1e-3, stages=True, side_bc=(1, 2, 5, 6)),
     dict(name="seam_quad_ns_bc_p3", dims=2, order=3, n=(5, 4), lo=(0, 0), hi=(2 * np.pi, 2 * np.pi), viscous=1,
          ic="channel_mach01", vcjh=1, jitter=0.1, steps=3, dt=1e-3, stages=True, side_bc=(3, 4, 13, 14)),
+    # Roe common flux (riemann_solve_type 2, 2-D only in the reference)
+    dict(name="seam_quad_roe_bc_p3", dims=2, order=3, n=(4, 4), lo=(-5, -5), hi=(5, 5), viscous=0,
+         ic="vortex_u1v0", vcjh=1, jitter=0.1, steps=3, dt=1e-3, stages=True, side_bc=(15, 4, 7, 16), riemann=2),
+    dict(name="seam_quad_roe_p3_jit", dims=2, order=3, n=(6, 6), lo=(-5, -5), hi=(5, 5), viscous=0,
+         ic="vortex_u1v0", vcjh=1, jitter=0.15, steps=3, dt=1e-3, stages=True, side_bc=(0, 0, 0, 0), riemann=2),
 ]
 
 

@@ -29,8 +29,10 @@ MIXED = ["mixed_pritet_p3", "mixed_pritet_p2", "mixed_hexpri_p3", "mixed_channel
 # 2-D quadrilateral boxes with a boundary on every side: Euler with
 # characteristic / subsonic outflow / slip wall / dual-consistent slip wall and
 # simple in- and outflow / supersonic in- and outflow, Navier-Stokes with
-# characteristic in- and outflow and moving isothermal / adiabatic walls
-SEAM_2D = ["seam_quad_bc_euler_p3", "seam_quad_bc_euler2_p2", "seam_quad_ns_bc_p3"]
+# characteristic in- and outflow and moving isothermal / adiabatic walls; the
+# Roe common flux (riemann_solve_type 2) with boundaries and periodic
+SEAM_2D = ["seam_quad_bc_euler_p3", "seam_quad_bc_euler2_p2", "seam_quad_ns_bc_p3", "seam_quad_roe_bc_p3",
+           "seam_quad_roe_p3_jit"]
 CASES = MIXED + SEAM_2D
 
 
@@ -124,6 +126,7 @@ def test_mixed_mesh_through_the_operator_seam_matches_the_reference(case):
     D = _dims(meta)
     F = D + 2
     visc = _visc(meta)
+    riemann = int(meta.get("riemann", 0))
     tf_key, ntc_key = _keys(meta)
     P = lambda t: t.data_ptr()  # noqa: E731
     dev = T._dev
@@ -197,11 +200,11 @@ def test_mixed_mesh_through_the_operator_seam_matches_the_reference(case):
         for tb in inters:
             ok(L.fr_op_int_inters_common_invFlux(tb["nfpi"], D, F, tb["ni"], P(tb["ul"]), P(tb["ur"]), P(tb["tl"]),
                                                  P(tb["tr"]), P(tb["al"]), P(tb["ar"]), P(tb["n"]), P(tb["dl"]),
-                                                 P(tb["dr"]), C.byref(ph), int(visc), None))
+                                                 P(tb["dr"]), C.byref(ph), riemann, int(visc), None))
         for tb in bdys:
             ok(L.fr_op_bdy_inters_common_invFlux(tb["nfpi"], D, F, tb["ni"], P(tb["ul"]), P(tb["tl"]), P(tb["al"]),
                                                  P(tb["n"]), P(tb["type"]), P(bdy_params), P(tb["dl"]), C.byref(ph),
-                                                 R_ref, 0, int(visc), None))
+                                                 R_ref, riemann, int(visc), None))
         for s in S.values():
             if not visc:
                 break

@@ -46,7 +46,7 @@ def _bind(L):
     L.fr_op_extrapolate_totalFlux.argtypes = [i, i, i, i, i, VP, VP, VP, VP]
     L.fr_op_calculate_divergence.argtypes = [i, i, i, i, VP, VP, VP, VP]
     L.fr_op_calculate_corrected_divergence.argtypes = [i, i, i, i, VP, VP, VP, VP, VP]
-    L.fr_op_int_inters_common_invFlux.argtypes = [i, i, i, i] + [VP] * 9 + [C.c_void_p, i, VP]
+    L.fr_op_int_inters_common_invFlux.argtypes = [i, i, i, i] + [VP] * 9 + [C.c_void_p, i, i, VP]
     L.fr_op_int_inters_common_viscFlux.argtypes = [i, i, i, i] + [VP] * 9 + [C.c_void_p, VP]
     L.fr_op_advance_rk45.argtypes = [i, i, i, i, dbl, dbl, VP, VP, VP, VP, VP, VP]
     return L
@@ -104,7 +104,7 @@ def test_operator_seam_matches_reference_stage_arrays(case):
     _ok(L.fr_op_evaluate_invFlux(nu, D, F, E, P(u), P(JG), P(tf), C.byref(ph), None))
     _ok(L.fr_op_int_inters_common_invFlux(nfpi, D, F, ni, P(tab["ul"]), P(tab["ur"]), P(tab["tl"]), P(tab["tr"]),
                                           P(tab["al"]), P(tab["ar"]), P(tab["n"]), P(tab["dl"]), P(tab["dr"]),
-                                          C.byref(ph), int(visc), None))
+                                          C.byref(ph), 0, int(visc), None))
     if visc:
         _ok(L.fr_op_correct_gradient(nu, nf, D, F, E, C.cast(arr_ptrs[5], VP), P(ddu), P(JG), P(dj), P(gup), None))
         _ok(L.fr_op_extrapolate_corrected_gradient(nf, nu, D, F, E, P(opp[0]), P(gup), P(gfp), None))
