@@ -229,6 +229,61 @@ fr_status dense_apply(int m, int k, long long ncols, const double* A, const doub
   return dense_apply_nd(m, k, ncols, 1, &A, B, 0, Cm, 0, beta, false, s);
 }
 
+// bespoke_SPMV's product (src/cuda_kernels.cu, bespoke_SPMV_kernel) on the
+// ELL operators of array_to_ellpack (src/funcs.cpp:961-1011): row i keeps
+// nnz_per_row slots s, entry data[i + m s] at column idx[i + m s] (padding
+// slots hold 0 at column 0).  c = q or c + q (add_flag) with q summed from 0
+// over the slots in order.  A tile of 32 columns of B is staged through
+// shared memory as in dense_apply_kernel; each thread keeps rows lane + 32 i
+// and columns warp + 8 j.
+template <int RM>
+__global__ void __launch_bounds__(kDenseThreads)
+spmv_ell_kernel(int m, int k, long long ncols, const double* __restrict__ data, const int* __restrict__ idx,
+                int nnz, const double* __restrict__ B, double* __restrict__ Cm, int add)
+{
+  extern __shared__ double sm[];
+  double* sB = sm;  // [k][kTileStride]
+  const long long c0 = (long long)blockIdx.x * kTileCols;
+  const int nc = (int)min((long long)kTileCols, ncols - c0);
+  const double* Bt = B + (size_t)c0 * k;
+  for (int i = threadIdx.x; i < nc * k; i += kDenseThreads) {
+    int c = i / k, l = i - c * k;
+    sB[l * kTileStride + c] = Bt[i];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wc = threadIdx.x >> 5;
+  double* Ct = Cm + (size_t)c0 * m;
+  for (int r0 = lane; r0 < m; r0 += 32 * RM) {
+    double q[RM][4];
+#pragma unroll
+    for (int i = 0; i < RM; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) q[i][j] = 0.0;
+    for (int s = 0; s < nnz; s++) {
+#pragma unroll
+      for (int i = 0; i < RM; i++) {
+        const int r = r0 + 32 * i;
+        if (r >= m) continue;
+        const double a = __ldg(data + r + (size_t)m * s);
+        const int l = __ldg(idx + r + (size_t)m * s);
+        if ((unsigned)l >= (unsigned)k) continue;  // a column outside the operator is never read
+#pragma unroll
+        for (int j = 0; j < 4; j++) q[i][j] = fma(a, sB[l * kTileStride + wc + 8 * j], q[i][j]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < RM; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int r = r0 + 32 * i, c = wc + 8 * j;
+        if (r < m && c < nc) {
+          double* p = Ct + (size_t)c * m + r;
+          *p = add ? *p + q[i][j] : q[i][j];
+        }
+      }
+  }
+}
+
 // ------------------------------------------------------------ pointwise kernels
 
 template <int D>
@@ -731,6 +786,34 @@ fr_status fr_op_bdy_inters_common_viscFlux(int n_fpts_per_inter, int n_dims, int
   else
     bdy_vis_kernel<3><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_fpts_per_inter, n_inters, disu_fpts_l, grad_disu_fpts_l, norm_tconf_fpts_l, tdA_fpts_l, norm_fpts, boundary_type, bdy_params, ph);
   return launched("bdy_vis_kernel");
+}
+
+fr_status fr_op_spmv_ell(int m, int n, int n_fields, int n_eles, const double* ell_data, const int* ell_indices,
+                         int nnz_per_row, const double* b, double* c, int cell_type, int order, int add_flag,
+                         void* stream)
+{
+  (void)cell_type;
+  (void)order;
+  if (m <= 0 || n <= 0 || n_fields <= 0 || n_eles < 0 || nnz_per_row < 0 || (add_flag != 0 && add_flag != 1) ||
+      !ell_data || !ell_indices || !b || !c)
+    return op_fail(FR_ERR_ARG, "bad arguments");
+  const long long cols = (long long)n_fields * n_eles;
+  if (cols == 0) return FR_OK;
+  const size_t smem = (size_t)n * kTileStride * sizeof(double);
+  if (smem > kDenseSmem || m > 32 * 8) return op_fail(FR_ERR_UNSUPPORTED, "sparse operator too large");
+  const long long blocks = (cols + kTileCols - 1) / kTileCols;
+  if (blocks > 2147483647LL) return op_fail(FR_ERR_ARG, "too many columns");
+  const int rm = (m + 31) / 32;
+  auto kern = rm == 1 ? spmv_ell_kernel<1> : rm == 2 ? spmv_ell_kernel<2> : rm == 3 ? spmv_ell_kernel<3>
+            : rm == 4 ? spmv_ell_kernel<4> : rm == 5 ? spmv_ell_kernel<5> : rm == 6 ? spmv_ell_kernel<6>
+            : rm == 7 ? spmv_ell_kernel<7> : spmv_ell_kernel<8>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return op_fail(FR_ERR_CUDA, cudaGetErrorString(e));
+  }
+  kern<<<(unsigned)blocks, kDenseThreads, smem, ST(stream)>>>(m, n, cols, ell_data, ell_indices, nnz_per_row, b, c,
+                                                             add_flag);
+  return launched("spmv_ell_kernel");
 }
 
 fr_status fr_op_advance_rk45(int n_upts, int n_fields, int n_eles, int stage, double dt, double const_src,

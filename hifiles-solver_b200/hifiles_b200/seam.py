@@ -90,6 +90,24 @@ def dense_operators(dims, P, upts_type=0, vcjh_scheme=1, eta=0.0):
                 opp_4=[F(a) for a in o2], opp_5=[F(a) for a in o5], opp_6=F(o0))
 
 
+def ellpack(a, zero_tol=1e-12):
+    """(data, indices, nnz_per_row) of a dense operator in the ELL layout of
+    array_to_ellpack (src/funcs.cpp:961-1011): entries with |a| >= 1e-12, in
+    increasing column order, slot s of row i at i + m s; padding slots hold 0
+    at column 0."""
+    a = np.asarray(a, dtype=np.float64)
+    m = a.shape[0]
+    keep = np.abs(a) >= zero_tol
+    nnz = int(keep.sum(axis=1).max()) if m else 0
+    data = np.zeros(nnz * m)
+    idx = np.zeros(nnz * m, dtype=np.int32)
+    for i in range(m):
+        cols = np.nonzero(keep[i])[0]
+        data[i + m * np.arange(len(cols))] = a[i, cols]
+        idx[i + m * np.arange(len(cols))] = cols
+    return data, idx, nnz
+
+
 def _bind(L):
     i, vp = C.c_int, _VP
     sig = {
@@ -105,6 +123,7 @@ def _bind(L):
         "fr_op_int_inters_common_invFlux": [i, i, i, i] + [vp] * 9 + [vp, i, i, vp],
         "fr_op_int_inters_common_viscFlux": [i, i, i, i] + [vp] * 9 + [vp, vp],
         "fr_op_advance_rk45": [i, i, i, i, C.c_double, C.c_double, vp, vp, vp, vp, vp, vp],
+        "fr_op_spmv_ell": [i, i, i, i, vp, vp, i, vp, vp, i, i, i, vp],
         "fr_op_set_gemm_precision": [i],
         "fr_op_check": [vp],
     }

@@ -433,6 +433,18 @@ fr_status fr_op_bdy_inters_common_viscFlux(int n_fpts_per_inter, int n_dims, int
                                            const double* bdy_params, const fr_phys_desc* phys, double R_ref,
                                            void* stream);
 
+/* The sparse operator product of the sparse_* options: replaces
+ * bespoke_SPMV, include/cuda_kernels.h:81 (same arguments; cell_type and
+ * order are accepted and unused).  The operator is m x n in the ELL layout of
+ * array_to_ellpack (src/funcs.cpp:961-1011): nnz_per_row slots per row,
+ * ell_data[i + m s] / ell_indices[i + m s]; b (n, n_eles, n_fields) and
+ * c (m, n_eles, n_fields) in the state layouts; c = A b (add_flag 0) or
+ * c += A b (add_flag 1).  m <= 256 and n <= ~850; entries whose column is
+ * outside 0..n-1 are skipped. */
+fr_status fr_op_spmv_ell(int m, int n, int n_fields, int n_eles, const double* ell_data, const int* ell_indices,
+                         int nnz_per_row, const double* b, double* c, int cell_type, int order, int add_flag,
+                         void* stream);
+
 /* eles::AdvanceSolution(stage, adv_type 3), include/eles.h:157; replaces
  * RK45_update_kernel_wrapper, include/cuda_kernels.h:30 (fixed dt):
  * res = a_s res + dt (-div/detjac + const_src + src); u += b_s res.

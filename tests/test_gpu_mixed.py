@@ -322,3 +322,62 @@ def test_mixed_mesh_driver_matches_the_reference_and_its_copies():
         E = u1.shape[1]
         for c in range(K):
             assert np.array_equal(u3[:, c * E:(c + 1) * E], u1)
+
+
+def test_ellpack_matches_the_reference_layout():
+    """seam.ellpack follows array_to_ellpack (src/funcs.cpp:961-1011): entries
+    >= 1e-12 in increasing column order, slot s of row i at i + m s, padding
+    0 at column 0; the dense operator is recovered from it."""
+    import hifiles_b200.seam as SM
+    a = np.array([[0.0, 2.0, 0.0, 3.0], [1.0, 0.0, 0.0, 0.0], [4.0, 5.0, 6.0, 1e-13]])
+    data, idx, nnz = SM.ellpack(a)
+    assert nnz == 3
+    m = a.shape[0]
+    assert list(idx[0::m]) == [1, 3, 0] and list(data[0::m]) == [2.0, 3.0, 0.0]
+    assert list(idx[1::m]) == [0, 0, 0] and list(data[1::m]) == [1.0, 0.0, 0.0]
+    assert list(idx[2::m]) == [0, 1, 2] and list(data[2::m]) == [4.0, 5.0, 6.0]
+    meta, arr = load("mixed_pritet_p3")
+    for t in meta["types"]:
+        op = arr["t%d_opp_3" % t["ele_type"]]
+        d, ix, nz = SM.ellpack(op)
+        back = np.zeros_like(op)
+        for s in range(nz):
+            for i in range(op.shape[0]):
+                back[i, ix[i + op.shape[0] * s]] += d[i + op.shape[0] * s]
+        assert np.array_equal(back, np.where(np.abs(op) >= 1e-12, op, 0.0))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["mixed_pritet_p3", "mixed_hexpri_p3"])
+def test_sparse_operator_product_matches_the_reference(case):
+    """fr_op_spmv_ell (bespoke_SPMV) on the reference's own operators in ELL
+    form: the extrapolation (add_flag 0) and the corrected divergence
+    (add_flag 1) of every element type against the reference's stage arrays."""
+    torch = pytest.importorskip("torch")
+    import hifiles_b200 as H
+    import hifiles_b200.seam as SM
+    L = SM._bind(H.lib())
+    meta, a = load(case)
+    dev = lambda x: torch.from_numpy(np.asfortranarray(x).ravel(order="F").copy()).cuda()  # noqa: E731
+    for t in meta["types"]:
+        X = "t%d_" % t["ele_type"]
+        nu, nf, E, F = t["n_upts"], t["n_fpts"], t["n_eles"], 5
+        d0, i0, z0 = SM.ellpack(a[X + "opp_0"])
+        d3, i3, z3 = SM.ellpack(a[X + "opp_3"])
+        # device copies stay referenced until the products have run
+        D0, I0, D3, I3 = dev(d0), dev(i0), dev(d3), dev(i3)
+        u = dev(a[X + "disu_upts_init"])
+        ufp = torch.zeros(nf * E * F, dtype=torch.float64, device="cuda")
+        st = L.fr_op_spmv_ell(nf, nu, F, E, D0.data_ptr(), I0.data_ptr(), z0, u.data_ptr(), ufp.data_ptr(),
+                              t["ele_type"], meta["order"], 0, None)
+        assert st == 0, H.lib().fr_last_error().decode()
+        jump = dev(a[X + "s10_norm_tconf_fpts"] - a[X + "s08_norm_tdisf_fpts"])
+        div = dev(a[X + "s09_div_tconf_upts"])
+        st = L.fr_op_spmv_ell(nu, nf, F, E, D3.data_ptr(), I3.data_ptr(), z3, jump.data_ptr(),
+                              div.data_ptr(), t["ele_type"], meta["order"], 1, None)
+        assert st == 0, H.lib().fr_last_error().decode()
+        torch.cuda.synchronize()
+        got0 = ufp.cpu().numpy().reshape((nf, E, F), order="F")
+        got3 = div.cpu().numpy().reshape((nu, E, F), order="F")
+        assert rel(got0, a[X + "s01_disu_fpts"]) <= 1e-12
+        assert rel(got3, a[X + "s11_div_tconf_upts"]) <= 1e-12
