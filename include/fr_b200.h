@@ -72,8 +72,11 @@ typedef struct {
 } fr_mesh_desc;
 
 typedef struct {
-  int order;             /* polynomial order P (quads 1..5, hexes 1..5)        */
-  int upts_type;         /* 0 Gauss, 1 Gauss-Lobatto (upts_type_quad/hexa)     */
+  int order;             /* polynomial order P (quads 1..5, hexes 1..4)        */
+  int upts_type;         /* upts_type_quad/hexa: 0 Gauss (the only points the
+                            solver object takes; 1, Gauss-Lobatto, returns
+                            FR_ERR_UNSUPPORTED here and is accepted by
+                            fr_line_operators)                                */
   int vcjh_scheme;       /* 0 VCJH with eta, 1 DG, 2 SD, 3 Hu, 4 c_+           */
   double eta;            /* used when vcjh_scheme == 0                         */
   int viscous;           /* 0 Euler, 1 Navier-Stokes                           */

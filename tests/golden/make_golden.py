@@ -200,6 +200,13 @@ CASES = [
          ic="tgv_mach01", vcjh=1, jitter=0.0, steps=3, dt=1e-3, stages=False),
     dict(name="hex_euler_p3_n3", dims=3, order=3, n=(3, 3, 3), lo=(0, 0, 0), hi=(2 * np.pi,) * 3, viscous=0,
          ic="tgv_mach01", vcjh=1, jitter=0.0, steps=3, dt=1e-3, stages=True),
+    # the ends of the built order range
+    dict(name="quad_vortex_p1_n8_jit", dims=2, order=1, n=(8, 8), lo=(-5, -5), hi=(5, 5), viscous=0,
+         ic="vortex_u1v0", vcjh=1, jitter=0.1, steps=10, dt=1e-3, stages=True),
+    dict(name="quad_vortex_p5_n4", dims=2, order=5, n=(4, 4), lo=(-5, -5), hi=(5, 5), viscous=0,
+         ic="vortex_u1v0", vcjh=2, jitter=0.0, steps=10, dt=1e-3, stages=True),
+    dict(name="hex_tgv_p1_n4_jit", dims=3, order=1, n=(4, 4, 4), lo=(0, 0, 0), hi=(2 * np.pi,) * 3, viscous=1,
+         ic="tgv_mach01", vcjh=2, jitter=0.1, steps=5, dt=1e-3, stages=True),
     # eddy-viscosity LES (input keys LES 1, SGS_model 1 = WALE / 0 = Smagorinsky)
     dict(name="hex_wale_p3_n3_jit", dims=3, order=3, n=(3, 3, 3), lo=(0, 0, 0), hi=(2 * np.pi,) * 3, viscous=1,
          ic="tgv_mach01", vcjh=1, jitter=0.1, steps=5, dt=1e-3, stages=True, les=1, sgs=1, filter_ratio=1.0),

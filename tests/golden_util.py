@@ -14,7 +14,8 @@ ROE_CASES = ["quad_vortex_roe_p3_n6_jit", "quad_ns_roe_p2_n5"]
 BC_CASES = ["quad_bc_euler_p3", "quad_bc_euler2_p2", "quad_bc_roe_p3", "quad_ns_bc_p3", "hex_channel_p2",
             "hex_channel_char_p3"]
 CASES = ["quad_vortex_p3_n6", "quad_vortex_p2_n5_jit", "quad_vortex_p3_n20", "hex_tgv_p3_n3",
-         "hex_tgv_p2_n3_jit", "hex_tgv_p4_n2", "hex_euler_p3_n3"] + LES_CASES + ROE_CASES
+         "hex_tgv_p2_n3_jit", "hex_tgv_p4_n2", "hex_euler_p3_n3", "quad_vortex_p1_n8_jit", "quad_vortex_p5_n4",
+         "hex_tgv_p1_n4_jit"] + LES_CASES + ROE_CASES
 
 
 def load(name):
