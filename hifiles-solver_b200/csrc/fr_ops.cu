@@ -42,7 +42,8 @@ constexpr int kDenseThreads = 256;
 constexpr int kMaxOps = 3;
 constexpr int kSmallOps = 8192;             // operator entries (all nd) staged in shared memory
 constexpr size_t kDenseSmem = 220 * 1024;
-constexpr size_t kStageSmem = 64 * 1024;    // operators are staged while a block stays within this
+constexpr size_t kStageSmem = 64 * 1024;    // fused products stage their operators while a block stays within this
+constexpr size_t kStageSmem1 = 112 * 1024;  // the same for a single product
 
 struct OpSet {
   const double* a[kMaxOps];
@@ -154,7 +155,7 @@ fr_status dense_launch(int m, int k, long long ncols, int nd, const OpSet& ops, 
                        double* Cm, long long sC, int beta, bool fan, cudaStream_t s, size_t smem, unsigned blocks)
 {
   const size_t a_bytes = (size_t)nd * m * k * sizeof(double);
-  const bool sa = (long long)nd * m * k <= kSmallOps && smem + a_bytes <= kStageSmem;
+  const bool sa = (long long)nd * m * k <= kSmallOps && smem + a_bytes <= (nd == 1 ? kStageSmem1 : kStageSmem);
   if (sa) smem += a_bytes;
   auto kern = fan ? (sa ? dense_apply_kernel<RM, true, true, LW> : dense_apply_kernel<RM, false, true, LW>)
                   : (sa ? dense_apply_kernel<RM, true, false, LW> : dense_apply_kernel<RM, false, false, LW>);
@@ -189,7 +190,7 @@ fr_status dense_apply_nd(int m, int k, long long ncols, int nd, const double* co
   const size_t smem1 = ((size_t)k * kTileStride + (size_t)kTileCols * m) * sizeof(double);
   // fused unless one operator could sit in shared memory but all nd cannot:
   // then nd single products with a staged operator are faster
-  const bool split = nd > 1 && (long long)m * k <= kSmallOps && smem1 + a1 <= kStageSmem &&
+  const bool split = nd > 1 && (long long)m * k <= kSmallOps && smem1 + a1 <= kStageSmem1 &&
                      !((long long)nd * m * k <= kSmallOps && smem + nd * a1 <= kStageSmem);
   if (g_gemm_mode || split || (nd > 1 && smem > kDenseSmem)) {
     for (int d = 0; d < nd; d++) {
