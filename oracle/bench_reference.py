@@ -8,7 +8,7 @@ configuration on a smaller periodic box (per-element work is the same; the
 reference is single-threaded and MPI is not built).  Throughput is the sum over
 processes of DOF updates per RK stage per second.
 
-TEST/BASELINE INFRASTRUCTURE ONLY: never part of the product path.
+TEST AND CPU-BASELINE INFRASTRUCTURE ONLY: never part of the product path.
 """
 import json
 import os

@@ -2,7 +2,7 @@
 hifiles_b200.learned_sgs at small scale (fine 32^3 hexes P=3 solved without a
 model, projected onto 8^3 P=3; decaying isotropic turbulence, u_rms 1,
 Mach 0.1, mu 1e-3), trained on the GPU with the library's kernels on two
-snapshots and judged on a third, held out, and by coarse runs from the
+snapshots and evaluated on a third, held out, and by coarse runs from the
 filtered initial field against the filtered fine solution.
 
 Measured on a B200 (seed 1): relative L2 error of the SGS dissipation

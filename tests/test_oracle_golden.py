@@ -65,7 +65,7 @@ def test_oracle_stage_arrays_match_reference(case):
 
 @pytest.mark.slow
 def test_oracle_vortex_1000_steps_matches_reference():
-    """BASELINE 2-D vortex (20x20 quads, P=3, c_dg, Rusanov, RK45, dt 1e-3, 1000 steps)."""
+    """The 2-D isentropic vortex workload (20x20 quads, P=3, c_dg, Rusanov, RK45, dt 1e-3, 1000 steps)."""
     meta, a = load("quad_vortex_p3_n20")
     m = _mesh(meta)
     u, _, nrm = m.rk45(_phys(meta), a["u0"], meta["dt"], meta["steps"])
