@@ -7,6 +7,7 @@
 
 #include <cuda_runtime.h>
 
+#include "fr_face_update.cuh"
 #include "fr_fused.cuh"
 #include "fr_host.hpp"
 
@@ -32,6 +33,8 @@ struct Bufs {
   void* BV = nullptr;              // viscous boundary normal flux (nbdy, F), from the gradient kernel
   int* mate = nullptr;
   unsigned char* side = nullptr;
+  double* idetj = nullptr;         // 1/detJ at the solution points (the update multiplies by it)
+  int* err = nullptr;              // set by a kernel whose bounded wait gave up
 };
 
 struct Tile {
@@ -75,7 +78,7 @@ FR_TILES(2, 5, T_({4, 160}), T_({4, 160}))
 FR_TILES(3, 1, T_({12, 128}), T_({12, 128}))
 FR_TILES(3, 2, T_({4, 128}, {2, 64}, {8, 256}), T_({4, 128}, {2, 64}, {8, 256}))
 FR_TILES(3, 3, T_({2, 128, 4}, {1, 64, 8}, {2, 192, 2}, {2, 128, 3}, {1, 96, 0}, {4, 256, 2}, {1, 96, 5}, {1, 96, 6},
-                  {1, 64, 8, 1}, {2, 128, 3, 1}, {1, 96, 10}), T_({2, 128}, {1, 64}, {4, 256}, {2, 96}, {4, 128}))
+                  {1, 64, 8, 1}, {2, 128, 3, 1}, {1, 96, 10}), T_({2, 192}, {1, 96}, {2, 128}, {1, 64}, {4, 256}, {4, 128}))
 FR_TILES(3, 4, T_({1, 128}, {1, 160}, {2, 256}), T_({1, 128}, {2, 256}, {1, 160}))
 #undef T_
 #undef FR_TILES
@@ -135,7 +138,9 @@ struct RunnerT : Runner {
     }
     return m;
   }
-  int launches_per_stage() const override { return visc ? 3 : 2; }
+  // the bulk-copy kernel folds the interface fluxes into the update (fr_face_update.cuh)
+  static constexpr bool FU = fu_bulk_ok<DIM, P, TC>();
+  int launches_per_stage() const override { return FU ? (visc ? 2 : 1) : (visc ? 3 : 2); }
   void set_riemann(int rs) override { riemann = rs; }
   void trace(const Bufs& b, int cur, cudaStream_t s) override
   {
@@ -189,7 +194,7 @@ struct RunnerT : Runner {
   }
   void face(const Bufs& b, int cur, cudaStream_t s) override
   {
-    if (b.nint + b.nbdy == 0) return;
+    if (FU || b.nint + b.nbdy == 0) return;
     if (DIM == 2 && riemann == 2) {
       if (visc) face_t<1, 2>(b, cur, s);
       else face_t<0, 2>(b, cur, s);
@@ -205,14 +210,35 @@ struct RunnerT : Runner {
     if constexpr (I < NUP) {
       if (I != usel) return update_i<I + 1, VISC, MODE>(b, cur, stage, dt, want_partial, s);
       constexpr int EPB = Tiles<DIM, P>::upd[I].epb, NT = Tiles<DIM, P>::upd[I].nt;
-      constexpr size_t sm = update_smem_bytes<DIM, P, EPB, NT, VISC, MODE, TC>();
-      static bool once = (set_smem((const void*)fr_update_kernel<DIM, P, EPB, NT, VISC, MODE, TC>, sm), true);
-      (void)once;
-      fr_update_kernel<DIM, P, EPB, NT, VISC, MODE, TC><<<(unsigned)((E + EPB - 1) / EPB), NT, sm, s>>>(
-          b.U, b.REG, (TC*)b.UF[cur ^ 1], (const TC*)b.CF, (const TC*)b.ND, (const TC*)b.DV, (const TC*)b.JG,
-          b.detj64, b.DIV, want_partial ? b.partial : nullptr, E, L, ph, kRK4A[stage], kRK4B[stage], dt,
-          stage == 0 ? 1 : 0);
+      if constexpr (FU) {
+        if constexpr (DIM == 2) {
+          if (riemann == 2) fu_launch<EPB, NT, VISC, MODE, 2>(b, cur, stage, dt, want_partial, s);
+          else fu_launch<EPB, NT, VISC, MODE, 0>(b, cur, stage, dt, want_partial, s);
+        } else {
+          fu_launch<EPB, NT, VISC, MODE, 0>(b, cur, stage, dt, want_partial, s);
+        }
+      } else {
+        constexpr size_t sm = update_smem_bytes<DIM, P, EPB, NT, VISC, MODE, TC>();
+        static bool once = (set_smem((const void*)fr_update_kernel<DIM, P, EPB, NT, VISC, MODE, TC>, sm), true);
+        (void)once;
+        fr_update_kernel<DIM, P, EPB, NT, VISC, MODE, TC><<<(unsigned)((E + EPB - 1) / EPB), NT, sm, s>>>(
+            b.U, b.REG, (TC*)b.UF[cur ^ 1], (const TC*)b.CF, (const TC*)b.ND, (const TC*)b.DV, (const TC*)b.JG,
+            b.detj64, b.DIV, want_partial ? b.partial : nullptr, E, L, ph, kRK4A[stage], kRK4B[stage], dt,
+            stage == 0 ? 1 : 0);
+      }
     }
+  }
+  template <int EPB, int NT, int VISC, int MODE, int RS>
+  void fu_launch(const Bufs& b, int cur, int stage, double dt, bool want_partial, cudaStream_t s)
+  {
+    constexpr size_t sm = face_update_smem_bytes<DIM, P, TC, VISC, MODE, EPB, NT>();
+    const void* kfn = (const void*)fr_face_update_kernel<DIM, P, EPB, NT, VISC, MODE, TC, RS>;
+    static bool once = (set_smem(kfn, sm), true);
+    (void)once;
+    fr_face_update_kernel<DIM, P, EPB, NT, VISC, MODE, TC, RS><<<(unsigned)((E + EPB - 1) / EPB), NT, sm, s>>>(
+        b.U, b.REG, (TC*)b.UF[cur ^ 1], (const TC*)b.UF[cur], b.mate, b.side, (const TC*)b.VF, (const TC*)b.ND,
+        (const TC*)b.DV, (const TC*)b.JG, (const TC*)b.nL, (const TC*)b.tdA, b.idetj, (const TC*)b.BV, b.DIV,
+        want_partial ? b.partial : nullptr, E, L, ph, kRK4A[stage], kRK4B[stage], dt, stage == 0 ? 1 : 0, b.err);
   }
   void update(const Bufs& b, int cur, int mode, int stage, double dt, bool want_partial, cudaStream_t s) override
   {

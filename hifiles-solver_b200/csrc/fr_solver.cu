@@ -118,6 +118,11 @@ fr_status upload_geometry(fr_solver* s)
   if ((st = upload_tc(s, s->b.tdA, m.tdA))) return st;
   if ((st = upload_tc(s, s->b.nL, m.nL))) return st;
   FR_CUDA(cudaMemcpy(s->b.detj64, m.detjac.data(), m.detjac.size() * 8, cudaMemcpyHostToDevice));
+  {
+    std::vector<double> inv(m.detjac.size());
+    for (size_t i = 0; i < inv.size(); i++) inv[i] = 1.0 / m.detjac[i];
+    FR_CUDA(cudaMemcpy(s->b.idetj, inv.data(), inv.size() * 8, cudaMemcpyHostToDevice));
+  }
   FR_CUDA(cudaMemcpy(s->b.mate, m.mate.data(), m.mate.size() * sizeof(int), cudaMemcpyHostToDevice));
   std::vector<unsigned char> side(m.mate.size());
   size_t E = m.ne;
@@ -156,6 +161,20 @@ fr_status check_launch(const char* what)
 {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(FR_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  return FR_OK;
+}
+
+// A kernel whose bounded wait gave up has set the solver's error flag; read
+// (and clear) it at the points where the host waits for the device anyway.
+fr_status check_device_flag(fr_solver* s, cudaStream_t st)
+{
+  int h = 0;
+  FR_CUDA(cudaMemcpyAsync(&h, s->b.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  FR_CUDA(cudaStreamSynchronize(st));
+  if (h) {
+    FR_CUDA(cudaMemsetAsync(s->b.err, 0, sizeof(int), st));
+    return fail(FR_ERR_TIMEOUT, "a stage kernel's wait for its bulk copies timed out");
+  }
   return FR_OK;
 }
 
@@ -267,6 +286,8 @@ static fr_status create_with_mesh(Mesh&& mesh, const Line1D& line, const fr_sche
   if ((st = dalloc(s.get(), &s->b.REG, nu * E * F))) return st;
   if ((st = dalloc(s.get(), &s->b.DIV, nu * E * F))) return st;
   if ((st = dalloc(s.get(), &s->b.detj64, nu * E))) return st;
+  if ((st = dalloc(s.get(), &s->b.idetj, nu * E))) return st;
+  if ((st = dalloc(s.get(), &s->b.err, 1))) return st;
   char* p;
   for (int i = 0; i < 2; i++) { if ((st = dalloc(s.get(), &p, nf * E * F * tc))) return st; s->b.UF[i] = p; }
   if (sd->viscous) {
@@ -296,6 +317,7 @@ static fr_status create_with_mesh(Mesh&& mesh, const Line1D& line, const fr_sche
   if ((st = dalloc(s.get(), &s->ke_partial, (size_t)s->nblk_ke))) return st;
   if ((st = dalloc(s.get(), &s->ke_out, 1))) return st;
   FR_CUDA(cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking));
+  FR_CUDA(cudaMemset(s->b.err, 0, sizeof(int)));
   FR_CUDA(cudaMemset(s->b.U, 0, nu * E * F * 8));
   FR_CUDA(cudaMemset(s->b.REG, 0, nu * E * F * 8));
   if ((st = upload_geometry(s.get()))) return st;
@@ -479,7 +501,7 @@ fr_status fr_solver_residual(fr_solver* s, double* host_div, void* stream)
   size_t n = (size_t)s->mesh.nu * s->mesh.ne * s->mesh.nfields;
   FR_CUDA(cudaMemcpyAsync(host_div, s->b.DIV, n * 8, cudaMemcpyDeviceToHost, st));
   FR_CUDA(cudaStreamSynchronize(st));
-  return FR_OK;
+  return check_device_flag(s, st);
 }
 
 fr_status fr_solver_rk_stage(fr_solver* s, int st, double dt, void* stream)
@@ -548,6 +570,8 @@ static fr_status advance_impl(fr_solver* s, int n_steps, double dt, double* norm
     FR_CUDA(cudaMemcpyAsync(norms_host, s->b.norms, F * 8, cudaMemcpyDeviceToHost, st));
     if (!wait) return FR_OK;
     FR_CUDA(cudaStreamSynchronize(st));
+    fr_status fl = check_device_flag(s, st);
+    if (fl) return fl;
     for (int k = 0; k < F; k++)
       if (!std::isfinite(norms_host[k])) return fail(FR_ERR_NONFINITE, "NaN/Inf in the residual");
   }
@@ -737,7 +761,7 @@ fr_status fr_solver_sync(fr_solver* s)
   if (!s) return fail(FR_ERR_ARG, "null solver");
   FR_CUDA(cudaSetDevice(s->device));
   FR_CUDA(cudaStreamSynchronize(s->own_stream));
-  return FR_OK;
+  return check_device_flag(s, s->own_stream);
 }
 
 }  // extern "C"
