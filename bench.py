@@ -18,7 +18,6 @@ max over ranks.  `--impl reference` times the reference's own CPU code
 (oracle/_ref, built from the reference sources) on the host cores.
 """
 import argparse
-import re
 import json
 import os
 import subprocess
@@ -46,6 +45,14 @@ def tgv_state(pos):
     v = -np.cos(x) * np.sin(y) * np.cos(z)
     return np.asfortranarray(np.stack([np.ones_like(x), u, v, np.zeros_like(x),
                                        p / (GAMMA - 1.0) + 0.5 * (u * u + v * v)], axis=-1))
+
+
+# DRAM bytes per element of one RK stage (dram__bytes_read.sum +
+# dram__bytes_write.sum of the gradient and interface/update kernels, summed
+# over one stage), from the full-size ncu capture of the bench workload with
+# these tiles (grad elements/CTA, threads, update elements/CTA, threads);
+# profiles/dram_tgv32_p3_fp64.md gives the command and the per-kernel split.
+MEASURED_TRAFFIC = {("fp64", 32, 3, (1, 64, 1, 64)): 53255}
 
 
 def alg_bytes_per_element(dims, P, viscous, s=8, m=8, t=8):
@@ -438,7 +445,13 @@ def run_b200(a, rank, world, local):
                      precision=1 if a.precision == "fp32" else 0, device=dev)
     u0 = tgv_state(s.geometry()["pos_upts"])
     s.set_state(u0)
-    tiles = s.autotune(5) if not a.no_tune else None
+    if a.tiles:
+        g, u = (int(x) for x in a.tiles.split(","))
+        s.select_tiles(g, u)
+        ti = s.tile_info(0, g), s.tile_info(1, u)
+        tiles = (ti[0][0], ti[0][1], ti[1][0], ti[1][1])
+    else:
+        tiles = s.autotune(5) if not a.no_tune else None
     dt = 1e-3
     E, nu, F = s.n_eles, s.n_upts, s.n_fields
     dof_step = E * nu * F * 5
@@ -477,14 +490,10 @@ def run_b200(a, rank, world, local):
     tc = 4 if a.precision == "fp32" else 8
     b_elem = alg_bytes_per_element(3, P, True, s=8, m=tc, t=tc)
     achieved = b_elem * E / (stage_ms * 1e-3) / 1e9
-    # measured DRAM bytes of one stage (the three kernels), from the ncu
-    # capture summarised in profiles/ (a line "DRAM bytes per element per stage: N")
-    traffic = None
-    tr_path = os.path.join(REPO, "profiles", "dram_tgv%d_p%d_%s.md" % (n, P, a.precision))
-    if os.path.exists(tr_path):
-        m = re.search(r"DRAM bytes per element per stage:\s*(\d+)", open(tr_path).read())
-        if m:
-            traffic = int(m.group(1)) * E
+    # DRAM bytes of one stage from an ncu capture of the same kernels and tiles
+    # (MEASURED_TRAFFIC); null when this run's autotuner picked other tiles
+    key = (a.precision, n, P, tuple(tiles) if tiles else None)
+    traffic = MEASURED_TRAFFIC[key] * E if key in MEASURED_TRAFFIC else None
 
     # --- end to end through the public API with host buffers
     pinned = torch.empty(u0.size, dtype=torch.float64, pin_memory=True)
@@ -538,11 +547,13 @@ def run_b200(a, rank, world, local):
                    "parallelism": "replicas" if world > 1 else "single GPU",
                    "tiles": {"grad_elements_per_cta": tiles[0], "grad_threads": tiles[1],
                              "update_elements_per_cta": tiles[2], "update_threads": tiles[3]} if tiles else None},
-        "roofline": {"bound": "hbm", "kernel": "one RK stage = fr_grad_kernel + fr_face_kernel + fr_update_kernel",
+        "roofline": {"bound": "hbm", "kernel": "one RK stage = fr_grad_kernel + fr_face_update_kernel",
                      "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / pk["hbm_gbs"], "peak_source": pk_src,
                      "alg_bytes_per_element": b_elem, "traffic": traffic,
-                     "ms_grad": ms_grad, "ms_face": ms_face, "ms_update": ms_upd, "ms_stage": stage_ms},
+                     "ms_grad": ms_grad, "ms_face_update": ms_upd, "ms_stage": stage_ms,
+                     "traffic_source": ("ncu capture, tiles %s" % (key[3],)) if traffic else
+                     "no ncu capture of this run's tiles"},
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
         "forms": forms,
     }
@@ -560,6 +571,7 @@ def main():
     ap.add_argument("--order", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--tiles", default="", help="gradient,update tile indices instead of autotuning (for captures)")
     ap.add_argument("--no-forms", action="store_true", help="skip the FP32 and batched forms")
     a = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))

@@ -2,11 +2,11 @@
 
 Runs the unmodified reference objects (oracle/_ref/ref_harness: the
 reference's set-up, CalcResidual and eles::AdvanceSolution, with a wall clock
-around its time-step loop) as independent processes, one per host thread, each
-on a bounded sample of the bench workload: the same TGV P=3 Navier-Stokes
-configuration on a smaller periodic box (per-element work is the same; the
-reference is single-threaded and MPI is not built).  Throughput is the sum over
-processes of DOF updates per RK stage per second.
+around its time-step loop) as independent processes, one per host thread (the
+reference is single-threaded and MPI is not built).  `run` (bench.py --impl
+reference) times the bench configuration itself; `measure` with a smaller box
+is the bounded sample behind bench.py's cpu_baseline.  Throughput is the sum
+over processes of DOF updates per RK stage per second.
 
 TEST AND CPU-BASELINE INFRASTRUCTURE ONLY: never part of the product path.
 """
@@ -66,16 +66,59 @@ def measure(n=10, P=3, steps=4, procs=None, dt=1e-3):
             "seconds": secs}
 
 
+def host_cpu():
+    """CPU model, logical and physical core counts of this host (from /proc/cpuinfo)."""
+    model, phys = "unknown", set()
+    try:
+        cur = {}
+        for line in open("/proc/cpuinfo"):
+            if ":" not in line:
+                if cur:
+                    phys.add((cur.get("physical id"), cur.get("core id")))
+                cur = {}
+                continue
+            k, v = [x.strip() for x in line.split(":", 1)]
+            cur[k] = v
+            if k == "model name":
+                model = v
+        if cur:
+            phys.add((cur.get("physical id"), cur.get("core id")))
+    except OSError:
+        pass
+    return {"model": model, "logical": os.cpu_count() or 1, "physical": len(phys) or None}
+
+
+def mem_available_bytes():
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable:"):
+                return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return None
+
+
 def run(a):
-    steps = max(1, min(a.steps, 6))
-    r = measure(n=10, P=a.order, steps=steps)
+    """The reference arm on the bench configuration itself (TGV n^3, P=3):
+    one single-threaded reference process per host thread, as many as the
+    host memory holds (about 0.7 GB per 16^3 hexes per process, measured),
+    each timing a.steps (at most 2) RK45 steps of the full mesh."""
+    steps = max(1, min(a.steps, 2))
+    need = 0.75e9 * (a.n / 16.0) ** 3
+    avail = mem_available_bytes()
+    procs = os.cpu_count() or 1
+    if avail:
+        procs = max(1, min(procs, int(0.8 * avail // need)))
+    r = measure(n=a.n, P=a.order, steps=steps, procs=procs)
+    cpu = host_cpu()
+    r["sample"] += "; host %s, %d logical / %s physical cores" % (cpu["model"], cpu["logical"], cpu["physical"])
     out = {
         "impl": "reference", "metric": "RK-stage DOF-updates/s (TGV P=3)", "value": r["value"],
         "unit": "DOF-updates/s", "n_gpus": 0, "steps": steps, "warmup": 0, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic TGV initial field)",
         "config": {"workload": "TGV %d^3 hex P=%d Navier-Stokes (Re 1600, Mach 0.1, Pr 0.71), Rusanov+LDG, c_dg, RK45"
                                % (a.n, a.order),
-                   "sample": r["sample"]},
+                   "sample": r["sample"], "same_config": True, "host_cpu": cpu},
         "cpu_baseline": {"value": r["value"], "unit": "DOF-updates/s", "cores": r["procs"], "kind": "reference",
                          "sample": r["sample"]},
         "e2e": {"value": r["value"], "unit": "DOF-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
