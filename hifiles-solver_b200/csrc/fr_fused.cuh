@@ -428,7 +428,8 @@ __host__ __device__ constexpr bool grad_alias()
 // Outputs VF (n_fpts, n_eles, F-1), ND (n_fpts, n_eles, F), DV (n_upts, n_eles, F),
 // BV (n_boundary_points, F) the viscous normal flux at boundary points (side
 // bits 2.. hold the boundary type, mate = -1 - position in the boundary
-// list), and, when GRAD is not null, the corrected physical gradient
+// list; with BV null the mesh has no boundary points and those bits are
+// ignored), and, when GRAD is not null, the corrected physical gradient
 // grad_disu_upts (n_upts, n_eles, F, D).
 template <int DIM, int P, int EPB, int NT, typename TC, int LES = 0, int MINB = 1, int VEC = 1, int PERS = 0>
 __global__ void __launch_bounds__(NT, MINB)
@@ -566,7 +567,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
       for (int m = 0; m <= P; m++) acc = acc + FR_SU(el, k, sl[m]) * Lc[m];
       return acc;
     };
-    if (psd[it] >> 2) {
+    if (BV && (psd[it] >> 2)) {
       BdyPoint<D, TC> q;
 #pragma unroll
       for (int k = 0; k < F; k++) q.u[k] = trace(k);
@@ -811,7 +812,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
         for (int k = 0; k < F; k++) uf[k] = FR_SUF(el, k, f);
 #pragma unroll
         for (int d = 0; d < D; d++) n[d] = PERS ? nL[own + NFE * d] : FR_SN(el, d * NF + f);
-        const int btype = sSide[el * NF + f] >> 2;
+        const int btype = BV ? sSide[el * NF + f] >> 2 : 0;
         if constexpr (LES == 0) {
           // the projection is accumulated as the flux is formed (no full flux held)
           if (btype) {
@@ -911,7 +912,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
       }
 #pragma unroll
       for (int d = 0; d < D; d++) n[d] = PERS ? nL[own + NFE * d] : FR_SN(el, d * NF + f);
-      const int btype = psd[it] >> 2;
+      const int btype = BV ? psd[it] >> 2 : 0;
       if constexpr (LES == 0) {
         // the projection is accumulated as the flux is formed (no full flux held)
         if (btype) {

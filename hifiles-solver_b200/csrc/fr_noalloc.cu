@@ -43,7 +43,10 @@ fr_status na_fail(fr_status s, const char* m)
 }
 
 // Set-up, once per device, with that device current: the device address of
-// the scratch array (its name in host code is only a stand-in).
+// the scratch array (its name in host code is only a stand-in).  The address
+// is kept for the life of the process, so the entry point must not be used
+// after a cudaDeviceReset of that device (the module, and the array with it,
+// is reloaded elsewhere).
 fr_status scratch_for_device(int dev, double** out)
 {
   if (dev < 0 || dev >= kMaxDevices) return na_fail(FR_ERR_ARG, "device index out of range");
@@ -101,14 +104,16 @@ fr_status run(const fr_residual_args* a, double* scratch, cudaStream_t s)
   const long long E = a->n_eles, NFE = (long long)S::NF * E;
   const int F = S::F;
   const bool visc = a->viscous != 0;
-  size_t need = (size_t)NFE * F * 2 + (size_t)S::NU * E * F;                  // UF, CF, DV
-  if (visc) need += (size_t)NFE * (F - 1) + (size_t)NFE * F;                  // VF, ND
+  // UF and CF always; the divergence DV, viscous projections VF and normal
+  // flux ND only on the viscous path (the Euler path forms them in the update)
+  size_t need = (size_t)NFE * F * 2;
+  if (visc) need += (size_t)S::NU * E * F + (size_t)NFE * (F - 1) + (size_t)NFE * F;
   if (need > kScratchDoubles) return na_fail(FR_ERR_ARG, "mesh too large for the fixed 32 MiB residual scratch");
   double* UF = scratch;
   double* CF = UF + NFE * F;
-  double* DV = CF + NFE * F;
-  double* VF = DV + (size_t)S::NU * E * F;
-  double* ND = VF + NFE * (F - 1);
+  double* DV = visc ? CF + NFE * F : nullptr;
+  double* VF = visc ? DV + (size_t)S::NU * E * F : nullptr;
+  double* ND = visc ? VF + NFE * (F - 1) : nullptr;
   Line<double> L;
   if (!make_line_noalloc(P, a->upts_type, a->vcjh_scheme, a->eta, L))
     return na_fail(FR_ERR_ARG, "unsupported point type or VCJH scheme for this order");

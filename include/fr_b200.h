@@ -488,8 +488,14 @@ fr_status fr_op_check(void* stream);
  * device looks up that array's device address, so make the first call before
  * any stream capture.  All calls share the array: calls whose work overlaps on
  * the GPU (different streams, different host threads) race and must be
- * serialised by the caller.  Meshes whose scratch would exceed 32 MiB are
- * rejected with FR_ERR_ARG (hex P=3 Navier-Stokes: ~1950 elements).
+ * serialised by the caller.  The looked-up address is kept for the life of
+ * the process: do not use this entry point after cudaDeviceReset on that
+ * device.  Meshes whose scratch would exceed 32 MiB are rejected with
+ * FR_ERR_ARG (hex P=3: ~1950 Navier-Stokes or ~4350 Euler elements).
+ * The mesh has no boundary points: every flux point is an interior point that
+ * appears in face_lr, mate >= 0 everywhere, and side bits 2..7 are zero (they
+ * are ignored).  Periodic meshes qualify; walled meshes go through the solver
+ * object or the per-operator boundary entry points.
  * Output: div_tconf_upts of one CalcResidual, FP64, identical to
  * fr_solver_residual on the same mesh and state.
  * ---------------------------------------------------------------------- */

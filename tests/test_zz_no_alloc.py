@@ -81,13 +81,17 @@ def _args(s, meta, keep, n_int, u_dev, out_dev):
                         keep["face"].data_ptr(), keep["fsign"].data_ptr(), out_dev.data_ptr())
 
 
-CASES = [
-    dict(dims=3, order=3, n=(3, 3, 2), lo=(0, 0, 0), hi=(2 * np.pi,) * 3, jitter=0.1, viscous=True, vcjh=1),
-    dict(dims=2, order=3, n=(6, 5), lo=(-5, -5), hi=(5, 5), jitter=0.15, viscous=False, vcjh=2),
-]
+# every (dims, order) the entry point is built for, Navier-Stokes and Euler,
+# on small jittered periodic boxes
+CASES = ([dict(dims=3, order=P, n=(3, 3, 2), lo=(0, 0, 0), hi=(2 * np.pi,) * 3, jitter=0.1, viscous=v, vcjh=1)
+          for P in (1, 2, 3, 4) for v in (True, False)] +
+         [dict(dims=2, order=P, n=(6, 5), lo=(-5, -5), hi=(5, 5), jitter=0.15, viscous=v, vcjh=2)
+          for P in (1, 2, 3, 4, 5) for v in (True, False)])
+IDS = ["%s_p%d_%s" % ("hex" if c["dims"] == 3 else "quad", c["order"], "ns" if c["viscous"] else "euler")
+       for c in CASES]
 
 
-@pytest.mark.parametrize("case", CASES, ids=["hex_p3_ns", "quad_p3_euler"])
+@pytest.mark.parametrize("case", CASES, ids=IDS)
 def test_noalloc_residual_matches_solver_on_two_calls(case):
     meta = dict(case, gamma=1.4, prandtl=0.71, mu_inf=1.0 / 1600.0, tau=1.0, pen_fact=0.5)
     s = H.Solver.box(case["dims"], case["order"], case["n"], case["lo"], case["hi"], jitter=case["jitter"], seed=5,
