@@ -35,7 +35,7 @@ def _prepare(work, n, P, dt):
 def measure(n=10, P=3, steps=4, procs=None, dt=1e-3):
     """Aggregate DOF-updates/s of `procs` concurrent reference processes."""
     if not os.path.exists(HARNESS):
-        raise FileNotFoundError("oracle/_ref/ref_harness is not built (make -C oracle ref)")
+        raise FileNotFoundError("oracle/_ref/ref_harness is not built (make -C oracle REF=<reference checkout> ref)")
     procs = procs or os.cpu_count() or 1
     work = tempfile.mkdtemp(prefix="fr_refbench_")
     _prepare(work, n, P, dt)

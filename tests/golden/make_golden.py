@@ -2,8 +2,8 @@
 """Generate the golden fixtures in tests/golden/ by running the reference itself.
 
 Runs only where the reference sources are available (it reads them under
-REF, default /root/reference) and where oracle/_ref/ref_harness has been built
-(`make -C oracle ref`).  For every case it
+--ref or HIFILES_REF) and where oracle/_ref/ref_harness has been built
+(`make -C oracle REF=<reference checkout> ref`).  For every case it
 
   1. writes a periodic box mesh (Gambit neutral format, the reader of
      src/geometry.cpp:1706-1880 and 1122-1307) and an input file derived from
@@ -22,7 +22,7 @@ The regression known-answer values of the reference's TGV test
 (testcases/regression_tests.py:300-310) are recorded in kat.json together
 with the value this script reproduces with the oracle.
 
-Usage:  python tests/golden/make_golden.py [--ref /root/reference]
+Usage:  python tests/golden/make_golden.py --ref <reference checkout>   (or HIFILES_REF=<dir>)
 """
 import argparse
 import json
@@ -324,7 +324,8 @@ def restart_read_fixture(ref, work):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("HIFILES_REF"), required="HIFILES_REF" not in os.environ,
+                    help="the reference checkout (or set HIFILES_REF)")
     ap.add_argument("--work", default=None)
     a = ap.parse_args()
     if not os.path.exists(HARNESS):

@@ -3,7 +3,7 @@
 running the reference itself.
 
 TEST INFRASTRUCTURE ONLY.  Runs where the reference sources are available and
-oracle/_ref/ref_harness is built (`make -C oracle ref`).  For every case it
+oracle/_ref/ref_harness is built (`make -C oracle REF=<reference checkout> ref`).  For every case it
 
   1. writes a jittered periodic box of mixed elements as a Gambit neutral file
      (element reader src/geometry.cpp:1706-1880: linear tets = Gambit type 6,
@@ -30,7 +30,7 @@ reference has no element for, so hexes and tets never share a face):
     for the second half (hex and prism meet on quadrilateral faces), periodic.
 Interior vertices move by a seeded jitter of up to `jitter` cell sizes.
 
-Usage:  python tests/golden/make_mixed.py [--ref /root/reference]
+Usage:  python tests/golden/make_mixed.py --ref <reference checkout>   (or HIFILES_REF=<dir>)
 """
 import argparse
 import itertools
@@ -294,7 +294,8 @@ def pack(out_dir, arr, par, meta):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("HIFILES_REF"), required="HIFILES_REF" not in os.environ,
+                    help="the reference checkout (or set HIFILES_REF)")
     ap.add_argument("--work", default=None)
     a = ap.parse_args()
     if not os.path.exists(G.HARNESS):
