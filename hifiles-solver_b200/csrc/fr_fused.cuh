@@ -1397,36 +1397,4 @@ fr_norm_finalize(const double* __restrict__ partial, int nblk, int F, double inv
   if (threadIdx.x == 0) out[k] = s[0] * inv_n;
 }
 
-// Kinetic energy: per-element quadrature with the point weights, block partials.
-template <int DIM, int P>
-__global__ void fr_ke_kernel(const double* __restrict__ U, const double* __restrict__ detj, long long E,
-                             Line<double> L, double* __restrict__ partial)
-{
-  using S = Shape<DIM, P>;
-  __shared__ double sred[32];
-  double acc = 0.0;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < E * S::NU;
-       i += (long long)gridDim.x * blockDim.x) {
-    long long e = i / S::NU;
-    int u = (int)(i - e * S::NU), a, b, c;
-    upt_abc<DIM, P>(u, a, b, c);
-    double w = L.w[a] * L.w[b] * (DIM == 3 ? L.w[c] : 1.0);
-    double rho = U[u + (size_t)S::NU * e], m2 = 0.0;
-#pragma unroll
-    for (int d = 0; d < DIM; d++) {
-      double mm = U[u + (size_t)S::NU * (e + E * (1 + d))];
-      m2 += mm * mm;
-    }
-    acc += w * detj[u + (size_t)S::NU * e] * 0.5 * m2 / rho;
-  }
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-  if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = acc;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int i = 0; i < (int)(blockDim.x >> 5); i++) s += sred[i];
-    partial[blockIdx.x] = s;
-  }
-}
-
 }  // namespace frb

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <unordered_map>
 
@@ -264,6 +265,85 @@ static void map_point(const Mesh& m, long long e, const double* r, double* pos, 
       double s = 0.0;
       for (int i = 0; i < ns; i++) s += dN[i + ns * k] * m.xv[(size_t)D * cv[i] + j];
       J[j + D * k] = s;
+    }
+}
+
+// n-point Gauss-Legendre rule on [-1, 1]: Newton's iteration on the Legendre
+// three-term recurrence from the Chebyshev-like first guesses
+// cos(pi (i + 3/4) / (n + 1/2)), weights 2 / ((1 - x^2) P_n'(x)^2).
+static void gauss_legendre(int n, double* x, double* w)
+{
+  const double pi = 3.14159265358979323846;
+  for (int i = 0; i < n; i++) {
+    double z = std::cos(pi * (i + 0.75) / (n + 0.5)), dp = 0.0;
+    for (int it = 0; it < 100; it++) {
+      double p0 = 1.0, p1 = z;
+      for (int k = 2; k <= n; k++) {
+        const double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+        p0 = p1;
+        p1 = p2;
+      }
+      if (n == 1) { p1 = z; p0 = 1.0; }
+      dp = n * (z * p1 - p0) / (z * z - 1.0);
+      const double dz = p1 / dp;
+      z -= dz;
+      if (std::fabs(dz) < 1e-16) break;
+    }
+    x[n - 1 - i] = z;
+    w[n - 1 - i] = 2.0 / ((1.0 - z * z) * dp * dp);
+  }
+}
+
+int volume_cubature(int dims, int rule, std::vector<double>& loc, std::vector<double>& w)
+{
+  if (rule < 1 || rule > 12 || (dims != 2 && dims != 3)) return 0;
+  double x[12], wx[12];
+  if (rule == 1) { x[0] = 0.0; wx[0] = 2.0; }
+  else gauss_legendre(rule, x, wx);
+  const int n = dims == 2 ? rule * rule : rule * rule * rule;
+  loc.assign((size_t)dims * n, 0.0);
+  w.assign((size_t)n, 0.0);
+  for (int q = 0; q < n; q++) {
+    int i0, i1, i2 = 0;
+    if (dims == 2) {               // quads: first coordinate fastest
+      i0 = q % rule; i1 = q / rule;
+      loc[2 * q] = x[i0]; loc[2 * q + 1] = x[i1];
+      w[q] = wx[i0] * wx[i1];
+    } else {                       // hexes: first coordinate slowest
+      i0 = q / (rule * rule); i1 = (q / rule) % rule; i2 = q % rule;
+      loc[3 * q] = x[i0]; loc[3 * q + 1] = x[i1]; loc[3 * q + 2] = x[i2];
+      w[q] = wx[i0] * wx[i1] * wx[i2];
+    }
+  }
+  return n;
+}
+
+void volume_cubature_setup(const Mesh& m, const Line1D& L, int nc, const double* loc, std::vector<double>& opp,
+                           std::vector<double>& detj)
+{
+  const int D = m.dims, n1 = m.n1, nu = m.nu;
+  const size_t E = m.ne;
+  opp.assign((size_t)nc * nu, 0.0);
+  for (int j = 0; j < nc; j++)
+    for (int k = 0; k < nu; k++) {
+      const int a = k % n1, b = (k / n1) % n1, c = D == 3 ? k / (n1 * n1) : 0;
+      double v = lagrange(loc[D * j], a, L.loc, n1) * lagrange(loc[D * j + 1], b, L.loc, n1);
+      if (D == 3) v = v * lagrange(loc[D * j + 2], c, L.loc, n1);
+      opp[j + (size_t)nc * k] = v;
+    }
+  detj.assign((size_t)nc * E, 0.0);
+  for (size_t e = 0; e < E; e++)
+    for (int j = 0; j < nc; j++) {
+      double p[3], J[9];
+      map_point(m, (long long)e, &loc[D * j], p, J);
+      double det;
+      if (D == 2) {
+        det = J[0] * J[3] - J[2] * J[1];
+      } else {
+        det = J[0] * (J[4] * J[8] - J[7] * J[5]) - J[3] * (J[1] * J[8] - J[7] * J[2]) +
+              J[6] * (J[1] * J[5] - J[4] * J[2]);
+      }
+      detj[j + (size_t)nc * e] = det;
     }
 }
 

@@ -67,6 +67,20 @@ struct Mesh {
   std::vector<unsigned char> bt;
 };
 
+// Default volume cubature of the integral diagnostics: the tensor
+// Gauss-Legendre rule of `rule` points per direction in the reference's point
+// order (quads: first coordinate fastest; hexes: first coordinate slowest),
+// in full double precision (the reference's data/cubature_{quad,hexa}.dat
+// print the same rules to 12-15 significant digits).  Returns the point count
+// (0 for an unsupported rule); loc is (dims, n) with the point index slowest.
+int volume_cubature(int dims, int rule, std::vector<double>& loc, std::vector<double>& w);
+// The reference's interpolation to the cubature points, opp(j, k) = the
+// nodal basis of solution point k at cubature point j (nc, nu), first index
+// fastest (eles::set_opp_volume_cubpts, src/eles.cpp:4111-4130), and the
+// Jacobian determinant at every cubature point (nc, ne) (src/eles.cpp:5320-5352).
+void volume_cubature_setup(const Mesh& m, const Line1D& L, int nc, const double* loc, std::vector<double>& opp,
+                           std::vector<double>& detj);
+
 // Local point sets (reference orderings) of the element type.
 void element_points(int dims, const Line1D& L, std::vector<double>& loc_upts, std::vector<double>& tloc_fpts,
                     std::vector<double>& tnorm_fpts);

@@ -48,7 +48,6 @@ struct Runner {
   virtual void grad(const Bufs& b, int cur, cudaStream_t s) = 0;
   virtual void face(const Bufs& b, int cur, cudaStream_t s) = 0;
   virtual void update(const Bufs& b, int cur, int mode, int stage, double dt, bool want_partial, cudaStream_t s) = 0;
-  virtual void ke(const Bufs& b, double* partial, int nblk, cudaStream_t s) = 0;
   virtual int flux_blocks() const = 0;      // blocks of the update kernel (norm partials)
   virtual int max_flux_blocks() const = 0;  // over all update-kernel tiles
   virtual int launches_per_stage() const = 0;
@@ -249,10 +248,6 @@ struct RunnerT : Runner {
       if (mode == 0) update_i<0, 0, 0>(b, cur, stage, dt, false, s);
       else update_i<0, 0, 1>(b, cur, stage, dt, want_partial, s);
     }
-  }
-  void ke(const Bufs& b, double* partial, int nblk, cudaStream_t s) override
-  {
-    fr_ke_kernel<DIM, P><<<nblk, 256, 0, s>>>(b.U, b.detj64, E, L64, partial);
   }
 };
 

@@ -18,12 +18,15 @@ namespace frb {
 
 thread_local std::string g_err;
 
+// blocks of the integral-diagnostics kernel (partial sums added in block order)
+constexpr int kDiagBlocks = 296;
+
 cudaError_t launch_sgs_inputs(int dims, int tc_size, const double* U, const void* G, const double* detj, long long npts,
                               int nu, long long E, int order, double filter_ratio, float* X, cudaStream_t st);
 void mlp_default_params(float* w);
-cudaError_t launch_diagnostics(int dims, int tc_size, const double* U, const void* G, const double* detj,
-                               const double* W, long long npts, int nu, double gamma, double* partial, int nblk,
-                               double* out, cudaStream_t st);
+cudaError_t launch_diagnostics(int dims, int tc_size, const double* U, const void* G, const double* opp,
+                               const double* W, const double* detj, long long E, int nu, int nc, double gamma,
+                               double* partial, int nblk, double* out, cudaStream_t st);
 
 static fr_status fail(fr_status s, const std::string& msg)
 {
@@ -68,13 +71,17 @@ struct fr_solver {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   double graph_dt[2] = {0, 0};
   long long launches = 0;
-  int nblk_ke = 0;
-  double* ke_partial = nullptr;
-  double* ke_out = nullptr;
+  // volume cubature of the integral diagnostics (reference volume_cub_order
+  // 3 by default): points (dims, nc), weights, and on the device the
+  // interpolation rows, weights and Jacobians at the cubature points
+  int vc_n = 0;
+  std::vector<double> vc_loc, vc_w;
+  bool vc_dirty = true;
+  double *vc_opp = nullptr, *vc_wd = nullptr, *vc_detj = nullptr;
   float* mlp = nullptr;             // learned-closure parameters (sgs_model 5)
   void* grad_buf = nullptr;         // gradient output of fr_solver_gradient (allocated on first use)
   float* feat_buf = nullptr;        // closure inputs of fr_solver_sgs_features (allocated on first use)
-  double *diag_w = nullptr, *diag_partial = nullptr, *diag_out = nullptr;   // integral diagnostics
+  double *diag_partial = nullptr, *diag_out = nullptr;   // integral diagnostics
   // asynchronous state upload (fr_solver_set_state_async): a device staging
   // copy of the state, filled on its own stream while earlier steps run
   double* staging = nullptr;
@@ -313,9 +320,9 @@ static fr_status create_with_mesh(Mesh&& mesh, const Line1D& line, const fr_sche
   if ((st = dalloc(s.get(), &s->b.side, nf * E))) return st;
   if ((st = dalloc(s.get(), &s->b.partial, (size_t)s->run->max_flux_blocks() * F))) return st;
   if ((st = dalloc(s.get(), &s->b.norms, F))) return st;
-  s->nblk_ke = 296;
-  if ((st = dalloc(s.get(), &s->ke_partial, (size_t)s->nblk_ke))) return st;
-  if ((st = dalloc(s.get(), &s->ke_out, 1))) return st;
+  s->vc_n = volume_cubature(m.dims, 3, s->vc_loc, s->vc_w);
+  if ((st = dalloc(s.get(), &s->diag_partial, (size_t)kDiagBlocks * 5))) return st;
+  if ((st = dalloc(s.get(), &s->diag_out, 5))) return st;
   FR_CUDA(cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking));
   FR_CUDA(cudaMemset(s->b.err, 0, sizeof(int)));
   FR_CUDA(cudaMemset(s->b.U, 0, nu * E * F * 8));
@@ -383,6 +390,7 @@ fr_status fr_solver_set_geometry(fr_solver* s, const double* detj, const double*
   finish_wiring(m);
   FR_CUDA(cudaSetDevice(s->device));
   drop_graphs(s);
+  s->vc_dirty = true;
   return upload_geometry(s);
 }
 
@@ -578,18 +586,70 @@ static fr_status advance_impl(fr_solver* s, int n_steps, double dt, double* norm
   return FR_OK;
 }
 
+// The device copies of the volume cubature (interpolation rows, weights,
+// Jacobians at the cubature points), rebuilt after the rule or the geometry changed.
+static fr_status volume_cubature_ready(fr_solver* s)
+{
+  if (!s->vc_dirty) return FR_OK;
+  const Mesh& m = s->mesh;
+  std::vector<double> opp, dj;
+  volume_cubature_setup(m, s->line, s->vc_n, s->vc_loc.data(), opp, dj);
+  for (void* p : {(void*)s->vc_opp, (void*)s->vc_wd, (void*)s->vc_detj})
+    if (p) {
+      for (size_t i = 0; i < s->allocs.size(); i++)
+        if (s->allocs[i] == p) { s->allocs.erase(s->allocs.begin() + i); break; }
+      cudaFree(p);
+    }
+  s->vc_opp = s->vc_wd = s->vc_detj = nullptr;
+  fr_status r;
+  if ((r = dalloc(s, &s->vc_opp, opp.size()))) return r;
+  if ((r = dalloc(s, &s->vc_wd, s->vc_w.size()))) return r;
+  if ((r = dalloc(s, &s->vc_detj, dj.size()))) return r;
+  FR_CUDA(cudaMemcpy(s->vc_opp, opp.data(), opp.size() * 8, cudaMemcpyHostToDevice));
+  FR_CUDA(cudaMemcpy(s->vc_wd, s->vc_w.data(), s->vc_w.size() * 8, cudaMemcpyHostToDevice));
+  FR_CUDA(cudaMemcpy(s->vc_detj, dj.data(), dj.size() * 8, cudaMemcpyHostToDevice));
+  s->vc_dirty = false;
+  return FR_OK;
+}
+
 fr_status fr_solver_kinetic_energy(fr_solver* s, double* out, void* stream)
 {
   if (!s || !out) return fail(FR_ERR_ARG, "null argument");
   FR_CUDA(cudaSetDevice(s->device));
   cudaStream_t st = STRM(s, stream);
-  s->run->ke(s->b, s->ke_partial, s->nblk_ke, st);
-  fr_norm_finalize<<<1, 256, 0, st>>>(s->ke_partial, s->nblk_ke, 1, 1.0, s->ke_out);
+  fr_status r = volume_cubature_ready(s);
+  if (r) return r;
+  const Mesh& m = s->mesh;
+  FR_CUDA(launch_diagnostics(m.dims, (int)s->tc_size, s->b.U, nullptr, s->vc_opp, s->vc_wd, s->vc_detj, m.ne, m.nu,
+                             s->vc_n, s->sch.gamma, s->diag_partial, kDiagBlocks, s->diag_out, st));
   s->launches += 2;
-  FR_CUDA(cudaGetLastError());
-  FR_CUDA(cudaMemcpyAsync(out, s->ke_out, 8, cudaMemcpyDeviceToHost, st));
+  FR_CUDA(cudaMemcpyAsync(out, s->diag_out, 8, cudaMemcpyDeviceToHost, st));
   FR_CUDA(cudaStreamSynchronize(st));
   return FR_OK;
+}
+
+fr_status fr_solver_set_volume_cubature(fr_solver* s, int n_cub, const double* loc, const double* weights)
+{
+  if (!s || n_cub <= 0 || !loc || !weights) return fail(FR_ERR_ARG, "bad argument");
+  const int D = s->mesh.dims;
+  for (int i = 0; i < n_cub * D; i++)
+    if (!(loc[i] >= -1.0 && loc[i] <= 1.0)) return fail(FR_ERR_ARG, "cubature points must lie in [-1, 1]");
+  s->vc_n = n_cub;
+  s->vc_loc.assign(loc, loc + (size_t)n_cub * D);
+  s->vc_w.assign(weights, weights + n_cub);
+  s->vc_dirty = true;
+  return FR_OK;
+}
+
+int fr_volume_cubature(int dims, int rule, double* loc, double* weights)
+{
+  std::vector<double> l, w;
+  const int n = volume_cubature(dims, rule, l, w);
+  if (n > 0) {
+    if (loc) memcpy(loc, l.data(), l.size() * 8);
+    if (weights) memcpy(weights, w.data(), w.size() * 8);
+  }
+  return n;
 }
 
 long long fr_solver_launch_count(const fr_solver* s) { return s ? s->launches : 0; }
@@ -805,19 +865,8 @@ fr_status fr_solver_integral_quantities(fr_solver* s, double out5[5], void* stre
   FR_CUDA(cudaSetDevice(s->device));
   cudaStream_t st = STRM(s, stream);
   const Mesh& m = s->mesh;
-  const int nblk = 296;
-  fr_status r;
-  if (!s->diag_w) {
-    std::vector<double> w((size_t)m.nu);
-    for (int u = 0; u < m.nu; u++) {
-      int a = u % m.n1, b = (u / m.n1) % m.n1, c = m.dims == 3 ? u / (m.n1 * m.n1) : 0;
-      w[u] = s->line.w[a] * s->line.w[b] * (m.dims == 3 ? s->line.w[c] : 1.0);
-    }
-    if ((r = dalloc(s, &s->diag_w, (size_t)m.nu))) return r;
-    if ((r = dalloc(s, &s->diag_partial, (size_t)nblk * 5))) return r;
-    if ((r = dalloc(s, &s->diag_out, 5))) return r;
-    FR_CUDA(cudaMemcpy(s->diag_w, w.data(), w.size() * 8, cudaMemcpyHostToDevice));
-  }
+  fr_status r = volume_cubature_ready(s);
+  if (r) return r;
   const size_t n = (size_t)m.nu * m.ne * m.nfields * m.dims;
   if (!s->grad_buf) {
     char* p;
@@ -827,8 +876,8 @@ fr_status fr_solver_integral_quantities(fr_solver* s, double out5[5], void* stre
   Bufs b = s->b;
   b.GRAD = s->grad_buf;
   s->run->grad(b, s->cur, st);
-  FR_CUDA(launch_diagnostics(m.dims, (int)s->tc_size, s->b.U, s->grad_buf, s->b.detj64, s->diag_w,
-                             (long long)m.nu * m.ne, m.nu, s->sch.gamma, s->diag_partial, nblk, s->diag_out, st));
+  FR_CUDA(launch_diagnostics(m.dims, (int)s->tc_size, s->b.U, s->grad_buf, s->vc_opp, s->vc_wd, s->vc_detj, m.ne,
+                             m.nu, s->vc_n, s->sch.gamma, s->diag_partial, kDiagBlocks, s->diag_out, st));
   s->launches += 3;
   FR_CUDA(cudaMemcpyAsync(out5, s->diag_out, 5 * 8, cudaMemcpyDeviceToHost, st));
   FR_CUDA(cudaStreamSynchronize(st));

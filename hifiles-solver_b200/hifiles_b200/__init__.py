@@ -96,6 +96,8 @@ def lib():
         "fr_solver_advance": (C.c_int, [vp, C.c_int, C.c_double, dp, vp]),
         "fr_solver_advance_async": (C.c_int, [vp, C.c_int, C.c_double, dp, vp]),
         "fr_solver_kinetic_energy": (C.c_int, [vp, dp, vp]),
+        "fr_solver_set_volume_cubature": (C.c_int, [vp, C.c_int, dp, dp]),
+        "fr_volume_cubature": (C.c_int, [C.c_int, C.c_int, dp, dp]),
         "fr_solver_launch_count": (C.c_longlong, [vp]),
         "fr_solver_stream": (vp, [vp]),
         "fr_solver_sync": (C.c_int, [vp]),
@@ -238,6 +240,35 @@ def line_operators(order, upts_type=0, vcjh_scheme=1, eta=0.0):
     return dict(loc=loc, Lm=Lm, Lp=Lp, D=D.reshape(n, n), gL=gL, gR=gR, w=w, eta=float(eta[0]))
 
 
+def volume_cubature(dims, rule):
+    """The tensor Gauss-Legendre volume cubature of `rule` points per direction
+    in the reference's point order, full double precision: (loc (dims, n),
+    weights (n))."""
+    n = lib().fr_volume_cubature(int(dims), int(rule), None, None)
+    if n <= 0:
+        raise ValueError("cubature rule must be 1..12")
+    loc = np.zeros((dims, n), order="F")
+    w = np.zeros(n)
+    lib().fr_volume_cubature(int(dims), int(rule), _dp(loc), _dp(w))
+    return loc, w
+
+
+def read_reference_cubature(path, dims, rule):
+    """A rule of the reference's cubature tables (data/cubature_quad.dat or
+    data/cubature_hexa.dat: a line "rule=N", then "locs(x)", "locs(y)"
+    [, "locs(z)"] and "weights", each followed by one value per line), for a
+    caller that has the reference's data directory: (loc (dims, n), weights)."""
+    n = rule ** dims
+    lines = [ln.strip() for ln in open(path)]
+    i = lines.index("rule=%d" % rule)
+    cols = []
+    for _ in range(dims + 1):
+        i += 1                          # the section title
+        cols.append([float(lines[i + 1 + q].split()[0]) for q in range(n)])
+        i += n
+    return np.asfortranarray(np.array(cols[:dims])), np.array(cols[dims])
+
+
 class Solver:
     """One element type (quads or hexes) on a periodic conforming mesh, resident on one GPU."""
 
@@ -264,6 +295,7 @@ class Solver:
         _check(L.fr_solver_sizes(self.h, sz))
         self.n_eles, self.n_upts, self.n_fpts, self.n_fields, self.dims, self.n_int = list(sz)
         self.viscous = bool(viscous)
+        self.order = int(order)
         self.precision = precision
         self.device = int(device)
 
@@ -406,6 +438,16 @@ class Solver:
         if w.size != mlp_n_params():
             raise ValueError("expected %d parameters" % mlp_n_params())
         _check(lib().fr_solver_set_sgs_mlp(self.h, w.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def set_volume_cubature(self, loc, weights):
+        """Volume cubature of the integral diagnostics: loc (dims, n) points in
+        [-1, 1]^dims, weights (n) -- e.g. a rule of the reference's own
+        data/cubature_*.dat tables (read_reference_cubature)."""
+        loc = np.asfortranarray(loc, dtype=np.float64)
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        if loc.shape != (self.dims, w.size):
+            raise ValueError("loc must be (dims, n) with n = len(weights)")
+        _check(lib().fr_solver_set_volume_cubature(self.h, int(w.size), _dp(loc), _dp(w)))
 
     def kinetic_energy(self, stream=None):
         v = C.c_double()

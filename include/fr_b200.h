@@ -155,8 +155,25 @@ fr_status fr_solver_advance(fr_solver* s, int n_steps, double dt, double* norms_
  * the stream is synchronised (fr_solver_sync). */
 fr_status fr_solver_advance_async(fr_solver* s, int n_steps, double dt, double* norms_host, void* stream);
 
-/* Volume integral of 0.5 rho |v|^2 (solution-point Gauss quadrature), FP64. */
+/* Volume integral of 0.5 rho |v|^2 on the solver's volume cubature (the
+ * "kineticenergy" integral quantity of eles::CalcIntegralQuantities,
+ * src/eles.cpp:6503-6641), FP64. */
 fr_status fr_solver_kinetic_energy(fr_solver* s, double* out_host, void* stream);
+
+/* The volume cubature of the integral diagnostics.  By default it is the
+ * reference's default rule (volume_cub_order 3: the tensor Gauss-Legendre rule
+ * of 3 points per direction) in full double precision; the reference's
+ * data/cubature_{quad,hexa}.dat print these rules to 12-15 significant
+ * digits.  fr_solver_set_volume_cubature takes any rule instead, e.g. the
+ * reference's own table (bit for bit) or another volume_cub_order
+ * (eles_quads / eles_hexas::set_volume_cubpts, src/eles_hexas.cpp:418-440):
+ * loc (dims, n_cub) with the point index slowest, points in [-1, 1]^dims.
+ * fr_volume_cubature writes the tensor Gauss-Legendre rule of `rule` points per
+ * direction in the reference's point order (quads: first coordinate fastest;
+ * hexes: first coordinate slowest), full double precision, and returns its point count (0: rule
+ * outside 1..12); loc or weights may be null to query the count. */
+fr_status fr_solver_set_volume_cubature(fr_solver* s, int n_cub, const double* loc, const double* weights);
+int fr_volume_cubature(int dims, int rule, double* loc, double* weights);
 
 /* Kernel launches issued by the solver since creation (for launch accounting). */
 long long fr_solver_launch_count(const fr_solver* s);
@@ -200,8 +217,9 @@ fr_status fr_solver_gradient(fr_solver* s, double* host_grad, void* stream);
  * eles::CalcIntegralQuantities (src/eles.cpp:6503-6641): out5 = kinetic
  * energy, enstrophy (rho |curl u|^2 / 2, the reference's "vorticity"),
  * pressure dilatation, strain colon product, deviatoric strain colon
- * product, each integrated with the tensor Gauss rule of the solution points
- * (the reference interpolates to a separate volume cubature rule).  Viscous
+ * product.  As in the reference, the state and its corrected gradient are
+ * interpolated to the volume cubature points (opp_volume_cubpts) and
+ * integrated with the rule's weights times the Jacobian there.  Viscous
  * solvers only (the corrected gradient comes from the gradient kernel). */
 fr_status fr_solver_integral_quantities(fr_solver* s, double out5[5], void* stream);
 

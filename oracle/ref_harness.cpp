@@ -11,7 +11,9 @@
 //   * with --stages, runs stage 0 of CalcResidual (src/solver.cpp:65-225) one
 //     operator at a time and dumps every intermediate array;
 //   * runs --steps RK45 steps exactly as main() does (src/HiFiLES.cpp:154-183)
-//     and records the residual norms of CalcNormResidual (src/output.cpp:1452).
+//     and records the residual norms of CalcNormResidual (src/output.cpp:1452);
+//   * with --integrals, evaluates the integral quantities of the initial state
+//     on the reference's volume cubature and dumps them with that cubature.
 // Output: one .npy per array (Fortran order = the reference's array<T> layout,
 // first index fastest) plus params.txt with the non-dimensional constants.
 //
@@ -312,23 +314,56 @@ static void staged_residual(solution& S)
   dump_stage(S, "s11", "div_tconf_upts");
 }
 
+// The reference's integral quantities of the current state
+// (output.cpp CalcIntegralQuantities -> eles::CalcIntegralQuantities,
+// src/eles.cpp:6503-6641) after one residual evaluation (stage 0 of
+// CalcResidual fills grad_disu_upts), and the volume cubature the reference
+// integrates on: loc/weight_volume_cubpts, opp_volume_cubpts and
+// vol_detjac_vol_cubpts (src/eles.cpp:4111-4130, 5320-5352).
+static void dump_integrals(solution& S)
+{
+  CalcResidual(0, 0, &S);
+  CalcIntegralQuantities(0, &S);
+  vector<double> iq;
+  for (int m = 0; m < run_input.n_integral_quantities; m++) iq.push_back(S.integral_quantities(m));
+  vector<int> shape(1, (int)iq.size());
+  write_npy("integral_quantities", iq.data(), "<f8", 8, shape);
+  for (int t = 0; t < S.n_ele_types; t++) {
+    eles* e = S.mesh_eles(t);
+    if (e->n_eles == 0) continue;
+    char pre[16]; snprintf(pre, sizeof pre, "t%d_", e->ele_type);
+    string P(pre);
+    dump(P + "loc_volume_cubpts", e->loc_volume_cubpts, 2);
+    dump(P + "weight_volume_cubpts", e->weight_volume_cubpts, 1);
+    dump(P + "opp_volume_cubpts", e->opp_volume_cubpts, 2);
+    vector<double> dj;
+    for (int i = 0; i < e->n_eles; i++)
+      for (int j = 0; j < e->n_cubpts_per_ele; j++) dj.push_back(e->vol_detjac_vol_cubpts(j)(i));
+    vector<int> sh; sh.push_back(e->n_cubpts_per_ele); sh.push_back(e->n_eles);
+    write_npy(P + "vol_detjac_vol_cubpts", dj.data(), "<f8", 8, sh);
+    dump(P + "grad_disu_upts_iq", e->grad_disu_upts, 4);
+    dump(P + "disu_upts_iq", e->disu_upts(0), 3);
+  }
+}
+
 int main(int argc, char** argv)
 {
   if (argc < 3) {
-    fprintf(stderr, "usage: ref_harness <input_file> <out_dir> [--ic NAME] [--steps N] [--stages] [--no-dump]"
+    fprintf(stderr, "usage: ref_harness <input_file> <out_dir> [--ic NAME] [--steps N] [--stages] [--no-dump] [--integrals]"
                     " [--write-restart N]\n");
     return 2;
   }
   g_out = argv[2];
   string ic;
   int steps = 0;
-  bool stages = false, nodump = false;
+  bool stages = false, nodump = false, integrals = false;
   int restart_out = -1;
   for (int a = 3; a < argc; a++) {
     if (!strcmp(argv[a], "--ic") && a + 1 < argc) ic = argv[++a];
     else if (!strcmp(argv[a], "--steps") && a + 1 < argc) steps = atoi(argv[++a]);
     else if (!strcmp(argv[a], "--stages")) stages = true;
     else if (!strcmp(argv[a], "--no-dump")) nodump = true;
+    else if (!strcmp(argv[a], "--integrals")) integrals = true;
     else if (!strcmp(argv[a], "--write-restart") && a + 1 < argc) restart_out = atoi(argv[++a]);
     else { fprintf(stderr, "bad argument %s\n", argv[a]); return 2; }
   }
@@ -348,6 +383,11 @@ int main(int argc, char** argv)
   for (int i = 0; i < 5; i++) S.norm_residual(i) = 0.0;
 
   if (!nodump) dump_setup(S);
+  if (integrals) {
+    dump_integrals(S);
+    printf("ref_harness done\n");
+    return 0;
+  }
 
   int first_stage = 0;
   if (stages) {

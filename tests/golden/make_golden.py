@@ -322,15 +322,73 @@ def restart_read_fixture(ref, work):
     print("restart read fixture: reference P3 state from our P2 file, shape", arr["t4_disu_upts_init"].shape)
 
 
+# integral quantities on the reference's volume cubature (volume_cub_order)
+IQ_CASES = [
+    dict(name="iq_hex_tgv_p3_n3_jit", dims=3, order=3, n=(3, 3, 3), lo=(0, 0, 0), hi=(2 * np.pi,) * 3, viscous=1,
+         ic="tgv_mach01", vcjh=1, jitter=0.1, cub=3),
+    dict(name="iq_hex_tgv_p2_n3_jit_cub5", dims=3, order=2, n=(3, 2, 3), lo=(0, 0, 0), hi=(2 * np.pi,) * 3,
+         viscous=1, ic="tgv_mach01", vcjh=2, jitter=0.1, cub=5),
+    dict(name="iq_quad_vortex_p3_n6_jit_cub4", dims=2, order=3, n=(6, 5), lo=(-5, -5), hi=(5, 5), viscous=1,
+         ic="vortex_u1v0", vcjh=1, jitter=0.15, cub=4),
+]
+IQ_NAMES = "5 kineticenergy vorticity pressuredilatation straincolonproduct devstraincolonproduct"
+
+
+def integral_fixtures(ref, work):
+    """The reference's own integral quantities (eles::CalcIntegralQuantities on
+    its volume cubature) of a state after one residual evaluation, with the
+    cubature points, weights, interpolation operator and Jacobians it used."""
+    env = dict(os.environ, HIFILES_HOME=os.path.join(REPO, "oracle", "_ref"))
+    for c in IQ_CASES:
+        d = os.path.join(work, c["name"])
+        os.makedirs(d, exist_ok=True)
+        xv, c2v = box_vertices(c["dims"], c["n"], c["lo"], c["hi"], c["jitter"], seed=12345)
+        write_gambit(os.path.join(d, "mesh.neu"), c["dims"], xv, c2v, c["n"])
+        L = [c["hi"][i] - c["lo"][i] for i in range(c["dims"])]
+        vals = {"equation": 0, "viscous": c["viscous"], "ic_form": 7 if c["ic"].startswith("tgv") else 1,
+                "order": c["order"], "dt_type": 0, "dt": 1e-3, "n_steps": 1, "adv_type": 3, "tau": 1.0,
+                "pen_fact": 0.5, "mesh_file": "mesh.neu", "dx_cyclic": "%.17g" % L[0], "dy_cyclic": "%.17g" % L[1],
+                "dz_cyclic": "%.17g" % (L[2] if c["dims"] == 3 else 0.0), "monitor_res_freq": 100000,
+                "plot_freq": 100000, "restart_dump_freq": 100000, "upts_type_quad": 0,
+                "vcjh_scheme_quad": c["vcjh"], "upts_type_hexa": 0, "vcjh_scheme_hexa": c["vcjh"], "prandtl": 0.71,
+                "Mach_free_stream": 0.1, "Re_free_stream": 1600.0, "gamma": 1.4, "fix_vis": 1, "res_norm_type": 1,
+                "volume_cub_order": c["cub"], "integral_quantities": IQ_NAMES}
+        write_input(os.path.join(d, "input"), os.path.join(ref, TGV_INPUT), vals)
+        out = os.path.join(d, "out")
+        os.makedirs(out, exist_ok=True)
+        r = subprocess.run([HARNESS, "input", out, "--ic", c["ic"], "--integrals"], cwd=d, env=env,
+                           capture_output=True, text=True)
+        if r.returncode != 0:
+            print(r.stdout[-2000:], r.stderr[-2000:])
+            raise RuntimeError("harness failed for " + c["name"])
+        arr, par = load_npy_dir(out)
+        T = "t%d_" % (1 if c["dims"] == 2 else 4)
+        meta = {k: (list(v) if isinstance(v, tuple) else v) for k, v in c.items()}
+        meta["physics"] = {k: par[k] for k in ("gamma", "prandtl", "mu_inf", "rt_inf", "c_sth", "fix_vis", "tau",
+                                                 "pen_fact")}
+        meta["quantities"] = IQ_NAMES.split()[1:]
+        meta["seed"] = 12345
+        fx = dict(u0=arr[T + "disu_upts_iq"], grad=arr[T + "grad_disu_upts_iq"], iq=arr["integral_quantities"],
+                  loc=arr[T + "loc_volume_cubpts"], weight=arr[T + "weight_volume_cubpts"],
+                  opp=arr[T + "opp_volume_cubpts"], detjac=arr[T + "vol_detjac_vol_cubpts"])
+        np.savez_compressed(os.path.join(HERE, c["name"] + ".npz"), meta=json.dumps(meta),
+                            **{k: np.asfortranarray(v) for k, v in fx.items()})
+        print(c["name"], "integral quantities", arr["integral_quantities"])
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=os.environ.get("HIFILES_REF"), required="HIFILES_REF" not in os.environ,
                     help="the reference checkout (or set HIFILES_REF)")
     ap.add_argument("--work", default=None)
+    ap.add_argument("--integrals", action="store_true", help="only the integral-quantity fixtures (iq_*.npz)")
     a = ap.parse_args()
     if not os.path.exists(HARNESS):
         subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "REF=" + a.ref, "ref"], check=True)
     work = a.work or tempfile.mkdtemp(prefix="fr_golden_")
+    if a.integrals:
+        integral_fixtures(a.ref, work)
+        return
     summary = {}
     for c in CASES:
         arr, par = run_case(a.ref, c, work)

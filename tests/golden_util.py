@@ -29,3 +29,38 @@ def rel(a, b):
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
     return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+
+
+# integral quantities on the reference's volume cubature (iq_*.npz from make_golden.py --integrals)
+IQ_CASES = ["iq_hex_tgv_p3_n3_jit", "iq_hex_tgv_p2_n3_jit_cub5", "iq_quad_vortex_p3_n6_jit_cub4"]
+
+
+def integral_quantities_numpy(u, grad, opp, weight, detjac, dims, gamma):
+    """numpy restatement of eles::CalcIntegralQuantities (src/eles.cpp:6503-6641):
+    state and gradient interpolated to the cubature points with opp (nc, nu),
+    the five quantities, weights x detJ at the cubature points.  Returns the
+    five integrals and the integrals of their absolute values (the scale
+    against which a cancelling sum such as the pressure dilatation is compared)."""
+    F = dims + 2
+    uc = np.einsum("jk,kem->jem", opp, u)                     # (nc, E, F)
+    gc = np.einsum("jk,kemn->jemn", opp, grad)                # (nc, E, F, D)
+    irho = 1.0 / uc[..., 0]
+    A = irho[..., None, None] * (gc[..., 1:1 + dims, :] - uc[..., 1:1 + dims, None] * irho[..., None, None] *
+                                 gc[..., 0:1, :])          # A[a][b] = d u_a / d x_b
+    tke = (0.5 * uc[..., 1:F - 1] * uc[..., 1:F - 1]).sum(axis=-1)
+    ke = irho * tke
+    wz = A[..., 1, 0] - A[..., 0, 1]
+    vort = wz * wz
+    if dims == 3:
+        vort = vort + (A[..., 2, 1] - A[..., 1, 2]) ** 2 + (A[..., 0, 2] - A[..., 2, 0]) ** 2
+    vort = vort * 0.5 / irho
+    p = (gamma - 1.0) * (uc[..., F - 1] - irho * tke)
+    pd = p * np.trace(A, axis1=-2, axis2=-1)
+    S = 0.5 * (A + np.swapaxes(A, -1, -2))
+    sc = (S * S).sum(axis=(-2, -1))
+    Sd = S - np.eye(dims) * (np.trace(S, axis1=-2, axis2=-1) / 3.0)[..., None, None]
+    dsc = (Sd * Sd).sum(axis=(-2, -1))
+    wj = weight[:, None] * detjac                             # (nc, E)
+    vals = [float((x * wj).sum()) for x in (ke, vort, pd, sc, dsc)]
+    mags = [float((np.abs(x) * wj).sum()) for x in (ke, vort, pd, sc, dsc)]
+    return vals, mags

@@ -1,58 +1,103 @@
-"""Integral diagnostics on the device (fr_solver_integral_quantities): the
-quantities of eles::CalcIntegralQuantities (src/eles.cpp:6503-6641) from the
-state and its corrected gradient, against the same formulas evaluated in
-numpy on the solver's own gradient, at 1e-12 relative."""
+"""Integral diagnostics on the device (fr_solver_integral_quantities,
+fr_solver_kinetic_energy): the quantities of eles::CalcIntegralQuantities
+(src/eles.cpp:6503-6641) on the reference's volume cubature, against the
+values the reference itself computed on the same mesh and state
+(tests/golden/iq_*.npz), and against the numpy restatement on the solver's
+own gradient.  Tolerance 1e-12 relative to the integral of each quantity's
+absolute value (the pressure dilatation is a cancelling sum)."""
 import numpy as np
 import pytest
 
 import hifiles_b200 as H
 import oracle as O
+from golden_util import IQ_CASES, integral_quantities_numpy, load
 
 pytestmark = pytest.mark.gpu
 
-
-def _numpy_quantities(u, g, detj, w1, dims, gamma):
-    F = dims + 2
-    q = u.reshape(-1, F, order="F")
-    gg = g.reshape(-1, F, dims, order="F")
-    nu = len(w1) ** dims
-    W = np.ones(nu)
-    for d in range(dims):
-        W = W * np.asarray(w1)[(np.arange(nu) // len(w1) ** d) % len(w1)]
-    wj = np.tile(W, q.shape[0] // nu) * detj.reshape(-1, order="F")
-    irho = 1.0 / q[:, 0]
-    A = irho[:, None, None] * (gg[:, 1:1 + dims, :] - q[:, 1:1 + dims, None] * irho[:, None, None] * gg[:, 0:1, :])
-    tke = 0.5 * (q[:, 1:1 + dims] ** 2).sum(axis=1)
-    ke = irho * tke
-    wz = A[:, 1, 0] - A[:, 0, 1]
-    en = wz * wz
-    if dims == 3:
-        en = en + (A[:, 2, 1] - A[:, 1, 2]) ** 2 + (A[:, 0, 2] - A[:, 2, 0]) ** 2
-    en = en * 0.5 / irho
-    p = (gamma - 1.0) * (q[:, -1] - irho * tke)
-    pd = p * np.trace(A, axis1=1, axis2=2)
-    S = 0.5 * (A + A.transpose(0, 2, 1))
-    sc = (S * S).sum(axis=(1, 2))
-    Sd = S - np.eye(dims)[None] * (np.trace(S, axis1=1, axis2=2) / 3.0)[:, None, None]
-    dsc = (Sd * Sd).sum(axis=(1, 2))
-    return [float((x * wj).sum()) for x in (ke, en, pd, sc, dsc)]
+NAMES = ("kineticenergy", "vorticity", "pressuredilatation", "straincolonproduct", "devstraincolonproduct")
 
 
-@pytest.mark.parametrize("dims,P,n,jit", [(3, 3, (4, 3, 3), 0.1), (3, 2, (3, 3, 3), 0.0), (2, 4, (4, 5), 0.1)])
-def test_integral_quantities_match_numpy(dims, P, n, jit):
+def _solver(meta):
+    ph = meta["physics"]
+    return H.Solver.box(meta["dims"], meta["order"], meta["n"], meta["lo"], meta["hi"], jitter=meta["jitter"],
+                        seed=meta["seed"], viscous=True, vcjh_scheme=meta["vcjh"], **ph)
+
+
+@pytest.mark.parametrize("case", IQ_CASES)
+def test_integral_quantities_match_reference(case):
+    meta, a = load(case)
+    s = _solver(meta)
+    s.set_volume_cubature(a["loc"], a["weight"])
+    s.set_state(a["u0"])
+    iq = s.integral_quantities()
+    _, mags = integral_quantities_numpy(a["u0"], a["grad"], a["opp"], a["weight"], a["detjac"], meta["dims"],
+                                        meta["physics"]["gamma"])
+    for k, want, m in zip(NAMES, a["iq"], mags):
+        assert abs(iq[k] - want) <= 1e-12 * m, (k, iq[k], want)
+    assert abs(s.kinetic_energy() - a["iq"][0]) <= 1e-12 * abs(a["iq"][0])
+
+
+@pytest.mark.parametrize("dims,P,n,jit,rule", [(3, 3, (4, 3, 3), 0.1, 3), (3, 2, (3, 3, 3), 0.0, 4),
+                                               (2, 4, (4, 5), 0.1, 6)])
+def test_integral_quantities_match_numpy(dims, P, n, jit, rule):
     lo, hi = [0.0] * dims, [2 * np.pi] * dims
     s = H.Solver.box(dims, P, n, lo, hi, jitter=jit, seed=3, viscous=True, gamma=1.4, prandtl=0.71,
                      mu_inf=1e-3, tau=1.0, pen_fact=0.5)
-    g = s.geometry()
-    pos = g["pos_upts"]
+    pos = s.geometry()["pos_upts"]
     u = O.ic_tgv(pos) if dims == 3 else O.ic_vortex(pos * (10 / (2 * np.pi)) - 5)
     u = np.asfortranarray(u + 0.02 * np.random.default_rng(2).standard_normal(u.shape) * (np.arange(u.shape[2]) > 0))
     s.set_state(u)
+    loc, w = H.volume_cubature(dims, rule)
+    if rule != 3:
+        s.set_volume_cubature(loc, w)
     iq = s.integral_quantities()
-    want = _numpy_quantities(u, s.gradient(), g["detjac_upts"], np.polynomial.legendre.leggauss(P + 1)[1], dims, 1.4)
-    for (k, v), w in zip(iq.items(), want):
-        assert abs(v - w) <= 1e-12 * max(abs(w), 1e-30) + 1e-14, (k, v, w)
+    # the interpolation rows and Jacobians at the cubature points, restated
+    x1 = H.line_operators(P)["loc"]
+    nl = len(x1)
+
+    def lag(x, m):
+        return np.prod([(x - x1[i]) / (x1[m] - x1[i]) for i in range(nl) if i != m], axis=0)
+    nu = nl ** dims
+    opp = np.ones((w.size, nu))
+    for k in range(nu):
+        for d in range(dims):
+            opp[:, k] *= lag(loc[d], (k // nl ** d) % nl)
+    vals, mags = integral_quantities_numpy(u, s.gradient(), opp, w, _detj_cub(s, loc), dims, 1.4)
+    for k, v, m in zip(NAMES, vals, mags):
+        assert abs(iq[k] - v) <= 1e-12 * m, (k, iq[k], v)
     assert abs(iq["kineticenergy"] - s.kinetic_energy()) <= 1e-13 * abs(iq["kineticenergy"])
+
+
+def _detj_cub(s, loc):
+    """Jacobian determinant of each element's bi/tri-linear map at the cubature points."""
+    D = s.dims
+    g = s.geometry()
+    # corner positions from the solution-point positions: the map is (bi/tri)linear,
+    # so fit it exactly from the element's points
+    pos = g["pos_upts"]                                   # (nu, E, D)
+    x1 = H.line_operators(s.order)["loc"]
+    nl = len(x1)
+    nu = nl ** D
+    R = np.array([[x1[(k // nl ** d) % nl] for d in range(D)] for k in range(nu)])
+    cols = [np.ones(nu)] + [R[:, d] for d in range(D)]
+    if D == 2:
+        cols += [R[:, 0] * R[:, 1]]
+    else:
+        cols += [R[:, 0] * R[:, 1], R[:, 0] * R[:, 2], R[:, 1] * R[:, 2], R[:, 0] * R[:, 1] * R[:, 2]]
+    M = np.stack(cols, axis=1)
+    coef = np.linalg.lstsq(M, pos.reshape(nu, -1), rcond=None)[0].reshape(M.shape[1], pos.shape[1], D)
+    out = np.zeros((loc.shape[1], pos.shape[1]))
+    for j in range(loc.shape[1]):
+        r = loc[:, j]
+        if D == 2:
+            dM = np.array([[0, 1, 0, r[1]], [0, 0, 1, r[0]]])
+        else:
+            dM = np.array([[0, 1, 0, 0, r[1], r[2], 0, r[1] * r[2]],
+                           [0, 0, 1, 0, r[0], 0, r[2], r[0] * r[2]],
+                           [0, 0, 0, 1, 0, r[0], r[1], r[0] * r[1]]])
+        J = np.einsum("ck,kei->eic", dM, coef)            # J[e, i, c] = d x_i / d r_c
+        out[j] = np.linalg.det(J)
+    return out
 
 
 def test_integral_quantities_need_the_viscous_path():

@@ -122,3 +122,31 @@ def test_mesh_errors_are_reported_not_fatal():
     flipped = c2v[:, [1, 0, 3, 2, 5, 4, 7, 6]]        # mirrored elements: negative Jacobian
     with pytest.raises(H.FrError):
         H.mesh_geometry(3, xv, flipped, [1, 1, 1], 2)
+
+
+@pytest.mark.parametrize("case", ["iq_hex_tgv_p3_n3_jit", "iq_hex_tgv_p2_n3_jit_cub5", "iq_quad_vortex_p3_n6_jit_cub4"])
+def test_default_volume_cubature_is_the_reference_rule(case):
+    """The default rule (tensor Gauss-Legendre, full precision) is the rule the
+    reference's cubature tables print to 12-15 digits, in its point order."""
+    import json
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", case + ".npz"))
+    meta = json.loads(str(z["meta"]))
+    loc, w = H.volume_cubature(meta["dims"], meta["cub"])
+    assert loc.shape == z["loc"].shape and w.shape == z["weight"].shape
+    assert np.abs(loc - z["loc"]).max() <= 1e-12
+    assert np.abs(w - z["weight"]).max() <= 1e-12
+    assert abs(w.sum() - 2.0 ** meta["dims"]) <= 1e-13
+
+
+def test_reference_cubature_table_reader(tmp_path):
+    """read_reference_cubature parses the reference's data/cubature_*.dat layout."""
+    loc, w = H.volume_cubature(2, 3)
+    lines = ["rule=2", "locs(x)"] + ["0.1"] * 4 + ["locs(y)"] + ["0.2"] * 4 + ["weights"] + ["1.0"] * 4
+    lines += ["rule=3", "locs(x)"] + ["%.15g" % x for x in loc[0]] + ["locs(y)"] + ["%.15g" % x for x in loc[1]]
+    lines += ["weights"] + ["%.12g" % x for x in w]
+    p = tmp_path / "cubature_quad.dat"
+    p.write_text("\n".join(lines) + "\n")
+    rl, rw = H.read_reference_cubature(str(p), 2, 3)
+    assert np.abs(rl - loc).max() < 1e-14 and np.abs(rw - w).max() < 1e-11
+    with pytest.raises(ValueError):
+        H.volume_cubature(3, 13)

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from golden_util import BC_CASES, CASES, GOLDEN, LES_CASES, ROE_CASES, load, rel
+from golden_util import BC_CASES, CASES, GOLDEN, IQ_CASES, LES_CASES, ROE_CASES, integral_quantities_numpy, load, rel
 
 
 def _mesh(meta):
@@ -81,3 +81,14 @@ def test_oracle_reproduces_reference_regression_kat():
     u0 = O.ic_tgv(m.geometry()["pos_upts"], p0=100.0)
     _, _, nrm = m.rk45(O.tgv_kat_physics(), u0, 1e-3, kat["test_iter"])
     assert np.all(np.abs(nrm[:, -1] - np.array(kat["test_vals"])) < kat["tol"])
+
+
+@pytest.mark.parametrize("case", IQ_CASES)
+def test_integral_quantity_restatement_matches_reference(case):
+    """The numpy restatement of eles::CalcIntegralQuantities (golden_util) on the
+    reference's own state, gradient and cubature gives the reference's values."""
+    meta, a = load(case)
+    vals, mags = integral_quantities_numpy(a["u0"], a["grad"], a["opp"], a["weight"], a["detjac"], meta["dims"],
+                                           meta["physics"]["gamma"])
+    for v, w, m in zip(vals, a["iq"], mags):
+        assert abs(v - w) <= 1e-13 * m
