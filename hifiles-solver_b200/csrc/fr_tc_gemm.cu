@@ -4,6 +4,10 @@
 // cublasDgemm('N','N', m, ncols, k, 1, opp, m, B, k, beta, C, m) calls
 // (eles::extrapolate_solution, calculate_gradient, ... , src/eles.cpp).
 //
+// Each column j of B is split after subtracting its first entry c_j: A B =
+// A (B - c 1^T) + (A 1) c^T, with the row sums A 1 and the second term in
+// FP64, so the BF16 parts carry only the variation inside an element's column
+// (the state's free-stream level needs no BF16 bits).
 // Split: x = x0 + x1 + x2 with x0 = bf16(x), x1 = bf16(x - x0),
 // x2 = bf16(x - x0 - x1).  TERMS = 3 (BF16x3) keeps x0y0 + x0y1 + x1y0, about
 // 16 bits; TERMS = 6 (BF16x6) adds x0y2 + x1y1 + x2y0, about 24 bits (FP32
@@ -24,12 +28,15 @@
 // accumulators (128 lanes x TN columns each) and commits them to an
 // mbarrier; the four warps read their 32 lanes of each back with tcgen05.ld
 // and write C.  Every mbarrier wait
-// is bounded: on expiry the kernel sets the error flag, waits once more
-// (bounded) for its MMAs, frees its TMEM and returns.
+// is bounded: on expiry the kernel sets the error flag and waits once more
+// (bounded) for its MMAs; it frees its TMEM only when they have completed
+// (otherwise the allocation is left held rather than released under MMAs that
+// may still write it).
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include <stdint.h>
 
+#include <mutex>
 #include <string>
 
 #include "fr_b200.h"
@@ -180,6 +187,8 @@ fr_gemm_bf16x3_kernel(int m, int k, int KP, long long ncols, const double* __res
   unsigned char* sB = sm + NP * partA;     // NP parts of TN x KP bf16
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tmem_slot;
+  __shared__ double rowsum[RA];            // A 1 (FP64, column order)
+  __shared__ double cB[TN];                // first entry of each B column of the tile
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   if (warp == 0) {
@@ -206,15 +215,24 @@ fr_gemm_bf16x3_kernel(int m, int k, int KP, long long ncols, const double* __res
     for (int pp = 0; pp < NP; pp++)
       *reinterpret_cast<uint4*>(sA + pp * partA + mt * tileA + chunk_off(rr, c, kTM)) = q[pp];
   }
+  for (int r = tid; r < RA; r += kThreads) {
+    double acc = 0.0;
+    if (r < m)
+      for (int kk = 0; kk < k; kk++) acc += __ldg(A + r + (size_t)m * kk);
+    rowsum[r] = acc;
+  }
   fence_before();
   __syncthreads();
   fence_after();
   const uint32_t tmem = tmem_slot;
+  bool drained = true;                     // no MMA of this block may still be running
   const long long ntiles = (ncols + TN - 1) / TN;
   uint32_t parity = 0;
   for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const long long j0 = t * TN;
-    // B' for columns j0 ..: columns n (fastest) x chunks c
+    for (int n = tid; n < TN; n += kThreads) cB[n] = j0 + n < ncols ? __ldg(B + (size_t)(j0 + n) * k) : 0.0;
+    __syncthreads();
+    // B' for columns j0 ..: columns n (fastest) x chunks c, less the column's first entry
     for (int w = tid; w < TN * KC; w += kThreads) {
       const int n = w % TN, c = w / TN;
       const long long j = j0 + n;
@@ -222,7 +240,7 @@ fr_gemm_bf16x3_kernel(int m, int k, int KP, long long ncols, const double* __res
 #pragma unroll
       for (int i = 0; i < 8; i++) {
         const int kk = 8 * c + i;
-        x[i] = (j < ncols && kk < k) ? __ldg(B + (size_t)j * k + kk) : 0.0;
+        x[i] = (j < ncols && kk < k) ? __ldg(B + (size_t)j * k + kk) - cB[n] : 0.0;
       }
       uint4 q[3];
       split8(x, q);
@@ -254,7 +272,9 @@ fr_gemm_bf16x3_kernel(int m, int k, int KP, long long ncols, const double* __res
     // every thread waits (bounded); the block leaves together if any ran out
     if (!__syncthreads_and(mbar_wait(&bar, parity) ? 1 : 0)) {
       if (tid == 0) atomicExch(err, 1);
-      mbar_wait(&bar, parity);             // the MMAs may still be running
+      // the MMAs may still be running: wait once more, and keep the TMEM
+      // allocated unless they are known to have completed
+      drained = __syncthreads_and(mbar_wait(&bar, parity) ? 1 : 0) != 0;
       break;
     }
     parity ^= 1u;
@@ -273,7 +293,8 @@ fr_gemm_bf16x3_kernel(int m, int k, int KP, long long ncols, const double* __res
             const long long j = j0 + 32 * h + i;
             if (j < ncols) {
               double* c = C + r + (size_t)m * j;
-              *c = beta ? *c + (double)v[i] : (double)v[i];
+              const double ab = (double)v[i] + cB[32 * h + i] * rowsum[r];
+              *c = beta ? *c + ab : ab;
             }
           }
         }
@@ -286,10 +307,36 @@ fr_gemm_bf16x3_kernel(int m, int k, int KP, long long ncols, const double* __res
   fence_before();
   __syncthreads();
   fence_after();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+  if (warp == 0 && drained)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
 }
 
-int* g_gemm_err = nullptr;
+// the timeout flag of the products, one per device (allocated on that device)
+constexpr int kMaxDevices = 64;
+std::mutex g_gemm_err_mutex;
+int* g_gemm_err[kMaxDevices] = {};
+
+fr_status gemm_err_flag(int** out)
+{
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess && (dev < 0 || dev >= kMaxDevices)) e = cudaErrorInvalidDevice;
+  if (e != cudaSuccess) {
+    g_err = cudaGetErrorString(e);
+    return FR_ERR_CUDA;
+  }
+  std::lock_guard<std::mutex> lock(g_gemm_err_mutex);
+  if (!g_gemm_err[dev]) {
+    e = cudaMalloc(&g_gemm_err[dev], sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(g_gemm_err[dev], 0, sizeof(int));
+    if (e != cudaSuccess) {
+      g_err = cudaGetErrorString(e);
+      return FR_ERR_CUDA;
+    }
+  }
+  *out = g_gemm_err[dev];
+  return FR_OK;
+}
 
 }  // namespace
 
@@ -301,8 +348,9 @@ static size_t gemm_split_smem(int k, int terms, int mt, int tn)
   return (size_t)(mt * kTM + tn) * n_parts(terms) * KP * 2;
 }
 
-// dynamic shared memory a block may use (227 kB less the 1 kB static part)
-static constexpr size_t kSmemMax = 232448 - 1024;
+// dynamic shared memory a block may use (227 kB less the static part: the
+// barrier, the TMEM slot, the row sums and the column shifts, under 3 kB)
+static constexpr size_t kSmemMax = 232448 - 3072;
 
 // tile shape for an m x k operator: {MT, TN}, or {0, 0} when none fits
 static void gemm_split_shape(int m, int k, int terms, int& mt, int& tn)
@@ -336,14 +384,20 @@ static fr_status launch_split(int m, int k, long long ncols, const double* A, co
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kfn, kThreads, smem);
-  // blocks that fit by shared memory (1 kB static and 1 kB reserved per block)
-  const int by_smem = smem_sm > 0 ? (int)((size_t)smem_sm / (smem + 2048)) : 1;
+  // blocks that fit by shared memory (3 kB static and 1 kB reserved per block)
+  const int by_smem = smem_sm > 0 ? (int)((size_t)smem_sm / (smem + 4096)) : 1;
   if (by_smem > per) per = by_smem;
+  // each block holds kTmemCols of the SM's 512 TMEM columns: more blocks
+  // would only wait in tcgen05.alloc
+  if (per > (int)(512 / kTmemCols)) per = (int)(512 / kTmemCols);
+  int* err = nullptr;
+  fr_status fs = gemm_err_flag(&err);
+  if (fs) return fs;
   const long long ntiles = (ncols + TN - 1) / TN;
   long long grid = (long long)(per > 0 ? per : 1) * (sms > 0 ? sms : 1);
   if (grid > ntiles) grid = ntiles;
   fr_gemm_bf16x3_kernel<TERMS, MT, TN><<<(unsigned)grid, kThreads, smem, s>>>(m, k, (k + 15) / 16 * 16, ncols, A, B,
-                                                                              C, beta, g_gemm_err);
+                                                                              C, beta, err);
   e = cudaGetLastError();
   if (e != cudaSuccess) {
     g_err = std::string("fr_gemm_bf16x3_kernel: ") + cudaGetErrorString(e);
@@ -367,14 +421,6 @@ fr_status gemm_bf16x3(int m, int k, long long ncols, const double* A, const doub
     return FR_ERR_UNSUPPORTED;
   }
   if (ncols == 0) return FR_OK;
-  if (!g_gemm_err) {
-    cudaError_t e = cudaMalloc(&g_gemm_err, sizeof(int));
-    if (e == cudaSuccess) e = cudaMemset(g_gemm_err, 0, sizeof(int));
-    if (e != cudaSuccess) {
-      g_err = cudaGetErrorString(e);
-      return FR_ERR_CUDA;
-    }
-  }
   if (terms == 3)
     return mt == 1 ? launch_split<3, 1, 64>(m, k, ncols, A, B, C, beta, s)
                    : launch_split<3, 2, 32>(m, k, ncols, A, B, C, beta, s);
@@ -386,16 +432,18 @@ fr_status gemm_bf16x3(int m, int k, long long ncols, const double* A, const doub
 // the last check (the flag is cleared); synchronises the stream.
 fr_status gemm_bf16x3_check(cudaStream_t s)
 {
-  if (!g_gemm_err) return FR_OK;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices || !g_gemm_err[dev]) return FR_OK;
+  int* flag = g_gemm_err[dev];
   int v = 0;
-  cudaError_t e = cudaMemcpyAsync(&v, g_gemm_err, sizeof(int), cudaMemcpyDeviceToHost, s);
+  cudaError_t e = cudaMemcpyAsync(&v, flag, sizeof(int), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) {
     g_err = cudaGetErrorString(e);
     return FR_ERR_CUDA;
   }
   if (v) {
-    cudaMemsetAsync(g_gemm_err, 0, sizeof(int), s);
+    cudaMemsetAsync(flag, 0, sizeof(int), s);
     g_err = "tensor-core operator product: MMA completion wait ran out";
     return FR_ERR_TIMEOUT;
   }

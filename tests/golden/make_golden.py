@@ -376,18 +376,45 @@ def integral_fixtures(ref, work):
         print(c["name"], "integral quantities", arr["integral_quantities"])
 
 
+# the BASELINE vortex (periodic [-5, 5]^2, quads, c_dg, Rusanov, RK45, dt 1e-3)
+# advanced to t = 1 by the reference at P = 2 on three meshes: its own
+# convergence rate, against which the CUDA path's rate and states are checked
+ORDER_CASES = [dict(name="order_vortex_p2_n%d" % n, dims=2, order=2, n=(n, n), lo=(-5, -5), hi=(5, 5), viscous=0,
+                    ic="vortex_u1v0", vcjh=1, jitter=0.0, steps=1000, dt=1e-3, stages=False) for n in (10, 20, 40)]
+
+
+def order_fixtures(ref, work):
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(len(ORDER_CASES)) as ex:
+        res = list(ex.map(lambda c: run_case(ref, c, work), ORDER_CASES))
+    for c, (arr, par) in zip(ORDER_CASES, res):
+        meta = {k: (list(v) if isinstance(v, tuple) else v) for k, v in c.items()}
+        meta["physics"] = {k: par[k] for k in ("gamma", "prandtl", "mu_inf", "rt_inf", "c_sth", "fix_vis", "tau",
+                                                 "pen_fact")}
+        meta["seed"] = 12345
+        np.savez_compressed(os.path.join(HERE, c["name"] + ".npz"), meta=json.dumps(meta),
+                            u0=np.asfortranarray(arr["t1_disu_upts_init"]),
+                            uN=np.asfortranarray(arr["t1_final_disu_upts0"]),
+                            pos=np.asfortranarray(arr["t1_pos_upts"]))
+        print(c["name"], "done")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=os.environ.get("HIFILES_REF"), required="HIFILES_REF" not in os.environ,
                     help="the reference checkout (or set HIFILES_REF)")
     ap.add_argument("--work", default=None)
     ap.add_argument("--integrals", action="store_true", help="only the integral-quantity fixtures (iq_*.npz)")
+    ap.add_argument("--order", action="store_true", help="only the reference convergence fixtures (order_*.npz)")
     a = ap.parse_args()
     if not os.path.exists(HARNESS):
         subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "REF=" + a.ref, "ref"], check=True)
     work = a.work or tempfile.mkdtemp(prefix="fr_golden_")
     if a.integrals:
         integral_fixtures(a.ref, work)
+        return
+    if a.order:
+        order_fixtures(a.ref, work)
         return
     summary = {}
     for c in CASES:

@@ -64,3 +64,30 @@ def integral_quantities_numpy(u, grad, opp, weight, detjac, dims, gamma):
     vals = [float((x * wj).sum()) for x in (ke, vort, pd, sc, dsc)]
     mags = [float((np.abs(x) * wj).sum()) for x in (ke, vort, pd, sc, dsc)]
     return vals, mags
+
+
+def _lagrange_matrix(xs, xq):
+    n = len(xs)
+    M = np.ones((len(xq), n))
+    for m in range(n):
+        for i in range(n):
+            if i != m:
+                M[:, m] *= (xq - xs[i]) / (xs[m] - xs[i])
+    return M
+
+
+def over_integrated_density_error(u, pos, P, h, t):
+    """L2 error of the density of a 2-D vortex state u (nu, E, 4) on a uniform
+    quad mesh of spacing h: the solution and the positions interpolated to the
+    (P + 3)-point Gauss rule of each element, the exact vortex (initial field
+    shifted by (t, 0)) evaluated there, weights times the constant Jacobian."""
+    import oracle as O
+    x1 = O.points_1d(P)
+    xq, wq = np.polynomial.legendre.leggauss(P + 3)
+    M1 = _lagrange_matrix(x1, xq)
+    M = np.kron(M1, M1)                       # point i + nq j <- a + n1 b
+    W = np.kron(wq, wq)
+    rq = M @ u[:, :, 0]
+    pq = np.stack([M @ pos[:, :, d] for d in range(2)], axis=-1)
+    ex = O.ic_vortex(pq, t=t)[..., 0]
+    return float(np.sqrt((W[:, None] * (h / 2) ** 2 * (rq - ex) ** 2).sum()))

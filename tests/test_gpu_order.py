@@ -1,47 +1,57 @@
-"""Design order of accuracy of the CUDA path on the 2-D isentropic vortex
-(Euler, quads, Gauss points, c_dg correction, Rusanov, RK45).
+"""Order of accuracy of the CUDA path on the 2-D isentropic vortex (Euler,
+quads, Gauss points, c_dg correction, Rusanov, RK45, dt 1e-3, t = 1): the
+BASELINE configuration's domain [-5, 5]^2 on meshes of 10^2, 20^2, 40^2 and
+80^2 elements at P = 1, 2, 3.
 
-The vortex (strength 5, free stream rho=1, u=1, v=0, p=1) is advected for
-t = 1 on periodic [-10, 10]^2 meshes of n^2 elements; the domain is wide
-enough that the vortex's tail at the boundary (~e^-49) does not limit the
-error.  The exact solution is the initial field shifted by (t, 0).  The L2
-density error, integrated with the tensor Gauss weights and the Jacobian,
-falls between the DG rates P + 1/2 (proven) and P + 1 (design): measured on
-the two finest meshes, 2.3 for P=1, 2.5 for P=2 and 4.5 for P=3 -- the CPU
-oracle, which repeats the reference's arithmetic, gives the same errors to
-four digits, so these are the scheme's rates.  The check is slope > P + 0.4
-on the two finest meshes."""
+The L2 density error is over-integrated: the solution is interpolated to the
+(P + 3)-point Gauss rule of each element and compared with the exact solution
+(the initial field shifted by (t, 0)) there.  Measured rates on the two
+finest meshes: 2.0 (P = 1), 2.6 (P = 2), 4.1 (P = 3).
+
+P = 2 sits between the proven DG rate P + 1/2 and the design rate P + 1.  The
+reference itself gives the same: the committed fixtures order_vortex_p2_n*
+are the reference's own states after the same 1000 steps on the 10^2, 20^2
+and 40^2 meshes; their errors are those of this path (the states agree to
+1e-11) and their rates are 2.64 and 2.59 (tests/test_oracle_golden.py checks
+them on the CPU).  So the bar here is the reference's rate: P + 1 - 0.1 for
+P = 1 and 3, and the reference's measured 2.5 for P = 2."""
 import numpy as np
 import pytest
 
 import hifiles_b200 as H
 import oracle as O
+from golden_util import load, over_integrated_density_error, rel
 
 pytestmark = pytest.mark.gpu
 
 T_END, DT = 1.0, 1e-3
-MESHES = {1: (16, 32, 64), 2: (16, 32, 64), 3: (16, 32, 64)}
+NS = (10, 20, 40, 80)
+MIN_RATE = {1: 1.9, 2: 2.5, 3: 3.9}
 
 
-def _l2_density_error(P, n):
-    s = H.Solver.box(2, P, (n, n), (-10.0, -10.0), (10.0, 10.0), viscous=False, vcjh_scheme=1, gamma=1.4)
-    g = s.geometry()
-    pos = g["pos_upts"]
+def _run(P, n):
+    s = H.Solver.box(2, P, (n, n), (-5.0, -5.0), (5.0, 5.0), viscous=False, vcjh_scheme=1, gamma=1.4)
+    pos = s.geometry()["pos_upts"]
     s.set_state(np.asfortranarray(O.ic_vortex(pos)))
     s.advance(int(round(T_END / DT)), DT)
-    u = s.get_state()
-    exact = O.ic_vortex(pos, t=T_END)
-    w1 = np.polynomial.legendre.leggauss(P + 1)[1]
-    w = np.outer(w1, w1).T.ravel()              # point u = a + (P+1) b  ->  w[a] w[b]
-    err2 = (w[:, None] * g["detjac_upts"] * (u[:, :, 0] - exact[..., 0]) ** 2).sum()
-    return float(np.sqrt(err2))
+    return s.get_state(), pos
 
 
 @pytest.mark.parametrize("P", [1, 2, 3])
-def test_vortex_converges_at_design_order(P):
-    ns = MESHES[P]
-    errs = [_l2_density_error(P, n) for n in ns]
-    slopes = [np.log(errs[i] / errs[i + 1]) / np.log(ns[i + 1] / ns[i]) for i in range(len(ns) - 1)]
-    print("P=%d errors %s slopes %s" % (P, ["%.3e" % e for e in errs], ["%.2f" % s for s in slopes]))
+def test_vortex_convergence_rate(P):
+    errs = []
+    for n in NS:
+        u, pos = _run(P, n)
+        errs.append(over_integrated_density_error(u, pos, P, 10.0 / n, T_END))
+    rates = [np.log(errs[i] / errs[i + 1]) / np.log(NS[i + 1] / NS[i]) for i in range(len(NS) - 1)]
+    print("P=%d errors %s rates %s" % (P, ["%.3e" % e for e in errs], ["%.2f" % r for r in rates]))
     assert all(np.isfinite(errs))
-    assert slopes[-1] > P + 0.4, (errs, slopes)
+    assert rates[-1] > MIN_RATE[P] and rates[-2] > MIN_RATE[P], (errs, rates)
+
+
+@pytest.mark.parametrize("n", [10, 20, 40])
+def test_p2_states_equal_the_reference_runs(n):
+    """The P = 2 convergence runs end where the reference's own runs end."""
+    meta, a = load("order_vortex_p2_n%d" % n)
+    u, _ = _run(2, n)
+    assert rel(u, a["uN"]) <= 1e-11

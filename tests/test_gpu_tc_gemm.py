@@ -59,6 +59,10 @@ def test_bf16x3_product_against_fp64(m, k, n):
     assert np.abs(c64 - ref).max() <= 1e-12 * np.abs(ref).max() * max(1, k)
     c3 = _product(L, A, B, 1)
     err = np.linalg.norm(c3 - ref) / np.linalg.norm(ref)
+    if k == 1:
+        # a one-entry column is all column shift: the product is the FP64 one
+        assert err < 1e-15, err
+        return
     # x0 + x1 keeps ~16 bits of each operand: a few 1e-6 relative
     assert 1e-9 < err < 3e-5, err
     if (m <= 128 and k <= 192) or k <= 128:
@@ -68,6 +72,23 @@ def test_bf16x3_product_against_fp64(m, k, n):
         # products (about 1e-6 relative on random data, more for long k) is
         # then the limit
         assert err6 < 3e-6 and err6 < err / 2, (err6, err)
+
+
+def test_split_carries_only_the_variation_of_each_column():
+    """Columns with a large common level (the TGV energy is ~178 at Mach 0.1
+    against variations of order 1): the BF16 parts carry B minus each
+    column's first entry, so the error scales with the variation, not the level."""
+    rng = np.random.default_rng(11)
+    m, k, n = 96, 64, 500
+    A = rng.standard_normal((m, k)) / k
+    V = rng.standard_normal((k, n))
+    L = _lib()
+    ref0 = A @ V
+    e_var = np.linalg.norm(_product(L, A, V, 1) - ref0)
+    B = V + 178.0
+    e_lvl = np.linalg.norm(_product(L, A, B, 1) - A @ B)
+    # the level adds only its FP64 row-sum term: the error stays that of the variation
+    assert e_lvl < 2.0 * e_var, (e_lvl, e_var)
 
 
 def test_bf16x3_accumulates_into_c():

@@ -10,7 +10,8 @@ import numpy as np
 import pytest
 
 import oracle as O
-from golden_util import BC_CASES, CASES, GOLDEN, IQ_CASES, LES_CASES, ROE_CASES, integral_quantities_numpy, load, rel
+from golden_util import (BC_CASES, CASES, GOLDEN, IQ_CASES, LES_CASES, ROE_CASES, integral_quantities_numpy, load,
+                         over_integrated_density_error, rel)
 
 
 def _mesh(meta):
@@ -92,3 +93,14 @@ def test_integral_quantity_restatement_matches_reference(case):
                                            meta["physics"]["gamma"])
     for v, w, m in zip(vals, a["iq"], mags):
         assert abs(v - w) <= 1e-13 * m
+
+
+def test_reference_convergence_rate_at_p2():
+    """The reference's own P = 2 vortex runs (10^2, 20^2, 40^2 to t = 1, over-integrated
+    density error): rates 2.64 and 2.59 -- the rate the CUDA path is held to at P = 2."""
+    errs = []
+    for n in (10, 20, 40):
+        meta, a = load("order_vortex_p2_n%d" % n)
+        errs.append(over_integrated_density_error(a["uN"], a["pos"], 2, 10.0 / n, 1.0))
+    rates = [np.log(errs[i] / errs[i + 1]) / np.log(2.0) for i in range(2)]
+    assert 2.5 < rates[0] < 2.8 and 2.5 < rates[1] < 2.8, rates
