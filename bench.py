@@ -209,6 +209,23 @@ def _time_steps(advance, stream, steps):
     return e0.elapsed_time(e1) / steps
 
 
+def ke_decay(s64, s32, u0, dt, steps, every):
+    """Config 2's kinetic-energy decay in the FP32 form against FP64 (the
+    kinetic energy on the reference's volume cubature every `every` steps)."""
+    series = {}
+    for name, s in (("fp64", s64), ("fp32", s32)):
+        s.set_state(u0)
+        ke = [s.kinetic_energy()]
+        for _ in range(steps // every):
+            s.advance(every, dt)
+            ke.append(s.kinetic_energy())
+        series[name] = ke
+    k64, k32 = np.array(series["fp64"]), np.array(series["fp32"])
+    return {"steps": steps, "every": every, "dt": dt, "ke_fp64": k64.tolist(),
+            "max_rel_error": float(np.max(np.abs(k32 - k64) / np.abs(k64))),
+            "decay_fp64": float(1.0 - k64[-1] / k64[0]), "decay_fp32": float(1.0 - k32[-1] / k32[0])}
+
+
 def measure_forms(a, dev, fp64_value, s64, u0):
     """The precision and batching forms beside the FP64 headline: the FP32
     form on the same workload with its L2 error against the FP64 path after 20
@@ -233,9 +250,11 @@ def measure_forms(a, dev, fp64_value, s64, u0):
     s32.advance(20, dt)
     u64, u32 = s64.get_state(), s32.get_state()
     l2 = float(np.linalg.norm(u32 - u64) / np.linalg.norm(u64))
+    ke = ke_decay(s64, s32, u0, dt, 200, 10)
     s32.close()
     out = {"fp32": {"value": dof_step / (ms32 * 1e-3), "ms_per_step": ms32, "l2_rel_vs_fp64_after_20_steps": l2,
-                    "ratio_to_fp64": dof_step / (ms32 * 1e-3) / fp64_value}}
+                    "ratio_to_fp64": dof_step / (ms32 * 1e-3) / fp64_value},
+           "ke_decay_fp32_vs_fp64": ke}
     for prec, name in ((0, "batched_fp64"), (1, "batched_fp32")):
         insts = batch_instances(prec)
         t0 = time.perf_counter()

@@ -339,6 +339,52 @@ __global__ void vis_flux_kernel(int nu, long long E, const double* __restrict__ 
     }
 }
 
+// The viscous flux with the eddy-viscosity SGS flux of eles::evaluate_viscFlux
+// with LES (src/eles.cpp:2369-2409): f = F_visc + F_sgs transformed and added
+// to tdisf_upts, and the SGS flux alone transformed into sgsf_upts
+// (sgsf_upts(j,i,k,l) = sum_m JGinv(l,m) F_sgs(k,m), summed from zero).
+template <int D>
+__global__ void vis_flux_les_kernel(int nu, long long E, const double* __restrict__ U, const double* __restrict__ GU,
+                                    const double* __restrict__ JG, const double* __restrict__ detj,
+                                    double* __restrict__ TF, double* __restrict__ SGS, PhysT<double> ph, double n1)
+{
+  constexpr int F = D + 2;
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)nu * E) return;
+  size_t NE = (size_t)nu * E;
+  double q[F], g[F][D], f[F][D], fs[F][D];
+#pragma unroll
+  for (int k = 0; k < F; k++) {
+    q[k] = U[i + NE * k];
+#pragma unroll
+    for (int d = 0; d < D; d++) g[k][d] = GU[i + NE * (k + (size_t)F * d)];
+  }
+  vis_flux<D, double>(ph, q, g, f);
+#pragma unroll
+  for (int k = 0; k < F; k++)
+#pragma unroll
+    for (int d = 0; d < D; d++) fs[k][d] = 0.0;
+  sgs_flux<D, double>(ph, q, g, detj[i], n1, fs);
+#pragma unroll
+  for (int k = 0; k < F; k++)
+#pragma unroll
+    for (int l = 0; l < D; l++) f[k][l] = f[k][l] + fs[k][l];
+  const double* G = JG + (size_t)D * D * i;
+#pragma unroll
+  for (int k = 0; k < F; k++)
+#pragma unroll
+    for (int l = 0; l < D; l++) {
+      double sg = 0.0;
+#pragma unroll
+      for (int mm = 0; mm < D; mm++) sg = sg + G[l + D * mm] * fs[k][mm];
+      SGS[i + NE * (k + (size_t)F * l)] = sg;
+      double acc = TF[i + NE * (k + (size_t)F * l)];
+#pragma unroll
+      for (int mm = 0; mm < D; mm++) acc = fma(G[l + D * mm], f[k][mm], acc);
+      TF[i + NE * (k + (size_t)F * l)] = acc;
+    }
+}
+
 // reference gradient -> physical gradient in place (src/eles.cpp:1822-1878)
 template <int D>
 __global__ void grad_transform_kernel(int nu, long long E, int F, double* __restrict__ GU,
@@ -428,12 +474,16 @@ __global__ void common_inv_kernel(int nfpi, int ni, double* const* __restrict__ 
   }
 }
 
+// sl_p / sr_p (LES): the two sides' SGS flux at the flux points, added to
+// their viscous fluxes before the LDG flux (src/int_inters.cpp:414-427); null
+// without LES.
 template <int D>
 __global__ void common_vis_kernel(int nfpi, int ni, double* const* __restrict__ ul_p, double* const* __restrict__ ur_p,
                                   double* const* __restrict__ gl_p, double* const* __restrict__ gr_p,
                                   double* const* __restrict__ tl_p, double* const* __restrict__ tr_p,
                                   double* const* __restrict__ al_p, double* const* __restrict__ ar_p,
-                                  double* const* __restrict__ n_p, PhysT<double> ph)
+                                  double* const* __restrict__ n_p, PhysT<double> ph,
+                                  double* const* __restrict__ sl_p = nullptr, double* const* __restrict__ sr_p = nullptr)
 {
   constexpr int F = D + 2;
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -453,6 +503,15 @@ __global__ void common_vis_kernel(int nfpi, int ni, double* const* __restrict__ 
   for (int d = 0; d < D; d++) nn[d] = *n_p[t + n * d];
   vis_flux<D, double>(ph, ul, gl, fl);
   vis_flux<D, double>(ph, ur, gr, fr);
+  if (sl_p) {
+#pragma unroll
+    for (int d = 0; d < D; d++)
+#pragma unroll
+      for (int k = 0; k < F; k++) {
+        fl[k][d] += *sl_p[t + n * (k + (long long)F * d)];
+        fr[k][d] += *sr_p[t + n * (k + (long long)F * d)];
+      }
+  }
   ldg_flux<D, double>(ph, ldg_beta<D, double>(ph.pen_fact, nn), ul, ur, fl, fr, nn, fn);
   double tal = *al_p[t], tar = *ar_p[t];
 #pragma unroll
@@ -666,6 +725,61 @@ fr_status fr_op_evaluate_viscFlux(int n_upts, int n_dims, int n_fields, int n_el
   if (n_dims == 2) vis_flux_kernel<2><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_upts, n_eles, disu_upts, grad_disu_upts, JGinv_upts, tdisf_upts, phys_of(phys));
   else vis_flux_kernel<3><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_upts, n_eles, disu_upts, grad_disu_upts, JGinv_upts, tdisf_upts, phys_of(phys));
   return launched("vis_flux_kernel");
+}
+
+fr_status fr_op_evaluate_viscFlux_les(int n_upts, int n_dims, int n_fields, int n_eles, const double* disu_upts,
+                                      const double* grad_disu_upts, const double* JGinv_upts,
+                                      const double* detjac_upts, double* tdisf_upts, double* sgsf_upts,
+                                      const fr_phys_desc* phys, int sgs_model, double filter_ratio, int order,
+                                      void* stream)
+{
+  if (!phys || !disu_upts || !grad_disu_upts || !JGinv_upts || !detjac_upts || !tdisf_upts || !sgsf_upts ||
+      !dims_ok(n_dims, n_fields) || order < 1)
+    return op_fail(FR_ERR_ARG, "bad arguments");
+  if (sgs_model != 0 && sgs_model != 1)
+    return op_fail(FR_ERR_UNSUPPORTED, "SGS models at the per-operator boundary: 0 (Smagorinsky), 1 (WALE)");
+  if (!(filter_ratio > 0.0)) return op_fail(FR_ERR_ARG, "filter_ratio must be positive");
+  long long n = (long long)n_upts * n_eles;
+  if (n == 0) return FR_OK;
+  PhysT<double> ph = phys_of(phys);
+  ph.sgs_model = sgs_model;
+  ph.filter_ratio = filter_ratio;
+  if (n_dims == 2)
+    vis_flux_les_kernel<2><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_upts, n_eles, disu_upts, grad_disu_upts, JGinv_upts, detjac_upts, tdisf_upts, sgsf_upts, ph, (double)(order + 1));
+  else
+    vis_flux_les_kernel<3><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_upts, n_eles, disu_upts, grad_disu_upts, JGinv_upts, detjac_upts, tdisf_upts, sgsf_upts, ph, (double)(order + 1));
+  return launched("vis_flux_les_kernel");
+}
+
+fr_status fr_op_evaluate_sgsFlux(int n_fpts, int n_upts, int n_dims, int n_fields, int n_eles, const double* opp_0,
+                                 const double* sgsf_upts, double* sgsf_fpts, void* stream)
+{
+  if (!opp_0 || !sgsf_upts || !sgsf_fpts || n_dims < 1 || n_dims > 3) return op_fail(FR_ERR_ARG, "bad arguments");
+  const long long cols = (long long)n_fields * n_eles;
+  for (int d = 0; d < n_dims; d++) {
+    fr_status st = dense_apply(n_fpts, n_upts, cols, opp_0, sgsf_upts + (size_t)n_upts * cols * d,
+                               sgsf_fpts + (size_t)n_fpts * cols * d, 0, ST(stream));
+    if (st) return st;
+  }
+  return FR_OK;
+}
+
+fr_status fr_op_int_inters_common_viscFlux_les(int n_fpts_per_inter, int n_dims, int n_fields, int n_inters,
+                                               double* const* disu_fpts_l, double* const* disu_fpts_r,
+                                               double* const* grad_disu_fpts_l, double* const* grad_disu_fpts_r,
+                                               double* const* norm_tconf_fpts_l, double* const* norm_tconf_fpts_r,
+                                               double* const* tdA_fpts_l, double* const* tdA_fpts_r,
+                                               double* const* norm_fpts, double* const* sgsf_fpts_l,
+                                               double* const* sgsf_fpts_r, const fr_phys_desc* phys, void* stream)
+{
+  if (!phys || !sgsf_fpts_l || !sgsf_fpts_r || !dims_ok(n_dims, n_fields)) return op_fail(FR_ERR_ARG, "bad arguments");
+  long long n = (long long)n_fpts_per_inter * n_inters;
+  if (n == 0) return FR_OK;
+  if (n_dims == 2)
+    common_vis_kernel<2><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_fpts_per_inter, n_inters, disu_fpts_l, disu_fpts_r, grad_disu_fpts_l, grad_disu_fpts_r, norm_tconf_fpts_l, norm_tconf_fpts_r, tdA_fpts_l, tdA_fpts_r, norm_fpts, phys_of(phys), sgsf_fpts_l, sgsf_fpts_r);
+  else
+    common_vis_kernel<3><<<grid_for(n, 128), 128, 0, ST(stream)>>>(n_fpts_per_inter, n_inters, disu_fpts_l, disu_fpts_r, grad_disu_fpts_l, grad_disu_fpts_r, norm_tconf_fpts_l, norm_tconf_fpts_r, tdA_fpts_l, tdA_fpts_r, norm_fpts, phys_of(phys), sgsf_fpts_l, sgsf_fpts_r);
+  return launched("common_vis_kernel");
 }
 
 fr_status fr_op_extrapolate_totalFlux(int n_fpts, int n_upts, int n_dims, int n_fields, int n_eles,

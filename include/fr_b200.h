@@ -387,6 +387,36 @@ fr_status fr_op_evaluate_viscFlux(int n_upts, int n_dims, int n_fields, int n_el
                                   const double* grad_disu_upts, const double* JGinv_upts, double* tdisf_upts,
                                   const fr_phys_desc* phys, void* stream);
 
+/* eles::evaluate_viscFlux with LES (eddy-viscosity SGS models), include/eles.h:142,
+ * src/eles.cpp:2321-2409 (the CPU path's form; its GPU wrapper
+ * evaluate_viscFlux_gpu_kernel_wrapper, include/cuda_kernels.h:48, has the
+ * same arguments plus sgsf_upts): tdisf_upts += JGinv (F_visc + F_sgs) and
+ * sgsf_upts (n_upts, n_eles, n_fields, n_dims) = JGinv F_sgs.  sgs_model 0
+ * Smagorinsky, 1 WALE (src/eles.cpp:2456-2778); the filter width uses detJ
+ * and order as calc_sgsf_upts does. */
+fr_status fr_op_evaluate_viscFlux_les(int n_upts, int n_dims, int n_fields, int n_eles, const double* disu_upts,
+                                      const double* grad_disu_upts, const double* JGinv_upts,
+                                      const double* detjac_upts, double* tdisf_upts, double* sgsf_upts,
+                                      const fr_phys_desc* phys, int sgs_model, double filter_ratio, int order,
+                                      void* stream);
+
+/* eles::evaluate_sgsFlux, include/eles.h:124 (src/eles.cpp:3294-3368, cublasDgemm
+ * on opp_0 per dimension): sgsf_fpts[.., d] = opp_0 * sgsf_upts[.., d]. */
+fr_status fr_op_evaluate_sgsFlux(int n_fpts, int n_upts, int n_dims, int n_fields, int n_eles, const double* opp_0,
+                                 const double* sgsf_upts, double* sgsf_fpts, void* stream);
+
+/* int_inters::calculate_common_viscFlux with LES, include/int_inters.h:64
+ * (src/int_inters.cpp:359-470): as fr_op_int_inters_common_viscFlux, each
+ * side's SGS flux at the flux point (tables sgsf_fpts_l/_r shaped like
+ * grad_disu_fpts_l/_r) added to its viscous flux before the LDG flux. */
+fr_status fr_op_int_inters_common_viscFlux_les(int n_fpts_per_inter, int n_dims, int n_fields, int n_inters,
+                                               double* const* disu_fpts_l, double* const* disu_fpts_r,
+                                               double* const* grad_disu_fpts_l, double* const* grad_disu_fpts_r,
+                                               double* const* norm_tconf_fpts_l, double* const* norm_tconf_fpts_r,
+                                               double* const* tdA_fpts_l, double* const* tdA_fpts_r,
+                                               double* const* norm_fpts, double* const* sgsf_fpts_l,
+                                               double* const* sgsf_fpts_r, const fr_phys_desc* phys, void* stream);
+
 /* eles::extrapolate_totalFlux, include/eles.h:121: norm_tdisf_fpts = sum_d opp_1[d] * tdisf_upts[d]. */
 fr_status fr_op_extrapolate_totalFlux(int n_fpts, int n_upts, int n_dims, int n_fields, int n_eles,
                                       const double* const* opp_1, const double* tdisf_upts, double* norm_tdisf_fpts,

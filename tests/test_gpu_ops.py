@@ -49,6 +49,9 @@ def _bind(L):
     L.fr_op_int_inters_common_invFlux.argtypes = [i, i, i, i] + [VP] * 9 + [C.c_void_p, i, i, VP]
     L.fr_op_int_inters_common_viscFlux.argtypes = [i, i, i, i] + [VP] * 9 + [C.c_void_p, VP]
     L.fr_op_advance_rk45.argtypes = [i, i, i, i, dbl, dbl, VP, VP, VP, VP, VP, VP]
+    L.fr_op_evaluate_viscFlux_les.argtypes = [i, i, i, i, VP, VP, VP, VP, VP, VP, C.c_void_p, i, dbl, i, VP]
+    L.fr_op_evaluate_sgsFlux.argtypes = [i, i, i, i, i, VP, VP, VP, VP]
+    L.fr_op_int_inters_common_viscFlux_les.argtypes = [i, i, i, i] + [VP] * 11 + [C.c_void_p, VP]
     return L
 
 
@@ -61,7 +64,8 @@ def _ok(st):
     assert st == 0, H.lib().fr_last_error().decode()
 
 
-@pytest.mark.parametrize("case", ["quad_vortex_p3_n6", "hex_tgv_p3_n3", "hex_tgv_p2_n3_jit", "hex_euler_p3_n3"])
+@pytest.mark.parametrize("case", ["quad_vortex_p3_n6", "hex_tgv_p3_n3", "hex_tgv_p2_n3_jit", "hex_euler_p3_n3",
+                                  "hex_wale_p3_n3_jit", "hex_smag_p2_n3", "quad_wale_p3_n6_jit"])
 def test_operator_seam_matches_reference_stage_arrays(case):
     meta, a = load(case)
     L = _bind(H.lib())
@@ -73,7 +77,8 @@ def test_operator_seam_matches_reference_stage_arrays(case):
     il, ir = m.interfaces()
     nfpi = (meta["order"] + 1) ** (D - 1)
     ni = len(il) // nfpi
-    ph = PhysDesc(**meta["physics"])
+    ph = PhysDesc(**{k: meta["physics"][k] for k, _ in PhysDesc._fields_})
+    les = bool(meta["physics"].get("les", 0))
     opp = {w: _dev(m.operator(w)) for w in (0, 3)}
     opd = {w: [_dev(m.operator(w, d)) for d in range(D)] for w in (1, 2, 5)}
     arr_ptrs = {w: (C.c_void_p * D)(*[t.data_ptr() for t in opd[w]]) for w in opd}
@@ -96,6 +101,10 @@ def test_operator_seam_matches_reference_stage_arrays(case):
     gk = (np.arange(F)[:, None] + F * np.arange(D)[None, :]).ravel(order="F")[None, :] * (nf * E)
     tab["gl"] = _ptr_table(gfp, il[:, None] + gk)
     tab["gr"] = _ptr_table(gfp, ir[:, None] + gk)
+    sgu = torch.zeros(nu * E * F * D, dtype=torch.float64, device="cuda")
+    sgf = torch.zeros(nf * E * F * D, dtype=torch.float64, device="cuda")
+    tab["sl"] = _ptr_table(sgf, il[:, None] + gk)
+    tab["sr"] = _ptr_table(sgf, ir[:, None] + gk)
     P = lambda t: t.data_ptr()  # noqa: E731
 
     _ok(L.fr_op_extrapolate_solution(nf, nu, F, E, P(opp[0]), P(u), P(ufp), None))
@@ -108,10 +117,21 @@ def test_operator_seam_matches_reference_stage_arrays(case):
     if visc:
         _ok(L.fr_op_correct_gradient(nu, nf, D, F, E, C.cast(arr_ptrs[5], VP), P(ddu), P(JG), P(dj), P(gup), None))
         _ok(L.fr_op_extrapolate_corrected_gradient(nf, nu, D, F, E, P(opp[0]), P(gup), P(gfp), None))
-        _ok(L.fr_op_evaluate_viscFlux(nu, D, F, E, P(u), P(gup), P(JG), P(tf), C.byref(ph), None))
+        if les:
+            _ok(L.fr_op_evaluate_viscFlux_les(nu, D, F, E, P(u), P(gup), P(JG), P(dj), P(tf), P(sgu), C.byref(ph),
+                                              meta["physics"]["sgs_model"], meta["physics"]["filter_ratio"],
+                                              meta["order"], None))
+            _ok(L.fr_op_evaluate_sgsFlux(nf, nu, D, F, E, P(opp[0]), P(sgu), P(sgf), None))
+        else:
+            _ok(L.fr_op_evaluate_viscFlux(nu, D, F, E, P(u), P(gup), P(JG), P(tf), C.byref(ph), None))
     _ok(L.fr_op_extrapolate_totalFlux(nf, nu, D, F, E, C.cast(arr_ptrs[1], VP), P(tf), P(ntd), None))
     _ok(L.fr_op_calculate_divergence(nu, D, F, E, C.cast(arr_ptrs[2], VP), P(tf), P(div), None))
-    if visc:
+    if visc and les:
+        _ok(L.fr_op_int_inters_common_viscFlux_les(nfpi, D, F, ni, P(tab["ul"]), P(tab["ur"]), P(tab["gl"]),
+                                                   P(tab["gr"]), P(tab["tl"]), P(tab["tr"]), P(tab["al"]),
+                                                   P(tab["ar"]), P(tab["n"]), P(tab["sl"]), P(tab["sr"]),
+                                                   C.byref(ph), None))
+    elif visc:
         _ok(L.fr_op_int_inters_common_viscFlux(nfpi, D, F, ni, P(tab["ul"]), P(tab["ur"]), P(tab["gl"]),
                                                P(tab["gr"]), P(tab["tl"]), P(tab["tr"]), P(tab["al"]),
                                                P(tab["ar"]), P(tab["n"]), C.byref(ph), None))
@@ -123,6 +143,11 @@ def test_operator_seam_matches_reference_stage_arrays(case):
     assert rel(_host(tf, (nu, E, F, D)), a["tdisf_upts0"]) <= tol
     assert rel(_host(ntd, (nf, E, F)), a["norm_tdisf_fpts0"]) <= tol
     assert rel(ntc_before, a["norm_tconf_fpts0"]) <= tol
+    if les:
+        # the SGS flux at the solution points (transformed) and its extrapolation
+        assert rel(_host(sgu, (nu, E, F, D)), a["sgsf_upts0"]) <= tol
+        want_f = np.einsum("fu,uekd->fekd", m.operator(0), a["sgsf_upts0"])
+        assert rel(_host(sgf, (nf, E, F, D)), want_f) <= tol
     if visc:
         assert rel(_host(ddu, (nf, E, F)), a["delta_disu_fpts0"]) <= tol
         assert rel(_host(gup, (nu, E, F, D)), a["grad_disu_upts0"]) <= tol
