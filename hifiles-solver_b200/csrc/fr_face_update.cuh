@@ -149,8 +149,9 @@ __device__ __noinline__ void fu_boundary(PhysT<TC> ph, int type, FUBdy<DIM, TC> 
 // flux of boundary points from the gradient kernel (side bits 2.. hold the
 // boundary type there, and mate = -1 - the point's place in the boundary
 // list).  err is set when a bounded wait for the bulk copies gives up.
-template <int DIM, int P, int EPB, int NT, int VISC, int MODE, typename TC, int RIEMANN = 0>
-__global__ void __launch_bounds__(NT)
+// MINB: CTAs per SM the registers are capped for.
+template <int DIM, int P, int EPB, int NT, int VISC, int MODE, typename TC, int RIEMANN = 0, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB)
 fr_face_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restrict__ UFn,
                       const TC* __restrict__ UF, const int* __restrict__ mate, const unsigned char* __restrict__ side,
                       const TC* __restrict__ VF, const TC* __restrict__ ND, const TC* __restrict__ DV,

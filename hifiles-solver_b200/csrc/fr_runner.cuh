@@ -77,7 +77,7 @@ FR_TILES(2, 5, T_({4, 160}), T_({4, 160}))
 FR_TILES(3, 1, T_({12, 128}), T_({12, 128}))
 FR_TILES(3, 2, T_({4, 128}, {2, 64}, {8, 256}), T_({4, 128}, {2, 64}, {8, 256}))
 FR_TILES(3, 3, T_({2, 128, 4}, {1, 64, 8}, {2, 192, 2}, {2, 128, 3}, {1, 96, 0}, {4, 256, 2}, {1, 96, 5}, {1, 96, 6},
-                  {1, 64, 8, 1}, {2, 128, 3, 1}, {1, 96, 10}), T_({2, 192}, {1, 96}, {2, 128}, {1, 64}, {4, 256}, {4, 128}))
+                  {1, 64, 8, 1}, {2, 128, 3, 1}, {1, 96, 10}), T_({1, 96, 7}, {1, 64, 8}, {1, 96}, {1, 64}, {2, 128}, {1, 96, 6}, {1, 64, 9}, {2, 192, 3}))
 FR_TILES(3, 4, T_({1, 128}, {1, 160}, {2, 256}), T_({1, 128}, {2, 256}, {1, 160}))
 #undef T_
 #undef FR_TILES
@@ -210,11 +210,12 @@ struct RunnerT : Runner {
       if (I != usel) return update_i<I + 1, VISC, MODE>(b, cur, stage, dt, want_partial, s);
       constexpr int EPB = Tiles<DIM, P>::upd[I].epb, NT = Tiles<DIM, P>::upd[I].nt;
       if constexpr (FU) {
+        constexpr int MB = Tiles<DIM, P>::upd[I].minb > 0 ? Tiles<DIM, P>::upd[I].minb : 1;
         if constexpr (DIM == 2) {
-          if (riemann == 2) fu_launch<EPB, NT, VISC, MODE, 2>(b, cur, stage, dt, want_partial, s);
-          else fu_launch<EPB, NT, VISC, MODE, 0>(b, cur, stage, dt, want_partial, s);
+          if (riemann == 2) fu_launch<EPB, NT, VISC, MODE, 2, MB>(b, cur, stage, dt, want_partial, s);
+          else fu_launch<EPB, NT, VISC, MODE, 0, MB>(b, cur, stage, dt, want_partial, s);
         } else {
-          fu_launch<EPB, NT, VISC, MODE, 0>(b, cur, stage, dt, want_partial, s);
+          fu_launch<EPB, NT, VISC, MODE, 0, MB>(b, cur, stage, dt, want_partial, s);
         }
       } else {
         constexpr size_t sm = update_smem_bytes<DIM, P, EPB, NT, VISC, MODE, TC>();
@@ -227,14 +228,14 @@ struct RunnerT : Runner {
       }
     }
   }
-  template <int EPB, int NT, int VISC, int MODE, int RS>
+  template <int EPB, int NT, int VISC, int MODE, int RS, int MB>
   void fu_launch(const Bufs& b, int cur, int stage, double dt, bool want_partial, cudaStream_t s)
   {
     constexpr size_t sm = face_update_smem_bytes<DIM, P, TC, VISC, MODE, EPB, NT>();
-    const void* kfn = (const void*)fr_face_update_kernel<DIM, P, EPB, NT, VISC, MODE, TC, RS>;
+    const void* kfn = (const void*)fr_face_update_kernel<DIM, P, EPB, NT, VISC, MODE, TC, RS, MB>;
     static bool once = (set_smem(kfn, sm), true);
     (void)once;
-    fr_face_update_kernel<DIM, P, EPB, NT, VISC, MODE, TC, RS><<<(unsigned)((E + EPB - 1) / EPB), NT, sm, s>>>(
+    fr_face_update_kernel<DIM, P, EPB, NT, VISC, MODE, TC, RS, MB><<<(unsigned)((E + EPB - 1) / EPB), NT, sm, s>>>(
         b.U, b.REG, (TC*)b.UF[cur ^ 1], (const TC*)b.UF[cur], b.mate, b.side, (const TC*)b.VF, (const TC*)b.ND,
         (const TC*)b.DV, (const TC*)b.JG, (const TC*)b.nL, (const TC*)b.tdA, b.idetj, (const TC*)b.BV, b.DIV,
         want_partial ? b.partial : nullptr, E, L, ph, kRK4A[stage], kRK4B[stage], dt, stage == 0 ? 1 : 0, b.err);

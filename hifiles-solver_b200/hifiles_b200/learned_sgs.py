@@ -322,6 +322,10 @@ def run_experiment(nf=24, nc=6, P=3, mu=2e-3, dt=1e-3, t_snaps=(0.25, 0.5), t_ev
     apriori["true_mean_dissipation"] = float(eps_true.mean())
     # a posteriori: coarse LES from the filtered initial field
     post = {}
+    spec_f = energy_spectrum(coarse, data[-1][1], nc)
+    kmax = nc * (P + 1) // 3                      # the well-resolved wavenumbers of the coarse mesh
+    tk = sorted(float(k) for k in ke_f)
+    diss_f = -np.diff([ke_f[k] for k in tk]) / np.diff(tk)
     for name in ("none", "wale", "learned"):
         kw2 = dict(kw)
         if name == "wale":
@@ -340,12 +344,55 @@ def run_experiment(nf=24, nc=6, P=3, mu=2e-3, dt=1e-3, t_snaps=(0.25, 0.5), t_ev
             t = ts
             kes[ts] = s.kinetic_energy()
         err = [abs(kes[ts] - ke_f[ts]) / ke_f[ts] for ts in kes]
-        post[name] = {"ke": {str(k): v for k, v in kes.items()}, "mean_rel_ke_error": float(np.mean(err))}
+        spec = energy_spectrum(s, s.get_state(), nc)
+        kes0 = dict(kes, **{0.0: ke_f[0.0]})
+        diss = -np.diff([kes0[k] for k in tk]) / np.diff(tk)
+        post[name] = {"ke": {str(k): v for k, v in kes.items()}, "mean_rel_ke_error": float(np.mean(err)),
+                      "spectrum_t_eval": spec.tolist(), "spectrum_log_error": spectrum_error(spec, spec_f, kmax),
+                      "dissipation_rate": diss.tolist(),
+                      "dissipation_rel_error": float(np.linalg.norm(diss - diss_f) / np.linalg.norm(diss_f))}
         s.close()
     return {"config": {"fine": nf, "coarse": nc, "order": P, "mu": mu, "dt": dt, "t_snaps": list(t_snaps),
                        "t_eval": t_eval, "seed": seed, "samples": int(len(Y))},
             "loss_history": [float(h) for h in hist], "filtered_fine_ke": {str(k): v for k, v in ke_f.items()},
+            "filtered_fine_spectrum_t_eval": spec_f.tolist(), "filtered_fine_dissipation_rate": diss_f.tolist(),
+            "spectrum_kmax": int(kmax),
             "a_priori": apriori, "a_posteriori": post, "params": w}
+
+
+def energy_spectrum(solver, q, n):
+    """Shell-averaged kinetic-energy spectrum E(k), k = 1 .. n(P+1)/2, of the
+    velocity of a state q (nu, E, 5) on the periodic box of n^3 elements:
+    the velocity is interpolated to the (P+1)^3 uniform cell centres of every
+    element, Fourier transformed on the n(P+1) grid, and E(k) sums
+    |u_hat|^2 / 2 over the wavenumbers with |k| in [k - 1/2, k + 1/2)."""
+    ijk, N1 = _grid(solver, n)
+    xg, _ = _gauss(N1 - 1)
+    xu = -1.0 + (2 * np.arange(N1) + 1) / N1
+    Lm = _lagrange(xg, xu)                              # [a, a'] = l_a(x_a')
+    M = n * N1
+    vel = q[:, :, 1:4] / q[:, :, :1]                    # (nu, E, 3)
+    grid = np.zeros((3, M, M, M))
+    v = vel.reshape(N1, N1, N1, -1, 3, order="F")       # [a, b, c, e, comp]
+    w = np.einsum("aA,bB,cC,abcem->ABCem", Lm, Lm, Lm, v)
+    for e in range(vel.shape[1]):
+        i, j, k = ijk[e]
+        grid[:, k * N1:(k + 1) * N1, j * N1:(j + 1) * N1, i * N1:(i + 1) * N1] = \
+            w[:, :, :, e, :].transpose(3, 2, 1, 0)      # [comp, z, y, x]
+    uh = np.fft.fftn(grid, axes=(1, 2, 3)) / M ** 3
+    e3 = 0.5 * (np.abs(uh) ** 2).sum(axis=0)
+    kk = np.fft.fftfreq(M, 1.0 / M)
+    kz, ky, kx = np.meshgrid(kk, kk, kk, indexing="ij")
+    kmag = np.sqrt(kx ** 2 + ky ** 2 + kz ** 2)
+    shells = np.rint(kmag).astype(np.int64)
+    spec = np.bincount(shells.ravel(), weights=e3.ravel(), minlength=M)
+    return spec[1:M // 2 + 1]
+
+
+def spectrum_error(spec, ref, kmax):
+    """Relative L2 distance of log E(k) from the reference's over k = 1 .. kmax."""
+    a, b = np.log(spec[:kmax]), np.log(ref[:kmax])
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
 def _ke(coarse, q):
