@@ -277,30 +277,53 @@ def measure_forms(a, dev, fp64_value, s64, u0):
                     "[2, 4] drawn with seed %d; DOF-updates per RK stage over all instances" % (BATCH_N, BATCH_SEED))
     out["operator_path"] = measure_operator_path(a, dev, s64, u0)
     out["tgv64_p4"] = measure_tgv64_p4(dev)
-    out["mixed_channel"] = {name: measure_mixed_channel(name) for name in ("mixed_channel_p2", "mixed_channel_p3")}
+    out["mixed_channel"] = {"p%d" % P: measure_mixed_channel(P) for P in (2, 3)}
     return out
 
 
-def measure_mixed_channel(case, target_dofs=10_000_000, steps=2, err_steps=10):
-    """The mixed tet/prism channel (isothermal and adiabatic walls on the
-    prisms' triangular faces, jittered vertices, periodic in x and z) through
-    the per-operator entry points: operators, metrics and wiring as the
-    reference's eles_tets / eles_pris / bdy_inters set them up (the committed
-    fixture of one small channel), tiled into independent copies up to
-    about 10 M DOFs.  FP64 operator products on the CUDA cores against BF16x3
-    and BF16x6 split products on the tensor cores, with their L2 error
-    against FP64 after `err_steps` steps."""
-    import json as _json
+# Channel flow at Mach 0.1, Re 1600 in the reference's non-dimensional units
+# (what its input processing makes of Mach_free_stream 0.1, Re_free_stream
+# 1600, T_wall = T_free_stream, free stream along x): the physics and the
+# boundary values of bdy_inters::set_bdy_params, in that order.
+CHANNEL_PHYSICS = {"gamma": 1.4, "prandtl": 0.71, "mu_inf": 0.000625, "rt_inf": 69.32142857142854,
+                   "c_sth": 0.41215868109222054, "fix_vis": 1.0, "tau": 1.0, "pen_fact": 0.5}
+CHANNEL_BDY = [1.0, 1.0, 0.0, 0.0, 71.4285714285714, 0.0, 0.0, 0.0, 1.0, 71.92982267888384, 1.002, 1.0, 0.0, 0.0]
+CHANNEL_R_REF = 71.42857142857142
+
+
+def channel_state(pos):
+    """Smooth non-uniform flow at the Mach 0.1 free stream (rho = 1, u = 1,
+    p = 1 / (gamma M^2)) at points pos (n, E, 3): the synthetic initial field
+    of the channel runs."""
+    x, y, z = pos[..., 0], pos[..., 1], pos[..., 2]
+    p0 = 1.0 / (GAMMA * 0.01)
+    rho = 1.0 + 0.05 * np.sin(x) * np.cos(y)
+    u, v, w = 1.0 + 0.1 * np.sin(y), 0.1 * np.cos(x), 0.05 * np.sin(x + y + z)
+    p = p0 * (1.0 + 0.01 * np.cos(x + y))
+    q = np.stack([rho, rho * u, rho * v, rho * w, p / (GAMMA - 1.0) + 0.5 * rho * (u * u + v * v + w * w)], -1)
+    return np.asfortranarray(q)
+
+
+def measure_mixed_channel(order, n=(40, 20, 20), steps=3, err_steps=10, dt=2e-4):
+    """The mixed-element channel: 40 x 20 x 20 cells on [0, 2 pi] x [0, 2] x
+    [0, pi], interior vertices jittered by up to +-0.15 h (seed 2024), the
+    first and last cell layer in y extruded as prisms (two per cell), six tets
+    per core cell, periodic in x and z, an isothermal wall at y = 0 and an
+    adiabatic one at y = 2 on the prisms' triangular faces.  Set up by the
+    library (operators, metrics, wiring: hifiles_b200.mixed) and advanced
+    through the fr_op_* entry points with FP64 operator products on the CUDA
+    cores and BF16x3 / BF16x6 split products on the tensor cores, with their
+    L2 error against FP64 after `err_steps` steps."""
     import torch
+    from hifiles_b200 import mixed as X
     from hifiles_b200 import seam
-    z = np.load(os.path.join(REPO, "tests", "golden", case + ".npz"))
-    meta = _json.loads(str(z["meta"]))
-    arrs = {k: np.asfortranarray(z[k]) for k in z.files if k != "meta"}
-    types, ints, bdys = seam.mixed_mesh_inputs(meta, arrs)
-    dofs_one = sum(t["u"].size for t in types.values())
-    copies = max(1, target_dofs // dofs_one)
-    tt, ti, tb = seam.tile_mixed_mesh(types, ints, bdys, copies)
-    m = seam.MixedOperatorMesh(tt, ti, meta["physics"], tb, meta["bdy"], meta["R_ref"])
+    t0 = time.time()
+    xv, cells, period, bfaces = X.channel_mesh(n)
+    M = X.MixedMesh(order, xv, cells, period, bfaces,
+                    X.ElementOpts(vcjh_scheme_tet=2, vcjh_scheme_tri=1, vcjh_scheme_pri_1d=1))
+    setup_s = time.time() - t0
+    types, ints, bdys = M.operator_inputs({t: channel_state(m["pos_upts"]) for t, m in M.types.items()})
+    m = seam.MixedOperatorMesh(types, ints, CHANNEL_PHYSICS, bdys, CHANNEL_BDY, CHANNEL_R_REF)
     u0 = {i: m.S[i]["u"].clone() for i in m.S}
 
     def reset():
@@ -308,7 +331,6 @@ def measure_mixed_channel(case, target_dofs=10_000_000, steps=2, err_steps=10):
             s["u"].copy_(u0[i])
             s["reg"].zero_()
 
-    dt = meta["dt"]
     res = {}
     for mode, name in ((0, "fp64"), (1, "bf16x3"), (2, "bf16x6")):
         reset()
@@ -324,11 +346,14 @@ def measure_mixed_channel(case, target_dofs=10_000_000, steps=2, err_steps=10):
         num = sum(float(torch.linalg.vector_norm(s["u"] - ref[i]) ** 2) for i, s in m.S.items())
         den = sum(float(torch.linalg.vector_norm(ref[i]) ** 2) for i in m.S)
         res[name]["l2_rel_vs_fp64_after_%d_steps" % err_steps] = (num / den) ** 0.5
-    cnt = meta["element_counts"]
-    res["workload"] = ("%d copies of a %s channel of order %d (%s tets, %s prisms per copy; isothermal wall at y = 0, "
-                       "adiabatic at y = 2 pi), %d DOFs; one step = 5 RK stages of CalcResidual through the fr_op_* "
-                       "entry points" % (copies, "x".join(str(v) for v in meta["n"]), meta["order"], cnt["6"],
-                                         cnt["5"], m.dofs))
+    finite = all(bool(torch.isfinite(s["u"]).all()) for s in m.S.values())
+    ne = {X.TET: 0, X.PRISM: 0}
+    ne.update({t: int(v["n_eles"]) for t, v in M.types.items()})
+    res["workload"] = ("channel %s cells of order %d: %d tets, %d prisms, %d DOFs, jitter 0.15 h; dt %g; one step = 5 "
+                       "RK stages of CalcResidual through the fr_op_* entry points" %
+                       ("x".join(str(v) for v in n), order, ne[X.TET], ne[X.PRISM], m.dofs, dt))
+    res["host_setup_s"] = setup_s
+    res["finite_after_error_run"] = finite
     del m
     torch.cuda.empty_cache()
     return res

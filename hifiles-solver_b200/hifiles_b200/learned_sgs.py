@@ -345,7 +345,7 @@ def run_experiment(nf=24, nc=6, P=3, mu=2e-3, dt=1e-3, t_snaps=(0.25, 0.5), t_ev
             kes[ts] = s.kinetic_energy()
         err = [abs(kes[ts] - ke_f[ts]) / ke_f[ts] for ts in kes]
         spec = energy_spectrum(s, s.get_state(), nc)
-        kes0 = dict(kes, **{0.0: ke_f[0.0]})
+        kes0 = {**kes, 0.0: ke_f[0.0]}
         diss = -np.diff([kes0[k] for k in tk]) / np.diff(tk)
         post[name] = {"ke": {str(k): v for k, v in kes.items()}, "mean_rel_ke_error": float(np.mean(err)),
                       "spectrum_t_eval": spec.tolist(), "spectrum_log_error": spectrum_error(spec, spec_f, kmax),

