@@ -309,18 +309,18 @@ static Mat vcjh_filter(int dims, int P, double c, const Mat& V, const std::vecto
 
 // ------------------------------------------------------------ element types
 struct Element {
-  int type = 0, P = 0, nu = 0, nf = 0, nface = 0;
+  int type = 0, D = 3, P = 0, nu = 0, nf = 0, nface = 0;
   int nfpf[6] = {};
   int face0[7] = {};                    // first flux point of each face
-  std::vector<double> lu, tf, tn;       // (n, 3) point-major
-  // tets: inverse Vandermonde of the solution points; prisms: of the
-  // triangle points, plus the 1-D points
+  std::vector<double> lu, tf, tn;       // (n, 3) point-major (z = 0 in 2-D)
+  // tets and triangles: inverse Vandermonde of the solution points; prisms:
+  // of the triangle points, plus the 1-D points
   std::vector<std::array<int, 3>> m3;
   std::vector<std::array<int, 2>> m2;
   Mat Vinv;
   int ntri = 0;
   std::vector<double> x1d;
-  Line1D line;                          // hexes and the prisms' 1-D direction
+  Line1D line;                          // quads, hexes and the prisms' 1-D direction
   Mat opp3;                             // (nu, nf) row-major
 };
 
@@ -329,7 +329,19 @@ static int tri_count(int P) { return (P + 1) * (P + 2) / 2; }
 // Nodal basis of every solution point at x (l[nu]).
 static void basis(const Element& E, const double* x, double* l)
 {
-  if (E.type == FR_ELE_TET) {
+  if (E.type == FR_ELE_TRI) {
+    std::vector<double> phi(E.nu);
+    for (int i = 0; i < E.nu; i++) phi[i] = dub2(x[0], x[1], E.m2[i][0], E.m2[i][1]);
+    for (int j = 0; j < E.nu; j++) {
+      double s = 0.0;
+      for (int i = 0; i < E.nu; i++) s += E.Vinv[(size_t)i * E.nu + j] * phi[i];
+      l[j] = s;
+    }
+  } else if (E.type == FR_ELE_QUAD) {
+    int n1 = E.P + 1;
+    for (int b = 0; b < n1; b++)
+      for (int a = 0; a < n1; a++) l[a + n1 * b] = lagrange(x[0], a, E.line.loc, n1) * lagrange(x[1], b, E.line.loc, n1);
+  } else if (E.type == FR_ELE_TET) {
     std::vector<double> phi(E.nu);
     for (int i = 0; i < E.nu; i++) phi[i] = dub3(x, E.m3[i]);
     for (int j = 0; j < E.nu; j++) {
@@ -363,7 +375,28 @@ static void basis(const Element& E, const double* x, double* l)
 // Derivative along reference coordinate d of every nodal basis function at x.
 static void dbasis(const Element& E, const double* x, int d, double* l)
 {
-  if (E.type == FR_ELE_TET) {
+  if (E.type == FR_ELE_TRI) {
+    std::vector<double> dphi(E.nu);
+    for (int i = 0; i < E.nu; i++) {
+      double gr, gs;
+      grad_dub2(x[0], x[1], E.m2[i][0], E.m2[i][1], gr, gs);
+      dphi[i] = d == 0 ? gr : gs;
+    }
+    for (int j = 0; j < E.nu; j++) {
+      double s = 0.0;
+      for (int i = 0; i < E.nu; i++) s += E.Vinv[(size_t)i * E.nu + j] * dphi[i];
+      l[j] = s;
+    }
+  } else if (E.type == FR_ELE_QUAD) {
+    int n1 = E.P + 1;
+    const double* X = E.line.loc;
+    for (int b = 0; b < n1; b++)
+      for (int a = 0; a < n1; a++) {
+        double fa = d == 0 ? dlagrange(x[0], a, X, n1) : lagrange(x[0], a, X, n1);
+        double fb = d == 1 ? dlagrange(x[1], b, X, n1) : lagrange(x[1], b, X, n1);
+        l[a + n1 * b] = fa * fb;
+      }
+  } else if (E.type == FR_ELE_TET) {
     std::vector<double> dphi(E.nu);
     for (int i = 0; i < E.nu; i++) { double g[3]; grad_dub3(x, E.m3[i], g); dphi[i] = g[d]; }
     for (int j = 0; j < E.nu; j++) {
@@ -414,9 +447,9 @@ static void set_faces(Element& E)
 // solution point k) of a modal basis given its Vandermonde V.
 static std::vector<Mat> nodal_derivatives(const Element& E)
 {
-  std::vector<Mat> D(3, Mat((size_t)E.nu * E.nu));
+  std::vector<Mat> D(E.D, Mat((size_t)E.nu * E.nu));
   std::vector<double> l(E.nu);
-  for (int d = 0; d < 3; d++)
+  for (int d = 0; d < E.D; d++)
     for (int k = 0; k < E.nu; k++) {
       dbasis(E, &E.lu[3 * k], d, l.data());
       for (int j = 0; j < E.nu; j++) D[d][(size_t)k * E.nu + j] = l[j];
@@ -655,6 +688,74 @@ static bool setup_prism(Element& E, const fr_element_opts& o, std::string& err)
   return true;
 }
 
+// Triangles (src/eles_tris.cpp:66-137 set-up, 185-272 points, 450-478
+// normals, 644-648 correction): flux points on the edges at the 1-D points
+// of fpts_type_tri.
+static bool setup_tri(Element& E, const fr_element_opts& o, std::string& err)
+{
+  int P = E.P, n1 = P + 1;
+  if (P < 1 || P > 5) { err = "triangles: order 1-5"; return false; }
+  E.D = 2;
+  E.nu = tri_count(P);
+  E.nface = 3;
+  for (int f = 0; f < 3; f++) E.nfpf[f] = n1;
+  set_faces(E);
+  const double* tri = o.upts_type_tri == 0 ? kTriInter[P] : o.upts_type_tri == 1 ? kTriAlpha[P] : nullptr;
+  if (!tri) { err = "triangles: point type 0 (interior) or 1 (alpha-optimised)"; return false; }
+  E.x1d.assign(n1, 0.0);
+  if (!points_1d(P, o.fpts_type_tri, E.x1d.data())) { err = "triangles: flux point type 0 (Gauss) or 1 (Lobatto)"; return false; }
+  const double* X = E.x1d.data();
+  E.lu.assign(3 * E.nu, 0.0);
+  for (int j = 0; j < E.nu; j++) { E.lu[3 * j] = tri[2 * j]; E.lu[3 * j + 1] = tri[2 * j + 1]; }
+  E.tf.assign(3 * E.nf, 0.0);
+  E.tn.assign(3 * E.nf, 0.0);
+  for (int f = 0; f < 3; f++)
+    for (int j = 0; j < n1; j++) {
+      double* t = &E.tf[3 * (n1 * f + j)];
+      double* n = &E.tn[3 * (n1 * f + j)];
+      if (f == 0) { t[0] = X[j]; t[1] = -1.0; n[1] = -1.0; }
+      else if (f == 1) { t[0] = X[P - j]; t[1] = X[j]; n[0] = n[1] = 1. / std::sqrt(2.); }
+      else { t[0] = -1.0; t[1] = X[P - j]; n[0] = -1.0; }
+    }
+  tri_modes(P, E.m2);
+  Mat V((size_t)E.nu * E.nu);
+  for (int i = 0; i < E.nu; i++)
+    for (int j = 0; j < E.nu; j++) V[(size_t)i * E.nu + j] = dub2(tri[2 * i], tri[2 * i + 1], E.m2[j][0], E.m2[j][1]);
+  if (!invert(E.nu, V, E.Vinv)) { err = "triangles: singular Vandermonde matrix"; return false; }
+  return tri_correction(P, tri, X, o.vcjh_scheme_tri, o.c_tri, E.opp3, err);
+}
+
+// Quadrilaterals in the reference's point orders (src/eles_quads.cpp:237-300),
+// corrected like the hexahedra.
+static bool setup_quad(Element& E, const fr_element_opts& o, std::string& err)
+{
+  if (!make_line(E.P, o.upts_type_quad, o.vcjh_scheme_quad, o.eta_quad, E.line, err)) return false;
+  int n1 = E.P + 1;
+  E.D = 2;
+  E.nu = n1 * n1;
+  E.nface = 4;
+  for (int f = 0; f < 4; f++) E.nfpf[f] = n1;
+  set_faces(E);
+  std::vector<double> lu, tf, tn;
+  element_points(2, E.line, lu, tf, tn);
+  E.lu.assign(3 * E.nu, 0.0); E.tf.assign(3 * E.nf, 0.0); E.tn.assign(3 * E.nf, 0.0);
+  for (int k = 0; k < E.nu; k++) for (int d = 0; d < 2; d++) E.lu[3 * k + d] = lu[2 * k + d];
+  for (int q = 0; q < E.nf; q++)
+    for (int d = 0; d < 2; d++) { E.tf[3 * q + d] = tf[2 * q + d]; E.tn[3 * q + d] = tn[2 * q + d]; }
+  E.opp3.assign((size_t)E.nu * E.nf, 0.0);
+  for (int q = 0; q < E.nf; q++) {
+    const double* t = &E.tf[3 * q];
+    const double* n = &E.tn[3 * q];
+    int ax = n[0] != 0 ? 0 : 1;
+    bool plus = n[ax] > 0;
+    for (int u = 0; u < E.nu; u++) {
+      int c[2] = {u % n1, u / n1};
+      if (E.line.loc[c[1 - ax]] == t[1 - ax]) E.opp3[(size_t)u * E.nf + q] = plus ? E.line.gR[c[ax]] : -E.line.gL[c[ax]];
+    }
+  }
+  return true;
+}
+
 // Hexahedra in the reference's point orders (src/eles_hexas.cpp:240-324),
 // correction g'_L / g'_R along the face normal on the line of solution points
 // through each flux point.
@@ -688,22 +789,39 @@ static bool make_element(int type, int P, const fr_element_opts& o, Element& E, 
 {
   E = Element();
   E.type = type; E.P = P;
+  if (type == FR_ELE_TRI) return setup_tri(E, o, err);
+  if (type == FR_ELE_QUAD) return setup_quad(E, o, err);
   if (type == FR_ELE_TET) return setup_tet(E, o, err);
   if (type == FR_ELE_PRISM) return setup_prism(E, o, err);
   if (type == FR_ELE_HEX) return setup_hex(E, o, err);
-  err = "element type: 2 (tetrahedron), 3 (prism) or 4 (hexahedron)";
+  err = "element type: 0 (triangle), 1 (quadrilateral), 2 (tetrahedron), 3 (prism) or 4 (hexahedron)";
   return false;
 }
 
 // ------------------------------------------------------------- geometry
-static int shape_nodes(int type) { return type == FR_ELE_TET ? 4 : type == FR_ELE_PRISM ? 6 : 8; }
+static int shape_nodes(int type)
+{
+  return type == FR_ELE_TRI ? 3 : type == FR_ELE_QUAD ? 4 : type == FR_ELE_TET ? 4 : type == FR_ELE_PRISM ? 6 : 8;
+}
+static int type_dims(int type) { return type == FR_ELE_TRI || type == FR_ELE_QUAD ? 2 : 3; }
 
 // Linear shape functions of the reference's vertex orders
 // (src/eles_tets.cpp:862-950, src/eles_pris.cpp:852-990,
 // src/eles_hexas.cpp:985-1060) and their derivatives dN[node + ns * d].
 static void shape(int type, const double* r, double* N, double* dN)
 {
-  if (type == FR_ELE_TET) {
+  if (type == FR_ELE_TRI) {
+    N[0] = -0.5 * (r[0] + r[1]); N[1] = 0.5 * (r[0] + 1.); N[2] = 0.5 * (r[1] + 1.);
+    dN[0] = -0.5; dN[1] = 0.5; dN[2] = 0.0;
+    dN[3] = -0.5; dN[4] = 0.0; dN[5] = 0.5;
+  } else if (type == FR_ELE_QUAD) {
+    static const double c2[2] = {-1.0, 1.0};
+    for (int s = 0; s < 4; s++) {
+      int a = s & 1, b = (s >> 1) & 1;
+      double la = lagrange(r[0], a, c2, 2), lb = lagrange(r[1], b, c2, 2);
+      N[s] = la * lb; dN[s] = dlagrange(r[0], a, c2, 2) * lb; dN[s + 4] = la * dlagrange(r[1], b, c2, 2);
+    }
+  } else if (type == FR_ELE_TET) {
     N[0] = -0.5 * (r[0] + r[1] + r[2] + 1.); N[1] = 0.5 * (r[0] + 1.); N[2] = 0.5 * (r[1] + 1.); N[3] = 0.5 * (r[2] + 1.);
     for (int d = 0; d < 3; d++)
       for (int k = 0; k < 4; k++) dN[k + 4 * d] = k == 0 ? -0.5 : (k == d + 1 ? 0.5 : 0.0);
@@ -729,23 +847,38 @@ static void shape(int type, const double* r, double* N, double* dN)
   }
 }
 
-// Position and Jacobian J[j + 3 k] = dx_j / dr_k of one element at r.
+// Position and Jacobian J[j + D k] = dx_j / dr_k of one element at r
+// (vertices xv with stride 3).
 static void map_point(int type, const double* xv, const int* cv, const double* r, double* pos, double* J)
 {
-  int ns = shape_nodes(type);
+  int ns = shape_nodes(type), D = type_dims(type);
   double N[8], dN[24];
   shape(type, r, N, dN);
-  for (int i = 0; i < 3; i++) {
+  for (int i = 0; i < D; i++) {
     double s = 0.0;
     for (int j = 0; j < ns; j++) s += N[j] * xv[3 * (size_t)cv[j] + i];
     pos[i] = s;
   }
-  for (int j = 0; j < 3; j++)
-    for (int k = 0; k < 3; k++) {
+  for (int j = 0; j < D; j++)
+    for (int k = 0; k < D; k++) {
       double s = 0.0;
       for (int i = 0; i < ns; i++) s += dN[i + ns * k] * xv[3 * (size_t)cv[i] + j];
-      J[j + 3 * k] = s;
+      J[j + D * k] = s;
     }
+}
+
+// 2-D: adj(J), det(J) and the transformed normal (src/eles.cpp:4615-4800).
+static double adjugate2(const double* J, double* G)
+{
+  double xr = J[0], xs = J[2], yr = J[1], ys = J[3];
+  G[0] = ys; G[2] = -xs; G[1] = -yr; G[3] = xr;
+  return xr * ys - xs * yr;
+}
+
+static void face_normal2(const double* J, const double* t, double* v)
+{
+  v[0] = (t[0] * J[3]) - (t[1] * J[1]);
+  v[1] = -(t[0] * J[2]) + (t[1] * J[0]);
 }
 
 // adj(J) in JGinv's layout (G[a + 3 b] = JGinv(a, b)) and det(J)
@@ -780,14 +913,15 @@ using namespace frb;
 using namespace frb::mixed;
 
 struct fr_mixed {
-  int order = 0;
+  int dims = 3, order = 0;
   int n_types = 0;
   int types[3] = {};                        // ele_type of each slot
   Element el[3];
   std::vector<int> c2v[3];                  // (ns, ne) per slot
   std::vector<long long> cell_of[3];        // global cell of each element
   std::vector<double> JG[3], dj[3], tdA[3], nrm[3], pu[3], pf[3];
-  // interface groups: triangular faces, quadrilateral faces
+  // interface groups: triangular faces (3-D) or edges (2-D), then
+  // quadrilateral faces
   int n_igroups = 0, igroup_nfpi[2] = {};
   std::vector<int> itab[2];                 // (6, nfpi, ni) with ni = size / (6 nfpi)
   int n_bgroups = 0, bgroup_nfpi[2] = {};
@@ -818,21 +952,30 @@ double wrap(double c, double L, double lo)
 }
 }  // namespace
 
-static const fr_element_opts kDefaultOpts = {0, 0, 0, 0.0, 0, 0, 0, 0.0, 0, 0.0, 0, 1, 0.0};
+static const fr_element_opts kDefaultOpts = {0, 0, 0, 0.0, 0, 0, 0, 0.0, 0, 0.0, 0, 1, 0.0, 0, 0, 0, 1, 0.0};
+
+static bool element_sizes(int ele_type, int P, int& nu, int& nfc, int* per)
+{
+  int nt = (P + 1) * (P + 2) / 2, nq = (P + 1) * (P + 1);
+  switch (ele_type) {
+    case FR_ELE_TRI: nu = nt; nfc = 3; for (int f = 0; f < 3; f++) per[f] = P + 1; return true;
+    case FR_ELE_QUAD: nu = nq; nfc = 4; for (int f = 0; f < 4; f++) per[f] = P + 1; return true;
+    case FR_ELE_TET: nu = nt * (P + 3) / 3; nfc = 4; for (int f = 0; f < 4; f++) per[f] = nt; return true;
+    case FR_ELE_PRISM: nu = nt * (P + 1); nfc = 5; per[0] = per[1] = nt; per[2] = per[3] = per[4] = nq; return true;
+    case FR_ELE_HEX: nu = nq * (P + 1); nfc = 6; for (int f = 0; f < 6; f++) per[f] = nq; return true;
+  }
+  return false;
+}
 
 extern "C" {
 
 fr_status fr_element_sizes(int ele_type, int order, int* n_upts, int* n_fpts, int* n_faces, int* n_fpts_per_face)
 {
   g_err.clear();
-  int P = order;
-  if (P < 1 || P > 5) return fail(FR_ERR_UNSUPPORTED, "order 1-5");
-  int nt = (P + 1) * (P + 2) / 2, nq = (P + 1) * (P + 1);
-  int nu, nfc, per[6];
-  if (ele_type == FR_ELE_TET) { nu = nt * (P + 3) / 3; nfc = 4; for (int f = 0; f < 4; f++) per[f] = nt; }
-  else if (ele_type == FR_ELE_PRISM) { nu = nt * (P + 1); nfc = 5; per[0] = per[1] = nt; per[2] = per[3] = per[4] = nq; }
-  else if (ele_type == FR_ELE_HEX) { nu = nq * (P + 1); nfc = 6; for (int f = 0; f < 6; f++) per[f] = nq; }
-  else return fail(FR_ERR_ARG, "element type: 2 (tetrahedron), 3 (prism) or 4 (hexahedron)");
+  if (order < 1 || order > 5) return fail(FR_ERR_UNSUPPORTED, "order 1-5");
+  int nu = 0, nfc = 0, per[6] = {};
+  if (!element_sizes(ele_type, order, nu, nfc, per))
+    return fail(FR_ERR_ARG, "element type: 0 (triangle), 1 (quadrilateral), 2 (tetrahedron), 3 (prism), 4 (hexahedron)");
   int nf = 0;
   for (int f = 0; f < nfc; f++) nf += per[f];
   if (n_upts) *n_upts = nu;
@@ -852,26 +995,26 @@ fr_status fr_element_operators(int ele_type, int order, const fr_element_opts* o
   Element E;
   std::string err;
   if (!make_element(ele_type, order, o, E, err)) return fail(FR_ERR_UNSUPPORTED, err);
-  int nu = E.nu, nf = E.nf;
+  int nu = E.nu, nf = E.nf, D = E.D;
   for (int k = 0; k < nu; k++)
-    for (int d = 0; d < 3; d++)
-      if (loc_upts) loc_upts[d + 3 * k] = E.lu[3 * k + d];
+    for (int d = 0; d < D; d++)
+      if (loc_upts) loc_upts[d + D * k] = E.lu[3 * k + d];
   for (int q = 0; q < nf; q++)
-    for (int d = 0; d < 3; d++) {
-      if (tloc_fpts) tloc_fpts[d + 3 * q] = E.tf[3 * q + d];
-      if (tnorm_fpts) tnorm_fpts[d + 3 * q] = E.tn[3 * q + d];
+    for (int d = 0; d < D; d++) {
+      if (tloc_fpts) tloc_fpts[d + D * q] = E.tf[3 * q + d];
+      if (tnorm_fpts) tnorm_fpts[d + D * q] = E.tn[3 * q + d];
     }
   std::vector<double> l(nu);
   for (int q = 0; q < nf; q++) {
     basis(E, &E.tf[3 * q], l.data());
     for (int u = 0; u < nu; u++) {
       if (opp_0) opp_0[q + (size_t)nf * u] = l[u];
-      for (int d = 0; d < 3; d++)
+      for (int d = 0; d < D; d++)
         if (opp_1) opp_1[q + (size_t)nf * (u + (size_t)nu * d)] = l[u] * E.tn[3 * q + d];
     }
   }
   if (opp_2)
-    for (int d = 0; d < 3; d++)
+    for (int d = 0; d < D; d++)
       for (int k = 0; k < nu; k++) {
         dbasis(E, &E.lu[3 * k], d, l.data());
         for (int u = 0; u < nu; u++) opp_2[k + (size_t)nu * (u + (size_t)nu * d)] = l[u];
@@ -880,33 +1023,41 @@ fr_status fr_element_operators(int ele_type, int order, const fr_element_opts* o
     for (int q = 0; q < nf; q++) {
       double v = E.opp3[(size_t)u * nf + q];
       if (opp_3) opp_3[u + (size_t)nu * q] = v;
-      for (int d = 0; d < 3; d++)
+      for (int d = 0; d < D; d++)
         if (opp_5) opp_5[u + (size_t)nu * (q + (size_t)nf * d)] = v * E.tn[3 * q + d];
     }
   return FR_OK;
 }
 
-fr_status fr_mixed_create(int order, const fr_element_opts* opts, long long n_verts, const double* xv,
+fr_status fr_mixed_create(int dims, int order, const fr_element_opts* opts, long long n_verts, const double* xv_in,
                           long long n_cells, const int* cell_type, const int* cell_verts, const double* period,
                           long long n_bfaces, const long long* bface_cell, const int* bface_face,
                           const int* bface_type, fr_mixed** out)
 {
   g_err.clear();
-  if (!out || !xv || !cell_type || !cell_verts || n_verts <= 0 || n_cells <= 0)
+  if (!out || !xv_in || !cell_type || !cell_verts || n_verts <= 0 || n_cells <= 0)
     return fail(FR_ERR_ARG, "null or empty mesh");
+  if (dims != 2 && dims != 3) return fail(FR_ERR_ARG, "dims must be 2 or 3");
   if (n_bfaces > 0 && (!bface_cell || !bface_face || !bface_type)) return fail(FR_ERR_ARG, "null boundary list");
   *out = nullptr;
+  const int D = dims;
   const fr_element_opts& o = opts ? *opts : kDefaultOpts;
   std::unique_ptr<fr_mixed> m(new fr_mixed());
+  m->dims = D;
   m->order = order;
-  // element slots in the order tets, prisms, hexes; per cell its slot/index
+  std::vector<double> xv((size_t)3 * n_verts, 0.0);     // stride 3, z = 0 in 2-D
+  for (long long v = 0; v < n_verts; v++)
+    for (int d = 0; d < D; d++) xv[3 * v + d] = xv_in[D * v + d];
+  // element slots in the order tris, quads, tets, prisms, hexes; per cell its slot/index
   std::vector<int> slot_of(n_cells);
   std::vector<long long> ele_of(n_cells);
   int slot_for[5] = {-1, -1, -1, -1, -1};
-  for (int t : {FR_ELE_TET, FR_ELE_PRISM, FR_ELE_HEX})
+  for (int t : {FR_ELE_TRI, FR_ELE_QUAD, FR_ELE_TET, FR_ELE_PRISM, FR_ELE_HEX})
     for (long long c = 0; c < n_cells; c++)
       if (cell_type[c] == t) {
+        if (type_dims(t) != D) return fail(FR_ERR_ARG, "cell type does not match dims");
         if (slot_for[t] < 0) {
+          if (m->n_types == 3) return fail(FR_ERR_ARG, "at most three element types");
           slot_for[t] = m->n_types;
           m->types[m->n_types] = t;
           std::string err;
@@ -917,7 +1068,7 @@ fr_status fr_mixed_create(int order, const fr_element_opts* opts, long long n_ve
       }
   for (long long c = 0; c < n_cells; c++) {
     int t = cell_type[c];
-    if (t < 0 || t > 4 || slot_for[t] < 0) return fail(FR_ERR_ARG, "cell type: 2 (tet), 3 (prism) or 4 (hex)");
+    if (t < 0 || t > 4 || slot_for[t] < 0) return fail(FR_ERR_ARG, "cell type: 0 (tri), 1 (quad), 2 (tet), 3 (prism) or 4 (hex)");
     int s = slot_for[t];
     slot_of[c] = s;
     ele_of[c] = (long long)m->cell_of[s].size();
@@ -928,32 +1079,32 @@ fr_status fr_mixed_create(int order, const fr_element_opts* opts, long long n_ve
       m->c2v[s].push_back(v);
     }
   }
-  // metrics (reference layouts: JGinv (3,3,nu,E), detjac (nu,E), tdA (nf,E), norm (nf,E,3))
+  // metrics (reference layouts: JGinv (D,D,nu,E), detjac (nu,E), tdA (nf,E), norm (nf,E,D))
   for (int s = 0; s < m->n_types; s++) {
     const Element& E = m->el[s];
     int ns = shape_nodes(E.type);
     size_t ne = m->cell_of[s].size(), nu = E.nu, nf = E.nf;
-    m->JG[s].assign(9 * nu * ne, 0.0); m->dj[s].assign(nu * ne, 0.0);
-    m->tdA[s].assign(nf * ne, 0.0); m->nrm[s].assign(3 * nf * ne, 0.0);
-    m->pu[s].assign(3 * nu * ne, 0.0); m->pf[s].assign(3 * nf * ne, 0.0);
+    m->JG[s].assign((size_t)D * D * nu * ne, 0.0); m->dj[s].assign(nu * ne, 0.0);
+    m->tdA[s].assign(nf * ne, 0.0); m->nrm[s].assign(D * nf * ne, 0.0);
+    m->pu[s].assign(D * nu * ne, 0.0); m->pf[s].assign(D * nf * ne, 0.0);
     for (size_t e = 0; e < ne; e++) {
       const int* cv = &m->c2v[s][ns * e];
       double p[3], J[9], G[9];
       for (size_t u = 0; u < nu; u++) {
-        map_point(E.type, xv, cv, &E.lu[3 * u], p, J);
-        double det = adjugate(J, G);
+        map_point(E.type, xv.data(), cv, &E.lu[3 * u], p, J);
+        double det = D == 2 ? adjugate2(J, G) : adjugate(J, G);
         if (!(det > 0)) return fail(FR_ERR_MESH, "non-positive Jacobian at a solution point");
         m->dj[s][u + nu * e] = det;
-        for (int a = 0; a < 9; a++) m->JG[s][a + 9 * (u + nu * e)] = G[a];
-        for (int d = 0; d < 3; d++) m->pu[s][u + nu * (e + ne * d)] = p[d];
+        for (int a = 0; a < D * D; a++) m->JG[s][a + D * D * (u + nu * e)] = G[a];
+        for (int d = 0; d < D; d++) m->pu[s][u + nu * (e + ne * d)] = p[d];
       }
       for (size_t q = 0; q < nf; q++) {
-        map_point(E.type, xv, cv, &E.tf[3 * q], p, J);
-        double v[3];
-        face_normal(J, &E.tn[3 * q], v);
-        double a = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        map_point(E.type, xv.data(), cv, &E.tf[3 * q], p, J);
+        double v[3] = {0, 0, 0};
+        if (D == 2) face_normal2(J, &E.tn[3 * q], v); else face_normal(J, &E.tn[3 * q], v);
+        double a = std::sqrt(D == 2 ? v[0] * v[0] + v[1] * v[1] : v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
         m->tdA[s][q + nf * e] = a;
-        for (int d = 0; d < 3; d++) {
+        for (int d = 0; d < D; d++) {
           m->nrm[s][q + nf * (e + ne * d)] = v[d] / a;
           m->pf[s][q + nf * (e + ne * d)] = p[d];
         }
@@ -974,15 +1125,16 @@ fr_status fr_mixed_create(int order, const fr_element_opts* opts, long long n_ve
   // flux points of paired faces by physical position; the lower cell is the
   // left side (the reference's CompConnectivity / cyclic search / rotation
   // tables, src/geometry.cpp:2412-2720, 3489-3666, src/inters.cpp:187-296)
-  double per[3] = {0, 0, 0}, lo[3] = {1e300, 1e300, 1e300}, h = 1e300;
+  double per[3] = {0, 0, 0}, lo[3] = {0, 0, 0}, h = 1e300;
   if (period)
-    for (int d = 0; d < 3; d++) per[d] = period[d];
+    for (int d = 0; d < D; d++) per[d] = period[d];
+  for (int d = 0; d < D; d++) lo[d] = 1e300;
   for (long long v = 0; v < n_verts; v++)
-    for (int d = 0; d < 3; d++) lo[d] = std::min(lo[d], xv[3 * v + d]);
+    for (int d = 0; d < D; d++) lo[d] = std::min(lo[d], xv[3 * v + d]);
   for (long long c = 0; c < n_cells; c++) {
     const int* cv = &cell_verts[8 * c];
     double s2 = 0;
-    for (int d = 0; d < 3; d++) { double t = xv[3 * (size_t)cv[1] + d] - xv[3 * (size_t)cv[0] + d]; s2 += t * t; }
+    for (int d = 0; d < D; d++) { double t = xv[3 * (size_t)cv[1] + d] - xv[3 * (size_t)cv[0] + d]; s2 += t * t; }
     h = std::min(h, std::sqrt(s2));
   }
   double tol = 1e-6 * h;
@@ -991,8 +1143,7 @@ fr_status fr_mixed_create(int order, const fr_element_opts* opts, long long n_ve
     return m->pf[s][q + nf * (e + ne * d)];
   };
   std::unordered_map<FKey, long long, FKeyHash> open;
-  std::vector<int> tabs[2], btabs[2];
-  int nt = (order + 1) * (order + 2) / 2, nq = (order + 1) * (order + 1);
+  int nt = (order + 1) * (order + 2) / 2;
   // per group: left/right triples, gathered as rows then transposed
   std::vector<std::array<int, 6>> rows[2];
   std::vector<std::array<int, 4>> brows[2];
@@ -1001,14 +1152,14 @@ fr_status fr_mixed_create(int order, const fr_element_opts* opts, long long n_ve
     const Element& E = m->el[s];
     size_t e = (size_t)ele_of[c];
     for (int fc = 0; fc < E.nface; fc++) {
-      int np = E.nfpf[fc], kind = np == nt ? 0 : 1, q0 = E.face0[fc];
+      int np = E.nfpf[fc], kind = (D == 2 || np == nt) ? 0 : 1, q0 = E.face0[fc];
       auto bi = bmap.find(c * 8 + fc);
       if (bi != bmap.end()) {
         for (int q = 0; q < np; q++) brows[kind].push_back({E.type, (int)e, q0 + q, bi->second});
         continue;
       }
       FKey k{{0, 0, 0}, kind};
-      for (int d = 0; d < 3; d++) {
+      for (int d = 0; d < D; d++) {
         double sm = 0;
         for (int q = 0; q < np; q++) sm += fpos(s, e, q0 + q, d);
         k.c[d] = (long long)std::llround(wrap(sm / np, per[d], lo[d]) / tol);
@@ -1028,7 +1179,7 @@ fr_status fr_mixed_create(int order, const fr_element_opts* opts, long long n_ve
         double bd = 1e300;
         for (int r = 0; r < np; r++) {
           double dd = 0;
-          for (int d = 0; d < 3; d++) {
+          for (int d = 0; d < D; d++) {
             double t = wrap(fpos(sa, ea, qa0 + q, d), per[d], lo[d]) - wrap(fpos(s, e, q0 + r, d), per[d], lo[d]);
             if (per[d] > 0) { if (t > 0.5 * per[d]) t -= per[d]; if (t < -0.5 * per[d]) t += per[d]; }
             dd += t * t;
@@ -1043,9 +1194,9 @@ fr_status fr_mixed_create(int order, const fr_element_opts* opts, long long n_ve
   }
   if (!open.empty()) return fail(FR_ERR_MESH, "unmatched faces without a boundary type");
   for (int kind = 0; kind < 2; kind++) {
-    int np = kind == 0 ? nt : nq;
     if (!rows[kind].empty()) {
       int g = m->n_igroups++;
+      int np = kind == 0 ? (D == 2 ? order + 1 : nt) : (order + 1) * (order + 1);
       size_t ni = rows[kind].size() / np;
       m->igroup_nfpi[g] = np;
       m->itab[g].assign(6 * rows[kind].size(), 0);
@@ -1055,6 +1206,7 @@ fr_status fr_mixed_create(int order, const fr_element_opts* opts, long long n_ve
     }
     if (!brows[kind].empty()) {
       int g = m->n_bgroups++;
+      int np = kind == 0 ? (D == 2 ? order + 1 : nt) : (order + 1) * (order + 1);
       size_t ni = brows[kind].size() / np;
       m->bgroup_nfpi[g] = np;
       m->btab[g].assign(4 * brows[kind].size(), 0);

@@ -1,11 +1,13 @@
-"""Meshes of tetrahedra, prisms and hexahedra for the per-operator path:
-the library's host set-up (include/fr_b200.h, fr_element_* and fr_mixed_*)
-and the jittered channel mesh (prism wall layers, tetrahedral core).
+"""Meshes of triangles and quadrilaterals (2-D) or tetrahedra, prisms and
+hexahedra (3-D) for the per-operator path: the library's host set-up
+(include/fr_b200.h, fr_element_* and fr_mixed_*) and the jittered channel
+mesh (prism wall layers, tetrahedral core).
 
 `MixedMesh(...).operator_inputs(states)` gives the (types, int_inters,
 bdy_inters) triple that `seam.MixedOperatorMesh` advances, the same arrays the
-reference's eles_tets / eles_pris / eles_hexas and int_inters / bdy_inters
-objects hold after their set-up (src/eles_tets.cpp:68-1415,
+reference's eles_tris / eles_quads / eles_tets / eles_pris / eles_hexas and
+int_inters / bdy_inters objects hold after their set-up
+(src/eles_tris.cpp:66-648, src/eles_tets.cpp:68-1415,
 src/eles_pris.cpp:51-1194, src/eles.cpp:3620-4800, src/int_inters.cpp:95-178,
 src/bdy_inters.cpp:111-203).
 """
@@ -16,8 +18,9 @@ import numpy as np
 
 from . import _check, box_mesh, lib
 
-TET, PRISM, HEX = 2, 3, 4
-_NODES = {TET: 4, PRISM: 6, HEX: 8}
+TRI, QUAD, TET, PRISM, HEX = 0, 1, 2, 3, 4
+_NODES = {TRI: 3, QUAD: 4, TET: 4, PRISM: 6, HEX: 8}
+_DIMS = {TRI: 2, QUAD: 2, TET: 3, PRISM: 3, HEX: 3}
 
 
 class ElementOpts(C.Structure):
@@ -27,12 +30,14 @@ class ElementOpts(C.Structure):
                 ("c_tet", C.c_double), ("upts_type_pri_tri", C.c_int), ("upts_type_pri_1d", C.c_int),
                 ("vcjh_scheme_tri", C.c_int), ("c_tri", C.c_double), ("vcjh_scheme_pri_1d", C.c_int),
                 ("eta_pri", C.c_double), ("upts_type_hexa", C.c_int), ("vcjh_scheme_hexa", C.c_int),
-                ("eta_hexa", C.c_double)]
+                ("eta_hexa", C.c_double), ("upts_type_tri", C.c_int), ("fpts_type_tri", C.c_int),
+                ("upts_type_quad", C.c_int), ("vcjh_scheme_quad", C.c_int), ("eta_quad", C.c_double)]
 
     def __init__(self, **kw):
         d = dict(upts_type_tet=0, fpts_type_tet=0, vcjh_scheme_tet=0, c_tet=0.0, upts_type_pri_tri=0,
                  upts_type_pri_1d=0, vcjh_scheme_tri=0, c_tri=0.0, vcjh_scheme_pri_1d=0, eta_pri=0.0,
-                 upts_type_hexa=0, vcjh_scheme_hexa=1, eta_hexa=0.0)
+                 upts_type_hexa=0, vcjh_scheme_hexa=1, eta_hexa=0.0, upts_type_tri=0, fpts_type_tri=0,
+                 upts_type_quad=0, vcjh_scheme_quad=1, eta_quad=0.0)
         unknown = set(kw) - set(d)
         if unknown:
             raise TypeError("unknown options: %s" % sorted(unknown))
@@ -53,7 +58,7 @@ def _lib():
     sigs = {
         "fr_element_sizes": [i, i, ip, ip, ip, ip],
         "fr_element_operators": [i, i, C.POINTER(ElementOpts), dp, dp, dp, dp, dp, dp, dp, dp],
-        "fr_mixed_create": [i, C.POINTER(ElementOpts), ll, dp, ll, ip, ip, dp, ll, lp, ip, ip, C.POINTER(vp)],
+        "fr_mixed_create": [i, i, C.POINTER(ElementOpts), ll, dp, ll, ip, ip, dp, ll, lp, ip, ip, C.POINTER(vp)],
         "fr_mixed_destroy": [vp],
         "fr_mixed_info": [vp, ip, ip, lp, ip, ip],
         "fr_mixed_metrics": [vp, i, dp, dp, dp, dp, dp, lp],
@@ -84,36 +89,39 @@ def element_sizes(ele_type, order):
 def element_operators(ele_type, order, opts=None):
     """Point sets and dense operators of one element type, as the
     reference's set_opp_0 .. set_opp_6 build them: opp_0, opp_3, opp_6
-    matrices, opp_1, opp_2, opp_4, opp_5 lists of three (column-major)."""
+    matrices, opp_1, opp_2, opp_4, opp_5 lists of D (column-major)."""
     L = _lib()
     nu, nf, _ = element_sizes(ele_type, order)
+    D = _DIMS[ele_type]
     A = lambda *s: np.zeros(s, order="F")  # noqa: E731
-    lu, tf, tn = A(3, nu), A(3, nf), A(3, nf)
-    o0, o1, o2, o3, o5 = A(nf, nu), A(nf, nu, 3), A(nu, nu, 3), A(nu, nf), A(nu, nf, 3)
+    lu, tf, tn = A(D, nu), A(D, nf), A(D, nf)
+    o0, o1, o2, o3, o5 = A(nf, nu), A(nf, nu, D), A(nu, nu, D), A(nu, nf), A(nu, nf, D)
     o = opts if opts is not None else ElementOpts()
     _check(L.fr_element_operators(ele_type, order, C.byref(o), _dp(lu), _dp(tf), _dp(tn), _dp(o0), _dp(o1),
                                   _dp(o2), _dp(o3), _dp(o5)))
-    split = lambda a: [np.asfortranarray(a[..., d]) for d in range(3)]  # noqa: E731
+    split = lambda a: [np.asfortranarray(a[..., d]) for d in range(D)]  # noqa: E731
     return dict(loc_upts=lu, tloc_fpts=tf, tnorm_fpts=tn, opp_0=o0, opp_1=split(o1), opp_2=split(o2), opp_3=o3,
                 opp_4=split(o2), opp_5=split(o5), opp_6=o0.copy(order="F"))
 
 
 class MixedMesh:
-    """A conforming mesh of tets, prisms and hexes of one order, set up on the
-    host by the library: per element type its operators and metrics, the
-    interface tables (triangular faces, then quadrilateral) and the boundary
-    tables.
+    """A conforming mesh of one order, triangles and quads (xv (n_verts, 2))
+    or tets, prisms and hexes (xv (n_verts, 3)), set up on the host by the
+    library: per element type its operators and metrics, the interface tables
+    (edges in 2-D; triangular faces, then quadrilateral, in 3-D) and the
+    boundary tables.
 
-    xv (n_verts, 3); cells a list of (ele_type, vertex ids) in the reference's
-    vertex orders (hexes in tensor order a + 2 b + 4 c); period (3,) periodic
-    lengths (0: not periodic); bfaces a list of (cell, local face, boundary
-    type)."""
+    cells is a list of (ele_type, vertex ids) in the reference's vertex orders
+    (quads in tensor order a + 2 b, hexes a + 2 b + 4 c); period (dims,)
+    periodic lengths (0: not periodic); bfaces a list of (cell, local face,
+    boundary type)."""
 
     def __init__(self, order, xv, cells, period=None, bfaces=(), opts=None):
         L = _lib()
         self.order = int(order)
         self.opts = opts if opts is not None else ElementOpts()
         xv = np.ascontiguousarray(xv, dtype=np.float64)
+        self.dims = D = xv.shape[1]
         n = len(cells)
         ct = np.array([c[0] for c in cells], dtype=np.int32)
         cv = np.full((n, 8), -1, dtype=np.int32)
@@ -121,13 +129,13 @@ class MixedMesh:
             if t not in _NODES or len(vs) != _NODES[t]:
                 raise ValueError("cell %d: type %r with %d vertices" % (k, t, len(vs)))
             cv[k, :len(vs)] = vs
-        per = np.zeros(3) if period is None else np.ascontiguousarray(period, dtype=np.float64)
+        per = np.zeros(D) if period is None else np.ascontiguousarray(period, dtype=np.float64)
         bf = np.array([b[0] for b in bfaces], dtype=np.int64)
         bfc = np.array([b[1] for b in bfaces], dtype=np.int32)
         bft = np.array([b[2] for b in bfaces], dtype=np.int32)
         h = C.c_void_p()
         ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))  # noqa: E731
-        _check(L.fr_mixed_create(self.order, C.byref(self.opts), xv.shape[0], _dp(xv), n, ip(ct), ip(cv), _dp(per),
+        _check(L.fr_mixed_create(D, self.order, C.byref(self.opts), xv.shape[0], _dp(xv), n, ip(ct), ip(cv), _dp(per),
                                  len(bf), bf.ctypes.data_as(C.POINTER(C.c_longlong)), ip(bfc), ip(bft), C.byref(h)))
         self._h = h
         try:
@@ -141,8 +149,8 @@ class MixedMesh:
                 nu, nf, _ = element_sizes(t, self.order)
                 E = ne[s]
                 A = lambda *shape: np.zeros(shape, order="F")  # noqa: E731
-                m = dict(JGinv_upts=A(3, 3, nu, E), detjac_upts=A(nu, E), tdA_fpts=A(nf, E), norm_fpts=A(nf, E, 3),
-                         pos_upts=A(nu, E, 3), cell=np.zeros(E, dtype=np.int64))
+                m = dict(JGinv_upts=A(D, D, nu, E), detjac_upts=A(nu, E), tdA_fpts=A(nf, E), norm_fpts=A(nf, E, D),
+                         pos_upts=A(nu, E, D), cell=np.zeros(E, dtype=np.int64))
                 _check(L.fr_mixed_metrics(h, s, _dp(m["JGinv_upts"]), _dp(m["detjac_upts"]), _dp(m["tdA_fpts"]),
                                           _dp(m["norm_fpts"]), _dp(m["pos_upts"]),
                                           m["cell"].ctypes.data_as(C.POINTER(C.c_longlong))))

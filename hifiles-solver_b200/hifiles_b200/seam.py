@@ -269,7 +269,8 @@ class MixedOperatorMesh:
     (4, n_fpts_per_inter, n_inters) arrays of the owning side's triple and the
     boundary type (bdy_inters, src/bdy_inters.cpp:111-203), whose boundary
     values `bdy` (14, bdy_inters::set_bdy_params order) and gas constant
-    `R_ref` apply.  Navier-Stokes; the state lives on the device."""
+    `R_ref` apply.  Navier-Stokes in 2-D (tris, quads) or 3-D; the state
+    lives on the device."""
 
     def __init__(self, types, int_inters, physics, bdy_inters=(), bdy=None, R_ref=1.0, device=0):
         import torch
@@ -277,8 +278,8 @@ class MixedOperatorMesh:
         self.L = _bind_bdy(_bind(lib()))
         dev = "cuda:%d" % device
         self.dev = dev
-        D = 3
-        F = 5
+        D = int(np.asarray(next(iter(types.values()))["JGinv_upts"]).shape[0])
+        F = D + 2
         self.D, self.F = D, F
         t = lambda a: torch.from_numpy(np.asfortranarray(a, dtype=np.float64).ravel(order="F").copy()).to(dev)  # noqa
         z = lambda n: torch.zeros(n, dtype=torch.float64, device=dev)  # noqa: E731

@@ -523,13 +523,14 @@ int fr_op_gemm_precision(void);
 fr_status fr_op_check(void* stream);
 
 /* ------------------------------------------------------------------------
- * Host set-up of tetrahedra, prisms and hexahedra for the per-operator path
- * (host only, FP64, no GPU needed).
+ * Host set-up of triangles, quadrilaterals, tetrahedra, prisms and hexahedra
+ * for the per-operator path (host only, FP64, no GPU needed).
  *
  * What the reference's element classes compute before the time loop: point
- * sets, nodal bases and the dense operators (eles_tets / eles_pris /
- * eles_hexas::setup_ele_type_specific with eles::set_opp_0 .. set_opp_6,
- * src/eles.cpp:3620-4060, src/eles_tets.cpp:68-1415,
+ * sets, nodal bases and the dense operators (eles_tris / eles_quads /
+ * eles_tets / eles_pris / eles_hexas::setup_ele_type_specific with
+ * eles::set_opp_0 .. set_opp_6, src/eles.cpp:3620-4060,
+ * src/eles_tris.cpp:66-648, src/eles_tets.cpp:68-1415,
  * src/eles_pris.cpp:51-1194), and for a mesh of those elements the metrics
  * (eles::set_transforms, src/eles.cpp:4557-4800) and the interface and
  * boundary tables (int_inters::set_interior, bdy_inters::set_boundary,
@@ -538,7 +539,7 @@ fr_status fr_op_check(void* stream);
  * end at 5); the SD-, HU-like and c+ simplex schemes exist for orders 2-5
  * (triangles 2-4), as in the reference.
  * ---------------------------------------------------------------------- */
-enum { FR_ELE_TET = 2, FR_ELE_PRISM = 3, FR_ELE_HEX = 4 };
+enum { FR_ELE_TRI = 0, FR_ELE_QUAD = 1, FR_ELE_TET = 2, FR_ELE_PRISM = 3, FR_ELE_HEX = 4 };
 
 typedef struct {
   int upts_type_tet;        /* 0 interior quadrature points, 1 alpha-optimised nodes      */
@@ -547,13 +548,18 @@ typedef struct {
   double c_tet;
   int upts_type_pri_tri;    /* prism triangle points: 0 interior, 1 alpha                 */
   int upts_type_pri_1d;     /* prism line points: 0 Gauss, 1 Gauss-Lobatto                */
-  int vcjh_scheme_tri;      /* prisms' triangle correction, as vcjh_scheme_tet            */
+  int vcjh_scheme_tri;      /* triangles and prisms' triangles, as vcjh_scheme_tet        */
   double c_tri;
   int vcjh_scheme_pri_1d;   /* prisms' line correction: 0 user eta_pri, 1 DG, 2 SD, 3 HU, 4 c+ */
   double eta_pri;
   int upts_type_hexa;       /* hexes: 0 Gauss, 1 Gauss-Lobatto                            */
   int vcjh_scheme_hexa;     /* as vcjh_scheme_pri_1d                                      */
   double eta_hexa;
+  int upts_type_tri;        /* triangles: 0 interior, 1 alpha                             */
+  int fpts_type_tri;        /* triangle edge points: 0 Gauss, 1 Gauss-Lobatto             */
+  int upts_type_quad;       /* quads: 0 Gauss, 1 Gauss-Lobatto                            */
+  int vcjh_scheme_quad;     /* as vcjh_scheme_pri_1d                                      */
+  double eta_quad;
 } fr_element_opts;
 
 /* Sizes of one element type: solution and flux points, faces, flux points
@@ -562,26 +568,28 @@ typedef struct {
 fr_status fr_element_sizes(int ele_type, int order, int* n_upts, int* n_fpts, int* n_faces, int* n_fpts_per_face);
 
 /* Point sets and dense operators of one element type in the reference's
- * layouts (first index fastest): loc_upts (3, n_upts), tloc_fpts and
- * tnorm_fpts (3, n_fpts); opp_0 (n_fpts, n_upts); opp_1 (n_fpts, n_upts, 3);
- * opp_2 (n_upts, n_upts, 3); opp_3 (n_upts, n_fpts); opp_5 (n_upts, n_fpts, 3).
- * The reference's opp_4 equals opp_2 and opp_6 equals opp_0.  opts NULL:
- * every field 0 except vcjh_scheme_hexa 1.  NULL outputs are skipped. */
+ * layouts (first index fastest), D = 2 for triangles and quads, 3 otherwise:
+ * loc_upts (D, n_upts), tloc_fpts and tnorm_fpts (D, n_fpts); opp_0
+ * (n_fpts, n_upts); opp_1 (n_fpts, n_upts, D); opp_2 (n_upts, n_upts, D);
+ * opp_3 (n_upts, n_fpts); opp_5 (n_upts, n_fpts, D).  The reference's opp_4
+ * equals opp_2 and opp_6 equals opp_0.  opts NULL: every field 0 except
+ * vcjh_scheme_hexa and vcjh_scheme_quad 1.  NULL outputs are skipped. */
 fr_status fr_element_operators(int ele_type, int order, const fr_element_opts* opts, double* loc_upts,
                                double* tloc_fpts, double* tnorm_fpts, double* opp_0, double* opp_1, double* opp_2,
                                double* opp_3, double* opp_5);
 
-/* A conforming mesh of tets, prisms and hexes of one order.  xv (3, n_verts);
- * cell_type (n_cells) element types; cell_verts (8, n_cells) vertex indices
- * in the reference's vertex order (tets 4, prisms 6, hexes 8 in tensor order
- * a + 2 b + 4 c; the rest of each column ignored); period[3] the periodic
- * length of each axis (0: not periodic), NULL for none; boundary faces
- * (cell, local face, reference boundary type 1-7 or 11-16).  Every other face
- * must meet another face (directly or through a periodic shift).  Elements of
- * each type are numbered in cell order; the element-type slots are ordered
- * tets, prisms, hexes (those present). */
+/* A conforming mesh of one order: triangles and quads (dims 2) or tets,
+ * prisms and hexes (dims 3).  xv (dims, n_verts); cell_type (n_cells)
+ * element types; cell_verts (8, n_cells) vertex indices in the reference's
+ * vertex order (tris 3; quads 4 in tensor order a + 2 b; tets 4; prisms 6;
+ * hexes 8 in tensor order a + 2 b + 4 c; the rest of each column ignored);
+ * period[dims] the periodic length of each axis (0: not periodic), NULL for
+ * none; boundary faces (cell, local face, reference boundary type 1-7 or
+ * 11-16).  Every other face must meet another face (directly or through a
+ * periodic shift).  Elements of each type are numbered in cell order; the
+ * element-type slots follow the type numbers (those present, at most three). */
 typedef struct fr_mixed fr_mixed;
-fr_status fr_mixed_create(int order, const fr_element_opts* opts, long long n_verts, const double* xv,
+fr_status fr_mixed_create(int dims, int order, const fr_element_opts* opts, long long n_verts, const double* xv,
                           long long n_cells, const int* cell_type, const int* cell_verts, const double* period,
                           long long n_bfaces, const long long* bface_cell, const int* bface_face,
                           const int* bface_type, fr_mixed** out);
@@ -589,13 +597,14 @@ fr_status fr_mixed_destroy(fr_mixed* m);
 /* ele_types and n_eles hold up to 3 entries (one per slot). */
 fr_status fr_mixed_info(const fr_mixed* m, int* n_types, int* ele_types, long long* n_eles, int* n_inter_groups,
                         int* n_bdy_groups);
-/* Metrics of slot `slot`: JGinv_upts (3, 3, n_upts, n_eles), detjac_upts
- * (n_upts, n_eles), tdA_fpts (n_fpts, n_eles), norm_fpts (n_fpts, n_eles, 3),
- * pos_upts (n_upts, n_eles, 3), cell_of_ele (n_eles) the mesh cell of each
- * element.  NULL outputs are skipped. */
+/* Metrics of slot `slot`: JGinv_upts (dims, dims, n_upts, n_eles),
+ * detjac_upts (n_upts, n_eles), tdA_fpts (n_fpts, n_eles), norm_fpts
+ * (n_fpts, n_eles, dims), pos_upts (n_upts, n_eles, dims), cell_of_ele
+ * (n_eles) the mesh cell of each element.  NULL outputs are skipped. */
 fr_status fr_mixed_metrics(const fr_mixed* m, int slot, double* JGinv_upts, double* detjac_upts, double* tdA_fpts,
                            double* norm_fpts, double* pos_upts, long long* cell_of_ele);
-/* Interface group `group` (triangular faces first, then quadrilateral):
+/* Interface group `group` (edges in 2-D; triangular faces first, then
+ * quadrilateral, in 3-D):
  * table (6, n_fpts_per_inter, n_inters) of (element type, element, flux
  * point) of the left and the right side of every interface point, the lower
  * cell being the left side; flux points are paired by position.  Query the

@@ -38,7 +38,8 @@ sys.path.insert(0, os.path.join(HERE, "golden"))
 import make_mixed as MM  # noqa: E402
 from hifiles_b200 import mixed as X  # noqa: E402
 
-CASES = ["mixed_pritet_p3", "mixed_pritet_p2", "mixed_hexpri_p3", "mixed_channel_p2", "mixed_channel_p3"]
+CASES = ["mixed_pritet_p3", "mixed_pritet_p2", "mixed_hexpri_p3", "mixed_channel_p2", "mixed_channel_p3",
+         "mixed_triquad_p3", "mixed_triquad_p2"]
 # Gambit hex node g sits in the reference's hex slot k = G2I.index(g)
 # (src/geometry.cpp:1860-1866)
 G2I = [0, 4, 1, 5, 2, 6, 3, 7]
@@ -47,6 +48,13 @@ G2I = [0, 4, 1, 5, 2, 6, 3, 7]
 def fixture_mesh(meta):
     """(xv, cells, period, bfaces, opts) of a fixture's mesh in the library's
     terms, from the same generator and seed the fixture writer used."""
+    if meta["kind"] == "triquad":
+        lo, hi = (0.0, 0.0), (2 * np.pi, 2 * np.pi)
+        xv, eles = MM.mixed_cells_2d(meta["n"], lo, hi, meta["jitter"], seed=12345)
+        cells = [({3: X.TRI, 2: X.QUAD}[gt], list(vs)) for gt, vs, _ in eles]
+        opts = X.ElementOpts(upts_type_tri=meta["tri_upts"], fpts_type_tri=meta["tri_fpts"],
+                             vcjh_scheme_tri=meta["vcjh_tri"], upts_type_quad=0, vcjh_scheme_quad=1)
+        return xv, cells, [hi[0] - lo[0], hi[1] - lo[1]], [], opts
     lo, hi = (0.0,) * 3, (2 * np.pi,) * 3
     xv, eles = MM.mixed_cells(meta["kind"], meta["n"], lo, hi, meta["jitter"], seed=12345)
     sbc = meta.get("side_bc", [0] * 6)
@@ -84,7 +92,7 @@ def test_element_operators_match_the_reference(case):
         assert _maxrel(ops["opp_6"], a[T + "opp_6"]) <= 1e-13
         assert _maxrel(ops["opp_3"], a[T + "opp_3"]) <= 1e-12, et
         for w, tol in ((1, 1e-13), (2, 1e-13), (4, 1e-13), (5, 1e-12)):
-            for d in range(3):
+            for d in range(meta.get("dims", 3)):
                 assert _maxrel(ops["opp_%d" % w][d], a[T + "opp_%d_%d" % (w, d)]) <= tol, (et, w, d)
 
 
