@@ -25,7 +25,8 @@ import pytest
 
 from golden_util import load, rel
 
-MIXED = ["mixed_pritet_p3", "mixed_pritet_p2", "mixed_hexpri_p3", "mixed_channel_p2", "mixed_channel_p3"]
+MIXED = ["mixed_pritet_p3", "mixed_pritet_p2", "mixed_hexpri_p3", "mixed_channel_p2", "mixed_channel_p3",
+         "mixed_triquad_p3", "mixed_triquad_p2"]
 # 2-D quadrilateral boxes with a boundary on every side: Euler with
 # characteristic / subsonic outflow / slip wall / dual-consistent slip wall and
 # simple in- and outflow / supersonic in- and outflow, Navier-Stokes with
