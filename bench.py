@@ -264,14 +264,25 @@ def measure_forms(a, dev, fp64_value, s64, u0):
         for i, inst in enumerate(insts):
             b.set_state(i, tgv_state(box_upts(inst["n"][0], inst["order"], L)))
         b.autotune(2)
+        chosen = b.merged
         stb = torch.cuda.ExternalStream(b.stream(), device=dev)
-        b.advance(3, dt)
-        l0 = b.launch_count()
-        msb = _time_steps(lambda k: b.advance(k, dt), stb, steps)
-        launches_per_step = (b.launch_count() - l0) // steps
+        # each launch form timed on the same state: per-group launches, merged
+        # launches with registers capped for 4 and for 3 CTAs per SM
+        forms = {}
+        for label, on, minb in (("per_group", 0, 4), ("merged_minb4", 1, 4), ("merged_minb3", 1, 3)):
+            for i, inst in enumerate(insts):
+                b.set_state(i, tgv_state(box_upts(inst["n"][0], inst["order"], L)))
+            b.set_merged(on, minb)
+            b.advance(3, dt)
+            l0 = b.launch_count()
+            ms_f = _time_steps(lambda k: b.advance(k, dt), stb, steps)
+            forms[label] = {"ms_per_step": ms_f, "launches_per_step": (b.launch_count() - l0) // steps}
+        best = ("merged_minb%d" % chosen) if chosen else "per_group"
+        msb, launches_per_step = forms[best]["ms_per_step"], forms[best]["launches_per_step"]
         v = b.dof() * 5 / (msb * 1e-3)
         out[name] = {"value": v, "ms_per_step": msb, "ratio_to_fp64": v / fp64_value, "groups": b.n_groups,
-                     "launches_per_step": launches_per_step, "graphs_per_step": 1, "setup_s": setup_s}
+                     "launches_per_step": launches_per_step, "graphs_per_step": 1, "setup_s": setup_s,
+                     "autotuned_launch_form": best, "launch_forms": forms}
         b.close()
     out["batch"] = ("%d periodic TGV instances (NS, Mach 0.1, Re 1600), sizes n^3 with n in [8, 24] and P in "
                     "[2, 4] drawn with seed %d; DOF-updates per RK stage over all instances" % (BATCH_N, BATCH_SEED))
@@ -337,15 +348,27 @@ def measure_mixed_channel(order, n=(40, 20, 20), steps=3, err_steps=10, dt=2e-4)
         m.advance(1, dt, gemm_precision=mode)
         ms = _time_steps(lambda k: m.advance(k, dt, gemm_precision=mode), m.stream, steps)
         res[name] = {"value": m.dofs * 5 / (ms * 1e-3), "ms_per_step": ms}
+    def l2(a, b):
+        num = sum(float(torch.linalg.vector_norm(a[i] - b[i]) ** 2) for i in a)
+        return (num / sum(float(torch.linalg.vector_norm(b[i]) ** 2) for i in b)) ** 0.5
+
+    # one residual of the initial state, and the state after err_steps steps
     reset()
+    m.residual(0)
+    torch.cuda.synchronize()
+    div0 = {i: s["div"].clone() for i, s in m.S.items()}
     m.advance(err_steps, dt, gemm_precision=0)
+    torch.cuda.synchronize()
     ref = {i: s["u"].clone() for i, s in m.S.items()}
     for mode, name in ((1, "bf16x3"), (2, "bf16x6")):
         reset()
+        m.residual(mode)
+        torch.cuda.synchronize()
+        res[name]["residual_l2_rel_vs_fp64"] = l2({i: s["div"] for i, s in m.S.items()}, div0)
+        reset()
         m.advance(err_steps, dt, gemm_precision=mode)
-        num = sum(float(torch.linalg.vector_norm(s["u"] - ref[i]) ** 2) for i, s in m.S.items())
-        den = sum(float(torch.linalg.vector_norm(ref[i]) ** 2) for i in m.S)
-        res[name]["l2_rel_vs_fp64_after_%d_steps" % err_steps] = (num / den) ** 0.5
+        torch.cuda.synchronize()
+        res[name]["l2_rel_vs_fp64_after_%d_steps" % err_steps] = l2({i: s["u"] for i, s in m.S.items()}, ref)
     finite = all(bool(torch.isfinite(s["u"]).all()) for s in m.S.values())
     ne = {X.TET: 0, X.PRISM: 0}
     ne.update({t: int(v["n_eles"]) for t, v in M.types.items()})

@@ -149,16 +149,18 @@ __device__ __noinline__ void fu_boundary(PhysT<TC> ph, int type, FUBdy<DIM, TC> 
 // flux of boundary points from the gradient kernel (side bits 2.. hold the
 // boundary type there, and mate = -1 - the point's place in the boundary
 // list).  err is set when a bounded wait for the bulk copies gives up.
-// MINB: CTAs per SM the registers are capped for.
-template <int DIM, int P, int EPB, int NT, int VISC, int MODE, typename TC, int RIEMANN = 0, int MINB = 1>
-__global__ void __launch_bounds__(NT, MINB)
-fr_face_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restrict__ UFn,
-                      const TC* __restrict__ UF, const int* __restrict__ mate, const unsigned char* __restrict__ side,
-                      const TC* __restrict__ VF, const TC* __restrict__ ND, const TC* __restrict__ DV,
-                      const TC* __restrict__ JG, const TC* __restrict__ nL, const TC* __restrict__ tdA,
-                      const double* __restrict__ idetj, const TC* __restrict__ BV, double* __restrict__ DIV,
-                      double* __restrict__ partial, long long E, Line<TC> L, PhysT<TC> ph, double rk_a,
-                      double rk_b, double dt, int first_stage, int* __restrict__ err)
+// MINB: CTAs per SM the registers are capped for.  The body serves element
+// block blk (fr_face_update_kernel: blockIdx.x; merged batch launches: their
+// share of the grid).
+template <int DIM, int P, int EPB, int NT, int VISC, int MODE, typename TC, int RIEMANN = 0>
+__device__ __forceinline__ void
+fr_face_update_body(long long blk, double* __restrict__ U, double* __restrict__ REG, TC* __restrict__ UFn,
+                    const TC* __restrict__ UF, const int* __restrict__ mate, const unsigned char* __restrict__ side,
+                    const TC* __restrict__ VF, const TC* __restrict__ ND, const TC* __restrict__ DV,
+                    const TC* __restrict__ JG, const TC* __restrict__ nL, const TC* __restrict__ tdA,
+                    const double* __restrict__ idetj, const TC* __restrict__ BV, double* __restrict__ DIV,
+                    double* __restrict__ partial, long long E, const Line<TC>& L, const PhysT<TC>& ph, double rk_a,
+                    double rk_b, double dt, int first_stage, int* __restrict__ err)
 {
   static_assert(fu_bulk_ok<DIM, P, TC>(), "bulk-copy face/update kernel needs 16-byte runs");
   using S = Shape<DIM, P>;
@@ -184,7 +186,7 @@ fr_face_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __re
   auto sRed = reinterpret_cast<double (*)[F]>(fr_smem + Q::oRED);
 
   const int tid = threadIdx.x;
-  const long long e0 = (long long)blockIdx.x * EPB;
+  const long long e0 = blk * EPB;
   const int nval = (int)(E - e0 < EPB ? E - e0 : EPB);
   const long long NFE = (long long)NF * E, NUE = (long long)NU * E;
   const bool want_reg = MODE == 1 && !first_stage;
@@ -498,7 +500,7 @@ fr_face_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __re
     if (partial && tid < F) {
       double v = 0.0;
       for (int i = 0; i < NT / 32; i++) v += sRed[i][tid];
-      partial[(size_t)blockIdx.x * F + tid] = v;
+      partial[(size_t)blk * F + tid] = v;
     }
     // traces of the updated state for the next stage: the opp_0 row of f in column order
 #pragma unroll
@@ -521,6 +523,21 @@ fr_face_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __re
       }
     }
   }
+}
+
+template <int DIM, int P, int EPB, int NT, int VISC, int MODE, typename TC, int RIEMANN = 0, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB)
+fr_face_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restrict__ UFn,
+                      const TC* __restrict__ UF, const int* __restrict__ mate, const unsigned char* __restrict__ side,
+                      const TC* __restrict__ VF, const TC* __restrict__ ND, const TC* __restrict__ DV,
+                      const TC* __restrict__ JG, const TC* __restrict__ nL, const TC* __restrict__ tdA,
+                      const double* __restrict__ idetj, const TC* __restrict__ BV, double* __restrict__ DIV,
+                      double* __restrict__ partial, long long E, Line<TC> L, PhysT<TC> ph, double rk_a,
+                      double rk_b, double dt, int first_stage, int* __restrict__ err)
+{
+  fr_face_update_body<DIM, P, EPB, NT, VISC, MODE, TC, RIEMANN>(blockIdx.x, U, REG, UFn, UF, mate, side, VF, ND, DV, JG,
+                                                                nL, tdA, idetj, BV, DIV, partial, E, L, ph, rk_a, rk_b,
+                                                                dt, first_stage, err);
 }
 
 }  // namespace frb

@@ -431,12 +431,16 @@ __host__ __device__ constexpr bool grad_alias()
 // list; with BV null the mesh has no boundary points and those bits are
 // ignored), and, when GRAD is not null, the corrected physical gradient
 // grad_disu_upts (n_upts, n_eles, F, D).
-template <int DIM, int P, int EPB, int NT, typename TC, int LES = 0, int MINB = 1, int VEC = 1, int PERS = 0>
-__global__ void __launch_bounds__(NT, MINB)
-fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const int* __restrict__ mate,
-               const unsigned char* __restrict__ side, const TC* __restrict__ JG, const TC* __restrict__ detj,
-               const TC* __restrict__ nL, TC* __restrict__ VF, TC* __restrict__ ND, TC* __restrict__ DV,
-               long long E, Line<TC> L, PhysT<TC> ph, TC* __restrict__ GRAD, TC* __restrict__ BV)
+// The body serves element block blk0 (and, with PERS, blk0 + k bstride);
+// fr_grad_kernel runs it for blockIdx.x, merged batch launches for their
+// share of the grid.
+template <int DIM, int P, int EPB, int NT, typename TC, int LES = 0, int VEC = 1, int PERS = 0>
+__device__ __forceinline__ void
+fr_grad_body(long long blk0, long long bstride, const double* __restrict__ U, const TC* __restrict__ UF,
+             const int* __restrict__ mate, const unsigned char* __restrict__ side, const TC* __restrict__ JG,
+             const TC* __restrict__ detj, const TC* __restrict__ nL, TC* __restrict__ VF, TC* __restrict__ ND,
+             TC* __restrict__ DV, long long E, const Line<TC>& L, const PhysT<TC>& ph, TC* __restrict__ GRAD,
+             TC* __restrict__ BV)
 {
   using S = Shape<DIM, P>;
   constexpr bool ALIAS = grad_alias<DIM, P, EPB, NT, TC, LES, PERS>();
@@ -463,7 +467,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
   // --- inputs to shared memory: state, metrics, neighbour traces.  16-byte
   // copies where the per-element runs are whole 16-byte units (global bases
   // 16-byte aligned), element-sized otherwise.  With PERS = 1 a block walks
-  // over element blocks blockIdx.x, + gridDim.x, ...; the next block's state,
+  // over element blocks blk0, + bstride, ...; the next block's state,
   // metrics and neighbour traces are fetched into their regions as soon as
   // the current block no longer reads them (after the solution-point phase),
   // so the copies overlap the divergence and flux-point phases, and the left
@@ -526,7 +530,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
     }
   };
 
-  long long blk = blockIdx.x;
+  long long blk = blk0;
   int nval = (int)(E - blk * EPB < EPB ? E - blk * EPB : EPB);
   unsigned char psd[IF];
   {
@@ -698,7 +702,7 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
 
   // --- the next block's state, metrics and wiring (PERS), or the left
   // normals into the metric region, fetched while the divergence runs
-  const long long nb = blk + gridDim.x;
+  const long long nb = blk + bstride;
   const bool more = PERS && nb < nblk;
   const int nvn = more ? (int)(E - nb * EPB < EPB ? E - nb * EPB : EPB) : 0;
   int mtn[IF];
@@ -988,6 +992,17 @@ fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const in
 #undef FR_SN
 }
 
+template <int DIM, int P, int EPB, int NT, typename TC, int LES = 0, int MINB = 1, int VEC = 1, int PERS = 0>
+__global__ void __launch_bounds__(NT, MINB)
+fr_grad_kernel(const double* __restrict__ U, const TC* __restrict__ UF, const int* __restrict__ mate,
+               const unsigned char* __restrict__ side, const TC* __restrict__ JG, const TC* __restrict__ detj,
+               const TC* __restrict__ nL, TC* __restrict__ VF, TC* __restrict__ ND, TC* __restrict__ DV,
+               long long E, Line<TC> L, PhysT<TC> ph, TC* __restrict__ GRAD, TC* __restrict__ BV)
+{
+  fr_grad_body<DIM, P, EPB, NT, TC, LES, VEC, PERS>(blockIdx.x, gridDim.x, U, UF, mate, side, JG, detj, nL, VF, ND,
+                                                     DV, E, L, ph, GRAD, BV);
+}
+
 // Boundary point j of the interface kernel (flat own index bf[j], type
 // bt[j]), out of line so that the interior path keeps few registers.
 template <int DIM, int VISC, typename TC, int RIEMANN>
@@ -1050,17 +1065,18 @@ __device__ __noinline__ void face_boundary(PhysT<TC> ph, long long j, const TC* 
 // two states, convective_flux_boundary, src/inters.cpp:368-387; Roe in 2-D
 // with RIEMANN 2; the own flux for slip_wall_dual, right_flux,
 // src/inters.cpp:299-308), plus the viscous part BV from the gradient kernel.
-// Blocks of exactly 128 threads (one shared staging column per thread).
+// Blocks of exactly 128 threads (one shared staging column per thread); the
+// body serves block blk (fr_face_kernel: blockIdx.x; merged batch launches:
+// their share of the grid).
 template <int DIM, int VISC, typename TC, int RIEMANN = 0>
-__global__ void __launch_bounds__(128)
-fr_face_kernel(const int2* __restrict__ face, const unsigned char* __restrict__ fsign, long long nint,
-               const TC* __restrict__ UF, const TC* __restrict__ VF, const TC* __restrict__ nL,
-               const TC* __restrict__ tdA, TC* __restrict__ CF, long long NFE, PhysT<TC> ph,
-               long long nbdy = 0, const int* __restrict__ bf = nullptr, const unsigned char* __restrict__ bt = nullptr,
-               const TC* __restrict__ BV = nullptr)
+__device__ __forceinline__ void
+fr_face_body(long long blk, const int2* __restrict__ face, const unsigned char* __restrict__ fsign, long long nint,
+             const TC* __restrict__ UF, const TC* __restrict__ VF, const TC* __restrict__ nL,
+             const TC* __restrict__ tdA, TC* __restrict__ CF, long long NFE, const PhysT<TC>& ph, long long nbdy,
+             const int* __restrict__ bf, const unsigned char* __restrict__ bt, const TC* __restrict__ BV)
 {
   constexpr int F = DIM + 2, D = DIM;
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long i = blk * 128 + threadIdx.x;
   if (i >= nint) {
     if (i - nint < nbdy) face_boundary<DIM, VISC, TC, RIEMANN>(ph, i - nint, UF, nL, tdA, CF, NFE, bf, bt, BV);
     return;
@@ -1125,6 +1141,17 @@ fr_face_kernel(const int2* __restrict__ face, const unsigned char* __restrict__ 
   for (int k = 0; k < F; k++) { CF[a + NFE * k] = cl[k]; CF[b + NFE * k] = cr[k]; }
 }
 
+template <int DIM, int VISC, typename TC, int RIEMANN = 0>
+__global__ void __launch_bounds__(128)
+fr_face_kernel(const int2* __restrict__ face, const unsigned char* __restrict__ fsign, long long nint,
+               const TC* __restrict__ UF, const TC* __restrict__ VF, const TC* __restrict__ nL,
+               const TC* __restrict__ tdA, TC* __restrict__ CF, long long NFE, PhysT<TC> ph,
+               long long nbdy = 0, const int* __restrict__ bf = nullptr, const unsigned char* __restrict__ bt = nullptr,
+               const TC* __restrict__ BV = nullptr)
+{
+  fr_face_body<DIM, VISC, TC, RIEMANN>(blockIdx.x, face, fsign, nint, UF, VF, nL, tdA, CF, NFE, ph, nbdy, bf, bt, BV);
+}
+
 // ---------------------------------------------------------------------------
 // Stage, last part (per element): norm_tconf - norm_tdisf, the VCJH
 // correction (calculate_corrected_divergence, src/eles.cpp:1594-1661), and
@@ -1171,12 +1198,15 @@ __host__ __device__ constexpr size_t update_smem_bytes()
 // where the element runs allow, VEC = 1; element-sized with VEC = 0 for
 // inputs only 8-byte aligned), so all of a block's loads are in flight
 // together.
+// The body serves element block blk (fr_update_kernel: blockIdx.x; merged
+// batch launches: their share of the grid).
 template <int DIM, int P, int EPB, int NT, int VISC, int MODE, typename TC, int VEC = 1>
-__global__ void __launch_bounds__(NT)
-fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restrict__ UFn, const TC* __restrict__ CF,
-                 const TC* __restrict__ ND, const TC* __restrict__ DV, const TC* __restrict__ JG,
-                 const double* __restrict__ detj, double* __restrict__ DIV, double* __restrict__ partial, long long E,
-                 Line<TC> L, PhysT<TC> ph, double rk_a, double rk_b, double dt, int first_stage)
+__device__ __forceinline__ void
+fr_update_body(long long blk, double* __restrict__ U, double* __restrict__ REG, TC* __restrict__ UFn,
+               const TC* __restrict__ CF, const TC* __restrict__ ND, const TC* __restrict__ DV,
+               const TC* __restrict__ JG, const double* __restrict__ detj, double* __restrict__ DIV,
+               double* __restrict__ partial, long long E, const Line<TC>& L, const PhysT<TC>& ph, double rk_a,
+               double rk_b, double dt, int first_stage)
 {
   using S = Shape<DIM, P>;
   using Q = UpdPlan<DIM, P, EPB, NT, VISC, MODE, TC>;
@@ -1194,7 +1224,7 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
   auto sJ = reinterpret_cast<TC (*)[DD * NU]>(sm0 + Q::oJ);
   auto sRed = reinterpret_cast<double (*)[F]>(sm0 + Q::oRED);
   fill_blockops<DIM, P, TC, NF>(B, L, threadIdx.x, NT);
-  const long long e0 = (long long)blockIdx.x * EPB;
+  const long long e0 = blk * EPB;
   const int nval = (int)(E - e0 < EPB ? E - e0 : EPB);
 
   // --- inputs to shared memory
@@ -1352,7 +1382,7 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
     if (partial && threadIdx.x < F) {
       double v = 0.0;
       for (int i = 0; i < NT / 32; i++) v += sRed[i][threadIdx.x];
-      partial[(size_t)blockIdx.x * F + threadIdx.x] = v;
+      partial[(size_t)blk * F + threadIdx.x] = v;
     }
     // traces of the updated state for the next stage
     for (int w = threadIdx.x; w < nval * NF; w += NT) {
@@ -1376,6 +1406,17 @@ fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restric
       }
     }
   }
+}
+
+template <int DIM, int P, int EPB, int NT, int VISC, int MODE, typename TC, int VEC = 1>
+__global__ void __launch_bounds__(NT)
+fr_update_kernel(double* __restrict__ U, double* __restrict__ REG, TC* __restrict__ UFn, const TC* __restrict__ CF,
+                 const TC* __restrict__ ND, const TC* __restrict__ DV, const TC* __restrict__ JG,
+                 const double* __restrict__ detj, double* __restrict__ DIV, double* __restrict__ partial, long long E,
+                 Line<TC> L, PhysT<TC> ph, double rk_a, double rk_b, double dt, int first_stage)
+{
+  fr_update_body<DIM, P, EPB, NT, VISC, MODE, TC, VEC>(blockIdx.x, U, REG, UFn, CF, ND, DV, JG, detj, DIV, partial, E,
+                                                       L, ph, rk_a, rk_b, dt, first_stage);
 }
 
 // Block partial sums -> norms: one CTA of 256 threads per field; thread t

@@ -7,7 +7,7 @@
 
 #include <cuda_runtime.h>
 
-#include "fr_face_update.cuh"
+#include "fr_batch_merged.cuh"
 #include "fr_fused.cuh"
 #include "fr_host.hpp"
 
@@ -60,6 +60,15 @@ struct Runner {
   virtual void select(int g, int u) = 0;
   virtual int grad_sel() const = 0;
   virtual int update_sel() const = 0;
+  // This group's slot of the merged batch launches (fr_batch_merged.cuh):
+  // fills *grad, *face and *upd (MergedGrad / MergedFace / MergedUpd of the
+  // runner's precision) for stage `stage` and returns the order, or 0 if the
+  // group cannot join them.
+  virtual int merged_args(const Bufs& b, int cur, int stage, double dt, void* grad, void* face, void* upd) const
+  {
+    (void)b; (void)cur; (void)stage; (void)dt; (void)grad; (void)face; (void)upd;
+    return 0;
+  }
 };
 
 // Compiled tile variants (elements per CTA, threads per CTA) of the gradient
@@ -239,6 +248,33 @@ struct RunnerT : Runner {
         b.U, b.REG, (TC*)b.UF[cur ^ 1], (const TC*)b.UF[cur], b.mate, b.side, (const TC*)b.VF, (const TC*)b.ND,
         (const TC*)b.DV, (const TC*)b.JG, (const TC*)b.nL, (const TC*)b.tdA, b.idetj, (const TC*)b.BV, b.DIV,
         want_partial ? b.partial : nullptr, E, L, ph, kRK4A[stage], kRK4B[stage], dt, stage == 0 ? 1 : 0, b.err);
+  }
+  int merged_args(const Bufs& b, int cur, int stage, double dt, void* gv, void* fv, void* uv) const override
+  {
+    if constexpr (DIM == 3 && P >= 2 && P <= 4) {
+      if (!visc || les || riemann != 0) return 0;
+      constexpr int EPB = MergedTile<P>::epb;
+      const long long nblk = (E + EPB - 1) / EPB;
+      *static_cast<MergedGrad<TC>*>(gv) =
+          MergedGrad<TC>{b.U, (const TC*)b.UF[cur], b.mate, b.side, (const TC*)b.JG, (const TC*)b.detj,
+                         (const TC*)b.nL, (TC*)b.VF, (TC*)b.ND, (TC*)b.DV, (TC*)b.BV, E, nblk, L, ph};
+      MergedFace<TC> f{};
+      if constexpr (!merged_fused<P, TC>()) {
+        const long long n = b.nint + b.nbdy;
+        f = MergedFace<TC>{b.face, b.fsign, b.nint, (const TC*)b.UF[cur], (const TC*)b.VF, (const TC*)b.nL,
+                           (const TC*)b.tdA, (TC*)b.CF, E * S::NF, b.nbdy, b.bf, b.bt, (const TC*)b.BV,
+                           (n + 127) / 128, ph};
+      }
+      *static_cast<MergedFace<TC>*>(fv) = f;
+      *static_cast<MergedUpd<TC>*>(uv) =
+          MergedUpd<TC>{b.U, b.REG, (TC*)b.UF[cur ^ 1], (const TC*)b.UF[cur], (const TC*)b.CF, b.mate, b.side,
+                        (const TC*)b.VF, (const TC*)b.ND, (const TC*)b.DV, (const TC*)b.JG, (const TC*)b.nL,
+                        (const TC*)b.tdA, b.detj64, b.idetj, (const TC*)b.BV, b.DIV, b.err, E, nblk, L, ph,
+                        kRK4A[stage], kRK4B[stage], dt, stage == 0 ? 1 : 0};
+      return P;
+    }
+    (void)b; (void)cur; (void)stage; (void)dt; (void)gv; (void)fv; (void)uv;
+    return 0;
   }
   void update(const Bufs& b, int cur, int mode, int stage, double dt, bool want_partial, cudaStream_t s) override
   {

@@ -1030,7 +1030,52 @@ struct fr_batch {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   double graph_dt[2] = {0, 0};
   long long launches = 0;
+  int merged = 0;                         // 1: one launch per stage kernel for all groups
+  int merged_minb = 4;                    // CTAs per SM the merged kernels' registers are capped for
 };
+
+namespace {
+
+// One stage of every group as merged launches (fr_batch_merged.cuh).
+template <typename TC>
+fr_status merged_stage_t(fr_batch* b, int k, double dt, cudaStream_t st)
+{
+  MergedGrads<TC> G{};
+  MergedFaces<TC> Fc{};
+  MergedUpds<TC> U{};
+  bool any_face = false;
+  for (fr_solver* s : b->groups) {
+    MergedGrad<TC> g{};
+    MergedFace<TC> f{};
+    MergedUpd<TC> u{};
+    int P = s->run->merged_args(s->b, s->cur, k, dt, &g, &f, &u);
+    if (P < 2 || P > 4) return fail(FR_ERR_UNSUPPORTED, "a group cannot join the merged launches");
+    G.s[P - 2] = g;
+    Fc.s[P - 2] = f;
+    U.s[P - 2] = u;
+    any_face = any_face || f.nblk > 0;
+  }
+  fr_status r = merged_stage_launch(sizeof(TC) == 4, &G, &Fc, any_face, &U, b->merged_minb, st);
+  for (fr_solver* s : b->groups) s->cur ^= 1;
+  return r;
+}
+
+// Groups that can run merged: hexahedra of orders 2-4, at most one group per
+// order, all viscous without LES, Rusanov, one precision.
+bool batch_mergeable(const fr_batch* b, std::string& why)
+{
+  int seen[5] = {0, 0, 0, 0, 0};
+  for (const fr_solver* s : b->groups) {
+    const fr_scheme_desc& d = s->sch;
+    if (s->mesh.dims != 3 || d.order < 2 || d.order > 4) { why = "merged launches take hexahedra of orders 2-4"; return false; }
+    if (seen[d.order]++) { why = "merged launches take one group per order"; return false; }
+    if (!d.viscous || d.les || d.riemann != 0) { why = "merged launches take viscous Rusanov groups without LES"; return false; }
+    if (d.precision != b->groups[0]->sch.precision) { why = "merged launches take one precision"; return false; }
+  }
+  return true;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -1165,8 +1210,76 @@ fr_status fr_batch_autotune(fr_batch* b, int reps)
   }
   for (int i = 0; i < 2; i++)
     if (b->graph[i]) { cudaGraphExecDestroy(b->graph[i]); b->graph[i] = nullptr; }
+  // per-group graph against merged launches (two register caps): time `reps`
+  // whole steps of each from the same state, restore the state after each
+  std::string why;
+  b->merged = 0;
+  if (!batch_mergeable(b, why)) return FR_OK;
+  FR_CUDA(cudaSetDevice(b->device));
+  std::vector<double*> saved(b->groups.size(), nullptr);
+  fr_status r = FR_OK;
+  for (size_t g = 0; g < b->groups.size() && r == FR_OK; g++) {
+    fr_solver* s = b->groups[g];
+    size_t bytes = sizeof(double) * (size_t)s->mesh.nu * s->mesh.ne * s->mesh.nfields;
+    if (cudaMalloc(&saved[g], bytes) != cudaSuccess) { saved[g] = nullptr; r = fail(FR_ERR_CUDA, "autotune state copy"); break; }
+    if (cudaMemcpyAsync(saved[g], s->b.U, bytes, cudaMemcpyDeviceToDevice, b->stream) != cudaSuccess)
+      r = fail(FR_ERR_CUDA, "autotune state copy");
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  double best = 1e30;
+  int best_mode = 0, best_minb = 4;
+  const int modes[3][2] = {{0, 4}, {1, 4}, {1, 3}};
+  if (r == FR_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+    r = fail(FR_ERR_CUDA, "autotune events");
+  for (int m = 0; m < 3 && r == FR_OK; m++) {
+    b->merged = modes[m][0];
+    b->merged_minb = modes[m][1];
+    for (int i = 0; i < 2; i++)
+      if (b->graph[i]) { cudaGraphExecDestroy(b->graph[i]); b->graph[i] = nullptr; }
+    const double dt = 1e-5;
+    r = fr_batch_advance(b, 2, dt, b->stream);                   // capture both graphs, warm up
+    if (r == FR_OK) cudaEventRecord(e0, b->stream);
+    if (r == FR_OK) r = fr_batch_advance(b, reps, dt, b->stream);
+    if (r == FR_OK) cudaEventRecord(e1, b->stream);
+    if (r == FR_OK && cudaEventSynchronize(e1) != cudaSuccess) r = fail(FR_ERR_CUDA, "autotune timing");
+    float ms = 0.f;
+    if (r == FR_OK) cudaEventElapsedTime(&ms, e0, e1);
+    if (r == FR_OK && ms < best) { best = ms; best_mode = modes[m][0]; best_minb = modes[m][1]; }
+    // back to the saved state (traces rebuilt from it)
+    for (size_t g = 0; g < b->groups.size() && r == FR_OK; g++) {
+      fr_solver* s = b->groups[g];
+      size_t bytes = sizeof(double) * (size_t)s->mesh.nu * s->mesh.ne * s->mesh.nfields;
+      if (cudaMemcpyAsync(s->b.U, saved[g], bytes, cudaMemcpyDeviceToDevice, b->stream) != cudaSuccess)
+        r = fail(FR_ERR_CUDA, "autotune state restore");
+      if (r == FR_OK) r = fr_solver_state_updated(s, b->stream);
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaStreamSynchronize(b->stream);
+  for (double* p : saved)
+    if (p) cudaFree(p);
+  b->merged = r == FR_OK ? best_mode : 0;
+  b->merged_minb = best_minb;
+  for (int i = 0; i < 2; i++)
+    if (b->graph[i]) { cudaGraphExecDestroy(b->graph[i]); b->graph[i] = nullptr; }
+  return r;
+}
+
+fr_status fr_batch_set_merged(fr_batch* b, int on, int minb)
+{
+  if (!b) return fail(FR_ERR_ARG, "null batch");
+  std::string why;
+  if (on && !batch_mergeable(b, why)) return fail(FR_ERR_UNSUPPORTED, why);
+  if (on && minb != 1 && minb != 3 && minb != 4) return fail(FR_ERR_ARG, "minb must be 1, 3 or 4");
+  b->merged = on ? 1 : 0;
+  if (on) b->merged_minb = minb;
+  for (int i = 0; i < 2; i++)
+    if (b->graph[i]) { cudaGraphExecDestroy(b->graph[i]); b->graph[i] = nullptr; }
   return FR_OK;
 }
+
+int fr_batch_merged(const fr_batch* b) { return b && b->merged ? b->merged_minb : 0; }
 
 fr_status fr_batch_advance(fr_batch* b, int n_steps, double dt, void* stream)
 {
@@ -1184,21 +1297,34 @@ fr_status fr_batch_advance(fr_batch* b, int n_steps, double dt, void* stream)
   for (fr_solver* s : b->groups)
     if (s->cur != c0) return fail(FR_ERR_ARG, "groups out of step");
   long long per_step = 0;
-  for (fr_solver* s : b->groups) per_step += 5 * s->run->launches_per_stage();
+  if (b->merged) {
+    bool any_face = false;
+    for (fr_solver* s : b->groups) any_face = any_face || s->run->launches_per_stage() == 3;
+    per_step = 5 * (any_face ? 3 : 2);
+  } else {
+    for (fr_solver* s : b->groups) per_step += 5 * s->run->launches_per_stage();
+  }
   for (int i = 0; i < n_steps; i++) {
     const int c = b->groups[0]->cur;
     if (!b->graph[c] || b->graph_dt[c] != dt) {
       if (b->graph[c]) { cudaGraphExecDestroy(b->graph[c]); b->graph[c] = nullptr; }
       cudaGraph_t gr;
       FR_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-      for (int k = 0; k < 5; k++)
+      fr_status cr = FR_OK;
+      for (int k = 0; k < 5 && cr == FR_OK; k++) {
+        if (b->merged) {
+          cr = b->groups[0]->sch.precision == 1 ? merged_stage_t<float>(b, k, dt, st) : merged_stage_t<double>(b, k, dt, st);
+          continue;
+        }
         for (fr_solver* s : b->groups) {
           long long l0 = s->launches;
           stage(s, k, dt, k == 4, st);
           s->launches = l0;
         }
+      }
       for (fr_solver* s : b->groups) s->cur = c;
       FR_CUDA(cudaStreamEndCapture(st, &gr));
+      if (cr) { cudaGraphDestroy(gr); return cr; }
       cudaError_t e = cudaGraphInstantiate(&b->graph[c], gr, 0);
       cudaGraphDestroy(gr);
       if (e != cudaSuccess) return fail(FR_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));

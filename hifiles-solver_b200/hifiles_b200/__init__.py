@@ -120,6 +120,8 @@ def lib():
         "fr_batch_set_state": (C.c_int, [vp, C.c_int, dp]),
         "fr_batch_get_state": (C.c_int, [vp, C.c_int, dp]),
         "fr_batch_autotune": (C.c_int, [vp, C.c_int]),
+        "fr_batch_set_merged": (C.c_int, [vp, C.c_int, C.c_int]),
+        "fr_batch_merged": (C.c_int, [vp]),
         "fr_batch_advance": (C.c_int, [vp, C.c_int, C.c_double, vp]),
         "fr_batch_launch_count": (C.c_longlong, [vp]),
         "fr_batch_stream": (vp, [vp]),
@@ -614,7 +616,17 @@ class Batch:
         return u
 
     def autotune(self, reps=3):
+        """Tiles per group, then per-group launches against merged launches (fr_batch_autotune)."""
         _check(lib().fr_batch_autotune(self.h, int(reps)))
+
+    def set_merged(self, on, minb=4):
+        """One launch per stage kernel for all groups (hex NS groups of orders 2-4; fr_batch_set_merged)."""
+        _check(lib().fr_batch_set_merged(self.h, int(bool(on)), int(minb)))
+
+    @property
+    def merged(self):
+        """Register cap (CTAs per SM) of the merged launches in use, 0 when the groups launch one by one."""
+        return int(lib().fr_batch_merged(self.h))
 
     def advance(self, n_steps, dt, stream=None):
         _check(lib().fr_batch_advance(self.h, int(n_steps), float(dt), stream))

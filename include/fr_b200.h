@@ -244,7 +244,21 @@ fr_status fr_batch_instance(const fr_batch* b, int i, int out4[4]);
  * it zeroes its RK register. */
 fr_status fr_batch_set_state(fr_batch* b, int i, const double* host_u);
 fr_status fr_batch_get_state(fr_batch* b, int i, double* host_u);
+/* Picks every group's tiles (fr_solver_autotune), then times `reps` whole
+ * steps run group by group against the merged launches below (registers
+ * capped for 4 and for 3 CTAs per SM) from the same state, keeps the fastest
+ * and restores the state. */
 fr_status fr_batch_autotune(fr_batch* b, int reps);
+/* Merged launches: each stage kernel (gradient, interface flux where an order
+ * needs it, update) runs once for all groups, its grid the groups' element
+ * blocks one after the other, each block running its group's order.  For
+ * batches of hexahedral Navier-Stokes groups (Rusanov, no LES, one precision)
+ * of orders 2, 3 and 4, at most one group per order; FR_ERR_UNSUPPORTED
+ * otherwise.  on 0 returns to one launch per group and stage kernel; minb
+ * (1, 3 or 4) caps the merged kernels' registers for that many CTAs per SM.
+ * fr_batch_merged returns the cap in use, 0 when not merged. */
+fr_status fr_batch_set_merged(fr_batch* b, int on, int minb);
+int fr_batch_merged(const fr_batch* b);
 fr_status fr_batch_advance(fr_batch* b, int n_steps, double dt, void* stream);
 long long fr_batch_launch_count(const fr_batch* b);
 void* fr_batch_stream(fr_batch* b);

@@ -62,3 +62,46 @@ def test_batch_errors():
     bad = np.full(b.shapes[0], np.nan, order="F")
     with pytest.raises(H.FrError):
         b.set_state(0, bad)
+
+
+# hexahedral Navier-Stokes groups of orders 2, 3 and 4 (periodic and walled):
+# the merged launches run each stage kernel once for all three groups
+MERGEABLE = [
+    dict(dims=3, order=2, n=(3, 2, 2), jitter=0.1, seed=5, **TGV, **NS),
+    dict(dims=3, order=3, n=(3, 3, 2), **TGV, **NS),
+    dict(dims=3, order=3, n=(2, 2, 2), side_bc=(0, 0, 12, 12, 0, 0), **TGV, **NS),
+    dict(dims=3, order=4, n=(2, 2, 3), **TGV, **NS),
+    dict(dims=3, order=2, n=(2, 3, 2), side_bc=(0, 0, 12, 12, 0, 0), **TGV, **NS),
+]
+
+
+@pytest.mark.parametrize("precision,minb", [(0, 4), (0, 3), (0, 1), (1, 4)])
+def test_merged_launches_equal_per_group_launches(precision, minb):
+    insts = [dict(inst, precision=precision) for inst in MERGEABLE]
+    grouped, merged = H.Batch(insts), H.Batch(insts)
+    for b in (grouped, merged):
+        for i, inst in enumerate(insts):
+            kw = dict(inst)
+            s = H.Solver.box(kw.pop("dims"), kw.pop("order"), kw.pop("n"), kw.pop("lo"), kw.pop("hi"), **kw)
+            b.set_state(i, _state(inst, s))
+            s.close()
+    merged.set_merged(True, minb)
+    assert merged.merged == minb and grouped.merged == 0
+    l0 = merged.launch_count()
+    grouped.advance(3, 1e-3)
+    merged.advance(3, 1e-3)
+    # gradient, interface flux (orders 2 and 4), update: three launches per stage for all groups
+    assert merged.launch_count() - l0 == 3 * 5 * 3
+    for i in range(len(insts)):
+        u = grouped.get_state(i)
+        assert np.isfinite(u).all(), i
+        assert np.array_equal(merged.get_state(i), u), i
+
+
+def test_merged_launches_refuse_other_batches():
+    b = H.Batch(INSTANCES)
+    with pytest.raises(H.FrError):
+        b.set_merged(True)
+    b.autotune(1)
+    assert b.merged == 0
+

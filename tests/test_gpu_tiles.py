@@ -47,3 +47,25 @@ def test_every_tile_variant_gives_identical_states(precision):
             assert np.array_equal(st, ref), ("gradient", s.tile_info(0, g), "update", s.tile_info(1, u))
     with pytest.raises(H.FrError):
         s.select_tiles(ng, 0)
+
+
+@pytest.mark.parametrize("case", ["hex_channel_p2", "hex_channel_char_p3"])
+def test_every_tile_variant_matches_the_reference_on_walled_meshes(case):
+    """The reference's walled channels (isothermal, adiabatic, slip and
+    characteristic boundaries): every tile variant ends where the reference
+    ends, so the boundary branches hold for every block shape."""
+    from golden_util import load, rel
+    meta, a = load(case)
+    s = H.Solver.box(meta["dims"], meta["order"], meta["n"], meta["lo"], meta["hi"], jitter=meta["jitter"],
+                     seed=meta["seed"], viscous=bool(meta["viscous"]), vcjh_scheme=meta["vcjh"],
+                     side_bc=meta.get("side_bc"), **meta["physics"])
+    ng, nu = s.tile_count()
+    bad = []
+    for g, u in [(g, 0) for g in range(ng)] + [(0, u) for u in range(1, nu)]:
+        s.set_state(a["u0"])
+        s.select_tiles(g, u)
+        s.advance(meta["steps"], meta["dt"])
+        r = rel(s.get_state(), a["uN"])
+        if not r <= 1e-12:
+            bad.append((s.tile_info(0, g), s.tile_info(1, u), r))
+    assert not bad, bad
