@@ -18,6 +18,7 @@ extern thread_local std::string g_err;
 fr_status gemm_bf16x3(int m, int k, long long ncols, const double* A, const double* B, double* C, int beta,
                       cudaStream_t s, int terms);
 fr_status gemm_bf16x3_check(cudaStream_t s);
+void gemm_set_prefetch(int on);
 }
 using namespace frb;
 
@@ -650,6 +651,12 @@ fr_status fr_op_set_gemm_precision(int mode)
 }
 
 int fr_op_gemm_precision(void) { return g_gemm_mode; }
+
+fr_status fr_op_set_gemm_pipelining(int on)
+{
+  gemm_set_prefetch(on);
+  return FR_OK;
+}
 
 fr_status fr_op_check(void* stream)
 {

@@ -172,7 +172,13 @@ __device__ __forceinline__ uint32_t chunk_off(int row, int kc, int R)
   return (uint32_t)((kc * (R / 8) + row / 8) * 128 + (row % 8) * 16);
 }
 
-template <int TERMS, int MT, int TN>
+// PF > 0: software-pipelined B.  Each thread holds the raw FP64 chunks it
+// splits for the next column tile in registers (at most PF chunks of 8
+// values: TN * KP / 8 <= PF * kThreads), loaded right after the current
+// tile's split, so the loads of tile t + 1 are in flight while tile t's MMAs
+// run and its accumulators are read back.  The arithmetic is the same as with
+// PF = 0 (B read at the split), so both give identical results.
+template <int TERMS, int MT, int TN, int PF = 0>
 __global__ void __launch_bounds__(kThreads)
 fr_gemm_bf16x3_kernel(int m, int k, int KP, long long ncols, const double* __restrict__ A,
                       const double* __restrict__ B, double* __restrict__ C, int beta, int* __restrict__ err)
@@ -228,24 +234,70 @@ fr_gemm_bf16x3_kernel(int m, int k, int KP, long long ncols, const double* __res
   bool drained = true;                     // no MMA of this block may still be running
   const long long ntiles = (ncols + TN - 1) / TN;
   uint32_t parity = 0;
-  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const long long j0 = t * TN;
-    for (int n = tid; n < TN; n += kThreads) cB[n] = j0 + n < ncols ? __ldg(B + (size_t)(j0 + n) * k) : 0.0;
-    __syncthreads();
-    // B' for columns j0 ..: columns n (fastest) x chunks c, less the column's first entry
-    for (int w = tid; w < TN * KC; w += kThreads) {
-      const int n = w % TN, c = w / TN;
-      const long long j = j0 + n;
-      double x[8];
+  constexpr int PFW = PF > 0 ? PF : 1;
+  double xn[PFW][8];                       // PF: the next tile's raw chunks (w = tid + q kThreads)
+  auto load_next = [&](long long tt) {
+    const long long jn = tt * TN;
+#pragma unroll
+    for (int q = 0; q < PFW; q++) {
+      const int w = tid + q * kThreads, n = w % TN, c = w / TN;
+      const long long j = jn + n;
 #pragma unroll
       for (int i = 0; i < 8; i++) {
         const int kk = 8 * c + i;
-        x[i] = (j < ncols && kk < k) ? __ldg(B + (size_t)j * k + kk) - cB[n] : 0.0;
+        xn[q][i] = (w < TN * KC && j < ncols && kk < k) ? __ldg(B + (size_t)j * k + kk) : 0.0;
       }
-      uint4 q[3];
-      split8(x, q);
+    }
+  };
+  if (PF > 0 && blockIdx.x < ntiles) load_next(blockIdx.x);
+  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const long long j0 = t * TN;
+    if constexpr (PF > 0) {
+      // the column levels: the thread holding chunk 0 of column n
 #pragma unroll
-      for (int pp = 0; pp < NP; pp++) *reinterpret_cast<uint4*>(sB + pp * partB + chunk_off(n, c, TN)) = q[pp];
+      for (int q = 0; q < PFW; q++) {
+        const int w = tid + q * kThreads;
+        if (w < TN) cB[w] = j0 + w < ncols ? xn[q][0] : 0.0;
+      }
+    } else {
+      for (int n = tid; n < TN; n += kThreads) cB[n] = j0 + n < ncols ? __ldg(B + (size_t)(j0 + n) * k) : 0.0;
+    }
+    __syncthreads();
+    // B' for columns j0 ..: columns n (fastest) x chunks c, less the column's first entry
+    if constexpr (PF > 0) {
+#pragma unroll
+      for (int q = 0; q < PFW; q++) {
+        const int w = tid + q * kThreads, n = w % TN, c = w / TN;
+        if (w >= TN * KC) continue;
+        const long long j = j0 + n;
+        double x[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          const int kk = 8 * c + i;
+          x[i] = (j < ncols && kk < k) ? xn[q][i] - cB[n] : 0.0;
+        }
+        uint4 qq[3];
+        split8(x, qq);
+#pragma unroll
+        for (int pp = 0; pp < NP; pp++) *reinterpret_cast<uint4*>(sB + pp * partB + chunk_off(n, c, TN)) = qq[pp];
+      }
+      // the next tile's loads stay in flight through this tile's MMAs and read-back
+      if (t + gridDim.x < ntiles) load_next(t + gridDim.x);
+    } else {
+      for (int w = tid; w < TN * KC; w += kThreads) {
+        const int n = w % TN, c = w / TN;
+        const long long j = j0 + n;
+        double x[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          const int kk = 8 * c + i;
+          x[i] = (j < ncols && kk < k) ? __ldg(B + (size_t)j * k + kk) - cB[n] : 0.0;
+        }
+        uint4 q[3];
+        split8(x, q);
+#pragma unroll
+        for (int pp = 0; pp < NP; pp++) *reinterpret_cast<uint4*>(sB + pp * partB + chunk_off(n, c, TN)) = q[pp];
+      }
     }
     // generic-proxy writes -> visible to the tensor cores' reads
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -348,6 +400,12 @@ static size_t gemm_split_smem(int k, int terms, int mt, int tn)
   return (size_t)(mt * kTM + tn) * n_parts(terms) * KP * 2;
 }
 
+// chunks of 8 B values a thread holds for the next column tile (software
+// pipelining; 0 turns it off); the pipelined form can be switched off for
+// comparisons (fr_tc_gemm_set_prefetch)
+constexpr int kPrefetchChunks = 4;
+int g_gemm_prefetch = 1;
+
 // dynamic shared memory a block may use (227 kB less the static part: the
 // barrier, the TMEM slot, the row sums and the column shifts, under 3 kB)
 static constexpr size_t kSmemMax = 232448 - 3072;
@@ -367,12 +425,12 @@ bool gemm_split_supported(int m, int k, int terms)
   return m >= 1 && mt > 0;
 }
 
-template <int TERMS, int MT, int TN>
+template <int TERMS, int MT, int TN, int PF>
 static fr_status launch_split(int m, int k, long long ncols, const double* A, const double* B, double* C, int beta,
                               cudaStream_t s)
 {
   const size_t smem = gemm_split_smem(k, TERMS, MT, TN);
-  const void* kfn = (const void*)fr_gemm_bf16x3_kernel<TERMS, MT, TN>;
+  const void* kfn = (const void*)fr_gemm_bf16x3_kernel<TERMS, MT, TN, PF>;
   cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) {
     g_err = cudaGetErrorString(e);
@@ -396,8 +454,8 @@ static fr_status launch_split(int m, int k, long long ncols, const double* A, co
   const long long ntiles = (ncols + TN - 1) / TN;
   long long grid = (long long)(per > 0 ? per : 1) * (sms > 0 ? sms : 1);
   if (grid > ntiles) grid = ntiles;
-  fr_gemm_bf16x3_kernel<TERMS, MT, TN><<<(unsigned)grid, kThreads, smem, s>>>(m, k, (k + 15) / 16 * 16, ncols, A, B,
-                                                                              C, beta, err);
+  fr_gemm_bf16x3_kernel<TERMS, MT, TN, PF><<<(unsigned)grid, kThreads, smem, s>>>(m, k, (k + 15) / 16 * 16, ncols, A,
+                                                                                  B, C, beta, err);
   e = cudaGetLastError();
   if (e != cudaSuccess) {
     g_err = std::string("fr_gemm_bf16x3_kernel: ") + cudaGetErrorString(e);
@@ -421,15 +479,28 @@ fr_status gemm_bf16x3(int m, int k, long long ncols, const double* A, const doub
     return FR_ERR_UNSUPPORTED;
   }
   if (ncols == 0) return FR_OK;
-  if (terms == 3)
-    return mt == 1 ? launch_split<3, 1, 64>(m, k, ncols, A, B, C, beta, s)
-                   : launch_split<3, 2, 32>(m, k, ncols, A, B, C, beta, s);
-  return mt == 1 ? launch_split<6, 1, 64>(m, k, ncols, A, B, C, beta, s)
-                 : launch_split<6, 2, 32>(m, k, ncols, A, B, C, beta, s);
+  // software-pipelined B when a thread's share of the column tile fits its
+  // registers (kPrefetchChunks chunks of 8 values)
+  const int kp = (k + 15) / 16 * 16;
+  // (measured: 2 % faster for BF16x3, 6 % slower for BF16x6, whose six MMA
+  // copies already overlap the loads of the other blocks)
+  const bool pf = terms == 3 && (long long)tn * (kp / 8) <= (long long)kPrefetchChunks * kThreads && g_gemm_prefetch;
+  if (terms == 3) {
+    if (mt == 1) return pf ? launch_split<3, 1, 64, kPrefetchChunks>(m, k, ncols, A, B, C, beta, s)
+                           : launch_split<3, 1, 64, 0>(m, k, ncols, A, B, C, beta, s);
+    return pf ? launch_split<3, 2, 32, kPrefetchChunks>(m, k, ncols, A, B, C, beta, s)
+              : launch_split<3, 2, 32, 0>(m, k, ncols, A, B, C, beta, s);
+  }
+  if (mt == 1) return pf ? launch_split<6, 1, 64, kPrefetchChunks>(m, k, ncols, A, B, C, beta, s)
+                         : launch_split<6, 1, 64, 0>(m, k, ncols, A, B, C, beta, s);
+  return pf ? launch_split<6, 2, 32, kPrefetchChunks>(m, k, ncols, A, B, C, beta, s)
+            : launch_split<6, 2, 32, 0>(m, k, ncols, A, B, C, beta, s);
 }
 
 // FR_ERR_TIMEOUT if a tensor-core product gave up waiting for its MMAs since
 // the last check (the flag is cleared); synchronises the stream.
+void gemm_set_prefetch(int on) { g_gemm_prefetch = on ? 1 : 0; }
+
 fr_status gemm_bf16x3_check(cudaStream_t s)
 {
   int dev = 0;

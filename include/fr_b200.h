@@ -534,6 +534,11 @@ fr_status fr_op_advance_rk45(int n_upts, int n_fields, int n_eles, int stage, do
  * MMAs since the last check. */
 fr_status fr_op_set_gemm_precision(int mode);
 int fr_op_gemm_precision(void);
+/* Tensor-core BF16x3 products: on (default) loads each block's next column
+ * tile into registers while the current tile's MMAs run (operators of up to
+ * 64 columns with 64-column tiles, 128 with 32); off reads B at the split.
+ * Both give identical results; the switch is for comparisons. */
+fr_status fr_op_set_gemm_pipelining(int on);
 fr_status fr_op_check(void* stream);
 
 /* ------------------------------------------------------------------------

@@ -160,3 +160,25 @@ def test_operator_path_step_matches_fused_solver_and_bf16x3_error_is_small():
     op.advance(2, 1e-3, gemm_precision=2)
     err6 = np.linalg.norm(op.get_state() - u64) / np.linalg.norm(u64)
     assert err6 < 1e-7 and err6 < err / 10, (err6, err)
+
+
+@pytest.mark.parametrize("m,k,n", [(96, 64, 5 * 1000 + 3), (64, 64, 64 * 37 + 5), (150, 125, 5 * 200 + 7),
+                                   (96, 64, 5 * 32 ** 3)])
+@pytest.mark.parametrize("mode", [1, 2])
+def test_pipelined_b_tiles_give_identical_products(m, k, n, mode):
+    """The next column tile loaded into registers during the current tile's
+    MMAs (fr_op_set_gemm_pipelining) changes no value of the product."""
+    rng = np.random.default_rng(11 + m + k + n)
+    A = rng.standard_normal((m, k))
+    B = rng.standard_normal((k, n)) + 3.0
+    L = _lib()
+    L.fr_op_set_gemm_pipelining.argtypes = [C.c_int]
+    try:
+        assert L.fr_op_set_gemm_pipelining(0) == 0
+        plain = _product(L, A, B, mode)
+        assert L.fr_op_set_gemm_pipelining(1) == 0
+        piped = _product(L, A, B, mode)
+    finally:
+        L.fr_op_set_gemm_pipelining(1)
+    assert np.isfinite(piped).all()
+    assert np.array_equal(plain, piped)
