@@ -210,3 +210,52 @@ def test_own_setup_advances_like_the_reference(case):
     for t in M.types:
         got = mesh.get_state(t)
         assert rel(got, a["t%d_final_disu_upts0" % t]) <= 1e-12, (case, t)
+
+
+def test_mixed_setup_rejects_bad_input():
+    """Unmatched faces, inverted cells, unknown types and boundary codes are
+    reported through fr_status, never by exiting."""
+    import hifiles_b200 as H
+    xv, cells, period, bfaces = X.channel_mesh((3, 3, 2), jitter=0.0, seed=1)
+    opts = X.ElementOpts(vcjh_scheme_tet=2, vcjh_scheme_tri=1, vcjh_scheme_pri_1d=1)
+    # walls removed: the prisms' outer faces are left unmatched
+    with pytest.raises(H.FrError, match="unmatched"):
+        X.MixedMesh(2, xv, cells, period, [], opts)
+    # an inverted tet
+    bad = list(cells)
+    i = next(i for i, (t, _) in enumerate(bad) if t == X.TET)
+    t, vs = bad[i]
+    bad[i] = (t, [vs[0], vs[2], vs[1], vs[3]])
+    with pytest.raises(H.FrError, match="Jacobian"):
+        X.MixedMesh(2, xv, bad, period, bfaces, opts)
+    # unknown boundary type
+    with pytest.raises(H.FrError):
+        X.MixedMesh(2, xv, cells, period, [(bfaces[0][0], bfaces[0][1], 9)] + list(bfaces[1:]), opts)
+    # orders outside the simplex tables, schemes without constants
+    with pytest.raises(H.FrError):
+        X.element_operators(X.TET, 6)
+    with pytest.raises(H.FrError):
+        X.element_operators(X.TRI, 5, X.ElementOpts(vcjh_scheme_tri=2))
+    # mixing 2-D and 3-D cells
+    with pytest.raises(ValueError):
+        X.MixedMesh(2, xv, [(X.TRI, [0, 1, 2, 3])], period, [], opts)
+
+
+@pytest.mark.parametrize("ele_type,P", [(X.TRI, 1), (X.TRI, 4), (X.QUAD, 2), (X.TET, 1), (X.TET, 4), (X.PRISM, 1),
+                                        (X.PRISM, 5), (X.HEX, 2)])
+def test_element_operators_are_consistent(ele_type, P):
+    """Properties every FR element's operators have: the nodal basis is a
+    partition of unity (opp_0 rows sum to 1), derivatives of a constant vanish
+    (opp_2 rows sum to 0), and opp_1 / opp_5 are opp_0 / opp_3 times the
+    reference normals."""
+    ops = X.element_operators(ele_type, P, X.ElementOpts(vcjh_scheme_tet=1, vcjh_scheme_tri=1,
+                                                          vcjh_scheme_pri_1d=1))
+    D = ops["loc_upts"].shape[0]
+    assert np.allclose(ops["opp_0"].sum(axis=1), 1.0, atol=1e-12)
+    for d in range(D):
+        assert np.allclose(ops["opp_2"][d].sum(axis=1), 0.0, atol=1e-11)
+        assert np.allclose(ops["opp_1"][d], ops["opp_0"] * ops["tnorm_fpts"][d][:, None], atol=0, rtol=0)
+        assert np.allclose(ops["opp_5"][d], ops["opp_3"] * ops["tnorm_fpts"][d][None, :], atol=0, rtol=0)
+    # the nodal basis at the solution points is the identity
+    nu = ops["opp_0"].shape[1]
+    assert ops["opp_2"][0].shape == (nu, nu)
