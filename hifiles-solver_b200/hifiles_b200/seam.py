@@ -402,6 +402,129 @@ class MixedOperatorMesh:
         self._ok(L.fr_op_check(sp))
 
 
+class _MixedStageType(C.Structure):
+    _fields_ = [("n_upts", C.c_int), ("n_fpts", C.c_int), ("n_eles", C.c_longlong), ("opp_0", _VP),
+                ("opp_1", _VP * 3), ("opp_2", _VP * 3), ("opp_3", _VP), ("opp_4", _VP * 3), ("opp_5", _VP * 3),
+                ("opp_6", _VP), ("JGinv_upts", _VP), ("detjac_upts", _VP), ("tdA_fpts", _VP), ("norm_fpts", _VP),
+                ("disu_upts", _VP), ("div_tconf_upts", _VP)]
+
+
+def _bind_stage(L):
+    i, vp, ll = C.c_int, _VP, C.c_longlong
+    L.fr_mixed_stage_create.argtypes = [i, i, vp, i, vp, vp, vp, i, vp, vp, vp, vp, C.c_double, vp, vp]
+    L.fr_mixed_stage_destroy.argtypes = [vp]
+    L.fr_mixed_stage_residual.argtypes = [vp, vp]
+    L.fr_mixed_stage_advance.argtypes = [vp, i, C.c_double, vp]
+    L.fr_mixed_stage_info.argtypes = [vp, C.POINTER(ll), C.POINTER(ll), C.POINTER(i)]
+    for f in ("fr_mixed_stage_create", "fr_mixed_stage_destroy", "fr_mixed_stage_residual", "fr_mixed_stage_advance",
+              "fr_mixed_stage_info"):
+        getattr(L, f).restype = C.c_int
+    return L
+
+
+class FusedMixedMesh:
+    """The mesh of `MixedOperatorMesh` (same arguments) advanced by the fused
+    stage of include/fr_b200.h (`fr_mixed_stage_*`): per element type and RK
+    stage one gradient kernel and one interface/update kernel, operator
+    products on the FP64 tensor cores.  Navier-Stokes in 3-D; tets, prisms
+    and hexes of orders 2 and 3.  The state of type i is `S[i]["u"]`
+    (n_upts, n_eles, 5) on the device, advanced in place; `residual()` writes
+    `S[i]["div"]`."""
+
+    def __init__(self, types, int_inters, physics, bdy_inters=(), bdy=None, R_ref=1.0, device=0):
+        import torch
+        self.torch = torch
+        self.L = _bind_stage(lib())
+        dev = "cuda:%d" % device
+        self.dev = dev
+        keys = list(types.keys())
+        pos = {k: j for j, k in enumerate(keys)}
+        D = int(np.asarray(types[keys[0]]["JGinv_upts"]).shape[0])
+        self.D, self.F = D, D + 2
+        keep = []  # host arrays the C call reads
+
+        def host(a):
+            a = np.asfortranarray(a, dtype=np.float64)
+            keep.append(a)
+            return a.ctypes.data
+
+        descs = (_MixedStageType * len(keys))()
+        self.S = {}
+        for j, k in enumerate(keys):
+            ty = types[k]
+            nu, E, _ = ty["u"].shape
+            nf = ty["opp_0"].shape[0]
+            s = dict(nu=nu, nf=nf, E=E)
+            s["u"] = torch.from_numpy(np.asfortranarray(ty["u"], dtype=np.float64).ravel(order="F").copy()).to(dev)
+            s["div"] = torch.zeros(nu * E * self.F, dtype=torch.float64, device=dev)
+            self.S[k] = s
+            d = descs[j]
+            d.n_upts, d.n_fpts, d.n_eles = nu, nf, E
+            d.opp_0, d.opp_3, d.opp_6 = host(ty["opp_0"]), host(ty["opp_3"]), host(ty["opp_6"])
+            for name in ("opp_1", "opp_2", "opp_4", "opp_5"):
+                arr = getattr(d, name)
+                for q in range(D):
+                    arr[q] = host(ty[name][q])
+            d.JGinv_upts, d.detjac_upts = host(ty["JGinv_upts"]), host(ty["detjac_upts"])
+            d.tdA_fpts, d.norm_fpts = host(ty["tdA_fpts"]), host(ty["norm_fpts"])
+            d.disu_upts, d.div_tconf_upts = s["u"].data_ptr(), s["div"].data_ptr()
+
+        def tables(ws, type_rows):
+            ptrs, nfpi, ni = [], [], []
+            for w in ws:
+                w = np.array(w, dtype=np.int32, order="F", copy=True)
+                for r in type_rows:
+                    t = w[r].copy()
+                    w[r] = -1
+                    for k, j in pos.items():
+                        w[r][t == k] = j
+                keep.append(w)
+                ptrs.append(w.ctypes.data)
+                nfpi.append(w.shape[1])
+                ni.append(w.shape[2])
+            n = len(ws)
+            return (n, (_VP * max(n, 1))(*ptrs), (C.c_int * max(n, 1))(*nfpi), (C.c_longlong * max(n, 1))(*ni))
+
+        ni_, ip, inf, inn = tables(int_inters, (0, 3))
+        nb_, bp, bnf, bnn = tables(bdy_inters, (0,))
+        bdy_arr = (C.c_double * 14)(*(list(bdy) if bdy is not None else [0.0] * 14))
+        self.ph = PhysDesc(**physics)
+        h = _VP()
+        _check(self.L.fr_mixed_stage_create(D, len(keys), descs, ni_, ip, inf, inn, nb_, bp, bnf, bnn, bdy_arr,
+                                            float(R_ref), C.byref(self.ph), C.byref(h)))
+        self.h = h
+        self.stream = torch.cuda.current_stream(dev)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.fr_mixed_stage_destroy(self.h)
+            self.h = None
+
+    @property
+    def dofs(self):
+        """Solution DOFs (points x fields) over all element types."""
+        return sum(s["nu"] * s["E"] * self.F for s in self.S.values())
+
+    @property
+    def launches_per_stage(self):
+        n = C.c_int()
+        _check(self.L.fr_mixed_stage_info(self.h, None, None, C.byref(n)))
+        return n.value
+
+    def get_state(self, i):
+        self.torch.cuda.synchronize()
+        s = self.S[i]
+        return s["u"].cpu().numpy().reshape((s["nu"], s["E"], self.F), order="F")
+
+    def residual(self):
+        """div_tconf_upts of every element type (one CalcResidual) into S[i]["div"]."""
+        _check(self.L.fr_mixed_stage_residual(self.h, _VP(self.stream.cuda_stream)))
+
+    def advance(self, n_steps, dt):
+        """n_steps RK45 steps (5 stages each)."""
+        _check(self.L.fr_mixed_stage_advance(self.h, int(n_steps), float(dt), _VP(self.stream.cuda_stream)))
+
+
 def tile_mixed_mesh(types, int_inters, bdy_inters, copies):
     """`copies` independent copies of a mixed mesh (element axis tiled, every
     copy's interfaces wired to its own elements), for throughput runs on a

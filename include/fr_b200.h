@@ -634,6 +634,62 @@ fr_status fr_mixed_inters(const fr_mixed* m, int group, int* n_fpts_per_inter, l
 fr_status fr_mixed_bdy_inters(const fr_mixed* m, int group, int* n_fpts_per_inter, long long* n_inters, int* table);
 
 /* ------------------------------------------------------------------------
+ * Fused RK stage for meshes of dense-operator element types.
+ *
+ * The per-operator sequence of CalcResidual (src/solver.cpp:65-225: for every
+ * element type extrapolate_solution, calculate_gradient, evaluate_invFlux;
+ * every interface type calculate_common_invFlux; correct_gradient,
+ * extrapolate_corrected_gradient, evaluate_viscFlux, extrapolate_totalFlux,
+ * calculate_divergence; calculate_common_viscFlux; calculate_corrected_divergence)
+ * and AdvanceSolution (src/eles.cpp:1155-1178), Navier-Stokes, Rusanov +
+ * LDG, 3-D, in two kernels per element type and stage whose operator
+ * products run on the FP64 tensor cores.  Inputs are what the per-operator
+ * entry points take: each type's operators and metrics as its eles object
+ * holds them (host arrays, column-major, the layouts of the fr_op_* calls;
+ * opp_1/2/4/5 one array per dimension), its state disu_upts and optional
+ * output div_tconf_upts on the device (n_upts, n_eles, n_fields), and the
+ * interface tables of fr_mixed_inters / fr_mixed_bdy_inters ((6 | 4,
+ * n_fpts_per_inter, n_inters) int arrays of (type index, element, flux point)
+ * per side, the boundary type last), on the host.  Every flux point must lie
+ * on exactly one interface or boundary (FR_ERR_MESH otherwise).  Element
+ * types with kernels: tets, prisms and hexes of orders 2 and 3
+ * (FR_ERR_UNSUPPORTED otherwise).  The stage keeps the RK register and the
+ * flux-point traces on the device; disu_upts is advanced in place.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+  int n_upts, n_fpts;
+  long long n_eles;
+  const double* opp_0;       /* (n_fpts, n_upts)                      */
+  const double* opp_1[3];    /* (n_fpts, n_upts) per dimension         */
+  const double* opp_2[3];    /* (n_upts, n_upts) per dimension         */
+  const double* opp_3;       /* (n_upts, n_fpts)                      */
+  const double* opp_4[3];    /* (n_upts, n_upts) per dimension         */
+  const double* opp_5[3];    /* (n_upts, n_fpts) per dimension         */
+  const double* opp_6;       /* (n_fpts, n_upts)                      */
+  const double* JGinv_upts;  /* (n_dims, n_dims, n_upts, n_eles)      */
+  const double* detjac_upts; /* (n_upts, n_eles)                      */
+  const double* tdA_fpts;    /* (n_fpts, n_eles)                      */
+  const double* norm_fpts;   /* (n_fpts, n_eles, n_dims)              */
+  double* disu_upts;         /* device (n_upts, n_eles, n_fields)     */
+  double* div_tconf_upts;    /* device, or NULL if residual() is not called */
+} fr_mixed_stage_type;
+
+typedef struct fr_mixed_stage fr_mixed_stage;
+fr_status fr_mixed_stage_create(int n_dims, int n_types, const fr_mixed_stage_type* types, int n_int_groups,
+                                const int* const* int_tables, const int* int_nfpi, const long long* int_ni,
+                                int n_bdy_groups, const int* const* bdy_tables, const int* bdy_nfpi,
+                                const long long* bdy_ni, const double* bdy_params, double R_ref,
+                                const fr_phys_desc* phys, fr_mixed_stage** out);
+fr_status fr_mixed_stage_destroy(fr_mixed_stage* s);
+/* div_tconf_upts of every type for the current state (one CalcResidual). */
+fr_status fr_mixed_stage_residual(fr_mixed_stage* s, void* stream);
+/* n_steps RK45 steps of dt (5 stages each) on the current state. */
+fr_status fr_mixed_stage_advance(fr_mixed_stage* s, int n_steps, double dt, void* stream);
+/* Flux points over all types, boundary points, kernel launches per stage. */
+fr_status fr_mixed_stage_info(const fr_mixed_stage* s, long long* n_flux_points, long long* n_boundary_points,
+                              int* launches_per_stage);
+
+/* ------------------------------------------------------------------------
  * Residual without device allocation.
  *
  * No counterpart in the reference.  For callers that cannot call cudaMalloc
