@@ -38,6 +38,7 @@
 // the start of a block), so padded products add exact zeros.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -199,9 +200,9 @@ __device__ __forceinline__ void load_state(double* sU, const double* __restrict_
 }
 
 // ------------------------------------------------------------------ kernel A
-template <int D, int NU, int NF, int EPB, int NTH>
-__global__ void __launch_bounds__(NTH) mixed_grad_kernel(MixedType t, MixedFpts m, const double* __restrict__ UFc,
-                                                         PhysT<double> ph)
+template <int D, int NU, int NF, int EPB, int NTH, int MINB>
+__global__ void __launch_bounds__(NTH, MINB) mixed_grad_kernel(MixedType t, MixedFpts m,
+                                                               const double* __restrict__ UFc, PhysT<double> ph)
 {
   using Q = MPlan<D, NU, NF, EPB>;
   constexpr int F = D + 2, NW = NTH / 32;
@@ -347,7 +348,10 @@ __global__ void __launch_bounds__(NTH) mixed_grad_kernel(MixedType t, MixedFpts 
   __syncthreads();
 
   // transformed flux at the solution points (evaluate_invFlux, then
-  // evaluate_viscFlux adding to it): rows (d, point) of X
+  // evaluate_viscFlux adding to it): rows (d, point) of X.  The viscous flux
+  // takes one reciprocal of rho (vis_flux_fast): its terms are ~1/Re of the
+  // inviscid flux they are added to, so its ulp-level differences from the
+  // reference's divisions stay far below the rounding of the sum.
   for (int i = tid; i < nval * NU; i += NTH) {
     const int el = i / NU, p = i - el * NU;
     const size_t gi = p + (size_t)NU * (e0 + el);
@@ -374,7 +378,7 @@ __global__ void __launch_bounds__(NTH) mixed_grad_kernel(MixedType t, MixedFpts 
       for (int k = 0; k < F; k++)
 #pragma unroll
         for (int c = 0; c < D; c++) gq[k][c] = sG[(el * F + k) * Q::ldG + c * NU + p];
-      vis_flux<D, double>(ph, q, gq, fv);
+      vis_flux_fast<D, double>(ph, q, gq, fv);
 #pragma unroll
       for (int k = 0; k < F; k++)
 #pragma unroll
@@ -415,10 +419,11 @@ __global__ void __launch_bounds__(NTH) mixed_grad_kernel(MixedType t, MixedFpts 
 // ------------------------------------------------------------------ kernel B
 // MODE 1: RK45 stage update (rk_a, rk_b, dt) and the new traces into UFn;
 // MODE 0: div_tconf_upts into t.DIV only.
-template <int D, int NU, int NF, int EPB, int NTH, int MODE>
-__global__ void __launch_bounds__(NTH) mixed_update_kernel(MixedType t, MixedFpts m, const double* __restrict__ UFc,
-                                                           double* __restrict__ UFn, PhysT<double> ph, double rk_a,
-                                                           double rk_b, double dt)
+template <int D, int NU, int NF, int EPB, int NTH, int MINB, int MODE>
+__global__ void __launch_bounds__(NTH, MINB) mixed_update_kernel(MixedType t, MixedFpts m,
+                                                                 const double* __restrict__ UFc,
+                                                                 double* __restrict__ UFn, PhysT<double> ph,
+                                                                 double rk_a, double rk_b, double dt)
 {
   using Q = MPlan<D, NU, NF, EPB>;
   constexpr int F = D + 2, NW = NTH / 32;
@@ -559,30 +564,65 @@ __global__ void __launch_bounds__(NTH) mixed_trace_kernel(MixedType t, long long
 }
 
 // ------------------------------------------------------------ dispatch
+// Launch shapes: elements per block, threads per block, blocks per SM the
+// registers are capped for.  Gradient and update kernels pick theirs
+// independently (fr_mixed_stage_autotune); the products give the same bits
+// in every shape, since each output is the same chain of k-steps.
+struct MixedShape {
+  int epb, nth, minb;
+};
+constexpr MixedShape kGradShapes[] = {{8, 256, 1}, {4, 128, 3}, {8, 128, 2}};
+constexpr MixedShape kUpdShapes[] = {{8, 256, 2}, {4, 128, 4}, {8, 128, 4}};
+constexpr int kNGrad = sizeof(kGradShapes) / sizeof(kGradShapes[0]);
+constexpr int kNUpd = sizeof(kUpdShapes) / sizeof(kUpdShapes[0]);
+
+using GradFn = void (*)(MixedType, MixedFpts, const double*, PhysT<double>);
+using UpdFn = void (*)(MixedType, MixedFpts, const double*, double*, PhysT<double>, double, double, double);
+using TraceFn = void (*)(MixedType, long long, double*);
+
 struct MixedKernels {
   int D, NU, NF;
-  size_t smem_a, smem_b, smem_c;
-  void (*grad)(MixedType, MixedFpts, const double*, PhysT<double>);
-  void (*upd0)(MixedType, MixedFpts, const double*, double*, PhysT<double>, double, double, double);
-  void (*upd1)(MixedType, MixedFpts, const double*, double*, PhysT<double>, double, double, double);
-  void (*trace)(MixedType, long long, double*);
+  GradFn grad[kNGrad];
+  size_t smem_a[kNGrad];
+  UpdFn upd0[kNUpd], upd1[kNUpd];
+  size_t smem_b[kNUpd];
+  TraceFn trace;
+  size_t smem_c;
 };
+
+template <int D, int NU, int NF, int V>
+void fill_grad(MixedKernels& k)
+{
+  constexpr MixedShape g = kGradShapes[V];
+  k.grad[V] = mixed_grad_kernel<D, NU, NF, g.epb, g.nth, g.minb>;
+  k.smem_a[V] = sizeof(double) * MPlan<D, NU, NF, g.epb>::nA;
+}
+
+template <int D, int NU, int NF, int V>
+void fill_upd(MixedKernels& k)
+{
+  constexpr MixedShape u = kUpdShapes[V];
+  k.upd0[V] = mixed_update_kernel<D, NU, NF, u.epb, u.nth, u.minb, 0>;
+  k.upd1[V] = mixed_update_kernel<D, NU, NF, u.epb, u.nth, u.minb, 1>;
+  k.smem_b[V] = sizeof(double) * MPlan<D, NU, NF, u.epb>::nB;
+}
 
 template <int D, int NU, int NF>
 MixedKernels mixed_kernels()
 {
-  using Q = MPlan<D, NU, NF, kMixedEPB>;
   MixedKernels k;
   k.D = D;
   k.NU = NU;
   k.NF = NF;
-  k.smem_a = sizeof(double) * Q::nA;
-  k.smem_b = sizeof(double) * Q::nB;
-  k.smem_c = sizeof(double) * Q::nC;
-  k.grad = mixed_grad_kernel<D, NU, NF, kMixedEPB, kMixedNT>;
-  k.upd0 = mixed_update_kernel<D, NU, NF, kMixedEPB, kMixedNT, 0>;
-  k.upd1 = mixed_update_kernel<D, NU, NF, kMixedEPB, kMixedNT, 1>;
+  fill_grad<D, NU, NF, 0>(k);
+  fill_grad<D, NU, NF, 1>(k);
+  fill_grad<D, NU, NF, 2>(k);
+  fill_upd<D, NU, NF, 0>(k);
+  fill_upd<D, NU, NF, 1>(k);
+  fill_upd<D, NU, NF, 2>(k);
+  static_assert(kNGrad == 3 && kNUpd == 3, "one fill per shape");
   k.trace = mixed_trace_kernel<D, NU, NF, kMixedEPB, kMixedNT>;
+  k.smem_c = sizeof(double) * MPlan<D, NU, NF, kMixedEPB>::nC;
   return k;
 }
 
@@ -630,6 +670,7 @@ struct fr_mixed_stage {
   std::vector<MixedType> types;
   std::vector<MixedKernels> kern;
   std::vector<void*> allocs;
+  std::vector<int> gv, uv;  // launch shape of each type's gradient and update kernels
   MixedFpts fp{};
   double* UF[2] = {nullptr, nullptr};
   int cur = 0;
@@ -665,55 +706,67 @@ struct fr_mixed_stage {
 
 namespace {
 
+unsigned blocks_of(long long E, int epb) { return (unsigned)((E + epb - 1) / epb); }
+
 fr_status launch_trace(fr_mixed_stage* s, cudaStream_t st)
 {
   for (int i = 0; i < s->n_types; i++) {
     const MixedType& t = s->types[i];
     if (t.E == 0) continue;
-    const unsigned blocks = (unsigned)((t.E + kMixedEPB - 1) / kMixedEPB);
-    s->kern[i].trace<<<blocks, kMixedNT, s->kern[i].smem_c, st>>>(t, s->NT, s->UF[s->cur]);
+    s->kern[i].trace<<<blocks_of(t.E, kMixedEPB), kMixedNT, s->kern[i].smem_c, st>>>(t, s->NT, s->UF[s->cur]);
     if (fr_status e = mlaunched("mixed_trace_kernel")) return e;
   }
   return FR_OK;
 }
 
-// one CalcResidual (+ the RK45 update of stage `stage` when mode is 1)
-fr_status launch_stage(fr_mixed_stage* s, int mode, int stage, double dt, cudaStream_t st)
+fr_status launch_grad(fr_mixed_stage* s, int i, int v, const double* UFc, cudaStream_t st)
+{
+  const MixedType& t = s->types[i];
+  const MixedShape& g = kGradShapes[v];
+  s->kern[i].grad[v]<<<blocks_of(t.E, g.epb), g.nth, s->kern[i].smem_a[v], st>>>(t, s->fp, UFc, s->ph);
+  return mlaunched("mixed_grad_kernel");
+}
+
+fr_status launch_upd(fr_mixed_stage* s, int i, int v, int mode, int stage, double dt, const double* UFc, double* UFn,
+                     cudaStream_t st)
 {
   static const double A[5] = {0.0, -0.417890474499852, -1.192151694642677, -1.697784692471528, -1.514183444257156};
   static const double B[5] = {0.149659021999229, 0.379210312999627, 0.822955029386982, 0.699450455949122,
                               0.153057247968152};
+  const MixedType& t = s->types[i];
+  const MixedShape& u = kUpdShapes[v];
+  auto k = mode ? s->kern[i].upd1[v] : s->kern[i].upd0[v];
+  k<<<blocks_of(t.E, u.epb), u.nth, s->kern[i].smem_b[v], st>>>(t, s->fp, UFc, UFn, s->ph, A[stage], B[stage], dt);
+  return mlaunched("mixed_update_kernel");
+}
+
+// one CalcResidual (+ the RK45 update of stage `stage` when mode is 1)
+fr_status launch_stage(fr_mixed_stage* s, int mode, int stage, double dt, cudaStream_t st)
+{
   const double* UFc = s->UF[s->cur];
   double* UFn = s->UF[s->cur ^ 1];
-  for (int i = 0; i < s->n_types; i++) {
-    const MixedType& t = s->types[i];
-    if (t.E == 0) continue;
-    const unsigned blocks = (unsigned)((t.E + kMixedEPB - 1) / kMixedEPB);
-    s->kern[i].grad<<<blocks, kMixedNT, s->kern[i].smem_a, st>>>(t, s->fp, UFc, s->ph);
-    if (fr_status e = mlaunched("mixed_grad_kernel")) return e;
-  }
-  for (int i = 0; i < s->n_types; i++) {
-    const MixedType& t = s->types[i];
-    if (t.E == 0) continue;
-    const unsigned blocks = (unsigned)((t.E + kMixedEPB - 1) / kMixedEPB);
-    auto k = mode ? s->kern[i].upd1 : s->kern[i].upd0;
-    k<<<blocks, kMixedNT, s->kern[i].smem_b, st>>>(t, s->fp, UFc, UFn, s->ph, A[stage], B[stage], dt);
-    if (fr_status e = mlaunched("mixed_update_kernel")) return e;
-  }
+  for (int i = 0; i < s->n_types; i++)
+    if (s->types[i].E > 0)
+      if (fr_status e = launch_grad(s, i, s->gv[i], UFc, st)) return e;
+  for (int i = 0; i < s->n_types; i++)
+    if (s->types[i].E > 0)
+      if (fr_status e = launch_upd(s, i, s->uv[i], mode, stage, dt, UFc, UFn, st)) return e;
   if (mode) s->cur ^= 1;
   return FR_OK;
 }
 
 fr_status set_smem(const MixedKernels& k)
 {
-  struct {
-    const void* f;
-    size_t b;
-  } list[] = {{(const void*)k.grad, k.smem_a}, {(const void*)k.upd0, k.smem_b}, {(const void*)k.upd1, k.smem_b},
-              {(const void*)k.trace, k.smem_c}};
+  std::vector<std::pair<const void*, size_t>> list;
+  for (int v = 0; v < kNGrad; v++) list.push_back({(const void*)k.grad[v], k.smem_a[v]});
+  for (int v = 0; v < kNUpd; v++) {
+    list.push_back({(const void*)k.upd0[v], k.smem_b[v]});
+    list.push_back({(const void*)k.upd1[v], k.smem_b[v]});
+  }
+  list.push_back({(const void*)k.trace, k.smem_c});
   for (auto& q : list) {
-    if (q.b > 227 * 1024) return mfail(FR_ERR_UNSUPPORTED, "element type too large for one block of shared memory");
-    if (cudaFuncSetAttribute(q.f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)q.b) != cudaSuccess)
+    if (q.second > 227 * 1024) return mfail(FR_ERR_UNSUPPORTED, "element type too large for one block of shared memory");
+    if (cudaFuncSetAttribute(q.first, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)q.second) != cudaSuccess)
       return mfail(FR_ERR_CUDA, "cudaFuncSetAttribute failed");
   }
   return FR_OK;
@@ -768,6 +821,8 @@ fr_status fr_mixed_stage_create(int n_dims, int n_types, const fr_mixed_stage_ty
                                                 " solution / " + std::to_string(NF) + " flux points"));
     if (fr_status e = set_smem(k)) return bail(e);
     s->kern.push_back(k);
+    s->gv.push_back(0);
+    s->uv.push_back(0);
     off[i + 1] = off[i] + (long long)NF * ty.n_eles;
   }
   s->NT = off[n_types];
@@ -912,6 +967,76 @@ fr_status fr_mixed_stage_advance(fr_mixed_stage* s, int n_steps, double dt, void
     for (int k = 0; k < 5; k++)
       if (fr_status e = launch_stage(s, 1, k, dt, st)) return e;
   return FR_OK;
+}
+
+fr_status fr_mixed_stage_set_launch(fr_mixed_stage* s, int type, int grad_shape, int update_shape)
+{
+  g_err.clear();
+  if (!s || type < 0 || type >= s->n_types || grad_shape < 0 || grad_shape >= kNGrad || update_shape < 0 ||
+      update_shape >= kNUpd)
+    return mfail(FR_ERR_ARG, "bad type or launch shape");
+  s->gv[type] = grad_shape;
+  s->uv[type] = update_shape;
+  return FR_OK;
+}
+
+fr_status fr_mixed_stage_get_launch(const fr_mixed_stage* s, int type, int* grad_shape, int* update_shape)
+{
+  g_err.clear();
+  if (!s || type < 0 || type >= s->n_types) return mfail(FR_ERR_ARG, "bad type");
+  if (grad_shape) *grad_shape = s->gv[type];
+  if (update_shape) *update_shape = s->uv[type];
+  return FR_OK;
+}
+
+fr_status fr_mixed_stage_autotune(fr_mixed_stage* s, void* stream)
+{
+  g_err.clear();
+  if (!s) return mfail(FR_ERR_ARG, "null stage");
+  cudaStream_t st = (cudaStream_t)stream;
+  // the update kernels are timed in residual mode, into a scratch output,
+  // so the state is not touched
+  size_t most = 1;
+  for (const MixedType& t : s->types) most = std::max(most, (size_t)((long long)t.NU * t.E * s->F));
+  double* scratch = nullptr;
+  if (cudaMalloc(&scratch, most * sizeof(double)) != cudaSuccess) return mfail(FR_ERR_CUDA, "device allocation failed");
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  fr_status rc = launch_trace(s, st);
+  const double* UFc = s->UF[s->cur];
+  constexpr int reps = 3;
+  for (int i = 0; i < s->n_types && rc == FR_OK; i++) {
+    if (s->types[i].E == 0) continue;
+    MixedType saved = s->types[i];
+    s->types[i].DIV = scratch;
+    for (int pass = 0; pass < 2 && rc == FR_OK; pass++) {
+      const int nv = pass == 0 ? kNGrad : kNUpd;
+      int pick = 0;
+      float best = 0.f;
+      for (int v = 0; v < nv && rc == FR_OK; v++) {
+        // one untimed launch, then the timed ones
+        for (int r = 0; r <= reps && rc == FR_OK; r++) {
+          if (r == 1) cudaEventRecord(e0, st);
+          rc = pass == 0 ? launch_grad(s, i, v, UFc, st) : launch_upd(s, i, v, 0, 0, 0.0, UFc, nullptr, st);
+        }
+        cudaEventRecord(e1, st);
+        if (cudaEventSynchronize(e1) != cudaSuccess) rc = mfail(FR_ERR_CUDA, "autotune timing failed");
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (v == 0 || ms < best) {
+          best = ms;
+          pick = v;
+        }
+      }
+      (pass == 0 ? s->gv : s->uv)[i] = pick;
+    }
+    s->types[i] = saved;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(scratch);
+  return rc;
 }
 
 fr_status fr_mixed_stage_info(const fr_mixed_stage* s, long long* n_flux_points, long long* n_boundary_points,

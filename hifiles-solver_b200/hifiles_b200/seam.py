@@ -416,8 +416,12 @@ def _bind_stage(L):
     L.fr_mixed_stage_residual.argtypes = [vp, vp]
     L.fr_mixed_stage_advance.argtypes = [vp, i, C.c_double, vp]
     L.fr_mixed_stage_info.argtypes = [vp, C.POINTER(ll), C.POINTER(ll), C.POINTER(i)]
+    L.fr_mixed_stage_set_launch.argtypes = [vp, i, i, i]
+    L.fr_mixed_stage_get_launch.argtypes = [vp, i, C.POINTER(i), C.POINTER(i)]
+    L.fr_mixed_stage_autotune.argtypes = [vp, vp]
     for f in ("fr_mixed_stage_create", "fr_mixed_stage_destroy", "fr_mixed_stage_residual", "fr_mixed_stage_advance",
-              "fr_mixed_stage_info"):
+              "fr_mixed_stage_info", "fr_mixed_stage_set_launch", "fr_mixed_stage_get_launch",
+              "fr_mixed_stage_autotune"):
         getattr(L, f).restype = C.c_int
     return L
 
@@ -493,6 +497,7 @@ class FusedMixedMesh:
         _check(self.L.fr_mixed_stage_create(D, len(keys), descs, ni_, ip, inf, inn, nb_, bp, bnf, bnn, bdy_arr,
                                             float(R_ref), C.byref(self.ph), C.byref(h)))
         self.h = h
+        self._pos = pos
         self.stream = torch.cuda.current_stream(dev)
 
     def __del__(self):
@@ -515,6 +520,24 @@ class FusedMixedMesh:
         self.torch.cuda.synchronize()
         s = self.S[i]
         return s["u"].cpu().numpy().reshape((s["nu"], s["E"], self.F), order="F")
+
+    def set_state(self, i, u):
+        s = self.S[i]
+        s["u"].copy_(self.torch.from_numpy(np.asfortranarray(u, dtype=np.float64).ravel(order="F")))
+
+    def launch(self, i):
+        """(gradient, update) launch shapes of element type i."""
+        g, u = C.c_int(), C.c_int()
+        _check(self.L.fr_mixed_stage_get_launch(self.h, self._pos[i], C.byref(g), C.byref(u)))
+        return g.value, u.value
+
+    def set_launch(self, i, grad_shape, update_shape):
+        _check(self.L.fr_mixed_stage_set_launch(self.h, self._pos[i], int(grad_shape), int(update_shape)))
+
+    def autotune(self):
+        """Time every launch shape on the current state, keep the fastest."""
+        _check(self.L.fr_mixed_stage_autotune(self.h, _VP(self.stream.cuda_stream)))
+        return {i: self.launch(i) for i in self.S}
 
     def residual(self):
         """div_tconf_upts of every element type (one CalcResidual) into S[i]["div"]."""

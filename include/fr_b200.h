@@ -685,6 +685,15 @@ fr_status fr_mixed_stage_destroy(fr_mixed_stage* s);
 fr_status fr_mixed_stage_residual(fr_mixed_stage* s, void* stream);
 /* n_steps RK45 steps of dt (5 stages each) on the current state. */
 fr_status fr_mixed_stage_advance(fr_mixed_stage* s, int n_steps, double dt, void* stream);
+/* Launch shapes of each type's two stage kernels: gradient 0 = 8 elements x
+ * 256 threads, 1 = 4 x 128, 2 = 8 x 128; update 0 = 8 x 256, 1 = 4 x 128,
+ * 2 = 8 x 128 (every shape gives the same bits).  create() sets 0 and 0;
+ * autotune() times every shape on the current state (the update kernels in
+ * residual mode, into scratch memory; the state is not changed) and keeps
+ * the fastest per type. */
+fr_status fr_mixed_stage_set_launch(fr_mixed_stage* s, int type, int grad_shape, int update_shape);
+fr_status fr_mixed_stage_get_launch(const fr_mixed_stage* s, int type, int* grad_shape, int* update_shape);
+fr_status fr_mixed_stage_autotune(fr_mixed_stage* s, void* stream);
 /* Flux points over all types, boundary points, kernel launches per stage. */
 fr_status fr_mixed_stage_info(const fr_mixed_stage* s, long long* n_flux_points, long long* n_boundary_points,
                               int* launches_per_stage);

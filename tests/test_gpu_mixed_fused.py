@@ -147,3 +147,31 @@ def test_fused_stage_rejects_unsupported_meshes():
                                  C.byref(h))
     assert st == FR_ERR_ARG
     assert not h.value
+
+
+@pytest.mark.gpu
+def test_fused_launch_shapes_give_the_same_bits():
+    """Every launch shape of the two stage kernels ends on the same state bit
+    for bit; autotune() leaves the state as it was."""
+    torch = pytest.importorskip("torch")
+    from hifiles_b200 import seam
+    meta, a = load("mixed_channel_p3")
+    types, ints, bdys = seam.mixed_mesh_inputs(meta, a)
+    out = {}
+    for shapes in ((0, 0), (1, 1), (2, 2), (1, 0), (0, 2)):
+        m = seam.FusedMixedMesh(types, ints, meta["physics"], bdys, meta["bdy"], meta["R_ref"])
+        for i in m.S:
+            m.set_launch(i, *shapes)
+            assert m.launch(i) == shapes
+        m.advance(2, meta["dt"])
+        out[shapes] = {i: m.get_state(i) for i in m.S}
+    for shapes, st in out.items():
+        for i in st:
+            assert np.array_equal(st[i], out[(0, 0)][i]), shapes
+    m = seam.FusedMixedMesh(types, ints, meta["physics"], bdys, meta["bdy"], meta["R_ref"])
+    before = {i: m.get_state(i) for i in m.S}
+    picked = m.autotune()
+    torch.cuda.synchronize()
+    for i in m.S:
+        assert np.array_equal(m.get_state(i), before[i])
+        assert all(0 <= v < 3 for v in picked[i])
