@@ -324,7 +324,9 @@ def measure_mixed_channel(order, n=(40, 20, 20), steps=3, err_steps=10, dt=2e-4)
     library (operators, metrics, wiring: hifiles_b200.mixed) and advanced
     through the fr_op_* entry points with FP64 operator products on the CUDA
     cores and BF16x3 / BF16x6 split products on the tensor cores, with their
-    L2 error against FP64 after `err_steps` steps."""
+    L2 error against FP64 after `err_steps` steps; and by the fused stage
+    (fr_mixed_stage_*, FP64 tensor-core products), against the per-operator
+    FP64 path."""
     import torch
     from hifiles_b200 import mixed as X
     from hifiles_b200 import seam
@@ -370,10 +372,30 @@ def measure_mixed_channel(order, n=(40, 20, 20), steps=3, err_steps=10, dt=2e-4)
         torch.cuda.synchronize()
         res[name]["l2_rel_vs_fp64_after_%d_steps" % err_steps] = l2({i: s["u"] for i, s in m.S.items()}, ref)
     finite = all(bool(torch.isfinite(s["u"]).all()) for s in m.S.values())
+    # the fused stage (fr_mixed_stage_*): two kernels per element type and RK
+    # stage, FP64 tensor-core products; launch shapes autotuned
+    f = seam.FusedMixedMesh(types, ints, CHANNEL_PHYSICS, bdys, CHANNEL_BDY, CHANNEL_R_REF)
+    shapes = f.autotune()
+    f.residual()
+    torch.cuda.synchronize()
+    fres = {"residual_l2_rel_vs_operator_path": l2({i: s["div"] for i, s in f.S.items()}, div0)}
+    u0f = {i: s["u"].clone() for i, s in f.S.items()}
+    f.advance(1, dt)
+    ms = _time_steps(lambda k: f.advance(k, dt), f.stream, steps)
+    fres.update({"value": f.dofs * 5 / (ms * 1e-3), "ms_per_step": ms, "launches_per_stage": f.launches_per_stage,
+                 "launch_shapes": {str(i): list(v) for i, v in shapes.items()}})
+    for i, s in f.S.items():
+        s["u"].copy_(u0f[i])
+    f.advance(err_steps, dt)
+    torch.cuda.synchronize()
+    fres["l2_rel_vs_operator_path_after_%d_steps" % err_steps] = l2({i: s["u"] for i, s in f.S.items()}, ref)
+    res["fused_fp64"] = fres
+    finite = finite and all(bool(torch.isfinite(s["u"]).all()) for s in f.S.values())
+    del f
     ne = {X.TET: 0, X.PRISM: 0}
     ne.update({t: int(v["n_eles"]) for t, v in M.types.items()})
     res["workload"] = ("channel %s cells of order %d: %d tets, %d prisms, %d DOFs, jitter 0.15 h; dt %g; one step = 5 "
-                       "RK stages of CalcResidual through the fr_op_* entry points" %
+                       "RK stages of CalcResidual (fp64/bf16x*: the fr_op_* entry points; fused_fp64: fr_mixed_stage_*)" %
                        ("x".join(str(v) for v in n), order, ne[X.TET], ne[X.PRISM], m.dofs, dt))
     res["host_setup_s"] = setup_s
     res["finite_after_error_run"] = finite

@@ -82,9 +82,12 @@ __host__ __device__ constexpr int tiles_per_unit(int ntl)
 }
 
 // Shared-memory plan and product shapes of one element type (doubles).
+constexpr size_t kMixedSmemMax = 227 * 1024;  // dynamic shared memory of one block
+__host__ __device__ constexpr int r2(int x) { return (x + 1) / 2 * 2; }  // 16-byte region starts
+
 template <int D, int NU, int NF, int EPB>
 struct MPlan {
-  static constexpr int F = D + 2;
+  static constexpr int F = D + 2, DD = D * D, EU = EPB * NU, EF = EPB * NF;
   static constexpr int N = EPB * F, NP = c8(N);          // (element, field) columns
   static constexpr int NG = N * D, NGP = c8(NG);         // (element, field, dimension) columns
   static constexpr int ldU = bank_ld(c4(NU));
@@ -95,16 +98,31 @@ struct MPlan {
   static constexpr int KS_U = c4(NU) / 4, KS_F = c4(NF) / 4, KS_T = c4(D * NU) / 4;
   static constexpr int NTL = NP / 8, NTLG = NGP / 8;
   static constexpr int TN = tiles_per_unit(NTL), TNG = tiles_per_unit(NTLG);
-  // kernel A: U | own traces | gradient | X (delta, then gradient at the
-  // flux points, then the transformed flux)
+  // kernel A: the matrices U | own traces | gradient (the neighbours' traces
+  // [F][EF] before it) | X (delta, then the gradient at the flux points, then
+  // the transformed flux); then what the load phase stages: left normals
+  // [D][EF], detJ [EU], JGinv [EPB][DD NU] (when it fits), mate and side [EF]
+  // ints each
   static constexpr int oU = 0, oUF = oU + NP * ldU, oG = oUF + NP * ldF, oX = oG + NP * ldG;
   static constexpr int nX = cmax(cmax(NP * ldF, NGP * ldF), NP * ldT);
-  static constexpr int nA = oX + nX;
-  // kernel B: the jump norm_tconf - norm_tdisf | the new state
-  static constexpr int oJ = 0, oUn = NP * ldF, nB = oUn + NP * ldU;
+  static constexpr int oNL = oX + r2(nX), oDJ = oNL + r2(D * EF), oJG = oDJ + r2(EU);
+  static constexpr bool SJ = sizeof(double) * (size_t)(oJG + r2(DD * EU) + EF) <= kMixedSmemMax;
+  static constexpr int oIA = oJG + (SJ ? r2(DD * EU) : 0);
+  static constexpr int nA = oIA + r2(EF);
+  // kernel B: the jump norm_tconf - norm_tdisf (norm_tdisf first) | own traces
+  // [F][EF] (the new state [NP][ldU] after the flux phase) | neighbours'
+  // traces | own and neighbours' viscous projections [F-1][EF] | left normals
+  // [D][EF] | tdA [EF] | div_tdisf, RK register, state [F][EU] | detJ [EU] |
+  // mate and side
+  static constexpr int oJ = 0, oUo = r2(NP * ldF), oUN = oUo + r2(cmax(F * EF, NP * ldU));
+  static constexpr int oVo = oUN + r2(F * EF), oVN = oVo + r2((F - 1) * EF), oNLb = oVN + r2((F - 1) * EF);
+  static constexpr int oTA = oNLb + r2(D * EF), oDV = oTA + r2(EF), oRG = oDV + r2(F * EU), oUO = oRG + r2(F * EU);
+  static constexpr int oDJb = oUO + r2(F * EU), oIB = oDJb + r2(EU);
+  static constexpr int nB = oIB + r2(EF);
   // trace kernel: the state
   static constexpr int nC = NP * ldU;
   static_assert(ldT >= c4(D * NU) && ldG >= c8(D * NU) && ldF >= c8(NF) && ldU >= c4(NU), "plan");
+  static_assert(F * EF <= NP * ldG, "the neighbours' traces fit in the gradient's place");
 };
 
 struct MixedType {
@@ -118,7 +136,7 @@ struct MixedType {
 struct MixedFpts {
   long long NT;  // flux points over all types
   const int* mate;
-  const unsigned char* side;
+  const int* side;  // bit 0 left side, bits 2.. boundary type
   const double* nL;   // [D][NT]
   const double* tdA;  // [NT]
   double* VF;         // [F-1][NT]
@@ -188,51 +206,96 @@ __device__ __forceinline__ void clear_smem(double* s, int n)
 }
 
 // the block's state into columns (element, field) of sU (rows = solution points)
-template <int F, int NU, int ldU>
+template <int F, int NU, int EPB, int ldU, int NTH>
 __device__ __forceinline__ void load_state(double* sU, const double* __restrict__ U, long long e0, long long E,
                                            int nval)
 {
-  const int n = nval * NU;
-  for (int i = threadIdx.x; i < F * n; i += blockDim.x) {
-    const int k = i / n, r = i - k * n, el = r / NU, p = r - el * NU;
+  constexpr int EU = EPB * NU;
+  for (int i = threadIdx.x; i < F * EU; i += NTH) {
+    const int k = i / EU, r = i - k * EU;
+    if (r >= nval * NU) continue;
+    const int el = r / NU, p = r - el * NU;
     sU[(el * F + k) * ldU + p] = U[(size_t)NU * e0 + (size_t)NU * E * k + r];
   }
 }
 
 // ------------------------------------------------------------------ kernel A
+// A load phase issues every global read of the block (state, traces, the
+// neighbours' traces through mate, normals, metrics, wiring) into shared
+// memory, so the loads are in flight together; the compute phases that follow
+// touch global memory only to write.
 template <int D, int NU, int NF, int EPB, int NTH, int MINB>
 __global__ void __launch_bounds__(NTH, MINB) mixed_grad_kernel(MixedType t, MixedFpts m,
                                                                const double* __restrict__ UFc, PhysT<double> ph)
 {
   using Q = MPlan<D, NU, NF, EPB>;
-  constexpr int F = D + 2, NW = NTH / 32;
+  constexpr int F = D + 2, NW = NTH / 32, DD = D * D, EU = Q::EU, EF = Q::EF;
   extern __shared__ __align__(16) double msm[];
   double* sU = msm + Q::oU;
   double* sUF = msm + Q::oUF;
   double* sG = msm + Q::oG;
   double* sX = msm + Q::oX;
+  double* sUN = sG;  // neighbours' traces, until the gradient product
+  double* sNL = msm + Q::oNL;
+  double* sDJ = msm + Q::oDJ;
+  double* sJG = msm + Q::oJG;
+  int* sMate = reinterpret_cast<int*>(msm + Q::oIA);
+  int* sSide = sMate + EF;
   const int tid = threadIdx.x, warp = tid >> 5;
   const long long E = t.E, NT = m.NT, e0 = (long long)blockIdx.x * EPB;
-  const int nval = (int)(E - e0 < EPB ? E - e0 : EPB);
+  const int nval = (int)(E - e0 < EPB ? E - e0 : EPB), nuv = nval * NU, nfv = nval * NF;
   const long long gb = t.off + (long long)NF * e0;
 
-  clear_smem(msm, Q::nA);
+  clear_smem(msm, Q::oNL);
   __syncthreads();
-  load_state<F, NU, Q::ldU>(sU, t.U, e0, E, nval);
-  for (int i = tid; i < F * nval * NF; i += NTH) {
-    const int k = i / (nval * NF), r = i - k * nval * NF, el = r / NF, f = r - el * NF;
-    sUF[(el * F + k) * Q::ldF + f] = UFc[gb + r + NT * k];
+  // load phase: asynchronous copies (cp.async), many in flight per thread;
+  // first everything at known addresses, then the neighbours' traces through
+  // the staged mate
+  for (int i = tid; i < F * EU; i += NTH) {
+    const int k = i / EU, r = i - k * EU;
+    if (r >= nuv) continue;
+    const int el = r / NU, p = r - el * NU;
+    cp_async<8>(&sU[(el * F + k) * Q::ldU + p], t.U + (size_t)NU * e0 + (size_t)NU * E * k + r);
   }
+  for (int i = tid; i < F * EF; i += NTH) {
+    const int k = i / EF, r = i - k * EF;
+    if (r >= nfv) continue;
+    const int el = r / NF, f = r - el * NF;
+    cp_async<8>(&sUF[(el * F + k) * Q::ldF + f], UFc + gb + r + NT * k);
+  }
+  for (int i = tid; i < EF; i += NTH)
+    if (i < nfv) {
+      cp_async<4>(&sMate[i], m.mate + gb + i);
+      cp_async<4>(&sSide[i], m.side + gb + i);
+    }
+  for (int i = tid; i < D * EF; i += NTH) {
+    const int d = i / EF, r = i - d * EF;
+    if (r < nfv) cp_async<8>(&sNL[i], m.nL + gb + r + NT * d);
+  }
+  for (int i = tid; i < EU; i += NTH)
+    if (i < nuv) cp_async<8>(&sDJ[i], t.detj + (size_t)NU * e0 + i);
+  if constexpr (Q::SJ)
+    for (int i = tid; i < DD * EU; i += NTH)
+      if (i < DD * nuv) cp_async<8>(&sJG[i], t.JG + (size_t)DD * NU * e0 + i);
+  cp_async_wait_all();
   __syncthreads();
+  for (int i = tid; i < F * EF; i += NTH) {
+    const int k = i / EF, r = i - k * EF;
+    if (r >= nfv) continue;
+    const int mt = sMate[r];
+    if (mt >= 0) cp_async<8>(&sUN[i], UFc + mt + NT * k);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  auto jg = [&](int i) { return Q::SJ ? sJG + DD * i : t.JG + (size_t)DD * ((size_t)NU * e0 + i); };
 
   // LDG common solution at the own flux points: delta = u_c - u_own into X
-  for (int i = tid; i < nval * NF; i += NTH) {
+  for (int i = tid; i < nfv; i += NTH) {
     const int el = i / NF, f = i - el * NF;
-    const long long g = gb + i;
-    const int mt = m.mate[g], sd = m.side[g];
+    const int sd = sSide[i];
     double n[D], uo[F];
 #pragma unroll
-    for (int d = 0; d < D; d++) n[d] = m.nL[g + NT * d];
+    for (int d = 0; d < D; d++) n[d] = sNL[d * EF + i];
 #pragma unroll
     for (int k = 0; k < F; k++) uo[k] = sUF[(el * F + k) * Q::ldF + f];
     double* dx = sX + (el * F) * Q::ldF + f;
@@ -248,7 +311,7 @@ __global__ void __launch_bounds__(NTH, MINB) mixed_grad_kernel(MixedType t, Mixe
       const double pen = ldg_beta<D, double>(ph.pen_fact, n);
 #pragma unroll
       for (int k = 0; k < F; k++) {
-        const double un = UFc[mt + NT * k];
+        const double un = sUN[k * EF + i];
         const double ul = left ? uo[k] : un, ur = left ? un : uo[k];
         const double uc = 0.5 * (ul + ur) - pen * (ul - ur);
         dx[k * Q::ldF] = uc - uo[k];
@@ -271,11 +334,10 @@ __global__ void __launch_bounds__(NTH, MINB) mixed_grad_kernel(MixedType t, Mixe
   __syncthreads();
 
   // physical gradient in place (transform_grad_disu_upts: JGinv / detJ)
-  for (int i = tid; i < nval * NU; i += NTH) {
+  for (int i = tid; i < nuv; i += NTH) {
     const int el = i / NU, p = i - el * NU;
-    const size_t gi = p + (size_t)NU * (e0 + el);
-    const double inv = 1.0 / t.detj[gi];
-    const double* G = t.JG + (size_t)D * D * gi;
+    const double inv = 1.0 / sDJ[i];
+    const double* G = jg(i);
     double Gm[D][D];
 #pragma unroll
     for (int r = 0; r < D; r++)
@@ -314,13 +376,13 @@ __global__ void __launch_bounds__(NTH, MINB) mixed_grad_kernel(MixedType t, Mixe
   __syncthreads();
 
   // viscous normal projections (interior points) and boundary viscous fluxes
-  for (int i = tid; i < nval * NF; i += NTH) {
+  for (int i = tid; i < nfv; i += NTH) {
     const int el = i / NF, f = i - el * NF;
     const long long g = gb + i;
-    const int mt = m.mate[g], sd = m.side[g];
+    const int mt = sMate[i], sd = sSide[i];
     double n[D], uo[F], gf[F][D];
 #pragma unroll
-    for (int d = 0; d < D; d++) n[d] = m.nL[g + NT * d];
+    for (int d = 0; d < D; d++) n[d] = sNL[d * EF + i];
 #pragma unroll
     for (int k = 0; k < F; k++) {
       uo[k] = sUF[(el * F + k) * Q::ldF + f];
@@ -352,10 +414,9 @@ __global__ void __launch_bounds__(NTH, MINB) mixed_grad_kernel(MixedType t, Mixe
   // takes one reciprocal of rho (vis_flux_fast): its terms are ~1/Re of the
   // inviscid flux they are added to, so its ulp-level differences from the
   // reference's divisions stay far below the rounding of the sum.
-  for (int i = tid; i < nval * NU; i += NTH) {
+  for (int i = tid; i < nuv; i += NTH) {
     const int el = i / NU, p = i - el * NU;
-    const size_t gi = p + (size_t)NU * (e0 + el);
-    const double* G = t.JG + (size_t)D * D * gi;
+    const double* G = jg(i);
     double q[F], tf[F][D];
     {
       double fi[F][D];
@@ -418,7 +479,8 @@ __global__ void __launch_bounds__(NTH, MINB) mixed_grad_kernel(MixedType t, Mixe
 
 // ------------------------------------------------------------------ kernel B
 // MODE 1: RK45 stage update (rk_a, rk_b, dt) and the new traces into UFn;
-// MODE 0: div_tconf_upts into t.DIV only.
+// MODE 0: div_tconf_upts into t.DIV only.  Like kernel A, a load phase first
+// stages every global read of the block in shared memory.
 template <int D, int NU, int NF, int EPB, int NTH, int MINB, int MODE>
 __global__ void __launch_bounds__(NTH, MINB) mixed_update_kernel(MixedType t, MixedFpts m,
                                                                  const double* __restrict__ UFc,
@@ -426,30 +488,88 @@ __global__ void __launch_bounds__(NTH, MINB) mixed_update_kernel(MixedType t, Mi
                                                                  double rk_a, double rk_b, double dt)
 {
   using Q = MPlan<D, NU, NF, EPB>;
-  constexpr int F = D + 2, NW = NTH / 32;
+  constexpr int F = D + 2, NW = NTH / 32, EU = Q::EU, EF = Q::EF;
   extern __shared__ __align__(16) double msm[];
   double* sJ = msm + Q::oJ;
-  double* sUn = msm + Q::oUn;
+  double* sUo = msm + Q::oUo;
+  double* sUn = sUo;  // the new state, after the flux phase
+  double* sUN = msm + Q::oUN;
+  double* sVo = msm + Q::oVo;
+  double* sVN = msm + Q::oVN;
+  double* sNL = msm + Q::oNLb;
+  double* sTA = msm + Q::oTA;
+  double* sDV = msm + Q::oDV;
+  double* sRG = msm + Q::oRG;
+  double* sUO = msm + Q::oUO;
+  double* sDJ = msm + Q::oDJb;
+  int* sMate = reinterpret_cast<int*>(msm + Q::oIB);
+  int* sSide = sMate + EF;
   const int tid = threadIdx.x, warp = tid >> 5;
   const long long E = t.E, NT = m.NT, e0 = (long long)blockIdx.x * EPB;
-  const int nval = (int)(E - e0 < EPB ? E - e0 : EPB);
+  const int nval = (int)(E - e0 < EPB ? E - e0 : EPB), nuv = nval * NU, nfv = nval * NF;
   const long long gb = t.off + (long long)NF * e0;
   const size_t NFE = (size_t)NF * E, NUE = (size_t)NU * E;
 
-  clear_smem(msm, Q::nB);
+  clear_smem(msm, Q::oUo);
+  __syncthreads();
+  // load phase: asynchronous copies, as in the gradient kernel
+  for (int i = tid; i < F * EF; i += NTH) {
+    const int k = i / EF, r = i - k * EF;
+    if (r >= nfv) continue;
+    const int el = r / NF, f = r - el * NF;
+    cp_async<8>(&sUo[i], UFc + gb + r + NT * k);
+    cp_async<8>(&sJ[(el * F + k) * Q::ldF + f], t.ND + (size_t)NF * e0 + r + NFE * k);
+  }
+  for (int i = tid; i < (F - 1) * EF; i += NTH) {
+    const int k = i / EF, r = i - k * EF;
+    if (r < nfv) cp_async<8>(&sVo[i], m.VF + gb + r + NT * k);
+  }
+  for (int i = tid; i < EF; i += NTH)
+    if (i < nfv) {
+      cp_async<4>(&sMate[i], m.mate + gb + i);
+      cp_async<4>(&sSide[i], m.side + gb + i);
+      cp_async<8>(&sTA[i], m.tdA + gb + i);
+    }
+  for (int i = tid; i < D * EF; i += NTH) {
+    const int d = i / EF, r = i - d * EF;
+    if (r < nfv) cp_async<8>(&sNL[i], m.nL + gb + r + NT * d);
+  }
+  for (int i = tid; i < F * EU; i += NTH) {
+    const int k = i / EU, r = i - k * EU;
+    if (r >= nuv) continue;
+    const size_t ix = (size_t)NU * e0 + r + NUE * k;
+    cp_async<8>(&sDV[i], t.DV + ix);
+    if (MODE == 1) {
+      cp_async<8>(&sRG[i], t.REG + ix);
+      cp_async<8>(&sUO[i], t.U + ix);
+    }
+  }
+  if (MODE == 1)
+    for (int i = tid; i < EU; i += NTH)
+      if (i < nuv) cp_async<8>(&sDJ[i], t.detj + (size_t)NU * e0 + i);
+  cp_async_wait_all();
+  __syncthreads();
+  for (int i = tid; i < F * EF; i += NTH) {
+    const int k = i / EF, r = i - k * EF;
+    if (r >= nfv) continue;
+    const int mt = sMate[r];
+    if (mt < 0) continue;
+    cp_async<8>(&sUN[i], UFc + mt + NT * k);
+    if (k < F - 1) cp_async<8>(&sVN[i], m.VF + mt + NT * k);
+  }
+  cp_async_wait_all();
   __syncthreads();
 
   // common normal fluxes times the own tdA, minus norm_tdisf
-  for (int i = tid; i < nval * NF; i += NTH) {
+  for (int i = tid; i < nfv; i += NTH) {
     const int el = i / NF, f = i - el * NF;
-    const long long g = gb + i;
-    const int mt = m.mate[g], sd = m.side[g];
+    const int mt = sMate[i], sd = sSide[i];
     double n[D], uo[F], c[F];
 #pragma unroll
-    for (int d = 0; d < D; d++) n[d] = m.nL[g + NT * d];
+    for (int d = 0; d < D; d++) n[d] = sNL[d * EF + i];
 #pragma unroll
-    for (int k = 0; k < F; k++) uo[k] = UFc[g + NT * k];
-    const double tl = m.tdA[g];
+    for (int k = 0; k < F; k++) uo[k] = sUo[k * EF + i];
+    const double tl = sTA[i];
     if (sd >> 2) {
       FUBdy<D, double> q;
 #pragma unroll
@@ -466,7 +586,7 @@ __global__ void __launch_bounds__(NTH, MINB) mixed_update_kernel(MixedType t, Mi
       double ul[F], ur[F], fn[F];
 #pragma unroll
       for (int k = 0; k < F; k++) {
-        const double v = UFc[mt + NT * k];
+        const double v = sUN[k * EF + i];
         ul[k] = left ? uo[k] : v;
         ur[k] = left ? v : uo[k];
       }
@@ -479,33 +599,41 @@ __global__ void __launch_bounds__(NTH, MINB) mixed_update_kernel(MixedType t, Mi
       const double pen = ldg_beta<D, double>(ph.pen_fact, n);
 #pragma unroll
       for (int k = 0; k < F; k++) {
-        const double ao = k ? m.VF[g + NT * (k - 1)] : 0.0, an = k ? m.VF[mt + NT * (k - 1)] : 0.0;
+        const double ao = k ? sVo[(k - 1) * EF + i] : 0.0, an = k ? sVN[(k - 1) * EF + i] : 0.0;
         const double fv = ldg_normal<double>(left ? ao : an, left ? an : ao, ul[k], ur[k], pen, ph.tau, nn);
         c[k] = left ? c[k] + fv * tl : c[k] + (-fv) * tl;
       }
     }
-    const size_t gi = f + (size_t)NF * (e0 + el);
 #pragma unroll
-    for (int k = 0; k < F; k++) sJ[(el * F + k) * Q::ldF + f] = c[k] - t.ND[gi + NFE * k];
+    for (int k = 0; k < F; k++) {
+      double* p = sJ + (el * F + k) * Q::ldF + f;
+      *p = c[k] - *p;
+    }
   }
   __syncthreads();
 
   // div_tconf = div_tdisf + opp_3 jump, then the RK45 update
   // (RK45_update_kernel: rhs = -div / detJ)
   {
+    if (MODE == 1)  // padding rows of the new state, read (times zero) by the trace product
+      for (int i = tid; i < Q::NP * (c4(NU) - NU); i += NTH) {
+        const int n = i / (c4(NU) - NU), r = NU + i % (c4(NU) - NU);
+        sUn[n * Q::ldU + r] = 0.0;
+      }
     auto bj = [&](int n) { return sJ + n * Q::ldF; };
     auto one = [&](int r, int n, double v) {
       const int el = n / F, k = n - el * F;
       if (r >= NU || el >= nval) return;
-      const size_t gi = r + (size_t)NU * (e0 + el), ix = gi + NUE * k;
-      const double div = v + t.DV[ix];
+      const int li = k * EU + el * NU + r;
+      const size_t ix = (size_t)NU * e0 + (size_t)el * NU + r + NUE * k;
+      const double div = v + sDV[li];
       if (MODE == 0) {
         t.DIV[ix] = div;
       } else {
-        const double rhs = -div / t.detj[gi] + 0.0 + 0.0;
-        const double res = fma(rk_a, t.REG[ix], dt * rhs);
+        const double rhs = -div / sDJ[el * NU + r] + 0.0 + 0.0;
+        const double res = fma(rk_a, sRG[li], dt * rhs);
         t.REG[ix] = res;
-        const double un = fma(rk_b, res, t.U[ix]);
+        const double un = fma(rk_b, res, sUO[li]);
         t.U[ix] = un;
         sUn[n * Q::ldU + r] = un;
       }
@@ -548,7 +676,7 @@ __global__ void __launch_bounds__(NTH) mixed_trace_kernel(MixedType t, long long
   const long long gb = t.off + (long long)NF * e0;
   clear_smem(msm, Q::nC);
   __syncthreads();
-  load_state<F, NU, Q::ldU>(msm, t.U, e0, E, nval);
+  load_state<F, NU, EPB, Q::ldU, NTH>(msm, t.U, e0, E, nval);
   __syncthreads();
   auto bu = [&](int n) { return msm + n * Q::ldU; };
   auto one = [&](int r, int n, double v) {
@@ -594,17 +722,18 @@ template <int D, int NU, int NF, int V>
 void fill_grad(MixedKernels& k)
 {
   constexpr MixedShape g = kGradShapes[V];
-  k.grad[V] = mixed_grad_kernel<D, NU, NF, g.epb, g.nth, g.minb>;
   k.smem_a[V] = sizeof(double) * MPlan<D, NU, NF, g.epb>::nA;
+  k.grad[V] = k.smem_a[V] <= kMixedSmemMax ? mixed_grad_kernel<D, NU, NF, g.epb, g.nth, g.minb> : nullptr;
 }
 
 template <int D, int NU, int NF, int V>
 void fill_upd(MixedKernels& k)
 {
   constexpr MixedShape u = kUpdShapes[V];
-  k.upd0[V] = mixed_update_kernel<D, NU, NF, u.epb, u.nth, u.minb, 0>;
-  k.upd1[V] = mixed_update_kernel<D, NU, NF, u.epb, u.nth, u.minb, 1>;
   k.smem_b[V] = sizeof(double) * MPlan<D, NU, NF, u.epb>::nB;
+  const bool fits = k.smem_b[V] <= kMixedSmemMax;
+  k.upd0[V] = fits ? mixed_update_kernel<D, NU, NF, u.epb, u.nth, u.minb, 0> : nullptr;
+  k.upd1[V] = fits ? mixed_update_kernel<D, NU, NF, u.epb, u.nth, u.minb, 1> : nullptr;
 }
 
 template <int D, int NU, int NF>
@@ -764,8 +893,13 @@ fr_status set_smem(const MixedKernels& k)
     list.push_back({(const void*)k.upd1[v], k.smem_b[v]});
   }
   list.push_back({(const void*)k.trace, k.smem_c});
+  bool any_grad = false, any_upd = false;
+  for (int v = 0; v < kNGrad; v++) any_grad = any_grad || k.grad[v];
+  for (int v = 0; v < kNUpd; v++) any_upd = any_upd || k.upd1[v];
+  if (!any_grad || !any_upd || k.smem_c > kMixedSmemMax)
+    return mfail(FR_ERR_UNSUPPORTED, "element type too large for one block of shared memory");
   for (auto& q : list) {
-    if (q.second > 227 * 1024) return mfail(FR_ERR_UNSUPPORTED, "element type too large for one block of shared memory");
+    if (!q.first) continue;  // a launch shape whose plan exceeds shared memory
     if (cudaFuncSetAttribute(q.first, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)q.second) != cudaSuccess)
       return mfail(FR_ERR_CUDA, "cudaFuncSetAttribute failed");
   }
@@ -821,8 +955,11 @@ fr_status fr_mixed_stage_create(int n_dims, int n_types, const fr_mixed_stage_ty
                                                 " solution / " + std::to_string(NF) + " flux points"));
     if (fr_status e = set_smem(k)) return bail(e);
     s->kern.push_back(k);
-    s->gv.push_back(0);
-    s->uv.push_back(0);
+    int g0 = 0, u0 = 0;
+    while (!k.grad[g0]) g0++;
+    while (!k.upd1[u0]) u0++;
+    s->gv.push_back(g0);
+    s->uv.push_back(u0);
     off[i + 1] = off[i] + (long long)NF * ty.n_eles;
   }
   s->NT = off[n_types];
@@ -868,7 +1005,8 @@ fr_status fr_mixed_stage_create(int n_dims, int n_types, const fr_mixed_stage_ty
 
   // flux-point space: neighbours, sides, left normals, own tdA
   std::vector<int> mate(NT, 0);
-  std::vector<unsigned char> side(NT, 0), seen(NT, 0);
+  std::vector<int> side(NT, 0);
+  std::vector<unsigned char> seen(NT, 0);
   std::vector<double> nL((size_t)D * NT, 0.0), tdA(NT, 0.0);
   auto gidx = [&](int ty, long long e, int f, long long* g) {
     if (ty < 0 || ty >= n_types || e < 0 || e >= types[ty].n_eles || f < 0 || f >= types[ty].n_fpts) return false;
@@ -913,7 +1051,7 @@ fr_status fr_mixed_stage_create(int n_dims, int n_types, const fr_mixed_stage_ty
       if (seen[g]) return bail(mfail(FR_ERR_MESH, "flux point wired twice"));
       seen[g] = 1;
       mate[g] = (int)(-1 - place);
-      side[g] = (unsigned char)(bt << 2);
+      side[g] = bt << 2;
       for (int d = 0; d < D; d++) nL[g + NT * d] = normal(q[0], q[1], q[2], d);
       place++;
     }
@@ -975,6 +1113,8 @@ fr_status fr_mixed_stage_set_launch(fr_mixed_stage* s, int type, int grad_shape,
   if (!s || type < 0 || type >= s->n_types || grad_shape < 0 || grad_shape >= kNGrad || update_shape < 0 ||
       update_shape >= kNUpd)
     return mfail(FR_ERR_ARG, "bad type or launch shape");
+  if (!s->kern[type].grad[grad_shape] || !s->kern[type].upd1[update_shape])
+    return mfail(FR_ERR_UNSUPPORTED, "launch shape exceeds shared memory for this element type");
   s->gv[type] = grad_shape;
   s->uv[type] = update_shape;
   return FR_OK;
@@ -1012,9 +1152,11 @@ fr_status fr_mixed_stage_autotune(fr_mixed_stage* s, void* stream)
     s->types[i].DIV = scratch;
     for (int pass = 0; pass < 2 && rc == FR_OK; pass++) {
       const int nv = pass == 0 ? kNGrad : kNUpd;
-      int pick = 0;
+      int pick = pass == 0 ? s->gv[i] : s->uv[i];
       float best = 0.f;
+      bool have = false;
       for (int v = 0; v < nv && rc == FR_OK; v++) {
+        if (pass == 0 ? !s->kern[i].grad[v] : !s->kern[i].upd0[v]) continue;
         // one untimed launch, then the timed ones
         for (int r = 0; r <= reps && rc == FR_OK; r++) {
           if (r == 1) cudaEventRecord(e0, st);
@@ -1024,9 +1166,10 @@ fr_status fr_mixed_stage_autotune(fr_mixed_stage* s, void* stream)
         if (cudaEventSynchronize(e1) != cudaSuccess) rc = mfail(FR_ERR_CUDA, "autotune timing failed");
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
-        if (v == 0 || ms < best) {
+        if (!have || ms < best) {
           best = ms;
           pick = v;
+          have = true;
         }
       }
       (pass == 0 ? s->gv : s->uv)[i] = pick;
