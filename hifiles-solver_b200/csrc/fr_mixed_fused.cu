@@ -34,8 +34,8 @@
 // column-major matrices, one column per (element, field[, dimension]), whose
 // leading dimension is 4 or 12 mod 16 doubles so that a fragment load hits
 // 16 distinct banks per half-warp.  Padding rows of the operators are zero
-// and every padding row of the data is finite (shared memory is cleared at
-// the start of a block), so padded products add exact zeros.
+// and every padding row of the data that a product reads is set to zero, so
+// padded products add exact zeros.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -199,10 +199,15 @@ __host__ __device__ constexpr int units(int mt)
   return mt * ((NTL + TN - 1) / TN);
 }
 
-__device__ __forceinline__ void clear_smem(double* s, int n)
+// zero rows r0 .. r1 - 1 of the first ncol columns of a column-major matrix:
+// the padding rows a product reads (times the operator's zero columns), which
+// must hold finite values
+template <int R0, int R1, int LD, int NCOL, int NTH>
+__device__ __forceinline__ void zero_pad_rows(double* a)
 {
-  double2* q = reinterpret_cast<double2*>(s);
-  for (int i = threadIdx.x; i < n / 2; i += blockDim.x) q[i] = make_double2(0.0, 0.0);
+  constexpr int W = R1 - R0;
+  if constexpr (W > 0)
+    for (int i = threadIdx.x; i < NCOL * W; i += NTH) a[(i / W) * LD + R0 + i % W] = 0.0;
 }
 
 // the block's state into columns (element, field) of sU (rows = solution points)
@@ -210,12 +215,14 @@ template <int F, int NU, int EPB, int ldU, int NTH>
 __device__ __forceinline__ void load_state(double* sU, const double* __restrict__ U, long long e0, long long E,
                                            int nval)
 {
-  constexpr int EU = EPB * NU;
-  for (int i = threadIdx.x; i < F * EU; i += NTH) {
-    const int k = i / EU, r = i - k * EU;
-    if (r >= nval * NU) continue;
+  const int nuv = nval * NU;
+  const size_t NUE = (size_t)NU * E;
+  for (int r = threadIdx.x; r < nuv; r += NTH) {
     const int el = r / NU, p = r - el * NU;
-    sU[(el * F + k) * ldU + p] = U[(size_t)NU * e0 + (size_t)NU * E * k + r];
+    double* dst = sU + el * F * ldU + p;
+    const double* src = U + (size_t)NU * e0 + r;
+#pragma unroll
+    for (int k = 0; k < F; k++) cp_async<8>(dst + k * ldU, src + NUE * k);
   }
 }
 
@@ -246,45 +253,40 @@ __global__ void __launch_bounds__(NTH, MINB) mixed_grad_kernel(MixedType t, Mixe
   const int nval = (int)(E - e0 < EPB ? E - e0 : EPB), nuv = nval * NU, nfv = nval * NF;
   const long long gb = t.off + (long long)NF * e0;
 
-  clear_smem(msm, Q::oNL);
-  __syncthreads();
   // load phase: asynchronous copies (cp.async), many in flight per thread;
   // first everything at known addresses, then the neighbours' traces through
-  // the staged mate
-  for (int i = tid; i < F * EU; i += NTH) {
-    const int k = i / EU, r = i - k * EU;
-    if (r >= nuv) continue;
-    const int el = r / NU, p = r - el * NU;
-    cp_async<8>(&sU[(el * F + k) * Q::ldU + p], t.U + (size_t)NU * e0 + (size_t)NU * E * k + r);
-  }
-  for (int i = tid; i < F * EF; i += NTH) {
-    const int k = i / EF, r = i - k * EF;
-    if (r >= nfv) continue;
+  // the staged mate.  The matrices are not cleared: only the padding rows
+  // the products read are zeroed (U here, delta and the flux before their
+  // products); every other padding entry only reaches outputs that are not
+  // written.
+  zero_pad_rows<NU, c4(NU), Q::ldU, Q::NP, NTH>(sU);
+  load_state<F, NU, EPB, Q::ldU, NTH>(sU, t.U, e0, E, nval);
+  for (int r = tid; r < nfv; r += NTH) {
     const int el = r / NF, f = r - el * NF;
-    cp_async<8>(&sUF[(el * F + k) * Q::ldF + f], UFc + gb + r + NT * k);
+    const long long g = gb + r;
+    double* dst = sUF + el * F * Q::ldF + f;
+#pragma unroll
+    for (int k = 0; k < F; k++) cp_async<8>(dst + k * Q::ldF, UFc + g + NT * k);
+#pragma unroll
+    for (int d = 0; d < D; d++) cp_async<8>(&sNL[d * EF + r], m.nL + g + NT * d);
+    cp_async<4>(&sMate[r], m.mate + g);
+    cp_async<4>(&sSide[r], m.side + g);
   }
-  for (int i = tid; i < EF; i += NTH)
-    if (i < nfv) {
-      cp_async<4>(&sMate[i], m.mate + gb + i);
-      cp_async<4>(&sSide[i], m.side + gb + i);
-    }
-  for (int i = tid; i < D * EF; i += NTH) {
-    const int d = i / EF, r = i - d * EF;
-    if (r < nfv) cp_async<8>(&sNL[i], m.nL + gb + r + NT * d);
+  for (int i = tid; i < nuv; i += NTH) {
+    cp_async<8>(&sDJ[i], t.detj + (size_t)NU * e0 + i);
+    if constexpr (Q::SJ)
+#pragma unroll
+      for (int q = 0; q < DD; q++) cp_async<8>(&sJG[i + q * nuv], t.JG + (size_t)DD * NU * e0 + i + q * nuv);
   }
-  for (int i = tid; i < EU; i += NTH)
-    if (i < nuv) cp_async<8>(&sDJ[i], t.detj + (size_t)NU * e0 + i);
-  if constexpr (Q::SJ)
-    for (int i = tid; i < DD * EU; i += NTH)
-      if (i < DD * nuv) cp_async<8>(&sJG[i], t.JG + (size_t)DD * NU * e0 + i);
   cp_async_wait_all();
   __syncthreads();
-  for (int i = tid; i < F * EF; i += NTH) {
-    const int k = i / EF, r = i - k * EF;
-    if (r >= nfv) continue;
+  for (int r = tid; r < nfv; r += NTH) {
     const int mt = sMate[r];
-    if (mt >= 0) cp_async<8>(&sUN[i], UFc + mt + NT * k);
+    if (mt < 0) continue;
+#pragma unroll
+    for (int k = 0; k < F; k++) cp_async<8>(&sUN[k * EF + r], UFc + mt + NT * k);
   }
+  zero_pad_rows<NF, c4(NF), Q::ldF, Q::NP, NTH>(sX);  // delta's padding rows
   cp_async_wait_all();
   __syncthreads();
   auto jg = [&](int i) { return Q::SJ ? sJG + DD * i : t.JG + (size_t)DD * ((size_t)NU * e0 + i); };
@@ -409,6 +411,7 @@ __global__ void __launch_bounds__(NTH, MINB) mixed_grad_kernel(MixedType t, Mixe
   }
   __syncthreads();
 
+  zero_pad_rows<D * NU, c4(D * NU), Q::ldT, Q::NP, NTH>(sX);  // the flux's padding rows
   // transformed flux at the solution points (evaluate_invFlux, then
   // evaluate_viscFlux adding to it): rows (d, point) of X.  The viscous flux
   // takes one reciprocal of rho (vis_flux_fast): its terms are ~1/Re of the
@@ -510,52 +513,47 @@ __global__ void __launch_bounds__(NTH, MINB) mixed_update_kernel(MixedType t, Mi
   const long long gb = t.off + (long long)NF * e0;
   const size_t NFE = (size_t)NF * E, NUE = (size_t)NU * E;
 
-  clear_smem(msm, Q::oUo);
-  __syncthreads();
   // load phase: asynchronous copies, as in the gradient kernel
-  for (int i = tid; i < F * EF; i += NTH) {
-    const int k = i / EF, r = i - k * EF;
-    if (r >= nfv) continue;
+  zero_pad_rows<NF, c4(NF), Q::ldF, Q::NP, NTH>(sJ);
+  for (int r = tid; r < nfv; r += NTH) {
     const int el = r / NF, f = r - el * NF;
-    cp_async<8>(&sUo[i], UFc + gb + r + NT * k);
-    cp_async<8>(&sJ[(el * F + k) * Q::ldF + f], t.ND + (size_t)NF * e0 + r + NFE * k);
-  }
-  for (int i = tid; i < (F - 1) * EF; i += NTH) {
-    const int k = i / EF, r = i - k * EF;
-    if (r < nfv) cp_async<8>(&sVo[i], m.VF + gb + r + NT * k);
-  }
-  for (int i = tid; i < EF; i += NTH)
-    if (i < nfv) {
-      cp_async<4>(&sMate[i], m.mate + gb + i);
-      cp_async<4>(&sSide[i], m.side + gb + i);
-      cp_async<8>(&sTA[i], m.tdA + gb + i);
+    const long long g = gb + r;
+    double* dj = sJ + el * F * Q::ldF + f;
+    const double* nd = t.ND + (size_t)NF * e0 + r;
+#pragma unroll
+    for (int k = 0; k < F; k++) {
+      cp_async<8>(&sUo[k * EF + r], UFc + g + NT * k);
+      cp_async<8>(dj + k * Q::ldF, nd + NFE * k);
     }
-  for (int i = tid; i < D * EF; i += NTH) {
-    const int d = i / EF, r = i - d * EF;
-    if (r < nfv) cp_async<8>(&sNL[i], m.nL + gb + r + NT * d);
+#pragma unroll
+    for (int k = 0; k < F - 1; k++) cp_async<8>(&sVo[k * EF + r], m.VF + g + NT * k);
+#pragma unroll
+    for (int d = 0; d < D; d++) cp_async<8>(&sNL[d * EF + r], m.nL + g + NT * d);
+    cp_async<4>(&sMate[r], m.mate + g);
+    cp_async<4>(&sSide[r], m.side + g);
+    cp_async<8>(&sTA[r], m.tdA + g);
   }
-  for (int i = tid; i < F * EU; i += NTH) {
-    const int k = i / EU, r = i - k * EU;
-    if (r >= nuv) continue;
-    const size_t ix = (size_t)NU * e0 + r + NUE * k;
-    cp_async<8>(&sDV[i], t.DV + ix);
-    if (MODE == 1) {
-      cp_async<8>(&sRG[i], t.REG + ix);
-      cp_async<8>(&sUO[i], t.U + ix);
+  for (int r = tid; r < nuv; r += NTH) {
+    const size_t ix = (size_t)NU * e0 + r;
+#pragma unroll
+    for (int k = 0; k < F; k++) {
+      cp_async<8>(&sDV[k * EU + r], t.DV + ix + NUE * k);
+      if (MODE == 1) {
+        cp_async<8>(&sRG[k * EU + r], t.REG + ix + NUE * k);
+        cp_async<8>(&sUO[k * EU + r], t.U + ix + NUE * k);
+      }
     }
+    if (MODE == 1) cp_async<8>(&sDJ[r], t.detj + ix);
   }
-  if (MODE == 1)
-    for (int i = tid; i < EU; i += NTH)
-      if (i < nuv) cp_async<8>(&sDJ[i], t.detj + (size_t)NU * e0 + i);
   cp_async_wait_all();
   __syncthreads();
-  for (int i = tid; i < F * EF; i += NTH) {
-    const int k = i / EF, r = i - k * EF;
-    if (r >= nfv) continue;
+  for (int r = tid; r < nfv; r += NTH) {
     const int mt = sMate[r];
     if (mt < 0) continue;
-    cp_async<8>(&sUN[i], UFc + mt + NT * k);
-    if (k < F - 1) cp_async<8>(&sVN[i], m.VF + mt + NT * k);
+#pragma unroll
+    for (int k = 0; k < F; k++) cp_async<8>(&sUN[k * EF + r], UFc + mt + NT * k);
+#pragma unroll
+    for (int k = 0; k < F - 1; k++) cp_async<8>(&sVN[k * EF + r], m.VF + mt + NT * k);
   }
   cp_async_wait_all();
   __syncthreads();
@@ -674,9 +672,9 @@ __global__ void __launch_bounds__(NTH) mixed_trace_kernel(MixedType t, long long
   const long long E = t.E, e0 = (long long)blockIdx.x * EPB;
   const int nval = (int)(E - e0 < EPB ? E - e0 : EPB);
   const long long gb = t.off + (long long)NF * e0;
-  clear_smem(msm, Q::nC);
-  __syncthreads();
+  zero_pad_rows<NU, c4(NU), Q::ldU, Q::NP, NTH>(msm);
   load_state<F, NU, EPB, Q::ldU, NTH>(msm, t.U, e0, E, nval);
+  cp_async_wait_all();
   __syncthreads();
   auto bu = [&](int n) { return msm + n * Q::ldU; };
   auto one = [&](int r, int n, double v) {
