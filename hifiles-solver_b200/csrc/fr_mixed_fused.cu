@@ -801,9 +801,17 @@ struct fr_mixed_stage {
   MixedFpts fp{};
   double* UF[2] = {nullptr, nullptr};
   int cur = 0;
+  // element types after the first run on side streams, forked from and
+  // joined to the caller's stream around each kernel of a stage
+  bool concurrent = true;
+  std::vector<cudaStream_t> side_streams;
+  std::vector<cudaEvent_t> fork_ev, join_ev;
   ~fr_mixed_stage()
   {
     for (void* p : allocs) cudaFree(p);
+    for (cudaStream_t q : side_streams) cudaStreamDestroy(q);
+    for (cudaEvent_t e : fork_ev) cudaEventDestroy(e);
+    for (cudaEvent_t e : join_ev) cudaEventDestroy(e);
   }
   template <class T>
   fr_status upload(const std::vector<T>& h, const T** out)
@@ -835,16 +843,6 @@ namespace {
 
 unsigned blocks_of(long long E, int epb) { return (unsigned)((E + epb - 1) / epb); }
 
-fr_status launch_trace(fr_mixed_stage* s, cudaStream_t st)
-{
-  for (int i = 0; i < s->n_types; i++) {
-    const MixedType& t = s->types[i];
-    if (t.E == 0) continue;
-    s->kern[i].trace<<<blocks_of(t.E, kMixedEPB), kMixedNT, s->kern[i].smem_c, st>>>(t, s->NT, s->UF[s->cur]);
-    if (fr_status e = mlaunched("mixed_trace_kernel")) return e;
-  }
-  return FR_OK;
-}
 
 fr_status launch_grad(fr_mixed_stage* s, int i, int v, const double* UFc, cudaStream_t st)
 {
@@ -867,17 +865,50 @@ fr_status launch_upd(fr_mixed_stage* s, int i, int v, int mode, int stage, doubl
   return mlaunched("mixed_update_kernel");
 }
 
+// the kernels of every element type, types after the first on their side
+// streams when concurrent (fork from st, join back into st)
+template <class Launch>
+fr_status for_types(fr_mixed_stage* s, cudaStream_t st, Launch launch)
+{
+  const bool par = s->concurrent && s->n_types > 1;
+  if (par) {
+    if (cudaEventRecord(s->fork_ev[0], st) != cudaSuccess) return mfail(FR_ERR_CUDA, "event record failed");
+    for (size_t j = 0; j < s->side_streams.size(); j++)
+      if (cudaStreamWaitEvent(s->side_streams[j], s->fork_ev[0], 0) != cudaSuccess)
+        return mfail(FR_ERR_CUDA, "stream wait failed");
+  }
+  for (int i = 0; i < s->n_types; i++) {
+    if (s->types[i].E == 0) continue;
+    if (fr_status e = launch(i, par && i > 0 ? s->side_streams[i - 1] : st)) return e;
+  }
+  if (par)
+    for (size_t j = 0; j < s->side_streams.size(); j++) {
+      if (cudaEventRecord(s->join_ev[j], s->side_streams[j]) != cudaSuccess ||
+          cudaStreamWaitEvent(st, s->join_ev[j], 0) != cudaSuccess)
+        return mfail(FR_ERR_CUDA, "stream join failed");
+    }
+  return FR_OK;
+}
+
+fr_status launch_trace(fr_mixed_stage* s, cudaStream_t st)
+{
+  return for_types(s, st, [&](int i, cudaStream_t q) {
+    const MixedType& t = s->types[i];
+    s->kern[i].trace<<<blocks_of(t.E, kMixedEPB), kMixedNT, s->kern[i].smem_c, q>>>(t, s->NT, s->UF[s->cur]);
+    return mlaunched("mixed_trace_kernel");
+  });
+}
+
 // one CalcResidual (+ the RK45 update of stage `stage` when mode is 1)
 fr_status launch_stage(fr_mixed_stage* s, int mode, int stage, double dt, cudaStream_t st)
 {
   const double* UFc = s->UF[s->cur];
   double* UFn = s->UF[s->cur ^ 1];
-  for (int i = 0; i < s->n_types; i++)
-    if (s->types[i].E > 0)
-      if (fr_status e = launch_grad(s, i, s->gv[i], UFc, st)) return e;
-  for (int i = 0; i < s->n_types; i++)
-    if (s->types[i].E > 0)
-      if (fr_status e = launch_upd(s, i, s->uv[i], mode, stage, dt, UFc, UFn, st)) return e;
+  if (fr_status e = for_types(s, st, [&](int i, cudaStream_t q) { return launch_grad(s, i, s->gv[i], UFc, q); }))
+    return e;
+  if (fr_status e = for_types(
+          s, st, [&](int i, cudaStream_t q) { return launch_upd(s, i, s->uv[i], mode, stage, dt, UFc, UFn, q); }))
+    return e;
   if (mode) s->cur ^= 1;
   return FR_OK;
 }
@@ -1071,6 +1102,19 @@ fr_status fr_mixed_stage_create(int n_dims, int n_types, const fr_mixed_stage_ty
   if (fr_status e = s->zeros((size_t)F * (place ? place : 1), &s->fp.BV)) return bail(e);
   if (fr_status e = s->zeros((size_t)F * NT, &s->UF[0])) return bail(e);
   if (fr_status e = s->zeros((size_t)F * NT, &s->UF[1])) return bail(e);
+  s->fork_ev.resize(1, nullptr);
+  if (cudaEventCreateWithFlags(&s->fork_ev[0], cudaEventDisableTiming) != cudaSuccess)
+    return bail(mfail(FR_ERR_CUDA, "event creation failed"));
+  for (int i = 1; i < n_types; i++) {
+    cudaStream_t q;
+    cudaEvent_t ev;
+    if (cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking) != cudaSuccess)
+      return bail(mfail(FR_ERR_CUDA, "stream creation failed"));
+    s->side_streams.push_back(q);
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+      return bail(mfail(FR_ERR_CUDA, "event creation failed"));
+    s->join_ev.push_back(ev);
+  }
   *out = s;
   return FR_OK;
 }
@@ -1115,6 +1159,14 @@ fr_status fr_mixed_stage_set_launch(fr_mixed_stage* s, int type, int grad_shape,
     return mfail(FR_ERR_UNSUPPORTED, "launch shape exceeds shared memory for this element type");
   s->gv[type] = grad_shape;
   s->uv[type] = update_shape;
+  return FR_OK;
+}
+
+fr_status fr_mixed_stage_set_concurrent(fr_mixed_stage* s, int on)
+{
+  g_err.clear();
+  if (!s) return mfail(FR_ERR_ARG, "null stage");
+  s->concurrent = on != 0;
   return FR_OK;
 }
 

@@ -419,9 +419,10 @@ def _bind_stage(L):
     L.fr_mixed_stage_set_launch.argtypes = [vp, i, i, i]
     L.fr_mixed_stage_get_launch.argtypes = [vp, i, C.POINTER(i), C.POINTER(i)]
     L.fr_mixed_stage_autotune.argtypes = [vp, vp]
+    L.fr_mixed_stage_set_concurrent.argtypes = [vp, i]
     for f in ("fr_mixed_stage_create", "fr_mixed_stage_destroy", "fr_mixed_stage_residual", "fr_mixed_stage_advance",
               "fr_mixed_stage_info", "fr_mixed_stage_set_launch", "fr_mixed_stage_get_launch",
-              "fr_mixed_stage_autotune"):
+              "fr_mixed_stage_autotune", "fr_mixed_stage_set_concurrent"):
         getattr(L, f).restype = C.c_int
     return L
 
@@ -533,6 +534,10 @@ class FusedMixedMesh:
 
     def set_launch(self, i, grad_shape, update_shape):
         _check(self.L.fr_mixed_stage_set_launch(self.h, self._pos[i], int(grad_shape), int(update_shape)))
+
+    def set_concurrent(self, on):
+        """Element types on side streams (True, default) or all on one stream."""
+        _check(self.L.fr_mixed_stage_set_concurrent(self.h, int(bool(on))))
 
     def autotune(self):
         """Time every launch shape on the current state, keep the fastest."""

@@ -696,6 +696,11 @@ fr_status fr_mixed_stage_advance(fr_mixed_stage* s, int n_steps, double dt, void
 fr_status fr_mixed_stage_set_launch(fr_mixed_stage* s, int type, int grad_shape, int update_shape);
 fr_status fr_mixed_stage_get_launch(const fr_mixed_stage* s, int type, int* grad_shape, int* update_shape);
 fr_status fr_mixed_stage_autotune(fr_mixed_stage* s, void* stream);
+/* on (default): the kernels of element types after the first run on side
+ * streams of the stage, forked from and joined back into the caller's stream
+ * around each kernel of a stage, so small types overlap large ones; off: all
+ * on the caller's stream.  Same bits either way. */
+fr_status fr_mixed_stage_set_concurrent(fr_mixed_stage* s, int on);
 /* Flux points over all types, boundary points, kernel launches per stage. */
 fr_status fr_mixed_stage_info(const fr_mixed_stage* s, long long* n_flux_points, long long* n_boundary_points,
                               int* launches_per_stage);

@@ -151,8 +151,9 @@ def test_fused_stage_rejects_unsupported_meshes():
 
 @pytest.mark.gpu
 def test_fused_launch_shapes_give_the_same_bits():
-    """Every launch shape of the two stage kernels ends on the same state bit
-    for bit; autotune() leaves the state as it was."""
+    """Every launch shape of the two stage kernels, and one stream instead of
+    side streams per element type, end on the same state bit for bit;
+    autotune() leaves the state as it was."""
     torch = pytest.importorskip("torch")
     from hifiles_b200 import seam
     meta, a = load("mixed_channel_p3")
@@ -165,6 +166,10 @@ def test_fused_launch_shapes_give_the_same_bits():
             assert m.launch(i) == shapes
         m.advance(2, meta["dt"])
         out[shapes] = {i: m.get_state(i) for i in m.S}
+    m = seam.FusedMixedMesh(types, ints, meta["physics"], bdys, meta["bdy"], meta["R_ref"])
+    m.set_concurrent(False)
+    m.advance(2, meta["dt"])
+    out["one stream"] = {i: m.get_state(i) for i in m.S}
     for shapes, st in out.items():
         for i in st:
             assert np.array_equal(st[i], out[(0, 0)][i]), shapes
