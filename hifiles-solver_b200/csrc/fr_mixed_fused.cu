@@ -85,7 +85,7 @@ __host__ __device__ constexpr int tiles_per_unit(int ntl)
 constexpr size_t kMixedSmemMax = 227 * 1024;  // dynamic shared memory of one block
 __host__ __device__ constexpr int r2(int x) { return (x + 1) / 2 * 2; }  // 16-byte region starts
 
-template <int D, int NU, int NF, int EPB>
+template <int D, int NU, int NF, int EPB, int MINB = 1>
 struct MPlan {
   static constexpr int F = D + 2, DD = D * D, EU = EPB * NU, EF = EPB * NF;
   static constexpr int N = EPB * F, NP = c8(N);          // (element, field) columns
@@ -106,7 +106,11 @@ struct MPlan {
   static constexpr int oU = 0, oUF = oU + NP * ldU, oG = oUF + NP * ldF, oX = oG + NP * ldG;
   static constexpr int nX = cmax(cmax(NP * ldF, NGP * ldF), NP * ldT);
   static constexpr int oNL = oX + r2(nX), oDJ = oNL + r2(D * EF), oJG = oDJ + r2(EU);
-  static constexpr bool SJ = sizeof(double) * (size_t)(oJG + r2(DD * EU) + EF) <= kMixedSmemMax;
+  // JGinv is staged when MINB blocks with it fit in an SM's shared memory
+  // (228 KB, 1 KB reserved per block), else read through the L1 cache
+  static constexpr bool SJ = (size_t)MINB * (sizeof(double) * (size_t)(oJG + r2(DD * EU) + r2(EF)) + 1024) <=
+                                 228 * 1024 &&
+                             sizeof(double) * (size_t)(oJG + r2(DD * EU) + r2(EF)) <= kMixedSmemMax;
   static constexpr int oIA = oJG + (SJ ? r2(DD * EU) : 0);
   static constexpr int nA = oIA + r2(EF);
   // kernel B: the jump norm_tconf - norm_tdisf (norm_tdisf first) | own traces
@@ -235,7 +239,7 @@ template <int D, int NU, int NF, int EPB, int NTH, int MINB>
 __global__ void __launch_bounds__(NTH, MINB) mixed_grad_kernel(MixedType t, MixedFpts m,
                                                                const double* __restrict__ UFc, PhysT<double> ph)
 {
-  using Q = MPlan<D, NU, NF, EPB>;
+  using Q = MPlan<D, NU, NF, EPB, MINB>;
   constexpr int F = D + 2, NW = NTH / 32, DD = D * D, EU = Q::EU, EF = Q::EF;
   extern __shared__ __align__(16) double msm[];
   double* sU = msm + Q::oU;
@@ -697,7 +701,7 @@ __global__ void __launch_bounds__(NTH) mixed_trace_kernel(MixedType t, long long
 struct MixedShape {
   int epb, nth, minb;
 };
-constexpr MixedShape kGradShapes[] = {{8, 256, 1}, {4, 128, 3}, {8, 128, 2}};
+constexpr MixedShape kGradShapes[] = {{8, 256, 1}, {4, 128, 3}, {8, 128, 2}, {4, 128, 4}};
 constexpr MixedShape kUpdShapes[] = {{8, 256, 2}, {4, 128, 4}, {8, 128, 4}};
 constexpr int kNGrad = sizeof(kGradShapes) / sizeof(kGradShapes[0]);
 constexpr int kNUpd = sizeof(kUpdShapes) / sizeof(kUpdShapes[0]);
@@ -720,7 +724,7 @@ template <int D, int NU, int NF, int V>
 void fill_grad(MixedKernels& k)
 {
   constexpr MixedShape g = kGradShapes[V];
-  k.smem_a[V] = sizeof(double) * MPlan<D, NU, NF, g.epb>::nA;
+  k.smem_a[V] = sizeof(double) * MPlan<D, NU, NF, g.epb, g.minb>::nA;
   k.grad[V] = k.smem_a[V] <= kMixedSmemMax ? mixed_grad_kernel<D, NU, NF, g.epb, g.nth, g.minb> : nullptr;
 }
 
@@ -744,10 +748,11 @@ MixedKernels mixed_kernels()
   fill_grad<D, NU, NF, 0>(k);
   fill_grad<D, NU, NF, 1>(k);
   fill_grad<D, NU, NF, 2>(k);
+  fill_grad<D, NU, NF, 3>(k);
   fill_upd<D, NU, NF, 0>(k);
   fill_upd<D, NU, NF, 1>(k);
   fill_upd<D, NU, NF, 2>(k);
-  static_assert(kNGrad == 3 && kNUpd == 3, "one fill per shape");
+  static_assert(kNGrad == 4 && kNUpd == 3, "one fill per shape");
   k.trace = mixed_trace_kernel<D, NU, NF, kMixedEPB, kMixedNT>;
   k.smem_c = sizeof(double) * MPlan<D, NU, NF, kMixedEPB>::nC;
   return k;
