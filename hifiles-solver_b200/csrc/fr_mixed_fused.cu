@@ -701,7 +701,7 @@ __global__ void __launch_bounds__(NTH) mixed_trace_kernel(MixedType t, long long
 struct MixedShape {
   int epb, nth, minb;
 };
-constexpr MixedShape kGradShapes[] = {{8, 256, 1}, {4, 128, 3}, {8, 128, 2}, {4, 128, 4}};
+constexpr MixedShape kGradShapes[] = {{8, 256, 1}, {4, 128, 3}, {8, 128, 2}, {4, 128, 4}, {8, 256, 2}};
 constexpr MixedShape kUpdShapes[] = {{8, 256, 2}, {4, 128, 4}, {8, 128, 4}};
 constexpr int kNGrad = sizeof(kGradShapes) / sizeof(kGradShapes[0]);
 constexpr int kNUpd = sizeof(kUpdShapes) / sizeof(kUpdShapes[0]);
@@ -749,10 +749,11 @@ MixedKernels mixed_kernels()
   fill_grad<D, NU, NF, 1>(k);
   fill_grad<D, NU, NF, 2>(k);
   fill_grad<D, NU, NF, 3>(k);
+  fill_grad<D, NU, NF, 4>(k);
   fill_upd<D, NU, NF, 0>(k);
   fill_upd<D, NU, NF, 1>(k);
   fill_upd<D, NU, NF, 2>(k);
-  static_assert(kNGrad == 4 && kNUpd == 3, "one fill per shape");
+  static_assert(kNGrad == 5 && kNUpd == 3, "one fill per shape");
   k.trace = mixed_trace_kernel<D, NU, NF, kMixedEPB, kMixedNT>;
   k.smem_c = sizeof(double) * MPlan<D, NU, NF, kMixedEPB>::nC;
   return k;

@@ -687,7 +687,8 @@ fr_status fr_mixed_stage_residual(fr_mixed_stage* s, void* stream);
 fr_status fr_mixed_stage_advance(fr_mixed_stage* s, int n_steps, double dt, void* stream);
 /* Launch shapes of each type's two stage kernels: gradient 0 = 8 elements x
  * 256 threads, 1 = 4 x 128, 2 = 8 x 128, 3 = 4 x 128 with registers for 4
- * blocks per SM; update 0 = 8 x 256, 1 = 4 x 128,
+ * blocks per SM, 4 = 8 x 256 with registers for 2; update 0 = 8 x 256,
+ * 1 = 4 x 128,
  * 2 = 8 x 128 (every shape gives the same bits; shapes whose shared memory
  * exceeds a block's return FR_ERR_UNSUPPORTED).  create() sets the first shape
  * that fits;

@@ -159,7 +159,7 @@ def test_fused_launch_shapes_give_the_same_bits():
     meta, a = load("mixed_channel_p3")
     types, ints, bdys = seam.mixed_mesh_inputs(meta, a)
     out = {}
-    for shapes in ((0, 0), (1, 1), (2, 2), (3, 0), (1, 0), (0, 2)):
+    for shapes in ((0, 0), (1, 1), (2, 2), (3, 0), (4, 1), (1, 0), (0, 2)):
         m = seam.FusedMixedMesh(types, ints, meta["physics"], bdys, meta["bdy"], meta["R_ref"])
         for i in m.S:
             m.set_launch(i, *shapes)
@@ -179,4 +179,4 @@ def test_fused_launch_shapes_give_the_same_bits():
     torch.cuda.synchronize()
     for i in m.S:
         assert np.array_equal(m.get_state(i), before[i])
-        assert 0 <= picked[i][0] < 4 and 0 <= picked[i][1] < 3
+        assert 0 <= picked[i][0] < 5 and 0 <= picked[i][1] < 3
