@@ -404,6 +404,32 @@ def measure_mixed_channel(order, n=(40, 20, 20), steps=3, err_steps=10, dt=2e-4)
     return res
 
 
+def measure_channel_fused(order, steps, warmup, n=(40, 20, 20), dt=2e-4, shapes=None):
+    """The channel of measure_mixed_channel through the fused stage alone
+    (fr_mixed_stage_*): launch shapes autotuned, or `shapes` ("g,u" for every
+    element type) for profile captures."""
+    import torch
+    from hifiles_b200 import mixed as X
+    from hifiles_b200 import seam
+    xv, cells, period, bfaces = X.channel_mesh(n)
+    M = X.MixedMesh(order, xv, cells, period, bfaces,
+                    X.ElementOpts(vcjh_scheme_tet=2, vcjh_scheme_tri=1, vcjh_scheme_pri_1d=1))
+    types, ints, bdys = M.operator_inputs({t: channel_state(m["pos_upts"]) for t, m in M.types.items()})
+    f = seam.FusedMixedMesh(types, ints, CHANNEL_PHYSICS, bdys, CHANNEL_BDY, CHANNEL_R_REF)
+    if shapes:
+        g, u = (int(v) for v in shapes.split(","))
+        for i in f.S:
+            f.set_launch(i, g, u)
+    else:
+        f.autotune()
+    f.advance(warmup, dt)
+    ms = _time_steps(lambda k: f.advance(k, dt), f.stream, steps)
+    return {"workload": "channel %s order %d, fused stage" % ("x".join(str(v) for v in n), order),
+            "n_eles": {str(t): int(m["n_eles"]) for t, m in M.types.items()}, "dofs": f.dofs,
+            "ms_per_step": ms, "value": f.dofs * 5 / (ms * 1e-3), "unit": "DOF-updates/s",
+            "launch_shapes": {str(i): list(f.launch(i)) for i in f.S}, "launches_per_stage": f.launches_per_stage}
+
+
 def measure_tgv64_p4(dev, n=64, P=4, steps=100, dt=2e-4):
     """The precision sweep on TGV 64^3 hexes at P = 4 (32.8 M points x 5
     fields, 1.3 GB per FP64 state): FP64 and FP32 forms of the fused path,
@@ -662,7 +688,15 @@ def main():
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--tiles", default="", help="gradient,update tile indices instead of autotuning (for captures)")
     ap.add_argument("--no-forms", action="store_true", help="skip the FP32 and batched forms")
+    ap.add_argument("--channel-fused", type=int, default=0, metavar="P",
+                    help="only the 40x20x20 tet/prism channel of order P through the fused stage (one JSON line)")
+    ap.add_argument("--shapes", default="", help="with --channel-fused: gradient,update launch shapes")
+    ap.add_argument("--channel-n", default="40,20,20", help="with --channel-fused: cells in x, y, z")
     a = ap.parse_args()
+    if a.channel_fused:
+        n = tuple(int(v) for v in a.channel_n.split(","))
+        print(json.dumps(measure_channel_fused(a.channel_fused, a.steps, a.warmup, n=n, shapes=a.shapes or None)))
+        return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
