@@ -322,8 +322,9 @@ def measure_mixed_channel(order, n=(40, 20, 20), steps=3, err_steps=10, dt=2e-4)
     per core cell, periodic in x and z, an isothermal wall at y = 0 and an
     adiabatic one at y = 2 on the prisms' triangular faces.  Set up by the
     library (operators, metrics, wiring: hifiles_b200.mixed) and advanced
-    through the fr_op_* entry points with FP64 operator products on the CUDA
-    cores and BF16x3 / BF16x6 split products on the tensor cores, with their
+    through the fr_op_* entry points with FP64 operator products on the FP64
+    tensor cores (fp64) or the CUDA cores and BF16x3 / BF16x6 split products
+    on the tcgen05 tensor cores, with their
     L2 error against FP64 after `err_steps` steps; and by the fused stage
     (fr_mixed_stage_*, FP64 tensor-core products), against the per-operator
     FP64 path."""
@@ -345,7 +346,7 @@ def measure_mixed_channel(order, n=(40, 20, 20), steps=3, err_steps=10, dt=2e-4)
             s["reg"].zero_()
 
     res = {}
-    for mode, name in ((0, "fp64"), (1, "bf16x3"), (2, "bf16x6")):
+    for mode, name in ((0, "fp64"), (3, "fp64_cuda_cores"), (1, "bf16x3"), (2, "bf16x6")):
         reset()
         m.advance(1, dt, gemm_precision=mode)
         ms = _time_steps(lambda k: m.advance(k, dt, gemm_precision=mode), m.stream, steps)
@@ -362,7 +363,7 @@ def measure_mixed_channel(order, n=(40, 20, 20), steps=3, err_steps=10, dt=2e-4)
     m.advance(err_steps, dt, gemm_precision=0)
     torch.cuda.synchronize()
     ref = {i: s["u"].clone() for i, s in m.S.items()}
-    for mode, name in ((1, "bf16x3"), (2, "bf16x6")):
+    for mode, name in ((3, "fp64_cuda_cores"), (1, "bf16x3"), (2, "bf16x6")):
         reset()
         m.residual(mode)
         torch.cuda.synchronize()
@@ -492,9 +493,10 @@ def measure_tgv64_p4(dev, n=64, P=4, steps=100, dt=2e-4):
 def measure_operator_path(a, dev, s64, u0):
     """The reference's residual as per-operator calls (dense opp_0 .. opp_6
     over all elements, pointer-table interface kernels): FP64 operator products
-    on the CUDA cores against the BF16 3-term split products on the tensor
-    cores, same workload, with the L2 error of the BF16 form after 20 steps,
-    and the extrapolation product alone (opp_0 U) in both precisions."""
+    on the FP64 tensor cores (default) and on the CUDA cores against the BF16
+    split products on the tcgen05 tensor cores, same workload, with the L2
+    error of each form against the first after 20 steps, and the
+    extrapolation product alone (opp_0 U) in every form."""
     import ctypes
     import torch
     from hifiles_b200 import seam
@@ -503,7 +505,7 @@ def measure_operator_path(a, dev, s64, u0):
     op = seam.OperatorStage(s64, phys, a.order, vcjh_scheme=1)
     dof_step = op.E * op.nu * op.F * 5
     res = {}
-    modes = ((0, "fp64"), (1, "bf16x3"), (2, "bf16x6"))
+    modes = ((0, "fp64"), (3, "fp64_cuda_cores"), (1, "bf16x3"), (2, "bf16x6"))
     for mode, name in modes:
         op.set_state(u0)
         op.advance(1, dt, gemm_precision=mode)
@@ -535,11 +537,12 @@ def measure_operator_path(a, dev, s64, u0):
         L.fr_op_set_gemm_precision(0)
         t = e0.elapsed_time(e1) / 3 * 1e-3
         bytes_ = 8.0 * (k + m) * ncols
-        flops = 2.0 * m * k * ncols * (1, 3, 6)[mode]
+        flops = 2.0 * m * k * ncols * {0: 1, 3: 1, 1: 3, 2: 6}[mode]
         res[name]["opp_0_product"] = {"ms": t * 1e3, "GB/s": bytes_ / t / 1e9, "TFLOP/s": flops / t / 1e12}
     res["workload"] = ("same TGV mesh and state; one step = 5 RK stages of CalcResidual through the fr_op_* "
-                       "entry points; operator products in FP64 on the CUDA cores, or BF16x3 / BF16x6 split "
-                       "products on the tcgen05 tensor cores with FP32 accumulation")
+                       "entry points; operator products in FP64 on the FP64 tensor cores (fp64) or the CUDA "
+                       "cores, or BF16x3 / BF16x6 split products on the tcgen05 tensor cores with FP32 "
+                       "accumulation")
     del op
     torch.cuda.empty_cache()
     return res

@@ -151,6 +151,154 @@ dense_apply_kernel(int m, int k, long long ncols, int nd, OpSet ops, const doubl
   }
 }
 
+// FP64 tensor-core form of the same products (mma.sync m8n8k4 f64): a block
+// stages a tile of 64-512 columns (the widest within 100 kB) of every B_d in
+// shared memory by asynchronous copies (column-major,
+// leading dimension ldk = 4 or 12 mod 16 doubles, rows k .. ceil4(k) zeroed),
+// and each warp unit computes 8 rows x 32 columns: the accumulator starts at
+// beta C, then runs over d and the k-steps in increasing order, so fused and
+// separate products agree bit for bit, and every column's result is the same
+// in any tiling.  Operator fragments are read from the column-major A_d
+// through the read-only cache (entries beyond m x k read as zero).
+constexpr int kMmaThreads = 256;
+constexpr int kMmaTN = 4;  // 8-column tiles per warp unit
+
+__device__ __forceinline__ void dmma8(double (&c)[2], double a, double b)
+{
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+      : "+d"(c[0]), "+d"(c[1])
+      : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void cp_async8(void* dst, const void* src)
+{
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+template <bool FAN, int NCT>
+__global__ void __launch_bounds__(kMmaThreads)
+dense_mma_kernel(int m, int k, long long ncols, int nd, OpSet ops, const double* __restrict__ B,
+                 long long strideB, double* __restrict__ Cm, long long strideC, int beta, int ldk)
+{
+  extern __shared__ __align__(16) double sm[];
+  const int nb = FAN ? 1 : nd;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int NW = kMmaThreads / 32;
+  const long long c0 = (long long)blockIdx.x * NCT;
+  const int nc = (int)min((long long)NCT, ncols - c0);
+  const int kp = (k + 3) & ~3;
+  // B tile: asynchronous copies, one column per warp pass with the lanes
+  // along k (contiguous in global memory), many columns in flight
+  for (int b = 0; b < nb; b++) {
+    const double* Bt = B + b * strideB + (size_t)c0 * k;
+    double* sb = sm + (size_t)b * NCT * ldk;
+    for (int c = warp; c < NCT; c += NW) {
+      if (c < nc)
+        for (int l = lane; l < k; l += 32) cp_async8(&sb[c * ldk + l], Bt + (size_t)c * k + l);
+      for (int l = k + lane; l < kp; l += 32) sb[c * ldk + l] = 0.0;
+    }
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncthreads();
+  const int MT = (m + 7) / 8, KS = kp / 4;
+  constexpr int NB = NCT / 8 / kMmaTN;
+  const int g = lane >> 2, t = lane & 3;
+  for (int u = warp; u < MT * NB; u += NW) {
+    const int mt = u / NB, nt0 = (u - mt * NB) * kMmaTN;
+    const int r = mt * 8 + g;
+    for (int o = 0; o < (FAN ? nd : 1); o++) {
+      double* Co = Cm + (FAN ? o * strideC : 0);
+      double acc[kMmaTN][2];
+#pragma unroll
+      for (int j = 0; j < kMmaTN; j++)
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+          const int n = (nt0 + j) * 8 + 2 * t + i;
+          acc[j][i] = (beta && r < m && n < nc) ? Co[r + (size_t)m * (c0 + n)] : 0.0;
+        }
+      const int d0 = FAN ? o : 0, d1 = FAN ? o + 1 : nd;
+      for (int d = d0; d < d1; d++) {
+        const double* A = ops.get(d);
+        const double* sb = sm + (size_t)(FAN ? 0 : d) * NCT * ldk;
+        const double* bp[kMmaTN];
+#pragma unroll
+        for (int j = 0; j < kMmaTN; j++) bp[j] = sb + ((nt0 + j) * 8 + g) * ldk + t;
+#pragma unroll 4
+        for (int ks = 0; ks < KS; ks++) {
+          const int c = ks * 4 + t;
+          const double a = (r < m && c < k) ? __ldg(A + r + (size_t)m * c) : 0.0;
+#pragma unroll
+          for (int j = 0; j < kMmaTN; j++) dmma8(acc[j], a, bp[j][ks * 4]);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kMmaTN; j++)
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+          const int n = (nt0 + j) * 8 + 2 * t + i;
+          if (r < m && n < nc) Co[r + (size_t)m * (c0 + n)] = acc[j][i];
+        }
+    }
+  }
+}
+
+int mma_ld(int k)
+{
+  int x = (k + 3) & ~3;
+  while (x % 16 != 4 && x % 16 != 12) x++;
+  return x;
+}
+
+size_t mma_smem(int k, int nb, int nct) { return (size_t)nb * nct * mma_ld(k) * sizeof(double); }
+
+// the column tile of every B_d fits one block's shared memory (128 columns, else 64)
+bool mma_fits(int k, int nb) { return mma_smem(k, nb, 64) <= 200 * 1024; }
+
+fr_status dense_mma_launch(int m, int k, long long ncols, int nd, const OpSet& ops, const double* B, long long sB,
+                           double* Cm, long long sC, int beta, bool fan, cudaStream_t s)
+{
+  const int ldk = mma_ld(k), nb = fan ? 1 : nd;
+  // the widest column tile within 100 kB (short operators get wide tiles, so
+  // a block's staging is spread over enough products), narrowed while the
+  // grid would not give every SM two blocks
+  int nct = 64;
+  for (int c : {512, 256, 128})
+    if (mma_smem(k, nb, c) <= 100 * 1024) {
+      nct = c;
+      break;
+    }
+  while (nct > 64 && (ncols + nct - 1) / nct < 2 * 148) nct /= 2;
+  const size_t smem = mma_smem(k, nb, nct);
+  auto pick = [&](auto kt, auto kf) { return fan ? kt : kf; };
+  auto kern = nct == 512   ? pick(dense_mma_kernel<true, 512>, dense_mma_kernel<false, 512>)
+              : nct == 256 ? pick(dense_mma_kernel<true, 256>, dense_mma_kernel<false, 256>)
+              : nct == 128 ? pick(dense_mma_kernel<true, 128>, dense_mma_kernel<false, 128>)
+                           : pick(dense_mma_kernel<true, 64>, dense_mma_kernel<false, 64>);
+  // every instantiation may use up to 100 kB: set once per device
+  static unsigned long long attr_set = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !(attr_set >> dev & 1ull)) {
+    const void* all[] = {(const void*)dense_mma_kernel<true, 512>, (const void*)dense_mma_kernel<false, 512>,
+                         (const void*)dense_mma_kernel<true, 256>, (const void*)dense_mma_kernel<false, 256>,
+                         (const void*)dense_mma_kernel<true, 128>, (const void*)dense_mma_kernel<false, 128>,
+                         (const void*)dense_mma_kernel<true, 64>, (const void*)dense_mma_kernel<false, 64>};
+    for (const void* f : all) {
+      cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+      if (e != cudaSuccess) return op_fail(FR_ERR_CUDA, cudaGetErrorString(e));
+    }
+    attr_set |= 1ull << dev;
+  } else if (dev >= 64 && smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return op_fail(FR_ERR_CUDA, cudaGetErrorString(e));
+  }
+  const long long blocks = (ncols + nct - 1) / nct;
+  if (blocks > 2147483647LL) return op_fail(FR_ERR_ARG, "too many columns");
+  kern<<<(unsigned)blocks, kMmaThreads, smem, s>>>(m, k, ncols, nd, ops, B, sB, Cm, sC, beta, ldk);
+  return launched("dense_mma_kernel");
+}
+
 template <int RM, int LW = 32>
 fr_status dense_launch(int m, int k, long long ncols, int nd, const OpSet& ops, const double* B, long long sB,
                        double* Cm, long long sC, int beta, bool fan, cudaStream_t s, size_t smem, unsigned blocks)
@@ -168,9 +316,11 @@ fr_status dense_launch(int m, int k, long long ncols, int nd, const OpSet& ops, 
   return launched("dense_apply_kernel");
 }
 
-// Precision of the operator products of this seam: 0 = FP64 (dense_apply_kernel),
-// 1 = BF16x3 and 2 = BF16x6 split products on the tensor cores, FP32
-// accumulation (fr_tc_gemm.cu).
+// Precision of the operator products of this seam: 0 = FP64 on the FP64
+// tensor cores (dense_mma_kernel; dense_apply_kernel when a column tile does
+// not fit shared memory), 1 = BF16x3 and 2 = BF16x6 split products on the
+// tcgen05 tensor cores, FP32 accumulation (fr_tc_gemm.cu), 3 = FP64 on the
+// CUDA cores (dense_apply_kernel).
 static int g_gemm_mode = 0;
 
 // nd operator products of one method (see dense_apply_kernel); FAN selects
@@ -193,13 +343,21 @@ fr_status dense_apply_nd(int m, int k, long long ncols, int nd, const double* co
   // then nd single products with a staged operator are faster
   const bool split = nd > 1 && (long long)m * k <= kSmallOps && smem1 + a1 <= kStageSmem1 &&
                      !((long long)nd * m * k <= kSmallOps && smem + nd * a1 <= kStageSmem);
-  if (g_gemm_mode || split || (nd > 1 && smem > kDenseSmem)) {
+  // FP64 products with short operators (k < 16) stay on the CUDA cores, where
+  // they measured faster; both forms give the same bits
+  if (g_gemm_mode == 0 && k >= 16 && mma_fits(k, fan ? 1 : nd)) {
+    OpSet ops{};
+    for (int d = 0; d < nd; d++) ops.a[d] = A[d];
+    return dense_mma_launch(m, k, ncols, nd, ops, B, strideB, Cm, strideC, beta, fan, s);
+  }
+  const bool tc = g_gemm_mode == 1 || g_gemm_mode == 2;
+  if (tc || split || (nd > 1 && smem > kDenseSmem)) {
     for (int d = 0; d < nd; d++) {
       const double* Bd = B + (fan ? 0 : d * strideB);
       double* Cd = Cm + (fan ? d * strideC : 0);
       const int bd = fan ? beta : (d > 0 ? 1 : beta);
-      fr_status st = g_gemm_mode ? gemm_bf16x3(m, k, ncols, A[d], Bd, Cd, bd, s, g_gemm_mode == 2 ? 6 : 3)
-                                 : dense_apply_nd(m, k, ncols, 1, A + d, Bd, 0, Cd, 0, bd, false, s);
+      fr_status st = tc ? gemm_bf16x3(m, k, ncols, A[d], Bd, Cd, bd, s, g_gemm_mode == 2 ? 6 : 3)
+                        : dense_apply_nd(m, k, ncols, 1, A + d, Bd, 0, Cd, 0, bd, false, s);
       if (st) return st;
     }
     return FR_OK;
@@ -644,8 +802,9 @@ extern "C" {
 
 fr_status fr_op_set_gemm_precision(int mode)
 {
-  if (mode < 0 || mode > 2)
-    return op_fail(FR_ERR_ARG, "GEMM precision: 0 (FP64), 1 (BF16x3) or 2 (BF16x6 tensor cores)");
+  if (mode < 0 || mode > 3)
+    return op_fail(FR_ERR_ARG,
+                   "GEMM precision: 0 (FP64 tensor cores), 1 (BF16x3), 2 (BF16x6) or 3 (FP64 CUDA cores)");
   g_gemm_mode = mode;
   return FR_OK;
 }

@@ -521,13 +521,18 @@ fr_status fr_op_advance_rk45(int n_upts, int n_fields, int n_eles, int stage, do
 /* Precision of the operator products (opp_0 .. opp_6 applied to all
  * elements, the reference's cublasDgemm calls) of the fr_op_* entry points,
  * process-wide like the reference's run_input:
- *   0  FP64 on the CUDA cores (default; parity with the reference),
+ *   0  FP64 (default; parity with the reference): operators of k >= 16
+ *      columns on the FP64 tensor cores (mma.sync m8n8k4 f64), shorter ones
+ *      and those whose 64-column operand tile exceeds shared memory on the
+ *      CUDA cores; both forms accumulate each output as one chain of fused
+ *      multiply-adds in k order, so they give the same bits,
  *   1  BF16x3: x = x0 + x1 + x2 in BF16, products x0y0 + x0y1 + x1y0 (about
  *      16 bits) on the tcgen05 tensor cores, FP32 accumulation, FP64 inputs
  *      and outputs; m x k operators with m <= 128 and k <= 288, or m <= 256
  *      and k <= 192 (hexes up to P = 4),
  *   2  BF16x6: the same plus x0y2 + x1y1 + x2y0 (about 24 bits); m <= 128
- *      and k <= 192, or m <= 256 and k <= 128 (hexes up to P = 4);
+ *      and k <= 192, or m <= 256 and k <= 128 (hexes up to P = 4),
+ *   3  FP64 on the CUDA cores;
  * larger operators return FR_ERR_UNSUPPORTED.
  * Pointwise kernels stay FP64.  fr_op_check synchronises the stream and
  * returns FR_ERR_TIMEOUT if a tensor-core product gave up waiting for its

@@ -124,7 +124,7 @@ def test_split_products_reject_operators_beyond_shared_memory():
         finally:
             L.fr_op_set_gemm_precision(0)
         assert st == 5, (mode, m, k)
-    assert L.fr_op_set_gemm_precision(3) == 1
+    assert L.fr_op_set_gemm_precision(4) == 1
 
 
 def _tgv(pos):
@@ -182,3 +182,54 @@ def test_pipelined_b_tiles_give_identical_products(m, k, n, mode):
         L.fr_op_set_gemm_pipelining(1)
     assert np.isfinite(piped).all()
     assert np.array_equal(plain, piped)
+
+
+@pytest.mark.parametrize("m,k,n", [(96, 64, 5 * 1000 + 3), (64, 96, 777), (40, 20, 5 * 8 + 3), (20, 40, 64),
+                                   (10, 24, 129), (1, 1, 5), (68, 40, 333), (250, 150, 70), (20, 20, 100),
+                                   (64, 64, 5 * 4096)])
+def test_fp64_tensor_core_product_matches_cuda_cores(m, k, n):
+    """Precision mode 0 (FP64 tensor cores) against mode 3 (FP64 CUDA cores)
+    and numpy: single products (extrapolate_solution), products fanned out
+    over the dimensions (calculate_gradient) and summed over them
+    (extrapolate_totalFlux); the two FP64 forms agree bit for bit."""
+    rng = np.random.default_rng(11 + m + k)
+    A = rng.standard_normal((m, k))
+    B = rng.standard_normal((k, n))
+    ref = A @ B
+    L = _lib()
+    c0, c3 = _product(L, A, B, 0), _product(L, A, B, 3)
+    assert np.abs(c0 - ref).max() <= 1e-13 * np.abs(ref).max() * max(1, k) ** 0.5
+    # the tensor-core product accumulates each k-step of 4 as successive
+    # fused multiply-adds in k order, like the CUDA-core chain: same bits
+    assert np.array_equal(c0, c3)
+    D, F = 3, 1
+    As = [rng.standard_normal((m, k)) for _ in range(D)]
+    Bs = [rng.standard_normal((k, n)) for _ in range(D)]
+    dA = [_dev(a) for a in As]
+    tab = (VP * D)(*[a.data_ptr() for a in dA])
+    out = {}
+    for mode in (0, 3):
+        assert L.fr_op_set_gemm_precision(mode) == 0
+        try:
+            # fan: G_d = A_d B (calculate_gradient: n_upts = m = k square only)
+            dB = _dev(Bs[0])
+            dS = _dev(np.concatenate([b.ravel(order="F") for b in Bs]))
+            dC = torch.zeros(m * n, dtype=torch.float64, device="cuda")
+            st = L.fr_op_extrapolate_totalFlux(m, k, D, F, n, C.cast(tab, VP), dS.data_ptr(), dC.data_ptr(), None)
+            assert st == 0, H.lib().fr_last_error().decode()
+            out[mode] = _host(dC, (m, n))
+            if m == k:
+                dG = torch.zeros(m * n * D, dtype=torch.float64, device="cuda")
+                st = L.fr_op_calculate_gradient(m, D, F, n, C.cast(tab, VP), dB.data_ptr(), dG.data_ptr(), None)
+                assert st == 0, H.lib().fr_last_error().decode()
+                out[(mode, "fan")] = _host(dG, (m, n, D))
+            assert L.fr_op_check(None) == 0
+        finally:
+            L.fr_op_set_gemm_precision(0)
+    want = sum(a @ b for a, b in zip(As, Bs))
+    scale = np.abs(want).max() * (D * k) ** 0.5
+    assert np.abs(out[0] - want).max() <= 1e-13 * scale
+    assert np.array_equal(out[0], out[3])
+    if m == k:
+        for d in range(D):
+            assert np.abs(out[(0, "fan")][..., d] - As[d] @ Bs[0]).max() <= 1e-13 * np.abs(ref).max() * k ** 0.5
