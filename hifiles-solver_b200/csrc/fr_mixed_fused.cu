@@ -366,11 +366,13 @@ __global__ void __launch_bounds__(NTH, MINB) mixed_grad_kernel(MixedType t, Mixe
   }
   __syncthreads();
 
-  // gradient at the flux points: columns ((element, field), dimension) of X
+  // gradient at the flux points: column d N + (element, field) of X for
+  // dimension d (dimension-major, so the 8 columns of a fragment load are
+  // consecutive columns of sG and hit distinct banks)
   {
     auto bg = [&](int n) {
-      const int c = n < Q::NG ? n : Q::NG - 1;
-      return sG + (c / D) * Q::ldG + (c % D) * NU;
+      const int c = n < Q::NG ? n : Q::NG - 1, d = c / Q::N;
+      return sG + (c - d * Q::N) * Q::ldG + d * NU;
     };
     auto epi = [&](int r, int n, double v0, double v1) {
       sX[n * Q::ldF + r] = v0;
@@ -393,7 +395,7 @@ __global__ void __launch_bounds__(NTH, MINB) mixed_grad_kernel(MixedType t, Mixe
     for (int k = 0; k < F; k++) {
       uo[k] = sUF[(el * F + k) * Q::ldF + f];
 #pragma unroll
-      for (int c = 0; c < D; c++) gf[k][c] = sX[((el * F + k) * D + c) * Q::ldF + f];
+      for (int c = 0; c < D; c++) gf[k][c] = sX[(c * Q::N + el * F + k) * Q::ldF + f];
     }
     if (sd >> 2) {
       BdyPoint<D, double> q;
@@ -883,7 +885,10 @@ fr_status for_types(fr_mixed_stage* s, cudaStream_t st, Launch launch)
       if (cudaStreamWaitEvent(s->side_streams[j], s->fork_ev[0], 0) != cudaSuccess)
         return mfail(FR_ERR_CUDA, "stream wait failed");
   }
-  for (int i = 0; i < s->n_types; i++) {
+  // the side-stream types go first, so their blocks are resident while the
+  // first type's blocks fill the rest of the GPU
+  for (int j = 1; j <= s->n_types; j++) {
+    const int i = j % s->n_types;
     if (s->types[i].E == 0) continue;
     if (fr_status e = launch(i, par && i > 0 ? s->side_streams[i - 1] : st)) return e;
   }
