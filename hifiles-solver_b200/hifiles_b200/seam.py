@@ -431,8 +431,8 @@ class FusedMixedMesh:
     """The mesh of `MixedOperatorMesh` (same arguments) advanced by the fused
     stage of include/fr_b200.h (`fr_mixed_stage_*`): per element type and RK
     stage one gradient kernel and one interface/update kernel, operator
-    products on the FP64 tensor cores.  Navier-Stokes in 3-D; tets, prisms
-    and hexes of orders 2 and 3.  The state of type i is `S[i]["u"]`
+    products on the FP64 tensor cores.  Navier-Stokes in 2-D (triangles,
+    quads) or 3-D (tets, prisms, hexes), orders 2 and 3.  The state of type i is `S[i]["u"]`
     (n_upts, n_eles, 5) on the device, advanced in place; `residual()` writes
     `S[i]["div"]`."""
 
@@ -595,12 +595,13 @@ def mixed_mesh_inputs(meta, arrays, state_key="disu_upts_init"):
     int_inters_<k> / bdy_inters_<k> wiring; `meta` lists the element types
     ({"index", "ele_type"}), interface and boundary types ({"index"})."""
     types = {}
+    dims = int(meta.get("dims", 3))
     for t in meta["types"]:
         X = "t%d_" % t["ele_type"]
         ty = {k: arrays[X + k] for k in ("opp_0", "opp_3", "opp_6", "JGinv_upts", "detjac_upts", "tdA_fpts",
                                          "norm_fpts")}
         for w in (1, 2, 4, 5):
-            ty["opp_%d" % w] = [arrays[X + "opp_%d_%d" % (w, d)] for d in range(3)]
+            ty["opp_%d" % w] = [arrays[X + "opp_%d_%d" % (w, d)] for d in range(dims)]
         ty["u"] = arrays[X + state_key]
         types[t["index"]] = ty
     ints = [arrays["int_inters_%d" % it["index"]] for it in meta["inters"]]

@@ -647,7 +647,7 @@ fr_status fr_mixed_bdy_inters(const fr_mixed* m, int group, int* n_fpts_per_inte
  * extrapolate_corrected_gradient, evaluate_viscFlux, extrapolate_totalFlux,
  * calculate_divergence; calculate_common_viscFlux; calculate_corrected_divergence)
  * and AdvanceSolution (src/eles.cpp:1155-1178), Navier-Stokes, Rusanov +
- * LDG, 3-D, in two kernels per element type and stage whose operator
+ * LDG, 2-D or 3-D, in two kernels per element type and stage whose operator
  * products run on the FP64 tensor cores.  Inputs are what the per-operator
  * entry points take: each type's operators and metrics as its eles object
  * holds them (host arrays, column-major, the layouts of the fr_op_* calls;
@@ -657,8 +657,8 @@ fr_status fr_mixed_bdy_inters(const fr_mixed* m, int group, int* n_fpts_per_inte
  * n_fpts_per_inter, n_inters) int arrays of (type index, element, flux point)
  * per side, the boundary type last), on the host.  Every flux point must lie
  * on exactly one interface or boundary (FR_ERR_MESH otherwise).  Element
- * types with kernels: tets, prisms and hexes of orders 2 and 3
- * (FR_ERR_UNSUPPORTED otherwise).  The stage keeps the RK register and the
+ * types with kernels: tets, prisms and hexes, triangles and quads, of orders
+ * 2 and 3 (FR_ERR_UNSUPPORTED otherwise).  The stage keeps the RK register and the
  * flux-point traces on the device; disu_upts is advanced in place.
  * ---------------------------------------------------------------------- */
 typedef struct {

@@ -1,5 +1,5 @@
 """The fused mixed-mesh stage (fr_mixed_stage_*, hifiles_b200.seam.FusedMixedMesh):
-tets, prisms and hexes advanced by one gradient kernel and one
+tets, prisms, hexes, triangles and quads advanced by one gradient kernel and one
 interface/update kernel per element type and RK stage, operator products on
 the FP64 tensor cores.
 
@@ -23,7 +23,8 @@ import pytest
 from golden_util import load, rel
 
 FR_ERR_ARG, FR_ERR_UNSUPPORTED = 1, 5  # fr_status codes of include/fr_b200.h
-FUSED = ["mixed_pritet_p3", "mixed_pritet_p2", "mixed_hexpri_p3", "mixed_channel_p2", "mixed_channel_p3"]
+FUSED = ["mixed_pritet_p3", "mixed_pritet_p2", "mixed_hexpri_p3", "mixed_channel_p2", "mixed_channel_p3",
+         "mixed_triquad_p2", "mixed_triquad_p3"]
 
 
 def _div(m, i):
@@ -118,7 +119,7 @@ def test_fused_channel_matches_the_operator_path(order):
 
 
 def test_fused_stage_rejects_unsupported_meshes():
-    """2-D meshes and element shapes without kernels are refused before any
+    """1-D meshes and element shapes without kernels are refused before any
     device work, with a reason."""
     import hifiles_b200 as H
     from hifiles_b200 import seam
@@ -126,7 +127,7 @@ def test_fused_stage_rejects_unsupported_meshes():
     ph = seam.PhysDesc(**CHANNEL_PHYSICS)
     d = (seam._MixedStageType * 1)()
     h = C.c_void_p()
-    st = L.fr_mixed_stage_create(2, 1, d, 0, None, None, None, 0, None, None, None, None, 1.0, C.byref(ph),
+    st = L.fr_mixed_stage_create(1, 1, d, 0, None, None, None, 0, None, None, None, None, 1.0, C.byref(ph),
                                  C.byref(h))
     assert st == FR_ERR_UNSUPPORTED and "3-D" in H.lib().fr_last_error().decode()
     # a tet of order 4 (35 solution, 60 flux points) has no kernels
