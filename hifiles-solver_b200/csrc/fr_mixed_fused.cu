@@ -302,7 +302,6 @@ fr_status fr_mixed_stage_create(int n_dims, int n_types, const fr_mixed_stage_ty
     if (!find_kernels(D, NU, NF, &k))
       return bail(mfail(FR_ERR_UNSUPPORTED, "fused mixed stage: no kernels for " + std::to_string(NU) +
                                                 " solution / " + std::to_string(NF) + " flux points"));
-    if (fr_status e = set_smem(k)) return bail(e);
     s->kern.push_back(k);
     int g0 = 0, u0 = 0;
     while (!k.grad[g0]) g0++;
@@ -313,44 +312,6 @@ fr_status fr_mixed_stage_create(int n_dims, int n_types, const fr_mixed_stage_ty
   }
   s->NT = off[n_types];
   const long long NT = s->NT;
-
-  // operators in fragment order
-  for (int i = 0; i < n_types; i++) {
-    const fr_mixed_stage_type& ty = types[i];
-    const int NU = ty.n_upts, NF = ty.n_fpts;
-    const long long E = ty.n_eles;
-    MixedType t{};
-    t.NU = NU;
-    t.NF = NF;
-    t.E = E;
-    t.off = off[i];
-    auto cm = [](const double* a, int rows) { return [a, rows](int r, int c) { return a[r + (size_t)rows * c]; }; };
-    std::vector<double> h;
-    h = fragments(D * NU, NU, [&](int r, int c) { return ty.opp_4[r / NU][r % NU + (size_t)NU * c]; });
-    if (fr_status e = s->upload(h, &t.A45u)) return bail(e);
-    h = fragments(D * NU, NF, [&](int r, int c) { return ty.opp_5[r / NU][r % NU + (size_t)NU * c]; });
-    if (fr_status e = s->upload(h, &t.A45f)) return bail(e);
-    h = fragments(NF, NU, cm(ty.opp_6, NF));
-    if (fr_status e = s->upload(h, &t.A6)) return bail(e);
-    h = fragments(NF, D * NU, [&](int r, int c) { return ty.opp_1[c / NU][r + (size_t)NF * (c % NU)]; });
-    if (fr_status e = s->upload(h, &t.A1)) return bail(e);
-    h = fragments(NU, D * NU, [&](int r, int c) { return ty.opp_2[c / NU][r + (size_t)NU * (c % NU)]; });
-    if (fr_status e = s->upload(h, &t.A2)) return bail(e);
-    h = fragments(NU, NF, cm(ty.opp_3, NU));
-    if (fr_status e = s->upload(h, &t.A3)) return bail(e);
-    h = fragments(NF, NU, cm(ty.opp_0, NF));
-    if (fr_status e = s->upload(h, &t.A0)) return bail(e);
-    std::vector<double> jg(ty.JGinv_upts, ty.JGinv_upts + (size_t)D * D * NU * E);
-    if (fr_status e = s->upload(jg, &t.JG)) return bail(e);
-    std::vector<double> dj(ty.detjac_upts, ty.detjac_upts + (size_t)NU * E);
-    if (fr_status e = s->upload(dj, &t.detj)) return bail(e);
-    t.U = ty.disu_upts;
-    t.DIV = ty.div_tconf_upts;
-    if (fr_status e = s->zeros((size_t)NU * E * F, &t.REG)) return bail(e);
-    if (fr_status e = s->zeros((size_t)NF * E * F, &t.ND)) return bail(e);
-    if (fr_status e = s->zeros((size_t)NU * E * F, &t.DV)) return bail(e);
-    s->types.push_back(t);
-  }
 
   // flux-point space: neighbours, sides, left normals, own tdA
   std::vector<int> mate(NT, 0);
@@ -412,6 +373,47 @@ fr_status fr_mixed_stage_create(int n_dims, int n_types, const fr_mixed_stage_ty
     for (long long e = 0; e < q.n_eles; e++)
       for (int f = 0; f < q.n_fpts; f++) tdA[off[i] + f + (long long)q.n_fpts * e] = q.tdA_fpts[f + (size_t)q.n_fpts * e];
   }
+  // every check above is on the host: device work starts here
+  for (const MixedKernels& k : s->kern)
+    if (fr_status e = set_smem(k)) return bail(e);
+  // operators in fragment order
+  for (int i = 0; i < n_types; i++) {
+    const fr_mixed_stage_type& ty = types[i];
+    const int NU = ty.n_upts, NF = ty.n_fpts;
+    const long long E = ty.n_eles;
+    MixedType t{};
+    t.NU = NU;
+    t.NF = NF;
+    t.E = E;
+    t.off = off[i];
+    auto cm = [](const double* a, int rows) { return [a, rows](int r, int c) { return a[r + (size_t)rows * c]; }; };
+    std::vector<double> h;
+    h = fragments(D * NU, NU, [&](int r, int c) { return ty.opp_4[r / NU][r % NU + (size_t)NU * c]; });
+    if (fr_status e = s->upload(h, &t.A45u)) return bail(e);
+    h = fragments(D * NU, NF, [&](int r, int c) { return ty.opp_5[r / NU][r % NU + (size_t)NU * c]; });
+    if (fr_status e = s->upload(h, &t.A45f)) return bail(e);
+    h = fragments(NF, NU, cm(ty.opp_6, NF));
+    if (fr_status e = s->upload(h, &t.A6)) return bail(e);
+    h = fragments(NF, D * NU, [&](int r, int c) { return ty.opp_1[c / NU][r + (size_t)NF * (c % NU)]; });
+    if (fr_status e = s->upload(h, &t.A1)) return bail(e);
+    h = fragments(NU, D * NU, [&](int r, int c) { return ty.opp_2[c / NU][r + (size_t)NU * (c % NU)]; });
+    if (fr_status e = s->upload(h, &t.A2)) return bail(e);
+    h = fragments(NU, NF, cm(ty.opp_3, NU));
+    if (fr_status e = s->upload(h, &t.A3)) return bail(e);
+    h = fragments(NF, NU, cm(ty.opp_0, NF));
+    if (fr_status e = s->upload(h, &t.A0)) return bail(e);
+    std::vector<double> jg(ty.JGinv_upts, ty.JGinv_upts + (size_t)D * D * NU * E);
+    if (fr_status e = s->upload(jg, &t.JG)) return bail(e);
+    std::vector<double> dj(ty.detjac_upts, ty.detjac_upts + (size_t)NU * E);
+    if (fr_status e = s->upload(dj, &t.detj)) return bail(e);
+    t.U = ty.disu_upts;
+    t.DIV = ty.div_tconf_upts;
+    if (fr_status e = s->zeros((size_t)NU * E * F, &t.REG)) return bail(e);
+    if (fr_status e = s->zeros((size_t)NF * E * F, &t.ND)) return bail(e);
+    if (fr_status e = s->zeros((size_t)NU * E * F, &t.DV)) return bail(e);
+    s->types.push_back(t);
+  }
+
   s->n_bpts = place;
   s->fp.NT = NT;
   if (fr_status e = s->upload(mate, &s->fp.mate)) return bail(e);

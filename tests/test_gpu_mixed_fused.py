@@ -181,3 +181,59 @@ def test_fused_launch_shapes_give_the_same_bits():
     for i in m.S:
         assert np.array_equal(m.get_state(i), before[i])
         assert 0 <= picked[i][0] < 5 and 0 <= picked[i][1] < 3
+
+
+def test_fused_stage_rejects_bad_wiring_before_device_work():
+    """Interface and boundary tables are checked on the host before anything
+    is allocated: a flux point wired twice or on no interface, entries out of
+    range, unknown boundary types."""
+    import hifiles_b200 as H
+    from hifiles_b200 import seam
+    L = seam._bind_stage(H.lib())
+    ph = seam.PhysDesc(**CHANNEL_PHYSICS)
+    nu, nf, E = 10, 24, 2  # two tets of order 2
+    keep = [np.zeros(9 * nu * nf * E)]
+    p = keep[0].ctypes.data
+    d = (seam._MixedStageType * 1)()
+    d[0].n_upts, d[0].n_fpts, d[0].n_eles = nu, nf, E
+    d[0].opp_0 = d[0].opp_3 = d[0].opp_6 = d[0].JGinv_upts = d[0].detjac_upts = d[0].tdA_fpts = p
+    d[0].norm_fpts = d[0].disu_upts = p
+    for name in ("opp_1", "opp_2", "opp_4", "opp_5"):
+        arr = getattr(d[0], name)
+        for q in range(3):
+            arr[q] = p
+
+    def create(ints=(), bdys=()):
+        def pack(ws):
+            ws = [np.asfortranarray(w, dtype=np.int32) for w in ws]
+            keep.extend(ws)
+            n = max(len(ws), 1)
+            return (len(ws), (C.c_void_p * n)(*[w.ctypes.data for w in ws]),
+                    (C.c_int * n)(*[w.shape[1] for w in ws]), (C.c_longlong * n)(*[w.shape[2] for w in ws]))
+        ni, ip, inf, inn = pack(ints)
+        nb, bp, bnf, bnn = pack(bdys)
+        h = C.c_void_p()
+        st = L.fr_mixed_stage_create(3, 1, d, ni, ip, inf, inn, nb, bp, bnf, bnn, None, 1.0, C.byref(ph), C.byref(h))
+        assert not h.value
+        return st, H.lib().fr_last_error().decode()
+
+    def inter(pairs):
+        w = np.zeros((6, 1, len(pairs)), dtype=np.int32)
+        for j, (t0, e0, f0, t1, e1, f1) in enumerate(pairs):
+            w[:, 0, j] = (t0, e0, f0, t1, e1, f1)
+        return w
+
+    full = [(0, 0, f, 0, 1, f) for f in range(nf)]
+    st, msg = create([inter(full[:-1] + [full[0]])])
+    assert st == 6 and "twice" in msg
+    st, msg = create([inter(full[:-1])])
+    assert st == 6 and "no interface" in msg
+    st, msg = create([inter(full[:-1] + [(0, 2, 0, 0, 1, 23)])])
+    assert st == 6 and "out of range" in msg
+    st, msg = create([inter(full[:-1] + [(1, 0, 23, 0, 1, 23)])])
+    assert st == 6 and "out of range" in msg
+    b = np.zeros((4, 1, 2), dtype=np.int32)
+    b[:, 0, 0] = (0, 0, 23, 9)
+    b[:, 0, 1] = (0, 1, 23, 7)
+    st, msg = create([inter(full[:-1])], [b])
+    assert st == 5 and "boundary type 9" in msg
