@@ -21,7 +21,7 @@ BUILD = os.path.join(HERE, "_build")
 SOURCES = ["fr_host.cpp", "fr_restart.cpp", "fr_vtu.cpp", "fr_solver.cu", "fr_ops.cu", "fr_noalloc.cu", "fr_runner_quad_f64.cu",
            "fr_runner_quad_f32.cu", "fr_runner_hex_f64_a.cu", "fr_runner_hex_f64_p3.cu", "fr_runner_hex_f64_p4.cu",
            "fr_runner_hex_f32.cu", "fr_mlp.cu", "fr_diag.cu", "fr_tc_gemm.cu", "fr_mixed.cpp", "fr_batch_merged.cu", "fr_mixed_fused.cu",
-           "fr_mixed_fused_2d.cu"]
+           "fr_mixed_fused_2d.cu", "fr_mixed_fused_p14.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 

@@ -70,9 +70,10 @@ fr_status mlaunched(const char* what)
 
 // (dims, solution points, flux points) with kernels: tets, prisms and hexes of
 // orders 2 and 3 here, triangles and quads of orders 2 and 3 in
-// fr_mixed_fused_2d.cu
+// fr_mixed_fused_2d.cu, orders 1 and 4 in fr_mixed_fused_p14.cu
 bool find_kernels(int D, int NU, int NF, MixedKernels* out)
 {
+  if (find_kernels_p14(D, NU, NF, out)) return true;
   if (D == 2) return find_kernels_2d(NU, NF, out);
   if (D != 3) return false;
 #define FR_MIXED_SHAPE(nu, nf) \

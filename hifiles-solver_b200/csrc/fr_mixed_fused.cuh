@@ -709,7 +709,9 @@ MixedKernels mixed_kernels()
 }
 
 
-// the kernels of the 2-D element types (fr_mixed_fused_2d.cu)
+// the kernels of the 2-D element types of orders 2 and 3 (fr_mixed_fused_2d.cu)
 bool find_kernels_2d(int NU, int NF, MixedKernels* out);
+// the kernels of orders 1 and 4 (fr_mixed_fused_p14.cu)
+bool find_kernels_p14(int D, int NU, int NF, MixedKernels* out);
 
 }  // namespace frb_mixed

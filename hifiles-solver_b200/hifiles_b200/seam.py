@@ -432,7 +432,7 @@ class FusedMixedMesh:
     stage of include/fr_b200.h (`fr_mixed_stage_*`): per element type and RK
     stage one gradient kernel and one interface/update kernel, operator
     products on the FP64 tensor cores.  Navier-Stokes in 2-D (triangles,
-    quads) or 3-D (tets, prisms, hexes), orders 2 and 3.  The state of type i is `S[i]["u"]`
+    quads) or 3-D (tets, prisms, hexes), orders 1 to 4 (hexes 1 to 3).  The state of type i is `S[i]["u"]`
     (n_upts, n_eles, 5) on the device, advanced in place; `residual()` writes
     `S[i]["div"]`."""
 

@@ -657,8 +657,8 @@ fr_status fr_mixed_bdy_inters(const fr_mixed* m, int group, int* n_fpts_per_inte
  * n_fpts_per_inter, n_inters) int arrays of (type index, element, flux point)
  * per side, the boundary type last), on the host.  Every flux point must lie
  * on exactly one interface or boundary (FR_ERR_MESH otherwise).  Element
- * types with kernels: tets, prisms and hexes, triangles and quads, of orders
- * 2 and 3 (FR_ERR_UNSUPPORTED otherwise).  The stage keeps the RK register and the
+ * types with kernels: tets, prisms, triangles and quads of orders 1 to 4,
+ * hexes of orders 1 to 3 (FR_ERR_UNSUPPORTED otherwise).  The stage keeps the RK register and the
  * flux-point traces on the device; disu_upts is advanced in place.
  * ---------------------------------------------------------------------- */
 typedef struct {

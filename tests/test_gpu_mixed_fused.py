@@ -130,10 +130,10 @@ def test_fused_stage_rejects_unsupported_meshes():
     st = L.fr_mixed_stage_create(1, 1, d, 0, None, None, None, 0, None, None, None, None, 1.0, C.byref(ph),
                                  C.byref(h))
     assert st == FR_ERR_UNSUPPORTED and "3-D" in H.lib().fr_last_error().decode()
-    # a tet of order 4 (35 solution, 60 flux points) has no kernels
-    keep = [np.zeros(35 * 60)]
+    # a hex of order 4 (125 solution, 150 flux points) has no kernels
+    keep = [np.zeros(9 * 125 * 150)]
     p = keep[0].ctypes.data
-    d[0].n_upts, d[0].n_fpts, d[0].n_eles = 35, 60, 1
+    d[0].n_upts, d[0].n_fpts, d[0].n_eles = 125, 150, 1
     d[0].opp_0 = d[0].opp_3 = d[0].opp_6 = d[0].JGinv_upts = d[0].detjac_upts = d[0].tdA_fpts = p
     d[0].norm_fpts = d[0].disu_upts = p
     for name in ("opp_1", "opp_2", "opp_4", "opp_5"):
@@ -142,7 +142,7 @@ def test_fused_stage_rejects_unsupported_meshes():
             arr[q] = p
     st = L.fr_mixed_stage_create(3, 1, d, 0, None, None, None, 0, None, None, None, None, 1.0, C.byref(ph),
                                  C.byref(h))
-    assert st == FR_ERR_UNSUPPORTED and "35" in H.lib().fr_last_error().decode()
+    assert st == FR_ERR_UNSUPPORTED and "125" in H.lib().fr_last_error().decode()
     d[0].n_upts = 0
     st = L.fr_mixed_stage_create(3, 1, d, 0, None, None, None, 0, None, None, None, None, 1.0, C.byref(ph),
                                  C.byref(h))
@@ -237,3 +237,52 @@ def test_fused_stage_rejects_bad_wiring_before_device_work():
     b[:, 0, 1] = (0, 1, 23, 7)
     st, msg = create([inter(full[:-1])], [b])
     assert st == 5 and "boundary type 9" in msg
+
+
+def _smooth_state(pos, dims):
+    """A smooth Mach-0.1-like state at points pos (n, E, dims)."""
+    x, y = pos[..., 0], pos[..., 1]
+    z = pos[..., 2] if dims == 3 else 0.0 * x
+    rho = 1.0 + 0.05 * np.sin(x) * np.cos(y)
+    u, v, w = 1.0 + 0.1 * np.sin(y), 0.1 * np.cos(x), 0.05 * np.sin(x + y + z)
+    p = 71.4285714285714 * (1.0 + 0.01 * np.cos(x + y))
+    if dims == 2:
+        return np.stack([rho, rho * u, rho * v, p / 0.4 + 0.5 * rho * (u * u + v * v)], -1)
+    return np.stack([rho, rho * u, rho * v, rho * w, p / 0.4 + 0.5 * rho * (u * u + v * v + w * w)], -1)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case,order", [("mixed_pritet_p3", 1), ("mixed_pritet_p3", 4), ("mixed_channel_p3", 1),
+                                        ("mixed_channel_p3", 4), ("mixed_hexpri_p3", 1), ("mixed_triquad_p3", 1),
+                                        ("mixed_triquad_p3", 4)])
+def test_fused_orders_1_and_4_match_the_operator_path(case, order):
+    """Orders 1 and 4 on the fixture meshes, set up by the library: the fused
+    stage's residual and its state after two RK45 steps match the
+    per-operator path's (the entry points pinned against the reference at
+    orders 2 and 3) at 1e-12."""
+    torch = pytest.importorskip("torch")
+    from hifiles_b200 import mixed as X
+    from hifiles_b200 import seam
+    from test_mixed_setup import fixture_mesh
+    meta, _ = load(case)
+    meta = dict(meta, order=order)
+    dims = int(meta.get("dims", 3))
+    xv, cells, period, bfaces, opts = fixture_mesh(meta)
+    opts.vcjh_scheme_tet = opts.vcjh_scheme_tri = 1  # DG: defined at every order
+    M = X.MixedMesh(order, xv, cells, period, bfaces, opts)
+    types, ints, bdys = M.operator_inputs({t: _smooth_state(m["pos_upts"], dims) for t, m in M.types.items()})
+    ref = seam.MixedOperatorMesh(types, ints, meta["physics"], bdys, meta["bdy"], meta["R_ref"])
+    fus = seam.FusedMixedMesh(types, ints, meta["physics"], bdys, meta["bdy"], meta["R_ref"])
+    ref.residual()
+    fus.residual()
+    torch.cuda.synchronize()
+    for t in M.types:
+        s = ref.S[t]
+        want = s["div"].cpu().numpy().reshape((s["nu"], s["E"], dims + 2), order="F")
+        assert rel(_div(fus, t), want) <= 1e-12, (case, order, t)
+    ref.advance(2, meta["dt"])
+    fus.advance(2, meta["dt"])
+    for t in M.types:
+        got, want = fus.get_state(t), ref.get_state(t)
+        assert np.isfinite(got).all()
+        assert rel(got, want) <= 1e-12, (case, order, t)
