@@ -432,9 +432,9 @@ class FusedMixedMesh:
     stage of include/fr_b200.h (`fr_mixed_stage_*`): per element type and RK
     stage one gradient kernel and one interface/update kernel, operator
     products on the FP64 tensor cores.  Navier-Stokes in 2-D (triangles,
-    quads) or 3-D (tets, prisms, hexes), orders 1 to 4 (hexes 1 to 3).  The state of type i is `S[i]["u"]`
-    (n_upts, n_eles, 5) on the device, advanced in place; `residual()` writes
-    `S[i]["div"]`."""
+    quads) or 3-D (tets, prisms, hexes), orders 1 to 4 (hexes 1 to 3).  The
+    state of type i is `S[i]["u"]` (n_upts, n_eles, n_fields) on the device,
+    advanced in place; `residual()` writes `S[i]["div"]`."""
 
     def __init__(self, types, int_inters, physics, bdy_inters=(), bdy=None, R_ref=1.0, device=0):
         import torch
