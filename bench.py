@@ -413,8 +413,10 @@ def measure_channel_fused(order, steps, warmup, n=(40, 20, 20), dt=2e-4, shapes=
     from hifiles_b200 import mixed as X
     from hifiles_b200 import seam
     xv, cells, period, bfaces = X.channel_mesh(n)
+    # the SD-like tet correction is tabulated for orders 2 and 3; DG elsewhere
     M = X.MixedMesh(order, xv, cells, period, bfaces,
-                    X.ElementOpts(vcjh_scheme_tet=2, vcjh_scheme_tri=1, vcjh_scheme_pri_1d=1))
+                    X.ElementOpts(vcjh_scheme_tet=2 if order in (2, 3) else 1, vcjh_scheme_tri=1,
+                                  vcjh_scheme_pri_1d=1))
     types, ints, bdys = M.operator_inputs({t: channel_state(m["pos_upts"]) for t, m in M.types.items()})
     f = seam.FusedMixedMesh(types, ints, CHANNEL_PHYSICS, bdys, CHANNEL_BDY, CHANNEL_R_REF)
     if shapes:
