@@ -304,9 +304,13 @@ fr_status fr_mixed_stage_create(int n_dims, int n_types, const fr_mixed_stage_ty
       return bail(mfail(FR_ERR_UNSUPPORTED, "fused mixed stage: no kernels for " + std::to_string(NU) +
                                                 " solution / " + std::to_string(NF) + " flux points"));
     s->kern.push_back(k);
-    int g0 = 0, u0 = 0;
-    while (!k.grad[g0]) g0++;
-    while (!k.upd1[u0]) u0++;
+    // defaults before any autotune: the shapes that measured fastest for
+    // tets (4 elements x 128 threads), else the first that fits
+    int g0 = 3, u0 = 1;
+    if (!k.grad[g0])
+      for (g0 = 0; !k.grad[g0];) g0++;
+    if (!k.upd1[u0])
+      for (u0 = 0; !k.upd1[u0];) u0++;
     s->gv.push_back(g0);
     s->uv.push_back(u0);
     off[i + 1] = off[i] + (long long)NF * ty.n_eles;

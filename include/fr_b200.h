@@ -695,8 +695,8 @@ fr_status fr_mixed_stage_advance(fr_mixed_stage* s, int n_steps, double dt, void
  * blocks per SM, 4 = 8 x 256 with registers for 2; update 0 = 8 x 256,
  * 1 = 4 x 128,
  * 2 = 8 x 128 (every shape gives the same bits; shapes whose shared memory
- * exceeds a block's return FR_ERR_UNSUPPORTED).  create() sets the first shape
- * that fits;
+ * exceeds a block's return FR_ERR_UNSUPPORTED).  create() sets gradient 3
+ * and update 1 (else the first shape that fits);
  * autotune() times every shape on the current state (the update kernels in
  * residual mode, into scratch memory; the state is not changed) and keeps
  * the fastest per type. */
