@@ -435,7 +435,11 @@ fr_status fr_mixed_stage_create(int n_dims, int n_types, const fr_mixed_stage_ty
   for (int i = 1; i < n_types; i++) {
     cudaStream_t q;
     cudaEvent_t ev;
-    if (cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking) != cudaSuccess)
+    // the side streams get the highest priority, so the small types' blocks
+    // take the SM slots that free up before the first type's remaining ones
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    if (cudaStreamCreateWithPriority(&q, cudaStreamNonBlocking, hi) != cudaSuccess)
       return bail(mfail(FR_ERR_CUDA, "stream creation failed"));
     s->side_streams.push_back(q);
     if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
