@@ -121,22 +121,35 @@ __device__ __forceinline__ void mma_unit(int u, const double* __restrict__ A1, B
     p1[j] = b1(n) + (lane & 3);
     p2[j] = KS2 > 0 ? b2(n) + (lane & 3) : p1[j];
   }
+  // operator fragments are fetched CH k-steps ahead of their MMAs, so their
+  // read-only-cache latency is paid once per CH steps
+  constexpr int CH = 8;
   const double* a1 = A1 + (size_t)mt * KS1 * 32 + lane;
-#pragma unroll 4
-  for (int ks = 0; ks < KS1; ks++) {
-    const double a = __ldg(a1 + ks * 32);
 #pragma unroll
-    for (int j = 0; j < TN; j++)
-      if (nt0 + j < NTL) dmma(acc[j], a, p1[j][ks * 4]);
+  for (int k0 = 0; k0 < KS1; k0 += CH) {
+    double af[CH];
+#pragma unroll
+    for (int i = 0; i < CH; i++) af[i] = k0 + i < KS1 ? __ldg(a1 + (k0 + i) * 32) : 0.0;
+#pragma unroll
+    for (int i = 0; i < CH; i++)
+      if (k0 + i < KS1)
+#pragma unroll
+        for (int j = 0; j < TN; j++)
+          if (nt0 + j < NTL) dmma(acc[j], af[i], p1[j][(k0 + i) * 4]);
   }
   if constexpr (KS2 > 0) {
     const double* a2 = A2 + (size_t)mt * KS2 * 32 + lane;
-#pragma unroll 4
-    for (int ks = 0; ks < KS2; ks++) {
-      const double a = __ldg(a2 + ks * 32);
 #pragma unroll
-      for (int j = 0; j < TN; j++)
-        if (nt0 + j < NTL) dmma(acc[j], a, p2[j][ks * 4]);
+    for (int k0 = 0; k0 < KS2; k0 += CH) {
+      double af[CH];
+#pragma unroll
+      for (int i = 0; i < CH; i++) af[i] = k0 + i < KS2 ? __ldg(a2 + (k0 + i) * 32) : 0.0;
+#pragma unroll
+      for (int i = 0; i < CH; i++)
+        if (k0 + i < KS2)
+#pragma unroll
+          for (int j = 0; j < TN; j++)
+            if (nt0 + j < NTL) dmma(acc[j], af[i], p2[j][(k0 + i) * 4]);
     }
   }
 #pragma unroll
