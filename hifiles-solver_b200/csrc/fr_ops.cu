@@ -224,12 +224,19 @@ dense_mma_kernel(int m, int k, long long ncols, int nd, OpSet ops, const double*
         const double* bp[kMmaTN];
 #pragma unroll
         for (int j = 0; j < kMmaTN; j++) bp[j] = sb + ((nt0 + j) * 8 + g) * ldk + t;
-#pragma unroll 4
-        for (int ks = 0; ks < KS; ks++) {
-          const int c = ks * 4 + t;
-          const double a = (r < m && c < k) ? __ldg(A + r + (size_t)m * c) : 0.0;
+        // operator fragments fetched 8 k-steps ahead of their MMAs
+        for (int k0 = 0; k0 < KS; k0 += 8) {
+          double af[8];
 #pragma unroll
-          for (int j = 0; j < kMmaTN; j++) dmma8(acc[j], a, bp[j][ks * 4]);
+          for (int i = 0; i < 8; i++) {
+            const int c = (k0 + i) * 4 + t;
+            af[i] = (k0 + i < KS && r < m && c < k) ? __ldg(A + r + (size_t)m * c) : 0.0;
+          }
+#pragma unroll
+          for (int i = 0; i < 8; i++)
+            if (k0 + i < KS)
+#pragma unroll
+              for (int j = 0; j < kMmaTN; j++) dmma8(acc[j], af[i], bp[j][(k0 + i) * 4]);
         }
       }
 #pragma unroll
