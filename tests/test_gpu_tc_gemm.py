@@ -233,3 +233,44 @@ def test_fp64_tensor_core_product_matches_cuda_cores(m, k, n):
     if m == k:
         for d in range(D):
             assert np.abs(out[(0, "fan")][..., d] - As[d] @ Bs[0]).max() <= 1e-13 * np.abs(ref).max() * k ** 0.5
+
+
+@pytest.mark.parametrize("nu,nf,E", [(20, 40, 300), (64, 96, 200), (40, 68, 77)])
+def test_fp64_tensor_core_products_that_add_to_their_output(nu, nf, E):
+    """The products that accumulate into existing data (beta = 1):
+    calculate_corrected_divergence (div += opp_3 (ntc - ntd)) and
+    correct_gradient (grad_d += opp_5[d] delta, then the JGinv/detJ
+    transform) give the same bits on the FP64 tensor cores (mode 0) as on the
+    CUDA cores (mode 3), and match numpy."""
+    rng = np.random.default_rng(nu + nf + E)
+    F, D = 5, 3
+    opp3 = rng.standard_normal((nu, nf))
+    opp5 = [rng.standard_normal((nu, nf)) for _ in range(D)]
+    ntd, ntc = rng.standard_normal((nf, E, F)), rng.standard_normal((nf, E, F))
+    div0 = rng.standard_normal((nu, E, F))
+    delta = rng.standard_normal((nf, E, F))
+    grad0 = rng.standard_normal((nu, E, F, D))
+    JG = rng.standard_normal((D, D, nu, E))
+    dj = 1.0 + rng.random((nu, E))
+    L = _lib()
+    d5 = [_dev(a) for a in opp5]
+    tab = (VP * D)(*[a.data_ptr() for a in d5])
+    out = {}
+    for mode in (0, 3):
+        assert L.fr_op_set_gemm_precision(mode) == 0
+        try:
+            dA, dntd, dntc, ddiv = _dev(opp3), _dev(ntd), _dev(ntc), _dev(div0)
+            st = L.fr_op_calculate_corrected_divergence(nu, nf, F, E, dA.data_ptr(), dntd.data_ptr(), dntc.data_ptr(),
+                                                        ddiv.data_ptr(), None)
+            assert st == 0, H.lib().fr_last_error().decode()
+            dd, dg, dJ, ddj = _dev(delta), _dev(grad0), _dev(JG), _dev(dj)
+            st = L.fr_op_correct_gradient(nu, nf, D, F, E, C.cast(tab, VP), dd.data_ptr(), dJ.data_ptr(),
+                                          ddj.data_ptr(), dg.data_ptr(), None)
+            assert st == 0, H.lib().fr_last_error().decode()
+            assert L.fr_op_check(None) == 0
+            out[mode] = (_host(ddiv, (nu, E, F)), _host(dg, (nu, E, F, D)))
+        finally:
+            L.fr_op_set_gemm_precision(0)
+    assert np.array_equal(out[0][0], out[3][0]) and np.array_equal(out[0][1], out[3][1])
+    want = div0 + np.einsum("uf,fek->uek", opp3, ntc - ntd)
+    assert np.abs(out[0][0] - want).max() <= 1e-13 * np.abs(want).max() * nf ** 0.5
