@@ -119,6 +119,7 @@ struct fr_mixed_stage {
   MixedFpts fp{};
   double* UF[2] = {nullptr, nullptr};
   int cur = 0;
+  int pf = 0;  // physics form: 0 Navier-Stokes, 1 Euler (Rusanov), 2 Euler (Roe)
   // element types after the first run on side streams, forked from and
   // joined to the caller's stream around each kernel of a stage
   bool concurrent = true;
@@ -166,7 +167,8 @@ fr_status launch_grad(fr_mixed_stage* s, int i, int v, const double* UFc, cudaSt
 {
   const MixedType& t = s->types[i];
   const MixedShape& g = kGradShapes[v];
-  s->kern[i].grad[v]<<<blocks_of(t.E, g.epb), g.nth, s->kern[i].smem_a[v], st>>>(t, s->fp, UFc, s->ph);
+  s->kern[i].grad[s->pf][v]<<<blocks_of(t.E, g.epb), g.nth, s->kern[i].smem_a[s->pf][v], st>>>(t, s->fp, UFc,
+                                                                                                 s->ph);
   return mlaunched("mixed_grad_kernel");
 }
 
@@ -178,7 +180,7 @@ fr_status launch_upd(fr_mixed_stage* s, int i, int v, int mode, int stage, doubl
                               0.153057247968152};
   const MixedType& t = s->types[i];
   const MixedShape& u = kUpdShapes[v];
-  auto k = mode ? s->kern[i].upd1[v] : s->kern[i].upd0[v];
+  auto k = mode ? s->kern[i].upd1[s->pf][v] : s->kern[i].upd0[s->pf][v];
   k<<<blocks_of(t.E, u.epb), u.nth, s->kern[i].smem_b[v], st>>>(t, s->fp, UFc, UFn, s->ph, A[stage], B[stage], dt);
   return mlaunched("mixed_update_kernel");
 }
@@ -234,18 +236,18 @@ fr_status launch_stage(fr_mixed_stage* s, int mode, int stage, double dt, cudaSt
   return FR_OK;
 }
 
-fr_status set_smem(const MixedKernels& k)
+fr_status set_smem(const MixedKernels& k, int pf)
 {
   std::vector<std::pair<const void*, size_t>> list;
-  for (int v = 0; v < kNGrad; v++) list.push_back({(const void*)k.grad[v], k.smem_a[v]});
+  for (int v = 0; v < kNGrad; v++) list.push_back({(const void*)k.grad[pf][v], k.smem_a[pf][v]});
   for (int v = 0; v < kNUpd; v++) {
-    list.push_back({(const void*)k.upd0[v], k.smem_b[v]});
-    list.push_back({(const void*)k.upd1[v], k.smem_b[v]});
+    list.push_back({(const void*)k.upd0[pf][v], k.smem_b[v]});
+    list.push_back({(const void*)k.upd1[pf][v], k.smem_b[v]});
   }
   list.push_back({(const void*)k.trace, k.smem_c});
   bool any_grad = false, any_upd = false;
-  for (int v = 0; v < kNGrad; v++) any_grad = any_grad || k.grad[v];
-  for (int v = 0; v < kNUpd; v++) any_upd = any_upd || k.upd1[v];
+  for (int v = 0; v < kNGrad; v++) any_grad = any_grad || k.grad[pf][v];
+  for (int v = 0; v < kNUpd; v++) any_upd = any_upd || k.upd1[pf][v];
   if (!any_grad || !any_upd || k.smem_c > kMixedSmemMax)
     return mfail(FR_ERR_UNSUPPORTED, "element type too large for one block of shared memory");
   for (auto& q : list) {
@@ -264,12 +266,18 @@ fr_status fr_mixed_stage_create(int n_dims, int n_types, const fr_mixed_stage_ty
                                 const int* const* int_tables, const int* int_nfpi, const long long* int_ni,
                                 int n_bdy_groups, const int* const* bdy_tables, const int* bdy_nfpi,
                                 const long long* bdy_ni, const double* bdy_params, double R_ref,
-                                const fr_phys_desc* phys, fr_mixed_stage** out)
+                                const fr_phys_desc* phys, int viscous, int riemann_solve_type,
+                                fr_mixed_stage** out)
 {
   g_err.clear();
   if (!out || !types || !phys || n_types < 1) return mfail(FR_ERR_ARG, "bad arguments");
   *out = nullptr;
   if (n_dims != 2 && n_dims != 3) return mfail(FR_ERR_UNSUPPORTED, "fused mixed stage: 2-D or 3-D meshes");
+  if (riemann_solve_type != 0 && riemann_solve_type != 2)
+    return mfail(FR_ERR_UNSUPPORTED, "fused mixed stage: riemann_solve_type 0 (Rusanov) or 2 (Roe)");
+  if (riemann_solve_type == 2 && (n_dims != 2 || viscous))
+    return mfail(FR_ERR_UNSUPPORTED, "fused mixed stage: the Roe flux with 2-D Euler only");
+  const int pf = viscous ? 0 : (riemann_solve_type == 2 ? 2 : 1);
   if ((n_int_groups > 0 && (!int_tables || !int_nfpi || !int_ni)) ||
       (n_bdy_groups > 0 && (!bdy_tables || !bdy_nfpi || !bdy_ni)) || n_int_groups < 0 || n_bdy_groups < 0)
     return mfail(FR_ERR_ARG, "null interface table");
@@ -282,6 +290,7 @@ fr_status fr_mixed_stage_create(int n_dims, int n_types, const fr_mixed_stage_ty
   s->D = D;
   s->F = F;
   s->n_types = n_types;
+  s->pf = pf;
   {
     Phys q{phys->gamma, phys->prandtl, phys->mu_inf, phys->rt_inf, phys->c_sth, phys->fix_vis, phys->tau,
            phys->pen_fact};
@@ -293,11 +302,11 @@ fr_status fr_mixed_stage_create(int n_dims, int n_types, const fr_mixed_stage_ty
   for (int i = 0; i < n_types; i++) {
     const fr_mixed_stage_type& ty = types[i];
     const int NU = ty.n_upts, NF = ty.n_fpts;
-    if (NU <= 0 || NF <= 0 || ty.n_eles < 0 || !ty.disu_upts || !ty.opp_0 || !ty.opp_3 || !ty.opp_6 ||
-        !ty.JGinv_upts || !ty.detjac_upts || !ty.tdA_fpts || !ty.norm_fpts)
+    if (NU <= 0 || NF <= 0 || ty.n_eles < 0 || !ty.disu_upts || !ty.opp_0 || !ty.opp_3 ||
+        (viscous && !ty.opp_6) || !ty.JGinv_upts || !ty.detjac_upts || !ty.tdA_fpts || !ty.norm_fpts)
       return bail(mfail(FR_ERR_ARG, "bad element type description"));
     for (int d = 0; d < D; d++)
-      if (!ty.opp_1[d] || !ty.opp_2[d] || !ty.opp_4[d] || !ty.opp_5[d])
+      if (!ty.opp_1[d] || !ty.opp_2[d] || (viscous && (!ty.opp_4[d] || !ty.opp_5[d])))
         return bail(mfail(FR_ERR_ARG, "missing operator"));
     MixedKernels k;
     if (!find_kernels(D, NU, NF, &k))
@@ -307,10 +316,12 @@ fr_status fr_mixed_stage_create(int n_dims, int n_types, const fr_mixed_stage_ty
     // defaults before any autotune: the shapes that measured fastest for
     // tets (4 elements x 128 threads), else the first that fits
     int g0 = 3, u0 = 1;
-    if (!k.grad[g0])
-      for (g0 = 0; !k.grad[g0];) g0++;
-    if (!k.upd1[u0])
-      for (u0 = 0; !k.upd1[u0];) u0++;
+    if (!k.grad[pf][g0])
+      for (g0 = 0; g0 < kNGrad - 1 && !k.grad[pf][g0];) g0++;
+    if (!k.upd1[pf][u0])
+      for (u0 = 0; u0 < kNUpd - 1 && !k.upd1[pf][u0];) u0++;
+    if (!k.grad[pf][g0] || !k.upd1[pf][u0])
+      return bail(mfail(FR_ERR_UNSUPPORTED, "element type too large for one block of shared memory"));
     s->gv.push_back(g0);
     s->uv.push_back(u0);
     off[i + 1] = off[i] + (long long)NF * ty.n_eles;
@@ -380,7 +391,7 @@ fr_status fr_mixed_stage_create(int n_dims, int n_types, const fr_mixed_stage_ty
   }
   // every check above is on the host: device work starts here
   for (const MixedKernels& k : s->kern)
-    if (fr_status e = set_smem(k)) return bail(e);
+    if (fr_status e = set_smem(k, s->pf)) return bail(e);
   // operators in fragment order
   for (int i = 0; i < n_types; i++) {
     const fr_mixed_stage_type& ty = types[i];
@@ -393,12 +404,14 @@ fr_status fr_mixed_stage_create(int n_dims, int n_types, const fr_mixed_stage_ty
     t.off = off[i];
     auto cm = [](const double* a, int rows) { return [a, rows](int r, int c) { return a[r + (size_t)rows * c]; }; };
     std::vector<double> h;
-    h = fragments(D * NU, NU, [&](int r, int c) { return ty.opp_4[r / NU][r % NU + (size_t)NU * c]; });
-    if (fr_status e = s->upload(h, &t.A45u)) return bail(e);
-    h = fragments(D * NU, NF, [&](int r, int c) { return ty.opp_5[r / NU][r % NU + (size_t)NU * c]; });
-    if (fr_status e = s->upload(h, &t.A45f)) return bail(e);
-    h = fragments(NF, NU, cm(ty.opp_6, NF));
-    if (fr_status e = s->upload(h, &t.A6)) return bail(e);
+    if (viscous) {  // the gradient's operators (opp_4, opp_5, opp_6)
+      h = fragments(D * NU, NU, [&](int r, int c) { return ty.opp_4[r / NU][r % NU + (size_t)NU * c]; });
+      if (fr_status e = s->upload(h, &t.A45u)) return bail(e);
+      h = fragments(D * NU, NF, [&](int r, int c) { return ty.opp_5[r / NU][r % NU + (size_t)NU * c]; });
+      if (fr_status e = s->upload(h, &t.A45f)) return bail(e);
+      h = fragments(NF, NU, cm(ty.opp_6, NF));
+      if (fr_status e = s->upload(h, &t.A6)) return bail(e);
+    }
     h = fragments(NF, D * NU, [&](int r, int c) { return ty.opp_1[c / NU][r + (size_t)NF * (c % NU)]; });
     if (fr_status e = s->upload(h, &t.A1)) return bail(e);
     h = fragments(NU, D * NU, [&](int r, int c) { return ty.opp_2[c / NU][r + (size_t)NU * (c % NU)]; });
@@ -486,7 +499,7 @@ fr_status fr_mixed_stage_set_launch(fr_mixed_stage* s, int type, int grad_shape,
   if (!s || type < 0 || type >= s->n_types || grad_shape < 0 || grad_shape >= kNGrad || update_shape < 0 ||
       update_shape >= kNUpd)
     return mfail(FR_ERR_ARG, "bad type or launch shape");
-  if (!s->kern[type].grad[grad_shape] || !s->kern[type].upd1[update_shape])
+  if (!s->kern[type].grad[s->pf][grad_shape] || !s->kern[type].upd1[s->pf][update_shape])
     return mfail(FR_ERR_UNSUPPORTED, "launch shape exceeds shared memory for this element type");
   s->gv[type] = grad_shape;
   s->uv[type] = update_shape;
@@ -537,7 +550,7 @@ fr_status fr_mixed_stage_autotune(fr_mixed_stage* s, void* stream)
       float best = 0.f;
       bool have = false;
       for (int v = 0; v < nv && rc == FR_OK; v++) {
-        if (pass == 0 ? !s->kern[i].grad[v] : !s->kern[i].upd0[v]) continue;
+        if (pass == 0 ? !s->kern[i].grad[s->pf][v] : !s->kern[i].upd0[s->pf][v]) continue;
         // one untimed launch, then the timed ones
         for (int r = 0; r <= reps && rc == FR_OK; r++) {
           if (r == 1) cudaEventRecord(e0, st);

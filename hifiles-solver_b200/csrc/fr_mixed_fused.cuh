@@ -446,11 +446,80 @@ __global__ void __launch_bounds__(NTH, MINB) mixed_grad_kernel(MixedType t, Mixe
   }
 }
 
+// ------------------------------------------------------ kernel A, Euler form
+// The inviscid stage needs no gradient: the transformed inviscid flux at the
+// solution points (evaluate_invFlux), then norm_tdisf = sum_d opp_1[d] f_d
+// and div_tdisf = sum_d opp_2[d] f_d.  JGinv is read through the L1 cache.
+template <int D, int NU, int NF, int EPB>
+struct MPlanInv {
+  using Q = MPlan<D, NU, NF, EPB>;
+  static constexpr int oU = 0, oT = Q::NP * Q::ldU, nI = oT + Q::NP * Q::ldT;
+};
+
+template <int D, int NU, int NF, int EPB, int NTH, int MINB>
+__global__ void __launch_bounds__(NTH, MINB) mixed_inv_kernel(MixedType t, MixedFpts m,
+                                                              const double* __restrict__ UFc, PhysT<double> ph)
+{
+  using Q = MPlan<D, NU, NF, EPB>;
+  using I = MPlanInv<D, NU, NF, EPB>;
+  constexpr int F = D + 2, NW = NTH / 32, DD = D * D;
+  extern __shared__ __align__(16) double msm[];
+  double* sU = msm + I::oU;
+  double* sT = msm + I::oT;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const long long E = t.E, e0 = (long long)blockIdx.x * EPB;
+  const int nval = (int)(E - e0 < EPB ? E - e0 : EPB), nuv = nval * NU;
+  (void)m;
+  (void)UFc;
+  zero_pad_rows<NU, c4(NU), Q::ldU, Q::NP, NTH>(sU);
+  zero_pad_rows<D * NU, c4(D * NU), Q::ldT, Q::NP, NTH>(sT);
+  load_state<F, NU, EPB, Q::ldU, NTH>(sU, t.U, e0, E, nval);
+  cp_async_wait_all();
+  __syncthreads();
+  for (int i = tid; i < nuv; i += NTH) {
+    const int el = i / NU, p = i - el * NU;
+    const double* G = t.JG + (size_t)DD * ((size_t)NU * e0 + i);
+    double q[F], fi[F][D];
+#pragma unroll
+    for (int k = 0; k < F; k++) q[k] = sU[(el * F + k) * Q::ldU + p];
+    inv_flux<D, double>(ph, q, fi);
+#pragma unroll
+    for (int k = 0; k < F; k++)
+#pragma unroll
+      for (int l = 0; l < D; l++) {
+        double acc = 0.0;
+#pragma unroll
+        for (int mm = 0; mm < D; mm++) acc = fma(G[l + D * mm], fi[k][mm], acc);
+        sT[(el * F + k) * Q::ldT + l * NU + p] = acc;
+      }
+  }
+  __syncthreads();
+  auto bt = [&](int n) { return sT + n * Q::ldT; };
+  const size_t NFE = (size_t)NF * E, NUE = (size_t)NU * E;
+  auto put = [&](double* out, int rows, size_t stride, int r, int n, double v) {
+    const int el = n / F, k = n - el * F;
+    if (r < rows && el < nval) out[r + (size_t)rows * (e0 + el) + stride * k] = v;
+  };
+  auto epi_nd = [&](int r, int n, double v0, double v1) {
+    put(t.ND, NF, NFE, r, n, v0);
+    put(t.ND, NF, NFE, r, n + 1, v1);
+  };
+  auto epi_dv = [&](int r, int n, double v0, double v1) {
+    put(t.DV, NU, NUE, r, n, v0);
+    put(t.DV, NU, NUE, r, n + 1, v1);
+  };
+  constexpr int U1 = units<Q::NTL, Q::TN>(Q::MT_F), U2 = units<Q::NTL, Q::TN>(Q::MT_U);
+  for (int u = warp; u < U1 + U2; u += NW) {
+    if (u < U1) mma_unit<Q::NTL, Q::TN, Q::KS_T, 0>(u, t.A1, bt, t.A1, bt, epi_nd);
+    else mma_unit<Q::NTL, Q::TN, Q::KS_T, 0>(u - U1, t.A2, bt, t.A2, bt, epi_dv);
+  }
+}
+
 // ------------------------------------------------------------------ kernel B
 // MODE 1: RK45 stage update (rk_a, rk_b, dt) and the new traces into UFn;
 // MODE 0: div_tconf_upts into t.DIV only.  Like kernel A, a load phase first
 // stages every global read of the block in shared memory.
-template <int D, int NU, int NF, int EPB, int NTH, int MINB, int MODE>
+template <int D, int NU, int NF, int EPB, int NTH, int MINB, int MODE, int VISC = 1, int RIEMANN = 0>
 __global__ void __launch_bounds__(NTH, MINB) mixed_update_kernel(MixedType t, MixedFpts m,
                                                                  const double* __restrict__ UFc,
                                                                  double* __restrict__ UFn, PhysT<double> ph,
@@ -491,8 +560,9 @@ __global__ void __launch_bounds__(NTH, MINB) mixed_update_kernel(MixedType t, Mi
       cp_async<8>(&sUo[k * EF + r], UFc + g + NT * k);
       cp_async<8>(dj + k * Q::ldF, nd + NFE * k);
     }
+    if constexpr (VISC != 0)
 #pragma unroll
-    for (int k = 0; k < F - 1; k++) cp_async<8>(&sVo[k * EF + r], m.VF + g + NT * k);
+      for (int k = 0; k < F - 1; k++) cp_async<8>(&sVo[k * EF + r], m.VF + g + NT * k);
 #pragma unroll
     for (int d = 0; d < D; d++) cp_async<8>(&sNL[d * EF + r], m.nL + g + NT * d);
     cp_async<4>(&sMate[r], m.mate + g);
@@ -518,8 +588,9 @@ __global__ void __launch_bounds__(NTH, MINB) mixed_update_kernel(MixedType t, Mi
     if (mt < 0) continue;
 #pragma unroll
     for (int k = 0; k < F; k++) cp_async<8>(&sUN[k * EF + r], UFc + mt + NT * k);
+    if constexpr (VISC != 0)
 #pragma unroll
-    for (int k = 0; k < F - 1; k++) cp_async<8>(&sVN[k * EF + r], m.VF + mt + NT * k);
+      for (int k = 0; k < F - 1; k++) cp_async<8>(&sVN[k * EF + r], m.VF + mt + NT * k);
   }
   cp_async_wait_all();
   __syncthreads();
@@ -539,12 +610,12 @@ __global__ void __launch_bounds__(NTH, MINB) mixed_update_kernel(MixedType t, Mi
 #pragma unroll
       for (int k = 0; k < F; k++) {
         q.ul[k] = uo[k];
-        q.bv[k] = m.BV[(size_t)(-1 - (long long)mt) * F + k];
+        q.bv[k] = VISC ? m.BV[(size_t)(-1 - (long long)mt) * F + k] : 0.0;
       }
 #pragma unroll
       for (int d = 0; d < D; d++) q.n[d] = n[d];
       q.tl = tl;
-      fu_boundary<D, 1, double, 0>(ph, sd >> 2, q, c, 1);
+      fu_boundary<D, VISC, double, RIEMANN>(ph, sd >> 2, q, c, 1);
     } else {
       const bool left = sd & 1;
       double ul[F], ur[F], fn[F];
@@ -554,18 +625,21 @@ __global__ void __launch_bounds__(NTH, MINB) mixed_update_kernel(MixedType t, Mi
         ul[k] = left ? uo[k] : v;
         ur[k] = left ? v : uo[k];
       }
-      rusanov<D, double>(ph, ul, ur, n, fn);
+      if constexpr (RIEMANN == 2 && D == 2) roe<double>(ph, ul, ur, n, fn);
+      else rusanov<D, double>(ph, ul, ur, n, fn);
 #pragma unroll
       for (int k = 0; k < F; k++) c[k] = left ? fn[k] * tl : -fn[k] * tl;
-      double nn = n[0] * n[0];
+      if constexpr (VISC != 0) {
+        double nn = n[0] * n[0];
 #pragma unroll
-      for (int d = 1; d < D; d++) nn = fma(n[d], n[d], nn);
-      const double pen = ldg_beta<D, double>(ph.pen_fact, n);
+        for (int d = 1; d < D; d++) nn = fma(n[d], n[d], nn);
+        const double pen = ldg_beta<D, double>(ph.pen_fact, n);
 #pragma unroll
-      for (int k = 0; k < F; k++) {
-        const double ao = k ? sVo[(k - 1) * EF + i] : 0.0, an = k ? sVN[(k - 1) * EF + i] : 0.0;
-        const double fv = ldg_normal<double>(left ? ao : an, left ? an : ao, ul[k], ur[k], pen, ph.tau, nn);
-        c[k] = left ? c[k] + fv * tl : c[k] + (-fv) * tl;
+        for (int k = 0; k < F; k++) {
+          const double ao = k ? sVo[(k - 1) * EF + i] : 0.0, an = k ? sVN[(k - 1) * EF + i] : 0.0;
+          const double fv = ldg_normal<double>(left ? ao : an, left ? an : ao, ul[k], ur[k], pen, ph.tau, nn);
+          c[k] = left ? c[k] + fv * tl : c[k] + (-fv) * tl;
+        }
       }
     }
 #pragma unroll
@@ -672,11 +746,16 @@ using GradFn = void (*)(MixedType, MixedFpts, const double*, PhysT<double>);
 using UpdFn = void (*)(MixedType, MixedFpts, const double*, double*, PhysT<double>, double, double, double);
 using TraceFn = void (*)(MixedType, long long, double*);
 
+// Physics forms: 0 Navier-Stokes (Rusanov + LDG), 1 Euler with Rusanov,
+// 2 Euler with Roe (2-D).  The Euler forms have one launch shape (gradient
+// slot 1: the flux kernel of 4 elements x 128 threads; update 1).
+constexpr int kNForms = 3;
+
 struct MixedKernels {
   int D, NU, NF;
-  GradFn grad[kNGrad];
-  size_t smem_a[kNGrad];
-  UpdFn upd0[kNUpd], upd1[kNUpd];
+  GradFn grad[kNForms][kNGrad];
+  size_t smem_a[kNForms][kNGrad];
+  UpdFn upd0[kNForms][kNUpd], upd1[kNForms][kNUpd];
   size_t smem_b[kNUpd];
   TraceFn trace;
   size_t smem_c;
@@ -686,8 +765,8 @@ template <int D, int NU, int NF, int V>
 void fill_grad(MixedKernels& k)
 {
   constexpr MixedShape g = kGradShapes[V];
-  k.smem_a[V] = sizeof(double) * MPlan<D, NU, NF, g.epb, g.minb>::nA;
-  k.grad[V] = k.smem_a[V] <= kMixedSmemMax ? mixed_grad_kernel<D, NU, NF, g.epb, g.nth, g.minb> : nullptr;
+  k.smem_a[0][V] = sizeof(double) * MPlan<D, NU, NF, g.epb, g.minb>::nA;
+  k.grad[0][V] = k.smem_a[0][V] <= kMixedSmemMax ? mixed_grad_kernel<D, NU, NF, g.epb, g.nth, g.minb> : nullptr;
 }
 
 template <int D, int NU, int NF, int V>
@@ -696,14 +775,32 @@ void fill_upd(MixedKernels& k)
   constexpr MixedShape u = kUpdShapes[V];
   k.smem_b[V] = sizeof(double) * MPlan<D, NU, NF, u.epb>::nB;
   const bool fits = k.smem_b[V] <= kMixedSmemMax;
-  k.upd0[V] = fits ? mixed_update_kernel<D, NU, NF, u.epb, u.nth, u.minb, 0> : nullptr;
-  k.upd1[V] = fits ? mixed_update_kernel<D, NU, NF, u.epb, u.nth, u.minb, 1> : nullptr;
+  k.upd0[0][V] = fits ? mixed_update_kernel<D, NU, NF, u.epb, u.nth, u.minb, 0> : nullptr;
+  k.upd1[0][V] = fits ? mixed_update_kernel<D, NU, NF, u.epb, u.nth, u.minb, 1> : nullptr;
+}
+
+template <int D, int NU, int NF>
+void fill_euler(MixedKernels& k)
+{
+  constexpr MixedShape g = kGradShapes[1], u = kUpdShapes[1];
+  const size_t sa = sizeof(double) * MPlanInv<D, NU, NF, g.epb>::nI;
+  const bool fa = sa <= kMixedSmemMax, fb = k.smem_b[1] <= kMixedSmemMax;
+  for (int f = 1; f < kNForms; f++) {
+    k.smem_a[f][1] = sa;
+    k.grad[f][1] = fa ? mixed_inv_kernel<D, NU, NF, g.epb, g.nth, g.minb> : nullptr;
+  }
+  k.upd0[1][1] = fb ? mixed_update_kernel<D, NU, NF, u.epb, u.nth, u.minb, 0, 0, 0> : nullptr;
+  k.upd1[1][1] = fb ? mixed_update_kernel<D, NU, NF, u.epb, u.nth, u.minb, 1, 0, 0> : nullptr;
+  if constexpr (D == 2) {
+    k.upd0[2][1] = fb ? mixed_update_kernel<D, NU, NF, u.epb, u.nth, u.minb, 0, 0, 2> : nullptr;
+    k.upd1[2][1] = fb ? mixed_update_kernel<D, NU, NF, u.epb, u.nth, u.minb, 1, 0, 2> : nullptr;
+  }
 }
 
 template <int D, int NU, int NF>
 MixedKernels mixed_kernels()
 {
-  MixedKernels k;
+  MixedKernels k{};
   k.D = D;
   k.NU = NU;
   k.NF = NF;
@@ -716,6 +813,7 @@ MixedKernels mixed_kernels()
   fill_upd<D, NU, NF, 1>(k);
   fill_upd<D, NU, NF, 2>(k);
   static_assert(kNGrad == 5 && kNUpd == 3, "one fill per shape");
+  fill_euler<D, NU, NF>(k);
   k.trace = mixed_trace_kernel<D, NU, NF, kMixedEPB, kMixedNT>;
   k.smem_c = sizeof(double) * MPlan<D, NU, NF, kMixedEPB>::nC;
   return k;

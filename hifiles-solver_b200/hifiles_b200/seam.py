@@ -411,7 +411,7 @@ class _MixedStageType(C.Structure):
 
 def _bind_stage(L):
     i, vp, ll = C.c_int, _VP, C.c_longlong
-    L.fr_mixed_stage_create.argtypes = [i, i, vp, i, vp, vp, vp, i, vp, vp, vp, vp, C.c_double, vp, vp]
+    L.fr_mixed_stage_create.argtypes = [i, i, vp, i, vp, vp, vp, i, vp, vp, vp, vp, C.c_double, vp, i, i, vp]
     L.fr_mixed_stage_destroy.argtypes = [vp]
     L.fr_mixed_stage_residual.argtypes = [vp, vp]
     L.fr_mixed_stage_advance.argtypes = [vp, i, C.c_double, vp]
@@ -431,12 +431,14 @@ class FusedMixedMesh:
     """The mesh of `MixedOperatorMesh` (same arguments) advanced by the fused
     stage of include/fr_b200.h (`fr_mixed_stage_*`): per element type and RK
     stage one gradient kernel and one interface/update kernel, operator
-    products on the FP64 tensor cores.  Navier-Stokes in 2-D (triangles,
-    quads) or 3-D (tets, prisms, hexes), orders 1 to 4 (hexes 1 to 3).  The
+    products on the FP64 tensor cores.  Navier-Stokes (viscous) or Euler
+    (Rusanov, or Roe in 2-D: riemann 2) in 2-D (triangles, quads) or 3-D
+    (tets, prisms, hexes), orders 1 to 4 (hexes 1 to 3).  The
     state of type i is `S[i]["u"]` (n_upts, n_eles, n_fields) on the device,
     advanced in place; `residual()` writes `S[i]["div"]`."""
 
-    def __init__(self, types, int_inters, physics, bdy_inters=(), bdy=None, R_ref=1.0, device=0):
+    def __init__(self, types, int_inters, physics, bdy_inters=(), bdy=None, R_ref=1.0, device=0, viscous=True,
+                 riemann=0):
         import torch
         self.torch = torch
         self.L = _bind_stage(lib())
@@ -465,8 +467,11 @@ class FusedMixedMesh:
             self.S[k] = s
             d = descs[j]
             d.n_upts, d.n_fpts, d.n_eles = nu, nf, E
-            d.opp_0, d.opp_3, d.opp_6 = host(ty["opp_0"]), host(ty["opp_3"]), host(ty["opp_6"])
+            d.opp_0, d.opp_3 = host(ty["opp_0"]), host(ty["opp_3"])
+            d.opp_6 = host(ty["opp_6"]) if ty.get("opp_6") is not None else None
             for name in ("opp_1", "opp_2", "opp_4", "opp_5"):
+                if ty.get(name) is None:
+                    continue  # Euler: no gradient operators
                 arr = getattr(d, name)
                 for q in range(D):
                     arr[q] = host(ty[name][q])
@@ -496,7 +501,8 @@ class FusedMixedMesh:
         self.ph = PhysDesc(**physics)
         h = _VP()
         _check(self.L.fr_mixed_stage_create(D, len(keys), descs, ni_, ip, inf, inn, nb_, bp, bnf, bnn, bdy_arr,
-                                            float(R_ref), C.byref(self.ph), C.byref(h)))
+                                            float(R_ref), C.byref(self.ph), int(bool(viscous)), int(riemann),
+                                            C.byref(h)))
         self.h = h
         self._pos = pos
         self.stream = torch.cuda.current_stream(dev)
@@ -598,10 +604,11 @@ def mixed_mesh_inputs(meta, arrays, state_key="disu_upts_init"):
     dims = int(meta.get("dims", 3))
     for t in meta["types"]:
         X = "t%d_" % t["ele_type"]
-        ty = {k: arrays[X + k] for k in ("opp_0", "opp_3", "opp_6", "JGinv_upts", "detjac_upts", "tdA_fpts",
-                                         "norm_fpts")}
-        for w in (1, 2, 4, 5):
-            ty["opp_%d" % w] = [arrays[X + "opp_%d_%d" % (w, d)] for d in range(dims)]
+        ty = {k: arrays.get(X + k) for k in ("opp_0", "opp_3", "opp_6", "JGinv_upts", "detjac_upts", "tdA_fpts",
+                                             "norm_fpts")}
+        for w in (1, 2, 4, 5):  # an Euler run's objects have no opp_4 / opp_5 / opp_6
+            ops = [arrays.get(X + "opp_%d_%d" % (w, d)) for d in range(dims)]
+            ty["opp_%d" % w] = None if any(o is None for o in ops) else ops
         ty["u"] = arrays[X + state_key]
         types[t["index"]] = ty
     ints = [arrays["int_inters_%d" % it["index"]] for it in meta["inters"]]

@@ -646,8 +646,10 @@ fr_status fr_mixed_bdy_inters(const fr_mixed* m, int group, int* n_fpts_per_inte
  * every interface type calculate_common_invFlux; correct_gradient,
  * extrapolate_corrected_gradient, evaluate_viscFlux, extrapolate_totalFlux,
  * calculate_divergence; calculate_common_viscFlux; calculate_corrected_divergence)
- * and AdvanceSolution (src/eles.cpp:1155-1178), Navier-Stokes, Rusanov +
- * LDG, 2-D or 3-D, in two kernels per element type and stage whose operator
+ * and AdvanceSolution (src/eles.cpp:1155-1178) -- Navier-Stokes (viscous 1;
+ * Rusanov + LDG) or Euler (viscous 0; Rusanov, or Roe in 2-D with
+ * riemann_solve_type 2), 2-D or 3-D -- in two kernels per element type and
+ * stage whose operator
  * products run on the FP64 tensor cores.  Inputs are what the per-operator
  * entry points take: each type's operators and metrics as its eles object
  * holds them (host arrays, column-major, the layouts of the fr_op_* calls;
@@ -670,7 +672,7 @@ typedef struct {
   const double* opp_3;       /* (n_upts, n_fpts)                      */
   const double* opp_4[3];    /* (n_upts, n_upts) per dimension         */
   const double* opp_5[3];    /* (n_upts, n_fpts) per dimension         */
-  const double* opp_6;       /* (n_fpts, n_upts)                      */
+  const double* opp_6;       /* (n_fpts, n_upts); opp_4/5/6 may be NULL for Euler */
   const double* JGinv_upts;  /* (n_dims, n_dims, n_upts, n_eles)      */
   const double* detjac_upts; /* (n_upts, n_eles)                      */
   const double* tdA_fpts;    /* (n_fpts, n_eles)                      */
@@ -684,7 +686,8 @@ fr_status fr_mixed_stage_create(int n_dims, int n_types, const fr_mixed_stage_ty
                                 const int* const* int_tables, const int* int_nfpi, const long long* int_ni,
                                 int n_bdy_groups, const int* const* bdy_tables, const int* bdy_nfpi,
                                 const long long* bdy_ni, const double* bdy_params, double R_ref,
-                                const fr_phys_desc* phys, fr_mixed_stage** out);
+                                const fr_phys_desc* phys, int viscous, int riemann_solve_type,
+                                fr_mixed_stage** out);
 fr_status fr_mixed_stage_destroy(fr_mixed_stage* s);
 /* div_tconf_upts of every type for the current state (one CalcResidual). */
 fr_status fr_mixed_stage_residual(fr_mixed_stage* s, void* stream);

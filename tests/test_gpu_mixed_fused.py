@@ -32,14 +32,24 @@ def _div(m, i):
     return s["div"].cpu().numpy().reshape((s["nu"], s["E"], m.F), order="F")
 
 
+# quadrilateral boxes with a boundary on every side, made by the reference:
+# Euler with characteristic / subsonic outflow / slip wall / dual-consistent
+# slip wall and with simple and supersonic in- and outflow, Navier-Stokes with
+# characteristic in- and outflow and moving isothermal and adiabatic walls,
+# the Roe flux with boundaries and periodic
+SEAM_2D = ["seam_quad_bc_euler_p3", "seam_quad_bc_euler2_p2", "seam_quad_ns_bc_p3", "seam_quad_roe_bc_p3",
+           "seam_quad_roe_p3_jit"]
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", FUSED)
+@pytest.mark.parametrize("case", FUSED + SEAM_2D)
 def test_fused_stage_matches_the_reference(case):
     torch = pytest.importorskip("torch")
     from hifiles_b200 import seam
     meta, a = load(case)
     types, ints, bdys = seam.mixed_mesh_inputs(meta, a)
-    m = seam.FusedMixedMesh(types, ints, meta["physics"], bdys, meta["bdy"], meta["R_ref"])
+    m = seam.FusedMixedMesh(types, ints, meta["physics"], bdys, meta["bdy"], meta["R_ref"],
+                            viscous=bool(meta.get("viscous", 1)), riemann=int(meta.get("riemann", 0)))
     assert m.launches_per_stage == 2 * len(types)
     m.residual()
     torch.cuda.synchronize()
@@ -127,7 +137,7 @@ def test_fused_stage_rejects_unsupported_meshes():
     ph = seam.PhysDesc(**CHANNEL_PHYSICS)
     d = (seam._MixedStageType * 1)()
     h = C.c_void_p()
-    st = L.fr_mixed_stage_create(1, 1, d, 0, None, None, None, 0, None, None, None, None, 1.0, C.byref(ph),
+    st = L.fr_mixed_stage_create(1, 1, d, 0, None, None, None, 0, None, None, None, None, 1.0, C.byref(ph), 1, 0,
                                  C.byref(h))
     assert st == FR_ERR_UNSUPPORTED and "3-D" in H.lib().fr_last_error().decode()
     # a hex of order 4 (125 solution, 150 flux points) has no kernels
@@ -140,11 +150,11 @@ def test_fused_stage_rejects_unsupported_meshes():
         arr = getattr(d[0], name)
         for q in range(3):
             arr[q] = p
-    st = L.fr_mixed_stage_create(3, 1, d, 0, None, None, None, 0, None, None, None, None, 1.0, C.byref(ph),
+    st = L.fr_mixed_stage_create(3, 1, d, 0, None, None, None, 0, None, None, None, None, 1.0, C.byref(ph), 1, 0,
                                  C.byref(h))
     assert st == FR_ERR_UNSUPPORTED and "125" in H.lib().fr_last_error().decode()
     d[0].n_upts = 0
-    st = L.fr_mixed_stage_create(3, 1, d, 0, None, None, None, 0, None, None, None, None, 1.0, C.byref(ph),
+    st = L.fr_mixed_stage_create(3, 1, d, 0, None, None, None, 0, None, None, None, None, 1.0, C.byref(ph), 1, 0,
                                  C.byref(h))
     assert st == FR_ERR_ARG
     assert not h.value
@@ -213,7 +223,8 @@ def test_fused_stage_rejects_bad_wiring_before_device_work():
         ni, ip, inf, inn = pack(ints)
         nb, bp, bnf, bnn = pack(bdys)
         h = C.c_void_p()
-        st = L.fr_mixed_stage_create(3, 1, d, ni, ip, inf, inn, nb, bp, bnf, bnn, None, 1.0, C.byref(ph), C.byref(h))
+        st = L.fr_mixed_stage_create(3, 1, d, ni, ip, inf, inn, nb, bp, bnf, bnn, None, 1.0, C.byref(ph), 1, 0,
+                                     C.byref(h))
         assert not h.value
         return st, H.lib().fr_last_error().decode()
 
