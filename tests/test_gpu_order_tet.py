@@ -81,3 +81,45 @@ def test_entropy_wave_convergence_rate_on_tetrahedra(P):
     print("tets P=%d errors %s rates %s" % (P, ["%.3e" % e for e in errs], ["%.2f" % r for r in rates]))
     assert all(np.isfinite(errs))
     assert rates[-1] > MIN_RATE[P], (errs, rates)
+
+
+def prism_box(n, L=2.0):
+    """Vertices and prisms of a periodic n^3 box: each x-y square split along
+    its (0,0)-(1,1) diagonal into two triangles, extruded in z."""
+    from hifiles_b200 import mixed as X
+    xv, _ = X.box_mesh(3, (n, n, n), (0.0, 0.0, 0.0), (L, L, L))
+    v = n + 1
+    vid = lambda i, j, k: i + v * (j + v * k)  # noqa: E731
+    cells = []
+    for k in range(n):
+        for j in range(n):
+            for i in range(n):
+                for tri in (((0, 0), (1, 0), (1, 1)), ((0, 0), (1, 1), (0, 1))):
+                    bot = [vid(i + a, j + b, k) for a, b in tri]
+                    top = [vid(i + a, j + b, k + 1) for a, b in tri]
+                    cells.append((X.PRISM, bot + top))
+    return xv, cells
+
+
+@pytest.mark.parametrize("P", [1, 2, 3])
+def test_entropy_wave_convergence_rate_on_prisms(P):
+    """The same entropy wave on 2 n^3 prisms (n = 4, 8, 16, 32).  Measured
+    rates: 2.73, 2.46, 2.13 (P = 1); 2.35, 2.63, 2.84 (P = 2); 4.41, 4.04, 3.99 (P = 3)."""
+    from hifiles_b200 import mixed as X
+    from hifiles_b200 import seam
+    errs = []
+    for n in NS:
+        xv, cells = prism_box(n)
+        M = X.MixedMesh(P, xv, cells, [2.0, 2.0, 2.0], [], X.ElementOpts(vcjh_scheme_tri=1, vcjh_scheme_pri_1d=1))
+        ty = M.types[X.PRISM]
+        pos = ty["pos_upts"]
+        types, ints, bdys = M.operator_inputs({X.PRISM: wave(pos)})
+        m = seam.FusedMixedMesh(types, ints, EULER, bdys, viscous=False)
+        m.advance(int(round(T_END / DT)), DT)
+        u = m.get_state(X.PRISM)
+        w = np.asarray(ty["detjac_upts"])
+        errs.append(np.sqrt(np.sum(w * (u[..., 0] - wave(pos, T_END)[..., 0]) ** 2) / np.sum(w)))
+    rates = [np.log(errs[i] / errs[i + 1]) / np.log(NS[i + 1] / NS[i]) for i in range(len(NS) - 1)]
+    print("prisms P=%d errors %s rates %s" % (P, ["%.3e" % e for e in errs], ["%.2f" % r for r in rates]))
+    assert all(np.isfinite(errs))
+    assert rates[-1] > MIN_RATE[P], (errs, rates)
