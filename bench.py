@@ -383,8 +383,18 @@ def measure_mixed_channel(order, n=(40, 20, 20), steps=3, err_steps=10, dt=2e-4)
     u0f = {i: s["u"].clone() for i, s in f.S.items()}
     f.advance(1, dt)
     ms = _time_steps(lambda k: f.advance(k, dt), f.stream, steps)
+    # operator-product flops of one stage (gradient kernel: [opp_4 | opp_5],
+    # opp_6, [opp_1], [opp_2]; update kernel: opp_3, opp_0), 5 fields
+    flops = 0.0
+    for s_ in f.S.values():
+        nu, nf, E = s_["nu"], s_["nf"], s_["E"]
+        D = 3
+        mac = 3 * nu * (nu + nf) * 5 + nf * nu * D * 5 + (nf + nu) * D * nu * 5 + 2 * nu * nf * 5
+        flops += 2.0 * mac * E
     fres.update({"value": f.dofs * 5 / (ms * 1e-3), "ms_per_step": ms, "launches_per_stage": f.launches_per_stage,
-                 "launch_shapes": {str(i): list(v) for i, v in shapes.items()}})
+                 "launch_shapes": {str(i): list(v) for i, v in shapes.items()},
+                 "operator_tflops": flops * 5 / (ms * 1e-3) / 1e12,
+                 "operator_flops_per_stage": flops})
     for i, s in f.S.items():
         s["u"].copy_(u0f[i])
     f.advance(err_steps, dt)
