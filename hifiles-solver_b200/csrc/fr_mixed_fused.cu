@@ -28,6 +28,9 @@
 //   div = div_tdisf + opp_3 (norm_tconf - norm_tdisf) -> RK45 update of the
 //   state and register (or div_tconf alone) -> traces of the new state,
 //   opp_0 U, into the other trace buffer.
+// Euler form: kernel A is mixed_inv_kernel (the transformed inviscid flux and
+//   norm_tdisf / div_tdisf alone); kernel B drops the viscous terms and takes
+//   the Roe flux instead of Rusanov when asked (2-D).
 //
 // Operator products run on the FP64 tensor cores (mma.sync m8n8k4 f64): each
 // operator is stored in fragment order (8-row tiles x 4-column steps, 32
