@@ -43,6 +43,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -123,6 +124,8 @@ struct fr_mixed_stage {
   double* UF[2] = {nullptr, nullptr};
   int cur = 0;
   int pf = 0;  // physics form: 0 Navier-Stokes, 1 Euler (Rusanov), 2 Euler (Roe)
+  std::vector<double*> partials;  // per type: [blocks of the smallest shape][F]
+  double* norms_dev = nullptr;    // [F]
   // element types after the first run on side streams, forked from and
   // joined to the caller's stream around each kernel of a stage
   bool concurrent = true;
@@ -165,6 +168,26 @@ namespace {
 
 unsigned blocks_of(long long E, int epb) { return (unsigned)((E + epb - 1) / epb); }
 
+// L1 residual norms (CalcNormResidual with res_norm_type 1, src/output.cpp:
+// 1452-1520): per type the block sums in block order, then the types in
+// order, over the solution points of all types
+struct NormParts {
+  const double* p[8];
+  int nb[8];
+};
+__global__ void mixed_norm_finalize(NormParts np, int n_types, int F, double n_upts, double* out)
+{
+  const int k = threadIdx.x;
+  if (k >= F) return;
+  double sum = 0.0;
+  for (int i = 0; i < n_types; i++) {
+    double ts = 0.0;
+    for (int b = 0; b < np.nb[i]; b++) ts += np.p[i][(size_t)b * F + k];
+    sum += ts;
+  }
+  out[k] = sum / n_upts;
+}
+
 
 fr_status launch_grad(fr_mixed_stage* s, int i, int v, const double* UFc, cudaStream_t st)
 {
@@ -176,12 +199,13 @@ fr_status launch_grad(fr_mixed_stage* s, int i, int v, const double* UFc, cudaSt
 }
 
 fr_status launch_upd(fr_mixed_stage* s, int i, int v, int mode, int stage, double dt, const double* UFc, double* UFn,
-                     cudaStream_t st)
+                     cudaStream_t st, bool norms = false)
 {
   static const double A[5] = {0.0, -0.417890474499852, -1.192151694642677, -1.697784692471528, -1.514183444257156};
   static const double B[5] = {0.149659021999229, 0.379210312999627, 0.822955029386982, 0.699450455949122,
                               0.153057247968152};
-  const MixedType& t = s->types[i];
+  MixedType t = s->types[i];
+  t.partial = norms ? s->partials[i] : nullptr;
   const MixedShape& u = kUpdShapes[v];
   auto k = mode ? s->kern[i].upd1[s->pf][v] : s->kern[i].upd0[s->pf][v];
   k<<<blocks_of(t.E, u.epb), u.nth, s->kern[i].smem_b[v], st>>>(t, s->fp, UFc, UFn, s->ph, A[stage], B[stage], dt);
@@ -225,15 +249,17 @@ fr_status launch_trace(fr_mixed_stage* s, cudaStream_t st)
   });
 }
 
-// one CalcResidual (+ the RK45 update of stage `stage` when mode is 1)
-fr_status launch_stage(fr_mixed_stage* s, int mode, int stage, double dt, cudaStream_t st)
+// one CalcResidual (+ the RK45 update of stage `stage` when mode is 1; with
+// norms, each block's residual sums into the partials)
+fr_status launch_stage(fr_mixed_stage* s, int mode, int stage, double dt, cudaStream_t st, bool norms = false)
 {
   const double* UFc = s->UF[s->cur];
   double* UFn = s->UF[s->cur ^ 1];
   if (fr_status e = for_types(s, st, [&](int i, cudaStream_t q) { return launch_grad(s, i, s->gv[i], UFc, q); }))
     return e;
-  if (fr_status e = for_types(
-          s, st, [&](int i, cudaStream_t q) { return launch_upd(s, i, s->uv[i], mode, stage, dt, UFc, UFn, q); }))
+  if (fr_status e = for_types(s, st, [&](int i, cudaStream_t q) {
+        return launch_upd(s, i, s->uv[i], mode, stage, dt, UFc, UFn, q, norms);
+      }))
     return e;
   if (mode) s->cur ^= 1;
   return FR_OK;
@@ -445,6 +471,13 @@ fr_status fr_mixed_stage_create(int n_dims, int n_types, const fr_mixed_stage_ty
   if (fr_status e = s->zeros((size_t)F * (place ? place : 1), &s->fp.BV)) return bail(e);
   if (fr_status e = s->zeros((size_t)F * NT, &s->UF[0])) return bail(e);
   if (fr_status e = s->zeros((size_t)F * NT, &s->UF[1])) return bail(e);
+  if (n_types > 8) return bail(mfail(FR_ERR_ARG, "at most 8 element types"));
+  for (int i = 0; i < n_types; i++) {
+    double* p = nullptr;
+    if (fr_status e = s->zeros((size_t)F * ((types[i].n_eles + 3) / 4 + 1), &p)) return bail(e);
+    s->partials.push_back(p);
+  }
+  if (fr_status e = s->zeros((size_t)F, &s->norms_dev)) return bail(e);
   s->fork_ev.resize(1, nullptr);
   if (cudaEventCreateWithFlags(&s->fork_ev[0], cudaEventDisableTiming) != cudaSuccess)
     return bail(mfail(FR_ERR_CUDA, "event creation failed"));
@@ -577,6 +610,32 @@ fr_status fr_mixed_stage_autotune(fr_mixed_stage* s, void* stream)
   cudaEventDestroy(e1);
   cudaFree(scratch);
   return rc;
+}
+
+fr_status fr_mixed_stage_advance_norms(fr_mixed_stage* s, int n_steps, double dt, double* res_norms, void* stream)
+{
+  g_err.clear();
+  if (!s || n_steps < 1 || !res_norms) return mfail(FR_ERR_ARG, "bad arguments");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (fr_status e = launch_trace(s, st)) return e;
+  for (int n = 0; n < n_steps; n++)
+    for (int k = 0; k < 5; k++)
+      if (fr_status e = launch_stage(s, 1, k, dt, st, n == n_steps - 1 && k == 4)) return e;
+  NormParts np{};
+  double n_upts = 0.0;
+  for (int i = 0; i < s->n_types; i++) {
+    np.p[i] = s->partials[i];
+    np.nb[i] = s->types[i].E > 0 ? (int)blocks_of(s->types[i].E, kUpdShapes[s->uv[i]].epb) : 0;
+    n_upts += (double)s->types[i].NU * (double)s->types[i].E;
+  }
+  mixed_norm_finalize<<<1, 32, 0, st>>>(np, s->n_types, s->F, n_upts, s->norms_dev);
+  if (fr_status e = mlaunched("mixed_norm_finalize")) return e;
+  if (cudaMemcpyAsync(res_norms, s->norms_dev, sizeof(double) * s->F, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return mfail(FR_ERR_CUDA, "norm read-back failed");
+  for (int k = 0; k < s->F; k++)
+    if (!std::isfinite(res_norms[k])) return mfail(FR_ERR_NONFINITE, "NaN residual encountered");
+  return FR_OK;
 }
 
 fr_status fr_mixed_stage_info(const fr_mixed_stage* s, long long* n_flux_points, long long* n_boundary_points,

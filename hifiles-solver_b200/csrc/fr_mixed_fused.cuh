@@ -74,6 +74,7 @@ struct MPlan {
   static constexpr int nC = NP * ldU;
   static_assert(ldT >= c4(D * NU) && ldG >= c8(D * NU) && ldF >= c8(NF) && ldU >= c4(NU), "plan");
   static_assert(F * EF <= NP * ldG, "the neighbours' traces fit in the gradient's place");
+  static_assert(F * EU <= oNLb - oUN, "residual terms fit in the neighbours' traces and projections");
 };
 
 struct MixedType {
@@ -82,6 +83,7 @@ struct MixedType {
   const double *A45u, *A45f, *A6, *A1, *A2, *A3, *A0;  // operators in fragment order
   const double *JG, *detj;
   double *U, *REG, *DIV, *ND, *DV;
+  double* partial;  // non-null on a stage whose residual norms are wanted: [block][F]
 };
 
 struct MixedFpts {
@@ -532,6 +534,7 @@ __global__ void __launch_bounds__(NTH, MINB) mixed_update_kernel(MixedType t, Mi
   double* sUo = msm + Q::oUo;
   double* sUn = sUo;  // the new state, after the flux phase
   double* sUN = msm + Q::oUN;
+  double* sRes = sUN;  // |div/detJ| [F][EU] for residual norms, after the flux phase
   double* sVo = msm + Q::oVo;
   double* sVN = msm + Q::oVN;
   double* sNL = msm + Q::oNLb;
@@ -668,6 +671,8 @@ __global__ void __launch_bounds__(NTH, MINB) mixed_update_kernel(MixedType t, Mi
       if (MODE == 0) {
         t.DIV[ix] = div;
       } else {
+        // |div/detJ - const_src - src| of compute_res_upts (src/eles.cpp:6086-6115)
+        if (t.partial) sRes[li] = fabs(div / sDJ[el * NU + r] - 0.0 - 0.0);
         const double rhs = -div / sDJ[el * NU + r] + 0.0 + 0.0;
         const double res = fma(rk_a, sRG[li], dt * rhs);
         t.REG[ix] = res;
@@ -685,6 +690,17 @@ __global__ void __launch_bounds__(NTH, MINB) mixed_update_kernel(MixedType t, Mi
   }
   if constexpr (MODE == 1) {
     __syncthreads();
+    if (t.partial && tid < F) {
+      // the block's L1 residual sum of field tid: cell by cell, points in
+      // order within a cell, as compute_res_upts adds them
+      double bs = 0.0;
+      for (int el = 0; el < nval; el++) {
+        double cs = 0.0;
+        for (int r = 0; r < NU; r++) cs += sRes[tid * EU + el * NU + r];
+        bs += cs;
+      }
+      t.partial[(size_t)blockIdx.x * F + tid] = bs;
+    }
     auto bu = [&](int n) { return sUn + n * Q::ldU; };
     auto one = [&](int r, int n, double v) {
       const int el = n / F, k = n - el * F;

@@ -420,9 +420,10 @@ def _bind_stage(L):
     L.fr_mixed_stage_get_launch.argtypes = [vp, i, C.POINTER(i), C.POINTER(i)]
     L.fr_mixed_stage_autotune.argtypes = [vp, vp]
     L.fr_mixed_stage_set_concurrent.argtypes = [vp, i]
+    L.fr_mixed_stage_advance_norms.argtypes = [vp, i, C.c_double, vp, vp]
     for f in ("fr_mixed_stage_create", "fr_mixed_stage_destroy", "fr_mixed_stage_residual", "fr_mixed_stage_advance",
               "fr_mixed_stage_info", "fr_mixed_stage_set_launch", "fr_mixed_stage_get_launch",
-              "fr_mixed_stage_autotune", "fr_mixed_stage_set_concurrent"):
+              "fr_mixed_stage_autotune", "fr_mixed_stage_set_concurrent", "fr_mixed_stage_advance_norms"):
         getattr(L, f).restype = C.c_int
     return L
 
@@ -554,9 +555,16 @@ class FusedMixedMesh:
         """div_tconf_upts of every element type (one CalcResidual) into S[i]["div"]."""
         _check(self.L.fr_mixed_stage_residual(self.h, _VP(self.stream.cuda_stream)))
 
-    def advance(self, n_steps, dt):
-        """n_steps RK45 steps (5 stages each)."""
-        _check(self.L.fr_mixed_stage_advance(self.h, int(n_steps), float(dt), _VP(self.stream.cuda_stream)))
+    def advance(self, n_steps, dt, norms=False):
+        """n_steps RK45 steps (5 stages each); with norms, returns the L1
+        residual norms of the last step (CalcNormResidual, res_norm_type 1)."""
+        if not norms:
+            _check(self.L.fr_mixed_stage_advance(self.h, int(n_steps), float(dt), _VP(self.stream.cuda_stream)))
+            return None
+        out = np.zeros(self.F)
+        _check(self.L.fr_mixed_stage_advance_norms(self.h, int(n_steps), float(dt), out.ctypes.data,
+                                                   _VP(self.stream.cuda_stream)))
+        return out
 
 
 def tile_mixed_mesh(types, int_inters, bdy_inters, copies):

@@ -693,6 +693,12 @@ fr_status fr_mixed_stage_destroy(fr_mixed_stage* s);
 fr_status fr_mixed_stage_residual(fr_mixed_stage* s, void* stream);
 /* n_steps RK45 steps of dt (5 stages each) on the current state. */
 fr_status fr_mixed_stage_advance(fr_mixed_stage* s, int n_steps, double dt, void* stream);
+/* The same, then the L1 residual norms of the last step into res_norms
+ * (n_fields host doubles): CalcNormResidual with res_norm_type 1
+ * (src/output.cpp:1452-1520), sum over every type's solution points of
+ * |div_tconf_upts / detjac_upts| of the last stage, over their number.
+ * Synchronises the stream; FR_ERR_NONFINITE for a NaN norm. */
+fr_status fr_mixed_stage_advance_norms(fr_mixed_stage* s, int n_steps, double dt, double* res_norms, void* stream);
 /* Launch shapes of each type's two stage kernels: gradient 0 = 8 elements x
  * 256 threads, 1 = 4 x 128, 2 = 8 x 128, 3 = 4 x 128 with registers for 4
  * blocks per SM, 4 = 8 x 256 with registers for 2; update 0 = 8 x 256,

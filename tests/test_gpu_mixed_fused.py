@@ -57,7 +57,11 @@ def test_fused_stage_matches_the_reference(case):
         got = _div(m, t["index"])
         assert np.isfinite(got).all()
         assert rel(got, a["t%d_s11_div_tconf_upts" % t["ele_type"]]) <= 1e-12, (case, t["ele_type"])
-    m.advance(meta["steps"], meta["dt"])
+    for step in range(meta["steps"]):
+        # the L1 residual norms of each step, as the reference's CalcNormResidual
+        norms = m.advance(1, meta["dt"], norms=True)
+        want = a["res_norms"][:, step]
+        assert np.all(np.abs(norms - want) <= 1e-12 * np.abs(want)), (case, step, norms, want)
     for t in meta["types"]:
         got = m.get_state(t["index"])
         assert rel(got, a["t%d_final_disu_upts0" % t["ele_type"]]) <= 1e-12, (case, t["ele_type"])
