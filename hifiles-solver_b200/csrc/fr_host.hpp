@@ -42,6 +42,12 @@ struct Line1D {
 
 bool make_line(int P, int upts_type, int vcjh_scheme, double eta, Line1D& out, std::string& err);
 
+// Row-major (nu_to, nu_from) matrix carrying values at the solution points
+// `from` of one element (type 0-4, the given order; D coordinates per point)
+// to the points `to` through that element's nodal basis (fr_mixed.cpp).
+bool nodal_interp(int type, int order, const double* from, int nu_from, const double* to, int nu_to,
+                  std::vector<double>& R, std::string& err);
+
 // Conforming mesh of one tensor element type with periodic wiring.
 struct Mesh {
   int dims = 0, P = 0, n1 = 0, nu = 0, nf = 0, nface = 0, nfpf = 0, nfields = 0;

@@ -907,6 +907,65 @@ static void face_normal(const double* J, const double* t, double* v)
 }
 
 }  // namespace mixed
+
+// Row-major (nu_to, nu_from) matrix whose row j holds every nodal basis
+// function of the points `from` (one element of `type` and `order`,
+// point-major with D = 2 or 3 coordinates each) at to[j]: the reference's
+// opp_r (eles::set_opp_r, src/eles.cpp:4135-4153) with the bases of
+// eval_nodal_basis_restart (src/eles_tris.cpp:585-600, src/eles_tets.cpp,
+// src/eles_pris.cpp).  Quads and hexes take their 1-D points from the x of
+// the first order + 1 points, prisms their triangle points from the first
+// (order+1)(order+2)/2 points and their 1-D points from z every that many.
+bool nodal_interp(int type, int order, const double* from, int nu_from, const double* to, int nu_to,
+                  std::vector<double>& R, std::string& err)
+{
+  using namespace mixed;
+  if (order < 0 || order > kMaxP) { err = "restart order 0-" + std::to_string(kMaxP); return false; }
+  const int D = type_dims(type), n1 = order + 1, nt = tri_count(order);
+  int nu = 0;
+  switch (type) {
+    case FR_ELE_TRI: nu = nt; break;
+    case FR_ELE_QUAD: nu = n1 * n1; break;
+    case FR_ELE_TET: nu = nt * (order + 3) / 3; break;
+    case FR_ELE_PRISM: nu = nt * n1; break;
+    case FR_ELE_HEX: nu = n1 * n1 * n1; break;
+    default: err = "element type 0-4"; return false;
+  }
+  if (nu_from != nu) { err = "point count does not match the order"; return false; }
+  Element E;
+  E.type = type; E.P = order; E.D = D; E.nu = nu;
+  Mat V;
+  int nv = 0;
+  if (type == FR_ELE_TRI || type == FR_ELE_PRISM) {
+    nv = nt;
+    tri_modes(order, E.m2);
+    V.resize((size_t)nt * nt);
+    for (int i = 0; i < nt; i++)
+      for (int j = 0; j < nt; j++) V[(size_t)i * nt + j] = dub2(from[D * i], from[D * i + 1], E.m2[j][0], E.m2[j][1]);
+    if (type == FR_ELE_PRISM) {
+      E.ntri = nt;
+      E.x1d.resize(n1);
+      for (int c = 0; c < n1; c++) E.x1d[c] = from[D * (nt * c) + 2];
+    }
+  } else if (type == FR_ELE_TET) {
+    nv = nu;
+    tet_modes(order, E.m3);
+    V.resize((size_t)nu * nu);
+    for (int i = 0; i < nu; i++)
+      for (int j = 0; j < nu; j++) V[(size_t)i * nu + j] = dub3(&from[3 * i], E.m3[j]);
+  } else {
+    E.line.P = order; E.line.n1 = n1;
+    for (int a = 0; a < n1; a++) E.line.loc[a] = from[D * a];
+  }
+  if (nv && !invert(nv, V, E.Vinv)) { err = "restart points give a singular Vandermonde matrix"; return false; }
+  R.assign((size_t)nu_to * nu, 0.0);
+  for (int j = 0; j < nu_to; j++) {
+    double x[3] = {to[D * j], to[D * j + 1], D == 3 ? to[D * j + 2] : 0.0};
+    basis(E, x, &R[(size_t)j * nu]);
+  }
+  return true;
+}
+
 }  // namespace frb
 
 using namespace frb;

@@ -925,7 +925,7 @@ fr_status fr_solver_write_restart(fr_solver* s, const char* path, double time)
   std::vector<double> u((size_t)m.nu * m.ne * m.nfields);
   fr_status r = fr_solver_get_state(s, u.data(), nullptr);
   if (r) return r;
-  fr_restart_block b{m.dims == 2 ? 1 : 4, s->sch.order, m.nu, (int)m.ne, m.nfields, s->line.loc, nullptr, u.data()};
+  fr_restart_block b{m.dims == 2 ? 1 : 4, s->sch.order, m.nu, (int)m.ne, m.nfields, s->line.loc, nullptr, u.data(), nullptr};
   return fr_restart_write(path, time, &b, 1);
 }
 

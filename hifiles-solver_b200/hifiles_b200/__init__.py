@@ -127,6 +127,7 @@ def lib():
         "fr_batch_stream": (vp, [vp]),
         "fr_restart_write": (C.c_int, [C.c_char_p, C.c_double, vp, C.c_int]),
         "fr_restart_read": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp, dp, dp]),
+        "fr_restart_read_points": (C.c_int, [C.c_char_p, C.c_int, C.c_int, dp, C.c_int, C.c_int, vp, dp, dp]),
         "fr_solver_write_restart": (C.c_int, [vp, C.c_char_p, C.c_double]),
         "fr_solver_read_restart": (C.c_int, [vp, C.c_char_p, dp]),
         "fr_solver_sgs_features": (C.c_int, [vp, C.POINTER(C.c_float), vp]),
@@ -527,30 +528,56 @@ def mlp_adam(d_w, d_grad, d_m, d_v, step, lr, stream=None):
 class RestartBlock(C.Structure):
     _fields_ = [("ele_type", C.c_int), ("order", C.c_int), ("n_upts", C.c_int), ("n_eles", C.c_int),
                 ("n_fields", C.c_int), ("loc_1d", C.POINTER(C.c_double)), ("ele2global", C.POINTER(C.c_int)),
-                ("disu_upts", C.POINTER(C.c_double))]
+                ("disu_upts", C.POINTER(C.c_double)), ("loc_pts", C.POINTER(C.c_double))]
+
+
+def _points(loc_pts, ele_type):
+    """Solution points as a C-ordered (n_upts, dims) array (element_operators' loc_upts is (dims, n_upts):
+    pass its transpose)."""
+    pts = np.ascontiguousarray(loc_pts, dtype=np.float64)
+    if pts.ndim != 2 or pts.shape[1] != (2 if ele_type in (0, 1) else 3):
+        raise ValueError("loc_pts must be (n_upts, dims)")
+    return pts
 
 
 def restart_write(path, time, blocks):
-    """blocks: list of dicts(ele_type, order, loc_1d, disu_upts (n_upts, n_eles, F), ele2global=None)."""
+    """blocks: list of dicts(ele_type, order, disu_upts (n_upts, n_eles, F), ele2global=None) with loc_1d
+    (quads, hexes: the 1-D points) or loc_pts (triangles, tets, prisms: the (n_upts, dims) solution points
+    of element_operators)."""
     keep, arr = [], (RestartBlock * len(blocks))()
     for i, b in enumerate(blocks):
         u = np.asfortranarray(b["disu_upts"], dtype=np.float64)
-        loc = np.ascontiguousarray(b["loc_1d"], dtype=np.float64)
+        loc = None if b.get("loc_1d") is None else np.ascontiguousarray(b["loc_1d"], dtype=np.float64)
+        pts = None if b.get("loc_pts") is None else _points(b["loc_pts"], b["ele_type"])
         g = None if b.get("ele2global") is None else np.ascontiguousarray(b["ele2global"], dtype=np.int32)
-        keep += [u, loc, g]
-        arr[i] = RestartBlock(int(b["ele_type"]), int(b["order"]), u.shape[0], u.shape[1], u.shape[2], _dp(loc),
-                              None if g is None else g.ctypes.data_as(C.POINTER(C.c_int)), _dp(u))
+        keep += [u, loc, pts, g]
+        arr[i] = RestartBlock(int(b["ele_type"]), int(b["order"]), u.shape[0], u.shape[1], u.shape[2],
+                              None if loc is None else _dp(loc),
+                              None if g is None else g.ctypes.data_as(C.POINTER(C.c_int)), _dp(u),
+                              None if pts is None else _dp(pts))
     _check(lib().fr_restart_write(str(path).encode(), float(time), arr, len(blocks)))
 
 
 def restart_read(path, ele_type, order, n_eles, n_fields, upts_type=0, ele2global=None):
-    """(disu_upts (n_upts, n_eles, F), time) of one element type's block."""
+    """(disu_upts (n_upts, n_eles, F), time) of the quad or hex block."""
     dims = 2 if ele_type == 1 else 3
     u = np.zeros(((order + 1) ** dims, n_eles, n_fields), order="F")
     g = None if ele2global is None else np.ascontiguousarray(ele2global, dtype=np.int32)
     t = C.c_double()
     _check(lib().fr_restart_read(str(path).encode(), int(ele_type), int(order), int(upts_type), int(n_eles),
                                  int(n_fields), None if g is None else g.ctypes.data, _dp(u), C.byref(t)))
+    return u, t.value
+
+
+def restart_read_points(path, ele_type, loc_pts, n_eles, n_fields, ele2global=None):
+    """(disu_upts (n_upts, n_eles, F), time) of one element type's block carried to the solution points
+    loc_pts ((n_upts, dims), as element_operators gives them)."""
+    pts = _points(loc_pts, ele_type)
+    u = np.zeros((pts.shape[0], n_eles, n_fields), order="F")
+    g = None if ele2global is None else np.ascontiguousarray(ele2global, dtype=np.int32)
+    t = C.c_double()
+    _check(lib().fr_restart_read_points(str(path).encode(), int(ele_type), pts.shape[0], _dp(pts), int(n_eles),
+                                        int(n_fields), None if g is None else g.ctypes.data, _dp(u), C.byref(t)))
     return u, t.value
 
 

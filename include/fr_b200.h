@@ -269,25 +269,40 @@ void* fr_batch_stream(fr_batch* b);
  * memory only; no GPU is touched by fr_restart_*.
  * ---------------------------------------------------------------------- */
 typedef struct {
-  int ele_type;            /* reference codes: 1 quads, 4 hexes                */
+  int ele_type;            /* reference codes: 0 triangles, 1 quads, 2 tets,
+                              3 prisms, 4 hexes                                 */
   int order;               /* polynomial order of the block                    */
   int n_upts, n_eles, n_fields;
-  const double* loc_1d;    /* order + 1 solution-point locations in 1-D        */
+  const double* loc_1d;    /* quads, hexes: order + 1 solution-point locations
+                              in 1-D                                          */
   const int* ele2global;   /* global element ids (NULL: 0 .. n_eles-1)         */
   const double* disu_upts; /* (n_upts, n_eles, n_fields)                       */
+  const double* loc_pts;   /* triangles, tets, prisms: the solution points,
+                              (n_upts, dims) point-major as
+                              fr_element_operators gives them                  */
 } fr_restart_block;
 
 /* Writes a restart file exactly as the reference does (%.15g numbers,
- * eles::write_restart_info / write_restart_data, src/eles_hexas.cpp:882-900,
- * src/eles.cpp:697-722); blocks with no elements are left out. */
+ * each type's write_restart_info, src/eles_tris.cpp:546-563,
+ * src/eles_tets.cpp:782-800, src/eles_pris.cpp:700-726,
+ * src/eles_hexas.cpp:882-900, and eles::write_restart_data,
+ * src/eles.cpp:697-722): element types in the order of their codes, at most
+ * one block per type; blocks with no elements are left out. */
 fr_status fr_restart_write(const char* path, double time, const fr_restart_block* blocks, int n_blocks);
-/* Reads the block of one element type into disu_upts (n_upts, n_eles,
+/* Reads the quad (1) or hex (4) block into disu_upts (n_upts, n_eles,
  * n_fields) of a solver of the given order and point family, interpolating
  * from the file's order when it differs (eles::set_opp_r,
  * src/eles.cpp:4135-4153).  Elements are matched by global id; every
  * element must be present.  time_out may be NULL. */
 fr_status fr_restart_read(const char* path, int ele_type, int order, int upts_type, int n_eles, int n_fields,
                           const int* ele2global, double* disu_upts, double* time_out);
+/* The same for any element type (read_restart_info of src/eles_tris.cpp:511,
+ * src/eles_tets.cpp:749, src/eles_pris.cpp:655): the file's block carried
+ * to the solution points loc_pts ((n_upts, dims) point-major) through the
+ * nodal basis on the file's points; points equal to the file's to 1e-13 take
+ * the file's values as they are. */
+fr_status fr_restart_read_points(const char* path, int ele_type, int n_upts, const double* loc_pts, int n_eles,
+                                 int n_fields, const int* ele2global, double* disu_upts, double* time_out);
 /* A solution as a VTK unstructured grid (.vtu, inline base64 binary), the
  * role of the reference's Paraview output (src/output.cpp:580-1055): points
  * are the solution points (pos_upts, (n_upts, n_eles, dims)), each element is

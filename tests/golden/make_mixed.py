@@ -30,6 +30,10 @@ reference has no element for, so hexes and tets never share a face):
     for the second half (hex and prism meet on quadrilateral faces), periodic.
 Interior vertices move by a seeded jitter of up to `jitter` cell sizes.
 
+With --restart-only it reruns mixed_triquad_p2 and mixed_pritet_p2 with the
+harness's --write-restart and keeps the reference's own restart files
+(write_restart, src/output.cpp:1057-1107) verbatim as rest_<name>.dat.
+
 Usage:  python tests/golden/make_mixed.py --ref <reference checkout>   (or HIFILES_REF=<dir>)
 """
 import argparse
@@ -242,7 +246,14 @@ CASES_2D = [
 ]
 
 
-def run_case_2d(ref, c, work):
+def keep_restart(d, c):
+    """The reference's own restart file of a run, kept verbatim as a fixture."""
+    src = os.path.join(d, "Rest_%09d_p%04d.dat" % (c["steps"], 0))
+    with open(src) as fi, open(os.path.join(HERE, "rest_" + c["name"] + ".dat"), "w") as fo:
+        fo.write(fi.read())
+
+
+def run_case_2d(ref, c, work, restart=False):
     d = os.path.join(work, c["name"])
     os.makedirs(d, exist_ok=True)
     lo, hi = (0.0, 0.0), (2 * np.pi, 2 * np.pi)
@@ -264,10 +275,14 @@ def run_case_2d(ref, c, work):
     os.makedirs(out, exist_ok=True)
     env = dict(os.environ, HIFILES_HOME=os.path.join(REPO, "oracle", "_ref"))
     args = [G.HARNESS, "input", out, "--ic", "channel_mach01", "--steps", str(c["steps"]), "--stages"]
+    if restart:
+        args += ["--write-restart", str(c["steps"])]
     r = subprocess.run(args, cwd=d, env=env, capture_output=True, text=True)
     if r.returncode != 0:
         print(r.stdout[-3000:], r.stderr[-3000:])
         raise RuntimeError("harness failed for " + c["name"])
+    if restart:
+        keep_restart(d, c)
     arr, par = G.load_npy_dir(out)
     return arr, par, eles
 
@@ -281,7 +296,7 @@ STAGES = ["s01_disu_fpts", "s03_tdisf_upts", "s04_norm_tconf_fpts", "s04_delta_d
           "s12_disu_upts0", "final_disu_upts0"]
 
 
-def run_case(ref, c, work):
+def run_case(ref, c, work, restart=False):
     d = os.path.join(work, c["name"])
     os.makedirs(d, exist_ok=True)
     lo, hi = (0.0, 0.0, 0.0), (2 * np.pi,) * 3
@@ -308,10 +323,14 @@ def run_case(ref, c, work):
     os.makedirs(out, exist_ok=True)
     env = dict(os.environ, HIFILES_HOME=os.path.join(REPO, "oracle", "_ref"))
     args = [G.HARNESS, "input", out, "--ic", c.get("ic", "tgv_mach01"), "--steps", str(c["steps"]), "--stages"]
+    if restart:
+        args += ["--write-restart", str(c["steps"])]
     r = subprocess.run(args, cwd=d, env=env, capture_output=True, text=True)
     if r.returncode != 0:
         print(r.stdout[-3000:], r.stderr[-3000:])
         raise RuntimeError("harness failed for " + c["name"])
+    if restart:
+        keep_restart(d, c)
     arr, par = G.load_npy_dir(out)
     types = []
     for line in open(os.path.join(out, "params.txt")):
@@ -384,10 +403,16 @@ def main():
                     help="the reference checkout (or set HIFILES_REF)")
     ap.add_argument("--work", default=None)
     ap.add_argument("--only-2d", action="store_true", help="write the 2-D triangle/quad fixtures only")
+    ap.add_argument("--restart-only", action="store_true",
+                    help="write only the reference's restart files of mixed_triquad_p2 and mixed_pritet_p2")
     a = ap.parse_args()
     if not os.path.exists(G.HARNESS):
         subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "REF=" + a.ref, "ref"], check=True)
     work = a.work or tempfile.mkdtemp(prefix="fr_mixed_")
+    if a.restart_only:
+        run_case_2d(a.ref, [c for c in CASES_2D if c["name"] == "mixed_triquad_p2"][0], work, restart=True)
+        run_case(a.ref, [c for c in CASES if c["name"] == "mixed_pritet_p2"][0], work, restart=True)
+        return
     for c in CASES_2D:
         arr, par, eles = run_case_2d(a.ref, c, work)
         meta = {k: (list(v) if isinstance(v, tuple) else v) for k, v in c.items()}

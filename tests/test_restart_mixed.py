@@ -1,0 +1,139 @@
+"""Restart files of triangles, tets and prisms (fr_restart_write /
+fr_restart_read_points, host only) against the files the reference itself
+wrote for the mixed fixtures (write_restart, src/output.cpp:1057-1107, with
+write_restart_info of src/eles_tris.cpp:546-563, src/eles_tets.cpp:782-800,
+src/eles_pris.cpp:700-726), and reading at another order through the nodal
+basis on the file's points (eles::set_opp_r, src/eles.cpp:4135-4153).
+
+The element ids of each block are taken from the reference's file; values
+cross the file as 15 significant digits, so states are compared at 1e-14
+normwise relative; files are compared byte for byte."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import hifiles_b200 as H
+import oracle as O
+from golden_util import GOLDEN, rel
+from hifiles_b200 import mixed as X
+
+NAMES = {0: "TRIS", 1: "QUADS", 2: "TETS", 3: "PRIS", 4: "HEXAS"}
+
+
+def fixture(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    meta = json.loads(str(z["meta"]))
+    if meta["kind"] == "triquad":
+        opts = X.ElementOpts(upts_type_tri=meta["tri_upts"], fpts_type_tri=meta["tri_fpts"])
+    else:
+        opts = X.ElementOpts(upts_type_tet=meta["tet_upts"], vcjh_scheme_tet=2, vcjh_scheme_tri=1,
+                             vcjh_scheme_pri_1d=1)
+    return meta, z, opts
+
+
+def file_ids(path, ele_type):
+    """The ele2global array of one block of a restart file."""
+    lines = open(path).read().split("\n")
+    i = lines.index(NAMES[ele_type])
+    j = lines.index("ele2global_ele array", i)
+    return np.array([int(v) for v in lines[j + 1].split()], dtype=np.int32)
+
+
+def blocks(meta, z, opts, path):
+    out = []
+    for t in meta["types"]:
+        et, P = t["ele_type"], meta["order"]
+        b = dict(ele_type=et, order=P, disu_upts=z["t%d_final_disu_upts0" % t["index"]],
+                 ele2global=file_ids(path, et))
+        if et in (1, 4):
+            b["loc_1d"] = O.points_1d(P)
+        else:
+            b["loc_pts"] = X.element_operators(et, P, opts)["loc_upts"].T
+        out.append(b)
+    return out
+
+
+CASES = ["mixed_triquad_p2", "mixed_pritet_p2"]
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_writer_reproduces_reference_mixed_file_byte_for_byte(name, tmp_path):
+    meta, z, opts = fixture(name)
+    path = os.path.join(GOLDEN, "rest_%s.dat" % name)
+    out = tmp_path / "Rest.dat"
+    bl = blocks(meta, z, opts, path)
+    H.restart_write(out, meta["steps"] * meta["dt"], bl[::-1])      # any block order: types go in code order
+    assert out.read_bytes() == open(path, "rb").read()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_reader_on_reference_mixed_file_gives_reference_state(name):
+    meta, z, opts = fixture(name)
+    path = os.path.join(GOLDEN, "rest_%s.dat" % name)
+    for b in blocks(meta, z, opts, path):
+        et = b["ele_type"]
+        pts = b.get("loc_pts")
+        if pts is None:
+            n1 = meta["order"] + 1
+            x = O.points_1d(meta["order"])
+            pts = np.array([(x[j % n1], x[j // n1]) for j in range(n1 * n1)])
+        u, t = H.restart_read_points(path, et, pts, b["disu_upts"].shape[1], b["disu_upts"].shape[2],
+                                     ele2global=b["ele2global"])
+        assert abs(t - meta["steps"] * meta["dt"]) < 1e-12
+        assert rel(u, b["disu_upts"]) <= 1e-14
+
+
+@pytest.mark.parametrize("et", [0, 2, 3])
+def test_another_order_carries_polynomials_exactly(et, tmp_path):
+    """A field of degree <= 2 written at order 2 and read at order 3 equals
+    the field at the order-3 points, and reading those back at order 2
+    returns what was written."""
+    opts = X.ElementOpts(upts_type_tet=1, vcjh_scheme_tet=2, vcjh_scheme_tri=1, vcjh_scheme_pri_1d=1)
+    p2 = X.element_operators(et, 2, opts)["loc_upts"].T.copy()
+    p3 = X.element_operators(et, 3, opts)["loc_upts"].T.copy()
+    rng = np.random.default_rng(7)
+    ne, F = 5, 4
+    c = rng.normal(size=(ne, F, 10))
+
+    def field(p):
+        x, y = p[:, 0], p[:, 1]
+        zz = p[:, 2] if p.shape[1] == 3 else 0.0 * x
+        mon = np.stack([np.ones_like(x), x, y, zz, x * x, x * y, y * y, x * zz, y * zz, zz * zz])
+        return np.einsum("efm,mj->jef", c, mon)
+
+    u2 = np.asfortranarray(field(p2))
+    f1 = tmp_path / "Rest2.dat"
+    H.restart_write(f1, 1.5, [dict(ele_type=et, order=2, loc_pts=p2, disu_upts=u2)])
+    u3, t = H.restart_read_points(f1, et, p3, ne, F)
+    assert t == 1.5
+    assert rel(u3, field(p3)) <= 1e-13
+    f2 = tmp_path / "Rest3.dat"
+    H.restart_write(f2, 1.5, [dict(ele_type=et, order=3, loc_pts=p3, disu_upts=u3)])
+    u2b, _ = H.restart_read_points(f2, et, p2, ne, F)
+    assert rel(u2b, u2) <= 1e-13
+
+
+def test_mixed_reader_and_writer_errors(tmp_path):
+    path = os.path.join(GOLDEN, "rest_mixed_triquad_p2.dat")
+    meta, z, opts = fixture("mixed_triquad_p2")
+    p2 = X.element_operators(0, 2, opts)["loc_upts"].T
+    ids = file_ids(path, 0)
+    with pytest.raises(H.FrError):
+        H.restart_read_points(path, 2, np.zeros((10, 3)), 4, 4)        # no TETS block
+    with pytest.raises(H.FrError):
+        H.restart_read_points(path, 0, p2, 17, 4)                      # ids 0..16: not all in the file
+    with pytest.raises(ValueError):
+        H.restart_read_points(path, 0, p2.T, 16, 4, ele2global=ids)    # points must be (n_upts, dims)
+    u = np.zeros((6, 2, 4), order="F")
+    with pytest.raises(H.FrError):                                    # triangles need their points
+        H.restart_write(tmp_path / "a.dat", 0.0, [dict(ele_type=0, order=2, disu_upts=u)])
+    with pytest.raises(H.FrError):                                    # one block per type
+        H.restart_write(tmp_path / "a.dat", 0.0, [dict(ele_type=0, order=2, loc_pts=p2, disu_upts=u)] * 2)
+    with pytest.raises(H.FrError):                                    # 6 points are order 2
+        H.restart_write(tmp_path / "a.dat", 0.0, [dict(ele_type=0, order=3, loc_pts=p2, disu_upts=u)])
+    # global ids select the elements: reversed ids give the reversed state
+    want = z["t0_final_disu_upts0"]
+    u, _ = H.restart_read_points(path, 0, p2, 16, 4, ele2global=ids[::-1].copy())
+    assert rel(u, want[:, ::-1, :]) <= 1e-14
