@@ -16,7 +16,7 @@ import itertools
 
 import numpy as np
 
-from . import _check, box_mesh, lib
+from . import _check, box_mesh, lib, restart_read_points, restart_write
 
 TRI, QUAD, TET, PRISM, HEX = 0, 1, 2, 3, 4
 _NODES = {TRI: 3, QUAD: 4, TET: 4, PRISM: 6, HEX: 8}
@@ -182,6 +182,31 @@ class MixedMesh:
                 "tdA_fpts", "norm_fpts")
         types = {t: dict({k: m[k] for k in keys}, u=np.asfortranarray(states[t])) for t, m in self.types.items()}
         return types, list(self.int_inters), list(self.bdy_inters)
+
+    def write_restart(self, path, time, states):
+        """states (element type -> (n_upts, n_eles, F)) as a restart file in
+        the reference's format (write_restart, src/output.cpp:1057-1107); the
+        element ids are the cells' indices, the reference's ele2global."""
+        blocks = []
+        for t, m in sorted(self.types.items()):
+            b = dict(ele_type=t, order=self.order, disu_upts=states[t], ele2global=m["cell"].astype(np.int32))
+            if t in (QUAD, HEX):
+                b["loc_1d"] = m["loc_upts"][0, :self.order + 1]
+            else:
+                b["loc_pts"] = m["loc_upts"].T
+            blocks.append(b)
+        restart_write(path, time, blocks)
+
+    def read_restart(self, path, n_fields=None):
+        """({element type: state (n_upts, n_eles, F)}, time) from a restart
+        file of any order, each block carried to this mesh's solution points
+        (read_restart, src/solver.cpp:390-445); F defaults to dims + 2."""
+        F = self.dims + 2 if n_fields is None else int(n_fields)
+        out, time = {}, None
+        for t, m in sorted(self.types.items()):
+            out[t], time = restart_read_points(path, t, m["loc_upts"].T, m["n_eles"], F,
+                                               ele2global=m["cell"].astype(np.int32))
+        return out, time
 
 
 def _tet_volume(xv, t):

@@ -137,3 +137,49 @@ def test_mixed_reader_and_writer_errors(tmp_path):
     want = z["t0_final_disu_upts0"]
     u, _ = H.restart_read_points(path, 0, p2, 16, 4, ele2global=ids[::-1].copy())
     assert rel(u, want[:, ::-1, :]) <= 1e-14
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_mixed_mesh_writes_the_reference_file(name, tmp_path):
+    """The library's own set-up of the fixture mesh (cell order = the
+    reference's element ids) writes the reference's file from the
+    reference's final state."""
+    from test_mixed_setup import fixture_mesh
+    meta, z, _ = fixture(name)
+    xv, cells, period, bfaces, opts = fixture_mesh(meta)
+    M = X.MixedMesh(meta["order"], xv, cells, period, bfaces, opts)
+    out = tmp_path / "Rest.dat"
+    M.write_restart(out, meta["steps"] * meta["dt"], {t: z["t%d_final_disu_upts0" % t] for t in M.types})
+    assert out.read_bytes() == open(os.path.join(GOLDEN, "rest_%s.dat" % name), "rb").read()
+    u, t = M.read_restart(out)
+    assert abs(t - meta["steps"] * meta["dt"]) < 1e-15
+    for et in M.types:
+        assert rel(u[et], z["t%d_final_disu_upts0" % et]) <= 1e-14
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_mixed_mesh_reads_a_file_of_another_order(name, tmp_path):
+    """A quadratic field of the physical coordinates, written from the
+    order-2 mesh, read by the order-3 mesh of the same cells: every element
+    type's map is at most bilinear, so the field lies in both spaces and
+    arrives exactly at the order-3 points."""
+    from test_mixed_setup import fixture_mesh
+    meta, _, _ = fixture(name)
+    xv, cells, period, bfaces, opts = fixture_mesh(meta)
+    M2 = X.MixedMesh(2, xv, cells, period, bfaces, opts)
+    M3 = X.MixedMesh(3, xv, cells, period, bfaces, opts)
+    D = M2.dims
+    rng = np.random.default_rng(3)
+    c = rng.normal(size=(D + 2, 1 + D + D * D))
+
+    def field(pos):                                    # pos (n_upts, n_eles, D)
+        mon = [np.ones(pos.shape[:2])] + [pos[..., d] for d in range(D)] + \
+              [pos[..., d] * pos[..., e] for d in range(D) for e in range(D)]
+        return np.asfortranarray(np.stack([sum(ck * m for ck, m in zip(c[k], mon)) for k in range(D + 2)], axis=-1))
+
+    out = tmp_path / "Rest.dat"
+    M2.write_restart(out, 0.25, {t: field(m["pos_upts"]) for t, m in M2.types.items()})
+    u, t = M3.read_restart(out)
+    assert t == 0.25
+    for et, m in M3.types.items():
+        assert rel(u[et], field(m["pos_upts"])) <= 1e-12, et
