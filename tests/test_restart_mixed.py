@@ -183,3 +183,35 @@ def test_mixed_mesh_reads_a_file_of_another_order(name, tmp_path):
     assert t == 0.25
     for et, m in M3.types.items():
         assert rel(u[et], field(m["pos_upts"])) <= 1e-12, et
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", CASES)
+def test_fused_run_continues_from_a_restart_file(name, tmp_path):
+    """The fused stage, restarted from the reference's restart file (state
+    after the fixture's steps) and from this library's own file of the same
+    run, continues like the uninterrupted run: 15 digits through the file
+    keep the next two steps within 1e-12 (normwise relative)."""
+    pytest.importorskip("torch")
+    from hifiles_b200 import seam
+    from test_mixed_setup import fixture_mesh
+    meta, z, _ = fixture(name)
+    xv, cells, period, bfaces, opts = fixture_mesh(meta)
+    M = X.MixedMesh(meta["order"], xv, cells, period, bfaces, opts)
+
+    def fused(states):
+        types, ints, bdys = M.operator_inputs(states)
+        return seam.FusedMixedMesh(types, ints, meta["physics"], bdys, meta["bdy"], meta["R_ref"])
+
+    m1 = fused({t: z["t%d_disu_upts_init" % t] for t in M.types})
+    m1.advance(meta["steps"], meta["dt"])
+    ours = tmp_path / "Rest.dat"
+    M.write_restart(ours, meta["steps"] * meta["dt"], {t: m1.get_state(t) for t in M.types})
+    m1.advance(2, meta["dt"])
+    for path in (os.path.join(GOLDEN, "rest_%s.dat" % name), ours):
+        u, t = M.read_restart(path)
+        assert abs(t - meta["steps"] * meta["dt"]) < 1e-15
+        m2 = fused(u)
+        m2.advance(2, meta["dt"])
+        for et in M.types:
+            assert rel(m2.get_state(et), m1.get_state(et)) <= 1e-12, (path, et)
