@@ -43,6 +43,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <sstream>
@@ -97,6 +98,22 @@ bool next_line(std::istream& in, std::string& s)
   if (!std::getline(in, s)) return false;
   if (!s.empty() && s.back() == '\r') s.pop_back();
   return true;
+}
+
+// The numbers of one line; false if a token is not a number.
+bool parse_numbers(const std::string& s, std::vector<double>& out)
+{
+  out.clear();
+  const char* p = s.c_str();
+  for (;;) {
+    while (*p == ' ' || *p == '\t') p++;
+    if (!*p) return true;
+    char* end = nullptr;
+    const double x = std::strtod(p, &end);
+    if (end == p) return false;
+    out.push_back(x);
+    p = end;
+  }
 }
 
 // The header of one block as write_restart_info prints it.
@@ -234,13 +251,20 @@ fr_status read_block(const char* path, int t, const double* mine, int nu, int n_
   for (int e = 0; e < n_eles; e++) where[ele2global ? ele2global[e] : e] = e;
   const size_t NE = (size_t)n_eles;
   std::vector<char> seen(n_eles, 0);
-  std::vector<double> v((size_t)nu_r * n_fields);
+  std::vector<double> v((size_t)nu_r * n_fields), row;
   for (long long i = 0; i < ne_r; i++) {
-    long long g;
-    if (!(f >> g)) return rs_fail(FR_ERR_ARG, "restart file: truncated element data");
-    for (int j = 0; j < nu_r; j++)
-      for (int k = 0; k < n_fields; k++)
-        if (!(f >> v[j + (size_t)nu_r * k])) return rs_fail(FR_ERR_ARG, "restart file: truncated element data");
+    // one line with the element's global id, then one line of n_fields values per point
+    if (!next_line(f, s) || !parse_numbers(s, row) || row.size() != 1)
+      return rs_fail(FR_ERR_ARG, "restart file: truncated element data");
+    const long long g = (long long)row[0];
+    for (int j = 0; j < nu_r; j++) {
+      if (!next_line(f, s) || !parse_numbers(s, row))
+        return rs_fail(FR_ERR_ARG, "restart file: truncated element data");
+      if ((int)row.size() != n_fields)
+        return rs_fail(FR_ERR_ARG, "restart file holds " + std::to_string(row.size()) + " fields per point, not " +
+                                       std::to_string(n_fields));
+      for (int k = 0; k < n_fields; k++) v[j + (size_t)nu_r * k] = row[k];
+    }
     auto it = where.find(g);
     if (it == where.end()) continue;                  // another rank's element
     const int e = it->second;

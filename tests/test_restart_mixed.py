@@ -126,6 +126,8 @@ def test_mixed_reader_and_writer_errors(tmp_path):
         H.restart_read_points(path, 0, p2, 17, 4)                      # ids 0..16: not all in the file
     with pytest.raises(ValueError):
         H.restart_read_points(path, 0, p2.T, 16, 4, ele2global=ids)    # points must be (n_upts, dims)
+    with pytest.raises(H.FrError, match="4 fields per point, not 5"):
+        H.restart_read_points(path, 0, p2, 16, 5, ele2global=ids)      # a 2-D file has 4 fields
     u = np.zeros((6, 2, 4), order="F")
     with pytest.raises(H.FrError):                                    # triangles need their points
         H.restart_write(tmp_path / "a.dat", 0.0, [dict(ele_type=0, order=2, disu_upts=u)])
