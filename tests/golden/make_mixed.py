@@ -30,7 +30,8 @@ reference has no element for, so hexes and tets never share a face):
     for the second half (hex and prism meet on quadrilateral faces), periodic.
 Interior vertices move by a seeded jitter of up to `jitter` cell sizes.
 
-With --restart-only it reruns mixed_triquad_p2 and mixed_pritet_p2 with the
+With --restart-only it reruns mixed_triquad_p2, mixed_pritet_p2 and
+mixed_hexpri_p3 with the
 harness's --write-restart and keeps the reference's own restart files
 (write_restart, src/output.cpp:1057-1107) verbatim as rest_<name>.dat.
 
@@ -411,7 +412,8 @@ def main():
     work = a.work or tempfile.mkdtemp(prefix="fr_mixed_")
     if a.restart_only:
         run_case_2d(a.ref, [c for c in CASES_2D if c["name"] == "mixed_triquad_p2"][0], work, restart=True)
-        run_case(a.ref, [c for c in CASES if c["name"] == "mixed_pritet_p2"][0], work, restart=True)
+        for name in ("mixed_pritet_p2", "mixed_hexpri_p3"):
+            run_case(a.ref, [c for c in CASES if c["name"] == name][0], work, restart=True)
         return
     for c in CASES_2D:
         arr, par, eles = run_case_2d(a.ref, c, work)

@@ -55,7 +55,7 @@ def blocks(meta, z, opts, path):
     return out
 
 
-CASES = ["mixed_triquad_p2", "mixed_pritet_p2"]
+CASES = ["mixed_triquad_p2", "mixed_pritet_p2", "mixed_hexpri_p3"]
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -75,10 +75,10 @@ def test_reader_on_reference_mixed_file_gives_reference_state(name):
     for b in blocks(meta, z, opts, path):
         et = b["ele_type"]
         pts = b.get("loc_pts")
-        if pts is None:
-            n1 = meta["order"] + 1
+        if pts is None:                                # quads, hexes: tensor points, x fastest
+            n1, D = meta["order"] + 1, 2 if et == 1 else 3
             x = O.points_1d(meta["order"])
-            pts = np.array([(x[j % n1], x[j // n1]) for j in range(n1 * n1)])
+            pts = np.array([[x[(j // n1 ** d) % n1] for d in range(D)] for j in range(n1 ** D)])
         u, t = H.restart_read_points(path, et, pts, b["disu_upts"].shape[1], b["disu_upts"].shape[2],
                                      ele2global=b["ele2global"])
         assert abs(t - meta["steps"] * meta["dt"]) < 1e-12
