@@ -85,7 +85,16 @@ def test_reader_on_reference_mixed_file_gives_reference_state(name):
         assert rel(u, b["disu_upts"]) <= 1e-14
 
 
-@pytest.mark.parametrize("et", [0, 2, 3])
+def _block(et, order, pts, u):
+    b = dict(ele_type=et, order=order, disu_upts=u)
+    if et in (1, 4):
+        b["loc_1d"] = pts[:order + 1, 0]
+    else:
+        b["loc_pts"] = pts
+    return b
+
+
+@pytest.mark.parametrize("et", [0, 1, 2, 3, 4])
 def test_another_order_carries_polynomials_exactly(et, tmp_path):
     """A field of degree <= 2 written at order 2 and read at order 3 equals
     the field at the order-3 points, and reading those back at order 2
@@ -105,12 +114,12 @@ def test_another_order_carries_polynomials_exactly(et, tmp_path):
 
     u2 = np.asfortranarray(field(p2))
     f1 = tmp_path / "Rest2.dat"
-    H.restart_write(f1, 1.5, [dict(ele_type=et, order=2, loc_pts=p2, disu_upts=u2)])
+    H.restart_write(f1, 1.5, [_block(et, 2, p2, u2)])
     u3, t = H.restart_read_points(f1, et, p3, ne, F)
     assert t == 1.5
     assert rel(u3, field(p3)) <= 1e-13
     f2 = tmp_path / "Rest3.dat"
-    H.restart_write(f2, 1.5, [dict(ele_type=et, order=3, loc_pts=p3, disu_upts=u3)])
+    H.restart_write(f2, 1.5, [_block(et, 3, p3, u3)])
     u2b, _ = H.restart_read_points(f2, et, p2, ne, F)
     assert rel(u2b, u2) <= 1e-13
 
