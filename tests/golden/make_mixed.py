@@ -33,7 +33,9 @@ Interior vertices move by a seeded jitter of up to `jitter` cell sizes.
 With --restart-only it reruns mixed_triquad_p2, mixed_pritet_p2 and
 mixed_hexpri_p3 with the
 harness's --write-restart and keeps the reference's own restart files
-(write_restart, src/output.cpp:1057-1107) verbatim as rest_<name>.dat.
+(write_restart, src/output.cpp:1057-1107) verbatim as rest_<name>.dat.  With --restart-read it runs the reference at order 3 on
+mixed_pritet_p2's mesh, restarted from that order-2 file, and keeps its
+states (rest_read_pritet_p2_to_p3.npz).
 
 Usage:  python tests/golden/make_mixed.py --ref <reference checkout>   (or HIFILES_REF=<dir>)
 """
@@ -303,22 +305,7 @@ def run_case(ref, c, work, restart=False):
     lo, hi = (0.0, 0.0, 0.0), (2 * np.pi,) * 3
     xv, eles = mixed_cells(c["kind"], c["n"], lo, hi, c["jitter"], seed=12345)
     write_mixed_gambit(os.path.join(d, "mesh.neu"), xv, eles, c.get("side_bc"))
-    L = [hi[i] - lo[i] for i in range(3)]
-    vals = {
-        "equation": 0, "viscous": 1, "riemann_solve_type": 0, "vis_riemann_solve_type": 0, "ic_form": 7,
-        "order": c["order"], "dt_type": 0, "dt": c["dt"], "n_steps": c["steps"], "adv_type": 3, "tau": 1.0,
-        "pen_fact": 0.5, "mesh_file": "mesh.neu", "dx_cyclic": "%.17g" % L[0], "dy_cyclic": "%.17g" % L[1],
-        "dz_cyclic": "%.17g" % L[2], "monitor_res_freq": 100000, "plot_freq": 100000, "restart_dump_freq": 100000,
-        "upts_type_hexa": 0, "vcjh_scheme_hexa": 1, "upts_type_tet": c["tet_upts"], "fpts_type_tet": 0, "vcjh_scheme_tet": 2,
-        "upts_type_pri_tri": 0, "upts_type_pri_1d": 0, "vcjh_scheme_pri_1d": 1, "vcjh_scheme_tri": 1,
-        "prandtl": 0.71, "Mach_free_stream": 0.1, "Re_free_stream": 1600.0, "gamma": 1.4, "fix_vis": 1,
-        "res_norm_type": 1,
-    }
-    if c.get("side_bc"):
-        # free stream along x, wall temperature = free-stream temperature
-        vals.update({"nx_free_stream": 1.0, "ny_free_stream": 0.0, "nz_free_stream": 0.0, "Mach_wall": 0.0,
-                     "nx_wall": 1.0, "ny_wall": 0.0, "nz_wall": 0.0, "rho_bound": 1.0, "u_bound": 1.0,
-                     "v_bound": 0.0, "w_bound": 0.0, "p_bound": 1.0, "T_wall": 300.0, "T_free_stream": 300.0})
+    vals = input_values_3d(c, [hi[i] - lo[i] for i in range(3)])
     G.write_input(os.path.join(d, "input"), os.path.join(ref, G.TGV_INPUT), vals)
     out = os.path.join(d, "out")
     os.makedirs(out, exist_ok=True)
@@ -340,6 +327,58 @@ def run_case(ref, c, work, restart=False):
             types.append(dict(index=int(p[1]), ele_type=int(p[3]), n_eles=int(p[5]), n_upts=int(p[7]),
                               n_fpts=int(p[9])))
     return arr, par, types, eles
+
+
+def input_values_3d(c, L):
+    """The reference's input keys of a 3-D mixed case (periodic lengths L)."""
+    vals = {
+        "equation": 0, "viscous": 1, "riemann_solve_type": 0, "vis_riemann_solve_type": 0, "ic_form": 7,
+        "order": c["order"], "dt_type": 0, "dt": c["dt"], "n_steps": c["steps"], "adv_type": 3, "tau": 1.0,
+        "pen_fact": 0.5, "mesh_file": "mesh.neu", "dx_cyclic": "%.17g" % L[0], "dy_cyclic": "%.17g" % L[1],
+        "dz_cyclic": "%.17g" % L[2], "monitor_res_freq": 100000, "plot_freq": 100000, "restart_dump_freq": 100000,
+        "upts_type_hexa": 0, "vcjh_scheme_hexa": 1, "upts_type_tet": c["tet_upts"], "fpts_type_tet": 0, "vcjh_scheme_tet": 2,
+        "upts_type_pri_tri": 0, "upts_type_pri_1d": 0, "vcjh_scheme_pri_1d": 1, "vcjh_scheme_tri": 1,
+        "prandtl": 0.71, "Mach_free_stream": 0.1, "Re_free_stream": 1600.0, "gamma": 1.4, "fix_vis": 1,
+        "res_norm_type": 1,
+    }
+    if c.get("side_bc"):
+        # free stream along x, wall temperature = free-stream temperature
+        vals.update({"nx_free_stream": 1.0, "ny_free_stream": 0.0, "nz_free_stream": 0.0, "Mach_wall": 0.0,
+                     "nx_wall": 1.0, "ny_wall": 0.0, "nz_wall": 0.0, "rho_bound": 1.0, "u_bound": 1.0,
+                     "v_bound": 0.0, "w_bound": 0.0, "p_bound": 1.0, "T_wall": 300.0, "T_free_stream": 300.0})
+    return vals
+
+
+def restart_read_fixture(ref, work):
+    """The reference reading its own order-2 restart file of mixed_pritet_p2
+    (rest_mixed_pritet_p2.dat) on the same mesh set up at order 3: read_restart
+    with each type's read_restart_info and eles::set_opp_r (src/solver.cpp:390-445,
+    src/eles_tets.cpp:749-780, src/eles_pris.cpp:655-698, src/eles.cpp:4135-4153)
+    -> its tet and prism disu_upts(0) at order 3, kept as
+    rest_read_pritet_p2_to_p3.npz."""
+    import shutil
+    c = dict([c for c in CASES if c["name"] == "mixed_pritet_p2"][0], order=3)
+    d = os.path.join(work, "restart_read_pritet")
+    os.makedirs(d, exist_ok=True)
+    shutil.copy(os.path.join(HERE, "rest_mixed_pritet_p2.dat"), os.path.join(d, "Rest_%09d_p%04d.dat" % (c["steps"], 0)))
+    lo, hi = (0.0, 0.0, 0.0), (2 * np.pi,) * 3
+    xv, eles = mixed_cells(c["kind"], c["n"], lo, hi, c["jitter"], seed=12345)
+    write_mixed_gambit(os.path.join(d, "mesh.neu"), xv, eles, None)
+    vals = input_values_3d(c, [hi[i] - lo[i] for i in range(3)])
+    vals.update({"restart_flag": 1, "restart_iter": c["steps"], "n_restart_files": 1})
+    G.write_input(os.path.join(d, "input"), os.path.join(ref, G.TGV_INPUT), vals)
+    out = os.path.join(d, "out")
+    os.makedirs(out, exist_ok=True)
+    env = dict(os.environ, HIFILES_HOME=os.path.join(REPO, "oracle", "_ref"))
+    r = subprocess.run([G.HARNESS, "input", out, "--steps", "0"], cwd=d, env=env, capture_output=True, text=True)
+    if r.returncode != 0:
+        print(r.stdout[-3000:], r.stderr[-3000:])
+        raise RuntimeError("harness failed reading a restart file")
+    arr, _ = G.load_npy_dir(out)
+    keep = {"t%d_u_p3_ref" % t: np.asfortranarray(arr["t%d_disu_upts_init" % t]) for t in (2, 3)}
+    np.savez_compressed(os.path.join(HERE, "rest_read_pritet_p2_to_p3.npz"),
+                        time=c["steps"] * c["dt"], **keep)
+    print("restart read fixture:", {k: v.shape for k, v in keep.items()})
 
 
 # 2-D quadrilateral boxes with boundaries on every side (side order x-, x+,
@@ -406,10 +445,15 @@ def main():
     ap.add_argument("--only-2d", action="store_true", help="write the 2-D triangle/quad fixtures only")
     ap.add_argument("--restart-only", action="store_true",
                     help="write only the reference's restart files of mixed_triquad_p2 and mixed_pritet_p2")
+    ap.add_argument("--restart-read", action="store_true",
+                    help="write only the fixture of the reference reading rest_mixed_pritet_p2.dat at order 3")
     a = ap.parse_args()
     if not os.path.exists(G.HARNESS):
         subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "REF=" + a.ref, "ref"], check=True)
     work = a.work or tempfile.mkdtemp(prefix="fr_mixed_")
+    if a.restart_read:
+        restart_read_fixture(a.ref, work)
+        return
     if a.restart_only:
         run_case_2d(a.ref, [c for c in CASES_2D if c["name"] == "mixed_triquad_p2"][0], work, restart=True)
         for name in ("mixed_pritet_p2", "mixed_hexpri_p3"):

@@ -226,3 +226,20 @@ def test_fused_run_continues_from_a_restart_file(name, tmp_path):
         m2.advance(2, meta["dt"])
         for et in M.types:
             assert rel(m2.get_state(et), m1.get_state(et)) <= 1e-12, (path, et)
+
+
+def test_order_change_matches_the_reference_reading_its_own_file():
+    """The reference set up at order 3 on mixed_pritet_p2's mesh, restarted
+    from its own order-2 file (rest_read_pritet_p2_to_p3.npz, made by
+    make_mixed.py --restart-read), against MixedMesh.read_restart of the same
+    file at order 3: tets and prisms through the nodal bases on the file's
+    points."""
+    from test_mixed_setup import fixture_mesh
+    meta, _, _ = fixture("mixed_pritet_p2")
+    want = np.load(os.path.join(GOLDEN, "rest_read_pritet_p2_to_p3.npz"))
+    xv, cells, period, bfaces, opts = fixture_mesh(meta)
+    M3 = X.MixedMesh(3, xv, cells, period, bfaces, opts)
+    u, t = M3.read_restart(os.path.join(GOLDEN, "rest_mixed_pritet_p2.dat"))
+    assert abs(t - float(want["time"])) < 1e-15
+    for et in (2, 3):
+        assert rel(u[et], want["t%d_u_p3_ref" % et]) <= 1e-14, (et, rel(u[et], want["t%d_u_p3_ref" % et]))
