@@ -34,8 +34,8 @@ With --restart-only it reruns mixed_triquad_p2, mixed_pritet_p2 and
 mixed_hexpri_p3 with the
 harness's --write-restart and keeps the reference's own restart files
 (write_restart, src/output.cpp:1057-1107) verbatim as rest_<name>.dat.  With --restart-read it runs the reference at order 3 on
-mixed_pritet_p2's mesh, restarted from that order-2 file, and keeps its
-states (rest_read_pritet_p2_to_p3.npz).
+the meshes of mixed_triquad_p2 and mixed_pritet_p2, restarted from those
+order-2 files, and keeps its states (rest_read_<kind>_p2_to_p3.npz).
 
 Usage:  python tests/golden/make_mixed.py --ref <reference checkout>   (or HIFILES_REF=<dir>)
 """
@@ -262,17 +262,7 @@ def run_case_2d(ref, c, work, restart=False):
     lo, hi = (0.0, 0.0), (2 * np.pi, 2 * np.pi)
     xv, eles = mixed_cells_2d(c["n"], lo, hi, c["jitter"], seed=12345)
     write_mixed_gambit(os.path.join(d, "mesh.neu"), xv, eles, [0, 0, 0, 0])
-    vals = {
-        "equation": 0, "viscous": 1, "riemann_solve_type": 0, "vis_riemann_solve_type": 0, "ic_form": 7,
-        "order": c["order"], "dt_type": 0, "dt": c["dt"], "n_steps": c["steps"], "adv_type": 3, "tau": 1.0,
-        "pen_fact": 0.5, "mesh_file": "mesh.neu", "dx_cyclic": "%.17g" % (hi[0] - lo[0]),
-        "dy_cyclic": "%.17g" % (hi[1] - lo[1]), "dz_cyclic": 0.0, "monitor_res_freq": 100000,
-        "plot_freq": 100000, "restart_dump_freq": 100000,
-        "upts_type_quad": 0, "vcjh_scheme_quad": 1, "upts_type_tri": c["tri_upts"], "fpts_type_tri": c["tri_fpts"],
-        "vcjh_scheme_tri": c["vcjh_tri"],
-        "prandtl": 0.71, "Mach_free_stream": 0.1, "Re_free_stream": 1600.0, "gamma": 1.4, "fix_vis": 1,
-        "res_norm_type": 1,
-    }
+    vals = input_values_2d(c, lo, hi)
     G.write_input(os.path.join(d, "input"), os.path.join(ref, G.TGV_INPUT), vals)
     out = os.path.join(d, "out")
     os.makedirs(out, exist_ok=True)
@@ -288,6 +278,21 @@ def run_case_2d(ref, c, work, restart=False):
         keep_restart(d, c)
     arr, par = G.load_npy_dir(out)
     return arr, par, eles
+
+
+def input_values_2d(c, lo, hi):
+    """The reference's input keys of a 2-D triangle/quad case."""
+    return {
+        "equation": 0, "viscous": 1, "riemann_solve_type": 0, "vis_riemann_solve_type": 0, "ic_form": 7,
+        "order": c["order"], "dt_type": 0, "dt": c["dt"], "n_steps": c["steps"], "adv_type": 3, "tau": 1.0,
+        "pen_fact": 0.5, "mesh_file": "mesh.neu", "dx_cyclic": "%.17g" % (hi[0] - lo[0]),
+        "dy_cyclic": "%.17g" % (hi[1] - lo[1]), "dz_cyclic": 0.0, "monitor_res_freq": 100000,
+        "plot_freq": 100000, "restart_dump_freq": 100000,
+        "upts_type_quad": 0, "vcjh_scheme_quad": 1, "upts_type_tri": c["tri_upts"], "fpts_type_tri": c["tri_fpts"],
+        "vcjh_scheme_tri": c["vcjh_tri"],
+        "prandtl": 0.71, "Mach_free_stream": 0.1, "Re_free_stream": 1600.0, "gamma": 1.4, "fix_vis": 1,
+        "res_norm_type": 1,
+    }
 
 
 # arrays kept per element type (prefix t<ele_type>_ in the harness output)
@@ -350,35 +355,46 @@ def input_values_3d(c, L):
 
 
 def restart_read_fixture(ref, work):
-    """The reference reading its own order-2 restart file of mixed_pritet_p2
-    (rest_mixed_pritet_p2.dat) on the same mesh set up at order 3: read_restart
-    with each type's read_restart_info and eles::set_opp_r (src/solver.cpp:390-445,
-    src/eles_tets.cpp:749-780, src/eles_pris.cpp:655-698, src/eles.cpp:4135-4153)
-    -> its tet and prism disu_upts(0) at order 3, kept as
-    rest_read_pritet_p2_to_p3.npz."""
+    """The reference reading its own order-2 restart files of
+    mixed_triquad_p2 and mixed_pritet_p2 (rest_<name>.dat) on the same meshes
+    set up at order 3: read_restart with each type's read_restart_info and
+    eles::set_opp_r (src/solver.cpp:390-445, src/eles_tris.cpp:511-543,
+    src/eles_tets.cpp:749-780, src/eles_pris.cpp:655-698,
+    src/eles.cpp:4135-4153) -> every type's disu_upts(0) at order 3, kept as
+    rest_read_<kind>_p2_to_p3.npz."""
     import shutil
-    c = dict([c for c in CASES if c["name"] == "mixed_pritet_p2"][0], order=3)
-    d = os.path.join(work, "restart_read_pritet")
-    os.makedirs(d, exist_ok=True)
-    shutil.copy(os.path.join(HERE, "rest_mixed_pritet_p2.dat"), os.path.join(d, "Rest_%09d_p%04d.dat" % (c["steps"], 0)))
-    lo, hi = (0.0, 0.0, 0.0), (2 * np.pi,) * 3
-    xv, eles = mixed_cells(c["kind"], c["n"], lo, hi, c["jitter"], seed=12345)
-    write_mixed_gambit(os.path.join(d, "mesh.neu"), xv, eles, None)
-    vals = input_values_3d(c, [hi[i] - lo[i] for i in range(3)])
-    vals.update({"restart_flag": 1, "restart_iter": c["steps"], "n_restart_files": 1})
-    G.write_input(os.path.join(d, "input"), os.path.join(ref, G.TGV_INPUT), vals)
-    out = os.path.join(d, "out")
-    os.makedirs(out, exist_ok=True)
-    env = dict(os.environ, HIFILES_HOME=os.path.join(REPO, "oracle", "_ref"))
-    r = subprocess.run([G.HARNESS, "input", out, "--steps", "0"], cwd=d, env=env, capture_output=True, text=True)
-    if r.returncode != 0:
-        print(r.stdout[-3000:], r.stderr[-3000:])
-        raise RuntimeError("harness failed reading a restart file")
-    arr, _ = G.load_npy_dir(out)
-    keep = {"t%d_u_p3_ref" % t: np.asfortranarray(arr["t%d_disu_upts_init" % t]) for t in (2, 3)}
-    np.savez_compressed(os.path.join(HERE, "rest_read_pritet_p2_to_p3.npz"),
-                        time=c["steps"] * c["dt"], **keep)
-    print("restart read fixture:", {k: v.shape for k, v in keep.items()})
+    for name in ("mixed_triquad_p2", "mixed_pritet_p2"):
+        two_d = name == "mixed_triquad_p2"
+        c = dict([c for c in (CASES_2D if two_d else CASES) if c["name"] == name][0], order=3)
+        d = os.path.join(work, "restart_read_" + c["kind"])
+        os.makedirs(d, exist_ok=True)
+        shutil.copy(os.path.join(HERE, "rest_%s.dat" % name), os.path.join(d, "Rest_%09d_p%04d.dat" % (c["steps"], 0)))
+        if two_d:
+            lo, hi = (0.0, 0.0), (2 * np.pi, 2 * np.pi)
+            xv, eles = mixed_cells_2d(c["n"], lo, hi, c["jitter"], seed=12345)
+            write_mixed_gambit(os.path.join(d, "mesh.neu"), xv, eles, [0, 0, 0, 0])
+            vals = input_values_2d(c, lo, hi)
+            kinds = (0, 1)
+        else:
+            lo, hi = (0.0, 0.0, 0.0), (2 * np.pi,) * 3
+            xv, eles = mixed_cells(c["kind"], c["n"], lo, hi, c["jitter"], seed=12345)
+            write_mixed_gambit(os.path.join(d, "mesh.neu"), xv, eles, None)
+            vals = input_values_3d(c, [hi[i] - lo[i] for i in range(3)])
+            kinds = (2, 3)
+        vals.update({"restart_flag": 1, "restart_iter": c["steps"], "n_restart_files": 1})
+        G.write_input(os.path.join(d, "input"), os.path.join(ref, G.TGV_INPUT), vals)
+        out = os.path.join(d, "out")
+        os.makedirs(out, exist_ok=True)
+        env = dict(os.environ, HIFILES_HOME=os.path.join(REPO, "oracle", "_ref"))
+        r = subprocess.run([G.HARNESS, "input", out, "--steps", "0"], cwd=d, env=env, capture_output=True, text=True)
+        if r.returncode != 0:
+            print(r.stdout[-3000:], r.stderr[-3000:])
+            raise RuntimeError("harness failed reading a restart file")
+        arr, _ = G.load_npy_dir(out)
+        keep = {"t%d_u_p3_ref" % t: np.asfortranarray(arr["t%d_disu_upts_init" % t]) for t in kinds}
+        np.savez_compressed(os.path.join(HERE, "rest_read_%s_p2_to_p3.npz" % c["kind"]),
+                            time=c["steps"] * c["dt"], **keep)
+        print("restart read fixture", c["kind"], {k: v.shape for k, v in keep.items()})
 
 
 # 2-D quadrilateral boxes with boundaries on every side (side order x-, x+,
@@ -446,7 +462,7 @@ def main():
     ap.add_argument("--restart-only", action="store_true",
                     help="write only the reference's restart files of mixed_triquad_p2 and mixed_pritet_p2")
     ap.add_argument("--restart-read", action="store_true",
-                    help="write only the fixture of the reference reading rest_mixed_pritet_p2.dat at order 3")
+                    help="write only the fixtures of the reference reading the order-2 restart files at order 3")
     a = ap.parse_args()
     if not os.path.exists(G.HARNESS):
         subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "REF=" + a.ref, "ref"], check=True)

@@ -228,18 +228,20 @@ def test_fused_run_continues_from_a_restart_file(name, tmp_path):
             assert rel(m2.get_state(et), m1.get_state(et)) <= 1e-12, (path, et)
 
 
-def test_order_change_matches_the_reference_reading_its_own_file():
-    """The reference set up at order 3 on mixed_pritet_p2's mesh, restarted
-    from its own order-2 file (rest_read_pritet_p2_to_p3.npz, made by
+@pytest.mark.parametrize("name", ["mixed_triquad_p2", "mixed_pritet_p2"])
+def test_order_change_matches_the_reference_reading_its_own_file(name):
+    """The reference set up at order 3 on a fixture's mesh, restarted from
+    its own order-2 file (rest_read_<kind>_p2_to_p3.npz, made by
     make_mixed.py --restart-read), against MixedMesh.read_restart of the same
-    file at order 3: tets and prisms through the nodal bases on the file's
-    points."""
+    file at order 3: every element type through the nodal bases on the
+    file's points."""
     from test_mixed_setup import fixture_mesh
-    meta, _, _ = fixture("mixed_pritet_p2")
-    want = np.load(os.path.join(GOLDEN, "rest_read_pritet_p2_to_p3.npz"))
+    meta, _, _ = fixture(name)
+    want = np.load(os.path.join(GOLDEN, "rest_read_%s_p2_to_p3.npz" % meta["kind"]))
     xv, cells, period, bfaces, opts = fixture_mesh(meta)
     M3 = X.MixedMesh(3, xv, cells, period, bfaces, opts)
-    u, t = M3.read_restart(os.path.join(GOLDEN, "rest_mixed_pritet_p2.dat"))
+    u, t = M3.read_restart(os.path.join(GOLDEN, "rest_%s.dat" % name))
     assert abs(t - float(want["time"])) < 1e-15
-    for et in (2, 3):
+    assert sorted(u) == sorted(int(k[1]) for k in want.files if k.endswith("_u_p3_ref"))
+    for et in u:
         assert rel(u[et], want["t%d_u_p3_ref" % et]) <= 1e-14, (et, rel(u[et], want["t%d_u_p3_ref" % et]))
