@@ -128,6 +128,7 @@ def lib():
         "fr_restart_write": (C.c_int, [C.c_char_p, C.c_double, vp, C.c_int]),
         "fr_restart_read": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp, dp, dp]),
         "fr_restart_read_points": (C.c_int, [C.c_char_p, C.c_int, C.c_int, dp, C.c_int, C.c_int, vp, dp, dp]),
+        "fr_vtu_write_mixed": (C.c_int, [C.c_char_p, C.c_int, vp, C.c_int, C.c_double]),
         "fr_solver_write_restart": (C.c_int, [vp, C.c_char_p, C.c_double]),
         "fr_solver_read_restart": (C.c_int, [vp, C.c_char_p, dp]),
         "fr_solver_sgs_features": (C.c_int, [vp, C.POINTER(C.c_float), vp]),
@@ -667,6 +668,25 @@ class Batch:
     def dof(self):
         """Degrees of freedom of the whole batch (sum of n_upts * n_eles * n_fields)."""
         return int(sum(a * b * c for a, b, c in self.shapes))
+
+
+class VtuBlock(C.Structure):
+    _fields_ = [("ele_type", C.c_int), ("n_eles", C.c_int), ("loc_pts", C.POINTER(C.c_double)),
+                ("pos_upts", C.POINTER(C.c_double)), ("disu_upts", C.POINTER(C.c_double))]
+
+
+def vtu_write_mixed(path, order, blocks, gamma=1.4):
+    """Host-only .vtu writer of a mixed mesh (see fr_vtu_write_mixed): blocks is a list of dicts(ele_type,
+    pos_upts (n_upts, n_eles, dims), disu_upts (n_upts, n_eles, dims + 2), loc_pts (triangles, tets,
+    prisms: the (n_upts, dims) solution points))."""
+    keep, arr = [], (VtuBlock * len(blocks))()
+    for i, b in enumerate(blocks):
+        pos = np.asfortranarray(b["pos_upts"], dtype=np.float64)
+        u = np.asfortranarray(b["disu_upts"], dtype=np.float64)
+        pts = None if b.get("loc_pts") is None else _points(b["loc_pts"], b["ele_type"])
+        keep += [pos, u, pts]
+        arr[i] = VtuBlock(int(b["ele_type"]), u.shape[1], None if pts is None else _dp(pts), _dp(pos), _dp(u))
+    _check(lib().fr_vtu_write_mixed(str(path).encode(), int(order), arr, len(blocks), float(gamma)))
 
 
 def vtu_write(path, dims, order, pos_upts, disu_upts, gamma=1.4):

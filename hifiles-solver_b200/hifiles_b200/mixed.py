@@ -16,7 +16,7 @@ import itertools
 
 import numpy as np
 
-from . import _check, box_mesh, lib, restart_read_points, restart_write
+from . import _check, box_mesh, lib, restart_read_points, restart_write, vtu_write_mixed
 
 TRI, QUAD, TET, PRISM, HEX = 0, 1, 2, 3, 4
 _NODES = {TRI: 3, QUAD: 4, TET: 4, PRISM: 6, HEX: 8}
@@ -196,6 +196,14 @@ class MixedMesh:
                 b["loc_pts"] = m["loc_upts"].T
             blocks.append(b)
         restart_write(path, time, blocks)
+
+    def write_vtu(self, path, states, gamma=1.4):
+        """states (element type -> (n_upts, n_eles, dims + 2)) as one .vtu
+        file (fr_vtu_write_mixed): the role of the reference's Paraview
+        output (src/output.cpp:580-1055)."""
+        vtu_write_mixed(path, self.order, [dict(ele_type=t, pos_upts=m["pos_upts"], disu_upts=states[t],
+                                                loc_pts=None if t in (QUAD, HEX) else m["loc_upts"].T)
+                                           for t, m in sorted(self.types.items())], gamma)
 
     def read_restart(self, path, n_fields=None):
         """({element type: state (n_upts, n_eles, F)}, time) from a restart

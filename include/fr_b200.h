@@ -312,6 +312,22 @@ fr_status fr_vtu_write(const char* path, int dims, int order, int n_eles, const 
                        const double* disu_upts, double gamma);
 /* The solver's current state as such a file (one device-to-host copy). */
 fr_status fr_solver_write_vtu(fr_solver* s, const char* path);
+/* One element type of a mixed mesh for fr_vtu_write_mixed. */
+typedef struct {
+  int ele_type;            /* 0 triangles, 1 quads, 2 tets, 3 prisms, 4 hexes   */
+  int n_eles;
+  const double* loc_pts;   /* triangles, tets, prisms: the solution points,
+                              (n_upts, dims) point-major as
+                              fr_element_operators gives them                  */
+  const double* pos_upts;  /* (n_upts, n_eles, dims)                           */
+  const double* disu_upts; /* (n_upts, n_eles, dims + 2)                       */
+} fr_vtu_block;
+/* A mixed mesh's solution as one .vtu file (all blocks of one dimension).
+ * Quads and hexes as fr_vtu_write; triangles, tets and prisms interpolated
+ * through their nodal basis to the equispaced lattice of order `order` (the
+ * reference's plot points, eles::set_opp_p) and cut into order^dims
+ * triangles, tetrahedra or wedges.  Host memory only. */
+fr_status fr_vtu_write_mixed(const char* path, int order, const fr_vtu_block* blocks, int n_blocks, double gamma);
 
 /* The solver's state to / from a restart file (global ids 0 .. n_eles-1). */
 fr_status fr_solver_write_restart(fr_solver* s, const char* path, double time);
