@@ -220,10 +220,16 @@ struct Items {
 // ---------------------------------------------------------------------------
 // Initial flux-point traces from the state (used once after the state is set).
 template <int DIM, int P, typename TC>
-__global__ void fr_trace_kernel(const double* __restrict__ U, TC* __restrict__ UF, long long E, Line<TC> L)
+__global__ void fr_trace_kernel(const double* __restrict__ U, TC* __restrict__ UF, long long E, Line<TC> L,
+                                double* __restrict__ Uout = nullptr)
 {
   using S = Shape<DIM, P>;
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  // with Uout, U is a staged state that the same pass copies into place
+  // (the grid then covers max(NF, NU) points per element)
+  if (Uout && i < E * S::NU)
+#pragma unroll
+    for (int k = 0; k < S::F; k++) Uout[i + (size_t)S::NU * E * k] = U[i + (size_t)S::NU * E * k];
   if (i >= E * S::NF) return;
   long long e = i / S::NF;
   int f = (int)(i - e * S::NF);

@@ -44,7 +44,8 @@ struct Tile {
 
 struct Runner {
   virtual ~Runner() {}
-  virtual void trace(const Bufs& b, int cur, cudaStream_t s) = 0;
+  // traces of the state; with src, the state src is also copied into b.U
+  virtual void trace(const Bufs& b, int cur, cudaStream_t s, const double* src = nullptr) = 0;
   virtual void grad(const Bufs& b, int cur, cudaStream_t s) = 0;
   virtual void face(const Bufs& b, int cur, cudaStream_t s) = 0;
   virtual void update(const Bufs& b, int cur, int mode, int stage, double dt, bool want_partial, cudaStream_t s) = 0;
@@ -150,10 +151,11 @@ struct RunnerT : Runner {
   static constexpr bool FU = fu_bulk_ok<DIM, P, TC>();
   int launches_per_stage() const override { return FU ? (visc ? 2 : 1) : (visc ? 3 : 2); }
   void set_riemann(int rs) override { riemann = rs; }
-  void trace(const Bufs& b, int cur, cudaStream_t s) override
+  void trace(const Bufs& b, int cur, cudaStream_t s, const double* src = nullptr) override
   {
-    long long n = E * S::NF;
-    fr_trace_kernel<DIM, P, TC><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b.U, (TC*)b.UF[cur], E, L);
+    long long n = E * (src && S::NU > S::NF ? S::NU : S::NF);
+    fr_trace_kernel<DIM, P, TC><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src ? src : b.U, (TC*)b.UF[cur], E, L,
+                                                                           src ? b.U : nullptr);
   }
 
   template <int I, int LES>

@@ -472,17 +472,19 @@ fr_status fr_solver_set_state_async(fr_solver* s, const double* host_u)
   return FR_OK;
 }
 
-// The staged state (if any) becomes the current state, in stream order.
+// The staged state (if any) becomes the current state, in stream order: one
+// pass copies it into place and extrapolates its traces.  The RK register
+// is left as it is: the first stage of a step writes it without reading it.
 static fr_status take_staged(fr_solver* s, cudaStream_t st)
 {
   if (!s->staged) return FR_OK;
-  size_t n = (size_t)s->mesh.nu * s->mesh.ne * s->mesh.nfields;
   FR_CUDA(cudaStreamWaitEvent(st, s->ev_staged, 0));
-  FR_CUDA(cudaMemcpyAsync(s->b.U, s->staging, n * 8, cudaMemcpyDeviceToDevice, st));
+  s->run->trace(s->b, s->cur, st, s->staging);
+  s->launches++;
+  if (fr_status r = check_launch("fr_trace_kernel")) return r;
   FR_CUDA(cudaEventRecord(s->ev_consumed, st));
-  FR_CUDA(cudaMemsetAsync(s->b.REG, 0, n * 8, st));
   s->staged = false;
-  return fr_solver_state_updated(s, st);
+  return FR_OK;
 }
 
 fr_status fr_solver_get_state(fr_solver* s, double* host_u, void* stream)
