@@ -126,8 +126,10 @@ fr_status fr_solver_set_state(fr_solver* s, const double* host_u, void* stream);
  * must stay unchanged until the copy is done -- into a device staging buffer
  * on the solver's copy stream, overlapping steps already queued.  The next
  * fr_solver_advance / fr_solver_advance_async takes it as the current state
- * (RK register cleared, traces rebuilt) in stream order.  One state can be
- * staged at a time (FR_ERR_ARG otherwise).  No counterpart in the reference. */
+ * (traces rebuilt in the same pass) in stream order; the RK register is not
+ * cleared, since the first stage of the next step writes it without reading
+ * it.  One state can be staged at a time (FR_ERR_ARG otherwise).  No
+ * counterpart in the reference. */
 fr_status fr_solver_set_state_async(fr_solver* s, const double* host_u);
 fr_status fr_solver_get_state(fr_solver* s, double* host_u, void* stream);
 /* Device pointers of the resident state and RK register (owned by the solver). */
