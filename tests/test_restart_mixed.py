@@ -245,3 +245,23 @@ def test_order_change_matches_the_reference_reading_its_own_file(name):
     assert sorted(u) == sorted(int(k[1]) for k in want.files if k.endswith("_u_p3_ref"))
     for et in u:
         assert rel(u[et], want["t%d_u_p3_ref" % et]) <= 1e-14, (et, rel(u[et], want["t%d_u_p3_ref" % et]))
+
+
+@pytest.mark.parametrize("et,order", [(0, 2), (0, 4), (1, 3), (2, 2), (2, 3), (3, 2), (3, 4), (4, 3)])
+def test_file_basis_equals_the_element_basis(et, order, tmp_path):
+    """Reading a file onto an element's flux points applies the nodal basis
+    built from the file's points; at the element's own solution points that
+    is the element's opp_0 (the extrapolation the reference builds in
+    set_opp_0, src/eles.cpp:3620-3676)."""
+    opts = X.ElementOpts(upts_type_tet=1, vcjh_scheme_tet=1, vcjh_scheme_tri=1, vcjh_scheme_pri_1d=1)
+    ops = X.element_operators(et, order, opts)
+    pts = ops["loc_upts"].T.copy()
+    rng = np.random.default_rng(11)
+    ne, F = 3, 4 if et in (0, 1) else 5
+    u = np.asfortranarray(rng.normal(size=(pts.shape[0], ne, F)))
+    path = tmp_path / "Rest.dat"
+    H.restart_write(path, 0.0, [_block(et, order, pts, u)])
+    got, _ = H.restart_read_points(path, et, ops["tloc_fpts"].T, ne, F)
+    u15 = H.restart_read_points(path, et, pts, ne, F)[0]           # the values as the file holds them
+    want = np.einsum("qj,jef->qef", ops["opp_0"], u15)
+    assert rel(got, want) <= 1e-13, rel(got, want)
