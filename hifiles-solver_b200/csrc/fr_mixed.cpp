@@ -569,8 +569,12 @@ static bool tri_correction(int P, const double* tri, const double* x1d, int sche
   for (int i = 0; i < nt; i++)
     for (int j = 0; j < nt; j++) V[(size_t)i * nt + j] = dub2(tri[2 * i], tri[2 * i + 1], m2[j][0], m2[j][1]);
   if (!invert(nt, V, Vinv)) { err = "prisms: singular triangle Vandermonde matrix"; return false; }
+  // The edge integrals use the reference's fixed 5-point Gauss rule
+  // (cubature_1d(10) in eval_div_dg_tri, src/funcs.cpp:819, takes (10 + 1) / 2
+  // points, src/cubature_1d.cpp:61): exact for the degree-2P integrands up to
+  // P = 4; at P = 5 the reference's lift is that rule's, and so is this one.
   std::vector<double> gx, gw;
-  gauss(P + 2, gx, gw);
+  gauss(5, gx, gw);
   Mat dg((size_t)nt * ne, 0.0);
   for (int e = 0; e < 3; e++) {
     double half = e == 1 ? std::sqrt(2.) : 1.0;

@@ -397,6 +397,49 @@ def restart_read_fixture(ref, work):
         print("restart read fixture", c["kind"], {k: v.shape for k, v in keep.items()})
 
 
+def operator_fixture(ref, work):
+    """The reference's element operators opp_0 .. opp_6 (per-type set-up of
+    eles_tris / eles_tets / eles_pris, src/eles.cpp:3620-4052) at the orders
+    the mixed fixtures do not cover, on small meshes of the fixtures' kinds
+    with the DG correction (vcjh scheme 1), kept as ops_<kind>_p<order>.npz."""
+    for kind, order in (("triquad", 1), ("triquad", 4), ("triquad", 5), ("pritet", 1), ("pritet", 4),
+                        ("pritet", 5)):
+        two_d = kind == "triquad"
+        base = [c for c in (CASES_2D if two_d else CASES) if c["name"] == "mixed_%s_p2" % kind][0]
+        c = dict(base, order=order, steps=1, vcjh_tri=1)
+        d = os.path.join(work, "ops_%s_p%d" % (kind, order))
+        os.makedirs(d, exist_ok=True)
+        if two_d:
+            lo, hi = (0.0, 0.0), (2 * np.pi, 2 * np.pi)
+            xv, eles = mixed_cells_2d(c["n"], lo, hi, c["jitter"], seed=12345)
+            write_mixed_gambit(os.path.join(d, "mesh.neu"), xv, eles, [0, 0, 0, 0])
+            vals = input_values_2d(c, lo, hi)
+            ic, kinds = "channel_mach01", (0, 1)
+        else:
+            lo, hi = (0.0, 0.0, 0.0), (2 * np.pi,) * 3
+            xv, eles = mixed_cells(c["kind"], c["n"], lo, hi, c["jitter"], seed=12345)
+            write_mixed_gambit(os.path.join(d, "mesh.neu"), xv, eles, None)
+            vals = input_values_3d(c, [hi[i] - lo[i] for i in range(3)])
+            vals["vcjh_scheme_tet"] = 1
+            ic, kinds = "tgv_mach01", (2, 3)
+        G.write_input(os.path.join(d, "input"), os.path.join(ref, G.TGV_INPUT), vals)
+        out = os.path.join(d, "out")
+        os.makedirs(out, exist_ok=True)
+        env = dict(os.environ, HIFILES_HOME=os.path.join(REPO, "oracle", "_ref"))
+        r = subprocess.run([G.HARNESS, "input", out, "--ic", ic, "--steps", "0"], cwd=d, env=env,
+                           capture_output=True, text=True)
+        if r.returncode != 0:
+            print(r.stdout[-3000:], r.stderr[-3000:])
+            raise RuntimeError("harness failed for operators of %s P%d" % (kind, order))
+        arr, _ = G.load_npy_dir(out)
+        keep = {k: np.asfortranarray(v) for k, v in arr.items()
+                if k[:3] in ("t%d_" % kinds[0], "t%d_" % kinds[1]) and k[3:].startswith("opp_")}
+        meta = dict(kind=kind, order=order, tri_upts=c.get("tri_upts"), tri_fpts=c.get("tri_fpts"),
+                    tet_upts=c.get("tet_upts"), vcjh=1)
+        np.savez_compressed(os.path.join(HERE, "ops_%s_p%d.npz" % (kind, order)), meta=json.dumps(meta), **keep)
+        print("operators", kind, order, sorted(keep))
+
+
 # 2-D quadrilateral boxes with boundaries on every side (side order x-, x+,
 # y-, y+), run through make_golden's writer and input; they exercise the
 # boundary entry points in 2-D and every boundary type but the moving walls'
@@ -461,12 +504,17 @@ def main():
     ap.add_argument("--only-2d", action="store_true", help="write the 2-D triangle/quad fixtures only")
     ap.add_argument("--restart-only", action="store_true",
                     help="write only the reference's restart files of mixed_triquad_p2 and mixed_pritet_p2")
+    ap.add_argument("--operators", action="store_true",
+                    help="write only the reference's element operators at orders 1, 4 and 5")
     ap.add_argument("--restart-read", action="store_true",
                     help="write only the fixtures of the reference reading the order-2 restart files at order 3")
     a = ap.parse_args()
     if not os.path.exists(G.HARNESS):
         subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "REF=" + a.ref, "ref"], check=True)
     work = a.work or tempfile.mkdtemp(prefix="fr_mixed_")
+    if a.operators:
+        operator_fixture(a.ref, work)
+        return
     if a.restart_read:
         restart_read_fixture(a.ref, work)
         return

@@ -96,6 +96,34 @@ def test_element_operators_match_the_reference(case):
                 assert _maxrel(ops["opp_%d" % w][d], a[T + "opp_%d_%d" % (w, d)]) <= tol, (et, w, d)
 
 
+@pytest.mark.parametrize("kind,order", [("triquad", 1), ("triquad", 4), ("triquad", 5), ("pritet", 1), ("pritet", 4),
+                                        ("pritet", 5)])
+def test_element_operators_match_the_reference_at_other_orders(kind, order):
+    """Orders 1, 4 and 5 with the DG correction, against the reference's own
+    operators (tests/golden/ops_<kind>_p<order>.npz, make_mixed.py
+    --operators).  At order 5 the triangle lift (triangles and the prisms'
+    triangular faces) follows the reference's 5-point edge rule."""
+    z = np.load(os.path.join(HERE, "golden", "ops_%s_p%d.npz" % (kind, order)))
+    meta = json.loads(str(z["meta"]))
+    if kind == "triquad":
+        opts = X.ElementOpts(upts_type_tri=meta["tri_upts"], fpts_type_tri=meta["tri_fpts"], vcjh_scheme_tri=1)
+        types, D = (X.TRI, X.QUAD), 2
+    else:
+        opts = X.ElementOpts(upts_type_tet=meta["tet_upts"], vcjh_scheme_tet=1, vcjh_scheme_tri=1,
+                             vcjh_scheme_pri_1d=1)
+        types, D = (X.TET, X.PRISM), 3
+    for et in types:
+        T = "t%d_" % et
+        ops = X.element_operators(et, order, opts)
+        assert ops["opp_0"].shape == z[T + "opp_0"].shape
+        assert _maxrel(ops["opp_0"], z[T + "opp_0"]) <= 1e-13
+        assert _maxrel(ops["opp_6"], z[T + "opp_6"]) <= 1e-13
+        assert _maxrel(ops["opp_3"], z[T + "opp_3"]) <= 1e-12, et
+        for w, tol in ((1, 1e-13), (2, 1e-13), (4, 1e-13), (5, 1e-12)):
+            for d in range(D):
+                assert _maxrel(ops["opp_%d" % w][d], z[T + "opp_%d_%d" % (w, d)]) <= tol, (et, w, d)
+
+
 def test_triangle_lift_is_exact():
     """The DG lift of a unit jump at edge point m, in the orthonormal basis,
     has the coefficients int_edge phi_i l_m ds; checked with an independent
