@@ -400,14 +400,20 @@ def restart_read_fixture(ref, work):
 def operator_fixture(ref, work):
     """The reference's element operators opp_0 .. opp_6 (per-type set-up of
     eles_tris / eles_tets / eles_pris, src/eles.cpp:3620-4052) at the orders
-    the mixed fixtures do not cover, on small meshes of the fixtures' kinds
-    with the DG correction (vcjh scheme 1), kept as ops_<kind>_p<order>.npz."""
-    for kind, order in (("triquad", 1), ("triquad", 4), ("triquad", 5), ("pritet", 1), ("pritet", 4),
-                        ("pritet", 5)):
+    and correction schemes the mixed fixtures do not cover, on small meshes
+    of the fixtures' kinds, kept as ops_<kind>_p<order>.npz (DG, vcjh scheme
+    1) or ops_<kind>_p<order>_s<scheme>.npz.  Tets take the scheme, and so do
+    triangles and the prisms' triangles where the reference defines it
+    (orders 2-4; src/funcs.cpp:586-635)."""
+    for kind, order, scheme in (("triquad", 1, 1), ("triquad", 4, 1), ("triquad", 5, 1), ("pritet", 1, 1),
+                                ("pritet", 4, 1), ("pritet", 5, 1), ("triquad", 4, 2), ("pritet", 4, 3),
+                                ("pritet", 5, 4)):
         two_d = kind == "triquad"
+        tri_scheme = scheme if order <= 4 else 1
         base = [c for c in (CASES_2D if two_d else CASES) if c["name"] == "mixed_%s_p2" % kind][0]
-        c = dict(base, order=order, steps=1, vcjh_tri=1)
-        d = os.path.join(work, "ops_%s_p%d" % (kind, order))
+        c = dict(base, order=order, steps=1, vcjh_tri=tri_scheme)
+        tag = "ops_%s_p%d" % (kind, order) + ("" if scheme == 1 else "_s%d" % scheme)
+        d = os.path.join(work, tag)
         os.makedirs(d, exist_ok=True)
         if two_d:
             lo, hi = (0.0, 0.0), (2 * np.pi, 2 * np.pi)
@@ -420,7 +426,8 @@ def operator_fixture(ref, work):
             xv, eles = mixed_cells(c["kind"], c["n"], lo, hi, c["jitter"], seed=12345)
             write_mixed_gambit(os.path.join(d, "mesh.neu"), xv, eles, None)
             vals = input_values_3d(c, [hi[i] - lo[i] for i in range(3)])
-            vals["vcjh_scheme_tet"] = 1
+            vals["vcjh_scheme_tet"] = scheme
+            vals["vcjh_scheme_tri"] = tri_scheme
             ic, kinds = "tgv_mach01", (2, 3)
         G.write_input(os.path.join(d, "input"), os.path.join(ref, G.TGV_INPUT), vals)
         out = os.path.join(d, "out")
@@ -435,9 +442,9 @@ def operator_fixture(ref, work):
         keep = {k: np.asfortranarray(v) for k, v in arr.items()
                 if k[:3] in ("t%d_" % kinds[0], "t%d_" % kinds[1]) and k[3:].startswith("opp_")}
         meta = dict(kind=kind, order=order, tri_upts=c.get("tri_upts"), tri_fpts=c.get("tri_fpts"),
-                    tet_upts=c.get("tet_upts"), vcjh=1)
-        np.savez_compressed(os.path.join(HERE, "ops_%s_p%d.npz" % (kind, order)), meta=json.dumps(meta), **keep)
-        print("operators", kind, order, sorted(keep))
+                    tet_upts=c.get("tet_upts"), vcjh_tet=scheme, vcjh_tri=tri_scheme)
+        np.savez_compressed(os.path.join(HERE, tag + ".npz"), meta=json.dumps(meta), **keep)
+        print("operators", tag, len(keep))
 
 
 # 2-D quadrilateral boxes with boundaries on every side (side order x-, x+,
@@ -505,7 +512,7 @@ def main():
     ap.add_argument("--restart-only", action="store_true",
                     help="write only the reference's restart files of mixed_triquad_p2 and mixed_pritet_p2")
     ap.add_argument("--operators", action="store_true",
-                    help="write only the reference's element operators at orders 1, 4 and 5")
+                    help="write only the reference's element operators at orders 1, 4 and 5 and other schemes")
     ap.add_argument("--restart-read", action="store_true",
                     help="write only the fixtures of the reference reading the order-2 restart files at order 3")
     a = ap.parse_args()

@@ -96,21 +96,24 @@ def test_element_operators_match_the_reference(case):
                 assert _maxrel(ops["opp_%d" % w][d], a[T + "opp_%d_%d" % (w, d)]) <= tol, (et, w, d)
 
 
-@pytest.mark.parametrize("kind,order", [("triquad", 1), ("triquad", 4), ("triquad", 5), ("pritet", 1), ("pritet", 4),
-                                        ("pritet", 5)])
-def test_element_operators_match_the_reference_at_other_orders(kind, order):
-    """Orders 1, 4 and 5 with the DG correction, against the reference's own
-    operators (tests/golden/ops_<kind>_p<order>.npz, make_mixed.py
-    --operators).  At order 5 the triangle lift (triangles and the prisms'
-    triangular faces) follows the reference's 5-point edge rule."""
-    z = np.load(os.path.join(HERE, "golden", "ops_%s_p%d.npz" % (kind, order)))
+@pytest.mark.parametrize("tag", ["triquad_p1", "triquad_p4", "triquad_p5", "pritet_p1", "pritet_p4", "pritet_p5",
+                                 "triquad_p4_s2", "pritet_p4_s3", "pritet_p5_s4"])
+def test_element_operators_match_the_reference_at_other_orders(tag):
+    """Orders 1, 4 and 5 with the DG correction, and the SD-like, HU-like
+    and c_+ schemes at orders 4 and 5, against the reference's own operators
+    (tests/golden/ops_<tag>.npz, make_mixed.py --operators).  At order 5 the
+    triangle lift (triangles and the prisms' triangular faces) follows the
+    reference's 5-point edge rule."""
+    z = np.load(os.path.join(HERE, "golden", "ops_%s.npz" % tag))
     meta = json.loads(str(z["meta"]))
-    if kind == "triquad":
-        opts = X.ElementOpts(upts_type_tri=meta["tri_upts"], fpts_type_tri=meta["tri_fpts"], vcjh_scheme_tri=1)
+    order = meta["order"]
+    if meta["kind"] == "triquad":
+        opts = X.ElementOpts(upts_type_tri=meta["tri_upts"], fpts_type_tri=meta["tri_fpts"],
+                             vcjh_scheme_tri=meta["vcjh_tri"])
         types, D = (X.TRI, X.QUAD), 2
     else:
-        opts = X.ElementOpts(upts_type_tet=meta["tet_upts"], vcjh_scheme_tet=1, vcjh_scheme_tri=1,
-                             vcjh_scheme_pri_1d=1)
+        opts = X.ElementOpts(upts_type_tet=meta["tet_upts"], vcjh_scheme_tet=meta["vcjh_tet"],
+                             vcjh_scheme_tri=meta["vcjh_tri"], vcjh_scheme_pri_1d=1)
         types, D = (X.TET, X.PRISM), 3
     for et in types:
         T = "t%d_" % et
