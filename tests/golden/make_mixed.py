@@ -439,10 +439,11 @@ def operator_fixture(ref, work):
             print(r.stdout[-3000:], r.stderr[-3000:])
             raise RuntimeError("harness failed for operators of %s P%d" % (kind, order))
         arr, _ = G.load_npy_dir(out)
+        metrics = ("detjac_upts", "JGinv_upts", "tdA_fpts", "norm_fpts")
         keep = {k: np.asfortranarray(v) for k, v in arr.items()
-                if k[:3] in ("t%d_" % kinds[0], "t%d_" % kinds[1]) and k[3:].startswith("opp_")}
-        meta = dict(kind=kind, order=order, tri_upts=c.get("tri_upts"), tri_fpts=c.get("tri_fpts"),
-                    tet_upts=c.get("tet_upts"), vcjh_tet=scheme, vcjh_tri=tri_scheme)
+                if k[:3] in ("t%d_" % kinds[0], "t%d_" % kinds[1]) and (k[3:].startswith("opp_") or k[3:] in metrics)}
+        meta = dict(kind=kind, order=order, n=list(c["n"]), jitter=c["jitter"], tri_upts=c.get("tri_upts"),
+                    tri_fpts=c.get("tri_fpts"), tet_upts=c.get("tet_upts"), vcjh_tet=scheme, vcjh_tri=tri_scheme)
         np.savez_compressed(os.path.join(HERE, tag + ".npz"), meta=json.dumps(meta), **keep)
         print("operators", tag, len(keep))
 

@@ -101,7 +101,7 @@ def test_element_operators_match_the_reference(case):
 def test_element_operators_match_the_reference_at_other_orders(tag):
     """Orders 1, 4 and 5 with the DG correction, and the SD-like, HU-like
     and c_+ schemes at orders 4 and 5, against the reference's own operators
-    (tests/golden/ops_<tag>.npz, make_mixed.py --operators).  At order 5 the
+    and metrics (tests/golden/ops_<tag>.npz, make_mixed.py --operators).  At order 5 the
     triangle lift (triangles and the prisms' triangular faces) follows the
     reference's 5-point edge rule."""
     z = np.load(os.path.join(HERE, "golden", "ops_%s.npz" % tag))
@@ -115,6 +115,14 @@ def test_element_operators_match_the_reference_at_other_orders(tag):
         opts = X.ElementOpts(upts_type_tet=meta["tet_upts"], vcjh_scheme_tet=meta["vcjh_tet"],
                              vcjh_scheme_tri=meta["vcjh_tri"], vcjh_scheme_pri_1d=1)
         types, D = (X.TET, X.PRISM), 3
+    # the metrics of the library's own set-up of the same mesh
+    xv, cells, period, bfaces, _ = fixture_mesh(dict(meta, vcjh_tri=meta["vcjh_tri"]))
+    M = X.MixedMesh(order, xv, cells, period, bfaces, opts)
+    assert sorted(M.types) == sorted(types)
+    for et, m in M.types.items():
+        for k in ("JGinv_upts", "detjac_upts", "tdA_fpts", "norm_fpts"):
+            assert m[k].shape == z["t%d_%s" % (et, k)].shape
+            assert rel(m[k], z["t%d_%s" % (et, k)]) <= 1e-15, (et, k)
     for et in types:
         T = "t%d_" % et
         ops = X.element_operators(et, order, opts)
