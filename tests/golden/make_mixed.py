@@ -355,17 +355,18 @@ def input_values_3d(c, L):
 
 
 def restart_read_fixture(ref, work):
-    """The reference reading its own order-2 restart files of
-    mixed_triquad_p2 and mixed_pritet_p2 (rest_<name>.dat) on the same meshes
-    set up at order 3: read_restart with each type's read_restart_info and
-    eles::set_opp_r (src/solver.cpp:390-445, src/eles_tris.cpp:511-543,
-    src/eles_tets.cpp:749-780, src/eles_pris.cpp:655-698,
-    src/eles.cpp:4135-4153) -> every type's disu_upts(0) at order 3, kept as
-    rest_read_<kind>_p2_to_p3.npz."""
+    """The reference reading its own restart files of mixed_triquad_p2 and
+    mixed_pritet_p2 (order 2, read at order 3) and of mixed_hexpri_p3 (order
+    3, read at order 2) on the same meshes: read_restart with each type's
+    read_restart_info and eles::set_opp_r (src/solver.cpp:390-445,
+    src/eles_tris.cpp:511-543, src/eles_tets.cpp:749-780,
+    src/eles_pris.cpp:655-698, src/eles.cpp:4135-4153) -> every type's
+    disu_upts(0) at the new order, kept as rest_read_<kind>_p<a>_to_p<b>.npz."""
     import shutil
-    for name in ("mixed_triquad_p2", "mixed_pritet_p2"):
+    for name, new_order in (("mixed_triquad_p2", 3), ("mixed_pritet_p2", 3), ("mixed_hexpri_p3", 2)):
         two_d = name == "mixed_triquad_p2"
-        c = dict([c for c in (CASES_2D if two_d else CASES) if c["name"] == name][0], order=3)
+        c0 = [c for c in (CASES_2D if two_d else CASES) if c["name"] == name][0]
+        c = dict(c0, order=new_order)
         d = os.path.join(work, "restart_read_" + c["kind"])
         os.makedirs(d, exist_ok=True)
         shutil.copy(os.path.join(HERE, "rest_%s.dat" % name), os.path.join(d, "Rest_%09d_p%04d.dat" % (c["steps"], 0)))
@@ -380,7 +381,7 @@ def restart_read_fixture(ref, work):
             xv, eles = mixed_cells(c["kind"], c["n"], lo, hi, c["jitter"], seed=12345)
             write_mixed_gambit(os.path.join(d, "mesh.neu"), xv, eles, None)
             vals = input_values_3d(c, [hi[i] - lo[i] for i in range(3)])
-            kinds = (2, 3)
+            kinds = (2, 3) if c["kind"] == "pritet" else (3, 4)
         vals.update({"restart_flag": 1, "restart_iter": c["steps"], "n_restart_files": 1})
         G.write_input(os.path.join(d, "input"), os.path.join(ref, G.TGV_INPUT), vals)
         out = os.path.join(d, "out")
@@ -391,8 +392,8 @@ def restart_read_fixture(ref, work):
             print(r.stdout[-3000:], r.stderr[-3000:])
             raise RuntimeError("harness failed reading a restart file")
         arr, _ = G.load_npy_dir(out)
-        keep = {"t%d_u_p3_ref" % t: np.asfortranarray(arr["t%d_disu_upts_init" % t]) for t in kinds}
-        np.savez_compressed(os.path.join(HERE, "rest_read_%s_p2_to_p3.npz" % c["kind"]),
+        keep = {"t%d_u_ref" % t: np.asfortranarray(arr["t%d_disu_upts_init" % t]) for t in kinds}
+        np.savez_compressed(os.path.join(HERE, "rest_read_%s_p%d_to_p%d.npz" % (c["kind"], c0["order"], new_order)),
                             time=c["steps"] * c["dt"], **keep)
         print("restart read fixture", c["kind"], {k: v.shape for k, v in keep.items()})
 

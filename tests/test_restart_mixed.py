@@ -228,23 +228,23 @@ def test_fused_run_continues_from_a_restart_file(name, tmp_path):
             assert rel(m2.get_state(et), m1.get_state(et)) <= 1e-12, (path, et)
 
 
-@pytest.mark.parametrize("name", ["mixed_triquad_p2", "mixed_pritet_p2"])
-def test_order_change_matches_the_reference_reading_its_own_file(name):
-    """The reference set up at order 3 on a fixture's mesh, restarted from
-    its own order-2 file (rest_read_<kind>_p2_to_p3.npz, made by
+@pytest.mark.parametrize("name,order", [("mixed_triquad_p2", 3), ("mixed_pritet_p2", 3), ("mixed_hexpri_p3", 2)])
+def test_order_change_matches_the_reference_reading_its_own_file(name, order):
+    """The reference set up at another order on a fixture's mesh, restarted
+    from its own restart file (rest_read_<kind>_p<a>_to_p<b>.npz, made by
     make_mixed.py --restart-read), against MixedMesh.read_restart of the same
-    file at order 3: every element type through the nodal bases on the
-    file's points."""
+    file at that order: every element type through the nodal bases on the
+    file's points, up (2 -> 3) and down (3 -> 2)."""
     from test_mixed_setup import fixture_mesh
     meta, _, _ = fixture(name)
-    want = np.load(os.path.join(GOLDEN, "rest_read_%s_p2_to_p3.npz" % meta["kind"]))
+    want = np.load(os.path.join(GOLDEN, "rest_read_%s_p%d_to_p%d.npz" % (meta["kind"], meta["order"], order)))
     xv, cells, period, bfaces, opts = fixture_mesh(meta)
-    M3 = X.MixedMesh(3, xv, cells, period, bfaces, opts)
-    u, t = M3.read_restart(os.path.join(GOLDEN, "rest_%s.dat" % name))
+    M = X.MixedMesh(order, xv, cells, period, bfaces, opts)
+    u, t = M.read_restart(os.path.join(GOLDEN, "rest_%s.dat" % name))
     assert abs(t - float(want["time"])) < 1e-15
-    assert sorted(u) == sorted(int(k[1]) for k in want.files if k.endswith("_u_p3_ref"))
+    assert sorted(u) == sorted(int(k[1]) for k in want.files if k.endswith("_u_ref"))
     for et in u:
-        assert rel(u[et], want["t%d_u_p3_ref" % et]) <= 1e-14, (et, rel(u[et], want["t%d_u_p3_ref" % et]))
+        assert rel(u[et], want["t%d_u_ref" % et]) <= 1e-14, (et, rel(u[et], want["t%d_u_ref" % et]))
 
 
 @pytest.mark.parametrize("et,order", [(0, 2), (0, 4), (1, 3), (2, 2), (2, 3), (3, 2), (3, 4), (4, 3)])
