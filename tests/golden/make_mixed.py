@@ -442,9 +442,12 @@ def operator_fixture(ref, work):
         arr, _ = G.load_npy_dir(out)
         metrics = ("detjac_upts", "JGinv_upts", "tdA_fpts", "norm_fpts")
         keep = {k: np.asfortranarray(v) for k, v in arr.items()
-                if k[:3] in ("t%d_" % kinds[0], "t%d_" % kinds[1]) and (k[3:].startswith("opp_") or k[3:] in metrics)}
+                if (k[:3] in ("t%d_" % kinds[0], "t%d_" % kinds[1]) and (k[3:].startswith("opp_") or k[3:] in metrics))
+                or k.startswith("int_inters_")}
+        inters = sorted(int(k[len("int_inters_"):]) for k in keep if k.startswith("int_inters_"))
         meta = dict(kind=kind, order=order, n=list(c["n"]), jitter=c["jitter"], tri_upts=c.get("tri_upts"),
-                    tri_fpts=c.get("tri_fpts"), tet_upts=c.get("tet_upts"), vcjh_tet=scheme, vcjh_tri=tri_scheme)
+                    tri_fpts=c.get("tri_fpts"), tet_upts=c.get("tet_upts"), vcjh_tet=scheme, vcjh_tri=tri_scheme,
+                    inters=inters)
         np.savez_compressed(os.path.join(HERE, tag + ".npz"), meta=json.dumps(meta), **keep)
         print("operators", tag, len(keep))
 

@@ -100,8 +100,9 @@ def test_element_operators_match_the_reference(case):
                                  "triquad_p4_s2", "pritet_p4_s3", "pritet_p5_s4"])
 def test_element_operators_match_the_reference_at_other_orders(tag):
     """Orders 1, 4 and 5 with the DG correction, and the SD-like, HU-like
-    and c_+ schemes at orders 4 and 5, against the reference's own operators
-    and metrics (tests/golden/ops_<tag>.npz, make_mixed.py --operators).  At order 5 the
+    and c_+ schemes at orders 4 and 5, against the reference's own operators,
+    metrics and interface wiring (tests/golden/ops_<tag>.npz, make_mixed.py
+    --operators).  At order 5 the
     triangle lift (triangles and the prisms' triangular faces) follows the
     reference's 5-point edge rule."""
     z = np.load(os.path.join(HERE, "golden", "ops_%s.npz" % tag))
@@ -123,6 +124,13 @@ def test_element_operators_match_the_reference_at_other_orders(tag):
         for k in ("JGinv_upts", "detjac_upts", "tdA_fpts", "norm_fpts"):
             assert m[k].shape == z["t%d_%s" % (et, k)].shape
             assert rel(m[k], z["t%d_%s" % (et, k)]) <= 1e-15, (et, k)
+    # and its interface wiring, left and right sides included
+    ref = [z["int_inters_%d" % i] for i in meta["inters"]]
+    assert [w.shape for w in M.int_inters] == [w.shape for w in ref]
+    for w, r in zip(M.int_inters, ref):
+        left_right = lambda x: {tuple(x[:3, q, i]): tuple(x[3:, q, i])  # noqa: E731
+                                for i in range(x.shape[2]) for q in range(x.shape[1])}
+        assert left_right(w) == left_right(r)
     for et in types:
         T = "t%d_" % et
         ops = X.element_operators(et, order, opts)
